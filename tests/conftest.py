@@ -1,0 +1,35 @@
+"""Shared test setup: the `gpu` marker, import paths and the fixtures of the golden box."""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+# Settings of the reference's regression case ff_small_box (regression_cases.py:253-262)
+SMALL_BOX_SETTINGS = dict(
+    cutoff=0.6, ewald_beta=6.0, pme_grid=(32, 32, 32), pme_order=6, lj_lrc=True, dipole_tol=1e-10, max_iter=500
+)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def golden_small_box():
+    return dict(np.load(os.path.join(GOLDEN, "ff_small_box.npz")))
+
+
+@pytest.fixture(scope="session")
+def small_box_system():
+    from pgm_jax_b200.systems import small_box
+
+    return small_box(0)
