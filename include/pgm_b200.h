@@ -1,0 +1,152 @@
+/*
+ * pgm_b200.h -- C ABI of the B200 (sm_100a) pGM electrostatics engine.
+ *
+ * One handle holds one force field over a batch of independent periodic systems (one system, or
+ * REMD replicas, PIMD beads, boxes of uneven sizes), each with its own box and PME mesh, evaluated
+ * together by the same kernels.  All array arguments of the compute calls are DEVICE pointers
+ * owned by the caller (as the buffers of a jax.ffi custom call are), concatenated over the systems
+ * in system order; the *_host variants take host pointers and copy.
+ *
+ * Units: nm, e, e nm, nm^3, kJ/mol, kJ/mol/nm (pgm_jax/md/forcefield.py:100).  Boxes are
+ * lower-triangular, lattice vectors as rows, in reduced form (pgm_jax/md/box.py:32).
+ *
+ * Errors: every entry point returns a PgmStatus; nothing is thrown across the boundary.
+ * Per-system conditions of a step (row overflow, CG not converged, non-finite energy) come back in
+ * the `status` output word of each system, as the reference reports them in Result.overflow and
+ * Result.residual (forcefield.py:716-746) and its driver checks for non-finite energies.
+ */
+#ifndef PGM_B200_H
+#define PGM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PGM_OK = 0,
+    PGM_ERR_INVALID = 1,   /* bad argument or setting (ValueError at construction, forcefield.py:902-906) */
+    PGM_ERR_CUDA = 2,      /* a CUDA runtime error; pgm_last_error() has the text */
+    PGM_ERR_NO_DEVICE = 3,
+    PGM_ERR_UNSUPPORTED = 4
+} PgmStatus;
+
+/* Bits of the per-system status word of a step. */
+#define PGM_STATUS_ROW_OVERFLOW 0x1u   /* a row had more in-cutoff pairs than the capacity: results invalid, resize and repeat */
+#define PGM_STATUS_CG_MAXITER   0x2u   /* CG stopped at max_iter above the tolerance */
+#define PGM_STATUS_NONFINITE    0x4u   /* non-finite energy */
+#define PGM_STATUS_BAD_BOX      0x8u   /* box not lower triangular / too small for the cutoff */
+
+/* Settings of one handle: the MDSettings fields of the path (forcefield.py:386-516). */
+typedef struct {
+    int elec;           /* 0 "q", 1 "qp", 2 "qi", 3 "qpi" (options.py ELEC_LEVELS) */
+    int vdw;            /* 0 "none", 1 "lj" */
+    int lj_lrc;         /* Amber vdwmeth=1 tail (lj.py:87) */
+    int precision;      /* 0 "mixed" (FP32 kernels, FP64 reductions), 1 "double" */
+    double cutoff;      /* pair cutoff [nm] (Cutoffs.cutoff) */
+    double ewald_beta;  /* [1/nm] (PMESettings.ewald_beta) */
+    int pme_order;      /* 4, 6 or 8 (PMESettings.order) */
+    double dipole_tol;  /* max|alpha r| / mean|alpha b| (Induction.tol) */
+    int max_iter;       /* Induction.max_iter */
+    int predictor;      /* 0 "none", 3 "mu3", 4 "mu4" (Induction.predictor) */
+    int fused;          /* Induction.fused */
+    int norm_refresh;   /* Induction.norm_refresh */
+    double peek;        /* Induction.peek */
+    int row_capacity;   /* pairs kept per row; 0: sized from the density (PGMForceField.size_rows) */
+} PgmSettings;
+
+/* One system of the batch: topology and parameters (host arrays, copied at creation). */
+typedef struct {
+    int n_atoms;
+    int n_mol;
+    const int32_t *mol_start;   /* (n_mol + 1) first atom of every molecule; molecules contiguous */
+    const double *q;            /* (n_atoms) [e] */
+    const double *radius;       /* (n_atoms) Gaussian radii [nm] */
+    const double *alpha;        /* (n_atoms) polarizabilities [nm^3], > 0 */
+    const double *lj_rmin_half; /* (n_atoms) LJ R* [nm] */
+    const double *lj_sqrt_eps;  /* (n_atoms) [sqrt(kJ/mol)] */
+    const double *masses;       /* (n_atoms) [amu] (molecular virial) */
+    int n_cov;
+    const int32_t *cov_i;       /* (n_cov) atom carrying the covalent dipole (local index) */
+    const int32_t *cov_j;       /* (n_cov) atom it points to (local index) */
+    const double *cov_c;        /* (n_cov) strength [e nm] */
+    int pme_grid[3];            /* K1, K2, K3: even, factors 2, 3, 5 only, <= 256 */
+    double box0[9];             /* a box of the run, to size the cell grid [nm] */
+} PgmSystemDesc;
+
+/* Induced-dipole solver state (InductionState, forcefield.py:679-713), device pointers, in/out. */
+typedef struct {
+    double *mu;      /* (N, 3) converged dipoles of the last solve [e nm] */
+    double *hist;    /* (4, N, 3) dipoles of the last steps, newest first */
+    int32_t *count;  /* (n_systems) steps recorded */
+    double *norm;    /* (n_systems) mean|alpha b| of the last unfused step */
+} PgmInduction;
+
+/* Outputs of a step (Result, forcefield.py:716-746), device pointers; any may be NULL. */
+typedef struct {
+    double *energy;       /* (n_systems, 3) elec, vdw, total [kJ/mol] */
+    double *forces;       /* (N, 3) [kJ/mol/nm] */
+    double *virial;       /* (n_systems, 3, 3) dE/d eps at fixed mu minus the LJ tail impulse [kJ/mol] */
+    int32_t *iterations;  /* (n_systems) CG iterations */
+    double *residual;     /* (n_systems) max|alpha r| / norm before the peek step */
+    uint32_t *status;     /* (n_systems) PGM_STATUS_* bits */
+} PgmOutputs;
+
+typedef struct PgmHandle PgmHandle;
+
+/* PGMForceField.__init__ (forcefield.py:868): settings and the systems of the batch. */
+PgmStatus pgm_create(const PgmSettings *settings, const PgmSystemDesc *systems, int n_systems, int device,
+                     PgmHandle **out);
+PgmStatus pgm_destroy(PgmHandle *h);
+
+/* PGMForceField.compute (forcefield.py:2489): solve the induced dipoles from the predictor state,
+ * then energies, forces and the molecular virial (strain_derivative, forcefield.py:2628, at the
+ * returned mu).  pos (N, 3), box (n_systems, 3, 3).  idx: candidate partners (N, idx_width),
+ * padding N_system (the reference's neighbour-list rows, local indices), or NULL to let the engine
+ * find the pairs with its own cell list.  stream: a cudaStream_t (NULL: the legacy stream). */
+PgmStatus pgm_compute(PgmHandle *h, void *stream, const double *pos, const double *box, const int32_t *idx,
+                      int idx_width, PgmInduction *ind, PgmOutputs *out);
+
+/* pgm_compute with host pointers (copies in and out; ind arrays and out arrays on the host). */
+PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, PgmInduction *ind, PgmOutputs *out);
+
+/* PGMForceField.energy (forcefield.py:2562): energy only, CG started from ind->mu (plain start), no
+ * history push; ind->mu receives the converged dipoles.  energy (n_systems, 3). */
+PgmStatus pgm_energy(PgmHandle *h, void *stream, const double *pos, const double *box, const int32_t *idx,
+                     int idx_width, PgmInduction *ind, double *energy, int32_t *iterations, uint32_t *status);
+
+/* PGMForceField.energy_fixed_mu + strain_derivative (forcefield.py:2249, 2628): energies (n_systems,
+ * 3), forces (N, 3) and molecular virial (n_systems, 3, 3) with the induced dipoles held at mu
+ * (N, 3).  Any output may be NULL. */
+PgmStatus pgm_energy_fixed_mu(PgmHandle *h, void *stream, const double *pos, const double *box, const int32_t *idx,
+                              int idx_width, const double *mu, double *energy, double *forces, double *virial,
+                              uint32_t *status);
+
+/* PGMForceField._field (forcefield.py:1428): the total field -dU/dd (N, 3) [e/nm^2] of charges
+ * (q != 0: the system's charges; 0: none) and dipoles d (N, 3). */
+PgmStatus pgm_field(PgmHandle *h, void *stream, const double *pos, const double *box, int with_charges,
+                    const double *d, double *field);
+
+/* PGMForceField.size_rows / grow_rows (forcefield.py:1269-1296): set the row capacity (pairs per
+ * row, rounded up to a multiple of 32); 0 restores the automatic size. */
+PgmStatus pgm_set_row_capacity(PgmHandle *h, int capacity);
+int pgm_row_capacity(const PgmHandle *h);
+
+/* Largest in-cutoff pair count of any row in the last step (for size_rows). */
+int pgm_max_row_count(PgmHandle *h);
+
+/* Total atoms, systems. */
+int pgm_num_atoms(const PgmHandle *h);
+int pgm_num_systems(const PgmHandle *h);
+
+/* Text of the last error of this thread. */
+const char *pgm_last_error(void);
+
+/* Kernels launched by the last pgm_compute / pgm_energy / pgm_field call (launch accounting). */
+long long pgm_last_launch_count(const PgmHandle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

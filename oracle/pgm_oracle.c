@@ -783,7 +783,7 @@ static void energy_forces(ctx_t *C, const double *pos, const double *H, const do
     pme_influence_virial(&C->P, sys->q, d, n, Wi);
     for (int k = 0; k < 9; ++k) W[k] += Wr[k] + KE * Wi[k];
     /* covalent-dipole frames: p_i = sum c unit(r_j - r_i) pulled back (vjp of forcefield.py:1032-1042) */
-    for (int m = 0; m < sys->ncov; ++m) {
+    for (int m = 0; m < (s->perm ? sys->ncov : 0); ++m) {
         int i = sys->cov_i[m], j = sys->cov_j[m];
         double v[3] = {pos[j * 3] - pos[i * 3], pos[j * 3 + 1] - pos[i * 3 + 1], pos[j * 3 + 2] - pos[i * 3 + 2]};
         min_image(v, H);

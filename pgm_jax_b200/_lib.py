@@ -1,0 +1,97 @@
+"""ctypes binding of the engine's C ABI (include/pgm_b200.h).
+
+The library is the product: there is no fallback.  Loading fails loudly when it is missing.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .build import LIB
+
+_i32 = C.c_int32
+_pd = C.POINTER(C.c_double)
+_pi = C.POINTER(C.c_int32)
+_pu = C.POINTER(C.c_uint32)
+
+# every symbol the header declares (tests check the library exports them)
+EXPORTS = (
+    "pgm_create", "pgm_destroy", "pgm_compute", "pgm_compute_host", "pgm_energy", "pgm_energy_fixed_mu", "pgm_field",
+    "pgm_set_row_capacity", "pgm_row_capacity", "pgm_max_row_count", "pgm_num_atoms", "pgm_num_systems",
+    "pgm_last_error", "pgm_last_launch_count",
+)
+
+STATUS_ROW_OVERFLOW = 0x1
+STATUS_CG_MAXITER = 0x2
+STATUS_NONFINITE = 0x4
+STATUS_BAD_BOX = 0x8
+
+
+class PgmSettings(C.Structure):
+    _fields_ = [
+        ("elec", C.c_int), ("vdw", C.c_int), ("lj_lrc", C.c_int), ("precision", C.c_int), ("cutoff", C.c_double),
+        ("ewald_beta", C.c_double), ("pme_order", C.c_int), ("dipole_tol", C.c_double), ("max_iter", C.c_int),
+        ("predictor", C.c_int), ("fused", C.c_int), ("norm_refresh", C.c_int), ("peek", C.c_double),
+        ("row_capacity", C.c_int),
+    ]
+
+
+class PgmSystemDesc(C.Structure):
+    _fields_ = [
+        ("n_atoms", C.c_int), ("n_mol", C.c_int), ("mol_start", _pi), ("q", _pd), ("radius", _pd), ("alpha", _pd),
+        ("lj_rmin_half", _pd), ("lj_sqrt_eps", _pd), ("masses", _pd), ("n_cov", C.c_int), ("cov_i", _pi),
+        ("cov_j", _pi), ("cov_c", _pd), ("pme_grid", C.c_int * 3), ("box0", C.c_double * 9),
+    ]
+
+
+class PgmInduction(C.Structure):
+    _fields_ = [("mu", C.c_void_p), ("hist", C.c_void_p), ("count", C.c_void_p), ("norm", C.c_void_p)]
+
+
+class PgmOutputs(C.Structure):
+    _fields_ = [
+        ("energy", C.c_void_p), ("forces", C.c_void_p), ("virial", C.c_void_p), ("iterations", C.c_void_p),
+        ("residual", C.c_void_p), ("status", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libpgm_b200.so (built in-tree by pgm_jax_b200.build); raise if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB
+    if not os.path.exists(p):
+        raise RuntimeError(f"the engine library {p} is not built: run pgm_jax_b200.build.build() (nvcc, sm_100a)")
+    lib = C.CDLL(p)
+    H = C.c_void_p
+    vp = C.c_void_p
+    lib.pgm_create.argtypes = [C.POINTER(PgmSettings), C.POINTER(PgmSystemDesc), C.c_int, C.c_int, C.POINTER(H)]
+    lib.pgm_destroy.argtypes = [H]
+    lib.pgm_compute.argtypes = [H, vp, vp, vp, vp, C.c_int, C.POINTER(PgmInduction), C.POINTER(PgmOutputs)]
+    lib.pgm_compute_host.argtypes = [H, vp, vp, C.POINTER(PgmInduction), C.POINTER(PgmOutputs)]
+    lib.pgm_energy.argtypes = [H, vp, vp, vp, vp, C.c_int, C.POINTER(PgmInduction), vp, vp, vp]
+    lib.pgm_energy_fixed_mu.argtypes = [H, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp, vp]
+    lib.pgm_field.argtypes = [H, vp, vp, vp, C.c_int, vp, vp]
+    lib.pgm_set_row_capacity.argtypes = [H, C.c_int]
+    lib.pgm_row_capacity.argtypes = [H]
+    lib.pgm_max_row_count.argtypes = [H]
+    lib.pgm_num_atoms.argtypes = [H]
+    lib.pgm_num_systems.argtypes = [H]
+    lib.pgm_last_launch_count.argtypes = [H]
+    lib.pgm_last_launch_count.restype = C.c_longlong
+    lib.pgm_last_error.restype = C.c_char_p
+    for n in ("pgm_create", "pgm_destroy", "pgm_compute", "pgm_compute_host", "pgm_energy", "pgm_energy_fixed_mu",
+              "pgm_field", "pgm_set_row_capacity"):
+        getattr(lib, n).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(f"pgm_b200 error {rc}: {load().pgm_last_error().decode()}")

@@ -1,0 +1,744 @@
+// pgm_api.cu -- host side of the B200 pGM engine: the handle, the buffers, the launch sequence
+// of a step and the C ABI declared in include/pgm_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/pgm_b200.h"
+#include "pgm_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+struct CudaError {
+  std::string msg;
+};
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) throw CudaError{std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+template <typename X>
+struct DBuf {
+  X *p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    n = count;
+    if (count) CK(cudaMalloc(&p, sizeof(X) * count));
+  }
+  void upload(const std::vector<X> &v) {
+    alloc(v.size());
+    if (!v.empty()) CK(cudaMemcpy(p, v.data(), sizeof(X) * v.size(), cudaMemcpyHostToDevice));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+// Host copy of the B-spline recursion at f = 0 and the moduli (pme.py:106-131).
+void host_bspline0(int order, double *th) {
+  std::vector<double> d(order + 1, 0.0);
+  double f = 0.0;
+  d[0] = 1.0 - f;
+  d[1] = f;
+  for (int n = 3; n <= order; ++n) {
+    double div = 1.0 / (n - 1.0);
+    d[n - 1] = div * f * d[n - 2];
+    for (int k = 1; k < n - 1; ++k) d[n - k - 1] = div * ((f + k) * d[n - k - 2] + (n - k - f) * d[n - k - 1]);
+    d[0] = div * (1.0 - f) * d[0];
+  }
+  for (int k = 0; k < order; ++k) th[k] = d[k];
+}
+
+std::vector<double> host_moduli(int K, int order) {
+  std::vector<double> th(order), mod(K);
+  host_bspline0(order, th.data());
+  for (int m = 0; m < K; ++m) {
+    double c = 0, s = 0;
+    for (int j = 0; j < order; ++j) {
+      double arg = 2.0 * M_PI * m * j / K;
+      c += th[j] * std::cos(arg);
+      s += th[j] * std::sin(arg);
+    }
+    mod[m] = c * c + s * s;
+  }
+  for (int m = 0; m < K; ++m)
+    if (mod[m] < 1e-7) mod[m] = 0.5 * (mod[(m - 1 + K) % K] + mod[(m + 1) % K]);
+  return mod;
+}
+
+// Radices of a length-K FFT (4s first, then 2, 3, 5); empty if K has another factor.
+std::vector<int> radices(int K) {
+  std::vector<int> r;
+  while (K % 4 == 0) { r.push_back(4); K /= 4; }
+  while (K % 2 == 0) { r.push_back(2); K /= 2; }
+  while (K % 3 == 0) { r.push_back(3); K /= 3; }
+  while (K % 5 == 0) { r.push_back(5); K /= 5; }
+  if (K != 1) r.clear();
+  return r;
+}
+
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual void compute(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
+                       PgmInduction *ind, PgmOutputs *out) = 0;
+  virtual void energy(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
+                      PgmInduction *ind, double *energy, int32_t *iters, uint32_t *status) = 0;
+  virtual void field(cudaStream_t st, const double *pos, const double *box, int with_q, const double *d, double *out) = 0;
+  virtual void fixed_mu(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
+                        const double *mu, double *energy, double *forces, double *virial, uint32_t *status) = 0;
+  virtual void set_capacity(int mc) = 0;
+  virtual int capacity() const = 0;
+  virtual int max_count() = 0;
+  int nt = 0, nsys = 0;
+  long long launches = 0;
+};
+
+template <typename T, int P>
+struct Engine : EngineBase {
+  PgmSettings set;
+  std::vector<pgm::SysInfo> hsys;
+  int nmol_total = 0, ncell = 0, ncov = 0, mc = 0, mc_auto = 0;
+  long long rgrid = 0, cgrid = 0;
+  int tiles_x = 0, tiles_y = 0, tiles_z = 0;
+  size_t smem_x = 0, smem_y = 0, smem_z = 0;
+  int nwblk = 0, ntblk = 0;
+  std::vector<int> natoms;
+
+  DBuf<pgm::SysInfo> d_sys;
+  DBuf<pgm::BoxInfo> d_box;
+  DBuf<pgm::CGSys> d_cg;
+  DBuf<pgm::EnergyAcc> d_eacc;
+  DBuf<unsigned> d_status;
+  DBuf<int> wb_sys, wb_atom0, tb_sys, tb_atom0, tile0_x, tile0_y, tile0_z;
+  DBuf<int> sysid, molid, molfirst, molend, mol_start, cov_start, cov_j, cov_i_flat, cov_j_flat;
+  DBuf<T> q, radius, alpha, ialpha, rminh, seps;
+  DBuf<double> mass, cov_c, cov_c_flat, bmod;
+  DBuf<int4> base;
+  DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D;
+  DBuf<double4> pperm, off, dEdd;
+  DBuf<int> cell_of, slot_of, cell_count, cell_start, cell_atoms;
+  DBuf<int> rn, rnsp, rk, dmax, dany;
+  DBuf<T> rx, ry, rz, rg0, rg1, rg2, rg3;
+  DBuf<T> Q, Phi, Ginf;
+  DBuf<pgm::c2<T>> C, tw;
+  DBuf<double> mu_tmp, forces_tmp, energy_tmp;
+  int *h_any = nullptr;
+
+  ~Engine() {
+    if (h_any) cudaFreeHost(h_any);
+  }
+
+  pgm::Dev<T> dev(const double *pos, const int32_t *idx, int idx_width, double *forces, unsigned *status) {
+    pgm::Dev<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.nsys = nsys; a.nt = nt; a.nmol = nmol_total; a.mc = mc; a.ncell = ncell; a.ncov = ncov;
+    a.order = P;
+    a.induce = (set.elec == 2 || set.elec == 3);
+    a.perm = (set.elec == 1 || set.elec == 3);
+    a.lj = set.vdw == 1;
+    a.lj_lrc = set.lj_lrc;
+    a.beta = set.ewald_beta; a.cutoff = set.cutoff;
+    a.c_self = 4.0 * std::pow(set.ewald_beta, 3) / (3.0 * pgm::SQRT_PI);
+    a.tol = set.dipole_tol; a.peek = set.peek; a.max_iter = set.max_iter;
+    a.sys = d_sys.p; a.box = d_box.p; a.cg = d_cg.p; a.eacc = d_eacc.p; a.status = status;
+    a.wb_sys = wb_sys.p; a.wb_atom0 = wb_atom0.p; a.tb_sys = tb_sys.p; a.tb_atom0 = tb_atom0.p;
+    a.sysid = sysid.p; a.molid = molid.p; a.molfirst = molfirst.p; a.molend = molend.p; a.mol_start = mol_start.p;
+    a.q = q.p; a.radius = radius.p; a.alpha = alpha.p; a.ialpha = ialpha.p; a.rminh = rminh.p; a.seps = seps.p;
+    a.mass = mass.p;
+    a.cov_start = cov_start.p; a.cov_j = cov_j.p; a.cov_i_flat = cov_i_flat.p; a.cov_j_flat = cov_j_flat.p;
+    a.cov_c = cov_c.p; a.cov_c_flat = cov_c_flat.p;
+    a.pos = pos;
+    a.base = base.p; a.frac = frac.p; a.pperm = pperm.p; a.off = off.p;
+    a.cell_of = cell_of.p; a.slot_of = slot_of.p; a.cell_count = cell_count.p; a.cell_start = cell_start.p;
+    a.cell_atoms = cell_atoms.p;
+    a.idx = idx; a.idx_width = idx_width;
+    a.rn = rn.p; a.rnsp = rnsp.p; a.rk = rk.p;
+    a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
+    a.max_count = dmax.p;
+    a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p;
+    a.Q = Q.p; a.Phi = Phi.p; a.Ginf = Ginf.p; a.C = C.p; a.tw = tw.p; a.bmod = bmod.p;
+    a.forces = forces; a.dEdd = dEdd.p;
+    return a;
+  }
+
+  void init(const PgmSettings *s, const PgmSystemDesc *systems, int n) {
+    set = *s;
+    nsys = n;
+    hsys.resize(n);
+    std::vector<int> h_sysid, h_molid, h_molfirst, h_molend, h_molstart, h_covstart, h_covj, h_covi_flat, h_covj_flat;
+    std::vector<T> h_q, h_rad, h_al, h_ial, h_rh, h_se;
+    std::vector<double> h_mass, h_covc, h_covc_flat, h_bmod;
+    std::vector<pgm::c2<T>> h_tw;
+    std::vector<int> twK;
+    std::vector<int> tw_off;
+    int atom0 = 0, mol0 = 0, cell0 = 0;
+    double rho_max = 0;
+    long long rg = 0, cg = 0;
+    auto tw_for = [&](int K) {
+      for (size_t t = 0; t < twK.size(); ++t)
+        if (twK[t] == K) return tw_off[t];
+      int o = (int)h_tw.size();
+      for (int m = 0; m < K; ++m) {
+        pgm::c2<T> c;
+        c.x = T(std::cos(2.0 * M_PI * m / K));
+        c.y = T(-std::sin(2.0 * M_PI * m / K));
+        h_tw.push_back(c);
+      }
+      twK.push_back(K);
+      tw_off.push_back(o);
+      return o;
+    };
+    for (int si = 0; si < n; ++si) {
+      const PgmSystemDesc &d = systems[si];
+      pgm::SysInfo &S = hsys[si];
+      std::memset(&S, 0, sizeof(S));
+      S.atom0 = atom0; S.natom = d.n_atoms; S.mol0 = mol0; S.nmol = d.n_mol;
+      for (int a = 0; a < 3; ++a) S.K[a] = d.pme_grid[a];
+      S.K3h = S.K[2] / 2 + 1;
+      S.rgrid0 = rg; S.cgrid0 = cg;
+      rg += (long long)S.K[0] * S.K[1] * S.K[2];
+      cg += (long long)S.K[0] * S.K[1] * S.K3h;
+      for (int a = 0; a < 3; ++a) {
+        std::vector<int> r = radices(S.K[a]);
+        S.nst[a] = (int)r.size();
+        for (size_t k = 0; k < r.size(); ++k) S.rad[a][k] = r[k];
+        S.tw[a] = tw_for(S.K[a]);
+        S.mod0[a] = (int)h_bmod.size();
+        std::vector<double> mm = host_moduli(S.K[a], P);
+        h_bmod.insert(h_bmod.end(), mm.begin(), mm.end());
+      }
+      // cell grid from the plane heights of box0: cells at least rc / 2 thick
+      const double *H = d.box0;
+      double det = H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) + H[2] * (H[3] * H[7] - H[4] * H[6]);
+      double vol = std::fabs(det);
+      auto cross = [&](int i, int j, double *o) {
+        o[0] = H[i * 3 + 1] * H[j * 3 + 2] - H[i * 3 + 2] * H[j * 3 + 1];
+        o[1] = H[i * 3 + 2] * H[j * 3 + 0] - H[i * 3 + 0] * H[j * 3 + 2];
+        o[2] = H[i * 3 + 0] * H[j * 3 + 1] - H[i * 3 + 1] * H[j * 3 + 0];
+      };
+      double cr[3];
+      int pairs[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+      for (int a = 0; a < 3; ++a) {
+        cross(pairs[a][0], pairs[a][1], cr);
+        double h = vol / std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        S.nc[a] = std::max(1, std::min(64, (int)std::floor(h / (0.5 * set.cutoff))));
+      }
+      S.cell0 = cell0;
+      cell0 += S.nc[0] * S.nc[1] * S.nc[2];
+      rho_max = std::max(rho_max, d.n_atoms / vol);
+      // atoms
+      double sq = 0, sq2 = 0, M[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < d.n_atoms; ++i) {
+        h_sysid.push_back(si);
+        h_q.push_back(T(d.q[i]));
+        h_rad.push_back(T(d.radius[i]));
+        h_al.push_back(T(d.alpha[i]));
+        h_ial.push_back(T(1.0 / d.alpha[i]));
+        h_rh.push_back(T(d.lj_rmin_half[i]));
+        h_se.push_back(T(d.lj_sqrt_eps[i]));
+        h_mass.push_back(d.masses[i]);
+        sq += d.q[i];
+        sq2 += d.q[i] * d.q[i];
+        double pw = 1.0;
+        for (int k = 0; k < 7; ++k) { M[k] += d.lj_sqrt_eps[i] * pw; pw *= d.lj_rmin_half[i]; }
+      }
+      static const double binom[7] = {1, 6, 15, 20, 15, 6, 1};
+      double SB = 0;
+      for (int k = 0; k < 7; ++k) SB += binom[k] * M[k] * M[6 - k];
+      S.tail_sb = 2.0 * SB;
+      S.sum_q = sq; S.sum_q2 = sq2;
+      for (int m = 0; m < d.n_mol; ++m) {
+        int a0 = d.mol_start[m], a1 = d.mol_start[m + 1];
+        h_molstart.push_back(atom0 + a0);
+        for (int i = a0; i < a1; ++i) {
+          h_molid.push_back(mol0 + m);
+          h_molfirst.push_back(atom0 + a0);
+          h_molend.push_back(atom0 + a1);
+        }
+      }
+      // covalent dipoles: CSR by carrying atom, and a flat list
+      std::vector<std::vector<std::pair<int, double>>> per(d.n_atoms);
+      for (int c = 0; c < d.n_cov; ++c) {
+        per[d.cov_i[c]].push_back({atom0 + d.cov_j[c], d.cov_c[c]});
+        h_covi_flat.push_back(atom0 + d.cov_i[c]);
+        h_covj_flat.push_back(atom0 + d.cov_j[c]);
+        h_covc_flat.push_back(d.cov_c[c]);
+      }
+      for (int i = 0; i < d.n_atoms; ++i) {
+        h_covstart.push_back((int)h_covj.size());
+        for (auto &pr : per[i]) { h_covj.push_back(pr.first); h_covc.push_back(pr.second); }
+      }
+      atom0 += d.n_atoms;
+      mol0 += d.n_mol;
+    }
+    h_molstart.push_back(atom0);
+    h_covstart.push_back((int)h_covj.size());
+    nt = atom0;
+    nmol_total = mol0;
+    ncell = cell0;
+    ncov = (int)h_covi_flat.size();
+    rgrid = rg;
+    cgrid = cg;
+    // default row capacity: the pairs in a cutoff sphere at the densest system, +25 %, + 16
+    double sphere = 4.0 / 3.0 * M_PI * std::pow(set.cutoff, 3) * rho_max;
+    mc_auto = std::max(32, (int)std::ceil((sphere * 1.25 + 16.0) / 32.0) * 32);
+    mc = set.row_capacity > 0 ? ((set.row_capacity + 31) / 32) * 32 : mc_auto;
+    // block maps
+    std::vector<int> wbs, wba, tbs, tba, tx, ty, tz;
+    int cx = 0, cy = 0, cz = 0;
+    for (int si = 0; si < n; ++si) {
+      const pgm::SysInfo &S = hsys[si];
+      for (int a = 0; a < S.natom; a += pgm::WARPS_PER_BLOCK) { wbs.push_back(si); wba.push_back(S.atom0 + a); }
+      for (int a = 0; a < S.natom; a += pgm::THREADS_PER_BLOCK) { tbs.push_back(si); tba.push_back(S.atom0 + a); }
+      tx.push_back(cx); ty.push_back(cy); tz.push_back(cz);
+      int nlines = S.K[0] * S.K[1];
+      int nt3 = (S.K3h + pgm::FFT_TILE - 1) / pgm::FFT_TILE;
+      cx += (nlines + 2 * pgm::FFT_PAIRS - 1) / (2 * pgm::FFT_PAIRS);
+      cy += S.K[0] * nt3;
+      cz += S.K[1] * nt3;
+      smem_x = std::max(smem_x, (size_t)2 * pgm::FFT_PAIRS * S.K[2] * sizeof(pgm::c2<T>));
+      smem_y = std::max(smem_y, (size_t)2 * pgm::FFT_TILE * (S.K[1] + 1) * sizeof(pgm::c2<T>));
+      smem_z = std::max(smem_z, (size_t)2 * pgm::FFT_TILE * (S.K[0] + 1) * sizeof(pgm::c2<T>));
+    }
+    tx.push_back(cx); ty.push_back(cy); tz.push_back(cz);
+    tiles_x = cx; tiles_y = cy; tiles_z = cz;
+    nwblk = (int)wbs.size();
+    ntblk = (int)tbs.size();
+    wb_sys.upload(wbs); wb_atom0.upload(wba); tb_sys.upload(tbs); tb_atom0.upload(tba);
+    tile0_x.upload(tx); tile0_y.upload(ty); tile0_z.upload(tz);
+    d_sys.upload(hsys);
+    d_box.alloc(n);
+    CK(cudaMemset(d_box.p, 0, sizeof(pgm::BoxInfo) * n));
+    std::vector<pgm::CGSys> hcg(n);
+    std::memset(hcg.data(), 0, sizeof(pgm::CGSys) * n);
+    for (int si = 0; si < n; ++si) hcg[si].n3 = 3 * hsys[si].natom;
+    d_cg.upload(hcg);
+    d_eacc.alloc(n);
+    d_status.alloc(n);
+    sysid.upload(h_sysid); molid.upload(h_molid); molfirst.upload(h_molfirst); molend.upload(h_molend);
+    mol_start.upload(h_molstart); cov_start.upload(h_covstart); cov_j.upload(h_covj);
+    cov_i_flat.upload(h_covi_flat); cov_j_flat.upload(h_covj_flat);
+    q.upload(h_q); radius.upload(h_rad); alpha.upload(h_al); ialpha.upload(h_ial); rminh.upload(h_rh); seps.upload(h_se);
+    mass.upload(h_mass); cov_c.upload(h_covc); cov_c_flat.upload(h_covc_flat); bmod.upload(h_bmod);
+    tw.upload(h_tw);
+    base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt);
+    pperm.alloc(nt); off.alloc(nt); dEdd.alloc(nt);
+    cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt);
+    rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(1); dany.alloc(1);
+    alloc_rows();
+    Q.alloc(rgrid); Phi.alloc(rgrid); Ginf.alloc(cgrid); C.alloc(cgrid);
+    CK(cudaMemset(Q.p, 0, sizeof(T) * rgrid));
+    mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
+    CK(cudaMallocHost(&h_any, sizeof(int)));
+    set_smem();
+  }
+
+  void alloc_rows() {
+    size_t m = (size_t)nt * mc;
+    rk.alloc(m); rx.alloc(m); ry.alloc(m); rz.alloc(m); rg0.alloc(m); rg1.alloc(m); rg2.alloc(m); rg3.alloc(m);
+  }
+
+  template <typename K>
+  void smem_attr(K kern, size_t bytes) {
+    if (bytes > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  }
+
+  void set_smem() {
+    smem_attr(pgm::k_fft_x_fwd<T, 0>, smem_x); smem_attr(pgm::k_fft_x_fwd<T, 1>, smem_x); smem_attr(pgm::k_fft_x_fwd<T, 2>, smem_x);
+    smem_attr(pgm::k_fft_x_inv<T, 0>, smem_x); smem_attr(pgm::k_fft_x_inv<T, 1>, smem_x); smem_attr(pgm::k_fft_x_inv<T, 2>, smem_x);
+    smem_attr(pgm::k_fft_y<T, 0>, smem_y); smem_attr(pgm::k_fft_y<T, 1>, smem_y); smem_attr(pgm::k_fft_y<T, 2>, smem_y);
+    smem_attr(pgm::k_fft_z_conv<T, 0, false>, smem_z); smem_attr(pgm::k_fft_z_conv<T, 1, false>, smem_z);
+    smem_attr(pgm::k_fft_z_conv<T, 2, false>, smem_z); smem_attr(pgm::k_fft_z_conv<T, 0, true>, smem_z);
+  }
+
+  void set_capacity(int c) override {
+    int want = c > 0 ? ((c + 31) / 32) * 32 : mc_auto;
+    if (want != mc) {
+      mc = want;
+      alloc_rows();
+    }
+  }
+  int capacity() const override { return mc; }
+  int max_count() override {
+    int v = 0;
+    CK(cudaMemcpy(&v, dmax.p, sizeof(int), cudaMemcpyDeviceToHost));
+    return v;
+  }
+
+  void check_launch() {
+    ++launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw CudaError{std::string("kernel launch: ") + cudaGetErrorString(e)};
+  }
+
+  int grid1(int n, int b = 256) { return (n + b - 1) / b; }
+
+  // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
+  // cell list, rows, influence function.
+  void prepare(cudaStream_t st, pgm::Dev<T> &a, const double *boxes) {
+    CK(cudaMemsetAsync(cell_count.p, 0, sizeof(int) * ncell, st));
+    CK(cudaMemsetAsync(dmax.p, 0, sizeof(int), st));
+    pgm::k_box<T><<<grid1(nsys, 64), 64, 0, st>>>(a, boxes); check_launch();
+    pgm::k_prep<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
+    pgm::k_mol<T><<<grid1(nmol_total), 256, 0, st>>>(a); check_launch();
+    pgm::k_scan_cells<<<1, 1024, 0, st>>>(cell_count.p, cell_start.p, ncell); check_launch();
+    pgm::k_scatter<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
+    pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a); check_launch();
+    pgm::k_influence<T><<<std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st>>>(a, cgrid); check_launch();
+  }
+
+  // Reciprocal-space potential phi of the grid spread from `vin` (with charges if WITH_Q).
+  template <bool WITH_Q, bool UPDATE_P, int ACT, bool ENERGY>
+  void pme(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin) {
+    pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
+    pgm::k_fft_x_fwd<T, ACT><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p); check_launch();
+    pgm::k_fft_y<T, ACT><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, -1); check_launch();
+    pgm::k_fft_z_conv<T, ACT, ENERGY><<<tiles_z, 256, smem_z, st>>>(a, tile0_z.p); check_launch();
+    pgm::k_fft_y<T, ACT><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, +1); check_launch();
+    pgm::k_fft_x_inv<T, ACT><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p); check_launch();
+  }
+
+  bool any_active(cudaStream_t st) {
+    CK(cudaMemcpyAsync(h_any, dany.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return *h_any != 0;
+  }
+
+  // The induced-dipole solve (forcefield.py:1917-2008 and 1714-1821).  mode 0: predictor start
+  // and history push (compute); mode 1: plain start from ind->mu, no push (energy).
+  void solve(cudaStream_t st, pgm::Dev<T> &a, PgmInduction *ind, int mode, double *mu_out, int32_t *iters, double *resid) {
+    const int K = set.predictor == 4 ? 4 : (set.predictor == 3 ? 3 : 0);
+    const double c4[4] = {4.0, -6.0, 4.0, -1.0}, c3[4] = {3.0, -3.0, 1.0, 0.0}, c0[4] = {0, 0, 0, 0};
+    const double *cc = K == 4 ? c4 : (K == 3 ? c3 : c0);
+    pgm::k_cg_setup<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, mode == 0 ? ind->count : nullptr, ind->norm, mode == 0 ? K : 0,
+                                                    set.fused, std::max(1, set.norm_refresh), mode);
+    check_launch();
+    if (mode == 1) {
+      // x0 = ind->mu with the plain start: X = mu, have = 1
+      pgm::k_energy_start<T><<<grid1(nt), 256, 0, st>>>(a, ind->mu);
+      check_launch();
+    } else {
+      pgm::k_start1<T><<<grid1(nt), 256, 0, st>>>(a, ind->hist, K, cc[0], cc[1], cc[2], cc[3]);
+      check_launch();
+    }
+    pme<true, false, 0, false>(st, a, D.p);
+    pgm::k_rowmat<T, P, true, 0, 0><<<nwblk, 256, 0, st>>>(a, D.p, Bv.p); check_launch();
+    pgm::k_start2<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+    pme<false, false, 2, false>(st, a, X.p);
+    pgm::k_rowmat<T, P, false, 1, 2><<<nwblk, 256, 0, st>>>(a, X.p, AP.p); check_launch();
+    pgm::k_start3<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
+    pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+    pgm::k_cg_begin<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p); check_launch();
+    for (int it = 0; it < set.max_iter; ++it) {
+      if (!any_active(st)) break;
+      pme<false, true, 1, false>(st, a, Pv.p);
+      pgm::k_rowmat<T, P, false, 1, 1><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p); check_launch();
+      pgm::k_cg_update<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+      pgm::k_cg_check<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p); check_launch();
+    }
+    pgm::k_cg_finish<T><<<grid1(nt), 256, 0, st>>>(a, mu_out, mode == 0 ? ind->hist : nullptr, mode == 0); check_launch();
+    pgm::k_cg_state_out<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, ind->count, ind->norm, iters, resid, a.status, mode == 0,
+                                                        set.dipole_tol);
+    check_launch();
+  }
+
+  // Energies, forces and virial at fixed mu (forcefield.py:2362-2430).
+  void energy_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, double *energy, double *virial) {
+    CK(cudaMemsetAsync(d_eacc.p, 0, sizeof(pgm::EnergyAcc) * nsys, st));
+    pgm::k_total_dipoles<T><<<grid1(nt), 256, 0, st>>>(a, mu); check_launch();
+    pme<true, false, 0, true>(st, a, D.p);
+    pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, mu); check_launch();
+    if (ncov) { pgm::k_cov_forces<T><<<grid1(ncov), 256, 0, st>>>(a); check_launch(); }
+    pgm::k_energy_finish<<<grid1(nsys, 64), 64, 0, st>>>(d_sys.p, d_box.p, d_eacc.p, nsys, set.ewald_beta, a.c_self, set.cutoff,
+                                                         set.vdw == 1, set.lj_lrc, a.induce, energy, virial, a.status);
+    check_launch();
+  }
+
+  void compute(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width, PgmInduction *ind,
+               PgmOutputs *out) override {
+    launches = 0;
+    unsigned *status = out->status ? out->status : d_status.p;
+    double *forces = out->forces ? out->forces : forces_tmp.p;
+    CK(cudaMemsetAsync(status, 0, sizeof(unsigned) * nsys, st));
+    pgm::Dev<T> a = dev(pos, idx, idx_width, forces, status);
+    prepare(st, a, box);
+    double *mu = ind->mu;
+    if (a.induce) {
+      solve(st, a, ind, 0, mu, out->iterations, out->residual);
+    } else {
+      CK(cudaMemsetAsync(mu, 0, sizeof(double) * 3 * nt, st));
+      if (out->iterations) CK(cudaMemsetAsync(out->iterations, 0, sizeof(int32_t) * nsys, st));
+      if (out->residual) CK(cudaMemsetAsync(out->residual, 0, sizeof(double) * nsys, st));
+    }
+    energy_pass(st, a, mu, out->energy ? out->energy : energy_tmp.p, out->virial);
+  }
+
+  void energy(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width, PgmInduction *ind,
+              double *energy_out, int32_t *iters, uint32_t *status_out) override {
+    launches = 0;
+    unsigned *status = status_out ? status_out : d_status.p;
+    CK(cudaMemsetAsync(status, 0, sizeof(unsigned) * nsys, st));
+    pgm::Dev<T> a = dev(pos, idx, idx_width, forces_tmp.p, status);
+    prepare(st, a, box);
+    if (a.induce) {
+      solve(st, a, ind, 1, ind->mu, iters, nullptr);
+    } else {
+      CK(cudaMemsetAsync(ind->mu, 0, sizeof(double) * 3 * nt, st));
+      if (iters) CK(cudaMemsetAsync(iters, 0, sizeof(int32_t) * nsys, st));
+    }
+    energy_pass(st, a, ind->mu, energy_out, nullptr);
+  }
+
+  void fixed_mu(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width, const double *mu,
+                double *energy_out, double *forces_out, double *virial, uint32_t *status_out) override {
+    launches = 0;
+    unsigned *status = status_out ? status_out : d_status.p;
+    CK(cudaMemsetAsync(status, 0, sizeof(unsigned) * nsys, st));
+    pgm::Dev<T> a = dev(pos, idx, idx_width, forces_out ? forces_out : forces_tmp.p, status);
+    prepare(st, a, box);
+    energy_pass(st, a, mu, energy_out ? energy_out : energy_tmp.p, virial);
+  }
+
+  void field(cudaStream_t st, const double *pos, const double *box, int with_q, const double *d, double *out) override {
+    launches = 0;
+    CK(cudaMemsetAsync(d_status.p, 0, sizeof(unsigned) * nsys, st));
+    pgm::Dev<T> a = dev(pos, nullptr, 0, forces_tmp.p, d_status.p);
+    prepare(st, a, box);
+    pgm::k_load_vec<T><<<grid1(nt), 256, 0, st>>>(a, d, D.p); check_launch();
+    if (with_q) {
+      pme<true, false, 0, false>(st, a, D.p);
+      pgm::k_rowmat<T, P, true, 0, 0><<<nwblk, 256, 0, st>>>(a, D.p, Bv.p); check_launch();
+    } else {
+      pme<false, false, 0, false>(st, a, D.p);
+      pgm::k_rowmat<T, P, false, 0, 0><<<nwblk, 256, 0, st>>>(a, D.p, Bv.p); check_launch();
+    }
+    pgm::k_store_vec<T><<<grid1(nt), 256, 0, st>>>(a, Bv.p, out); check_launch();
+  }
+};
+
+}  // namespace
+
+struct PgmHandle {
+  std::unique_ptr<EngineBase> eng;
+  int device = 0;
+};
+
+static PgmStatus fail(PgmStatus s, const std::string &m) {
+  g_err = m;
+  return s;
+}
+
+extern "C" {
+
+const char *pgm_last_error(void) { return g_err.c_str(); }
+
+PgmStatus pgm_create(const PgmSettings *s, const PgmSystemDesc *systems, int n, int device, PgmHandle **out) {
+  if (!s || !systems || n <= 0 || !out) return fail(PGM_ERR_INVALID, "null argument or no systems");
+  if (s->elec < 0 || s->elec > 3) return fail(PGM_ERR_INVALID, "elec must be 0..3 (q, qp, qi, qpi)");
+  if (s->vdw < 0 || s->vdw > 1) return fail(PGM_ERR_INVALID, "vdw must be 0 (none) or 1 (lj)");
+  if (s->precision < 0 || s->precision > 1) return fail(PGM_ERR_INVALID, "precision must be 0 (mixed) or 1 (double)");
+  if (!(s->cutoff > 0) || !(s->ewald_beta > 0)) return fail(PGM_ERR_INVALID, "cutoff and ewald_beta must be positive");
+  if (s->pme_order != 4 && s->pme_order != 6 && s->pme_order != 8) return fail(PGM_ERR_UNSUPPORTED, "pme_order must be 4, 6 or 8");
+  if (s->predictor != 0 && s->predictor != 3 && s->predictor != 4)
+    return fail(PGM_ERR_INVALID, "predictor must be 0 (none), 3 (mu3) or 4 (mu4)");
+  if (s->max_iter < 0) return fail(PGM_ERR_INVALID, "max_iter must be >= 0");
+  for (int i = 0; i < n; ++i) {
+    const PgmSystemDesc &d = systems[i];
+    if (d.n_atoms <= 0 || d.n_mol <= 0 || !d.mol_start || !d.q || !d.radius || !d.alpha || !d.lj_rmin_half || !d.lj_sqrt_eps ||
+        !d.masses)
+      return fail(PGM_ERR_INVALID, "system " + std::to_string(i) + ": missing arrays");
+    if (d.mol_start[0] != 0 || d.mol_start[d.n_mol] != d.n_atoms) return fail(PGM_ERR_INVALID, "mol_start must span the atoms");
+    for (int m = 0; m < d.n_mol; ++m)
+      if (d.mol_start[m + 1] <= d.mol_start[m]) return fail(PGM_ERR_INVALID, "empty molecule");
+    for (int a = 0; a < d.n_atoms; ++a)
+      if (!(d.alpha[a] > 0)) return fail(PGM_ERR_UNSUPPORTED, "polarizabilities must be positive");
+    for (int c = 0; c < d.n_cov; ++c)
+      if (d.cov_i[c] < 0 || d.cov_i[c] >= d.n_atoms || d.cov_j[c] < 0 || d.cov_j[c] >= d.n_atoms)
+        return fail(PGM_ERR_INVALID, "covalent dipole index out of range");
+    for (int a = 0; a < 3; ++a) {
+      int K = d.pme_grid[a];
+      if (K < 2 * s->pme_order || K > 256 || K % 2 || radices(K).empty())
+        return fail(PGM_ERR_UNSUPPORTED, "PME grid sizes must be even, 2, 3, 5-smooth, >= 2 order and <= 256");
+    }
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PGM_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(PGM_ERR_INVALID, "device index out of range");
+  try {
+    CK(cudaSetDevice(device));
+    auto h = new PgmHandle();
+    h->device = device;
+    if (s->precision == 0) {
+      if (s->pme_order == 4) h->eng.reset(new Engine<float, 4>());
+      else if (s->pme_order == 6) h->eng.reset(new Engine<float, 6>());
+      else h->eng.reset(new Engine<float, 8>());
+    } else {
+      if (s->pme_order == 4) h->eng.reset(new Engine<double, 4>());
+      else if (s->pme_order == 6) h->eng.reset(new Engine<double, 6>());
+      else h->eng.reset(new Engine<double, 8>());
+    }
+    if (s->precision == 0) {
+      if (s->pme_order == 4) static_cast<Engine<float, 4> *>(h->eng.get())->init(s, systems, n);
+      else if (s->pme_order == 6) static_cast<Engine<float, 6> *>(h->eng.get())->init(s, systems, n);
+      else static_cast<Engine<float, 8> *>(h->eng.get())->init(s, systems, n);
+    } else {
+      if (s->pme_order == 4) static_cast<Engine<double, 4> *>(h->eng.get())->init(s, systems, n);
+      else if (s->pme_order == 6) static_cast<Engine<double, 6> *>(h->eng.get())->init(s, systems, n);
+      else static_cast<Engine<double, 8> *>(h->eng.get())->init(s, systems, n);
+    }
+    h->eng->nsys = n;
+    *out = h;
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  } catch (std::exception &e) {
+    return fail(PGM_ERR_CUDA, e.what());
+  }
+}
+
+PgmStatus pgm_destroy(PgmHandle *h) {
+  if (!h) return PGM_ERR_INVALID;
+  cudaSetDevice(h->device);
+  delete h;
+  return PGM_OK;
+}
+
+PgmStatus pgm_compute(PgmHandle *h, void *stream, const double *pos, const double *box, const int32_t *idx, int idx_width,
+                      PgmInduction *ind, PgmOutputs *out) {
+  if (!h || !pos || !box || !ind || !out || !ind->mu) return fail(PGM_ERR_INVALID, "null argument");
+  if (h->eng && (h->eng->nt > 0) && (!ind->hist || !ind->count || !ind->norm)) return fail(PGM_ERR_INVALID, "induction state incomplete");
+  if (idx && idx_width <= 0) return fail(PGM_ERR_INVALID, "idx_width must be positive with idx");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->compute((cudaStream_t)stream, pos, box, idx, idx_width, ind, out);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, PgmInduction *ind, PgmOutputs *out) {
+  if (!h || !pos || !box || !ind || !out || !ind->mu || !ind->hist || !ind->count || !ind->norm)
+    return fail(PGM_ERR_INVALID, "null argument");
+  EngineBase *e = h->eng.get();
+  size_t n3 = (size_t)3 * e->nt, ns = e->nsys;
+  double *d = nullptr;
+  try {
+    CK(cudaSetDevice(h->device));
+    // one device block: pos, box, mu, hist, norm, energy, forces, virial, residual | count, iterations, status
+    size_t nd = n3 + 9 * ns + n3 + 4 * n3 + ns + 3 * ns + n3 + 9 * ns + ns;
+    size_t ni = 3 * ns;
+    CK(cudaMalloc(&d, sizeof(double) * nd + sizeof(int32_t) * ni));
+    double *dpos = d, *dbox = dpos + n3, *dmu = dbox + 9 * ns, *dhist = dmu + n3, *dnorm = dhist + 4 * n3, *den = dnorm + ns,
+           *dF = den + 3 * ns, *dvir = dF + n3, *dres = dvir + 9 * ns;
+    int32_t *dcount = reinterpret_cast<int32_t *>(dres + ns), *dit = dcount + ns;
+    uint32_t *dst = reinterpret_cast<uint32_t *>(dit + ns);
+    cudaStream_t st = 0;
+    CK(cudaMemcpyAsync(dpos, pos, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dbox, box, sizeof(double) * 9 * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dmu, ind->mu, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dhist, ind->hist, sizeof(double) * 4 * n3, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dnorm, ind->norm, sizeof(double) * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dcount, ind->count, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
+    PgmInduction di{dmu, dhist, dcount, dnorm};
+    PgmOutputs dout{den, dF, dvir, dit, dres, dst};
+    e->compute(st, dpos, dbox, nullptr, 0, &di, &dout);
+    CK(cudaMemcpyAsync(ind->mu, dmu, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ind->hist, dhist, sizeof(double) * 4 * n3, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ind->norm, dnorm, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ind->count, dcount, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, st));
+    if (out->energy) CK(cudaMemcpyAsync(out->energy, den, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, st));
+    if (out->forces) CK(cudaMemcpyAsync(out->forces, dF, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));
+    if (out->virial) CK(cudaMemcpyAsync(out->virial, dvir, sizeof(double) * 9 * ns, cudaMemcpyDeviceToHost, st));
+    if (out->iterations) CK(cudaMemcpyAsync(out->iterations, dit, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, st));
+    if (out->residual) CK(cudaMemcpyAsync(out->residual, dres, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+    if (out->status) CK(cudaMemcpyAsync(out->status, dst, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaFree(d));
+    return PGM_OK;
+  } catch (CudaError &err) {
+    if (d) cudaFree(d);
+    return fail(PGM_ERR_CUDA, err.msg);
+  }
+}
+
+PgmStatus pgm_energy(PgmHandle *h, void *stream, const double *pos, const double *box, const int32_t *idx, int idx_width,
+                     PgmInduction *ind, double *energy, int32_t *iterations, uint32_t *status) {
+  if (!h || !pos || !box || !ind || !ind->mu || !energy) return fail(PGM_ERR_INVALID, "null argument");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->energy((cudaStream_t)stream, pos, box, idx, idx_width, ind, energy, iterations, status);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_energy_fixed_mu(PgmHandle *h, void *stream, const double *pos, const double *box, const int32_t *idx,
+                              int idx_width, const double *mu, double *energy, double *forces, double *virial,
+                              uint32_t *status) {
+  if (!h || !pos || !box || !mu) return fail(PGM_ERR_INVALID, "null argument");
+  if (idx && idx_width <= 0) return fail(PGM_ERR_INVALID, "idx_width must be positive with idx");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->fixed_mu((cudaStream_t)stream, pos, box, idx, idx_width, mu, energy, forces, virial, status);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_field(PgmHandle *h, void *stream, const double *pos, const double *box, int with_charges, const double *d,
+                    double *field) {
+  if (!h || !pos || !box || !d || !field) return fail(PGM_ERR_INVALID, "null argument");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->field((cudaStream_t)stream, pos, box, with_charges, d, field);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_set_row_capacity(PgmHandle *h, int capacity) {
+  if (!h || capacity < 0) return fail(PGM_ERR_INVALID, "bad capacity");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->set_capacity(capacity);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+int pgm_row_capacity(const PgmHandle *h) { return h ? h->eng->capacity() : -1; }
+
+int pgm_max_row_count(PgmHandle *h) {
+  if (!h) return -1;
+  try {
+    return h->eng->max_count();
+  } catch (CudaError &e) {
+    g_err = e.msg;
+    return -1;
+  }
+}
+
+int pgm_num_atoms(const PgmHandle *h) { return h ? h->eng->nt : -1; }
+int pgm_num_systems(const PgmHandle *h) { return h ? h->eng->nsys : -1; }
+long long pgm_last_launch_count(const PgmHandle *h) { return h ? h->eng->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,1276 @@
+// pgm_kernels.cuh -- the sm_100a kernels of the pGM step.
+//
+// Layout in HBM (all systems of a batch concatenated; a block never straddles two systems):
+//   atoms      SoA per-atom parameters (T) and state; 3-vectors as 16/32-byte v4<T> for single loads
+//   rows       [atom][capacity] structure of arrays: partner k (int32), x, y, z, G0..G3 (T);
+//              molecule partners first (the rigid special table), then the in-cutoff neighbours
+//   PME        per system a real grid K1 x K2 x K3 (k3 fastest) and a half-complex grid
+//              K1 x K2 x (K3/2 + 1), both as flat offsets into batch-wide buffers
+//   reductions per-system FP64 accumulators (CGSys, EnergyAcc), filled by block partials + atomics
+//
+// Reference correspondence (pgm_jax/md/...): row build forcefield.py:1140-1195, radial kernels
+// kernels.py:76-118 + forcefield.py:1318-1338, direct field forcefield.py:1395-1433, PME
+// pme.py:243-411, CG forcefield.py:1714-1821, start forcefield.py:1917-2008, energy and forces
+// forcefield.py:2011-2045,2294-2430, strain derivative forcefield.py:608-662,2628-2695.
+#pragma once
+#include "pgm_device.cuh"
+
+namespace pgm {
+
+template <typename T>
+struct Dev {
+  int nsys, nt, nmol, mc, ncell, ncov;
+  int order;
+  int induce, perm, lj, lj_lrc;
+  double beta, cutoff, c_self, tol, peek;
+  int max_iter;
+  const SysInfo *sys;
+  BoxInfo *box;
+  CGSys *cg;
+  EnergyAcc *eacc;
+  unsigned *status;
+  // block maps (warp-per-atom and thread-per-atom kernels)
+  const int *wb_sys, *wb_atom0, *tb_sys, *tb_atom0;
+  // atoms
+  const int *sysid, *molid, *molfirst, *molend, *mol_start;
+  const T *q, *radius, *alpha, *ialpha, *rminh, *seps;
+  const double *mass;
+  const int *cov_start, *cov_j, *cov_i_flat, *cov_j_flat;
+  const double *cov_c, *cov_c_flat;
+  // per step
+  const double *pos;
+  int4 *base;
+  v4<T> *frac;
+  double4 *pperm, *off;
+  int *cell_of, *slot_of, *cell_count, *cell_start, *cell_atoms;
+  const int *idx;
+  int idx_width;
+  // rows
+  int *rn, *rnsp, *rk;
+  T *rx, *ry, *rz, *rg0, *rg1, *rg2, *rg3;
+  int *max_count;
+  // vectors
+  v4<T> *X, *R, *Z, *P, *AP, *B, *D;
+  // grids
+  T *Q, *Phi, *Ginf;
+  c2<T> *C;
+  const c2<T> *tw;
+  const double *bmod;
+  // outputs of the energy pass
+  double *forces;
+  double4 *dEdd;
+};
+
+// ------------------------------------------------------------------ box and per-atom set-up
+template <typename T>
+__global__ void k_box(Dev<T> a, const double *boxes) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.nsys) return;
+  const double *H = boxes + 9 * s;
+  BoxInfo &B = a.box[s];
+  int changed = 0;
+  for (int k = 0; k < 9; ++k) changed |= (B.H[k] != H[k]);
+  double d = H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) + H[2] * (H[3] * H[7] - H[4] * H[6]);
+  double Hi[9];  // cofactor inverse (box.py:195-234)
+  Hi[0] = (H[4] * H[8] - H[5] * H[7]) / d; Hi[1] = (H[2] * H[7] - H[1] * H[8]) / d; Hi[2] = (H[1] * H[5] - H[2] * H[4]) / d;
+  Hi[3] = (H[5] * H[6] - H[3] * H[8]) / d; Hi[4] = (H[0] * H[8] - H[2] * H[6]) / d; Hi[5] = (H[2] * H[3] - H[0] * H[5]) / d;
+  Hi[6] = (H[3] * H[7] - H[4] * H[6]) / d; Hi[7] = (H[1] * H[6] - H[0] * H[7]) / d; Hi[8] = (H[0] * H[4] - H[1] * H[3]) / d;
+  for (int k = 0; k < 9; ++k) { B.H[k] = H[k]; B.Hinv[k] = Hi[k]; }
+  B.vol = fabs(d);
+  const SysInfo &S = a.sys[s];
+  for (int ax = 0; ax < 3; ++ax) {
+    // plane height h_a = 1 / |column a of H^-1|
+    double c0 = Hi[0 * 3 + ax], c1 = Hi[1 * 3 + ax], c2v = Hi[2 * 3 + ax];
+    B.h[ax] = 1.0 / sqrt(c0 * c0 + c1 * c1 + c2v * c2v);
+    int nc = S.nc[ax];
+    int R = (int)ceil(a.cutoff * nc / B.h[ax] - 1e-12);
+    B.R[ax] = (2 * R + 1 >= nc) ? -1 : R;
+  }
+  B.changed = changed;
+  int bad = (fabs(H[1]) > 1e-12 * fabs(H[0])) || (fabs(H[2]) > 1e-12 * fabs(H[0])) || (fabs(H[5]) > 1e-12 * fabs(H[0])) ||
+            !(H[0] > 0 && H[4] > 0 && H[8] > 0);
+  double mc = 0.5 * fmin(H[0], fmin(H[4], H[8]));
+  if (a.cutoff > mc) bad = 1;
+  B.bad = bad;
+  if (bad) atomicOr(&a.status[s], 0x8u);
+}
+
+// Fractional coordinates, spline base and offset (pme.py:269-304), permanent dipoles
+// (forcefield.py:1032-1042) and the cell of every atom.
+template <typename T>
+__global__ void k_prep(Dev<T> a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  int s = a.sysid[i];
+  const SysInfo &S = a.sys[s];
+  const BoxInfo &B = a.box[s];
+  double px = a.pos[3 * i], py = a.pos[3 * i + 1], pz = a.pos[3 * i + 2];
+  double uc[3];
+  int4 b;
+  v4<T> f;
+  int bb[3];
+  T ff[3];
+  bool finite = true;
+  for (int ax = 0; ax < 3; ++ax) {
+    double u = px * B.Hinv[0 * 3 + ax] + py * B.Hinv[1 * 3 + ax] + pz * B.Hinv[2 * 3 + ax];
+    double fr = u - floor(u);
+    if (!(fr >= 0.0 && fr < 1.0)) { fr = 0.0; finite = false; }  // non-finite position: keep indices in range
+    uc[ax] = fr;
+    double w = fr * S.K[ax];
+    double fl = floor(w);
+    int bv = (int)fl;
+    if (bv >= S.K[ax]) bv -= S.K[ax];  // w rounded up to K: grid point K is point 0
+    if (bv < 0) bv = 0;
+    bb[ax] = bv;
+    ff[ax] = T(w - fl);
+  }
+  if (!finite) atomicOr(&a.status[s], 0x4u);
+  b.x = bb[0]; b.y = bb[1]; b.z = bb[2]; b.w = 0;
+  f.x = ff[0]; f.y = ff[1]; f.z = ff[2]; f.w = T(0);
+  a.base[i] = b;
+  a.frac[i] = f;
+  double4 p = make_double4(0, 0, 0, 0);
+  if (a.perm) {
+    for (int c = a.cov_start[i]; c < a.cov_start[i + 1]; ++c) {
+      int j = a.cov_j[c];
+      double vx = a.pos[3 * j] - px, vy = a.pos[3 * j + 1] - py, vz = a.pos[3 * j + 2] - pz;
+      min_image(vx, vy, vz, B.H);
+      double l = sqrt(vx * vx + vy * vy + vz * vz);
+      double cc = a.cov_c[c] / l;
+      p.x += cc * vx; p.y += cc * vy; p.z += cc * vz;
+    }
+  }
+  a.pperm[i] = p;
+  int c0 = max(0, min((int)(uc[0] * S.nc[0]), S.nc[0] - 1));
+  int c1 = max(0, min((int)(uc[1] * S.nc[1]), S.nc[1] - 1));
+  int c2v = max(0, min((int)(uc[2] * S.nc[2]), S.nc[2] - 1));
+  int cell = S.cell0 + (c0 * S.nc[1] + c1) * S.nc[2] + c2v;
+  a.cell_of[i] = cell;
+  a.slot_of[i] = atomicAdd(&a.cell_count[cell], 1);
+}
+
+// Offsets of every atom from its molecule's centre of mass (molecule made whole from its first
+// atom), for the molecular virial.
+template <typename T>
+__global__ void k_mol(Dev<T> a) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.nmol) return;
+  int i0 = a.mol_start[m], i1 = a.mol_start[m + 1];
+  const BoxInfo &B = a.box[a.sysid[i0]];
+  double cx = 0, cy = 0, cz = 0, mt = 0;
+  for (int i = i0; i < i1; ++i) {
+    double vx = a.pos[3 * i] - a.pos[3 * i0], vy = a.pos[3 * i + 1] - a.pos[3 * i0 + 1], vz = a.pos[3 * i + 2] - a.pos[3 * i0 + 2];
+    min_image(vx, vy, vz, B.H);
+    a.off[i] = make_double4(vx, vy, vz, 0);
+    cx += a.mass[i] * vx; cy += a.mass[i] * vy; cz += a.mass[i] * vz; mt += a.mass[i];
+  }
+  cx /= mt; cy /= mt; cz /= mt;
+  for (int i = i0; i < i1; ++i) {
+    double4 o = a.off[i];
+    a.off[i] = make_double4(o.x - cx, o.y - cy, o.z - cz, 0);
+  }
+}
+
+// Exclusive scan of the cell counts of all systems (one block).
+__global__ void k_scan_cells(const int *count, int *start, int n) {
+  __shared__ int part[1024];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024) {
+    int i = base + threadIdx.x;
+    int v = i < n ? count[i] : 0;
+    part[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      int t = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+      __syncthreads();
+      part[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < n) start[i] = carry + part[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += part[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) start[n] = carry;
+}
+
+template <typename T>
+__global__ void k_scatter(Dev<T> a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  a.cell_atoms[a.cell_start[a.cell_of[i]] + a.slot_of[i]] = i;
+}
+
+// ------------------------------------------------------------------ pair rows
+// One warp per atom: the molecule partners (always kept inside the cutoff; the rigid special
+// table of md/topology.py:161-178), then the neighbours from the cell list (or from the caller's
+// candidate rows), masked to r < rc, compacted by ballot into the row, with the radial kernels
+// G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] of every kept pair.
+template <typename T>
+__device__ __forceinline__ void row_candidate(const Dev<T> &a, int i, int j, bool ok, double pix, double piy, double piz,
+                                              const double *H, double rc2, T Ri2, int base, int &count, int lane) {
+  double x = 0, y = 0, z = 0;
+  bool keep = false;
+  if (ok) {
+    x = pix - a.pos[3 * j]; y = piy - a.pos[3 * j + 1]; z = piz - a.pos[3 * j + 2];
+    min_image(x, y, z, H);
+    keep = x * x + y * y + z * z < rc2;
+  }
+  unsigned bal = __ballot_sync(0xffffffffu, keep);
+  if (keep) {
+    int slot = count + __popc(bal & ((1u << lane) - 1u));
+    if (slot < a.mc) {
+      T xt = T(x), yt = T(y), zt = T(z);
+      T r = t_sqrt(xt * xt + yt * yt + zt * zt);
+      T Rk = a.radius[j];
+      T aik = t_rsqrt(T(2) * (Ri2 + Rk * Rk));
+      T A[4], Bb[4];
+      erf_kernels<T>(aik, r, A);
+      erf_kernels<T>(T(a.beta), r, Bb);
+      size_t o = (size_t)base + slot;
+      a.rk[o] = j;
+      a.rx[o] = xt; a.ry[o] = yt; a.rz[o] = zt;
+      a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = A[1] - Bb[1]; a.rg2[o] = A[2] - Bb[2]; a.rg3[o] = A[3] - Bb[3];
+    }
+  }
+  count += __popc(bal);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int blk = blockIdx.x;
+  int s = a.wb_sys[blk];
+  int i = a.wb_atom0[blk] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
+  const BoxInfo &B = a.box[s];
+  double H[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) H[k] = B.H[k];
+  double pix = a.pos[3 * i], piy = a.pos[3 * i + 1], piz = a.pos[3 * i + 2];
+  double rc2 = a.cutoff * a.cutoff;
+  T Ri = a.radius[i], Ri2 = Ri * Ri;
+  int base = i * a.mc;
+  int count = 0;
+  int mf = a.molfirst[i], me = a.molend[i];
+  for (int j0 = mf; j0 < me; j0 += 32) {
+    int j = j0 + lane;
+    row_candidate<T>(a, i, j, j < me && j != i, pix, piy, piz, H, rc2, Ri2, base, count, lane);
+  }
+  int nsp = count;
+  int mi = a.molid[i];
+  if (a.idx) {  // the caller's candidate rows (local indices, padding natom)
+    const int *row = a.idx + (size_t)i * a.idx_width;
+    for (int c0 = 0; c0 < a.idx_width; c0 += 32) {
+      int c = c0 + lane;
+      int jl = c < a.idx_width ? row[c] : S.natom;
+      bool ok = jl >= 0 && jl < S.natom;
+      int j = S.atom0 + (ok ? jl : 0);
+      ok = ok && a.molid[j] != mi;
+      row_candidate<T>(a, i, j, ok, pix, piy, piz, H, rc2, Ri2, base, count, lane);
+    }
+  } else {  // cell list: cells within R of the atom's cell along each axis
+    int cell = a.cell_of[i] - S.cell0;
+    int n0 = S.nc[0], n1 = S.nc[1], n2 = S.nc[2];
+    int ci2 = cell % n2, ci1 = (cell / n2) % n1, ci0 = cell / (n1 * n2);
+    int R0 = B.R[0], R1 = B.R[1], R2 = B.R[2];
+    int lo0 = R0 < 0 ? 0 : -R0, hi0 = R0 < 0 ? n0 - 1 : R0;
+    int lo1 = R1 < 0 ? 0 : -R1, hi1 = R1 < 0 ? n1 - 1 : R1;
+    for (int d0 = lo0; d0 <= hi0; ++d0) {
+      int c0 = R0 < 0 ? d0 : ((ci0 + d0) % n0 + n0) % n0;
+      for (int d1 = lo1; d1 <= hi1; ++d1) {
+        int c1 = R1 < 0 ? d1 : ((ci1 + d1) % n1 + n1) % n1;
+        int rowc = S.cell0 + (c0 * n1 + c1) * n2;
+        // contiguous k3 ranges of cells: one or two segments
+        int segs[2][2];
+        int nseg = 0;
+        if (R2 < 0) {
+          segs[0][0] = 0; segs[0][1] = n2 - 1; nseg = 1;
+        } else {
+          int lo = ci2 - R2, hi = ci2 + R2;
+          if (lo < 0) { segs[0][0] = lo + n2; segs[0][1] = n2 - 1; segs[1][0] = 0; segs[1][1] = hi; nseg = 2; }
+          else if (hi >= n2) { segs[0][0] = lo; segs[0][1] = n2 - 1; segs[1][0] = 0; segs[1][1] = hi - n2; nseg = 2; }
+          else { segs[0][0] = lo; segs[0][1] = hi; nseg = 1; }
+        }
+        for (int g = 0; g < nseg; ++g) {
+          int a0 = a.cell_start[rowc + segs[g][0]], a1 = a.cell_start[rowc + segs[g][1] + 1];
+          for (int t0 = a0; t0 < a1; t0 += 32) {
+            int t = t0 + lane;
+            int j = t < a1 ? a.cell_atoms[t] : i;
+            bool ok = t < a1 && a.molid[j] != mi;
+            row_candidate<T>(a, i, j, ok, pix, piy, piz, H, rc2, Ri2, base, count, lane);
+          }
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    a.rn[i] = count;
+    a.rnsp[i] = nsp;
+    if (count > a.mc) atomicOr(&a.status[s], 0x1u);
+    atomicMax(a.max_count, count);
+  }
+}
+
+// ------------------------------------------------------------------ PME influence function
+// G(m) = exp(-pi^2 |m*|^2 / beta^2) / (2 pi V |m*|^2) / (b1 b2 b3), 0 at m = 0 (pme.py:243-267),
+// on the half spectrum, computed in FP64, stored in T; recomputed only when the box changed.
+template <typename T>
+__global__ void k_influence(Dev<T> a, long long total) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+    int s = 0;
+    while (s + 1 < a.nsys && a.sys[s + 1].cgrid0 <= g) ++s;
+    const SysInfo &S = a.sys[s];
+    const BoxInfo &B = a.box[s];
+    if (!B.changed) continue;
+    long long l = g - S.cgrid0;
+    int m3 = (int)(l % S.K3h);
+    long long t = l / S.K3h;
+    int k2 = (int)(t % S.K[1]), k1 = (int)(t / S.K[1]);
+    int m1 = k1 <= (S.K[0] - 1) / 2 ? k1 : k1 - S.K[0];
+    int m2 = k2 <= (S.K[1] - 1) / 2 ? k2 : k2 - S.K[1];
+    if (S.K[0] % 2 == 0 && k1 == S.K[0] / 2) m1 = -S.K[0] / 2;
+    if (S.K[1] % 2 == 0 && k2 == S.K[1] / 2) m2 = -S.K[1] / 2;
+    double mv[3];
+    for (int c = 0; c < 3; ++c) mv[c] = m1 * B.Hinv[c * 3 + 0] + m2 * B.Hinv[c * 3 + 1] + m3 * B.Hinv[c * 3 + 2];
+    double msq = mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2];
+    double G = 0.0;
+    if (msq > 0) {
+      G = exp(-PI * PI * msq / (a.beta * a.beta)) / (2.0 * PI * B.vol * msq);
+      G /= a.bmod[S.mod0[0] + k1] * a.bmod[S.mod0[1] + k2] * a.bmod[S.mod0[2] + m3];
+    }
+    a.Ginf[g] = T(G);
+  }
+}
+
+// ------------------------------------------------------------------ spread (pme.py:306-337)
+// One warp per atom, the P^3 stencil over the lanes, atomic adds into the system's grid.  With
+// UPDATE_P the CG direction is first advanced, p = z + beta p (forcefield.py:1812), and spread.
+template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT>
+__global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
+  __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
+  if (ACT == 1 && !a.cg[s].active) return;
+  if (ACT == 2 && !a.cg[s].sweep2) return;
+  v4<T> d;
+  if (UPDATE_P) {
+    v4<T> z = a.Z[i], p = a.P[i];
+    T bt = T(a.cg[s].beta);
+    d.x = z.x + bt * p.x; d.y = z.y + bt * p.y; d.z = z.z + bt * p.z; d.w = T(0);
+    __syncwarp();
+    if (lane == 0) a.P[i] = d;
+  } else {
+    d = vin[i];
+  }
+  const BoxInfo &B = a.box[s];
+  int4 b = a.base[i];
+  v4<T> f = a.frac[i];
+  if (lane < 3) {
+    T th[P], dth[P];
+    bspline<T, P, false>(lane == 0 ? f.x : (lane == 1 ? f.y : f.z), th, dth, nullptr);
+#pragma unroll
+    for (int k = 0; k < P; ++k) { sh[warp][0][lane][k] = th[k]; sh[warp][1][lane][k] = dth[k]; }
+  }
+  __syncwarp();
+  T e[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax)
+    e[ax] = T((double(d.x) * B.Hinv[0 * 3 + ax] + double(d.y) * B.Hinv[1 * 3 + ax] + double(d.z) * B.Hinv[2 * 3 + ax]) * S.K[ax]);
+  T qi = WITH_Q ? a.q[i] : T(0);
+  T *grid = a.Q + S.rgrid0;
+  const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2];
+  for (int p = lane; p < P * P * P; p += 32) {
+    int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
+    T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2], t3 = sh[warp][0][2][j3];
+    T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2], u3 = sh[warp][1][2][j3];
+    T v = (qi * t1 + e[0] * u1) * t2 * t3 + e[1] * t1 * u2 * t3 + e[2] * t1 * t2 * u3;
+    int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
+    int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
+    int i3 = b.z + j3; if (i3 >= K3) i3 -= K3;
+    atomicAdd(grid + ((size_t)i1 * K2 + i2) * K3 + i3, v);
+  }
+}
+
+// ------------------------------------------------------------------ FFT (shared memory, Stockham)
+template <typename T>
+__device__ __forceinline__ c2<T> cmul(c2<T> a, c2<T> b) {
+  c2<T> r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+
+// In-shared-memory Stockham autosort FFT of `nl` lines of length L (line stride ld) by the
+// block; radices 2, 3, 4, 5; sign -1 forward, +1 inverse; tw[m] = exp(-2 pi i m / L).  Returns
+// the buffer that holds the result.
+template <typename T>
+__device__ c2<T> *fft_lines(c2<T> *x, c2<T> *y, int L, int nl, int ld, const int *rad, int nst, const c2<T> *tw, int sign) {
+  int Ns = 1;
+  for (int st = 0; st < nst; ++st) {
+    const int R = rad[st];
+    const int LR = L / R;
+    const int stride = L / (Ns * R);
+    for (int w = threadIdx.x; w < LR * nl; w += blockDim.x) {
+      int line = w / LR, j = w - line * LR;
+      const c2<T> *in = x + line * ld;
+      c2<T> *out = y + line * ld;
+      int k = j % Ns;
+      c2<T> v[5];
+      for (int r = 0; r < R; ++r) {
+        c2<T> u = in[j + r * LR];
+        if (r > 0 && Ns > 1) {
+          c2<T> t = tw[(r * k * stride) % L];
+          if (sign > 0) t.y = -t.y;
+          u = cmul<T>(u, t);
+        }
+        v[r] = u;
+      }
+      const T sg = T(sign);
+      c2<T> o[5];
+      if (R == 2) {
+        o[0].x = v[0].x + v[1].x; o[0].y = v[0].y + v[1].y;
+        o[1].x = v[0].x - v[1].x; o[1].y = v[0].y - v[1].y;
+      } else if (R == 4) {
+        c2<T> a0, a1, b0, b1;
+        a0.x = v[0].x + v[2].x; a0.y = v[0].y + v[2].y;
+        a1.x = v[0].x - v[2].x; a1.y = v[0].y - v[2].y;
+        b0.x = v[1].x + v[3].x; b0.y = v[1].y + v[3].y;
+        b1.x = v[1].x - v[3].x; b1.y = v[1].y - v[3].y;
+        // sign * i * b1
+        c2<T> ib1;
+        ib1.x = -sg * b1.y; ib1.y = sg * b1.x;
+        o[0].x = a0.x + b0.x; o[0].y = a0.y + b0.y;
+        o[2].x = a0.x - b0.x; o[2].y = a0.y - b0.y;
+        o[1].x = a1.x + ib1.x; o[1].y = a1.y + ib1.y;
+        o[3].x = a1.x - ib1.x; o[3].y = a1.y - ib1.y;
+      } else if (R == 3) {
+        const T c = T(-0.5), sn = sg * T(0.86602540378443864676);
+        c2<T> t1, t2;
+        t1.x = v[1].x + v[2].x; t1.y = v[1].y + v[2].y;
+        t2.x = v[1].x - v[2].x; t2.y = v[1].y - v[2].y;
+        o[0].x = v[0].x + t1.x; o[0].y = v[0].y + t1.y;
+        c2<T> m;
+        m.x = v[0].x + c * t1.x; m.y = v[0].y + c * t1.y;
+        // +- i sn t2
+        o[1].x = m.x - sn * t2.y; o[1].y = m.y + sn * t2.x;
+        o[2].x = m.x + sn * t2.y; o[2].y = m.y - sn * t2.x;
+      } else {  // R == 5
+        const T c1 = T(0.30901699437494742410), c2v = T(-0.80901699437494742410);
+        const T s1 = sg * T(0.95105651629515357212), s2 = sg * T(0.58778525229247312917);
+        c2<T> a1, a2, b1, b2;
+        a1.x = v[1].x + v[4].x; a1.y = v[1].y + v[4].y;
+        b1.x = v[1].x - v[4].x; b1.y = v[1].y - v[4].y;
+        a2.x = v[2].x + v[3].x; a2.y = v[2].y + v[3].y;
+        b2.x = v[2].x - v[3].x; b2.y = v[2].y - v[3].y;
+        o[0].x = v[0].x + a1.x + a2.x; o[0].y = v[0].y + a1.y + a2.y;
+        c2<T> m1, m2, n1, n2;
+        m1.x = v[0].x + c1 * a1.x + c2v * a2.x; m1.y = v[0].y + c1 * a1.y + c2v * a2.y;
+        m2.x = v[0].x + c2v * a1.x + c1 * a2.x; m2.y = v[0].y + c2v * a1.y + c1 * a2.y;
+        n1.x = s1 * b1.x + s2 * b2.x; n1.y = s1 * b1.y + s2 * b2.y;
+        n2.x = s2 * b1.x - s1 * b2.x; n2.y = s2 * b1.y - s1 * b2.y;
+        // o1 = m1 + i n1, o4 = m1 - i n1, o2 = m2 + i n2, o3 = m2 - i n2
+        o[1].x = m1.x - n1.y; o[1].y = m1.y + n1.x;
+        o[4].x = m1.x + n1.y; o[4].y = m1.y - n1.x;
+        o[2].x = m2.x - n2.y; o[2].y = m2.y + n2.x;
+        o[3].x = m2.x + n2.y; o[3].y = m2.y - n2.x;
+      }
+      int dst = (j / Ns) * Ns * R + k;
+      for (int r = 0; r < R; ++r) out[dst + r * Ns] = o[r];
+    }
+    __syncthreads();
+    c2<T> *t = x; x = y; y = t;
+    Ns *= R;
+  }
+  return x;
+}
+
+// Which system a CTA of an FFT pass belongs to: tile prefix per system in `tile0` (nsys + 1).
+__device__ __forceinline__ int tile_system(const int *tile0, int nsys, int b) {
+  int s = 0;
+  while (s + 1 < nsys && tile0[s + 1] <= b) ++s;
+  return s;
+}
+
+// k3 pass, real -> half complex: two real lines packed as one complex line (z = a + i b), one
+// length-K3 FFT, untangled; the real grid is cleared as it is read (ready for the next spread).
+template <typename T, int ACT>
+__global__ void k_fft_x_fwd(Dev<T> a, const int *tile0) {
+  extern __shared__ unsigned char smem_raw[];
+  int s = tile_system(tile0, a.nsys, blockIdx.x);
+  if (ACT == 1 && !a.cg[s].active) return;
+  if (ACT == 2 && !a.cg[s].sweep2) return;
+  const SysInfo &S = a.sys[s];
+  const int K3 = S.K[2], K3h = S.K3h, nlines = S.K[0] * S.K[1];
+  int tile = blockIdx.x - tile0[s];
+  int l0 = tile * 2 * FFT_PAIRS;  // first real line
+  int np = min(FFT_PAIRS, (nlines - l0) / 2);
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3;
+  T *Q = a.Q + S.rgrid0 + (size_t)l0 * K3;
+  for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
+    int rl = t / K3, k = t - rl * K3;
+    T v = Q[t];
+    Q[t] = T(0);
+    T *dst = reinterpret_cast<T *>(&x[(rl >> 1) * K3 + k]);
+    dst[rl & 1] = v;
+  }
+  __syncthreads();
+  c2<T> *res = fft_lines<T>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], -1);
+  c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
+  for (int t = threadIdx.x; t < np * K3h; t += blockDim.x) {
+    int cl = t / K3h, m = t - cl * K3h;
+    c2<T> Z = res[cl * K3 + m], W = res[cl * K3 + (m == 0 ? 0 : K3 - m)];
+    c2<T> A, Bv;
+    A.x = T(0.5) * (Z.x + W.x); A.y = T(0.5) * (Z.y - W.y);
+    // (Z - conj W) / (2 i)
+    T dx = Z.x - W.x, dy = Z.y + W.y;
+    Bv.x = T(0.5) * dy; Bv.y = -T(0.5) * dx;
+    C[(size_t)(2 * cl) * K3h + m] = A;
+    C[(size_t)(2 * cl + 1) * K3h + m] = Bv;
+  }
+}
+
+// k3 pass, half complex -> real (the inverse of k_fft_x_fwd, unnormalised): writes phi.
+template <typename T, int ACT>
+__global__ void k_fft_x_inv(Dev<T> a, const int *tile0) {
+  extern __shared__ unsigned char smem_raw[];
+  int s = tile_system(tile0, a.nsys, blockIdx.x);
+  if (ACT == 1 && !a.cg[s].active) return;
+  if (ACT == 2 && !a.cg[s].sweep2) return;
+  const SysInfo &S = a.sys[s];
+  const int K3 = S.K[2], K3h = S.K3h, nlines = S.K[0] * S.K[1];
+  int tile = blockIdx.x - tile0[s];
+  int l0 = tile * 2 * FFT_PAIRS;
+  int np = min(FFT_PAIRS, (nlines - l0) / 2);
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3;
+  const c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
+  for (int t = threadIdx.x; t < np * K3; t += blockDim.x) {
+    int cl = t / K3, m = t - cl * K3;
+    bool up = m > K3 / 2;
+    int mm = up ? K3 - m : m;
+    c2<T> A = C[(size_t)(2 * cl) * K3h + mm], Bv = C[(size_t)(2 * cl + 1) * K3h + mm];
+    if (mm == 0 || 2 * mm == K3) { A.y = T(0); Bv.y = T(0); }
+    if (up) { A.y = -A.y; Bv.y = -Bv.y; }
+    c2<T> Z;
+    Z.x = A.x - Bv.y; Z.y = A.y + Bv.x;
+    x[cl * K3 + m] = Z;
+  }
+  __syncthreads();
+  c2<T> *res = fft_lines<T>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], +1);
+  T *Phi = a.Phi + S.rgrid0 + (size_t)l0 * K3;
+  for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
+    int rl = t / K3, k = t - rl * K3;
+    c2<T> z = res[(rl >> 1) * K3 + k];
+    Phi[t] = (rl & 1) ? z.y : z.x;
+  }
+}
+
+// k2 pass (both directions): tiles of FFT_TILE consecutive m3 at one k1.
+template <typename T, int ACT>
+__global__ void k_fft_y(Dev<T> a, const int *tile0, int sign) {
+  extern __shared__ unsigned char smem_raw[];
+  int s = tile_system(tile0, a.nsys, blockIdx.x);
+  if (ACT == 1 && !a.cg[s].active) return;
+  if (ACT == 2 && !a.cg[s].sweep2) return;
+  const SysInfo &S = a.sys[s];
+  const int K2 = S.K[1], K3h = S.K3h;
+  const int ntile3 = (K3h + FFT_TILE - 1) / FFT_TILE;
+  int tile = blockIdx.x - tile0[s];
+  int k1 = tile / ntile3, m30 = (tile % ntile3) * FFT_TILE;
+  const int ld = K2 + 1;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld;
+  c2<T> *C = a.C + S.cgrid0 + (size_t)k1 * K2 * K3h;
+  for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
+    int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
+    int m3 = m30 + c;
+    c2<T> v;
+    v.x = T(0); v.y = T(0);
+    if (m3 < K3h) v = C[(size_t)k2 * K3h + m3];
+    x[c * ld + k2] = v;
+  }
+  __syncthreads();
+  c2<T> *res = fft_lines<T>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], a.tw + S.tw[1], sign);
+  for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
+    int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
+    int m3 = m30 + c;
+    if (m3 < K3h) C[(size_t)k2 * K3h + m3] = res[c * ld + k2];
+  }
+}
+
+// k1 pass with the convolution: forward FFT along k1, multiply by 2 G(m) (phi = dE/dQ =
+// 2 K^3 irfft(G F[Q]), pme.py:370-376), inverse FFT.  With ENERGY the reciprocal energy
+// sum w3 G |F|^2 (pme.py:390-411) and the influence part of the virial are accumulated.
+template <typename T, int ACT, bool ENERGY>
+__global__ void k_fft_z_conv(Dev<T> a, const int *tile0) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ double red[7][8];
+  int s = tile_system(tile0, a.nsys, blockIdx.x);
+  if (ACT == 1 && !a.cg[s].active) return;
+  if (ACT == 2 && !a.cg[s].sweep2) return;
+  const SysInfo &S = a.sys[s];
+  const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2], K3h = S.K3h;
+  const int ntile3 = (K3h + FFT_TILE - 1) / FFT_TILE;
+  int tile = blockIdx.x - tile0[s];
+  int k2 = tile / ntile3, m30 = (tile % ntile3) * FFT_TILE;
+  const int ld = K1 + 1;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld;
+  c2<T> *C = a.C + S.cgrid0 + (size_t)k2 * K3h;
+  const size_t rs = (size_t)K2 * K3h;
+  for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
+    int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
+    int m3 = m30 + c;
+    c2<T> v;
+    v.x = T(0); v.y = T(0);
+    if (m3 < K3h) v = C[k1 * rs + m3];
+    x[c * ld + k1] = v;
+  }
+  __syncthreads();
+  c2<T> *res = fft_lines<T>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], -1);
+  c2<T> *oth = res == x ? y : x;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  const BoxInfo &B = a.box[s];
+  const T *G = a.Ginf + S.cgrid0 + (size_t)k2 * K3h;
+  for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
+    int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
+    int m3 = m30 + c;
+    if (m3 >= K3h) continue;
+    T g = G[k1 * rs + m3];
+    c2<T> F = res[c * ld + k1];
+    if (ENERGY && g != T(0)) {
+      double w3 = (m3 == 0 || 2 * m3 == K3) ? 1.0 : 2.0;
+      double e = w3 * double(g) * (double(F.x) * double(F.x) + double(F.y) * double(F.y));
+      int m1 = k1 <= (K1 - 1) / 2 ? k1 : k1 - K1;
+      int m2 = k2 <= (K2 - 1) / 2 ? k2 : k2 - K2;
+      if (K1 % 2 == 0 && k1 == K1 / 2) m1 = -K1 / 2;
+      if (K2 % 2 == 0 && k2 == K2 / 2) m2 = -K2 / 2;
+      double mv[3];
+      for (int cc = 0; cc < 3; ++cc) mv[cc] = m1 * B.Hinv[cc * 3 + 0] + m2 * B.Hinv[cc * 3 + 1] + m3 * B.Hinv[cc * 3 + 2];
+      double msq = mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2];
+      double fac = 2.0 * (PI * PI / (a.beta * a.beta) + 1.0 / msq);
+      acc[0] += e;
+      acc[1] += e * (fac * mv[0] * mv[0] - 1.0);
+      acc[2] += e * (fac * mv[1] * mv[1] - 1.0);
+      acc[3] += e * (fac * mv[2] * mv[2] - 1.0);
+      acc[4] += e * fac * mv[0] * mv[1];
+      acc[5] += e * fac * mv[0] * mv[2];
+      acc[6] += e * fac * mv[1] * mv[2];
+    }
+    T g2 = T(2) * g;
+    F.x *= g2; F.y *= g2;
+    res[c * ld + k1] = F;
+  }
+  if (ENERGY) {
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = 0; k < 7; ++k) {
+      double v = warp_sum<double>(acc[k]);
+      if (lane == 0) red[k][warp] = v;
+    }
+  }
+  __syncthreads();
+  if (ENERGY && threadIdx.x < 7) {
+    double v = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+    atomicAdd(&a.eacc[s].vinf[threadIdx.x], v);
+  }
+  c2<T> *res2 = fft_lines<T>(res, oth, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], +1);
+  for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
+    int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
+    int m3 = m30 + c;
+    if (m3 < K3h) C[k1 * rs + m3] = res2[c * ld + k1];
+  }
+}
+
+// ------------------------------------------------------------------ row field + PME gather
+// One warp per atom.  s_i = sum_k de_ik/dd_i (forcefield.py:1395-1402) + dU_rec/dd_i
+// (pme.py:378-388), then by MODE:
+//   0 FIELD  out = -(s - c_self d)                       (forcefield.py:1428-1433)
+//   1 OPER   out = d / alpha + s - c_self d, and p.Ap    (forcefield.py:1694-1712, 1806-1807)
+template <typename T, int P, bool WITH_Q, int MODE, int ACT>
+__global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
+  __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
+  __shared__ double red[WARPS_PER_BLOCK];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  bool valid = i < S.atom0 + S.natom;
+  if (ACT == 1 && !a.cg[s].active) return;   // uniform over the block
+  if (ACT == 2 && !a.cg[s].sweep2) return;
+  double dotv = 0.0;
+  if (valid) {
+    int n = min(a.rn[i], a.mc);
+    size_t base = (size_t)i * a.mc;
+    T f0 = 0, f1 = 0, f2 = 0;
+    for (int t = lane; t < n; t += 32) {
+      size_t o = base + t;
+      int k = a.rk[o];
+      T x = a.rx[o], y = a.ry[o], z = a.rz[o], g1 = a.rg1[o], g2 = a.rg2[o];
+      v4<T> dk = D[k];
+      T dkx = dk.x * x + dk.y * y + dk.z * z;
+      T c = -g2 * dkx;
+      if (WITH_Q) c -= a.q[k] * g1;
+      f0 += c * x + g1 * dk.x;
+      f1 += c * y + g1 * dk.y;
+      f2 += c * z + g1 * dk.z;
+    }
+    const BoxInfo &B = a.box[s];
+    int4 b = a.base[i];
+    v4<T> fr = a.frac[i];
+    if (lane < 3) {
+      T th[P], dth[P];
+      bspline<T, P, false>(lane == 0 ? fr.x : (lane == 1 ? fr.y : fr.z), th, dth, nullptr);
+#pragma unroll
+      for (int k = 0; k < P; ++k) { sh[warp][0][lane][k] = th[k]; sh[warp][1][lane][k] = dth[k]; }
+    }
+    __syncwarp();
+    const T *phi = a.Phi + S.rgrid0;
+    const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2];
+    T g0 = 0, g1 = 0, g2 = 0;
+    for (int p = lane; p < P * P * P; p += 32) {
+      int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
+      int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
+      int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
+      int i3 = b.z + j3; if (i3 >= K3) i3 -= K3;
+      T ph = phi[((size_t)i1 * K2 + i2) * K3 + i3];
+      T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2], t3 = sh[warp][0][2][j3];
+      T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2], u3 = sh[warp][1][2][j3];
+      g0 += ph * u1 * t2 * t3;
+      g1 += ph * t1 * u2 * t3;
+      g2 += ph * t1 * t2 * u3;
+    }
+    f0 = warp_sum<T>(f0); f1 = warp_sum<T>(f1); f2 = warp_sum<T>(f2);
+    g0 = warp_sum<T>(g0); g1 = warp_sum<T>(g1); g2 = warp_sum<T>(g2);
+    if (lane == 0) {
+      // dU/dd_b = sum_a g_a Hinv[b][a] K_a
+      T es[9];
+#pragma unroll
+      for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa) es[bb * 3 + aa] = T(B.Hinv[bb * 3 + aa] * S.K[aa]);
+      T r0 = g0 * es[0] + g1 * es[1] + g2 * es[2];
+      T r1 = g0 * es[3] + g1 * es[4] + g2 * es[5];
+      T r2 = g0 * es[6] + g1 * es[7] + g2 * es[8];
+      v4<T> di = D[i];
+      T cs = T(a.c_self);
+      v4<T> o;
+      if (MODE == 0) {
+        o.x = -(f0 + r0 - cs * di.x); o.y = -(f1 + r1 - cs * di.y); o.z = -(f2 + r2 - cs * di.z);
+      } else {
+        T ia = a.ialpha[i];
+        o.x = di.x * ia + f0 + r0 - cs * di.x;
+        o.y = di.y * ia + f1 + r1 - cs * di.y;
+        o.z = di.z * ia + f2 + r2 - cs * di.z;
+        dotv = double(di.x * o.x) + double(di.y * o.y) + double(di.z * o.z);
+      }
+      o.w = T(0);
+      out[i] = o;
+    }
+  }
+  if (MODE == 1) {
+    if (lane == 0) red[warp] = dotv;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = 0;
+      for (int w = 0; w < WARPS_PER_BLOCK; ++w) v += red[w];
+      atomicAdd(&a.cg[s].acc_pap, v);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ CG
+// Start, step 1 (thread per atom): the predictor guess x0h = sum c_j hist_j (forcefield.py:605,
+// 1956-1958) and the dipoles of the first field sweep: p + x0h (fused start) or p (plain).
+template <typename T>
+__global__ void k_start1(Dev<T> a, const double *hist, int K, double c0, double c1, double c2, double c3) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  int s = a.sysid[i];
+  const CGSys &G = a.cg[s];
+  double x0[3] = {0, 0, 0};
+  if (G.have) {
+    const double cc[4] = {c0, c1, c2, c3};
+    for (int j = 0; j < K; ++j)
+      for (int c = 0; c < 3; ++c) x0[c] += cc[j] * hist[((size_t)j * a.nt + i) * 3 + c];
+  }
+  double4 p = a.pperm[i];
+  v4<T> d, x;
+  if (G.fused) { d.x = T(p.x + x0[0]); d.y = T(p.y + x0[1]); d.z = T(p.z + x0[2]); }
+  else { d.x = T(p.x); d.y = T(p.y); d.z = T(p.z); }
+  d.w = T(0);
+  x.x = T(x0[0]); x.y = T(x0[1]); x.z = T(x0[2]); x.w = T(0);
+  a.D[i] = d;
+  a.X[i] = x;
+}
+
+// Start, step 2: fused: r0 = field(q, p + x0) - x0 / alpha; plain: b = field(q, p), the norm
+// mean|alpha b| and, without history, x0 = alpha b (forcefield.py:1960-1997).
+template <typename T>
+__global__ void k_start2(Dev<T> a) {
+  __shared__ double red[THREADS_PER_BLOCK / 32];
+  int s = a.tb_sys[blockIdx.x];
+  int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const SysInfo &S = a.sys[s];
+  CGSys &G = a.cg[s];
+  double sab = 0.0;
+  if (i < S.atom0 + S.natom) {
+    v4<T> b = a.B[i];
+    v4<T> x = a.X[i];
+    T al = a.alpha[i];
+    if (G.fused) {
+      T ia = a.ialpha[i];
+      v4<T> r;
+      r.x = b.x - x.x * ia; r.y = b.y - x.y * ia; r.z = b.z - x.z * ia; r.w = T(0);
+      a.R[i] = r;
+    } else {
+      double ax = double(a.alpha[i]) * double(b.x), ay = double(a.alpha[i]) * double(b.y), az = double(a.alpha[i]) * double(b.z);
+      sab = fabs(ax) + fabs(ay) + fabs(az);
+      if (!G.have) { x.x = T(ax); x.y = T(ay); x.z = T(az); x.w = T(0); a.X[i] = x; }
+      (void)al;
+    }
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  sab = warp_sum<double>(sab);
+  if (lane == 0) red[warp] = sab;
+  __syncthreads();
+  if (threadIdx.x == 0 && !G.fused) {
+    double v = 0;
+    for (int w = 0; w < THREADS_PER_BLOCK / 32; ++w) v += red[w];
+    atomicAdd(&G.acc_abs, v);
+  }
+}
+
+// Start, step 3 (plain start only): r0 = b - A x0.
+template <typename T>
+__global__ void k_start3(Dev<T> a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  int s = a.sysid[i];
+  if (a.cg[s].fused) return;
+  v4<T> b = a.B[i], ap = a.AP[i], r;
+  r.x = b.x - ap.x; r.y = b.y - ap.y; r.z = b.z - ap.z; r.w = T(0);
+  a.R[i] = r;
+}
+
+// CG initialisation: z = alpha r, p = z, r.z and max|alpha r| (forcefield.py:1796-1819).
+template <typename T>
+__global__ void k_cg_init(Dev<T> a) {
+  __shared__ double red[THREADS_PER_BLOCK / 32];
+  __shared__ unsigned long long mx[THREADS_PER_BLOCK / 32];
+  int s = a.tb_sys[blockIdx.x];
+  int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const SysInfo &S = a.sys[s];
+  double rz = 0, m = 0;
+  if (i < S.atom0 + S.natom) {
+    v4<T> r = a.R[i];
+    T al = a.alpha[i];
+    v4<T> z;
+    z.x = al * r.x; z.y = al * r.y; z.z = al * r.z; z.w = T(0);
+    a.Z[i] = z;
+    a.P[i] = z;
+    rz = double(r.x * z.x) + double(r.y * z.y) + double(r.z * z.z);
+    m = fmax(fabs(double(z.x)), fmax(fabs(double(z.y)), fabs(double(z.z))));
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  rz = warp_sum<double>(rz);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) { red[warp] = rz; mx[warp] = (unsigned long long)__double_as_longlong(m); }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0;
+    unsigned long long mm = 0;
+    for (int w = 0; w < THREADS_PER_BLOCK / 32; ++w) { v += red[w]; mm = max(mm, mx[w]); }
+    atomicAdd(&a.cg[s].acc_rz, v);
+    atomicMax(&a.cg[s].acc_max, mm);
+  }
+}
+
+// Per-system scalars after the start: norm, r.z, err, active; *any = some system iterates.
+__global__ void k_cg_begin(CGSys *cg, int nsys, double tol, int max_iter, int *any) {
+  __shared__ int act;
+  if (threadIdx.x == 0) act = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+    CGSys &G = cg[s];
+    if (!G.fused) G.norm = G.acc_abs / G.n3 + 1e-300;
+    G.rz = G.acc_rz;
+    G.err = __longlong_as_double((long long)G.acc_max) / G.norm;
+    G.beta = 0.0;
+    G.it = 0;
+    G.active = (G.err > tol) && (max_iter > 0);
+    G.acc_abs = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0; G.acc_num = 0;
+    if (G.active) atomicOr(&act, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *any = act;
+}
+
+// One CG update (thread per atom): x += a p, r' = r - a Ap, z' = alpha r', and the sums of
+// z'.(r' - r), r'.z', max|z'| (forcefield.py:1802-1814).
+template <typename T>
+__global__ void k_cg_update(Dev<T> a) {
+  __shared__ double red[2][THREADS_PER_BLOCK / 32];
+  __shared__ unsigned long long mx[THREADS_PER_BLOCK / 32];
+  int s = a.tb_sys[blockIdx.x];
+  CGSys &G = a.cg[s];
+  if (!G.active) return;
+  int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const SysInfo &S = a.sys[s];
+  double num = 0, rzn = 0, m = 0;
+  if (i < S.atom0 + S.natom) {
+    T st = T(G.rz / fmax(G.acc_pap, 1e-300));
+    v4<T> x = a.X[i], r = a.R[i], p = a.P[i], ap = a.AP[i];
+    T al = a.alpha[i];
+    x.x += st * p.x; x.y += st * p.y; x.z += st * p.z;
+    v4<T> rn, z;
+    rn.x = r.x - st * ap.x; rn.y = r.y - st * ap.y; rn.z = r.z - st * ap.z; rn.w = T(0);
+    z.x = al * rn.x; z.y = al * rn.y; z.z = al * rn.z; z.w = T(0);
+    num = double(z.x * (rn.x - r.x)) + double(z.y * (rn.y - r.y)) + double(z.z * (rn.z - r.z));
+    rzn = double(rn.x * z.x) + double(rn.y * z.y) + double(rn.z * z.z);
+    m = fmax(fabs(double(z.x)), fmax(fabs(double(z.y)), fabs(double(z.z))));
+    a.X[i] = x;
+    a.R[i] = rn;
+    a.Z[i] = z;
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  num = warp_sum<double>(num);
+  rzn = warp_sum<double>(rzn);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) { red[0][warp] = num; red[1][warp] = rzn; mx[warp] = (unsigned long long)__double_as_longlong(m); }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v0 = 0, v1 = 0;
+    unsigned long long mm = 0;
+    for (int w = 0; w < THREADS_PER_BLOCK / 32; ++w) { v0 += red[0][w]; v1 += red[1][w]; mm = max(mm, mx[w]); }
+    atomicAdd(&G.acc_num, v0);
+    atomicAdd(&G.acc_rz, v1);
+    atomicMax(&G.acc_max, mm);
+  }
+}
+
+// Per-system scalars after an update: beta (Polak-Ribiere), r.z, err, iteration count and the
+// loop condition err > tol and it < max_iter (forcefield.py:1798-1816).  *any = some system
+// still iterating.
+__global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *any) {
+  __shared__ int act;
+  if (threadIdx.x == 0) act = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+    CGSys &G = cg[s];
+    if (G.active) {
+      G.beta = G.acc_num / fmax(G.rz, 1e-300);
+      G.rz = G.acc_rz;
+      G.err = __longlong_as_double((long long)G.acc_max) / G.norm;
+      G.it += 1;
+      G.active = (G.err > tol) && (G.it < max_iter);
+    }
+    G.acc_num = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0;
+    if (G.active) atomicOr(&act, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *any = act;
+}
+
+// After the loop: the peek step mu = x + peek alpha r (forcefield.py:1819-1820), the dipoles
+// in FP64, the history push (forcefield.py:2005-2007) and mu + p for the energy pass.
+template <typename T>
+__global__ void k_cg_finish(Dev<T> a, double *mu, double *hist, int push) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  v4<T> x = a.X[i], r = a.R[i];
+  T al = a.alpha[i];
+  T pk = T(a.peek);
+  if (a.peek != 0.0) { x.x += pk * r.x * al; x.y += pk * r.y * al; x.z += pk * r.z * al; }
+  double m[3] = {double(x.x), double(x.y), double(x.z)};
+  for (int c = 0; c < 3; ++c) mu[3 * i + c] = m[c];
+  if (push) {
+    size_t st = (size_t)a.nt * 3;
+    for (int c = 0; c < 3; ++c) {
+      size_t o = (size_t)3 * i + c;
+      hist[3 * st + o] = hist[2 * st + o];
+      hist[2 * st + o] = hist[st + o];
+      hist[st + o] = hist[o];
+      hist[o] = m[c];
+    }
+  }
+}
+
+__global__ void k_cg_state_out(const CGSys *cg, int nsys, int32_t *count, double *norm, int32_t *iters, double *resid,
+                               unsigned *status, int push, double tol) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  const CGSys &G = cg[s];
+  if (push) { count[s] += 1; norm[s] = G.norm; }
+  if (iters) iters[s] = G.it;
+  if (resid) resid[s] = G.err;
+  if (G.err > tol) atomicOr(&status[s], 0x2u);
+}
+
+// Per-system start of a solve: which predictor start applies (forcefield.py:1951-1966).
+// mode 0: history predictor (compute); mode 1: the guess is the state's mu, plain start (energy,
+// forcefield.py:2606-2612).
+__global__ void k_cg_setup(CGSys *cg, int nsys, const int32_t *count, const double *norm, int K, int fused, int refresh,
+                           int mode) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  CGSys &G = cg[s];
+  int c = count ? count[s] : 0;
+  G.have = mode == 1 ? 1 : (K > 0 && c >= K);
+  G.fused = mode == 0 && G.have && fused && (c % refresh) != 0;
+  G.sweep2 = !G.fused;
+  G.active = 0;
+  G.norm = G.fused ? norm[s] : 1.0;
+  G.acc_abs = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0; G.acc_num = 0;
+}
+
+// Energy-only start: x0 = the state's mu, first sweep at d = p.
+template <typename T>
+__global__ void k_energy_start(Dev<T> a, const double *mu) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  double4 p = a.pperm[i];
+  v4<T> d, x;
+  d.x = T(p.x); d.y = T(p.y); d.z = T(p.z); d.w = T(0);
+  x.x = T(mu[3 * i]); x.y = T(mu[3 * i + 1]); x.z = T(mu[3 * i + 2]); x.w = T(0);
+  a.D[i] = d;
+  a.X[i] = x;
+}
+
+// ------------------------------------------------------------------ energy, forces, virial
+// One warp per atom over its row: pair energies and their row gradients with the analytic
+// kernels G0..G3 (forcefield.py:2294-2360), LJ rows, the row field at (q, d) (dE/dd), the pair
+// virial sum g (x) x - gx (x) off; then the PME gradients of the atom: dU/dd and dU/dr through the
+// spline derivatives (the autodiff of pme.py:390-411 written out).
+template <typename T, int P>
+__global__ void __launch_bounds__(256) k_forces(Dev<T> a, const double *mu) {
+  __shared__ T sh[WARPS_PER_BLOCK][3][3][P];
+  __shared__ double red[WARPS_PER_BLOCK][16];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  bool valid = i < S.atom0 + S.natom;
+  double vals[16];
+  for (int k = 0; k < 16; ++k) vals[k] = 0.0;
+  if (valid) {
+    const BoxInfo &B = a.box[s];
+    v4<T> di = a.D[i];
+    T qi = a.q[i], rhi = a.rminh[i], sei = a.seps[i];
+    int n = min(a.rn[i], a.mc), nsp = a.rnsp[i];
+    size_t base = (size_t)i * a.mc;
+    T gx0 = 0, gx1 = 0, gx2 = 0, gl0 = 0, gl1 = 0, gl2 = 0, fd0 = 0, fd1 = 0, fd2 = 0;
+    T ee = 0, el = 0;
+    T w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = lane; t < n; t += 32) {
+      size_t o = base + t;
+      int k = a.rk[o];
+      T x = a.rx[o], y = a.ry[o], z = a.rz[o];
+      T G0 = a.rg0[o], G1 = a.rg1[o], G2 = a.rg2[o], G3 = a.rg3[o];
+      v4<T> dk = a.D[k];
+      T qk = a.q[k];
+      T dix = di.x * x + di.y * y + di.z * z;
+      T dkx = dk.x * x + dk.y * y + dk.z * z;
+      T didk = di.x * dk.x + di.y * dk.y + di.z * dk.z;
+      T tt = qi * dkx - qk * dix;
+      ee += qi * qk * G0 + tt * G1 - G2 * dix * dkx + G1 * didk;
+      T radial = -qi * qk * G1 - tt * G2 + G3 * dix * dkx - G2 * didk;
+      T gxv = radial * x + qi * G1 * dk.x - qk * G1 * di.x - G2 * (di.x * dkx + dk.x * dix);
+      T gyv = radial * y + qi * G1 * dk.y - qk * G1 * di.y - G2 * (di.y * dkx + dk.y * dix);
+      T gzv = radial * z + qi * G1 * dk.z - qk * G1 * di.z - G2 * (di.z * dkx + dk.z * dix);
+      T c = -qk * G1 - G2 * dkx;
+      fd0 += c * x + G1 * dk.x; fd1 += c * y + G1 * dk.y; fd2 += c * z + G1 * dk.z;
+      T kx = T(KE) * gxv, ky = T(KE) * gyv, kz = T(KE) * gzv;
+      if (a.lj && t >= nsp) {
+        T rm = rhi + a.rminh[k], ep = sei * a.seps[k];
+        T r2 = x * x + y * y + z * z;
+        T s2 = rm * rm / r2, s6 = s2 * s2 * s2;
+        el += ep * (s6 * s6 - T(2) * s6);
+        T dl = ep * T(12) * (s6 - s6 * s6) / r2;
+        gl0 += dl * x; gl1 += dl * y; gl2 += dl * z;
+        kx += dl * x; ky += dl * y; kz += dl * z;
+      }
+      gx0 += gxv; gx1 += gyv; gx2 += gzv;
+      w[0] += kx * x; w[1] += kx * y; w[2] += kx * z;
+      w[3] += ky * x; w[4] += ky * y; w[5] += ky * z;
+      w[6] += kz * x; w[7] += kz * y; w[8] += kz * z;
+    }
+    // reciprocal gradients of the atom
+    int4 b = a.base[i];
+    v4<T> fr = a.frac[i];
+    if (lane < 3) {
+      T th[P], dth[P], d2[P];
+      bspline<T, P, true>(lane == 0 ? fr.x : (lane == 1 ? fr.y : fr.z), th, dth, d2);
+#pragma unroll
+      for (int k = 0; k < P; ++k) { sh[warp][0][lane][k] = th[k]; sh[warp][1][lane][k] = dth[k]; sh[warp][2][lane][k] = d2[k]; }
+    }
+    __syncwarp();
+    T es[9];
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+      for (int aa = 0; aa < 3; ++aa) es[bb * 3 + aa] = T(B.Hinv[bb * 3 + aa] * S.K[aa]);
+    T e0 = di.x * es[0] + di.y * es[3] + di.z * es[6];
+    T e1 = di.x * es[1] + di.y * es[4] + di.z * es[7];
+    T e2 = di.x * es[2] + di.y * es[5] + di.z * es[8];
+    const T *phi = a.Phi + S.rgrid0;
+    const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2];
+    T ge0 = 0, ge1 = 0, ge2 = 0, gw0 = 0, gw1 = 0, gw2 = 0;
+    for (int p = lane; p < P * P * P; p += 32) {
+      int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
+      int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
+      int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
+      int i3 = b.z + j3; if (i3 >= K3) i3 -= K3;
+      T ph = phi[((size_t)i1 * K2 + i2) * K3 + i3];
+      T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2], t3 = sh[warp][0][2][j3];
+      T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2], u3 = sh[warp][1][2][j3];
+      T v1 = sh[warp][2][0][j1], v2 = sh[warp][2][1][j2], v3 = sh[warp][2][2][j3];
+      ge0 += ph * u1 * t2 * t3;
+      ge1 += ph * t1 * u2 * t3;
+      ge2 += ph * t1 * t2 * u3;
+      gw0 += ph * (qi * u1 * t2 * t3 + e0 * v1 * t2 * t3 + e1 * u1 * u2 * t3 + e2 * u1 * t2 * u3);
+      gw1 += ph * (qi * t1 * u2 * t3 + e0 * u1 * u2 * t3 + e1 * t1 * v2 * t3 + e2 * t1 * u2 * u3);
+      gw2 += ph * (qi * t1 * t2 * u3 + e0 * u1 * t2 * u3 + e1 * t1 * u2 * u3 + e2 * t1 * t2 * v3);
+    }
+    T red_in[24] = {gx0, gx1, gx2, gl0, gl1, gl2, fd0, fd1, fd2, ee, el, ge0, ge1, ge2, gw0, gw1, gw2,
+                    w[0], w[1], w[2], w[3], w[4], w[5], w[6]};
+#pragma unroll
+    for (int k = 0; k < 24; ++k) red_in[k] = warp_sum<T>(red_in[k]);
+    T w7 = warp_sum<T>(w[7]), w8 = warp_sum<T>(w[8]);
+    if (lane == 0) {
+      double gd[3], gr[3];
+      for (int bb = 0; bb < 3; ++bb) {
+        gd[bb] = double(red_in[11]) * double(es[bb * 3 + 0]) + double(red_in[12]) * double(es[bb * 3 + 1]) + double(red_in[13]) * double(es[bb * 3 + 2]);
+        gr[bb] = double(red_in[14]) * double(es[bb * 3 + 0]) + double(red_in[15]) * double(es[bb * 3 + 1]) + double(red_in[16]) * double(es[bb * 3 + 2]);
+      }
+      double d3[3] = {double(di.x), double(di.y), double(di.z)};
+      double gx[3] = {double(red_in[0]), double(red_in[1]), double(red_in[2])};
+      double gl[3] = {double(red_in[3]), double(red_in[4]), double(red_in[5])};
+      double fd[3] = {double(red_in[6]), double(red_in[7]), double(red_in[8])};
+      double4 of = a.off[i];
+      double ofs[3] = {of.x, of.y, of.z};
+      double cs = a.c_self;
+      double dE[3];
+      for (int c = 0; c < 3; ++c) {
+        a.forces[3 * i + c] = -(KE * gx[c] + gl[c] + KE * gr[c]);
+        dE[c] = KE * (fd[c] + gd[c] - cs * d3[c]);
+      }
+      a.dEdd[i] = make_double4(dE[0], dE[1], dE[2], 0);
+      vals[0] = double(red_in[9]);
+      vals[1] = double(red_in[10]);
+      vals[2] = d3[0] * d3[0] + d3[1] * d3[1] + d3[2] * d3[2];
+      if (a.induce && mu) {
+        double m0 = mu[3 * i], m1 = mu[3 * i + 1], m2 = mu[3 * i + 2];
+        vals[3] = (m0 * m0 + m1 * m1 + m2 * m2) / (2.0 * double(a.alpha[i]));
+      }
+      // virial: 1/2 sum_rows g (x) x - (KE gx + gl) (x) off - KE (dU/dr (x) off + dU/dd (x) d)
+      double wsum[9] = {double(red_in[17]), double(red_in[18]), double(red_in[19]), double(red_in[20]), double(red_in[21]),
+                        double(red_in[22]), double(red_in[23]), double(w7), double(w8)};
+      for (int aa = 0; aa < 3; ++aa)
+        for (int bb = 0; bb < 3; ++bb)
+          vals[4 + aa * 3 + bb] = 0.5 * wsum[aa * 3 + bb] - (KE * gx[aa] + gl[aa]) * ofs[bb] - KE * (gr[aa] * ofs[bb] + gd[aa] * d3[bb]);
+    }
+  }
+  if (lane == 0)
+    for (int k = 0; k < 13; ++k) red[warp][k] = vals[k];
+  __syncthreads();
+  if (threadIdx.x < 13) {
+    double v = 0;
+    for (int w2 = 0; w2 < WARPS_PER_BLOCK; ++w2) v += red[w2][threadIdx.x];
+    EnergyAcc &E = a.eacc[s];
+    double *dst = threadIdx.x == 0 ? &E.e_pair : threadIdx.x == 1 ? &E.e_lj : threadIdx.x == 2 ? &E.d2
+                  : threadIdx.x == 3 ? &E.upol : &E.vir[threadIdx.x - 4];
+    atomicAdd(dst, v);
+  }
+}
+
+// Covalent-dipole frames: p_i = sum c unit(r_j - r_i); the pull-back of dE/dd_i onto r_i and r_j
+// (the vector-Jacobian product of forcefield.py:2412).  One thread per covalent dipole.
+template <typename T>
+__global__ void k_cov_forces(Dev<T> a) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.ncov || !a.perm) return;
+  int i = a.cov_i_flat[m], j = a.cov_j_flat[m];
+  const BoxInfo &B = a.box[a.sysid[i]];
+  double vx = a.pos[3 * j] - a.pos[3 * i], vy = a.pos[3 * j + 1] - a.pos[3 * i + 1], vz = a.pos[3 * j + 2] - a.pos[3 * i + 2];
+  min_image(vx, vy, vz, B.H);
+  double l = sqrt(vx * vx + vy * vy + vz * vz);
+  double ux = vx / l, uy = vy / l, uz = vz / l;
+  double4 g = a.dEdd[i];
+  double ug = ux * g.x + uy * g.y + uz * g.z;
+  double c = a.cov_c_flat[m] / l;
+  double gx = c * (g.x - ux * ug), gy = c * (g.y - uy * ug), gz = c * (g.z - uz * ug);
+  atomicAdd(&a.forces[3 * j], -gx); atomicAdd(&a.forces[3 * j + 1], -gy); atomicAdd(&a.forces[3 * j + 2], -gz);
+  atomicAdd(&a.forces[3 * i], gx); atomicAdd(&a.forces[3 * i + 1], gy); atomicAdd(&a.forces[3 * i + 2], gz);
+}
+
+// Energies and virial of every system (forcefield.py:2011-2045, 2420-2430, lj.py:87-114):
+// E_elec = KE [rows/2 + U_rec + U_self + U_bg + U_pol], E_vdw = rows/2 + tail.
+__global__ void k_energy_finish(const SysInfo *sys, const BoxInfo *box, const EnergyAcc *E, int nsys, double beta, double c_self,
+                                double cutoff, int lj, int lj_lrc, int induce, double *energy, double *virial, unsigned *status) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  const EnergyAcc &e = E[s];
+  const SysInfo &S = sys[s];
+  double vol = box[s].vol;
+  double uself = -(beta / SQRT_PI) * S.sum_q2 - 0.5 * c_self * e.d2;
+  double ubg = -PI * S.sum_q * S.sum_q / (2.0 * vol * beta * beta);
+  double upol = induce ? e.upol : 0.0;
+  double elec = 0.5 * KE * e.e_pair + KE * (e.vinf[0] + uself + ubg + upol);
+  double tail = (lj && lj_lrc) ? -2.0 * PI * S.tail_sb / (3.0 * vol * cutoff * cutoff * cutoff) : 0.0;
+  double vdw = 0.5 * e.e_lj + tail;
+  if (energy) {
+    energy[3 * s] = elec;
+    energy[3 * s + 1] = vdw;
+    energy[3 * s + 2] = elec + vdw;
+  }
+  if (!isfinite(elec + vdw)) atomicOr(&status[s], 0x4u);
+  if (virial) {
+    double W[9];
+    for (int k = 0; k < 9; ++k) W[k] = e.vir[k];
+    W[0] += KE * e.vinf[1]; W[4] += KE * e.vinf[2]; W[8] += KE * e.vinf[3];
+    W[1] += KE * e.vinf[4]; W[3] += KE * e.vinf[4];
+    W[2] += KE * e.vinf[5]; W[6] += KE * e.vinf[5];
+    W[5] += KE * e.vinf[6]; W[7] += KE * e.vinf[6];
+    for (int c = 0; c < 3; ++c) W[4 * c] += -KE * ubg - 2.0 * tail;
+    for (int k = 0; k < 9; ++k) virial[9 * s + k] = W[k];
+  }
+}
+
+// d = p + mu (energy pass), in T.
+template <typename T>
+__global__ void k_total_dipoles(Dev<T> a, const double *mu) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  double4 p = a.pperm[i];
+  double m0 = mu ? mu[3 * i] : 0.0, m1 = mu ? mu[3 * i + 1] : 0.0, m2 = mu ? mu[3 * i + 2] : 0.0;
+  v4<T> d;
+  d.x = T(p.x + m0); d.y = T(p.y + m1); d.z = T(p.z + m2); d.w = T(0);
+  a.D[i] = d;
+}
+
+// Copy of a (N, 3) FP64 array into v4<T> (pgm_field input).
+template <typename T>
+__global__ void k_load_vec(Dev<T> a, const double *v, v4<T> *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  v4<T> d;
+  d.x = T(v[3 * i]); d.y = T(v[3 * i + 1]); d.z = T(v[3 * i + 2]); d.w = T(0);
+  out[i] = d;
+}
+
+template <typename T>
+__global__ void k_store_vec(Dev<T> a, const v4<T> *in, double *v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  v4<T> d = in[i];
+  v[3 * i] = double(d.x); v[3 * i + 1] = double(d.y); v[3 * i + 2] = double(d.z);
+}
+
+}  // namespace pgm

@@ -1,0 +1,211 @@
+"""Parity of the sm_100a engine with the FP64 oracle and the reference's golden vectors.
+
+Tolerances: the double-precision engine agrees with the oracle to ~1e-10 relative; mixed precision
+(FP32 pair/PME kernels, FP64 reductions) is held to 1e-6 relative in energy and 1e-5 RMS relative
+in forces and induced dipoles, the bar the reference states for its mixed path against float64.
+"""
+
+import numpy as np
+import pytest
+import torch
+from conftest import SMALL_BOX_SETTINGS
+
+pytestmark = pytest.mark.gpu
+
+import oracle as O  # noqa: E402
+
+
+def ff_for(system, H, prec="double", **kw):
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+
+    st = dict(SMALL_BOX_SETTINGS)
+    st.update(kw)
+    return PGMForceField(system, H, MDSettings(precision=prec, **st))
+
+
+def rms_rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b**2)))
+
+
+@pytest.fixture(scope="module")
+def box(small_box_system, golden_small_box):
+    s, pos, H = small_box_system
+    o = O.Oracle(s, SMALL_BOX_SETTINGS)
+    return s, pos, H, o, o.compute(pos, H)
+
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_field_of_charges_and_dipoles(box, prec):
+    """The field sweep (rows + PME + self term) against the oracle's _field."""
+    s, pos, H, o, _ = box
+    rng = np.random.default_rng(3)
+    d = rng.normal(scale=0.01, size=(s.n, 3))
+    ref = o.field(pos, H, s.q, d)
+    ff = ff_for(s, H, prec)
+    got = ff.field(pos, H, d, charges=True).cpu().numpy()
+    tol = 1e-10 if prec == "double" else 2e-6
+    assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), np.abs(got - ref).max() / np.abs(ref).max()
+    ref0 = o.field(pos, H, None, d)
+    got0 = ff.field(pos, H, d, charges=False).cpu().numpy()
+    assert np.abs(got0 - ref0).max() <= tol * np.abs(ref0).max()
+
+
+def test_compute_double_matches_golden(box, golden_small_box):
+    """FP64 engine: ff_small_box energies, forces, dipoles, iterations, virial (reference golden)."""
+    s, pos, H, o, r = box
+    g = golden_small_box
+    ff = ff_for(s, H, "double")
+    res = ff.compute(pos, H, None, ff.init_induction())
+    assert int(res.status[0]) & ~0x2 == 0
+    for k in ("elec", "vdw", "total"):
+        ref = float(g[f"double.energy.{k}"])
+        assert abs(float(res.energy[k][0]) - ref) <= 1e-9 * abs(ref), (k, float(res.energy[k][0]), ref)
+    assert int(res.iterations[0]) == int(g["double.iterations"])
+    F = res.forces.cpu().numpy()
+    assert np.abs(F - g["double.forces"]).max() <= 1e-8 * np.abs(g["double.forces"]).max()
+    mu = res.induction.mu.cpu().numpy()
+    assert np.abs(mu - g["double.mu"]).max() <= 1e-9 * np.abs(g["double.mu"]).max()
+    W = res.virial[0].cpu().numpy()
+    assert np.abs(W - g["double.strain"]).max() <= 1e-7 * np.abs(g["double.strain"]).max()
+
+
+def test_compute_mixed_within_tolerance(box, golden_small_box):
+    """Mixed precision against the float64 golden: 1e-6 energy, 1e-5 RMS forces / dipoles."""
+    s, pos, H, o, r = box
+    g = golden_small_box
+    ff = ff_for(s, H, "mixed")
+    res = ff.compute(pos, H, None, ff.init_induction())
+    for k in ("elec", "total"):
+        ref = float(g[f"double.energy.{k}"])
+        assert abs(float(res.energy[k][0]) - ref) <= 1e-6 * abs(ref), (k, float(res.energy[k][0]), ref)
+    assert abs(float(res.energy["vdw"][0]) - float(g["double.energy.vdw"])) <= 1e-5 * abs(float(g["double.energy.vdw"]))
+    assert rms_rel(res.forces.cpu().numpy(), g["double.forces"]) <= 1e-5
+    assert rms_rel(res.induction.mu.cpu().numpy(), g["double.mu"]) <= 1e-5
+    assert abs(int(res.iterations[0]) - int(g["mixed.iterations"])) <= 2
+
+
+@pytest.mark.parametrize("elec", ["q", "qp", "qi", "qpi"])
+def test_elec_levels_match_oracle(small_box_system, elec):
+    s, pos, H = small_box_system
+    st = dict(SMALL_BOX_SETTINGS, elec=elec)
+    r = O.Oracle(s, st).compute(pos, H)
+    ff = ff_for(s, H, "double", elec=elec)
+    res = ff.compute(pos, H)
+    assert abs(float(res.energy["total"][0]) - r["energy"]["total"]) <= 1e-9 * abs(r["energy"]["total"])
+    assert np.abs(res.forces.cpu().numpy() - r["forces"]).max() <= 1e-8 * np.abs(r["forces"]).max()
+    assert int(res.iterations[0]) == r["iterations"]
+
+
+def test_candidate_rows_equal_cell_list(box):
+    """Rows from the caller's candidate list (the reference's idx) equal the engine's cell list."""
+    s, pos, H, o, r = box
+    ff = ff_for(s, H, "double")
+    idx = ff.rows_for(pos, H)
+    a = ff.compute(pos, H, None)
+    b = ff.compute(pos, H, idx)
+    assert abs(float(a.energy["total"][0]) - float(b.energy["total"][0])) <= 1e-11 * abs(float(a.energy["total"][0]))
+    assert np.abs(a.forces.cpu().numpy() - b.forces.cpu().numpy()).max() <= 1e-9 * float(a.forces.abs().max())
+
+
+def test_energy_and_fixed_mu_paths(box):
+    """energy() (CG from the state's mu) and energy_fixed_mu() agree with compute()."""
+    s, pos, H, o, r = box
+    ff = ff_for(s, H, "double")
+    res = ff.compute(pos, H)
+    E, ind, it, ov = ff.energy(pos, H, None, res.induction)
+    assert abs(float(E[0]) - float(res.energy["total"][0])) <= 1e-8 * abs(float(E[0]))
+    Ef, parts = ff.energy_fixed_mu(pos, H, res.induction.mu)
+    assert abs(float(Ef[0]) - float(res.energy["total"][0])) <= 1e-11 * abs(float(Ef[0]))
+    assert np.abs(parts["forces"].cpu().numpy() - res.forces.cpu().numpy()).max() <= 1e-9 * float(res.forces.abs().max())
+    ref = o.energy_fixed_mu(pos, H, res.induction.mu.cpu().numpy())
+    assert abs(float(Ef[0]) - ref["total"]) <= 1e-10 * abs(ref["total"])
+
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_predictor_steps_match_oracle(small_box_system, prec):
+    """Six steps with the mu4 predictor and the fused start (history, count, norm carried)."""
+    s, pos, H = small_box_system
+    st = dict(SMALL_BOX_SETTINGS, dipole_tol=1e-8, norm_refresh=5)
+    o = O.Oracle(s, st)
+    ff = ff_for(s, H, prec, dipole_tol=1e-8, norm_refresh=5)
+    ind_o = o.init_induction()
+    ind_g = ff.init_induction()
+    rng = np.random.default_rng(1)
+    x = pos.copy()
+    for step in range(6):
+        x = x + rng.normal(scale=2e-4, size=x.shape)
+        ro = o.compute(x, H, ind_o)
+        ind_o = ro["induction"]
+        rg = ff.compute(x, H, None, ind_g)
+        ind_g = rg.induction
+        e_ref = ro["energy"]["total"]
+        tol_e = 1e-10 if prec == "double" else 1e-6
+        assert abs(float(rg.energy["total"][0]) - e_ref) <= tol_e * abs(e_ref), (step, float(rg.energy["total"][0]), e_ref)
+        if prec == "double":
+            assert int(rg.iterations[0]) == ro["iterations"], (step, int(rg.iterations[0]), ro["iterations"])
+        else:
+            assert abs(int(rg.iterations[0]) - ro["iterations"]) <= 1
+        assert rms_rel(rg.forces.cpu().numpy(), ro["forces"]) <= (1e-9 if prec == "double" else 1e-5)
+    assert int(ind_g.count[0]) == 6 == ind_o["count"]
+
+
+def test_batch_equals_separate_systems(small_box_system):
+    """A batch of uneven systems (two boxes, different sizes and grids) equals separate evaluations."""
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.systems import small_box
+
+    s0, p0, H0 = small_box_system
+    s1, p1, H1 = small_box(5, nw=40, nm=2)
+    st = MDSettings(precision="double", **dict(SMALL_BOX_SETTINGS, dipole_tol=1e-8))
+    grids = [(32, 32, 32), (36, 30, 32)]
+    fb = PGMForceField([s0, s1], [H0, H1], st, pme_grids=grids)
+    rb = fb.compute(np.concatenate([p0, p1]), np.stack([H0, H1]))
+    for k, (s, p, H, g) in enumerate([(s0, p0, H0, grids[0]), (s1, p1, H1, grids[1])]):
+        f = PGMForceField(s, H, st, pme_grids=[g])
+        r = f.compute(p, H)
+        assert abs(float(rb.energy["total"][k]) - float(r.energy["total"][0])) <= 1e-10 * abs(float(r.energy["total"][0]))
+        assert int(rb.iterations[k]) == int(r.iterations[0])
+        sl = slice(int(fb.offsets[k]), int(fb.offsets[k + 1]))
+        assert np.abs(rb.forces[sl].cpu().numpy() - r.forces.cpu().numpy()).max() <= 1e-9 * float(r.forces.abs().max())
+
+
+def test_water512_fp64_matches_oracle():
+    """512 pGM3P-25 waters (24.83 A box, 9 A cutoff, PME 48^3 order 6, beta 0.4/A, tol 1e-8), FP64."""
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(8, 2.483, seed=0)
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(48, 48, 48), pme_order=6, dipole_tol=1e-8, max_iter=100)
+    r = O.Oracle(s, st).compute(pos, H)
+    ff = PGMForceField(s, H, MDSettings(precision="double", **st))
+    g = ff.compute(pos, H)
+    assert abs(float(g.energy["total"][0]) - r["energy"]["total"]) <= 1e-9 * abs(r["energy"]["total"])
+    assert rms_rel(g.forces.cpu().numpy(), r["forces"]) <= 1e-9
+    assert int(g.iterations[0]) == r["iterations"]
+    assert np.abs(g.virial[0].cpu().numpy() - r["virial"]).max() <= 1e-7 * np.abs(r["virial"]).max()
+    ffm = PGMForceField(s, H, MDSettings(precision="mixed", **st))
+    m = ffm.compute(pos, H)
+    assert abs(float(m.energy["total"][0]) - r["energy"]["total"]) <= 1e-6 * abs(r["energy"]["total"])
+    assert rms_rel(m.forces.cpu().numpy(), r["forces"]) <= 1e-5
+    assert rms_rel(m.induction.mu.cpu().numpy(), r["mu"]) <= 1e-5
+
+
+def test_row_overflow_is_reported_and_recovers(box):
+    """A capacity below the largest row sets the overflow bit; growing it repeats the step correctly."""
+    s, pos, H, o, r = box
+    ff = ff_for(s, H, "double")
+    ff.set_capacity(32)
+    res = ff.compute(pos, H)
+    assert bool(res.overflow[0])
+    ff.grow_rows(ff.capacity * 8)
+    res = ff.compute(pos, H)
+    assert not bool(res.overflow[0])
+    assert abs(float(res.energy["total"][0]) - r["energy"]["total"]) <= 1e-9 * abs(r["energy"]["total"])
+
+
+def test_cg_max_iter_status(box):
+    s, pos, H, o, r = box
+    ff = ff_for(s, H, "double", max_iter=3)
+    res = ff.compute(pos, H)
+    assert int(res.iterations[0]) == 3 and int(res.status[0]) & 0x2

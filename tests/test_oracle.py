@@ -103,3 +103,16 @@ def test_oracle_elec_levels(small_box_system, elec):
     else:
         assert r["iterations"] > 0
     assert np.isfinite(r["energy"]["total"])
+
+
+def test_oracle_forces_without_permanent_dipoles_are_pure_charge(small_box_system):
+    """At level "q" the covalent frames carry no dipole, so the forces are central differences of E."""
+    s, pos, H = small_box_system
+    o = O.Oracle(s, dict(SMALL_BOX_SETTINGS, elec="q"))
+    r = o.compute(pos, H)
+    h = 1e-6
+    for a, k in [(0, 0), (7, 2)]:
+        d = np.zeros_like(pos)
+        d[a, k] = h
+        fd = -(o.energy_fixed_mu(pos + d, H, r["mu"])["total"] - o.energy_fixed_mu(pos - d, H, r["mu"])["total"]) / (2 * h)
+        assert abs(fd - r["forces"][a, k]) < 1e-5 * max(1.0, abs(fd))
