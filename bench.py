@@ -1,0 +1,342 @@
+"""Benchmark: pGM rigid-water MD on the B200 engine, ns/day and CG iterations per step.
+
+Workload (one GPU): 4096 pGM3P-25 waters (12,288 atoms) on a seeded jittered 16^3 lattice in a
+4.966 nm cubic box, cutoff 0.9 nm, Ewald 4.0 / nm, PME 96^3 order 6, mixed precision (FP32 pair /
+PME / CG vectors, FP64 reductions), Langevin NVT 298 K with gamma 2 / ps, dt 1 fs, CG to max|alpha
+r| / mean|alpha b| <= 1e-6 from the mu4 predictor (the plain solver).  A step is one captured CUDA
+graph: rigid-body kick/drift/Langevin, the force call (rows, PME, CG as a device-side while loop,
+energy / forces / virial), closing kick.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one process per GPU) every rank runs its own independent replica (the path
+has no exchange step: replicas only); value = total ns/day over the ranks, time = max over ranks.
+--impl reference times the CPU restatement of the reference's algorithm (the FP64 oracle, all host
+threads) on the same workload, on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SIDE, EDGE_NM, GRID = 16, 4.966, 96
+DT_FS, GAMMA, TEMP, TOL = 1.0, 2.0, 298.0, 1e-6
+METRIC = "ns/day & CG iters/step on 1 B200: NN-guess vs plain CG at residual≤1e-6"
+CONFIG = {
+    "workload": "4096 rigid pGM3P-25 waters, 4.966 nm box, PME 96^3 o6, rc 0.9 nm, beta 4.0/nm, Langevin 298 K "
+    "gamma 2/ps, dt 1 fs, mixed precision, CG tol 1e-6 (plain CG from the mu4 predictor)",
+    "atoms": 12288,
+    "pme_grid": [GRID, GRID, GRID],
+    "cutoff_nm": 0.9,
+    "dt_fs": DT_FS,
+    "cg_tol": TOL,
+    "solver": "plain CG (mu4 predictor, fused start)",
+    "l2": "working set larger than L2: pair rows 8 x 4 B x 12288 x capacity = 164 MB (126 MB L2)",
+    "seeds": {"positions": 0, "velocities_thermostat": 1},
+}
+
+
+def settings(precision="mixed"):
+    from pgm_jax_b200.forcefield import MDSettings
+
+    return MDSettings(precision=precision, cutoff=0.9, ewald_beta=4.0, pme_grid=(GRID, GRID, GRID), pme_order=6,
+                      dipole_tol=TOL, max_iter=100, predictor="mu4")
+
+
+def ns_per_day(ms_per_step: float) -> float:
+    return 86.4 * DT_FS / ms_per_step
+
+
+def bytes_per_step(n_atoms: int, pairs: float, n_it: float, K: int) -> float:
+    """Algorithmic bytes of one MD step: row build 32 B/pair, (n_it + 1) CG sweeps of 24 B/pair, the
+    force pass 40 B/pair, (n_it + 2) PME passes of 24 K^3 + 288 N bytes, 400 B/atom of state."""
+    return pairs * (32 + 24 * (n_it + 1) + 40) + (n_it + 2) * (24 * K**3 + 288 * n_atoms) + 400 * n_atoms
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index: int) -> None:
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference(steps: int, warmup: int, budget_s: float = 120.0):
+    """The FP64 CPU oracle (restatement of the reference's algorithm) on the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402  (the checker; this is the reference arm / CPU baseline)
+
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(N_SIDE, EDGE_NM, seed=0)
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(GRID, GRID, GRID), pme_order=6, dipole_tol=TOL, max_iter=100)
+    cores = os.cpu_count() or 1
+    o = O.Oracle(s, st, nthreads=cores)
+    ind = o.init_induction()
+    rng = np.random.default_rng(1)
+    x = pos.copy()
+    times, iters = [], []
+    t_start = time.perf_counter()
+    n = 0
+    while n < max(1, steps):
+        x = x + rng.normal(scale=2e-4, size=x.shape)  # a moving geometry, so the predictor works as in MD
+        t0 = time.perf_counter()
+        r = o.compute(x, H, ind)
+        dt = time.perf_counter() - t0
+        ind = r["induction"]
+        n += 1
+        if n > min(warmup, 1):
+            times.append(dt)
+            iters.append(r["iterations"])
+        if time.perf_counter() - t_start > budget_s and times:
+            break
+    ms = 1e3 * float(np.mean(times))
+    return {
+        "value": ns_per_day(ms), "ms_per_step": ms, "cores": cores, "steps_timed": len(times),
+        "cg_iters_per_step": float(np.mean(iters)),
+        "sample": f"{len(times)} force steps of the 4096-water workload (FP64 oracle, {cores} threads, after "
+        f"{min(warmup, 1)} untimed); the rigid-body integrator's cost (<1%) is not included",
+    }
+
+
+def run_reference(args) -> None:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    r = cpu_reference(args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "ns/day", "n_gpus": args.gpus,
+        "steps": r["steps_timed"], "warmup": min(args.warmup, 1), "ms_per_step": r["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": CONFIG, "cg_iters_per_step": r["cg_iters_per_step"],
+        "cpu_baseline": {"value": r["value"], "unit": "ns/day", "cores": r["cores"], "kind": "port", "sample": r["sample"]},
+        "e2e": {"value": r["value"], "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (JAX) is not installable here (no jax/jax_md wheels, no network); its algorithm is "
+        "timed through the project's FP64 C restatement (oracle/)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from pgm_jax_b200 import _lib
+    from pgm_jax_b200.forcefield import PGMForceField
+    from pgm_jax_b200.md import RigidMD
+    from pgm_jax_b200.systems import water_box
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    s, pos, H = water_box(N_SIDE, EDGE_NM, seed=0)
+    ff = PGMForceField(s, H, settings(), device=local)
+    md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
+    lib = ff._lib
+    # warm-up: direct steps (rows sized), then capture and replay
+    for _ in range(max(1, args.warmup)):
+        md.step()
+    md.stream.synchronize()
+    md.capture()
+    md.run(max(3, args.warmup))
+    md.stream.synchronize()
+    it0 = int(md.result.iterations[0])
+    # timed region: K graph replays between CUDA events on the MD stream; clocks sampled meanwhile
+    iters = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clk = Clocks(local)
+    ev0.record(md.stream)
+    it_sum = torch.zeros((), dtype=torch.int64, device=dev)
+    for _ in range(args.steps):
+        md.run(1)
+        with torch.cuda.stream(md.stream):
+            it_sum += md.result.iterations[0].to(torch.int64)
+    ev1.record(md.stream)
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    n_it = float(it_sum.item()) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    status = int(md.result.status[0])
+    launches = args.steps * (md.launches_outside_loop + n_it * md.launches_per_iteration)
+    # the dominant kernel: the CG matvec, timed alone with CUDA events on the MD stream
+    pairs = int(lib.pgm_row_pairs(ff._h))
+    kt = {}
+    for which, name in ((0, "cg_matvec"), (1, "spread"), (2, "fft_chain"), (3, "forces"), (4, "rows")):
+        v = C_double()
+        _lib.check(lib.pgm_profile_kernel(ff._h, C_void_p(md.stream.cuda_stream), which, 20, byref(v)))
+        kt[name] = v.value
+    peak, peak_kind = peaks()
+    mv_bytes = 24.0 * pairs + 32.0 * ff.n  # rows (k, x, y, z, G1, G2) + the dipole vector in and out
+    mv_gbs = mv_bytes / (kt["cg_matvec"] * 1e-3) / 1e9
+    step_bytes = bytes_per_step(ff.n, pairs, n_it, GRID)
+    # end to end: the force call through the C ABI with host buffers (positions in, forces out and
+    # the induction state in and out every step), the integrator on the GPU
+    e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
+    value = ws * ns_per_day(ms_max)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "config": CONFIG, "cg_iters_per_step": n_it, "cg_iters_first_step": it0,
+            "status": status, "gpu_launches": int(round(launches)),
+            "clocks": clocks,
+            "roofline": {
+                "bound": "hbm", "kernel": "k_rowmat (CG matvec: row field + PME gather)",
+                "achieved": mv_gbs, "peak": peak, "unit": "GB/s", "frac": mv_gbs / peak, "peak_kind": peak_kind,
+                "traffic": None, "bytes_per_launch": mv_bytes, "ms_per_launch": kt["cg_matvec"],
+                "step_bytes": step_bytes, "step_gbs": step_bytes / (ms_max * 1e-3) / 1e9,
+                "step_frac": step_bytes / (ms_max * 1e-3) / 1e9 / peak,
+            },
+            "kernel_ms": kt, "pairs": pairs, "row_capacity": ff.capacity,
+            "e2e": e2e,
+            "published_reference": "44 ns/day, 4096 waters, mixed, tol 1e-5, 1x RTX PRO 6000 Blackwell (README.md:448)",
+        }
+        if args.cpu_baseline:
+            r = cpu_reference(3, 1, budget_s=40.0)
+            line["cpu_baseline"] = {"value": r["value"], "unit": "ns/day", "cores": r["cores"], "kind": "port",
+                                    "sample": r["sample"]}
+        print(json.dumps(line), flush=True)
+    del md
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
+    """MD with the force call through pgm_compute_host: host positions in, host forces out, per step."""
+    import ctypes as C
+
+    n = ff.n
+    S = ff.nsys
+    pin = lambda *shape, dt=torch.float64: torch.empty(shape, dtype=dt, pin_memory=True)  # noqa: E731
+    h_pos, h_F, h_box = pin(n, 3), pin(n, 3), pin(S, 3, 3)
+    h_mu, h_hist = pin(n, 3), pin(4, n, 3)
+    h_cnt, h_norm = pin(S, dt=torch.int32), pin(S)
+    h_E, h_V, h_it, h_res, h_st = pin(S, 3), pin(S, 3, 3), pin(S, dt=torch.int32), pin(S), pin(S, dt=torch.int32)
+    md.stream.synchronize()
+    h_box.copy_(md.box.cpu())
+    h_mu.copy_(md.ind.mu.cpu()); h_hist.copy_(md.ind.hist.cpu()); h_cnt.copy_(md.ind.count.cpu()); h_norm.copy_(md.ind.norm.cpu())
+    ind = _lib.PgmInduction(h_mu.data_ptr(), h_hist.data_ptr(), h_cnt.data_ptr(), h_norm.data_ptr())
+    out = _lib.PgmOutputs(h_E.data_ptr(), h_F.data_ptr(), h_V.data_ptr(), h_it.data_ptr(), h_res.data_ptr(), h_st.data_ptr())
+    st = C.c_void_p(md.stream.cuda_stream)
+    steps = max(3, min(steps, 200))
+
+    def one():
+        _lib.check(lib.pgm_rigid_begin_step(md._h, st, md.dt, md.gamma, C.c_void_p(md.kT.data_ptr()), md.seed,
+                                            C.c_void_p(md.forces.data_ptr()), C.c_void_p(md.com.data_ptr()),
+                                            C.c_void_p(md.quat.data_ptr()), C.c_void_p(md.mom.data_ptr()),
+                                            C.c_void_p(md.angmom.data_ptr()), C.c_void_p(md.pos.data_ptr()),
+                                            C.c_void_p(md.box.data_ptr())))
+        h_pos.copy_(md.pos, non_blocking=True)
+        md.stream.synchronize()
+        _lib.check(lib.pgm_compute_host(ff._h, C.c_void_p(h_pos.data_ptr()), C.c_void_p(h_box.data_ptr()), C.byref(ind),
+                                        C.byref(out)))
+        md.forces.copy_(h_F, non_blocking=True)
+        _lib.check(lib.pgm_rigid_end_step(md._h, st, md.dt, C.c_void_p(md.forces.data_ptr()), C.c_void_p(md.quat.data_ptr()),
+                                          C.c_void_p(md.mom.data_ptr()), C.c_void_p(md.angmom.data_ptr())))
+
+    with torch.cuda.stream(md.stream):
+        for _ in range(2):
+            one()
+        md.stream.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            one()
+        md.stream.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / steps
+    b = 8 * n * 3
+    h2d = b + 9 * 8 * S + 5 * b + 4 * S + 8 * S + b  # positions, box, mu + hist, count, norm; forces back to the integrator
+    d2h = b + b + 5 * b + 4 * S + 8 * S + 8 * (3 + 9 + 1) * S + 8 * S  # positions out; forces, state, energy, virial...
+    return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "steps": steps, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "path": "pgm_compute_host (C ABI, pinned host buffers: positions in; forces, energies, virial, induction "
+            "state out) with the rigid-body kernels on the GPU; wall clock around the loop"}
+
+
+from ctypes import byref, c_double as C_double, c_void_p as C_void_p  # noqa: E402
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

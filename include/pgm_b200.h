@@ -10,6 +10,11 @@
  * Units: nm, e, e nm, nm^3, kJ/mol, kJ/mol/nm (pgm_jax/md/forcefield.py:100).  Boxes are
  * lower-triangular, lattice vectors as rows, in reduced form (pgm_jax/md/box.py:32).
  *
+ * Graphs: pgm_compute and pgm_energy may be called while the stream is being captured (stream
+ * capture, any mode); the CG loop is then recorded as a device-side while loop (conditional graph
+ * node) that runs until every system has converged or reached max_iter, so a replayed step never
+ * returns to the host.  Outside capture the loop is driven from the host.
+ *
  * Errors: every entry point returns a PgmStatus; nothing is thrown across the boundary.
  * Per-system conditions of a step (row overflow, CG not converged, non-finite energy) come back in
  * the `status` output word of each system, as the reference reports them in Result.overflow and
@@ -143,8 +148,55 @@ int pgm_num_systems(const PgmHandle *h);
 /* Text of the last error of this thread. */
 const char *pgm_last_error(void);
 
-/* Kernels launched by the last pgm_compute / pgm_energy / pgm_field call (launch accounting). */
+/* Kernels launched by the last pgm_compute / pgm_energy / pgm_field call, counting one CG iteration
+ * when the call was captured into a CUDA graph (the loop then runs as a conditional while node),
+ * and the kernels of one CG iteration (launch accounting). */
 long long pgm_last_launch_count(const PgmHandle *h);
+long long pgm_launches_per_iteration(const PgmHandle *h);
+
+/* Average duration [ms] of one launch of a kernel of the last pgm_compute, re-run `reps` times on
+ * `stream` between CUDA events on the state that step left: 0 the CG matvec (row field + PME
+ * gather), 1 the PME spread, 2 the five FFT/convolution passes, 3 the energy/force pass, 4 the row
+ * build.  The last pgm_compute's position array must still be valid. */
+PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, double *ms_per_launch);
+
+/* In-cutoff pairs (both rows of every pair) of the last step's row build. */
+long long pgm_row_pairs(PgmHandle *h);
+
+/* ------------------------------------------------------------------ rigid-molecule MD driver
+ * The caller of the force field in the MD benchmarks: the rigid-body step of pgm_jax/md/
+ * integrate.py:743-761 (B A O A B) with md/rigid.py bodies and the Langevin O-step of
+ * md/thermostats.py:195-240.  Bodies: centre of mass X (M, 3), quaternion q (M, 4, body -> space,
+ * w first), momentum P (M, 3) and body-frame angular momentum L (M, 3), device arrays; atoms at
+ * X + R(q) b_i with `body` b (N, 3) in each molecule's principal frame and `inertia` (M, 3) its
+ * principal moments.  Units amu, nm, ps, kJ/mol. */
+typedef struct PgmRigid PgmRigid;
+
+PgmStatus pgm_rigid_create(int n_mol, const int32_t *mol_start, const int32_t *mol_system, const double *masses,
+                           const double *body, const double *inertia, int device, PgmRigid **out);
+PgmStatus pgm_rigid_destroy(PgmRigid *r);
+
+/* Kick (with the forces of the previous step; NULL: none), drift, Langevin (gamma [1/ps] > 0, kT
+ * [kJ/mol] per system, device; the noise is drawn from (seed, the handle's step counter)), drift;
+ * writes the atom positions pos (N, 3) for the next force call.  box (n_systems, 3, 3) keeps the
+ * centres in the box. */
+PgmStatus pgm_rigid_begin_step(PgmRigid *r, void *stream, double dt, double gamma, const double *kT, uint64_t seed,
+                               const double *forces, double *com, double *quat, double *mom, double *angmom, double *pos,
+                               const double *box);
+/* Set the step counter of the Langevin noise (it advances by one at every pgm_rigid_end_step). */
+PgmStatus pgm_rigid_set_step(PgmRigid *r, uint64_t step);
+/* Closing half kick with the new forces. */
+PgmStatus pgm_rigid_end_step(PgmRigid *r, void *stream, double dt, const double *forces, const double *quat, double *mom,
+                             double *angmom);
+/* Kinetic energy per system (device, n_systems). */
+PgmStatus pgm_rigid_kinetic(PgmRigid *r, void *stream, const double *mom, const double *angmom, double *ke);
+const char *pgm_rigid_last_error(void);
+
+/* Stream capture of engine calls into a replayable CUDA graph (exec is a cudaGraphExec_t). */
+PgmStatus pgm_graph_begin(void *stream);
+PgmStatus pgm_graph_end(void *stream, void **exec_out);
+PgmStatus pgm_graph_launch(void *exec, void *stream);
+PgmStatus pgm_graph_destroy(void *exec);
 
 #ifdef __cplusplus
 }

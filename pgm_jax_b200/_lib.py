@@ -19,7 +19,9 @@ _pu = C.POINTER(C.c_uint32)
 EXPORTS = (
     "pgm_create", "pgm_destroy", "pgm_compute", "pgm_compute_host", "pgm_energy", "pgm_energy_fixed_mu", "pgm_field",
     "pgm_set_row_capacity", "pgm_row_capacity", "pgm_max_row_count", "pgm_num_atoms", "pgm_num_systems",
-    "pgm_last_error", "pgm_last_launch_count",
+    "pgm_last_error", "pgm_last_launch_count", "pgm_launches_per_iteration", "pgm_profile_kernel", "pgm_row_pairs", "pgm_rigid_create", "pgm_rigid_destroy",
+    "pgm_rigid_begin_step", "pgm_rigid_set_step", "pgm_rigid_end_step", "pgm_rigid_kinetic", "pgm_rigid_last_error", "pgm_graph_begin",
+    "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy",
 )
 
 STATUS_ROW_OVERFLOW = 0x1
@@ -85,6 +87,26 @@ def load(path: str | None = None):
     lib.pgm_last_launch_count.argtypes = [H]
     lib.pgm_last_launch_count.restype = C.c_longlong
     lib.pgm_last_error.restype = C.c_char_p
+    lib.pgm_profile_kernel.argtypes = [H, vp, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.pgm_profile_kernel.restype = C.c_int
+    lib.pgm_row_pairs.argtypes = [H]
+    lib.pgm_row_pairs.restype = C.c_longlong
+    lib.pgm_launches_per_iteration.argtypes = [H]
+    lib.pgm_launches_per_iteration.restype = C.c_longlong
+    lib.pgm_rigid_create.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int, C.POINTER(H)]
+    lib.pgm_rigid_destroy.argtypes = [H]
+    lib.pgm_rigid_begin_step.argtypes = [H, vp, C.c_double, C.c_double, vp, C.c_uint64, vp, vp, vp, vp, vp, vp, vp]
+    lib.pgm_rigid_set_step.argtypes = [H, C.c_uint64]
+    lib.pgm_rigid_end_step.argtypes = [H, vp, C.c_double, vp, vp, vp, vp]
+    lib.pgm_rigid_kinetic.argtypes = [H, vp, vp, vp, vp]
+    lib.pgm_rigid_last_error.restype = C.c_char_p
+    lib.pgm_graph_begin.argtypes = [vp]
+    lib.pgm_graph_end.argtypes = [vp, C.POINTER(vp)]
+    lib.pgm_graph_launch.argtypes = [vp, vp]
+    lib.pgm_graph_destroy.argtypes = [vp]
+    for n in ("pgm_rigid_create", "pgm_rigid_destroy", "pgm_rigid_begin_step", "pgm_rigid_set_step", "pgm_rigid_end_step", "pgm_rigid_kinetic",
+              "pgm_graph_begin", "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy"):
+        getattr(lib, n).restype = C.c_int
     for n in ("pgm_create", "pgm_destroy", "pgm_compute", "pgm_compute_host", "pgm_energy", "pgm_energy_fixed_mu",
               "pgm_field", "pgm_set_row_capacity"):
         getattr(lib, n).restype = C.c_int

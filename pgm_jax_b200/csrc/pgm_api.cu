@@ -92,7 +92,9 @@ std::vector<int> radices(int K) {
 }
 
 struct EngineBase {
-  virtual ~EngineBase() {}
+  virtual ~EngineBase() {
+    if (host_scratch) cudaFree(host_scratch);
+  }
   virtual void compute(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
                        PgmInduction *ind, PgmOutputs *out) = 0;
   virtual void energy(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
@@ -103,7 +105,12 @@ struct EngineBase {
   virtual void set_capacity(int mc) = 0;
   virtual int capacity() const = 0;
   virtual int max_count() = 0;
+  virtual long long launches_per_iteration() const = 0;
+  virtual double profile(cudaStream_t st, int which, int reps) = 0;
+  virtual long long row_pairs() = 0;
   int nt = 0, nsys = 0;
+  double *host_scratch = nullptr;  // device block of pgm_compute_host (allocated on first use)
+  size_t host_scratch_bytes = 0;
   long long launches = 0;
 };
 
@@ -137,9 +144,13 @@ struct Engine : EngineBase {
   DBuf<pgm::c2<T>> C, tw;
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
   int *h_any = nullptr;
+  const double *last_pos = nullptr;
+  cudaStream_t side = nullptr;
+  long long per_iter = 0;
 
   ~Engine() {
     if (h_any) cudaFreeHost(h_any);
+    if (side) cudaStreamDestroy(side);
   }
 
   pgm::Dev<T> dev(const double *pos, const int32_t *idx, int idx_width, double *forces, unsigned *status) {
@@ -373,6 +384,52 @@ struct Engine : EngineBase {
     }
   }
   int capacity() const override { return mc; }
+  long long launches_per_iteration() const override { return per_iter; }
+
+  // Average duration [ms] of one launch of a kernel of the last step, re-run `reps` times on the
+  // state that step left (rows, vectors, grids): 0 the CG matvec (rows + PME gather), 1 the spread,
+  // 2 the FFT/convolution chain (five passes), 3 the energy/force pass, 4 the row build.
+  double profile(cudaStream_t st, int which, int reps) override {
+    pgm::Dev<T> a = dev(nullptr, nullptr, 0, forces_tmp.p, d_status.p);
+    a.pos = last_pos;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto one = [&]() {
+      if (which == 0) pgm::k_rowmat<T, P, false, 1, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
+      else if (which == 1) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
+      else if (which == 2) {
+        pgm::k_fft_x_fwd<T, 0><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p);
+        pgm::k_fft_y<T, 0><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, -1);
+        pgm::k_fft_z_conv<T, 0, false><<<tiles_z, 256, smem_z, st>>>(a, tile0_z.p);
+        pgm::k_fft_y<T, 0><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, +1);
+        pgm::k_fft_x_inv<T, 0><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p);
+      } else if (which == 3) pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, nullptr);
+      else pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
+    };
+    one();  // warm-up
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; ++r) one();
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (which == 1) CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // the spread grid must start at zero
+    CK(cudaEventDestroy(e0));
+    CK(cudaEventDestroy(e1));
+    CK(cudaGetLastError());
+    return ms / reps;
+  }
+
+  // In-cutoff pairs of the last row build (sum over rows).
+  long long row_pairs() override {
+    std::vector<int> h(nt);
+    CK(cudaMemcpy(h.data(), rn.p, sizeof(int) * nt, cudaMemcpyDeviceToHost));
+    long long t = 0;
+    for (int v : h) t += std::min(v, mc);
+    return t;
+  }
   int max_count() override {
     int v = 0;
     CK(cudaMemcpy(&v, dmax.p, sizeof(int), cudaMemcpyDeviceToHost));
@@ -412,6 +469,14 @@ struct Engine : EngineBase {
     pgm::k_fft_x_inv<T, ACT><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p); check_launch();
   }
 
+  // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check.
+  void iteration(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
+    pme<false, true, 1, false>(st, a, Pv.p);
+    pgm::k_rowmat<T, P, false, 1, 1><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p); check_launch();
+    pgm::k_cg_update<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+    pgm::k_cg_check<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, cond, use_cond); check_launch();
+  }
+
   bool any_active(cudaStream_t st) {
     CK(cudaMemcpyAsync(h_any, dany.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -443,12 +508,40 @@ struct Engine : EngineBase {
     pgm::k_start3<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
     pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
     pgm::k_cg_begin<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p); check_launch();
-    for (int it = 0; it < set.max_iter; ++it) {
-      if (!any_active(st)) break;
-      pme<false, true, 1, false>(st, a, Pv.p);
-      pgm::k_rowmat<T, P, false, 1, 1><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p); check_launch();
-      pgm::k_cg_update<T><<<ntblk, 256, 0, st>>>(a); check_launch();
-      pgm::k_cg_check<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p); check_launch();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs == cudaStreamCaptureStatusActive) {
+      // captured: a conditional while node whose body is one CG iteration; the body's last kernel
+      // sets the condition to "some system still iterating" (bounded by max_iter on the device)
+      cudaGraph_t g;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t nd = 0;
+      unsigned long long id;
+      CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+      cudaGraphConditionalHandle cond;
+      CK(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams np = {};
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = cond;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      cudaGraphNode_t node;
+      CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+      cudaGraph_t body = np.conditional.phGraph_out[0];
+      CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+      if (!side) CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      CK(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      long long l0 = launches;
+      iteration(side, a, cond, 1);
+      per_iter = launches - l0;
+      CK(cudaStreamEndCapture(side, &body));
+    } else {
+      for (int it = 0; it < set.max_iter; ++it) {
+        if (!any_active(st)) break;
+        long long l0 = launches;
+        iteration(st, a, 0, 0);
+        per_iter = launches - l0;
+      }
     }
     pgm::k_cg_finish<T><<<grid1(nt), 256, 0, st>>>(a, mu_out, mode == 0 ? ind->hist : nullptr, mode == 0); check_launch();
     pgm::k_cg_state_out<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, ind->count, ind->norm, iters, resid, a.status, mode == 0,
@@ -475,6 +568,7 @@ struct Engine : EngineBase {
     double *forces = out->forces ? out->forces : forces_tmp.p;
     CK(cudaMemsetAsync(status, 0, sizeof(unsigned) * nsys, st));
     pgm::Dev<T> a = dev(pos, idx, idx_width, forces, status);
+    last_pos = pos;
     prepare(st, a, box);
     double *mu = ind->mu;
     if (a.induce) {
@@ -639,10 +733,19 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
   double *d = nullptr;
   try {
     CK(cudaSetDevice(h->device));
-    // one device block: pos, box, mu, hist, norm, energy, forces, virial, residual | count, iterations, status
+    // one device block, kept by the handle: pos, box, mu, hist, norm, energy, forces, virial,
+    // residual | count, iterations, status
     size_t nd = n3 + 9 * ns + n3 + 4 * n3 + ns + 3 * ns + n3 + 9 * ns + ns;
     size_t ni = 3 * ns;
-    CK(cudaMalloc(&d, sizeof(double) * nd + sizeof(int32_t) * ni));
+    size_t bytes = sizeof(double) * nd + sizeof(int32_t) * ni;
+    if (e->host_scratch_bytes < bytes) {
+      if (e->host_scratch) cudaFree(e->host_scratch);
+      e->host_scratch = nullptr;
+      e->host_scratch_bytes = 0;
+      CK(cudaMalloc(&e->host_scratch, bytes));
+      e->host_scratch_bytes = bytes;
+    }
+    d = e->host_scratch;
     double *dpos = d, *dbox = dpos + n3, *dmu = dbox + 9 * ns, *dhist = dmu + n3, *dnorm = dhist + 4 * n3, *den = dnorm + ns,
            *dF = den + 3 * ns, *dvir = dF + n3, *dres = dvir + 9 * ns;
     int32_t *dcount = reinterpret_cast<int32_t *>(dres + ns), *dit = dcount + ns;
@@ -668,10 +771,8 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
     if (out->residual) CK(cudaMemcpyAsync(out->residual, dres, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
     if (out->status) CK(cudaMemcpyAsync(out->status, dst, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    CK(cudaFree(d));
     return PGM_OK;
   } catch (CudaError &err) {
-    if (d) cudaFree(d);
     return fail(PGM_ERR_CUDA, err.msg);
   }
 }
@@ -740,5 +841,28 @@ int pgm_max_row_count(PgmHandle *h) {
 int pgm_num_atoms(const PgmHandle *h) { return h ? h->eng->nt : -1; }
 int pgm_num_systems(const PgmHandle *h) { return h ? h->eng->nsys : -1; }
 long long pgm_last_launch_count(const PgmHandle *h) { return h ? h->eng->launches : -1; }
+long long pgm_launches_per_iteration(const PgmHandle *h) { return h ? h->eng->launches_per_iteration() : -1; }
+
+PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, double *ms_per_launch) {
+  if (!h || !ms_per_launch || reps <= 0 || which < 0 || which > 4) return fail(PGM_ERR_INVALID, "bad argument");
+  if (!static_cast<bool>(h->eng)) return fail(PGM_ERR_INVALID, "no engine");
+  try {
+    CK(cudaSetDevice(h->device));
+    *ms_per_launch = h->eng->profile((cudaStream_t)stream, which, reps);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+long long pgm_row_pairs(PgmHandle *h) {
+  if (!h) return -1;
+  try {
+    return h->eng->row_pairs();
+  } catch (CudaError &e) {
+    g_err = e.msg;
+    return -1;
+  }
+}
 
 }  // extern "C"

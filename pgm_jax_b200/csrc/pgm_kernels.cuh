@@ -958,7 +958,8 @@ __global__ void k_cg_update(Dev<T> a) {
 // Per-system scalars after an update: beta (Polak-Ribiere), r.z, err, iteration count and the
 // loop condition err > tol and it < max_iter (forcefield.py:1798-1816).  *any = some system
 // still iterating.
-__global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *any) {
+__global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *any, cudaGraphConditionalHandle cond,
+                           int use_cond) {
   __shared__ int act;
   if (threadIdx.x == 0) act = 0;
   __syncthreads();
@@ -975,7 +976,10 @@ __global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *a
     if (G.active) atomicOr(&act, 1);
   }
   __syncthreads();
-  if (threadIdx.x == 0) *any = act;
+  if (threadIdx.x == 0) {
+    *any = act;
+    if (use_cond) cudaGraphSetConditional(cond, act ? 1u : 0u);  // the captured while loop of the solve
+  }
 }
 
 // After the loop: the peek step mu = x + peek alpha r (forcefield.py:1819-1820), the dipoles

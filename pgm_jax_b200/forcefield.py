@@ -295,6 +295,21 @@ class PGMForceField:
         energy = {"elec": E[:, 0], "vdw": E[:, 1], "total": E[:, 2]}
         return Result(energy, F, ind, I, R, (Sst & _lib.STATUS_ROW_OVERFLOW) != 0, V, Sst)
 
+    def compute_into(self, pos: torch.Tensor, boxes: torch.Tensor, ind: InductionState, forces: torch.Tensor) -> Result:
+        """compute() into persistent buffers, with no allocation (for CUDA-graph capture).
+
+        pos (N, 3) and boxes (S, 3, 3) float64 CUDA tensors; forces (N, 3) receives the forces.  The
+        energy, virial, iterations, residual and status of the Result are this instance's buffers,
+        overwritten by the next call.
+        """
+        di = _lib.PgmInduction(ind.mu.data_ptr(), ind.hist.data_ptr(), ind.count.data_ptr(), ind.norm.data_ptr())
+        out = _lib.PgmOutputs(self._energy.data_ptr(), forces.data_ptr(), self._virial.data_ptr(), self._iters.data_ptr(),
+                              self._resid.data_ptr(), self._status.data_ptr())
+        _lib.check(self._lib.pgm_compute(self._h, self._stream(), _ptr(pos), _ptr(boxes), None, 0, C.byref(di), C.byref(out)))
+        E = self._energy
+        return Result({"elec": E[:, 0], "vdw": E[:, 1], "total": E[:, 2]}, forces, ind, self._iters, self._resid,
+                      (self._status & _lib.STATUS_ROW_OVERFLOW) != 0, self._virial, self._status)
+
     def energy(self, pos, H, idx=None, ind: InductionState | None = None):
         """Energy only, dipoles solved from ind.mu, no history push (forcefield.py:2562).
 
