@@ -114,14 +114,35 @@ struct EngineBase {
   long long launches = 0;
 };
 
+// Mesh lengths with a compiled FFT plan (others run the runtime-length kernels).
+template <typename F>
+void with_fft_len(int L, F &&f) {
+  switch (L) {
+    case 32: f(std::integral_constant<int, 32>{}); break;
+    case 48: f(std::integral_constant<int, 48>{}); break;
+    case 64: f(std::integral_constant<int, 64>{}); break;
+    case 72: f(std::integral_constant<int, 72>{}); break;
+    case 96: f(std::integral_constant<int, 96>{}); break;
+    case 128: f(std::integral_constant<int, 128>{}); break;
+    case 192: f(std::integral_constant<int, 192>{}); break;
+    default: f(std::integral_constant<int, 0>{}); break;
+  }
+}
+
+// The systems of one FFT pass launch: same mesh length along the pass's axis.
+struct FftGroup {
+  int K = 0, ng = 0, ntiles = 0;
+  size_t smem = 0;
+  DBuf<int> sys, tile0;
+};
+
 template <typename T, int P>
 struct Engine : EngineBase {
   PgmSettings set;
   std::vector<pgm::SysInfo> hsys;
   int nmol_total = 0, ncell = 0, ncov = 0, mc = 0, mc_auto = 0;
   long long rgrid = 0, cgrid = 0;
-  int tiles_x = 0, tiles_y = 0, tiles_z = 0;
-  size_t smem_x = 0, smem_y = 0, smem_z = 0;
+  std::vector<std::unique_ptr<FftGroup>> gx, gy, gz;
   int nwblk = 0, ntblk = 0;
   std::vector<int> natoms;
 
@@ -130,7 +151,7 @@ struct Engine : EngineBase {
   DBuf<pgm::CGSys> d_cg;
   DBuf<pgm::EnergyAcc> d_eacc;
   DBuf<unsigned> d_status;
-  DBuf<int> wb_sys, wb_atom0, tb_sys, tb_atom0, tile0_x, tile0_y, tile0_z;
+  DBuf<int> wb_sys, wb_atom0, tb_sys, tb_atom0;
   DBuf<int> sysid, molid, molfirst, molend, mol_start, cov_start, cov_j, cov_i_flat, cov_j_flat;
   DBuf<T> q, radius, alpha, ialpha, rminh, seps;
   DBuf<double> mass, cov_c, cov_c_flat, bmod;
@@ -138,6 +159,7 @@ struct Engine : EngineBase {
   DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D;
   DBuf<double4> pperm, off, dEdd;
   DBuf<int> cell_of, slot_of, cell_count, cell_start, cell_atoms;
+  DBuf<double4> spos;
   DBuf<int> rn, rnsp, rk, dmax, dany;
   DBuf<T> rx, ry, rz, rg0, rg1, rg2, rg3;
   DBuf<T> Q, Phi, Ginf;
@@ -176,6 +198,7 @@ struct Engine : EngineBase {
     a.base = base.p; a.frac = frac.p; a.pperm = pperm.p; a.off = off.p;
     a.cell_of = cell_of.p; a.slot_of = slot_of.p; a.cell_count = cell_count.p; a.cell_start = cell_start.p;
     a.cell_atoms = cell_atoms.p;
+    a.spos = spos.p;
     a.idx = idx; a.idx_width = idx_width;
     a.rn = rn.p; a.rnsp = rnsp.p; a.rk = rk.p;
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
@@ -309,28 +332,45 @@ struct Engine : EngineBase {
     mc_auto = std::max(32, (int)std::ceil((sphere * 1.25 + 16.0) / 32.0) * 32);
     mc = set.row_capacity > 0 ? ((set.row_capacity + 31) / 32) * 32 : mc_auto;
     // block maps
-    std::vector<int> wbs, wba, tbs, tba, tx, ty, tz;
-    int cx = 0, cy = 0, cz = 0;
+    std::vector<int> wbs, wba, tbs, tba;
     for (int si = 0; si < n; ++si) {
       const pgm::SysInfo &S = hsys[si];
       for (int a = 0; a < S.natom; a += pgm::WARPS_PER_BLOCK) { wbs.push_back(si); wba.push_back(S.atom0 + a); }
       for (int a = 0; a < S.natom; a += pgm::THREADS_PER_BLOCK) { tbs.push_back(si); tba.push_back(S.atom0 + a); }
-      tx.push_back(cx); ty.push_back(cy); tz.push_back(cz);
-      int nlines = S.K[0] * S.K[1];
-      int nt3 = (S.K3h + pgm::FFT_TILE - 1) / pgm::FFT_TILE;
-      cx += (nlines + 2 * pgm::FFT_PAIRS - 1) / (2 * pgm::FFT_PAIRS);
-      cy += S.K[0] * nt3;
-      cz += S.K[1] * nt3;
-      smem_x = std::max(smem_x, (size_t)2 * pgm::FFT_PAIRS * S.K[2] * sizeof(pgm::c2<T>));
-      smem_y = std::max(smem_y, (size_t)2 * pgm::FFT_TILE * (S.K[1] + 1) * sizeof(pgm::c2<T>));
-      smem_z = std::max(smem_z, (size_t)2 * pgm::FFT_TILE * (S.K[0] + 1) * sizeof(pgm::c2<T>));
     }
-    tx.push_back(cx); ty.push_back(cy); tz.push_back(cz);
-    tiles_x = cx; tiles_y = cy; tiles_z = cz;
     nwblk = (int)wbs.size();
     ntblk = (int)tbs.size();
     wb_sys.upload(wbs); wb_atom0.upload(wba); tb_sys.upload(tbs); tb_atom0.upload(tba);
-    tile0_x.upload(tx); tile0_y.upload(ty); tile0_z.upload(tz);
+    // FFT launch groups per axis: systems with the same mesh length share one launch
+    auto groups = [&](int axis, std::vector<std::unique_ptr<FftGroup>> &out) {
+      std::vector<int> Ks;
+      for (auto &S : hsys)
+        if (std::find(Ks.begin(), Ks.end(), S.K[axis]) == Ks.end()) Ks.push_back(S.K[axis]);
+      for (int K : Ks) {
+        std::unique_ptr<FftGroup> g(new FftGroup());
+        g->K = K;
+        std::vector<int> gs, gt{0};
+        for (int si = 0; si < n; ++si) {
+          const pgm::SysInfo &S = hsys[si];
+          if (S.K[axis] != K) continue;
+          int tiles = axis == 2 ? (S.K[0] * S.K[1] + 2 * pgm::FFT_PAIRS - 1) / (2 * pgm::FFT_PAIRS)
+                    : axis == 1 ? (S.K[0] * S.K3h + pgm::FFT_TILE - 1) / pgm::FFT_TILE
+                                : (S.K[1] * S.K3h + pgm::FFT_TILE - 1) / pgm::FFT_TILE;
+          gs.push_back(si);
+          gt.push_back(gt.back() + tiles);
+        }
+        g->ng = (int)gs.size();
+        g->ntiles = gt.back();
+        g->smem = axis == 2 ? (size_t)2 * pgm::FFT_PAIRS * K * sizeof(pgm::c2<T>)
+                            : (size_t)2 * pgm::FFT_TILE * (K + 1) * sizeof(pgm::c2<T>);
+        g->sys.upload(gs);
+        g->tile0.upload(gt);
+        out.push_back(std::move(g));
+      }
+    };
+    groups(2, gx);
+    groups(1, gy);
+    groups(0, gz);
     d_sys.upload(hsys);
     d_box.alloc(n);
     CK(cudaMemset(d_box.p, 0, sizeof(pgm::BoxInfo) * n));
@@ -348,7 +388,7 @@ struct Engine : EngineBase {
     tw.upload(h_tw);
     base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt);
     pperm.alloc(nt); off.alloc(nt); dEdd.alloc(nt);
-    cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt);
+    cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt); spos.alloc(nt);
     rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(1); dany.alloc(1);
     alloc_rows();
     Q.alloc(rgrid); Phi.alloc(rgrid); Ginf.alloc(cgrid); C.alloc(cgrid);
@@ -369,11 +409,55 @@ struct Engine : EngineBase {
   }
 
   void set_smem() {
-    smem_attr(pgm::k_fft_x_fwd<T, 0>, smem_x); smem_attr(pgm::k_fft_x_fwd<T, 1>, smem_x); smem_attr(pgm::k_fft_x_fwd<T, 2>, smem_x);
-    smem_attr(pgm::k_fft_x_inv<T, 0>, smem_x); smem_attr(pgm::k_fft_x_inv<T, 1>, smem_x); smem_attr(pgm::k_fft_x_inv<T, 2>, smem_x);
-    smem_attr(pgm::k_fft_y<T, 0>, smem_y); smem_attr(pgm::k_fft_y<T, 1>, smem_y); smem_attr(pgm::k_fft_y<T, 2>, smem_y);
-    smem_attr(pgm::k_fft_z_conv<T, 0, false>, smem_z); smem_attr(pgm::k_fft_z_conv<T, 1, false>, smem_z);
-    smem_attr(pgm::k_fft_z_conv<T, 2, false>, smem_z); smem_attr(pgm::k_fft_z_conv<T, 0, true>, smem_z);
+    for (auto &g : gx)
+      with_fft_len(g->K, [&](auto Lc) {
+        constexpr int L = decltype(Lc)::value;
+        smem_attr(pgm::k_fft_x_fwd<T, L>, g->smem);
+        smem_attr(pgm::k_fft_x_inv<T, L>, g->smem);
+      });
+    for (auto &g : gy)
+      with_fft_len(g->K, [&](auto Lc) {
+        constexpr int L = decltype(Lc)::value;
+        smem_attr(pgm::k_fft_y<T, L>, g->smem);
+      });
+    for (auto &g : gz)
+      with_fft_len(g->K, [&](auto Lc) {
+        constexpr int L = decltype(Lc)::value;
+        smem_attr(pgm::k_fft_z_conv<T, L, false>, g->smem);
+        smem_attr(pgm::k_fft_z_conv<T, L, true>, g->smem);
+      });
+  }
+
+  // The five passes of one reciprocal-space convolution (r2c, k2, k1 with G, k2, c2r).
+  void fft_chain(cudaStream_t st, pgm::Dev<T> &a, int act, bool energy) {
+    for (auto &g : gx)
+      with_fft_len(g->K, [&](auto Lc) {
+        pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+        check_launch();
+      });
+    for (auto &g : gy)
+      with_fft_len(g->K, [&](auto Lc) {
+        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, -1);
+        check_launch();
+      });
+    for (auto &g : gz)
+      with_fft_len(g->K, [&](auto Lc) {
+        if (energy)
+          pgm::k_fft_z_conv<T, decltype(Lc)::value, true><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+        else
+          pgm::k_fft_z_conv<T, decltype(Lc)::value, false><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+        check_launch();
+      });
+    for (auto &g : gy)
+      with_fft_len(g->K, [&](auto Lc) {
+        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, +1);
+        check_launch();
+      });
+    for (auto &g : gx)
+      with_fft_len(g->K, [&](auto Lc) {
+        pgm::k_fft_x_inv<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+        check_launch();
+      });
   }
 
   void set_capacity(int c) override {
@@ -399,14 +483,11 @@ struct Engine : EngineBase {
       if (which == 0) pgm::k_rowmat<T, P, false, 1, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
       else if (which == 1) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
       else if (which == 2) {
-        pgm::k_fft_x_fwd<T, 0><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p);
-        pgm::k_fft_y<T, 0><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, -1);
-        pgm::k_fft_z_conv<T, 0, false><<<tiles_z, 256, smem_z, st>>>(a, tile0_z.p);
-        pgm::k_fft_y<T, 0><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, +1);
-        pgm::k_fft_x_inv<T, 0><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p);
+        fft_chain(st, a, 0, false);
       } else if (which == 3) pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, nullptr);
       else pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
     };
+    long long l0 = launches;
     one();  // warm-up
     CK(cudaGetLastError());
     CK(cudaEventRecord(e0, st));
@@ -416,6 +497,7 @@ struct Engine : EngineBase {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, e0, e1));
     if (which == 1) CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // the spread grid must start at zero
+    launches = l0;
     CK(cudaEventDestroy(e0));
     CK(cudaEventDestroy(e1));
     CK(cudaGetLastError());
@@ -462,11 +544,7 @@ struct Engine : EngineBase {
   template <bool WITH_Q, bool UPDATE_P, int ACT, bool ENERGY>
   void pme(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin) {
     pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
-    pgm::k_fft_x_fwd<T, ACT><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p); check_launch();
-    pgm::k_fft_y<T, ACT><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, -1); check_launch();
-    pgm::k_fft_z_conv<T, ACT, ENERGY><<<tiles_z, 256, smem_z, st>>>(a, tile0_z.p); check_launch();
-    pgm::k_fft_y<T, ACT><<<tiles_y, 256, smem_y, st>>>(a, tile0_y.p, +1); check_launch();
-    pgm::k_fft_x_inv<T, ACT><<<tiles_x, 256, smem_x, st>>>(a, tile0_x.p); check_launch();
+    fft_chain(st, a, ACT, ENERGY);
   }
 
   // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check.

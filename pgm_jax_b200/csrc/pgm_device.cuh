@@ -54,6 +54,7 @@ struct SysInfo {
 // Box-dependent values of one system, recomputed on the device every step from the caller's box.
 struct BoxInfo {
   double H[9], Hinv[9], vol;
+  double idiag[3];      // 1 / H_aa (minimum image by multiplication)
   double h[3];          // distances between lattice planes
   int R[3];             // cell search range (-1: whole axis)
   int changed;          // box differs from the previous step (influence function recomputed)
@@ -75,6 +76,16 @@ struct EnergyAcc {
   double vir[9];        // pair + reciprocal (positional and dipolar) parts [kJ/mol]
   double vinf[7];       // influence-function part: E then xx, yy, zz, xy, xz, yz [e^2/nm]
 };
+
+// Sequential minimum image with the inverse diagonal precomputed (the row-build hot loop).
+__device__ __forceinline__ void min_image_fast(double &x, double &y, double &z, const double *H, const double *id) {
+  double n = rint(z * id[2]);
+  x -= n * H[6]; y -= n * H[7]; z -= n * H[8];
+  n = rint(y * id[1]);
+  x -= n * H[3]; y -= n * H[4];
+  n = rint(x * id[0]);
+  x -= n * H[0];
+}
 
 // Sequential minimum image for a reduced lower-triangular box (pgm_jax/md/box.py:130-153).
 __device__ __forceinline__ void min_image(double &x, double &y, double &z, const double *H) {

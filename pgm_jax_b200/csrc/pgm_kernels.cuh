@@ -43,6 +43,7 @@ struct Dev {
   v4<T> *frac;
   double4 *pperm, *off;
   int *cell_of, *slot_of, *cell_count, *cell_start, *cell_atoms;
+  double4 *spos;  // positions in cell order, .w = molecule
   const int *idx;
   int idx_width;
   // rows
@@ -77,6 +78,7 @@ __global__ void k_box(Dev<T> a, const double *boxes) {
   Hi[6] = (H[3] * H[7] - H[4] * H[6]) / d; Hi[7] = (H[1] * H[6] - H[0] * H[7]) / d; Hi[8] = (H[0] * H[4] - H[1] * H[3]) / d;
   for (int k = 0; k < 9; ++k) { B.H[k] = H[k]; B.Hinv[k] = Hi[k]; }
   B.vol = fabs(d);
+  for (int c = 0; c < 3; ++c) B.idiag[c] = 1.0 / H[4 * c];
   const SysInfo &S = a.sys[s];
   for (int ax = 0; ax < 3; ++ax) {
     // plane height h_a = 1 / |column a of H^-1|
@@ -200,46 +202,74 @@ template <typename T>
 __global__ void k_scatter(Dev<T> a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
-  a.cell_atoms[a.cell_start[a.cell_of[i]] + a.slot_of[i]] = i;
+  int t = a.cell_start[a.cell_of[i]] + a.slot_of[i];
+  a.cell_atoms[t] = i;
+  a.spos[t] = make_double4(a.pos[3 * i], a.pos[3 * i + 1], a.pos[3 * i + 2], (double)a.molid[i]);
 }
 
 // ------------------------------------------------------------------ pair rows
 // One warp per atom: the molecule partners (always kept inside the cutoff; the rigid special
 // table of md/topology.py:161-178), then the neighbours from the cell list (or from the caller's
-// candidate rows), masked to r < rc, compacted by ballot into the row, with the radial kernels
-// G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] of every kept pair.
+// candidate rows), masked to r < rc (forcefield.py:1140-1195).  Kept pairs are staged in shared
+// memory in order, and the radial kernels G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] of the
+// staged pairs are evaluated 32 at a time on a full warp, then written to the row (coalesced).
+constexpr int STAGE = 64;
+
 template <typename T>
-__device__ __forceinline__ void row_candidate(const Dev<T> &a, int i, int j, bool ok, double pix, double piy, double piz,
-                                              const double *H, double rc2, T Ri2, int base, int &count, int lane) {
-  double x = 0, y = 0, z = 0;
-  bool keep = false;
-  if (ok) {
-    x = pix - a.pos[3 * j]; y = piy - a.pos[3 * j + 1]; z = piz - a.pos[3 * j + 2];
-    min_image(x, y, z, H);
-    keep = x * x + y * y + z * z < rc2;
-  }
-  unsigned bal = __ballot_sync(0xffffffffu, keep);
-  if (keep) {
-    int slot = count + __popc(bal & ((1u << lane) - 1u));
+struct RowStage {
+  int j[WARPS_PER_BLOCK][STAGE];
+  T x[WARPS_PER_BLOCK][STAGE], y[WARPS_PER_BLOCK][STAGE], z[WARPS_PER_BLOCK][STAGE];
+};
+
+template <typename T>
+__device__ __forceinline__ void rows_flush(const Dev<T> &a, RowStage<T> &st, int w, int lane, int nf, int &nst, int &written,
+                                           size_t base, T Ri2) {
+  if (lane < nf) {
+    int j = st.j[w][lane];
+    T xt = st.x[w][lane], yt = st.y[w][lane], zt = st.z[w][lane];
+    int slot = written + lane;
     if (slot < a.mc) {
-      T xt = T(x), yt = T(y), zt = T(z);
       T r = t_sqrt(xt * xt + yt * yt + zt * zt);
       T Rk = a.radius[j];
       T aik = t_rsqrt(T(2) * (Ri2 + Rk * Rk));
       T A[4], Bb[4];
       erf_kernels<T>(aik, r, A);
       erf_kernels<T>(T(a.beta), r, Bb);
-      size_t o = (size_t)base + slot;
+      size_t o = base + slot;
       a.rk[o] = j;
       a.rx[o] = xt; a.ry[o] = yt; a.rz[o] = zt;
       a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = A[1] - Bb[1]; a.rg2[o] = A[2] - Bb[2]; a.rg3[o] = A[3] - Bb[3];
     }
   }
-  count += __popc(bal);
+  written += nf;
+  int rem = nst - nf;
+  __syncwarp();
+  int j2 = 0;
+  T x2 = 0, y2 = 0, z2 = 0;
+  if (lane < rem) { j2 = st.j[w][nf + lane]; x2 = st.x[w][nf + lane]; y2 = st.y[w][nf + lane]; z2 = st.z[w][nf + lane]; }
+  __syncwarp();
+  if (lane < rem) { st.j[w][lane] = j2; st.x[w][lane] = x2; st.y[w][lane] = y2; st.z[w][lane] = z2; }
+  __syncwarp();
+  nst = rem;
+}
+
+template <typename T>
+__device__ __forceinline__ void rows_stage(const Dev<T> &a, RowStage<T> &st, int w, int lane, bool keep, int j, double x,
+                                           double y, double z, int &nst, int &written, size_t base, T Ri2) {
+  unsigned bal = __ballot_sync(0xffffffffu, keep);
+  if (keep) {
+    int pos = nst + __popc(bal & ((1u << lane) - 1u));
+    st.j[w][pos] = j;
+    st.x[w][pos] = T(x); st.y[w][pos] = T(y); st.z[w][pos] = T(z);
+  }
+  nst += __popc(bal);
+  __syncwarp();
+  if (nst >= 32) rows_flush<T>(a, st, w, lane, 32, nst, written, base, Ri2);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
+  __shared__ RowStage<T> st;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int blk = blockIdx.x;
   int s = a.wb_sys[blk];
@@ -247,20 +277,28 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
   const SysInfo &S = a.sys[s];
   if (i >= S.atom0 + S.natom) return;
   const BoxInfo &B = a.box[s];
-  double H[9];
+  double H[9], id[3];
 #pragma unroll
   for (int k = 0; k < 9; ++k) H[k] = B.H[k];
+  id[0] = B.idiag[0]; id[1] = B.idiag[1]; id[2] = B.idiag[2];
   double pix = a.pos[3 * i], piy = a.pos[3 * i + 1], piz = a.pos[3 * i + 2];
   double rc2 = a.cutoff * a.cutoff;
   T Ri = a.radius[i], Ri2 = Ri * Ri;
-  int base = i * a.mc;
-  int count = 0;
+  size_t base = (size_t)i * a.mc;
+  int nst = 0, written = 0;
   int mf = a.molfirst[i], me = a.molend[i];
   for (int j0 = mf; j0 < me; j0 += 32) {
     int j = j0 + lane;
-    row_candidate<T>(a, i, j, j < me && j != i, pix, piy, piz, H, rc2, Ri2, base, count, lane);
+    bool keep = false;
+    double x = 0, y = 0, z = 0;
+    if (j < me && j != i) {
+      x = pix - a.pos[3 * j]; y = piy - a.pos[3 * j + 1]; z = piz - a.pos[3 * j + 2];
+      min_image_fast(x, y, z, H, id);
+      keep = x * x + y * y + z * z < rc2;
+    }
+    rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
   }
-  int nsp = count;
+  int nsp = written + nst;
   int mi = a.molid[i];
   if (a.idx) {  // the caller's candidate rows (local indices, padding natom)
     const int *row = a.idx + (size_t)i * a.idx_width;
@@ -270,7 +308,14 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
       bool ok = jl >= 0 && jl < S.natom;
       int j = S.atom0 + (ok ? jl : 0);
       ok = ok && a.molid[j] != mi;
-      row_candidate<T>(a, i, j, ok, pix, piy, piz, H, rc2, Ri2, base, count, lane);
+      bool keep = false;
+      double x = 0, y = 0, z = 0;
+      if (ok) {
+        x = pix - a.pos[3 * j]; y = piy - a.pos[3 * j + 1]; z = piz - a.pos[3 * j + 2];
+        min_image_fast(x, y, z, H, id);
+        keep = x * x + y * y + z * z < rc2;
+      }
+      rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
     }
   } else {  // cell list: cells within R of the atom's cell along each axis
     int cell = a.cell_of[i] - S.cell0;
@@ -284,7 +329,6 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
       for (int d1 = lo1; d1 <= hi1; ++d1) {
         int c1 = R1 < 0 ? d1 : ((ci1 + d1) % n1 + n1) % n1;
         int rowc = S.cell0 + (c0 * n1 + c1) * n2;
-        // contiguous k3 ranges of cells: one or two segments
         int segs[2][2];
         int nseg = 0;
         if (R2 < 0) {
@@ -299,19 +343,30 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
           int a0 = a.cell_start[rowc + segs[g][0]], a1 = a.cell_start[rowc + segs[g][1] + 1];
           for (int t0 = a0; t0 < a1; t0 += 32) {
             int t = t0 + lane;
-            int j = t < a1 ? a.cell_atoms[t] : i;
-            bool ok = t < a1 && a.molid[j] != mi;
-            row_candidate<T>(a, i, j, ok, pix, piy, piz, H, rc2, Ri2, base, count, lane);
+            bool keep = false;
+            int j = 0;
+            double x = 0, y = 0, z = 0;
+            if (t < a1) {
+              double4 pj = a.spos[t];
+              if ((int)pj.w != mi) {
+                x = pix - pj.x; y = piy - pj.y; z = piz - pj.z;
+                min_image_fast(x, y, z, H, id);
+                keep = x * x + y * y + z * z < rc2;
+                if (keep) j = a.cell_atoms[t];
+              }
+            }
+            rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
           }
         }
       }
     }
   }
+  while (nst > 0) rows_flush<T>(a, st, warp, lane, min(nst, 32), nst, written, base, Ri2);
   if (lane == 0) {
-    a.rn[i] = count;
+    a.rn[i] = written;
     a.rnsp[i] = nsp;
-    if (count > a.mc) atomicOr(&a.status[s], 0x1u);
-    atomicMax(a.max_count, count);
+    if (written > a.mc) atomicOr(&a.status[s], 0x1u);
+    atomicMax(a.max_count, written);
   }
 }
 
@@ -407,108 +462,163 @@ __device__ __forceinline__ c2<T> cmul(c2<T> a, c2<T> b) {
   return r;
 }
 
-// In-shared-memory Stockham autosort FFT of `nl` lines of length L (line stride ld) by the
-// block; radices 2, 3, 4, 5; sign -1 forward, +1 inverse; tw[m] = exp(-2 pi i m / L).  Returns
-// the buffer that holds the result.
+// Radix plan of a length-L transform: radix 4 first, then 2, 3, 5 (constexpr and runtime).
+__host__ __device__ constexpr int fft_nst(int L) {
+  int n = 0;
+  while (L % 4 == 0) { L /= 4; ++n; }
+  while (L % 2 == 0) { L /= 2; ++n; }
+  while (L % 3 == 0) { L /= 3; ++n; }
+  while (L % 5 == 0) { L /= 5; ++n; }
+  return n;
+}
+__host__ __device__ constexpr int fft_radix(int L, int st) {
+  int n = 0;
+  while (L % 4 == 0) { if (n == st) return 4; L /= 4; ++n; }
+  while (L % 2 == 0) { if (n == st) return 2; L /= 2; ++n; }
+  while (L % 3 == 0) { if (n == st) return 3; L /= 3; ++n; }
+  while (L % 5 == 0) { if (n == st) return 5; L /= 5; ++n; }
+  return 1;
+}
+
+// R-point DFT in registers, sign -1 forward / +1 inverse.
+template <typename T, int R>
+__device__ __forceinline__ void butterfly(c2<T> *v, T sg) {
+  c2<T> o[R];
+  if constexpr (R == 2) {
+    o[0].x = v[0].x + v[1].x; o[0].y = v[0].y + v[1].y;
+    o[1].x = v[0].x - v[1].x; o[1].y = v[0].y - v[1].y;
+  } else if constexpr (R == 4) {
+    c2<T> a0, a1, b0, b1, ib1;
+    a0.x = v[0].x + v[2].x; a0.y = v[0].y + v[2].y;
+    a1.x = v[0].x - v[2].x; a1.y = v[0].y - v[2].y;
+    b0.x = v[1].x + v[3].x; b0.y = v[1].y + v[3].y;
+    b1.x = v[1].x - v[3].x; b1.y = v[1].y - v[3].y;
+    ib1.x = -sg * b1.y; ib1.y = sg * b1.x;  // sign * i * b1
+    o[0].x = a0.x + b0.x; o[0].y = a0.y + b0.y;
+    o[2].x = a0.x - b0.x; o[2].y = a0.y - b0.y;
+    o[1].x = a1.x + ib1.x; o[1].y = a1.y + ib1.y;
+    o[3].x = a1.x - ib1.x; o[3].y = a1.y - ib1.y;
+  } else if constexpr (R == 3) {
+    const T c = T(-0.5), sn = sg * T(0.86602540378443864676);
+    c2<T> t1, t2, m;
+    t1.x = v[1].x + v[2].x; t1.y = v[1].y + v[2].y;
+    t2.x = v[1].x - v[2].x; t2.y = v[1].y - v[2].y;
+    o[0].x = v[0].x + t1.x; o[0].y = v[0].y + t1.y;
+    m.x = v[0].x + c * t1.x; m.y = v[0].y + c * t1.y;
+    o[1].x = m.x - sn * t2.y; o[1].y = m.y + sn * t2.x;
+    o[2].x = m.x + sn * t2.y; o[2].y = m.y - sn * t2.x;
+  } else {
+    static_assert(R == 5, "radix");
+    const T c1 = T(0.30901699437494742410), c2v = T(-0.80901699437494742410);
+    const T s1 = sg * T(0.95105651629515357212), s2 = sg * T(0.58778525229247312917);
+    c2<T> a1, a2, b1, b2, m1, m2, n1, n2;
+    a1.x = v[1].x + v[4].x; a1.y = v[1].y + v[4].y;
+    b1.x = v[1].x - v[4].x; b1.y = v[1].y - v[4].y;
+    a2.x = v[2].x + v[3].x; a2.y = v[2].y + v[3].y;
+    b2.x = v[2].x - v[3].x; b2.y = v[2].y - v[3].y;
+    o[0].x = v[0].x + a1.x + a2.x; o[0].y = v[0].y + a1.y + a2.y;
+    m1.x = v[0].x + c1 * a1.x + c2v * a2.x; m1.y = v[0].y + c1 * a1.y + c2v * a2.y;
+    m2.x = v[0].x + c2v * a1.x + c1 * a2.x; m2.y = v[0].y + c2v * a1.y + c1 * a2.y;
+    n1.x = s1 * b1.x + s2 * b2.x; n1.y = s1 * b1.y + s2 * b2.y;
+    n2.x = s2 * b1.x - s1 * b2.x; n2.y = s2 * b1.y - s1 * b2.y;
+    o[1].x = m1.x - n1.y; o[1].y = m1.y + n1.x;
+    o[4].x = m1.x + n1.y; o[4].y = m1.y - n1.x;
+    o[2].x = m2.x - n2.y; o[2].y = m2.y + n2.x;
+    o[3].x = m2.x + n2.y; o[3].y = m2.y - n2.x;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = o[r];
+}
+
+// One Stockham stage (radix R, NS points already combined) of nl lines of length L in shared
+// memory: v_r = x[j + r L/R] w^(r k), k = j mod NS, DFT_R, y[(j / NS) NS R + k + r NS].
+template <typename T, int R>
+__device__ __forceinline__ void fft_stage(const c2<T> *x, c2<T> *y, int L, int NS, int nl, int ld, const c2<T> *tw, int sign) {
+  const int LR = L / R, stride = L / (NS * R);
+  const T sg = T(sign);
+  for (int w = threadIdx.x; w < LR * nl; w += blockDim.x) {
+    int line = w / LR, j = w - line * LR;
+    int k = j % NS;
+    const c2<T> *in = x + line * ld;
+    c2<T> *out = y + line * ld;
+    c2<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      c2<T> u = in[j + r * LR];
+      if (r > 0) {
+        c2<T> t = tw[r * k * stride];
+        if (sign > 0) t.y = -t.y;
+        u = cmul<T>(u, t);
+      }
+      v[r] = u;
+    }
+    butterfly<T, R>(v, sg);
+    int dst = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[dst + r * NS] = v[r];
+  }
+  __syncthreads();
+}
+
+// Compile-time length: every index constant folds (L, R, NS template-known).
+template <typename T, int L, int ST, int NS>
+__device__ __forceinline__ c2<T> *fft_run_ct(c2<T> *x, c2<T> *y, int nl, int ld, const c2<T> *tw, int sign) {
+  if constexpr (ST == fft_nst(L)) {
+    return x;
+  } else {
+    constexpr int R = fft_radix(L, ST);
+    fft_stage<T, R>(x, y, L, NS, nl, ld, tw, sign);
+    return fft_run_ct<T, L, ST + 1, NS * R>(y, x, nl, ld, tw, sign);
+  }
+}
+
+// Runtime length (fallback for meshes without a compiled plan).
 template <typename T>
-__device__ c2<T> *fft_lines(c2<T> *x, c2<T> *y, int L, int nl, int ld, const int *rad, int nst, const c2<T> *tw, int sign) {
-  int Ns = 1;
+__device__ c2<T> *fft_run_rt(c2<T> *x, c2<T> *y, int L, int nl, int ld, const int *rad, int nst, const c2<T> *tw, int sign) {
+  int NS = 1;
   for (int st = 0; st < nst; ++st) {
     const int R = rad[st];
-    const int LR = L / R;
-    const int stride = L / (Ns * R);
-    for (int w = threadIdx.x; w < LR * nl; w += blockDim.x) {
-      int line = w / LR, j = w - line * LR;
-      const c2<T> *in = x + line * ld;
-      c2<T> *out = y + line * ld;
-      int k = j % Ns;
-      c2<T> v[5];
-      for (int r = 0; r < R; ++r) {
-        c2<T> u = in[j + r * LR];
-        if (r > 0 && Ns > 1) {
-          c2<T> t = tw[(r * k * stride) % L];
-          if (sign > 0) t.y = -t.y;
-          u = cmul<T>(u, t);
-        }
-        v[r] = u;
-      }
-      const T sg = T(sign);
-      c2<T> o[5];
-      if (R == 2) {
-        o[0].x = v[0].x + v[1].x; o[0].y = v[0].y + v[1].y;
-        o[1].x = v[0].x - v[1].x; o[1].y = v[0].y - v[1].y;
-      } else if (R == 4) {
-        c2<T> a0, a1, b0, b1;
-        a0.x = v[0].x + v[2].x; a0.y = v[0].y + v[2].y;
-        a1.x = v[0].x - v[2].x; a1.y = v[0].y - v[2].y;
-        b0.x = v[1].x + v[3].x; b0.y = v[1].y + v[3].y;
-        b1.x = v[1].x - v[3].x; b1.y = v[1].y - v[3].y;
-        // sign * i * b1
-        c2<T> ib1;
-        ib1.x = -sg * b1.y; ib1.y = sg * b1.x;
-        o[0].x = a0.x + b0.x; o[0].y = a0.y + b0.y;
-        o[2].x = a0.x - b0.x; o[2].y = a0.y - b0.y;
-        o[1].x = a1.x + ib1.x; o[1].y = a1.y + ib1.y;
-        o[3].x = a1.x - ib1.x; o[3].y = a1.y - ib1.y;
-      } else if (R == 3) {
-        const T c = T(-0.5), sn = sg * T(0.86602540378443864676);
-        c2<T> t1, t2;
-        t1.x = v[1].x + v[2].x; t1.y = v[1].y + v[2].y;
-        t2.x = v[1].x - v[2].x; t2.y = v[1].y - v[2].y;
-        o[0].x = v[0].x + t1.x; o[0].y = v[0].y + t1.y;
-        c2<T> m;
-        m.x = v[0].x + c * t1.x; m.y = v[0].y + c * t1.y;
-        // +- i sn t2
-        o[1].x = m.x - sn * t2.y; o[1].y = m.y + sn * t2.x;
-        o[2].x = m.x + sn * t2.y; o[2].y = m.y - sn * t2.x;
-      } else {  // R == 5
-        const T c1 = T(0.30901699437494742410), c2v = T(-0.80901699437494742410);
-        const T s1 = sg * T(0.95105651629515357212), s2 = sg * T(0.58778525229247312917);
-        c2<T> a1, a2, b1, b2;
-        a1.x = v[1].x + v[4].x; a1.y = v[1].y + v[4].y;
-        b1.x = v[1].x - v[4].x; b1.y = v[1].y - v[4].y;
-        a2.x = v[2].x + v[3].x; a2.y = v[2].y + v[3].y;
-        b2.x = v[2].x - v[3].x; b2.y = v[2].y - v[3].y;
-        o[0].x = v[0].x + a1.x + a2.x; o[0].y = v[0].y + a1.y + a2.y;
-        c2<T> m1, m2, n1, n2;
-        m1.x = v[0].x + c1 * a1.x + c2v * a2.x; m1.y = v[0].y + c1 * a1.y + c2v * a2.y;
-        m2.x = v[0].x + c2v * a1.x + c1 * a2.x; m2.y = v[0].y + c2v * a1.y + c1 * a2.y;
-        n1.x = s1 * b1.x + s2 * b2.x; n1.y = s1 * b1.y + s2 * b2.y;
-        n2.x = s2 * b1.x - s1 * b2.x; n2.y = s2 * b1.y - s1 * b2.y;
-        // o1 = m1 + i n1, o4 = m1 - i n1, o2 = m2 + i n2, o3 = m2 - i n2
-        o[1].x = m1.x - n1.y; o[1].y = m1.y + n1.x;
-        o[4].x = m1.x + n1.y; o[4].y = m1.y - n1.x;
-        o[2].x = m2.x - n2.y; o[2].y = m2.y + n2.x;
-        o[3].x = m2.x + n2.y; o[3].y = m2.y - n2.x;
-      }
-      int dst = (j / Ns) * Ns * R + k;
-      for (int r = 0; r < R; ++r) out[dst + r * Ns] = o[r];
-    }
-    __syncthreads();
+    if (R == 4) fft_stage<T, 4>(x, y, L, NS, nl, ld, tw, sign);
+    else if (R == 2) fft_stage<T, 2>(x, y, L, NS, nl, ld, tw, sign);
+    else if (R == 3) fft_stage<T, 3>(x, y, L, NS, nl, ld, tw, sign);
+    else fft_stage<T, 5>(x, y, L, NS, nl, ld, tw, sign);
     c2<T> *t = x; x = y; y = t;
-    Ns *= R;
+    NS *= R;
   }
   return x;
 }
 
-// Which system a CTA of an FFT pass belongs to: tile prefix per system in `tile0` (nsys + 1).
-__device__ __forceinline__ int tile_system(const int *tile0, int nsys, int b) {
-  int s = 0;
-  while (s + 1 < nsys && tile0[s + 1] <= b) ++s;
-  return s;
+template <typename T, int L>
+__device__ __forceinline__ c2<T> *fft_lines(c2<T> *x, c2<T> *y, int Lrt, int nl, int ld, const int *rad, int nst, const c2<T> *tw,
+                                            int sign) {
+  if constexpr (L == 0) return fft_run_rt<T>(x, y, Lrt, nl, ld, rad, nst, tw, sign);
+  else return fft_run_ct<T, L, 0, 1>(x, y, nl, ld, tw, sign);
+}
+
+// A launch of an FFT pass covers a group of systems with the same mesh length along the pass's
+// axis: block -> (group member g, tile) by the tile prefix gtile0 (ng + 1 entries).
+__device__ __forceinline__ int group_member(const int *gtile0, int ng, int b) {
+  int g = 0;
+  while (g + 1 < ng && gtile0[g + 1] <= b) ++g;
+  return g;
+}
+
+template <typename T>
+__device__ __forceinline__ bool pass_active(const Dev<T> &a, int s, int act) {
+  return act == 0 || (act == 1 && a.cg[s].active) || (act == 2 && a.cg[s].sweep2);
 }
 
 // k3 pass, real -> half complex: two real lines packed as one complex line (z = a + i b), one
 // length-K3 FFT, untangled; the real grid is cleared as it is read (ready for the next spread).
-template <typename T, int ACT>
-__global__ void k_fft_x_fwd(Dev<T> a, const int *tile0) {
+template <typename T, int L>
+__global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
   extern __shared__ unsigned char smem_raw[];
-  int s = tile_system(tile0, a.nsys, blockIdx.x);
-  if (ACT == 1 && !a.cg[s].active) return;
-  if (ACT == 2 && !a.cg[s].sweep2) return;
+  int g = group_member(gtile0, ng, blockIdx.x);
+  int s = gsys[g];
+  if (!pass_active(a, s, act)) return;
   const SysInfo &S = a.sys[s];
-  const int K3 = S.K[2], K3h = S.K3h, nlines = S.K[0] * S.K[1];
-  int tile = blockIdx.x - tile0[s];
+  const int K3 = L ? L : S.K[2], K3h = K3 / 2 + 1, nlines = S.K[0] * S.K[1];
+  int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;  // first real line
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
   c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3;
@@ -521,15 +631,14 @@ __global__ void k_fft_x_fwd(Dev<T> a, const int *tile0) {
     dst[rl & 1] = v;
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], -1);
+  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], -1);
   c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
   for (int t = threadIdx.x; t < np * K3h; t += blockDim.x) {
     int cl = t / K3h, m = t - cl * K3h;
     c2<T> Z = res[cl * K3 + m], W = res[cl * K3 + (m == 0 ? 0 : K3 - m)];
     c2<T> A, Bv;
     A.x = T(0.5) * (Z.x + W.x); A.y = T(0.5) * (Z.y - W.y);
-    // (Z - conj W) / (2 i)
-    T dx = Z.x - W.x, dy = Z.y + W.y;
+    T dx = Z.x - W.x, dy = Z.y + W.y;  // (Z - conj W) / (2 i)
     Bv.x = T(0.5) * dy; Bv.y = -T(0.5) * dx;
     C[(size_t)(2 * cl) * K3h + m] = A;
     C[(size_t)(2 * cl + 1) * K3h + m] = Bv;
@@ -537,15 +646,15 @@ __global__ void k_fft_x_fwd(Dev<T> a, const int *tile0) {
 }
 
 // k3 pass, half complex -> real (the inverse of k_fft_x_fwd, unnormalised): writes phi.
-template <typename T, int ACT>
-__global__ void k_fft_x_inv(Dev<T> a, const int *tile0) {
+template <typename T, int L>
+__global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
   extern __shared__ unsigned char smem_raw[];
-  int s = tile_system(tile0, a.nsys, blockIdx.x);
-  if (ACT == 1 && !a.cg[s].active) return;
-  if (ACT == 2 && !a.cg[s].sweep2) return;
+  int g = group_member(gtile0, ng, blockIdx.x);
+  int s = gsys[g];
+  if (!pass_active(a, s, act)) return;
   const SysInfo &S = a.sys[s];
-  const int K3 = S.K[2], K3h = S.K3h, nlines = S.K[0] * S.K[1];
-  int tile = blockIdx.x - tile0[s];
+  const int K3 = L ? L : S.K[2], K3h = K3 / 2 + 1, nlines = S.K[0] * S.K[1];
+  int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
   c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3;
@@ -562,7 +671,7 @@ __global__ void k_fft_x_inv(Dev<T> a, const int *tile0) {
     x[cl * K3 + m] = Z;
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], +1);
+  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], +1);
   T *Phi = a.Phi + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
     int rl = t / K3, k = t - rl * K3;
@@ -571,80 +680,85 @@ __global__ void k_fft_x_inv(Dev<T> a, const int *tile0) {
   }
 }
 
-// k2 pass (both directions): tiles of FFT_TILE consecutive m3 at one k1.
-template <typename T, int ACT>
-__global__ void k_fft_y(Dev<T> a, const int *tile0, int sign) {
+// k2 pass (both directions): FFT_TILE consecutive columns (k1, m3) of the flattened K1 x K3h
+// column index, each a line over k2 with stride K3h.
+template <typename T, int L>
+__global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act, int sign) {
   extern __shared__ unsigned char smem_raw[];
-  int s = tile_system(tile0, a.nsys, blockIdx.x);
-  if (ACT == 1 && !a.cg[s].active) return;
-  if (ACT == 2 && !a.cg[s].sweep2) return;
+  int g = group_member(gtile0, ng, blockIdx.x);
+  int s = gsys[g];
+  if (!pass_active(a, s, act)) return;
   const SysInfo &S = a.sys[s];
-  const int K2 = S.K[1], K3h = S.K3h;
-  const int ntile3 = (K3h + FFT_TILE - 1) / FFT_TILE;
-  int tile = blockIdx.x - tile0[s];
-  int k1 = tile / ntile3, m30 = (tile % ntile3) * FFT_TILE;
+  const int K2 = L ? L : S.K[1], K3h = S.K3h, ncol = S.K[0] * K3h;
+  int c0 = (blockIdx.x - gtile0[g]) * FFT_TILE;
   const int ld = K2 + 1;
   c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld;
-  c2<T> *C = a.C + S.cgrid0 + (size_t)k1 * K2 * K3h;
+  c2<T> *C = a.C + S.cgrid0;
   for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
     int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
-    int m3 = m30 + c;
+    int col = c0 + c;
     c2<T> v;
     v.x = T(0); v.y = T(0);
-    if (m3 < K3h) v = C[(size_t)k2 * K3h + m3];
+    if (col < ncol) {
+      int k1 = col / K3h, m3 = col - k1 * K3h;
+      v = C[((size_t)k1 * K2 + k2) * K3h + m3];
+    }
     x[c * ld + k2] = v;
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], a.tw + S.tw[1], sign);
+  c2<T> *res = fft_lines<T, L>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], a.tw + S.tw[1], sign);
   for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
     int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
-    int m3 = m30 + c;
-    if (m3 < K3h) C[(size_t)k2 * K3h + m3] = res[c * ld + k2];
+    int col = c0 + c;
+    if (col < ncol) {
+      int k1 = col / K3h, m3 = col - k1 * K3h;
+      C[((size_t)k1 * K2 + k2) * K3h + m3] = res[c * ld + k2];
+    }
   }
 }
 
-// k1 pass with the convolution: forward FFT along k1, multiply by 2 G(m) (phi = dE/dQ =
-// 2 K^3 irfft(G F[Q]), pme.py:370-376), inverse FFT.  With ENERGY the reciprocal energy
-// sum w3 G |F|^2 (pme.py:390-411) and the influence part of the virial are accumulated.
-template <typename T, int ACT, bool ENERGY>
-__global__ void k_fft_z_conv(Dev<T> a, const int *tile0) {
+// k1 pass with the convolution: FFT_TILE consecutive columns c = k2 K3h + m3 (contiguous in
+// memory), forward FFT along k1, multiply by 2 G(m) (phi = dE/dQ = 2 K^3 irfft(G F[Q]),
+// pme.py:370-376), inverse FFT.  With ENERGY the reciprocal energy sum w3 G |F|^2
+// (pme.py:390-411) and the influence part of the virial are accumulated.
+template <typename T, int L, bool ENERGY>
+__global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ double red[7][8];
-  int s = tile_system(tile0, a.nsys, blockIdx.x);
-  if (ACT == 1 && !a.cg[s].active) return;
-  if (ACT == 2 && !a.cg[s].sweep2) return;
+  int g = group_member(gtile0, ng, blockIdx.x);
+  int s = gsys[g];
+  if (!pass_active(a, s, act)) return;
   const SysInfo &S = a.sys[s];
-  const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2], K3h = S.K3h;
-  const int ntile3 = (K3h + FFT_TILE - 1) / FFT_TILE;
-  int tile = blockIdx.x - tile0[s];
-  int k2 = tile / ntile3, m30 = (tile % ntile3) * FFT_TILE;
+  const int K1 = L ? L : S.K[0], K2 = S.K[1], K3 = S.K[2], K3h = S.K3h, ncol = K2 * K3h;
+  int c0 = (blockIdx.x - gtile0[g]) * FFT_TILE;
   const int ld = K1 + 1;
   c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld;
-  c2<T> *C = a.C + S.cgrid0 + (size_t)k2 * K3h;
-  const size_t rs = (size_t)K2 * K3h;
+  c2<T> *C = a.C + S.cgrid0;
+  const size_t rs = (size_t)ncol;
   for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
     int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
-    int m3 = m30 + c;
+    int col = c0 + c;
     c2<T> v;
     v.x = T(0); v.y = T(0);
-    if (m3 < K3h) v = C[k1 * rs + m3];
+    if (col < ncol) v = C[k1 * rs + col];
     x[c * ld + k1] = v;
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], -1);
+  c2<T> *res = fft_lines<T, L>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], -1);
   c2<T> *oth = res == x ? y : x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const BoxInfo &B = a.box[s];
-  const T *G = a.Ginf + S.cgrid0 + (size_t)k2 * K3h;
+  const T *G = a.Ginf + S.cgrid0;
   for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
     int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
-    int m3 = m30 + c;
-    if (m3 >= K3h) continue;
-    T g = G[k1 * rs + m3];
+    int col = c0 + c;
+    if (col >= ncol) continue;
+    T gv = G[k1 * rs + col];
     c2<T> F = res[c * ld + k1];
-    if (ENERGY && g != T(0)) {
+    if (ENERGY && gv != T(0)) {
+      int k2 = col / K3h, m3 = col - k2 * K3h;
       double w3 = (m3 == 0 || 2 * m3 == K3) ? 1.0 : 2.0;
-      double e = w3 * double(g) * (double(F.x) * double(F.x) + double(F.y) * double(F.y));
+      double e = w3 * double(gv) * (double(F.x) * double(F.x) + double(F.y) * double(F.y));
       int m1 = k1 <= (K1 - 1) / 2 ? k1 : k1 - K1;
       int m2 = k2 <= (K2 - 1) / 2 ? k2 : k2 - K2;
       if (K1 % 2 == 0 && k1 == K1 / 2) m1 = -K1 / 2;
@@ -661,7 +775,7 @@ __global__ void k_fft_z_conv(Dev<T> a, const int *tile0) {
       acc[5] += e * fac * mv[0] * mv[2];
       acc[6] += e * fac * mv[1] * mv[2];
     }
-    T g2 = T(2) * g;
+    T g2 = T(2) * gv;
     F.x *= g2; F.y *= g2;
     res[c * ld + k1] = F;
   }
@@ -678,11 +792,11 @@ __global__ void k_fft_z_conv(Dev<T> a, const int *tile0) {
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
     atomicAdd(&a.eacc[s].vinf[threadIdx.x], v);
   }
-  c2<T> *res2 = fft_lines<T>(res, oth, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], +1);
+  c2<T> *res2 = fft_lines<T, L>(res, oth, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], +1);
   for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
     int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
-    int m3 = m30 + c;
-    if (m3 < K3h) C[k1 * rs + m3] = res2[c * ld + k1];
+    int col = c0 + c;
+    if (col < ncol) C[k1 * rs + col] = res2[c * ld + k1];
   }
 }
 

@@ -191,17 +191,27 @@ def test_water512_fp64_matches_oracle():
     assert rms_rel(m.induction.mu.cpu().numpy(), r["mu"]) <= 1e-5
 
 
-def test_row_overflow_is_reported_and_recovers(box):
-    """A capacity below the largest row sets the overflow bit; growing it repeats the step correctly."""
-    s, pos, H, o, r = box
-    ff = ff_for(s, H, "double")
-    ff.set_capacity(32)
+def test_row_overflow_is_reported_and_recovers():
+    """A capacity below the largest row sets the overflow bit; growing it repeats the step correctly.
+
+    (The driver's resize-and-repeat of the reference, driver.py:117-151, forcefield.py:1286.)
+    """
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(8, 2.483, seed=0)
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(48, 48, 48), pme_order=6, dipole_tol=1e-8, max_iter=100)
+    ff = PGMForceField(s, H, MDSettings(precision="double", **st))
+    ref = ff.compute(pos, H)
+    assert not bool(ref.overflow[0])
+    big = ff.capacity
+    ff.set_capacity(64)
     res = ff.compute(pos, H)
-    assert bool(res.overflow[0])
-    ff.grow_rows(ff.capacity * 8)
+    assert bool(res.overflow[0]) and ff.capacity == 64
+    ff.grow_rows(big)
     res = ff.compute(pos, H)
     assert not bool(res.overflow[0])
-    assert abs(float(res.energy["total"][0]) - r["energy"]["total"]) <= 1e-9 * abs(r["energy"]["total"])
+    assert abs(float(res.energy["total"][0]) - float(ref.energy["total"][0])) <= 1e-10 * abs(float(ref.energy["total"][0]))
 
 
 def test_cg_max_iter_status(box):
