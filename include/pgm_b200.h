@@ -42,6 +42,7 @@ typedef enum {
 #define PGM_STATUS_CG_MAXITER   0x2u   /* CG stopped at max_iter above the tolerance */
 #define PGM_STATUS_NONFINITE    0x4u   /* non-finite energy */
 #define PGM_STATUS_BAD_BOX      0x8u   /* box not lower triangular / too small for the cutoff */
+#define PGM_STATUS_LIST_OVERFLOW 0x10u /* an atom had more candidates within cutoff + skin than the list capacity */
 
 /* Settings of one handle: the MDSettings fields of the path (forcefield.py:386-516). */
 typedef struct {
@@ -59,6 +60,9 @@ typedef struct {
     int norm_refresh;   /* Induction.norm_refresh */
     double peek;        /* Induction.peek */
     int row_capacity;   /* pairs kept per row; 0: sized from the density (PGMForceField.size_rows) */
+    double skin;        /* Verlet skin of the engine's candidate list [nm] (NeighborList.skin); clipped so
+                           that cutoff + skin fits the smallest box, 0: rebuilt every step */
+    int list_capacity;  /* candidates kept per atom; 0: sized from the density */
 } PgmSettings;
 
 /* One system of the batch: topology and parameters (host arrays, copied at creation). */
@@ -137,6 +141,14 @@ PgmStatus pgm_field(PgmHandle *h, void *stream, const double *pos, const double 
  * row, rounded up to a multiple of 32); 0 restores the automatic size. */
 PgmStatus pgm_set_row_capacity(PgmHandle *h, int capacity);
 int pgm_row_capacity(const PgmHandle *h);
+
+/* Candidates kept per atom in the engine's Verlet list (rounded up to a multiple of 32; 0:
+ * automatic); the list is rebuilt at the next call. */
+PgmStatus pgm_set_list_capacity(PgmHandle *h, int capacity);
+int pgm_list_capacity(const PgmHandle *h);
+/* Steps since creation at which the candidate list was rebuilt (host counter of calls that found
+ * the rebuild flag set is not kept; this reads the device counter). */
+long long pgm_list_rebuilds(PgmHandle *h);
 
 /* Largest in-cutoff pair count of any row in the last step (for size_rows). */
 int pgm_max_row_count(PgmHandle *h);

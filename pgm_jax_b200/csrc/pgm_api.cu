@@ -103,6 +103,9 @@ struct EngineBase {
   virtual void fixed_mu(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
                         const double *mu, double *energy, double *forces, double *virial, uint32_t *status) = 0;
   virtual void set_capacity(int mc) = 0;
+  virtual void set_list_capacity(int c) = 0;
+  virtual int list_capacity() const = 0;
+  virtual long long list_rebuilds() = 0;
   virtual int capacity() const = 0;
   virtual int max_count() = 0;
   virtual long long launches_per_iteration() const = 0;
@@ -140,7 +143,8 @@ template <typename T, int P>
 struct Engine : EngineBase {
   PgmSettings set;
   std::vector<pgm::SysInfo> hsys;
-  int nmol_total = 0, ncell = 0, ncov = 0, mc = 0, mc_auto = 0;
+  int nmol_total = 0, ncell = 0, ncov = 0, mc = 0, mc_auto = 0, cc = 0, cc_auto = 0;
+  double skin = 0.0;
   long long rgrid = 0, cgrid = 0;
   std::vector<std::unique_ptr<FftGroup>> gx, gy, gz;
   int nwblk = 0, ntblk = 0;
@@ -159,7 +163,9 @@ struct Engine : EngineBase {
   DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D;
   DBuf<double4> pperm, off, dEdd;
   DBuf<int> cell_of, slot_of, cell_count, cell_start, cell_atoms;
-  DBuf<double4> spos;
+  DBuf<double4> spos, pos_ref, pos4;
+  DBuf<int> cand, ncand, nb_flag;
+  DBuf<long long> nb_builds;
   DBuf<int> rn, rnsp, rk, dmax, dany;
   DBuf<T> rx, ry, rz, rg0, rg1, rg2, rg3;
   DBuf<T> Q, Phi, Ginf;
@@ -199,6 +205,8 @@ struct Engine : EngineBase {
     a.cell_of = cell_of.p; a.slot_of = slot_of.p; a.cell_count = cell_count.p; a.cell_start = cell_start.p;
     a.cell_atoms = cell_atoms.p;
     a.spos = spos.p;
+    a.skin = skin; a.cc = cc; a.nb_flag = nb_flag.p; a.nb_builds = nb_builds.p; a.cand = cand.p; a.ncand = ncand.p;
+    a.pos_ref = pos_ref.p; a.pos4 = pos4.p;
     a.idx = idx; a.idx_width = idx_width;
     a.rn = rn.p; a.rnsp = rnsp.p; a.rk = rk.p;
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
@@ -331,6 +339,16 @@ struct Engine : EngineBase {
     double sphere = 4.0 / 3.0 * M_PI * std::pow(set.cutoff, 3) * rho_max;
     mc_auto = std::max(32, (int)std::ceil((sphere * 1.25 + 16.0) / 32.0) * 32);
     mc = set.row_capacity > 0 ? ((set.row_capacity + 31) / 32) * 32 : mc_auto;
+    // Verlet skin: cutoff + skin must stay within half of every box (minimum image)
+    double halfmin = 1e300;
+    for (int si = 0; si < n; ++si) {
+      const double *H = systems[si].box0;
+      halfmin = std::min(halfmin, 0.5 * std::min(H[0], std::min(H[4], H[8])));
+    }
+    skin = std::max(0.0, std::min(set.skin, halfmin - set.cutoff));
+    double shell = 4.0 / 3.0 * M_PI * std::pow(set.cutoff + skin, 3) * rho_max;
+    cc_auto = std::max(32, (int)std::ceil((shell * 1.25 + 32.0) / 32.0) * 32);
+    cc = set.list_capacity > 0 ? ((set.list_capacity + 31) / 32) * 32 : cc_auto;
     // block maps
     std::vector<int> wbs, wba, tbs, tba;
     for (int si = 0; si < n; ++si) {
@@ -389,6 +407,10 @@ struct Engine : EngineBase {
     base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt);
     pperm.alloc(nt); off.alloc(nt); dEdd.alloc(nt);
     cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt); spos.alloc(nt);
+    pos_ref.alloc(nt); pos4.alloc(nt); ncand.alloc(nt); cand.alloc((size_t)nt * cc); nb_flag.alloc(1); nb_builds.alloc(1);
+    CK(cudaMemset(cell_count.p, 0, sizeof(int) * ncell));
+    CK(cudaMemset(nb_builds.p, 0, sizeof(long long)));
+    { int one = 1; CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice)); }
     rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(1); dany.alloc(1);
     alloc_rows();
     Q.alloc(rgrid); Phi.alloc(rgrid); Ginf.alloc(cgrid); C.alloc(cgrid);
@@ -529,15 +551,37 @@ struct Engine : EngineBase {
   // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
   // cell list, rows, influence function.
   void prepare(cudaStream_t st, pgm::Dev<T> &a, const double *boxes) {
-    CK(cudaMemsetAsync(cell_count.p, 0, sizeof(int) * ncell, st));
     CK(cudaMemsetAsync(dmax.p, 0, sizeof(int), st));
     pgm::k_box<T><<<grid1(nsys, 64), 64, 0, st>>>(a, boxes); check_launch();
     pgm::k_prep<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
     pgm::k_mol<T><<<grid1(nmol_total), 256, 0, st>>>(a); check_launch();
-    pgm::k_scan_cells<<<1, 1024, 0, st>>>(cell_count.p, cell_start.p, ncell); check_launch();
-    pgm::k_scatter<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
+    if (!a.idx) {  // the Verlet candidate list, rebuilt on the device when the flag is up
+      pgm::k_cell_assign<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
+      pgm::k_scan_cells<<<1, 1024, 0, st>>>(cell_count.p, cell_start.p, ncell, nb_flag.p); check_launch();
+      pgm::k_scatter<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
+      pgm::k_cand<T><<<nwblk, 256, 0, st>>>(a); check_launch();
+      pgm::k_nb_finish<<<std::max(1, std::min(1024, grid1(ncell))), 256, 0, st>>>(cell_count.p, ncell, nb_flag.p, nb_builds.p);
+      check_launch();
+      pgm::k_nb_lower<<<1, 1, 0, st>>>(nb_flag.p, nb_builds.p); check_launch();
+    }
     pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a); check_launch();
     pgm::k_influence<T><<<std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st>>>(a, cgrid); check_launch();
+  }
+
+  void set_list_capacity(int c) override {
+    int want = c > 0 ? ((c + 31) / 32) * 32 : cc_auto;
+    if (want != cc) {
+      cc = want;
+      cand.alloc((size_t)nt * cc);
+    }
+    int one = 1;
+    CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice));
+  }
+  int list_capacity() const override { return cc; }
+  long long list_rebuilds() override {
+    long long v = 0;
+    CK(cudaMemcpy(&v, nb_builds.p, sizeof(v), cudaMemcpyDeviceToHost));
+    return v;
   }
 
   // Reciprocal-space potential phi of the grid spread from `vin` (with charges if WITH_Q).
@@ -905,6 +949,29 @@ PgmStatus pgm_set_row_capacity(PgmHandle *h, int capacity) {
 }
 
 int pgm_row_capacity(const PgmHandle *h) { return h ? h->eng->capacity() : -1; }
+
+PgmStatus pgm_set_list_capacity(PgmHandle *h, int capacity) {
+  if (!h || capacity < 0) return fail(PGM_ERR_INVALID, "bad capacity");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->set_list_capacity(capacity);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+int pgm_list_capacity(const PgmHandle *h) { return h ? h->eng->list_capacity() : -1; }
+
+long long pgm_list_rebuilds(PgmHandle *h) {
+  if (!h) return -1;
+  try {
+    return h->eng->list_rebuilds();
+  } catch (CudaError &e) {
+    g_err = e.msg;
+    return -1;
+  }
+}
 
 int pgm_max_row_count(PgmHandle *h) {
   if (!h) return -1;

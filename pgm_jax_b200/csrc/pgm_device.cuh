@@ -56,7 +56,7 @@ struct BoxInfo {
   double H[9], Hinv[9], vol;
   double idiag[3];      // 1 / H_aa (minimum image by multiplication)
   double h[3];          // distances between lattice planes
-  int R[3];             // cell search range (-1: whole axis)
+  int R[3];             // cell search range of the candidate list (-1: whole axis)
   int changed;          // box differs from the previous step (influence function recomputed)
   int bad;              // not lower triangular or too small for the cutoff
 };

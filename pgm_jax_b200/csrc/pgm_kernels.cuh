@@ -23,6 +23,13 @@ struct Dev {
   int order;
   int induce, perm, lj, lj_lrc;
   double beta, cutoff, c_self, tol, peek;
+  double skin;            // Verlet skin of the candidate list
+  int cc;                 // candidate capacity per atom
+  int *nb_flag;           // candidate list must be rebuilt
+  long long *nb_builds;   // rebuild counter
+  int *cand, *ncand;      // candidates (N, cc) and counts
+  double4 *pos_ref;       // positions at the last rebuild
+  double4 *pos4;          // positions this step, .w = molecule
   int max_iter;
   const SysInfo *sys;
   BoxInfo *box;
@@ -85,10 +92,11 @@ __global__ void k_box(Dev<T> a, const double *boxes) {
     double c0 = Hi[0 * 3 + ax], c1 = Hi[1 * 3 + ax], c2v = Hi[2 * 3 + ax];
     B.h[ax] = 1.0 / sqrt(c0 * c0 + c1 * c1 + c2v * c2v);
     int nc = S.nc[ax];
-    int R = (int)ceil(a.cutoff * nc / B.h[ax] - 1e-12);
+    int R = (int)ceil((a.cutoff + a.skin) * nc / B.h[ax] - 1e-12);
     B.R[ax] = (2 * R + 1 >= nc) ? -1 : R;
   }
   B.changed = changed;
+  if (changed) atomicOr(a.nb_flag, 1);
   int bad = (fabs(H[1]) > 1e-12 * fabs(H[0])) || (fabs(H[2]) > 1e-12 * fabs(H[0])) || (fabs(H[5]) > 1e-12 * fabs(H[0])) ||
             !(H[0] > 0 && H[4] > 0 && H[8] > 0);
   double mc = 0.5 * fmin(H[0], fmin(H[4], H[8]));
@@ -143,6 +151,33 @@ __global__ void k_prep(Dev<T> a) {
     }
   }
   a.pperm[i] = p;
+  a.pos4[i] = make_double4(px, py, pz, (double)a.molid[i]);
+  // Verlet list: rebuild when an atom moved more than skin / 2 since the last build
+  double4 r0 = a.pos_ref[i];
+  double dx = px - r0.x, dy = py - r0.y, dz = pz - r0.z;
+  min_image(dx, dy, dz, B.H);
+  double h2 = 0.25 * a.skin * a.skin;
+  if (!(dx * dx + dy * dy + dz * dz <= h2)) atomicOr(a.nb_flag, 1);
+  (void)uc;
+}
+
+// Cell of every atom (only when the candidate list is rebuilt).
+template <typename T>
+__global__ void k_cell_assign(Dev<T> a) {
+  if (!*a.nb_flag) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  int s = a.sysid[i];
+  const SysInfo &S = a.sys[s];
+  const BoxInfo &B = a.box[s];
+  double4 p = a.pos4[i];
+  double uc[3];
+  for (int ax = 0; ax < 3; ++ax) {
+    double u = p.x * B.Hinv[0 * 3 + ax] + p.y * B.Hinv[1 * 3 + ax] + p.z * B.Hinv[2 * 3 + ax];
+    double fr = u - floor(u);
+    if (!(fr >= 0.0 && fr < 1.0)) fr = 0.0;
+    uc[ax] = fr;
+  }
   int c0 = max(0, min((int)(uc[0] * S.nc[0]), S.nc[0] - 1));
   int c1 = max(0, min((int)(uc[1] * S.nc[1]), S.nc[1] - 1));
   int c2v = max(0, min((int)(uc[2] * S.nc[2]), S.nc[2] - 1));
@@ -174,7 +209,8 @@ __global__ void k_mol(Dev<T> a) {
 }
 
 // Exclusive scan of the cell counts of all systems (one block).
-__global__ void k_scan_cells(const int *count, int *start, int n) {
+__global__ void k_scan_cells(const int *count, int *start, int n, const int *flag) {
+  if (!*flag) return;
   __shared__ int part[1024];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
@@ -200,11 +236,95 @@ __global__ void k_scan_cells(const int *count, int *start, int n) {
 
 template <typename T>
 __global__ void k_scatter(Dev<T> a) {
+  if (!*a.nb_flag) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   int t = a.cell_start[a.cell_of[i]] + a.slot_of[i];
   a.cell_atoms[t] = i;
-  a.spos[t] = make_double4(a.pos[3 * i], a.pos[3 * i + 1], a.pos[3 * i + 2], (double)a.molid[i]);
+  a.spos[t] = a.pos4[i];
+}
+
+// ------------------------------------------------------------------ Verlet candidate list
+// One warp per atom when the list is rebuilt: every atom of another molecule within
+// cutoff + skin, found through the cell list (cells within R along each axis), compacted by ballot;
+// the positions of the build are kept for the displacement test (the reference's neighbour list,
+// md/neighbors.py:169-304, rebuilt when an atom moved more than skin / 2).
+template <typename T>
+__global__ void __launch_bounds__(256) k_cand(Dev<T> a) {
+  if (!*a.nb_flag) return;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
+  const BoxInfo &B = a.box[s];
+  double H[9], id[3];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) H[k] = B.H[k];
+  id[0] = B.idiag[0]; id[1] = B.idiag[1]; id[2] = B.idiag[2];
+  double4 pi = a.pos4[i];
+  int mi = (int)pi.w;
+  double rl = a.cutoff + a.skin, rl2 = rl * rl;
+  int *out = a.cand + (size_t)i * a.cc;
+  int count = 0;
+  int cell = a.cell_of[i] - S.cell0;
+  int n0 = S.nc[0], n1 = S.nc[1], n2 = S.nc[2];
+  int ci2 = cell % n2, ci1 = (cell / n2) % n1, ci0 = cell / (n1 * n2);
+  int R0 = B.R[0], R1 = B.R[1], R2 = B.R[2];
+  int lo0 = R0 < 0 ? 0 : -R0, hi0 = R0 < 0 ? n0 - 1 : R0;
+  int lo1 = R1 < 0 ? 0 : -R1, hi1 = R1 < 0 ? n1 - 1 : R1;
+  for (int d0 = lo0; d0 <= hi0; ++d0) {
+    int c0 = R0 < 0 ? d0 : ((ci0 + d0) % n0 + n0) % n0;
+    for (int d1 = lo1; d1 <= hi1; ++d1) {
+      int c1 = R1 < 0 ? d1 : ((ci1 + d1) % n1 + n1) % n1;
+      int rowc = S.cell0 + (c0 * n1 + c1) * n2;
+      int segs[2][2];
+      int nseg = 0;
+      if (R2 < 0) {
+        segs[0][0] = 0; segs[0][1] = n2 - 1; nseg = 1;
+      } else {
+        int lo = ci2 - R2, hi = ci2 + R2;
+        if (lo < 0) { segs[0][0] = lo + n2; segs[0][1] = n2 - 1; segs[1][0] = 0; segs[1][1] = hi; nseg = 2; }
+        else if (hi >= n2) { segs[0][0] = lo; segs[0][1] = n2 - 1; segs[1][0] = 0; segs[1][1] = hi - n2; nseg = 2; }
+        else { segs[0][0] = lo; segs[0][1] = hi; nseg = 1; }
+      }
+      for (int g = 0; g < nseg; ++g) {
+        int a0 = a.cell_start[rowc + segs[g][0]], a1 = a.cell_start[rowc + segs[g][1] + 1];
+        for (int t0 = a0; t0 < a1; t0 += 32) {
+          int t = t0 + lane;
+          bool keep = false;
+          if (t < a1) {
+            double4 pj = a.spos[t];
+            if ((int)pj.w != mi) {
+              double x = pi.x - pj.x, y = pi.y - pj.y, z = pi.z - pj.z;
+              min_image_fast(x, y, z, H, id);
+              keep = x * x + y * y + z * z < rl2;
+            }
+          }
+          unsigned bal = __ballot_sync(0xffffffffu, keep);
+          if (keep) {
+            int slot = count + __popc(bal & ((1u << lane) - 1u));
+            if (slot < a.cc) out[slot] = a.cell_atoms[t];
+          }
+          count += __popc(bal);
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    a.ncand[i] = count;
+    a.pos_ref[i] = pi;
+    if (count > a.cc) atomicOr(&a.status[s], 0x10u);
+  }
+}
+
+// End of a rebuild: clear the cell counts for the next one, count it, lower the flag.
+__global__ void k_nb_finish(int *cell_count, int ncell, int *flag, long long *builds) {
+  if (!*flag) return;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) cell_count[c] = 0;
+}
+__global__ void k_nb_lower(int *flag, long long *builds) {
+  if (*flag) { *flag = 0; *builds += 1; }
 }
 
 // ------------------------------------------------------------------ pair rows
@@ -317,48 +437,22 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
       }
       rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
     }
-  } else {  // cell list: cells within R of the atom's cell along each axis
-    int cell = a.cell_of[i] - S.cell0;
-    int n0 = S.nc[0], n1 = S.nc[1], n2 = S.nc[2];
-    int ci2 = cell % n2, ci1 = (cell / n2) % n1, ci0 = cell / (n1 * n2);
-    int R0 = B.R[0], R1 = B.R[1], R2 = B.R[2];
-    int lo0 = R0 < 0 ? 0 : -R0, hi0 = R0 < 0 ? n0 - 1 : R0;
-    int lo1 = R1 < 0 ? 0 : -R1, hi1 = R1 < 0 ? n1 - 1 : R1;
-    for (int d0 = lo0; d0 <= hi0; ++d0) {
-      int c0 = R0 < 0 ? d0 : ((ci0 + d0) % n0 + n0) % n0;
-      for (int d1 = lo1; d1 <= hi1; ++d1) {
-        int c1 = R1 < 0 ? d1 : ((ci1 + d1) % n1 + n1) % n1;
-        int rowc = S.cell0 + (c0 * n1 + c1) * n2;
-        int segs[2][2];
-        int nseg = 0;
-        if (R2 < 0) {
-          segs[0][0] = 0; segs[0][1] = n2 - 1; nseg = 1;
-        } else {
-          int lo = ci2 - R2, hi = ci2 + R2;
-          if (lo < 0) { segs[0][0] = lo + n2; segs[0][1] = n2 - 1; segs[1][0] = 0; segs[1][1] = hi; nseg = 2; }
-          else if (hi >= n2) { segs[0][0] = lo; segs[0][1] = n2 - 1; segs[1][0] = 0; segs[1][1] = hi - n2; nseg = 2; }
-          else { segs[0][0] = lo; segs[0][1] = hi; nseg = 1; }
-        }
-        for (int g = 0; g < nseg; ++g) {
-          int a0 = a.cell_start[rowc + segs[g][0]], a1 = a.cell_start[rowc + segs[g][1] + 1];
-          for (int t0 = a0; t0 < a1; t0 += 32) {
-            int t = t0 + lane;
-            bool keep = false;
-            int j = 0;
-            double x = 0, y = 0, z = 0;
-            if (t < a1) {
-              double4 pj = a.spos[t];
-              if ((int)pj.w != mi) {
-                x = pix - pj.x; y = piy - pj.y; z = piz - pj.z;
-                min_image_fast(x, y, z, H, id);
-                keep = x * x + y * y + z * z < rc2;
-                if (keep) j = a.cell_atoms[t];
-              }
-            }
-            rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
-          }
-        }
+  } else {  // the engine's Verlet candidates (within cutoff + skin at the last rebuild)
+    const int *row = a.cand + (size_t)i * a.cc;
+    int nc = min(a.ncand[i], a.cc);
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      int c = c0 + lane;
+      bool keep = false;
+      int j = 0;
+      double x = 0, y = 0, z = 0;
+      if (c < nc) {
+        j = row[c];
+        double4 pj = a.pos4[j];
+        x = pix - pj.x; y = piy - pj.y; z = piz - pj.z;
+        min_image_fast(x, y, z, H, id);
+        keep = x * x + y * y + z * z < rc2;
       }
+      rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
     }
   }
   while (nst > 0) rows_flush<T>(a, st, warp, lane, min(nst, 32), nst, written, base, Ri2);

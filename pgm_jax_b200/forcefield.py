@@ -154,7 +154,7 @@ class PGMForceField:
             ELEC_LEVELS[settings.elec], int(settings.vdw == "lj"), int(settings.lj_lrc),
             int(settings.precision == "double"), float(settings.cutoff), float(settings.ewald_beta), int(settings.pme_order),
             float(settings.dipole_tol), int(settings.max_iter), PREDICTORS[settings.predictor], int(settings.fused),
-            int(settings.norm_refresh), float(settings.peek), int(row_capacity or 0),
+            int(settings.norm_refresh), float(settings.peek), int(row_capacity or 0), float(settings.skin), 0,
         )
         descs = (_lib.PgmSystemDesc * self.nsys)()
         self._keep = []
@@ -229,6 +229,18 @@ class PGMForceField:
         self.set_capacity(int(np.ceil((c * (1.0 + 0.5 * (factor - 1.0)) + 8) / 8.0) * 8))
         return self.capacity
 
+    @property
+    def list_capacity(self) -> int:
+        """Candidates kept per atom in the engine's Verlet list."""
+        return int(self._lib.pgm_list_capacity(self._h))
+
+    def set_list_capacity(self, c: int) -> None:
+        _lib.check(self._lib.pgm_set_list_capacity(self._h, int(c)))
+
+    def list_rebuilds(self) -> int:
+        """How many times the Verlet candidate list has been rebuilt."""
+        return int(self._lib.pgm_list_rebuilds(self._h))
+
     def grow_rows(self, old: int) -> None:
         """Widen the rows by at least 8 after an overflow at capacity `old` (forcefield.py:1286)."""
         self.set_capacity(max(self.capacity, int(old) + 8))
@@ -293,7 +305,7 @@ class PGMForceField:
         out = _lib.PgmOutputs(E.data_ptr(), F.data_ptr(), V.data_ptr(), I.data_ptr(), R.data_ptr(), Sst.data_ptr())
         _lib.check(self._lib.pgm_compute(self._h, self._stream(), _ptr(x), _ptr(b), _ptr(it), w, C.byref(di), C.byref(out)))
         energy = {"elec": E[:, 0], "vdw": E[:, 1], "total": E[:, 2]}
-        return Result(energy, F, ind, I, R, (Sst & _lib.STATUS_ROW_OVERFLOW) != 0, V, Sst)
+        return Result(energy, F, ind, I, R, (Sst & (_lib.STATUS_ROW_OVERFLOW | _lib.STATUS_LIST_OVERFLOW)) != 0, V, Sst)
 
     def compute_into(self, pos: torch.Tensor, boxes: torch.Tensor, ind: InductionState, forces: torch.Tensor) -> Result:
         """compute() into persistent buffers, with no allocation (for CUDA-graph capture).
@@ -308,7 +320,7 @@ class PGMForceField:
         _lib.check(self._lib.pgm_compute(self._h, self._stream(), _ptr(pos), _ptr(boxes), None, 0, C.byref(di), C.byref(out)))
         E = self._energy
         return Result({"elec": E[:, 0], "vdw": E[:, 1], "total": E[:, 2]}, forces, ind, self._iters, self._resid,
-                      (self._status & _lib.STATUS_ROW_OVERFLOW) != 0, self._virial, self._status)
+                      (self._status & (_lib.STATUS_ROW_OVERFLOW | _lib.STATUS_LIST_OVERFLOW)) != 0, self._virial, self._status)
 
     def energy(self, pos, H, idx=None, ind: InductionState | None = None):
         """Energy only, dipoles solved from ind.mu, no history push (forcefield.py:2562).
