@@ -251,6 +251,8 @@ struct Engine : EngineBase {
       S.atom0 = atom0; S.natom = d.n_atoms; S.mol0 = mol0; S.nmol = d.n_mol;
       for (int a = 0; a < 3; ++a) S.K[a] = d.pme_grid[a];
       S.K3h = S.K[2] / 2 + 1;
+      rg = (rg + 63) / 64 * 64;  // every system's grids start 256-byte aligned (16-byte vector atomics)
+      cg = (cg + 63) / 64 * 64;
       S.rgrid0 = rg; S.cgrid0 = cg;
       rg += (long long)S.K[0] * S.K[1] * S.K[2];
       cg += (long long)S.K[0] * S.K[1] * S.K3h;
