@@ -168,8 +168,11 @@ long long pgm_launches_per_iteration(const PgmHandle *h);
 
 /* Average duration [ms] of one launch of a kernel of the last pgm_compute, re-run `reps` times on
  * `stream` between CUDA events on the state that step left: 0 the CG matvec (row field + PME
- * gather), 1 the PME spread, 2 the five FFT/convolution passes, 3 the energy/force pass, 4 the row
- * build.  The last pgm_compute's position array must still be valid. */
+ * gather in one kernel), 1 the PME spread, 2 the five FFT/convolution passes, 3 the energy/force
+ * pass, 4 the row build, 5 the first FFT pass alone, 6 a spread followed by the first FFT pass,
+ * 7 the row field alone, 8 the PME gather + operator assembly alone, 9 a whole operator sweep as
+ * the solver runs it (spread, row field beside the FFT chain, gather).  The last pgm_compute's
+ * position array must still be valid. */
 PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, double *ms_per_launch);
 
 /* In-cutoff pairs (both rows of every pair) of the last step's row build. */

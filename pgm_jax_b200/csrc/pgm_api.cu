@@ -160,7 +160,7 @@ struct Engine : EngineBase {
   DBuf<T> q, radius, alpha, ialpha, rminh, seps;
   DBuf<double> mass, cov_c, cov_c_flat, bmod;
   DBuf<int4> base;
-  DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D;
+  DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D, Fv;
   DBuf<double4> pperm, off, dEdd;
   DBuf<int> cell_of, slot_of, cell_count, cell_start, cell_atoms;
   DBuf<double4> spos, pos_ref, pos4;
@@ -173,12 +173,16 @@ struct Engine : EngineBase {
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
   int *h_any = nullptr;
   const double *last_pos = nullptr;
-  cudaStream_t side = nullptr;
+  cudaStream_t side = nullptr, aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   long long per_iter = 0;
 
   ~Engine() {
     if (h_any) cudaFreeHost(h_any);
     if (side) cudaStreamDestroy(side);
+    if (aux) cudaStreamDestroy(aux);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 
   pgm::Dev<T> dev(const double *pos, const int32_t *idx, int idx_width, double *forces, unsigned *status) {
@@ -211,7 +215,7 @@ struct Engine : EngineBase {
     a.rn = rn.p; a.rnsp = rnsp.p; a.rk = rk.p;
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
     a.max_count = dmax.p;
-    a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p;
+    a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p; a.F = Fv.p;
     a.Q = Q.p; a.Phi = Phi.p; a.Ginf = Ginf.p; a.C = C.p; a.tw = tw.p; a.bmod = bmod.p;
     a.forces = forces; a.dEdd = dEdd.p;
     return a;
@@ -406,7 +410,7 @@ struct Engine : EngineBase {
     q.upload(h_q); radius.upload(h_rad); alpha.upload(h_al); ialpha.upload(h_ial); rminh.upload(h_rh); seps.upload(h_se);
     mass.upload(h_mass); cov_c.upload(h_covc); cov_c_flat.upload(h_covc_flat); bmod.upload(h_bmod);
     tw.upload(h_tw);
-    base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt);
+    base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt); Fv.alloc(nt);
     pperm.alloc(nt); off.alloc(nt); dEdd.alloc(nt);
     cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt); spos.alloc(nt);
     pos_ref.alloc(nt); pos4.alloc(nt); ncand.alloc(nt); cand.alloc((size_t)nt * cc); nb_flag.alloc(1); nb_builds.alloc(1);
@@ -419,6 +423,9 @@ struct Engine : EngineBase {
     CK(cudaMemset(Q.p, 0, sizeof(T) * rgrid));
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
     CK(cudaMallocHost(&h_any, sizeof(int)));
+    CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     set_smem();
   }
 
@@ -509,7 +516,23 @@ struct Engine : EngineBase {
       else if (which == 2) {
         fft_chain(st, a, 0, false);
       } else if (which == 3) pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, nullptr);
-      else pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
+      else if (which == 4) pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
+      else if (which == 5) {
+        for (auto &g : gx)
+          with_fft_len(g->K, [&](auto Lc) {
+            pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
+          });
+      } else if (which == 6) {
+        pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
+        for (auto &g : gx)
+          with_fft_len(g->K, [&](auto Lc) {
+            pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
+          });
+      } else if (which == 7) pgm::k_rowfield<T, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, Fv.p);
+      else if (which == 8) pgm::k_rowmat<T, P, false, 1, 0, false><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
+      else {  // 9: a whole operator sweep with the row/PME overlap
+        sweep<false, false, 0, 1>(st, a, Pv.p, AP.p);
+      }
     };
     long long l0 = launches;
     one();  // warm-up
@@ -593,10 +616,24 @@ struct Engine : EngineBase {
     fft_chain(st, a, ACT, ENERGY);
   }
 
+  // One field sweep of the dipoles vin (charges with WITH_Q): the spread (after the CG direction
+  // update with UPDATE_P), then the row field on a second stream beside the FFT chain, joined by
+  // the PME gather that assembles MODE 0 (field) or 1 (operator, with p.Ap) into out.
+  template <bool WITH_Q, bool UPDATE_P, int ACT, int MODE>
+  void sweep(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin, pgm::v4<T> *out) {
+    pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
+    CK(cudaEventRecord(ev_fork, st));
+    CK(cudaStreamWaitEvent(aux, ev_fork, 0));
+    pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, aux>>>(a, vin, Fv.p); check_launch();
+    CK(cudaEventRecord(ev_join, aux));
+    fft_chain(st, a, ACT, false);
+    CK(cudaStreamWaitEvent(st, ev_join, 0));
+    pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false><<<nwblk, 256, 0, st>>>(a, vin, out); check_launch();
+  }
+
   // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check.
   void iteration(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
-    pme<false, true, 1, false>(st, a, Pv.p);
-    pgm::k_rowmat<T, P, false, 1, 1><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p); check_launch();
+    sweep<false, true, 1, 1>(st, a, Pv.p, AP.p);
     pgm::k_cg_update<T><<<ntblk, 256, 0, st>>>(a); check_launch();
     pgm::k_cg_check<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, cond, use_cond); check_launch();
   }
@@ -624,11 +661,9 @@ struct Engine : EngineBase {
       pgm::k_start1<T><<<grid1(nt), 256, 0, st>>>(a, ind->hist, K, cc[0], cc[1], cc[2], cc[3]);
       check_launch();
     }
-    pme<true, false, 0, false>(st, a, D.p);
-    pgm::k_rowmat<T, P, true, 0, 0><<<nwblk, 256, 0, st>>>(a, D.p, Bv.p); check_launch();
+    sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
     pgm::k_start2<T><<<ntblk, 256, 0, st>>>(a); check_launch();
-    pme<false, false, 2, false>(st, a, X.p);
-    pgm::k_rowmat<T, P, false, 1, 2><<<nwblk, 256, 0, st>>>(a, X.p, AP.p); check_launch();
+    sweep<false, false, 2, 1>(st, a, X.p, AP.p);
     pgm::k_start3<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
     pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
     pgm::k_cg_begin<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p); check_launch();
@@ -737,13 +772,8 @@ struct Engine : EngineBase {
     pgm::Dev<T> a = dev(pos, nullptr, 0, forces_tmp.p, d_status.p);
     prepare(st, a, box);
     pgm::k_load_vec<T><<<grid1(nt), 256, 0, st>>>(a, d, D.p); check_launch();
-    if (with_q) {
-      pme<true, false, 0, false>(st, a, D.p);
-      pgm::k_rowmat<T, P, true, 0, 0><<<nwblk, 256, 0, st>>>(a, D.p, Bv.p); check_launch();
-    } else {
-      pme<false, false, 0, false>(st, a, D.p);
-      pgm::k_rowmat<T, P, false, 0, 0><<<nwblk, 256, 0, st>>>(a, D.p, Bv.p); check_launch();
-    }
+    if (with_q) sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
+    else sweep<false, false, 0, 0>(st, a, D.p, Bv.p);
     pgm::k_store_vec<T><<<grid1(nt), 256, 0, st>>>(a, Bv.p, out); check_launch();
   }
 };
@@ -991,7 +1021,7 @@ long long pgm_last_launch_count(const PgmHandle *h) { return h ? h->eng->launche
 long long pgm_launches_per_iteration(const PgmHandle *h) { return h ? h->eng->launches_per_iteration() : -1; }
 
 PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, double *ms_per_launch) {
-  if (!h || !ms_per_launch || reps <= 0 || which < 0 || which > 4) return fail(PGM_ERR_INVALID, "bad argument");
+  if (!h || !ms_per_launch || reps <= 0 || which < 0 || which > 9) return fail(PGM_ERR_INVALID, "bad argument");
   if (!static_cast<bool>(h->eng)) return fail(PGM_ERR_INVALID, "no engine");
   try {
     CK(cudaSetDevice(h->device));

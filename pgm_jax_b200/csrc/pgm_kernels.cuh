@@ -59,6 +59,7 @@ struct Dev {
   int *max_count;
   // vectors
   v4<T> *X, *R, *Z, *P, *AP, *B, *D;
+  v4<T> *F;  // row field of a sweep (computed concurrently with the PME chain)
   // grids
   T *Q, *Phi, *Ginf;
   c2<T> *C;
@@ -927,7 +928,58 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
 // (pme.py:378-388), then by MODE:
 //   0 FIELD  out = -(s - c_self d)                       (forcefield.py:1428-1433)
 //   1 OPER   out = d / alpha + s - c_self d, and p.Ap    (forcefield.py:1694-1712, 1806-1807)
-template <typename T, int P, bool WITH_Q, int MODE, int ACT>
+// The row part alone: F_i = sum_k de_ik/dd_i, one warp per atom (runs beside the PME chain).
+template <typename T, bool WITH_Q, int ACT>
+__global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ F) {
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
+  if (ACT == 1 && !a.cg[s].active) return;
+  if (ACT == 2 && !a.cg[s].sweep2) return;
+  int n = min(a.rn[i], a.mc);
+  size_t base = (size_t)i * a.mc;
+  T f0 = 0, f1 = 0, f2 = 0;
+  auto pair = [&](int k, T x, T y, T z, T g1, T g2) {
+    v4<T> dk = D[k];
+    T dkx = dk.x * x + dk.y * y + dk.z * z;
+    T c = -g2 * dkx;
+    if (WITH_Q) c -= a.q[k] * g1;
+    f0 += c * x + g1 * dk.x;
+    f1 += c * y + g1 * dk.y;
+    f2 += c * z + g1 * dk.z;
+  };
+  if constexpr (sizeof(T) == 4) {
+    const int4 *k4 = reinterpret_cast<const int4 *>(a.rk + base);
+    const float4 *x4 = reinterpret_cast<const float4 *>(a.rx + base), *y4 = reinterpret_cast<const float4 *>(a.ry + base),
+                 *z4 = reinterpret_cast<const float4 *>(a.rz + base), *p4 = reinterpret_cast<const float4 *>(a.rg1 + base),
+                 *q4 = reinterpret_cast<const float4 *>(a.rg2 + base);
+    for (int t4 = lane; 4 * t4 < n; t4 += 32) {
+      int4 kk = k4[t4];
+      float4 xx = x4[t4], yy = y4[t4], zz = z4[t4], g1 = p4[t4], g2 = q4[t4];
+      int t = 4 * t4;
+      pair(kk.x, xx.x, yy.x, zz.x, g1.x, g2.x);
+      if (t + 1 < n) pair(kk.y, xx.y, yy.y, zz.y, g1.y, g2.y);
+      if (t + 2 < n) pair(kk.z, xx.z, yy.z, zz.z, g1.z, g2.z);
+      if (t + 3 < n) pair(kk.w, xx.w, yy.w, zz.w, g1.w, g2.w);
+    }
+  } else {
+    for (int t = lane; t < n; t += 32) {
+      size_t o = base + t;
+      pair(a.rk[o], a.rx[o], a.ry[o], a.rz[o], a.rg1[o], a.rg2[o]);
+    }
+  }
+  f0 = warp_sum<T>(f0); f1 = warp_sum<T>(f1); f2 = warp_sum<T>(f2);
+  if (lane == 0) {
+    v4<T> o;
+    o.x = f0; o.y = f1; o.z = f2; o.w = T(0);
+    F[i] = o;
+  }
+}
+
+// ROWS: the row sum is computed here; otherwise it is read from a.F (k_rowfield).
+template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true>
 __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
   __shared__ double red[WARPS_PER_BLOCK];
@@ -940,7 +992,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
   if (ACT == 2 && !a.cg[s].sweep2) return;
   double dotv = 0.0;
   if (valid) {
-    int n = min(a.rn[i], a.mc);
+    int n = ROWS ? min(a.rn[i], a.mc) : 0;
     size_t base = (size_t)i * a.mc;
     T f0 = 0, f1 = 0, f2 = 0;
     auto pair = [&](int k, T x, T y, T z, T g1, T g2) {
@@ -998,9 +1050,10 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
       g1 += ph * t1 * u2 * t3;
       g2 += ph * t1 * t2 * u3;
     }
-    f0 = warp_sum<T>(f0); f1 = warp_sum<T>(f1); f2 = warp_sum<T>(f2);
+    if (ROWS) { f0 = warp_sum<T>(f0); f1 = warp_sum<T>(f1); f2 = warp_sum<T>(f2); }
     g0 = warp_sum<T>(g0); g1 = warp_sum<T>(g1); g2 = warp_sum<T>(g2);
     if (lane == 0) {
+      if (!ROWS) { v4<T> fr = a.F[i]; f0 = fr.x; f1 = fr.y; f2 = fr.z; }
       // dU/dd_b = sum_a g_a Hinv[b][a] K_a
       T es[9];
 #pragma unroll
