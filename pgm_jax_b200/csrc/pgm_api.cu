@@ -173,16 +173,20 @@ struct Engine : EngineBase {
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
   int *h_any = nullptr;
   const double *last_pos = nullptr;
-  cudaStream_t side = nullptr, aux = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t side = nullptr, aux = nullptr, aux_b = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork_b = nullptr, ev_join_b = nullptr;
+  bool in_body = false;  // enqueueing the CG while-loop body (its own capture sequence)
   long long per_iter = 0;
 
   ~Engine() {
     if (h_any) cudaFreeHost(h_any);
     if (side) cudaStreamDestroy(side);
     if (aux) cudaStreamDestroy(aux);
+    if (aux_b) cudaStreamDestroy(aux_b);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_fork_b) cudaEventDestroy(ev_fork_b);
+    if (ev_join_b) cudaEventDestroy(ev_join_b);
   }
 
   pgm::Dev<T> dev(const double *pos, const int32_t *idx, int idx_width, double *forces, unsigned *status) {
@@ -424,8 +428,11 @@ struct Engine : EngineBase {
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
     CK(cudaMallocHost(&h_any, sizeof(int)));
     CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&aux_b, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_fork_b, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join_b, cudaEventDisableTiming));
     set_smem();
   }
 
@@ -621,13 +628,16 @@ struct Engine : EngineBase {
   // the PME gather that assembles MODE 0 (field) or 1 (operator, with p.Ap) into out.
   template <bool WITH_Q, bool UPDATE_P, int ACT, int MODE>
   void sweep(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin, pgm::v4<T> *out) {
+    // the loop body is captured as a sequence of its own: it forks to its own stream
+    cudaStream_t ax = in_body ? aux_b : aux;
+    cudaEvent_t ef = in_body ? ev_fork_b : ev_fork, ej = in_body ? ev_join_b : ev_join;
     pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
-    CK(cudaEventRecord(ev_fork, st));
-    CK(cudaStreamWaitEvent(aux, ev_fork, 0));
-    pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, aux>>>(a, vin, Fv.p); check_launch();
-    CK(cudaEventRecord(ev_join, aux));
+    CK(cudaEventRecord(ef, st));
+    CK(cudaStreamWaitEvent(ax, ef, 0));
+    pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, ax>>>(a, vin, Fv.p); check_launch();
+    CK(cudaEventRecord(ej, ax));
     fft_chain(st, a, ACT, false);
-    CK(cudaStreamWaitEvent(st, ev_join, 0));
+    CK(cudaStreamWaitEvent(st, ej, 0));
     pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false><<<nwblk, 256, 0, st>>>(a, vin, out); check_launch();
   }
 
@@ -691,7 +701,16 @@ struct Engine : EngineBase {
       if (!side) CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
       CK(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
       long long l0 = launches;
-      iteration(side, a, cond, 1);
+      in_body = true;
+      try {
+        iteration(side, a, cond, 1);
+      } catch (...) {
+        in_body = false;
+        cudaGraph_t junk;
+        cudaStreamEndCapture(side, &junk);
+        throw;
+      }
+      in_body = false;
       per_iter = launches - l0;
       CK(cudaStreamEndCapture(side, &body));
     } else {

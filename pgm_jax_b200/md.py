@@ -168,11 +168,15 @@ class RigidMD:
         self.stream.synchronize()
         st = self._stream()
         _lib.check(self._lib.pgm_graph_begin(st))
+        ex = C.c_void_p()
         try:
             self._step_enqueue()
-        finally:
-            ex = C.c_void_p()
-            _lib.check(self._lib.pgm_graph_end(st, C.byref(ex)))
+        except Exception:
+            self._lib.pgm_graph_end(st, C.byref(ex))  # close the capture; the error is the one raised
+            if ex.value:
+                self._lib.pgm_graph_destroy(ex)
+            raise
+        _lib.check(self._lib.pgm_graph_end(st, C.byref(ex)))
         self._graph = ex
         self.launches_outside_loop = self.ff.last_launch_count() + 2 - int(self._lib.pgm_launches_per_iteration(self.ff._h))
         self.launches_per_iteration = int(self._lib.pgm_launches_per_iteration(self.ff._h))
