@@ -178,6 +178,27 @@ PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, do
 /* In-cutoff pairs (both rows of every pair) of the last step's row build. */
 long long pgm_row_pairs(PgmHandle *h);
 
+/* ------------------------------------------------------------------ allocation-free field
+ * pgm_field_static has no counterpart in the reference.  It is for callers that must not allocate
+ * device memory: a jax.ffi custom call inside XLA (XLA has reserved most of the GPU memory for its
+ * own allocator and passes the call all the buffers it may use) or code recording a CUDA graph.  It
+ * computes the same total field -dU/dd (N, 3) [e/nm^2] as pgm_field, in FP64, for one system, with
+ * every intermediate in one static device array of the library (1 MB, held by each GPU that loads
+ * the library until exit) and no handle: no cudaMalloc, cudaFree or allocating library call.
+ * All pointers are device pointers: pos (N, 3), box (3, 3), q and radius (N), d (N, 3), field (N, 3).
+ * Limits: N <= PGM_STATIC_MAX_ATOMS, each mesh size <= PGM_STATIC_MAX_K with K1 K2 K3 <=
+ * PGM_STATIC_MAX_GRID, order 4, 6 or 8; larger inputs return PGM_ERR_UNSUPPORTED with a message in
+ * pgm_static_last_error().  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams or threads at the same time) race on it. */
+#define PGM_STATIC_MAX_ATOMS 4096
+#define PGM_STATIC_MAX_K 64
+#define PGM_STATIC_MAX_GRID 32768
+PgmStatus pgm_field_static(void *stream, int n_atoms, const double *pos, const double *box, const double *q,
+                           const double *radius, double cutoff, double ewald_beta, const int *pme_grid, int pme_order,
+                           int with_charges, const double *d, double *field);
+const char *pgm_static_last_error(void);
+
 /* ------------------------------------------------------------------ rigid-molecule MD driver
  * The caller of the force field in the MD benchmarks: the rigid-body step of pgm_jax/md/
  * integrate.py:743-761 (B A O A B) with md/rigid.py bodies and the Langevin O-step of

@@ -21,7 +21,7 @@ EXPORTS = (
     "pgm_set_row_capacity", "pgm_row_capacity", "pgm_set_list_capacity", "pgm_list_capacity", "pgm_list_rebuilds", "pgm_max_row_count", "pgm_num_atoms", "pgm_num_systems",
     "pgm_last_error", "pgm_last_launch_count", "pgm_launches_per_iteration", "pgm_profile_kernel", "pgm_row_pairs", "pgm_rigid_create", "pgm_rigid_destroy",
     "pgm_rigid_begin_step", "pgm_rigid_set_step", "pgm_rigid_end_step", "pgm_rigid_kinetic", "pgm_rigid_last_error", "pgm_graph_begin",
-    "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy",
+    "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
 )
 
 STATUS_ROW_OVERFLOW = 0x1
@@ -106,6 +106,9 @@ def load(path: str | None = None):
     lib.pgm_rigid_end_step.argtypes = [H, vp, C.c_double, vp, vp, vp, vp]
     lib.pgm_rigid_kinetic.argtypes = [H, vp, vp, vp, vp]
     lib.pgm_rigid_last_error.restype = C.c_char_p
+    lib.pgm_field_static.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_double, C.c_double, vp, C.c_int, C.c_int, vp, vp]
+    lib.pgm_field_static.restype = C.c_int
+    lib.pgm_static_last_error.restype = C.c_char_p
     lib.pgm_graph_begin.argtypes = [vp]
     lib.pgm_graph_end.argtypes = [vp, C.POINTER(vp)]
     lib.pgm_graph_launch.argtypes = [vp, vp]
