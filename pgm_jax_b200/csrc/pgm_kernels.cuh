@@ -843,8 +843,8 @@ __global__ void __launch_bounds__(256) k_spread_x(Dev<T> a, const v4<T> *__restr
     tot += cnt[nb];
   }
   {
-    for (int fl = threadIdx.x; fl < tot; fl += blockDim.x) {
-      int nb = 0, ff = fl;
+    for (int f = threadIdx.x; f < tot; f += blockDim.x) {
+      int nb = 0, ff = f;
       while (ff >= cnt[nb]) { ff -= cnt[nb]; ++nb; }
       int i = a.bin_atoms[r0[nb] + ff];
       int4 b = a.base[i];
