@@ -165,10 +165,6 @@ struct Engine : EngineBase {
   DBuf<int> cell_of, slot_of, cell_count, cell_start, cell_atoms;
   DBuf<double4> spos, pos_ref, pos4;
   DBuf<int> cand, ncand, nb_flag;
-  DBuf<int> bin_of, bin_slot, bin_count, bin_start, bin_atoms, d_one;
-  int nbin = 0;
-  bool binned = false;                             // all meshes take the binned spread
-  std::vector<std::unique_ptr<FftGroup>> gbx;      // binned spread + k3 pass launches
   DBuf<long long> nb_builds;
   DBuf<int> rn, rnsp, rk, dmax, dany;
   DBuf<T> rx, ry, rz, rg0, rg1, rg2, rg3;
@@ -220,8 +216,6 @@ struct Engine : EngineBase {
     a.spos = spos.p;
     a.skin = skin; a.cc = cc; a.nb_flag = nb_flag.p; a.nb_builds = nb_builds.p; a.cand = cand.p; a.ncand = ncand.p;
     a.pos_ref = pos_ref.p; a.pos4 = pos4.p;
-    a.bin_of = bin_of.p; a.bin_slot = bin_slot.p; a.bin_count = bin_count.p; a.bin_start = bin_start.p;
-    a.bin_atoms = bin_atoms.p;
     a.idx = idx; a.idx_width = idx_width;
     a.rn = rn.p; a.rnsp = rnsp.p; a.rk = rk.p;
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
@@ -298,8 +292,6 @@ struct Engine : EngineBase {
       }
       S.cell0 = cell0;
       cell0 += S.nc[0] * S.nc[1] * S.nc[2];
-      S.nb1 = S.K[0] / 4; S.nb2 = S.K[1] / 4; S.bin0 = nbin;
-      nbin += S.nb1 * S.nb2 + 1;
       rho_max = std::max(rho_max, d.n_atoms / vol);
       // atoms
       double sq = 0, sq2 = 0, M[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -408,27 +400,6 @@ struct Engine : EngineBase {
     groups(2, gx);
     groups(1, gy);
     groups(0, gz);
-    binned = true;
-    for (auto &S : hsys)
-      if (S.K[0] % 4 || S.K[1] % 4 || S.K[0] < 12 || S.K[1] < 12) binned = false;
-    if (binned) {
-      for (auto &g0 : gx) {  // same K3 groups as the k3 pass, tiles = 4 x 4 blocks of lines
-        std::unique_ptr<FftGroup> g(new FftGroup());
-        g->K = g0->K;
-        std::vector<int> gs, gt{0};
-        for (int si = 0; si < n; ++si) {
-          if (hsys[si].K[2] != g0->K) continue;
-          gs.push_back(si);
-          gt.push_back(gt.back() + hsys[si].nb1 * hsys[si].nb2);
-        }
-        g->ng = (int)gs.size();
-        g->ntiles = gt.back();
-        g->smem = (size_t)2 * pgm::FFT_PAIRS * g0->K * sizeof(pgm::c2<T>);
-        g->sys.upload(gs);
-        g->tile0.upload(gt);
-        gbx.push_back(std::move(g));
-      }
-    }
     d_sys.upload(hsys);
     d_box.alloc(n);
     CK(cudaMemset(d_box.p, 0, sizeof(pgm::BoxInfo) * n));
@@ -447,9 +418,7 @@ struct Engine : EngineBase {
     base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt); Fv.alloc(nt);
     pperm.alloc(nt); off.alloc(nt); dEdd.alloc(nt);
     cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt); spos.alloc(nt);
-    pos_ref.alloc(nt); pos4.alloc(nt);
-    bin_of.alloc(nt); bin_slot.alloc(nt); bin_count.alloc(nbin); bin_start.alloc(nbin + 1); bin_atoms.alloc(nt);
-    d_one.upload(std::vector<int>{1}); ncand.alloc(nt); cand.alloc((size_t)nt * cc); nb_flag.alloc(1); nb_builds.alloc(1);
+    pos_ref.alloc(nt); pos4.alloc(nt); ncand.alloc(nt); cand.alloc((size_t)nt * cc); nb_flag.alloc(1); nb_builds.alloc(1);
     CK(cudaMemset(cell_count.p, 0, sizeof(int) * ncell));
     CK(cudaMemset(nb_builds.p, 0, sizeof(long long)));
     { int one = 1; CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice)); }
@@ -496,17 +465,10 @@ struct Engine : EngineBase {
         smem_attr(pgm::k_fft_z_conv<T, L, false>, g->smem);
         smem_attr(pgm::k_fft_z_conv<T, L, true>, g->smem);
       });
-    for (auto &g : gbx)
-      with_fft_len(g->K, [&](auto Lc) {
-        constexpr int L = decltype(Lc)::value;
-        smem_attr(pgm::k_spread_x<T, L, P, false>, g->smem);
-        smem_attr(pgm::k_spread_x<T, L, P, true>, g->smem);
-      });
   }
 
   // The five passes of one reciprocal-space convolution (r2c, k2, k1 with G, k2, c2r).
-  void fft_chain(cudaStream_t st, pgm::Dev<T> &a, int act, bool energy, bool x_fwd = true) {
-    if (x_fwd)
+  void fft_chain(cudaStream_t st, pgm::Dev<T> &a, int act, bool energy) {
     for (auto &g : gx)
       with_fft_len(g->K, [&](auto Lc) {
         pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
@@ -558,12 +520,9 @@ struct Engine : EngineBase {
     CK(cudaEventCreate(&e1));
     auto one = [&]() {
       if (which == 0) pgm::k_rowmat<T, P, false, 1, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
-      else if (which == 1) {
-        if (binned) spread_x<false>(st, a, Pv.p, 0);
-        else pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
-      }
+      else if (which == 1) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
       else if (which == 2) {
-        fft_chain(st, a, 0, false, !binned);
+        fft_chain(st, a, 0, false);
       } else if (which == 3) pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, nullptr);
       else if (which == 4) pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
       else if (which == 5) {
@@ -629,12 +588,6 @@ struct Engine : EngineBase {
     pgm::k_box<T><<<grid1(nsys, 64), 64, 0, st>>>(a, boxes); check_launch();
     pgm::k_prep<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
     pgm::k_mol<T><<<grid1(nmol_total), 256, 0, st>>>(a); check_launch();
-    if (binned) {  // atoms by spline base, for the binned spread of every sweep of this step
-      CK(cudaMemsetAsync(bin_count.p, 0, sizeof(int) * nbin, st));
-      pgm::k_bin_assign<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
-      pgm::k_scan_cells<<<1, 1024, 0, st>>>(bin_count.p, bin_start.p, nbin, d_one.p); check_launch();
-      pgm::k_bin_scatter<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
-    }
     if (!a.idx) {  // the Verlet candidate list, rebuilt on the device when the flag is up
       pgm::k_cell_assign<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
       pgm::k_scan_cells<<<1, 1024, 0, st>>>(cell_count.p, cell_start.p, ncell, nb_flag.p); check_launch();
@@ -667,27 +620,8 @@ struct Engine : EngineBase {
   // Reciprocal-space potential phi of the grid spread from `vin` (with charges if WITH_Q).
   template <bool WITH_Q, bool UPDATE_P, int ACT, bool ENERGY>
   void pme(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin) {
-    if (binned) {  // atomic-free: the spread is fused with the k3 pass
-      if (UPDATE_P) {
-        pgm::k_update_p<T><<<ntblk, 256, 0, st>>>(a); check_launch();
-        vin = Pv.p;
-      }
-      spread_x<WITH_Q>(st, a, vin, ACT);
-      fft_chain(st, a, ACT, ENERGY, false);
-      return;
-    }
     pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
     fft_chain(st, a, ACT, ENERGY);
-  }
-
-  template <bool WITH_Q>
-  void spread_x(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin, int act) {
-    for (auto &g : gbx)
-      with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_spread_x<T, decltype(Lc)::value, P, WITH_Q><<<g->ntiles, 256, g->smem, st>>>(a, vin, g->sys.p, g->tile0.p, g->ng,
-                                                                                            act);
-        check_launch();
-      });
   }
 
   // One field sweep of the dipoles vin (charges with WITH_Q): the spread (after the CG direction

@@ -47,7 +47,6 @@ struct SysInfo {
   int nst[3];           // FFT stages per axis
   int rad[3][MAX_STAGES];
   int mod0[3];          // offsets of the B-spline moduli of each axis
-  int nb1, nb2, bin0;   // spline-base bins of 4 x 4 (k1, k2) lines (binned spread), their offset
   double tail_sb;       // 2 sum_k C(6,k) M_k M_(6-k) of the LJ tail (lj.py:87-114)
   double sum_q, sum_q2; // charges
 };

@@ -60,7 +60,6 @@ struct Dev {
   // vectors
   v4<T> *X, *R, *Z, *P, *AP, *B, *D;
   v4<T> *F;  // row field of a sweep (computed concurrently with the PME chain)
-  int *bin_of, *bin_slot, *bin_count, *bin_start, *bin_atoms;  // atoms binned by spline base
   // grids
   T *Q, *Phi, *Ginf;
   c2<T> *C;
@@ -766,144 +765,6 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, co
     Bv.x = T(0.5) * dy; Bv.y = -T(0.5) * dx;
     C[(size_t)(2 * cl) * K3h + m] = A;
     C[(size_t)(2 * cl + 1) * K3h + m] = Bv;
-  }
-}
-
-// ------------------------------------------------------------------ binned spread fused with the k3 pass
-// Atoms are binned once per step by their spline base (b1 / 4, b2 / 4).  A CTA owns the 16 real
-// lines of a 4 x 4 block of (k1, k2); the atoms whose P x P stencil columns can reach it lie in the
-// 3 x 3 bins (T1 - 2 .. T1) x (T2 - 2 .. T2) (P - 1 <= 7 < 8).  Each thread takes one atom, adds its
-// stencil points that fall in the block to the block's lines in shared memory, and the block is
-// then transformed along k3 as in k_fft_x_fwd.  No global atomics, no real grid in HBM
-// (pme.py:306-337 then the first axis of pme.py:374).
-template <typename T>
-__global__ void k_bin_assign(Dev<T> a) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nt) return;
-  const SysInfo &S = a.sys[a.sysid[i]];
-  int4 b = a.base[i];
-  int bin = S.bin0 + (b.x >> 2) * S.nb2 + (b.y >> 2);
-  a.bin_of[i] = bin;
-  a.bin_slot[i] = atomicAdd(&a.bin_count[bin], 1);
-}
-
-template <typename T>
-__global__ void k_bin_scatter(Dev<T> a) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nt) return;
-  a.bin_atoms[a.bin_start[a.bin_of[i]] + a.bin_slot[i]] = i;
-}
-
-// p = z + beta p for the systems still iterating (forcefield.py:1812), before the binned sweep.
-template <typename T>
-__global__ void k_update_p(Dev<T> a) {
-  int s = a.tb_sys[blockIdx.x];
-  if (!a.cg[s].active) return;
-  int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
-  const SysInfo &S = a.sys[s];
-  if (i >= S.atom0 + S.natom) return;
-  v4<T> z = a.Z[i], p = a.P[i];
-  T bt = T(a.cg[s].beta);
-  p.x = z.x + bt * p.x; p.y = z.y + bt * p.y; p.z = z.z + bt * p.z; p.w = T(0);
-  a.P[i] = p;
-}
-
-template <typename T, int L, int P, bool WITH_Q>
-__global__ void __launch_bounds__(256) k_spread_x(Dev<T> a, const v4<T> *__restrict__ vin, const int *gsys, const int *gtile0,
-                                                  int ng, int act) {
-  extern __shared__ unsigned char smem_raw[];
-  int g = group_member(gtile0, ng, blockIdx.x);
-  int s = gsys[g];
-  if (!pass_active(a, s, act)) return;
-  const SysInfo &S = a.sys[s];
-  const BoxInfo &B = a.box[s];
-  const int K1 = S.K[0], K2 = S.K[1], K3 = L ? L : S.K[2], K3h = K3 / 2 + 1;
-  int tile = blockIdx.x - gtile0[g];
-  int T1 = tile / S.nb2, T2 = tile - T1 * S.nb2;
-  int k10 = 4 * T1, k20 = 4 * T2;
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3;
-  T *line = reinterpret_cast<T *>(y);  // 16 real lines of K3 (the y buffer, before the FFT uses it)
-  for (int t = threadIdx.x; t < 16 * K3; t += blockDim.x) line[t] = T(0);
-  __syncthreads();
-  T es[9];
-#pragma unroll
-  for (int bb = 0; bb < 3; ++bb)
-#pragma unroll
-    for (int aa = 0; aa < 3; ++aa) es[bb * 3 + aa] = T(B.Hinv[bb * 3 + aa] * S.K[aa]);
-  // the 3 x 3 candidate bins as one flat list of atoms (about 190 for a 96^3 mesh of 12k atoms)
-  int r0[9], cnt[9], tot = 0;
-#pragma unroll
-  for (int nb = 0; nb < 9; ++nb) {
-    int B1 = T1 - 2 + nb / 3, B2 = T2 - 2 + nb % 3;
-    if (B1 < 0) B1 += S.nb1;
-    if (B2 < 0) B2 += S.nb2;
-    int bin = S.bin0 + B1 * S.nb2 + B2;
-    r0[nb] = a.bin_start[bin];
-    cnt[nb] = a.bin_start[bin + 1] - r0[nb];
-    tot += cnt[nb];
-  }
-  {
-    for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-      int nb = 0, ff = f;
-      while (ff >= cnt[nb]) { ff -= cnt[nb]; ++nb; }
-      int i = a.bin_atoms[r0[nb] + ff];
-      int4 b = a.base[i];
-      // offsets of the block's first line from the atom's base, modulo the mesh
-      int o1 = k10 - b.x; if (o1 < -K1 / 2) o1 += K1; if (o1 > K1 / 2) o1 -= K1;
-      int o2 = k20 - b.y; if (o2 < -K2 / 2) o2 += K2; if (o2 > K2 / 2) o2 -= K2;
-      int j1lo = max(0, o1), j1hi = min(P - 1, o1 + 3), j2lo = max(0, o2), j2hi = min(P - 1, o2 + 3);
-      if (j1lo > j1hi || j2lo > j2hi) continue;
-      v4<T> f = a.frac[i];
-      T t1[P], u1[P], t2[P], u2[P], t3[P], u3[P];
-      bspline<T, P, false>(f.x, t1, u1, nullptr);
-      bspline<T, P, false>(f.y, t2, u2, nullptr);
-      bspline<T, P, false>(f.z, t3, u3, nullptr);
-      v4<T> d = vin[i];
-      T e0 = d.x * es[0] + d.y * es[3] + d.z * es[6];
-      T e1 = d.x * es[1] + d.y * es[4] + d.z * es[7];
-      T e2 = d.x * es[2] + d.y * es[5] + d.z * es[8];
-      T qi = WITH_Q ? a.q[i] : T(0);
-#pragma unroll
-      for (int j1 = 0; j1 < P; ++j1) {
-        if (j1 < j1lo || j1 > j1hi) continue;
-#pragma unroll
-        for (int j2 = 0; j2 < P; ++j2) {
-          if (j2 < j2lo || j2 > j2hi) continue;
-          T A = (qi * t1[j1] + e0 * u1[j1]) * t2[j2] + e1 * t1[j1] * u2[j2], Bw = e2 * t1[j1] * t2[j2];
-          T *ln = line + ((j1 - o1) * 4 + (j2 - o2)) * K3;
-#pragma unroll
-          for (int j3 = 0; j3 < P; ++j3) {
-            int k3 = b.z + j3;
-            if (k3 >= K3) k3 -= K3;
-            atomicAdd(ln + k3, A * t3[j3] + Bw * u3[j3]);
-          }
-        }
-      }
-    }
-  }
-  __syncthreads();
-  // pack the 16 lines (a, b) = (k1 - k10, k2 - k20) as 8 complex lines: (a, 2c) + i (a, 2c + 1)
-  for (int t = threadIdx.x; t < 8 * K3; t += blockDim.x) {
-    int cl = t / K3, k = t - cl * K3;
-    c2<T> z;
-    z.x = line[(2 * cl) * K3 + k];
-    z.y = line[(2 * cl + 1) * K3 + k];
-    x[cl * K3 + k] = z;
-  }
-  __syncthreads();
-  c2<T> *res = fft_lines<T, L>(x, y, K3, 8, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], -1);
-  c2<T> *C = a.C + S.cgrid0;
-  for (int t = threadIdx.x; t < 8 * K3h; t += blockDim.x) {
-    int cl = t / K3h, m = t - cl * K3h;
-    c2<T> Z = res[cl * K3 + m], W = res[cl * K3 + (m == 0 ? 0 : K3 - m)];
-    c2<T> A, Bv;
-    A.x = T(0.5) * (Z.x + W.x); A.y = T(0.5) * (Z.y - W.y);
-    T dx = Z.x - W.x, dy = Z.y + W.y;
-    Bv.x = T(0.5) * dy; Bv.y = -T(0.5) * dx;
-    int la = (2 * cl) >> 2, lb = (2 * cl) & 3;  // line (la, lb) and (la, lb + 1)
-    size_t l0 = (size_t)(k10 + la) * K2 + (k20 + lb);
-    C[l0 * K3h + m] = A;
-    C[(l0 + 1) * K3h + m] = Bv;
   }
 }
 
