@@ -524,7 +524,10 @@ struct Engine : EngineBase {
       else if (which == 2) {
         fft_chain(st, a, 0, false);
       } else if (which == 3) pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, nullptr);
-      else if (which == 4) pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
+      else if (which == 4) {
+        pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
+        pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a);
+      }
       else if (which == 5) {
         for (auto &g : gx)
           with_fft_len(g->K, [&](auto Lc) {
@@ -598,6 +601,7 @@ struct Engine : EngineBase {
       pgm::k_nb_lower<<<1, 1, 0, st>>>(nb_flag.p, nb_builds.p); check_launch();
     }
     pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a); check_launch();
+    pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a); check_launch();
     pgm::k_influence<T><<<std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st>>>(a, cgrid); check_launch();
   }
 
@@ -629,9 +633,13 @@ struct Engine : EngineBase {
   // the PME gather that assembles MODE 0 (field) or 1 (operator, with p.Ap) into out.
   template <bool WITH_Q, bool UPDATE_P, int ACT, int MODE>
   void sweep(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin, pgm::v4<T> *out) {
-    if (!overlap) {  // measured faster on B200 at 12k atoms: one kernel does rows + gather after the FFTs
-      pme<WITH_Q, UPDATE_P, ACT, false>(st, a, vin);
-      pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, true><<<nwblk, 256, 0, st>>>(a, vin, out); check_launch();
+    if (!overlap) {
+      // one stream: the row field runs between the spread and the first FFT pass, while the L2
+      // still processes the spread's atomic adds, then the FFTs and the PME gather
+      pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
+      pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, st>>>(a, UPDATE_P ? Pv.p : vin, Fv.p); check_launch();
+      fft_chain(st, a, ACT, false);
+      pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false><<<nwblk, 256, 0, st>>>(a, UPDATE_P ? Pv.p : vin, out); check_launch();
       return;
     }
     // the loop body is captured as a sequence of its own: it forks to its own stream

@@ -329,68 +329,29 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 }
 
 // ------------------------------------------------------------------ pair rows
-// One warp per atom: the molecule partners (always kept inside the cutoff; the rigid special
-// table of md/topology.py:161-178), then the neighbours from the cell list (or from the caller's
-// candidate rows), masked to r < rc (forcefield.py:1140-1195).  Kept pairs are staged in shared
-// memory in order, and the radial kernels G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] of the
-// staged pairs are evaluated 32 at a time on a full warp, then written to the row (coalesced).
-constexpr int STAGE = 64;
-
+// Two kernels.  k_rows: one warp per atom finds the row -- the molecule partners (always kept
+// inside the cutoff; the rigid special table of md/topology.py:161-178), then the candidates of the
+// Verlet list (or the caller's rows), masked to r < rc (forcefield.py:1140-1195) -- and writes k, x,
+// y, z compacted by ballot; the next chunk of candidates is loaded before the current one is
+// tested.  k_row_kernels: one thread per row entry evaluates the radial kernels
+// G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] (forcefield.py:1314-1338, kernels.py:76-118).
 template <typename T>
-struct RowStage {
-  int j[WARPS_PER_BLOCK][STAGE];
-  T x[WARPS_PER_BLOCK][STAGE], y[WARPS_PER_BLOCK][STAGE], z[WARPS_PER_BLOCK][STAGE];
-};
-
-template <typename T>
-__device__ __forceinline__ void rows_flush(const Dev<T> &a, RowStage<T> &st, int w, int lane, int nf, int &nst, int &written,
-                                           size_t base, T Ri2) {
-  if (lane < nf) {
-    int j = st.j[w][lane];
-    T xt = st.x[w][lane], yt = st.y[w][lane], zt = st.z[w][lane];
-    int slot = written + lane;
-    if (slot < a.mc) {
-      T r = t_sqrt(xt * xt + yt * yt + zt * zt);
-      T Rk = a.radius[j];
-      T aik = t_rsqrt(T(2) * (Ri2 + Rk * Rk));
-      T A[4], Bb[4];
-      erf_kernels<T>(aik, r, A);
-      erf_kernels<T>(T(a.beta), r, Bb);
-      size_t o = base + slot;
-      a.rk[o] = j;
-      a.rx[o] = xt; a.ry[o] = yt; a.rz[o] = zt;
-      a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = A[1] - Bb[1]; a.rg2[o] = A[2] - Bb[2]; a.rg3[o] = A[3] - Bb[3];
-    }
-  }
-  written += nf;
-  int rem = nst - nf;
-  __syncwarp();
-  int j2 = 0;
-  T x2 = 0, y2 = 0, z2 = 0;
-  if (lane < rem) { j2 = st.j[w][nf + lane]; x2 = st.x[w][nf + lane]; y2 = st.y[w][nf + lane]; z2 = st.z[w][nf + lane]; }
-  __syncwarp();
-  if (lane < rem) { st.j[w][lane] = j2; st.x[w][lane] = x2; st.y[w][lane] = y2; st.z[w][lane] = z2; }
-  __syncwarp();
-  nst = rem;
-}
-
-template <typename T>
-__device__ __forceinline__ void rows_stage(const Dev<T> &a, RowStage<T> &st, int w, int lane, bool keep, int j, double x,
-                                           double y, double z, int &nst, int &written, size_t base, T Ri2) {
+__device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, double x, double y, double z, size_t base, int &count,
+                                         int lane) {
   unsigned bal = __ballot_sync(0xffffffffu, keep);
   if (keep) {
-    int pos = nst + __popc(bal & ((1u << lane) - 1u));
-    st.j[w][pos] = j;
-    st.x[w][pos] = T(x); st.y[w][pos] = T(y); st.z[w][pos] = T(z);
+    int slot = count + __popc(bal & ((1u << lane) - 1u));
+    if (slot < a.mc) {
+      size_t o = base + slot;
+      a.rk[o] = j;
+      a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
+    }
   }
-  nst += __popc(bal);
-  __syncwarp();
-  if (nst >= 32) rows_flush<T>(a, st, w, lane, 32, nst, written, base, Ri2);
+  count += __popc(bal);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
-  __shared__ RowStage<T> st;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int blk = blockIdx.x;
   int s = a.wb_sys[blk];
@@ -402,67 +363,82 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
 #pragma unroll
   for (int k = 0; k < 9; ++k) H[k] = B.H[k];
   id[0] = B.idiag[0]; id[1] = B.idiag[1]; id[2] = B.idiag[2];
-  double pix = a.pos[3 * i], piy = a.pos[3 * i + 1], piz = a.pos[3 * i + 2];
+  double4 pi = a.pos4[i];
   double rc2 = a.cutoff * a.cutoff;
-  T Ri = a.radius[i], Ri2 = Ri * Ri;
   size_t base = (size_t)i * a.mc;
-  int nst = 0, written = 0;
+  int count = 0;
   int mf = a.molfirst[i], me = a.molend[i];
   for (int j0 = mf; j0 < me; j0 += 32) {
     int j = j0 + lane;
     bool keep = false;
     double x = 0, y = 0, z = 0;
     if (j < me && j != i) {
-      x = pix - a.pos[3 * j]; y = piy - a.pos[3 * j + 1]; z = piz - a.pos[3 * j + 2];
+      double4 pj = a.pos4[j];
+      x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane);
   }
-  int nsp = written + nst;
-  int mi = a.molid[i];
+  int nsp = count;
+  int mi = (int)pi.w;
+  const int *row;
+  int nc;
   if (a.idx) {  // the caller's candidate rows (local indices, padding natom)
-    const int *row = a.idx + (size_t)i * a.idx_width;
-    for (int c0 = 0; c0 < a.idx_width; c0 += 32) {
-      int c = c0 + lane;
-      int jl = c < a.idx_width ? row[c] : S.natom;
-      bool ok = jl >= 0 && jl < S.natom;
-      int j = S.atom0 + (ok ? jl : 0);
-      ok = ok && a.molid[j] != mi;
-      bool keep = false;
-      double x = 0, y = 0, z = 0;
-      if (ok) {
-        x = pix - a.pos[3 * j]; y = piy - a.pos[3 * j + 1]; z = piz - a.pos[3 * j + 2];
-        min_image_fast(x, y, z, H, id);
-        keep = x * x + y * y + z * z < rc2;
-      }
-      rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
-    }
-  } else {  // the engine's Verlet candidates (within cutoff + skin at the last rebuild)
-    const int *row = a.cand + (size_t)i * a.cc;
-    int nc = min(a.ncand[i], a.cc);
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-      int c = c0 + lane;
-      bool keep = false;
-      int j = 0;
-      double x = 0, y = 0, z = 0;
-      if (c < nc) {
-        j = row[c];
-        double4 pj = a.pos4[j];
-        x = pix - pj.x; y = piy - pj.y; z = piz - pj.z;
-        min_image_fast(x, y, z, H, id);
-        keep = x * x + y * y + z * z < rc2;
-      }
-      rows_stage<T>(a, st, warp, lane, keep, j, x, y, z, nst, written, base, Ri2);
-    }
+    row = a.idx + (size_t)i * a.idx_width;
+    nc = a.idx_width;
+  } else {      // the engine's Verlet candidates (within cutoff + skin at the last rebuild)
+    row = a.cand + (size_t)i * a.cc;
+    nc = min(a.ncand[i], a.cc);
   }
-  while (nst > 0) rows_flush<T>(a, st, warp, lane, min(nst, 32), nst, written, base, Ri2);
+  auto load = [&](int c, int &j, double4 &pj) {
+    j = -1;
+    if (c < nc) {
+      int jl = row[c];
+      if (a.idx) j = (jl >= 0 && jl < S.natom) ? S.atom0 + jl : -1;
+      else j = jl;
+      if (j >= 0) pj = a.pos4[j];
+    }
+  };
+  int jn = -1;
+  double4 pn = make_double4(0, 0, 0, -1);
+  load(lane, jn, pn);
+  for (int c0 = 0; c0 < nc; c0 += 32) {
+    int j = jn;
+    double4 pj = pn;
+    load(c0 + 32 + lane, jn, pn);  // prefetch the next chunk
+    bool keep = false;
+    double x = 0, y = 0, z = 0;
+    if (j >= 0 && (int)pj.w != mi) {
+      x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
+      min_image_fast(x, y, z, H, id);
+      keep = x * x + y * y + z * z < rc2;
+    }
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane);
+  }
   if (lane == 0) {
-    a.rn[i] = written;
+    a.rn[i] = count;
     a.rnsp[i] = nsp;
-    if (written > a.mc) atomicOr(&a.status[s], 0x1u);
-    atomicMax(a.max_count, written);
+    if (count > a.mc) atomicOr(&a.status[s], 0x1u);
+    atomicMax(a.max_count, count);
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_row_kernels(Dev<T> a) {
+  size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  int i = (int)(t / a.mc), slot = (int)(t - (size_t)i * a.mc);
+  if (i >= a.nt || slot >= min(a.rn[i], a.mc)) return;
+  size_t o = (size_t)i * a.mc + slot;
+  T x = a.rx[o], y = a.ry[o], z = a.rz[o];
+  int k = a.rk[o];
+  T Ri = a.radius[i], Rk = a.radius[k];
+  T r = t_sqrt(x * x + y * y + z * z);
+  T aik = t_rsqrt(T(2) * (Ri * Ri + Rk * Rk));
+  T A[4], Bb[4];
+  erf_kernels<T>(aik, r, A);
+  erf_kernels<T>(T(a.beta), r, Bb);
+  a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = A[1] - Bb[1]; a.rg2[o] = A[2] - Bb[2]; a.rg3[o] = A[3] - Bb[3];
 }
 
 // ------------------------------------------------------------------ PME influence function
