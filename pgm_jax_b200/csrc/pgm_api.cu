@@ -554,7 +554,7 @@ struct Engine : EngineBase {
     CK(cudaEventSynchronize(e1));
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, e0, e1));
-    if (which == 1) CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // the spread grid must start at zero
+    CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // leave the spread grid cleared
     launches = l0;
     CK(cudaEventDestroy(e0));
     CK(cudaEventDestroy(e1));
@@ -624,6 +624,7 @@ struct Engine : EngineBase {
   // Reciprocal-space potential phi of the grid spread from `vin` (with charges if WITH_Q).
   template <bool WITH_Q, bool UPDATE_P, int ACT, bool ENERGY>
   void pme(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin) {
+    CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // the spread accumulates into a cleared grid
     pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
     fft_chain(st, a, ACT, ENERGY);
   }
@@ -636,6 +637,7 @@ struct Engine : EngineBase {
     if (!overlap) {
       // one stream: the row field runs between the spread and the first FFT pass, while the L2
       // still processes the spread's atomic adds, then the FFTs and the PME gather
+      CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // the spread accumulates into a cleared grid
       pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
       pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, st>>>(a, UPDATE_P ? Pv.p : vin, Fv.p); check_launch();
       fft_chain(st, a, ACT, false);
@@ -645,6 +647,7 @@ struct Engine : EngineBase {
     // the loop body is captured as a sequence of its own: it forks to its own stream
     cudaStream_t ax = in_body ? aux_b : aux;
     cudaEvent_t ef = in_body ? ev_fork_b : ev_fork, ej = in_body ? ev_join_b : ev_join;
+    CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));
     pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
     CK(cudaEventRecord(ef, st));
     CK(cudaStreamWaitEvent(ax, ef, 0));

@@ -99,6 +99,8 @@ __device__ __forceinline__ void min_image(double &x, double &y, double &z, const
 
 // B_0..B_3 of erf(a r)/r: 15-term Taylor series where (a r)^2 < 1, else the closed-form
 // recursion (pgm_jax/md/kernels.py:76-118).
+// (The series divides by the odd integers 2m + 2n + 1 as multiplications by their reciprocals, and
+// the closed form multiplies by 1/r: the same expressions, rounded once more per term.)
 template <typename T>
 __device__ __forceinline__ void erf_kernels(T a, T r, T B[4]) {
   const T x = a * r, s = x * x;
@@ -107,20 +109,20 @@ __device__ __forceinline__ void erf_kernels(T a, T r, T B[4]) {
     T t = T(1), acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
 #pragma unroll
     for (int m = 0; m < 15; ++m) {
-      acc0 += t / T(2 * m + 1);
-      acc1 += t / T(2 * m + 3);
-      acc2 += t / T(2 * m + 5);
-      acc3 += t / T(2 * m + 7);
-      t *= -s / T(m + 1);
+      acc0 += t * T(1.0 / (2 * m + 1));
+      acc1 += t * T(1.0 / (2 * m + 3));
+      acc2 += t * T(1.0 / (2 * m + 5));
+      acc3 += t * T(1.0 / (2 * m + 7));
+      t *= -s * T(1.0 / (m + 1));
     }
     B[0] = c0 * acc0;
     B[1] = c0 * a2x2 * acc1;
     B[2] = c0 * a2x2 * a2x2 * acc2;
     B[3] = c0 * a2x2 * a2x2 * a2x2 * acc3;
   } else {
-    const T ir2 = T(1) / (r * r);
+    const T ir = T(1) / r, ir2 = ir * ir;
     const T c = c0 * t_exp(-s);
-    B[0] = t_erf(x) / r;
+    B[0] = t_erf(x) * ir;
     B[1] = (B[0] - c) * ir2;
     B[2] = (T(3) * B[1] - a2x2 * c) * ir2;
     B[3] = (T(5) * B[2] - a2x2 * a2x2 * c) * ir2;

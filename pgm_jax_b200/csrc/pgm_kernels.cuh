@@ -708,7 +708,7 @@ __device__ __forceinline__ bool pass_active(const Dev<T> &a, int s, int act) {
 }
 
 // k3 pass, real -> half complex: two real lines packed as one complex line (z = a + i b), one
-// length-K3 FFT, untangled; the real grid is cleared as it is read (ready for the next spread).
+// length-K3 FFT, untangled.
 template <typename T, int L>
 __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
   extern __shared__ unsigned char smem_raw[];
@@ -724,10 +724,8 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, co
   T *Q = a.Q + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
     int rl = t / K3, k = t - rl * K3;
-    T v = Q[t];
-    Q[t] = T(0);
     T *dst = reinterpret_cast<T *>(&x[(rl >> 1) * K3 + k]);
-    dst[rl & 1] = v;
+    dst[rl & 1] = Q[t];
   }
   __syncthreads();
   c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], -1);
