@@ -471,30 +471,30 @@ struct Engine : EngineBase {
   void fft_chain(cudaStream_t st, pgm::Dev<T> &a, int act, bool energy) {
     for (auto &g : gx)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+        pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
         check_launch();
       });
     for (auto &g : gy)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, -1);
+        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, -1);
         check_launch();
       });
     for (auto &g : gz)
       with_fft_len(g->K, [&](auto Lc) {
         if (energy)
-          pgm::k_fft_z_conv<T, decltype(Lc)::value, true><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+          pgm::k_fft_z_conv<T, decltype(Lc)::value, true><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
         else
-          pgm::k_fft_z_conv<T, decltype(Lc)::value, false><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+          pgm::k_fft_z_conv<T, decltype(Lc)::value, false><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
         check_launch();
       });
     for (auto &g : gy)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, +1);
+        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, +1);
         check_launch();
       });
     for (auto &g : gx)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_x_inv<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+        pgm::k_fft_x_inv<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
         check_launch();
       });
   }
@@ -531,13 +531,13 @@ struct Engine : EngineBase {
       else if (which == 5) {
         for (auto &g : gx)
           with_fft_len(g->K, [&](auto Lc) {
-            pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
+            pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
           });
       } else if (which == 6) {
         pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
         for (auto &g : gx)
           with_fft_len(g->K, [&](auto Lc) {
-            pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, 256, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
+            pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
           });
       } else if (which == 7) pgm::k_rowfield<T, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, Fv.p);
       else if (which == 8) pgm::k_rowmat<T, P, false, 1, 0, false><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
