@@ -720,15 +720,16 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, co
   int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;  // first real line
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
   T *Q = a.Q + S.rgrid0 + (size_t)l0 * K3;
+  for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];  // twiddles in shared memory
   for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
     int rl = t / K3, k = t - rl * K3;
     T *dst = reinterpret_cast<T *>(&x[(rl >> 1) * K3 + k]);
     dst[rl & 1] = Q[t];
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], -1);
+  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, -1);
   c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
   for (int t = threadIdx.x; t < np * K3h; t += blockDim.x) {
     int cl = t / K3h, m = t - cl * K3h;
@@ -754,8 +755,9 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
   int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
   const c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
+  for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];
   for (int t = threadIdx.x; t < np * K3; t += blockDim.x) {
     int cl = t / K3, m = t - cl * K3;
     bool up = m > K3 / 2;
@@ -768,7 +770,7 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
     x[cl * K3 + m] = Z;
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], a.tw + S.tw[2], +1);
+  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, +1);
   T *Phi = a.Phi + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
     int rl = t / K3, k = t - rl * K3;
@@ -789,8 +791,9 @@ __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const 
   const int K2 = L ? L : S.K[1], K3h = S.K3h, ncol = S.K[0] * K3h;
   int c0 = (blockIdx.x - gtile0[g]) * FFT_TILE;
   const int ld = K2 + 1;
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld, *tws = y + FFT_TILE * ld;
   c2<T> *C = a.C + S.cgrid0;
+  for (int t = threadIdx.x; t < K2; t += blockDim.x) tws[t] = a.tw[S.tw[1] + t];
   for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
     int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
     int col = c0 + c;
@@ -803,7 +806,7 @@ __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const 
     x[c * ld + k2] = v;
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], a.tw + S.tw[1], sign);
+  c2<T> *res = fft_lines<T, L>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], tws, sign);
   for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
     int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
     int col = c0 + c;
@@ -829,9 +832,10 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
   const int K1 = L ? L : S.K[0], K2 = S.K[1], K3 = S.K[2], K3h = S.K3h, ncol = K2 * K3h;
   int c0 = (blockIdx.x - gtile0[g]) * FFT_TILE;
   const int ld = K1 + 1;
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld, *tws = y + FFT_TILE * ld;
   c2<T> *C = a.C + S.cgrid0;
   const size_t rs = (size_t)ncol;
+  for (int t = threadIdx.x; t < K1; t += blockDim.x) tws[t] = a.tw[S.tw[0] + t];
   for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
     int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
     int col = c0 + c;
@@ -841,7 +845,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
     x[c * ld + k1] = v;
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], -1);
+  c2<T> *res = fft_lines<T, L>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], tws, -1);
   c2<T> *oth = res == x ? y : x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const BoxInfo &B = a.box[s];
@@ -889,7 +893,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
     atomicAdd(&a.eacc[s].vinf[threadIdx.x], v);
   }
-  c2<T> *res2 = fft_lines<T, L>(res, oth, K1, FFT_TILE, ld, S.rad[0], S.nst[0], a.tw + S.tw[0], +1);
+  c2<T> *res2 = fft_lines<T, L>(res, oth, K1, FFT_TILE, ld, S.rad[0], S.nst[0], tws, +1);
   for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
     int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
     int col = c0 + c;
