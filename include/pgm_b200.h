@@ -55,7 +55,8 @@ typedef struct {
     int pme_order;      /* 4, 6 or 8 (PMESettings.order) */
     double dipole_tol;  /* max|alpha r| / mean|alpha b| (Induction.tol) */
     int max_iter;       /* Induction.max_iter */
-    int predictor;      /* 0 "none", 3 "mu3", 4 "mu4" (Induction.predictor) */
+    int predictor;      /* 0 "none", 3 "mu3", 4 "mu4" (Induction.predictor); 5 the learned guess
+                           (pgm_set_nn_model; mu4 until a model is set) */
     int fused;          /* Induction.fused */
     int norm_refresh;   /* Induction.norm_refresh */
     double peek;        /* Induction.peek */
@@ -177,6 +178,31 @@ PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, do
 
 /* In-cutoff pairs (both rows of every pair) of the last step's row build. */
 long long pgm_row_pairs(PgmHandle *h);
+
+/* ------------------------------------------------------------------ learned initial guess
+ * No counterpart in the reference (its guesses are the mu3 / mu4 / ls predictors,
+ * forcefield.py:1917-2008).  A message-passing model on the short-range graph predicts the
+ * converged dipoles from the permanent field b and the last two steps' dipoles; with predictor 5
+ * the solve starts from that prediction (an unfused start: the field sweep for b, the features, the
+ * model, the residual sweep) and CG iterates to the same tolerance.
+ * Features per atom: 16 rotation invariants (float, (N, 16)) and 27 vector channels (float,
+ * (N, 27, 3)): alpha b, mu_{n-1}, mu_{n-2} and their radial-basis neighbour sums over edges r < the
+ * graph cutoff, plain and projected on the edge direction.  The model (pgm_nn_param_count() floats,
+ * device) is the MLP of pgm_nn_predict. */
+PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff);
+/* Features at a geometry: hist (4, N, 3) device (newest first, as PgmInduction.hist); inv, vec device. */
+PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist, float *inv,
+                          float *vec);
+int pgm_nn_param_count(void);
+/* mu (n, 3) = sum_c c_c(inv) vec_c with c = MLP(inv): BF16 tensor cores, FP32 accumulation. */
+PgmStatus pgm_nn_predict(void *stream, const float *weights, const float *inv, const float *vec, int n, float *mu);
+/* Training: loss += sum |mu - target|^2 * inv_scale (double, device) and grad += dloss/dweights. */
+PgmStatus pgm_nn_loss_grad(void *stream, const float *weights, const float *inv, const float *vec, const float *target, int n,
+                           float inv_scale, float *grad, double *loss);
+/* One Adam step (bias-corrected at `step` >= 1) on the weights; clears grad. */
+PgmStatus pgm_nn_adam(void *stream, float *weights, float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                      float eps, int step);
+const char *pgm_nn_last_error(void);
 
 /* ------------------------------------------------------------------ allocation-free field
  * pgm_field_static has no counterpart in the reference.  It is for callers that must not allocate

@@ -22,6 +22,8 @@ EXPORTS = (
     "pgm_last_error", "pgm_last_launch_count", "pgm_launches_per_iteration", "pgm_profile_kernel", "pgm_row_pairs", "pgm_rigid_create", "pgm_rigid_destroy",
     "pgm_rigid_begin_step", "pgm_rigid_set_step", "pgm_rigid_end_step", "pgm_rigid_kinetic", "pgm_rigid_last_error", "pgm_graph_begin",
     "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
+    "pgm_set_nn_model", "pgm_nn_features", "pgm_nn_param_count", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam",
+    "pgm_nn_last_error",
 )
 
 STATUS_ROW_OVERFLOW = 0x1
@@ -109,6 +111,14 @@ def load(path: str | None = None):
     lib.pgm_field_static.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_double, C.c_double, vp, C.c_int, C.c_int, vp, vp]
     lib.pgm_field_static.restype = C.c_int
     lib.pgm_static_last_error.restype = C.c_char_p
+    lib.pgm_set_nn_model.argtypes = [H, vp, C.c_float, C.c_float]
+    lib.pgm_nn_features.argtypes = [H, vp, vp, vp, vp, vp, vp]
+    lib.pgm_nn_predict.argtypes = [vp, vp, vp, vp, C.c_int, vp]
+    lib.pgm_nn_loss_grad.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_float, vp, vp]
+    lib.pgm_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
+    lib.pgm_nn_last_error.restype = C.c_char_p
+    for n in ("pgm_set_nn_model", "pgm_nn_features", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam"):
+        getattr(lib, n).restype = C.c_int
     lib.pgm_graph_begin.argtypes = [vp]
     lib.pgm_graph_end.argtypes = [vp, C.POINTER(vp)]
     lib.pgm_graph_launch.argtypes = [vp, vp]

@@ -103,6 +103,8 @@ struct EngineBase {
   virtual void fixed_mu(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
                         const double *mu, double *energy, double *forces, double *virial, uint32_t *status) = 0;
   virtual void set_capacity(int mc) = 0;
+  virtual void set_nn(const float *w, float sigma, float rg) = 0;
+  virtual void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, float *inv, float *vec) = 0;
   virtual void set_list_capacity(int c) = 0;
   virtual int list_capacity() const = 0;
   virtual long long list_rebuilds() = 0;
@@ -171,6 +173,9 @@ struct Engine : EngineBase {
   DBuf<T> Q, Phi, Ginf;
   DBuf<pgm::c2<T>> C, tw;
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
+  DBuf<float> nn_w, nn_inv, nn_vec, nn_mu;  // learned guess: model and per-atom features
+  bool nn_on = false;
+  float nn_sigma = 0.02f, nn_rg = 0.5f;
   int *h_any = nullptr;
   const double *last_pos = nullptr;
   cudaStream_t side = nullptr, aux = nullptr, aux_b = nullptr;
@@ -427,6 +432,8 @@ struct Engine : EngineBase {
     Q.alloc(rgrid); Phi.alloc(rgrid); Ginf.alloc(cgrid); C.alloc(cgrid);
     CK(cudaMemset(Q.p, 0, sizeof(T) * rgrid));
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
+    nn_w.alloc(pgmnn::NN_NPARAM); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
+    nn_mu.alloc((size_t)nt * 3);
     CK(cudaMallocHost(&h_any, sizeof(int)));
     CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&aux_b, cudaStreamNonBlocking));
@@ -497,6 +504,25 @@ struct Engine : EngineBase {
         pgm::k_fft_x_inv<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
         check_launch();
       });
+  }
+
+  void set_nn(const float *w, float sigma, float rg) override {
+    nn_on = w != nullptr;
+    if (w) CK(cudaMemcpy(nn_w.p, w, sizeof(float) * pgmnn::NN_NPARAM, cudaMemcpyDeviceToDevice));
+    nn_sigma = sigma;
+    nn_rg = rg;
+  }
+
+  // Features of the learned guess at a geometry (rows, the permanent field b, the history).
+  void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, float *inv, float *vec) override {
+    launches = 0;
+    CK(cudaMemsetAsync(d_status.p, 0, sizeof(unsigned) * nsys, st));
+    pgm::Dev<T> a = dev(pos, nullptr, 0, forces_tmp.p, d_status.p);
+    prepare(st, a, box);
+    pgm::k_total_dipoles<T><<<grid1(nt), 256, 0, st>>>(a, nullptr); check_launch();
+    sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
+    pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, hist, nn_sigma, nn_rg, inv ? inv : nn_inv.p, vec ? vec : nn_vec.p);
+    check_launch();
   }
 
   void set_capacity(int c) override {
@@ -674,11 +700,16 @@ struct Engine : EngineBase {
   // The induced-dipole solve (forcefield.py:1917-2008 and 1714-1821).  mode 0: predictor start
   // and history push (compute); mode 1: plain start from ind->mu, no push (energy).
   void solve(cudaStream_t st, pgm::Dev<T> &a, PgmInduction *ind, int mode, double *mu_out, int32_t *iters, double *resid) {
-    const int K = set.predictor == 4 ? 4 : (set.predictor == 3 ? 3 : 0);
+    // predictor 5 ("nn"): the learned guess from the permanent field and the last two dipoles,
+    // for systems with two steps of history (unfused start); without a model, mu4
+    const bool use_nn = mode == 0 && set.predictor == 5 && nn_on;
+    const int pred = set.predictor == 5 ? (nn_on ? 0 : 4) : set.predictor;
+    const int K = pred == 4 ? 4 : (pred == 3 ? 3 : 0);
     const double c4[4] = {4.0, -6.0, 4.0, -1.0}, c3[4] = {3.0, -3.0, 1.0, 0.0}, c0[4] = {0, 0, 0, 0};
     const double *cc = K == 4 ? c4 : (K == 3 ? c3 : c0);
-    pgm::k_cg_setup<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, mode == 0 ? ind->count : nullptr, ind->norm, mode == 0 ? K : 0,
-                                                    set.fused, std::max(1, set.norm_refresh), mode);
+    pgm::k_cg_setup<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, mode == 0 ? ind->count : nullptr, ind->norm,
+                                                    mode == 0 ? (use_nn ? 2 : K) : 0, use_nn ? 0 : set.fused,
+                                                    std::max(1, set.norm_refresh), mode);
     check_launch();
     if (mode == 1) {
       // x0 = ind->mu with the plain start: X = mu, have = 1
@@ -689,6 +720,13 @@ struct Engine : EngineBase {
       check_launch();
     }
     sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
+    if (use_nn) {
+      pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, ind->hist, nn_sigma, nn_rg, nn_inv.p, nn_vec.p); check_launch();
+      cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st);
+      if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
+      ++launches;
+      pgm::k_nn_set_x<T><<<grid1(nt), 256, 0, st>>>(a, nn_mu.p); check_launch();
+    }
     pgm::k_start2<T><<<ntblk, 256, 0, st>>>(a); check_launch();
     sweep<false, false, 2, 1>(st, a, X.p, AP.p);
     pgm::k_start3<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
@@ -837,8 +875,8 @@ PgmStatus pgm_create(const PgmSettings *s, const PgmSystemDesc *systems, int n, 
   if (s->precision < 0 || s->precision > 1) return fail(PGM_ERR_INVALID, "precision must be 0 (mixed) or 1 (double)");
   if (!(s->cutoff > 0) || !(s->ewald_beta > 0)) return fail(PGM_ERR_INVALID, "cutoff and ewald_beta must be positive");
   if (s->pme_order != 4 && s->pme_order != 6 && s->pme_order != 8) return fail(PGM_ERR_UNSUPPORTED, "pme_order must be 4, 6 or 8");
-  if (s->predictor != 0 && s->predictor != 3 && s->predictor != 4)
-    return fail(PGM_ERR_INVALID, "predictor must be 0 (none), 3 (mu3) or 4 (mu4)");
+  if (s->predictor != 0 && s->predictor != 3 && s->predictor != 4 && s->predictor != 5)
+    return fail(PGM_ERR_INVALID, "predictor must be 0 (none), 3 (mu3), 4 (mu4) or 5 (learned guess)");
   if (s->max_iter < 0) return fail(PGM_ERR_INVALID, "max_iter must be >= 0");
   for (int i = 0; i < n; ++i) {
     const PgmSystemDesc &d = systems[i];
@@ -999,6 +1037,29 @@ PgmStatus pgm_field(PgmHandle *h, void *stream, const double *pos, const double 
   try {
     CK(cudaSetDevice(h->device));
     h->eng->field((cudaStream_t)stream, pos, box, with_charges, d, field);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff) {
+  if (!h || !(sigma > 0) || !(graph_cutoff > 0)) return fail(PGM_ERR_INVALID, "bad argument");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->set_nn(weights, sigma, graph_cutoff);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist, float *inv,
+                          float *vec) {
+  if (!h || !pos || !box || !hist || !inv || !vec) return fail(PGM_ERR_INVALID, "null argument");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->nn_features((cudaStream_t)stream, pos, box, hist, inv, vec);
     return PGM_OK;
   } catch (CudaError &e) {
     return fail(PGM_ERR_CUDA, e.msg);

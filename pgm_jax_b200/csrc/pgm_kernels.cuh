@@ -14,6 +14,7 @@
 // forcefield.py:2011-2045,2294-2430, strain derivative forcefield.py:608-662,2628-2695.
 #pragma once
 #include "pgm_device.cuh"
+#include "pgm_nn.cuh"
 
 namespace pgm {
 
@@ -1066,6 +1067,111 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
       atomicAdd(&a.cg[s].acc_pap, v);
     }
   }
+}
+
+// ------------------------------------------------------------------ learned guess: features
+// One warp per atom over its pair row, edges with r < rg (the short-range graph): vector channels
+// (e nm) v0 = alpha_i b_i, v1 = mu_{n-1,i}, v2 = mu_{n-2,i}, and for each of them and 4 radial
+// bases phi_k(r) = exp(-((r - 0.1 (k + 1) nm) / 0.1 nm)^2) (cos(pi r / rg) + 1) / 2 the aggregates
+// A_ck = sum_j phi_k v_c,j and D_ck = sum_j phi_k (v_c,j . u) u (u = x / r); 16 rotation invariants
+// for the MLP (pgm_nn.cu).  The model mixes the 27 channels: the prediction turns with the system.
+template <typename T>
+__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *hist, float sigma, float rg, float *inv, float *vec) {
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
+  const size_t st = (size_t)a.nt * 3;
+  float acc[2][3][4][3];
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int x = 0; x < 3; ++x) acc[q][c][k][x] = 0.f;
+  int n = min(a.rn[i], a.mc);
+  size_t base = (size_t)i * a.mc;
+  for (int t = lane; t < n; t += 32) {
+    size_t o = base + t;
+    float x = float(a.rx[o]), y = float(a.ry[o]), z = float(a.rz[o]);
+    float r = sqrtf(x * x + y * y + z * z);
+    if (r >= rg) continue;
+    int j = a.rk[o];
+    float ir = 1.f / r, u[3] = {x * ir, y * ir, z * ir};
+    float fc = 0.5f * (cospif(r / rg) + 1.f);
+    float phi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float d = (r - 0.1f * (k + 1)) * 10.f;
+      phi[k] = expf(-d * d) * fc;
+    }
+    v4<T> bj = a.B[j];
+    float aj = float(a.alpha[j]);
+    float v[3][3] = {{aj * float(bj.x), aj * float(bj.y), aj * float(bj.z)},
+                     {float(hist[3 * j]), float(hist[3 * j + 1]), float(hist[3 * j + 2])},
+                     {float(hist[st + 3 * j]), float(hist[st + 3 * j + 1]), float(hist[st + 3 * j + 2])}};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float pr = v[c][0] * u[0] + v[c][1] * u[1] + v[c][2] * u[2];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int xx = 0; xx < 3; ++xx) {
+          acc[0][c][k][xx] += phi[k] * v[c][xx];
+          acc[1][c][k][xx] += phi[k] * pr * u[xx];
+        }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int x = 0; x < 3; ++x) acc[q][c][k][x] = warp_sum<float>(acc[q][c][k][x]);
+  if (lane != 0) return;
+  v4<T> bi = a.B[i];
+  float ai = float(a.alpha[i]);
+  float self[3][3] = {{ai * float(bi.x), ai * float(bi.y), ai * float(bi.z)},
+                      {float(hist[3 * i]), float(hist[3 * i + 1]), float(hist[3 * i + 2])},
+                      {float(hist[st + 3 * i]), float(hist[st + 3 * i + 1]), float(hist[st + 3 * i + 2])}};
+  float *V = vec + (size_t)i * pgmnn::NN_CH * 3;
+  for (int c = 0; c < 3; ++c)
+    for (int x = 0; x < 3; ++x) V[3 * c + x] = self[c][x];
+  for (int q = 0; q < 2; ++q)
+    for (int c = 0; c < 3; ++c)
+      for (int k = 0; k < 4; ++k)
+        for (int x = 0; x < 3; ++x) V[3 * (3 + q * 12 + c * 4 + k) + x] = acc[q][c][k][x];
+  auto dot = [](const float *p, const float *q) { return p[0] * q[0] + p[1] * q[1] + p[2] * q[2]; };
+  float is = 1.f / sigma, is2 = is * is;
+  float *F = inv + (size_t)i * pgmnn::NN_IN;
+  F[0] = ai * 1e3f;
+  F[1] = float(a.radius[i]) / 0.06f;
+  F[2] = sqrtf(dot(self[0], self[0])) * is;
+  F[3] = sqrtf(dot(self[1], self[1])) * is;
+  F[4] = sqrtf(dot(self[2], self[2])) * is;
+  F[5] = dot(self[0], self[1]) * is2;
+  F[6] = dot(self[1], self[2]) * is2;
+  F[7] = dot(self[0], self[2]) * is2;
+  for (int k = 0; k < 4; ++k) {
+    F[8 + k] = sqrtf(dot(acc[0][0][k], acc[0][0][k])) * is;
+    F[12 + k] = sqrtf(dot(acc[0][1][k], acc[0][1][k])) * is;
+  }
+}
+
+// x0 = the model's prediction for the systems with a history (count >= 2).
+template <typename T>
+__global__ void k_nn_set_x(Dev<T> a, const float *mu) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  if (!a.cg[a.sysid[i]].have) return;
+  v4<T> x;
+  x.x = T(mu[3 * i]); x.y = T(mu[3 * i + 1]); x.z = T(mu[3 * i + 2]); x.w = T(0);
+  a.X[i] = x;
 }
 
 // ------------------------------------------------------------------ CG

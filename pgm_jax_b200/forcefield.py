@@ -25,7 +25,7 @@ from . import _lib
 from .systems import System, grid_size
 
 ELEC_LEVELS = {"q": 0, "qp": 1, "qi": 2, "qpi": 3}
-PREDICTORS = {"none": 0, "mu3": 3, "mu4": 4}
+PREDICTORS = {"none": 0, "mu3": 3, "mu4": 4, "nn": 5}  # "nn": the learned guess (learned.py), mu4 until installed
 
 # The settings of MDSettings that this engine implements, with the reference's defaults
 # (forcefield.py:142-516).  Other reference settings (iEL, IPS, DE / GVDW, split rows, the local
@@ -73,7 +73,7 @@ class MDSettings:
         if self.vdw not in ("lj", "none"):
             raise ValueError(f"vdw {self.vdw!r}: this engine implements 'lj' and 'none'")
         if self.predictor not in PREDICTORS:
-            raise ValueError(f"unknown predictor {self.predictor!r} (mu4 | mu3 | none)")
+            raise ValueError(f"unknown predictor {self.predictor!r} (mu4 | mu3 | none | nn)")
         if self.precision not in ("mixed", "double"):
             raise ValueError(f"precision {self.precision!r} (mixed | double)")
         if not (self.cutoff > 0):

@@ -1,0 +1,138 @@
+"""The learned initial guess of the induced-dipole solve: data, training and use.
+
+A message-passing model on the short-range graph (edges r < 0.5 nm taken from the pair rows)
+predicts the converged induced dipoles of a step from the permanent field b of that step and the
+dipoles of the two previous steps; the engine's solver starts CG from the prediction (predictor
+"nn", an unfused start) and iterates to the same tolerance, so the plain solver judges the guess.
+The model (csrc/pgm_nn.cu): 16 rotation invariants -> MLP 64 -> 64 (SiLU) -> 27 coefficients that
+mix 27 vector channels per atom (csrc/pgm_kernels.cuh k_nn_features), so the prediction rotates
+with the system.  Training runs on the GPU with the project's BF16 tensor-core forward/backward
+kernels and Adam; the data are (features, converged dipoles) pairs written while the plain solver
+runs MD.  The reference has no counterpart (pgm_jax/md/forcefield.py:1917-2008 has the mu3, mu4
+and least-squares predictors only).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+
+N_IN, N_HID, N_OUT, N_CH = 16, 64, 32, 27
+SIGMA = 0.02  # e nm, scale of the invariants
+GRAPH_CUTOFF = 0.5  # nm
+
+
+def init_weights(seed: int = 0) -> np.ndarray:
+    """Flat FP32 weights (w1, b1, w2, b2, w3, b3): small random layers and an output bias that makes
+    the untrained model the linear extrapolation 2 mu_{n-1} - mu_{n-2}."""
+    rng = np.random.default_rng(seed)
+    w1 = rng.normal(scale=1.0 / np.sqrt(N_IN), size=(N_IN, N_HID))
+    w2 = rng.normal(scale=1.0 / np.sqrt(N_HID), size=(N_HID, N_HID))
+    w3 = rng.normal(scale=1e-3, size=(N_HID, N_OUT))
+    b3 = np.zeros(N_OUT)
+    b3[1], b3[2] = 2.0, -1.0
+    flat = np.concatenate([w1.ravel(), np.zeros(N_HID), w2.ravel(), np.zeros(N_HID), w3.ravel(), b3]).astype(np.float32)
+    assert flat.size == _lib.load().pgm_nn_param_count()
+    return flat
+
+
+def _p(t: torch.Tensor):
+    return C.c_void_p(t.data_ptr())
+
+
+def features(ff, pos: torch.Tensor, boxes: torch.Tensor, hist: torch.Tensor):
+    """Invariants (N, 16) and vector channels (N, 27, 3) of the learned guess at a geometry."""
+    n = ff.n
+    inv = torch.empty((n, N_IN), dtype=torch.float32, device=ff.device)
+    vec = torch.empty((n, N_CH, 3), dtype=torch.float32, device=ff.device)
+    _lib.check(ff._lib.pgm_nn_features(ff._h, ff._stream(), _p(pos), _p(boxes), _p(hist), _p(inv), _p(vec)))
+    return inv, vec
+
+
+class GuessModel:
+    """Device weights of the model with its Adam state."""
+
+    def __init__(self, weights: np.ndarray | None = None, device: int = 0, seed: int = 0) -> None:
+        self.dev = torch.device("cuda", device)
+        w = init_weights(seed) if weights is None else np.asarray(weights, np.float32)
+        self.w = torch.tensor(w, device=self.dev)
+        self.g = torch.zeros_like(self.w)
+        self.m = torch.zeros_like(self.w)
+        self.v = torch.zeros_like(self.w)
+        self.step = 0
+        self.lib = _lib.load()
+
+    def _stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def predict(self, inv: torch.Tensor, vec: torch.Tensor) -> torch.Tensor:
+        mu = torch.empty((inv.shape[0], 3), dtype=torch.float32, device=self.dev)
+        _lib.check(self.lib.pgm_nn_predict(self._stream(), _p(self.w), _p(inv), _p(vec), int(inv.shape[0]), _p(mu)))
+        return mu
+
+    def loss_grad(self, inv, vec, target, scale: float) -> float:
+        """Adds d loss / d w to self.g; returns loss = scale * sum |mu - target|^2."""
+        loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        _lib.check(self.lib.pgm_nn_loss_grad(self._stream(), _p(self.w), _p(inv), _p(vec), _p(target), int(inv.shape[0]),
+                                             float(scale), _p(self.g), _p(loss)))
+        return float(loss.item())
+
+    def adam(self, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
+        self.step += 1
+        _lib.check(self.lib.pgm_nn_adam(self._stream(), _p(self.w), _p(self.g), _p(self.m), _p(self.v), lr, beta1, beta2, eps,
+                                        self.step))
+
+    def train(self, data: dict, iters: int = 400, batch: int = 16384, lr: float = 2e-3, seed: int = 0, log=None) -> list:
+        """Adam on minibatches of (inv, vec, target) (dict of device tensors); returns the losses
+        (mean |mu - target|^2 / SIGMA^2 per atom)."""
+        n = data["inv"].shape[0]
+        g = torch.Generator(device=self.dev)
+        g.manual_seed(seed)
+        losses = []
+        for it in range(iters):
+            idx = torch.randint(0, n, (min(batch, n),), device=self.dev, generator=g)
+            scale = 1.0 / (idx.numel() * SIGMA**2)
+            loss = self.loss_grad(data["inv"][idx].contiguous(), data["vec"][idx].contiguous(), data["target"][idx].contiguous(),
+                                  scale)
+            lr_t = lr * 0.5 * (1.0 + np.cos(np.pi * it / iters))  # cosine decay
+            self.adam(lr=lr_t)
+            losses.append(loss)
+            if log and (it % 100 == 0 or it == iters - 1):
+                log(f"  train {it:5d}  loss {loss:.4e}")
+        return losses
+
+    def install(self, ff) -> None:
+        """Use the model as the solver's initial guess (predictor "nn")."""
+        _lib.check(ff._lib.pgm_set_nn_model(ff._h, _p(self.w), SIGMA, GRAPH_CUTOFF))
+
+
+def collect(md, steps: int, every: int = 1) -> dict:
+    """Run `steps` MD steps with the plain solver and keep (features, converged dipoles) of every
+    `every`-th step (once the history holds two steps)."""
+    ff = md.ff
+    keep = {"inv": [], "vec": [], "target": []}
+    for k in range(steps):
+        hist = md.ind.hist.clone()
+        count = int(md.ind.count.min())
+        md.step()
+        if count >= 2 and k % every == 0:
+            with torch.cuda.stream(md.stream):
+                inv, vec = features(ff, md.pos, md.box, hist)
+            md.stream.synchronize()
+            keep["inv"].append(inv)
+            keep["vec"].append(vec)
+            keep["target"].append(md.ind.mu.to(torch.float32).clone())
+    return {k: torch.cat(v) for k, v in keep.items()}
+
+
+def guess_errors(model: GuessModel, data: dict) -> dict:
+    """RMS error (e nm) of the model's guess and of the linear extrapolation 2 mu1 - mu2 on data."""
+    mu = model.predict(data["inv"], data["vec"])
+    lin = 2.0 * data["vec"][:, 1] - data["vec"][:, 2]
+    t = data["target"]
+    rms = lambda x: float(torch.sqrt(torch.mean((x - t) ** 2)))  # noqa: E731
+    return {"model": rms(mu), "linear": rms(lin), "target_rms": float(torch.sqrt(torch.mean(t * t)))}
