@@ -182,17 +182,20 @@ long long pgm_row_pairs(PgmHandle *h);
 /* ------------------------------------------------------------------ learned initial guess
  * No counterpart in the reference (its guesses are the mu3 / mu4 / ls predictors,
  * forcefield.py:1917-2008).  A message-passing model on the short-range graph predicts the
- * converged dipoles from the permanent field b and the last two steps' dipoles; with predictor 5
+ * converged dipoles from the permanent field b (of this step and the last) and the last two steps'
+ * dipoles; with predictor 5
  * the solve starts from that prediction (an unfused start: the field sweep for b, the features, the
  * model, the residual sweep) and CG iterates to the same tolerance.
  * Features per atom: 16 rotation invariants (float, (N, 16)) and 27 vector channels (float,
- * (N, 27, 3)): alpha b, mu_{n-1}, mu_{n-2} and their radial-basis neighbour sums over edges r < the
+ * (N, 27, 3)): alpha (b - b_prev), mu_{n-1}, mu_{n-2} and their radial-basis neighbour sums over edges r < the
  * graph cutoff, plain and projected on the edge direction.  The model (pgm_nn_param_count() floats,
  * device) is the MLP of pgm_nn_predict. */
 PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff);
-/* Features at a geometry: hist (4, N, 3) device (newest first, as PgmInduction.hist); inv, vec device. */
-PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist, float *inv,
-                          float *vec);
+/* Features at a geometry: hist (4, N, 3) device (newest first, as PgmInduction.hist); b_prev (N, 3)
+ * the permanent field of the previous step or NULL (channel 0 is then alpha b instead of
+ * alpha (b - b_prev)); b_out (N, 3) receives this step's permanent field (or NULL); inv, vec device. */
+PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist,
+                          const double *b_prev, double *b_out, float *inv, float *vec);
 int pgm_nn_param_count(void);
 /* mu (n, 3) = sum_c c_c(inv) vec_c with c = MLP(inv): BF16 tensor cores, FP32 accumulation. */
 PgmStatus pgm_nn_predict(void *stream, const float *weights, const float *inv, const float *vec, int n, float *mu);

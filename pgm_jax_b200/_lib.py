@@ -112,7 +112,7 @@ def load(path: str | None = None):
     lib.pgm_field_static.restype = C.c_int
     lib.pgm_static_last_error.restype = C.c_char_p
     lib.pgm_set_nn_model.argtypes = [H, vp, C.c_float, C.c_float]
-    lib.pgm_nn_features.argtypes = [H, vp, vp, vp, vp, vp, vp]
+    lib.pgm_nn_features.argtypes = [H, vp, vp, vp, vp, vp, vp, vp, vp]
     lib.pgm_nn_predict.argtypes = [vp, vp, vp, vp, C.c_int, vp]
     lib.pgm_nn_loss_grad.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_float, vp, vp]
     lib.pgm_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]

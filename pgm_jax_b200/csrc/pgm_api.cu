@@ -104,7 +104,8 @@ struct EngineBase {
                         const double *mu, double *energy, double *forces, double *virial, uint32_t *status) = 0;
   virtual void set_capacity(int mc) = 0;
   virtual void set_nn(const float *w, float sigma, float rg) = 0;
-  virtual void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, float *inv, float *vec) = 0;
+  virtual void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const double *bprev,
+                           double *b_out, float *inv, float *vec) = 0;
   virtual void set_list_capacity(int c) = 0;
   virtual int list_capacity() const = 0;
   virtual long long list_rebuilds() = 0;
@@ -174,7 +175,8 @@ struct Engine : EngineBase {
   DBuf<pgm::c2<T>> C, tw;
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
   DBuf<float> nn_w, nn_inv, nn_vec, nn_mu;  // learned guess: model and per-atom features
-  bool nn_on = false;
+  bool nn_on = false, nn_bprev_ok = false;
+  DBuf<pgm::v4<T>> nn_bprev;
   float nn_sigma = 0.02f, nn_rg = 0.5f;
   int *h_any = nullptr;
   const double *last_pos = nullptr;
@@ -433,7 +435,7 @@ struct Engine : EngineBase {
     CK(cudaMemset(Q.p, 0, sizeof(T) * rgrid));
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
     nn_w.alloc(pgmnn::NN_NPARAM); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
-    nn_mu.alloc((size_t)nt * 3);
+    nn_mu.alloc((size_t)nt * 3); nn_bprev.alloc(nt);
     CK(cudaMallocHost(&h_any, sizeof(int)));
     CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&aux_b, cudaStreamNonBlocking));
@@ -508,21 +510,25 @@ struct Engine : EngineBase {
 
   void set_nn(const float *w, float sigma, float rg) override {
     nn_on = w != nullptr;
+    nn_bprev_ok = false;
     if (w) CK(cudaMemcpy(nn_w.p, w, sizeof(float) * pgmnn::NN_NPARAM, cudaMemcpyDeviceToDevice));
     nn_sigma = sigma;
     nn_rg = rg;
   }
 
   // Features of the learned guess at a geometry (rows, the permanent field b, the history).
-  void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, float *inv, float *vec) override {
+  void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const double *bprev,
+                   double *b_out, float *inv, float *vec) override {
     launches = 0;
     CK(cudaMemsetAsync(d_status.p, 0, sizeof(unsigned) * nsys, st));
     pgm::Dev<T> a = dev(pos, nullptr, 0, forces_tmp.p, d_status.p);
     prepare(st, a, box);
     pgm::k_total_dipoles<T><<<grid1(nt), 256, 0, st>>>(a, nullptr); check_launch();
     sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
-    pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, hist, nn_sigma, nn_rg, inv ? inv : nn_inv.p, vec ? vec : nn_vec.p);
+    if (bprev) { pgm::k_vec_from_f64<T><<<grid1(nt), 256, 0, st>>>(nt, bprev, nn_bprev.p); check_launch(); }
+    pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, hist, bprev ? nn_bprev.p : nullptr, nn_sigma, nn_rg, inv, vec);
     check_launch();
+    if (b_out) { pgm::k_store_vec<T><<<grid1(nt), 256, 0, st>>>(a, Bv.p, b_out); check_launch(); }
   }
 
   void set_capacity(int c) override {
@@ -721,7 +727,11 @@ struct Engine : EngineBase {
     }
     sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
     if (use_nn) {
-      pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, ind->hist, nn_sigma, nn_rg, nn_inv.p, nn_vec.p); check_launch();
+      pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, ind->hist, nn_bprev_ok ? nn_bprev.p : nullptr, nn_sigma, nn_rg, nn_inv.p,
+                                                    nn_vec.p);
+      check_launch();
+      pgm::k_copy_vec<T><<<grid1(nt), 256, 0, st>>>(nt, Bv.p, nn_bprev.p); check_launch();  // b of this step for the next
+      nn_bprev_ok = true;
       cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st);
       if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
       ++launches;
@@ -1054,12 +1064,12 @@ PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, floa
   }
 }
 
-PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist, float *inv,
-                          float *vec) {
+PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist,
+                          const double *b_prev, double *b_out, float *inv, float *vec) {
   if (!h || !pos || !box || !hist || !inv || !vec) return fail(PGM_ERR_INVALID, "null argument");
   try {
     CK(cudaSetDevice(h->device));
-    h->eng->nn_features((cudaStream_t)stream, pos, box, hist, inv, vec);
+    h->eng->nn_features((cudaStream_t)stream, pos, box, hist, b_prev, b_out, inv, vec);
     return PGM_OK;
   } catch (CudaError &e) {
     return fail(PGM_ERR_CUDA, e.msg);

@@ -1071,12 +1071,14 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
 
 // ------------------------------------------------------------------ learned guess: features
 // One warp per atom over its pair row, edges with r < rg (the short-range graph): vector channels
-// (e nm) v0 = alpha_i b_i, v1 = mu_{n-1,i}, v2 = mu_{n-2,i}, and for each of them and 4 radial
+// (e nm) v0 = alpha_i (b_i - b_prev,i) (the change of the permanent field since the last step; b
+// itself without bprev), v1 = mu_{n-1,i}, v2 = mu_{n-2,i}, and for each of them and 4 radial
 // bases phi_k(r) = exp(-((r - 0.1 (k + 1) nm) / 0.1 nm)^2) (cos(pi r / rg) + 1) / 2 the aggregates
 // A_ck = sum_j phi_k v_c,j and D_ck = sum_j phi_k (v_c,j . u) u (u = x / r); 16 rotation invariants
 // for the MLP (pgm_nn.cu).  The model mixes the 27 channels: the prediction turns with the system.
 template <typename T>
-__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *hist, float sigma, float rg, float *inv, float *vec) {
+__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *hist, const v4<T> *bprev, float sigma, float rg,
+                                                     float *inv, float *vec) {
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
@@ -1109,6 +1111,7 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *his
       phi[k] = expf(-d * d) * fc;
     }
     v4<T> bj = a.B[j];
+    if (bprev) { v4<T> q = bprev[j]; bj.x -= q.x; bj.y -= q.y; bj.z -= q.z; }
     float aj = float(a.alpha[j]);
     float v[3][3] = {{aj * float(bj.x), aj * float(bj.y), aj * float(bj.z)},
                      {float(hist[3 * j]), float(hist[3 * j + 1]), float(hist[3 * j + 2])},
@@ -1135,6 +1138,7 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *his
         for (int x = 0; x < 3; ++x) acc[q][c][k][x] = warp_sum<float>(acc[q][c][k][x]);
   if (lane != 0) return;
   v4<T> bi = a.B[i];
+  if (bprev) { v4<T> q = bprev[i]; bi.x -= q.x; bi.y -= q.y; bi.z -= q.z; }
   float ai = float(a.alpha[i]);
   float self[3][3] = {{ai * float(bi.x), ai * float(bi.y), ai * float(bi.z)},
                       {float(hist[3 * i]), float(hist[3 * i + 1]), float(hist[3 * i + 2])},
@@ -1161,6 +1165,21 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *his
     F[8 + k] = sqrtf(dot(acc[0][0][k], acc[0][0][k])) * is;
     F[12 + k] = sqrtf(dot(acc[0][1][k], acc[0][1][k])) * is;
   }
+}
+
+template <typename T>
+__global__ void k_copy_vec(int n, const v4<T> *src, v4<T> *dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i];
+}
+
+template <typename T>
+__global__ void k_vec_from_f64(int n, const double *src, v4<T> *dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  v4<T> d;
+  d.x = T(src[3 * i]); d.y = T(src[3 * i + 1]); d.z = T(src[3 * i + 2]); d.w = T(0);
+  dst[i] = d;
 }
 
 // x0 = the model's prediction for the systems with a history (count >= 2).

@@ -1,8 +1,9 @@
 """The learned initial guess of the induced-dipole solve: data, training and use.
 
 A message-passing model on the short-range graph (edges r < 0.5 nm taken from the pair rows)
-predicts the converged induced dipoles of a step from the permanent field b of that step and the
-dipoles of the two previous steps; the engine's solver starts CG from the prediction (predictor
+predicts the converged induced dipoles of a step from the permanent field b (of that step and the
+previous one: the change alpha (b_n - b_{n-1}) is its response channel) and the dipoles of the two
+previous steps; the engine's solver starts CG from the prediction (predictor
 "nn", an unfused start) and iterates to the same tolerance, so the plain solver judges the guess.
 The model (csrc/pgm_nn.cu): 16 rotation invariants -> MLP 64 -> 64 (SiLU) -> 27 coefficients that
 mix 27 vector channels per atom (csrc/pgm_kernels.cuh k_nn_features), so the prediction rotates
@@ -32,7 +33,7 @@ def init_weights(seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed)
     w1 = rng.normal(scale=1.0 / np.sqrt(N_IN), size=(N_IN, N_HID))
     w2 = rng.normal(scale=1.0 / np.sqrt(N_HID), size=(N_HID, N_HID))
-    w3 = rng.normal(scale=1e-3, size=(N_HID, N_OUT))
+    w3 = np.zeros((N_HID, N_OUT))  # the untrained model is exactly the extrapolation
     b3 = np.zeros(N_OUT)
     b3[1], b3[2] = 2.0, -1.0
     flat = np.concatenate([w1.ravel(), np.zeros(N_HID), w2.ravel(), np.zeros(N_HID), w3.ravel(), b3]).astype(np.float32)
@@ -44,13 +45,17 @@ def _p(t: torch.Tensor):
     return C.c_void_p(t.data_ptr())
 
 
-def features(ff, pos: torch.Tensor, boxes: torch.Tensor, hist: torch.Tensor):
-    """Invariants (N, 16) and vector channels (N, 27, 3) of the learned guess at a geometry."""
+def features(ff, pos: torch.Tensor, boxes: torch.Tensor, hist: torch.Tensor, b_prev: torch.Tensor | None = None):
+    """Invariants (N, 16), vector channels (N, 27, 3) and the permanent field b (N, 3) at a geometry.
+
+    b_prev: the previous step's b (then channel 0 is alpha (b - b_prev), as in the solver)."""
     n = ff.n
     inv = torch.empty((n, N_IN), dtype=torch.float32, device=ff.device)
     vec = torch.empty((n, N_CH, 3), dtype=torch.float32, device=ff.device)
-    _lib.check(ff._lib.pgm_nn_features(ff._h, ff._stream(), _p(pos), _p(boxes), _p(hist), _p(inv), _p(vec)))
-    return inv, vec
+    b = torch.empty((n, 3), dtype=torch.float64, device=ff.device)
+    _lib.check(ff._lib.pgm_nn_features(ff._h, ff._stream(), _p(pos), _p(boxes), _p(hist),
+                                       None if b_prev is None else _p(b_prev), _p(b), _p(inv), _p(vec)))
+    return inv, vec, b
 
 
 class GuessModel:
@@ -115,17 +120,21 @@ def collect(md, steps: int, every: int = 1) -> dict:
     `every`-th step (once the history holds two steps)."""
     ff = md.ff
     keep = {"inv": [], "vec": [], "target": []}
+    b_prev = None
     for k in range(steps):
-        hist = md.ind.hist.clone()
+        md.stream.synchronize()
         count = int(md.ind.count.min())
+        with torch.cuda.stream(md.stream):  # everything on the MD stream, in order
+            hist = md.ind.hist.clone()
         md.step()
-        if count >= 2 and k % every == 0:
-            with torch.cuda.stream(md.stream):
-                inv, vec = features(ff, md.pos, md.box, hist)
-            md.stream.synchronize()
+        with torch.cuda.stream(md.stream):
+            inv, vec, b = features(ff, md.pos, md.box, hist, b_prev)
+        md.stream.synchronize()
+        if count >= 2 and b_prev is not None and k % every == 0:
             keep["inv"].append(inv)
             keep["vec"].append(vec)
             keep["target"].append(md.ind.mu.to(torch.float32).clone())
+        b_prev = b
     return {k: torch.cat(v) for k, v in keep.items()}
 
 

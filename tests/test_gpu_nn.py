@@ -52,8 +52,9 @@ def test_features_turn_with_the_system():
     hist = rng.normal(scale=0.01, size=(4, s.n, 3))
     R = np.array([[0.0, -1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
     pos_r = (pos @ R.T) % 1.25
-    inv0, vec0 = features(ff, _dev(pos, torch.float64), _dev(H[None], torch.float64), _dev(hist, torch.float64))
-    inv1, vec1 = features(ff, _dev(pos_r, torch.float64), _dev(H[None], torch.float64), _dev(hist @ R.T, torch.float64))
+    inv0, vec0, b0 = features(ff, _dev(pos, torch.float64), _dev(H[None], torch.float64), _dev(hist, torch.float64))
+    inv1, vec1, b1 = features(ff, _dev(pos_r, torch.float64), _dev(H[None], torch.float64), _dev(hist @ R.T, torch.float64))
+    assert np.abs(b0.cpu().numpy() @ R.T - b1.cpu().numpy()).max() <= 1e-8 * float(b0.abs().max())
     inv0, inv1 = inv0.cpu().numpy(), inv1.cpu().numpy()
     assert np.abs(inv0 - inv1).max() <= 1e-4 * max(1.0, np.abs(inv0).max())
     v0, v1 = vec0.cpu().numpy(), vec1.cpu().numpy()
@@ -79,7 +80,8 @@ def test_trained_guess_beats_extrapolation_and_solves_to_tolerance():
     before = guess_errors(model, held)
     model.train(train, iters=400, batch=8192, lr=2e-3)
     after = guess_errors(model, held)
-    assert after["model"] < 0.9 * before["linear"], (before, after)
+    assert abs(before["model"] - before["linear"]) <= 1e-3 * before["linear"]  # untrained = extrapolation
+    assert after["model"] < 0.8 * before["linear"], (before, after)
     model.install(ff)
     its = []
     for _ in range(8):
