@@ -240,6 +240,7 @@ def run_engine(args) -> None:
     # end to end: the force call through the C ABI with host buffers (positions in, forces out and
     # the induction state in and out every step), the integrator on the GPU
     e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
+    nn = run_nn_guess(s, pos, H, rank, args, torch) if args.nn else None
     value = ws * ns_per_day(ms_max)
     if rank == 0:
         line = {
@@ -259,6 +260,8 @@ def run_engine(args) -> None:
             "e2e": e2e,
             "published_reference": "44 ns/day, 4096 waters, mixed, tol 1e-5, 1x RTX PRO 6000 Blackwell (README.md:448)",
         }
+        if nn is not None:
+            line["nn_guess"] = nn
         if args.cpu_baseline:
             r = cpu_reference(3, 1, budget_s=40.0)
             line["cpu_baseline"] = {"value": r["value"], "unit": "ns/day", "cores": r["cores"], "kind": "port",
@@ -268,6 +271,48 @@ def run_engine(args) -> None:
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_nn_guess(s, pos, H, rank, args, torch) -> dict:
+    """The learned guess on the same workload: plain-solver MD writes (features, converged dipoles),
+    the model trains on the GPU, then graph-replayed MD starts every CG from its prediction (the
+    unfused start: one more field sweep per step than the fused mu4 start)."""
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.learned import GuessModel, collect, guess_errors
+    from pgm_jax_b200.md import RigidMD
+
+    st = settings()
+    ff = PGMForceField(s, H, MDSettings(**{**st.__dict__, "predictor": "nn"}), device=torch.cuda.current_device())
+    md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=11 + rank)
+    t0 = time.perf_counter()
+    train = collect(md, 24)
+    held = collect(md, 4)
+    model = GuessModel(seed=0)
+    before = guess_errors(model, held)
+    model.train(train, iters=600, batch=32768, lr=2e-3)
+    after = guess_errors(model, held)
+    t_train = time.perf_counter() - t0
+    model.install(ff)
+    for _ in range(3):
+        md.step()
+    md.capture()
+    md.run(3)
+    md.stream.synchronize()
+    steps = max(10, min(args.steps, 200))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    it_sum = torch.zeros((), dtype=torch.int64, device=ff.device)
+    ev0.record(md.stream)
+    for _ in range(steps):
+        md.run(1)
+        with torch.cuda.stream(md.stream):
+            it_sum += ff._iters[0].to(torch.int64)
+    ev1.record(md.stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "cg_iters_per_step": float(it_sum.item()) / steps,
+            "steps": steps, "guess_rms_e_nm": {"untrained_linear_extrapolation": before["linear"], "trained": after["model"]},
+            "train_frames": 24, "train_samples": int(train["inv"].shape[0]), "train_seconds": t_train,
+            "start": "unfused: field sweep for b, features + model, residual sweep (the mu4 start is one fused sweep)"}
 
 
 def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
@@ -331,6 +376,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-nn", dest="nn", action="store_false", help="skip the learned-guess comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
