@@ -1,11 +1,16 @@
-"""Benchmark: pGM rigid-water MD on the B200 engine, ns/day and CG iterations per step.
+"""Benchmark: pGM rigid-water MD on the B200 engine, ns/day and CG iterations per step, with the
+learned initial guess against plain CG.
 
 Workload (one GPU): 4096 pGM3P-25 waters (12,288 atoms) on a seeded jittered 16^3 lattice in a
 4.966 nm cubic box, cutoff 0.9 nm, Ewald 4.0 / nm, PME 96^3 order 6, mixed precision (FP32 pair /
 PME / CG vectors, FP64 reductions), Langevin NVT 298 K with gamma 2 / ps, dt 1 fs, CG to max|alpha
-r| / mean|alpha b| <= 1e-6 from the mu4 predictor (the plain solver).  A step is one captured CUDA
-graph: rigid-body kick/drift/Langevin, the force call (rows, PME, CG as a device-side while loop,
-energy / forces / virial), closing kick.
+r| / mean|alpha b| <= 1e-6.  A step is one captured CUDA graph: rigid-body kick/drift/Langevin, the
+force call (rows, PME, CG as a device-side while loop, energy / forces / virial), closing kick.
+
+The headline run starts every solve from the learned guess (mu4 + the model's correction, fused
+start): plain-solver MD on the same workload writes the training pairs, the model trains on the GPU
+(outside the timed region), then the timed MD uses it.  Beside it, the same MD with plain CG from
+the previous step's dipoles (mu1) and from the reference's default mu4 predictor.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -36,23 +41,23 @@ DT_FS, GAMMA, TEMP, TOL = 1.0, 2.0, 298.0, 1e-6
 METRIC = "ns/day & CG iters/step on 1 B200: NN-guess vs plain CG at residual≤1e-6"
 CONFIG = {
     "workload": "4096 rigid pGM3P-25 waters, 4.966 nm box, PME 96^3 o6, rc 0.9 nm, beta 4.0/nm, Langevin 298 K "
-    "gamma 2/ps, dt 1 fs, mixed precision, CG tol 1e-6 (plain CG from the mu4 predictor)",
+    "gamma 2/ps, dt 1 fs, mixed precision, CG tol 1e-6 from the learned guess",
     "atoms": 12288,
     "pme_grid": [GRID, GRID, GRID],
     "cutoff_nm": 0.9,
     "dt_fs": DT_FS,
     "cg_tol": TOL,
-    "solver": "plain CG (mu4 predictor, fused start)",
+    "solver": "CG from mu4 + the learned correction (fused start); plain CG from mu1 and mu4 beside it",
     "l2": "working set larger than L2: pair rows 8 x 4 B x 12288 x capacity = 164 MB (126 MB L2)",
     "seeds": {"positions": 0, "velocities_thermostat": 1},
 }
 
 
-def settings(precision="mixed"):
+def settings(precision="mixed", predictor="mu4"):
     from pgm_jax_b200.forcefield import MDSettings
 
     return MDSettings(precision=precision, cutoff=0.9, ewald_beta=4.0, pme_grid=(GRID, GRID, GRID), pme_order=6,
-                      dipole_tol=TOL, max_iter=100, predictor="mu4")
+                      dipole_tol=TOL, max_iter=100, predictor=predictor)
 
 
 def ns_per_day(ms_per_step: float) -> float:
@@ -188,9 +193,10 @@ def run_engine(args) -> None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     s, pos, H = water_box(N_SIDE, EDGE_NM, seed=0)
-    ff = PGMForceField(s, H, settings(), device=local)
+    ff = PGMForceField(s, H, settings(predictor="nn" if args.nn else "mu4"), device=local)
     md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
     lib = ff._lib
+    train_info = train_guess(md, ff) if args.nn else None  # plain-solver MD writes the data; GPU training
     # warm-up: direct steps (rows sized), then capture and replay
     for _ in range(max(1, args.warmup)):
         md.step()
@@ -200,23 +206,12 @@ def run_engine(args) -> None:
     md.stream.synchronize()
     it0 = int(md.result.iterations[0])
     # timed region: K graph replays between CUDA events on the MD stream; clocks sampled meanwhile
-    iters = []
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     clk = Clocks(local)
-    ev0.record(md.stream)
-    it_sum = torch.zeros((), dtype=torch.int64, device=dev)
-    for _ in range(args.steps):
-        md.run(1)
-        with torch.cuda.stream(md.stream):
-            it_sum += md.result.iterations[0].to(torch.int64)
-    ev1.record(md.stream)
-    torch.cuda.synchronize(dev)
+    ms, n_it = timed_replays(md, args.steps, torch)
     clocks = clk.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    n_it = float(it_sum.item()) / args.steps
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if ws > 1:
         dist.barrier()
@@ -229,7 +224,7 @@ def run_engine(args) -> None:
     kt = {}
     for which, name in ((0, "cg_matvec_fused"), (1, "spread"), (2, "fft_chain"), (3, "forces"), (4, "rows"),
                         (5, "fft_x_fwd_alone"), (6, "spread_then_fft_x_fwd"), (7, "row_field"), (8, "pme_gather"),
-                        (9, "cg_sweep")):
+                        (9, "cg_sweep")) + (((10, "nn_chan"), (11, "nn_features"), (12, "nn_model")) if args.nn else ()):
         v = C_double()
         _lib.check(lib.pgm_profile_kernel(ff._h, C_void_p(md.stream.cuda_stream), which, 20, byref(v)))
         kt[name] = v.value
@@ -240,7 +235,8 @@ def run_engine(args) -> None:
     # end to end: the force call through the C ABI with host buffers (positions in, forces out and
     # the induction state in and out every step), the integrator on the GPU
     e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
-    nn = run_nn_guess(s, pos, H, rank, args, torch) if args.nn else None
+    # plain CG on the same workload: from the previous step's dipoles and from mu4
+    plain = {p: run_plain(s, pos, H, rank, p, args, torch) for p in (("mu1", "mu4") if args.nn else ())}
     value = ws * ns_per_day(ms_max)
     if rank == 0:
         line = {
@@ -260,8 +256,10 @@ def run_engine(args) -> None:
             "e2e": e2e,
             "published_reference": "44 ns/day, 4096 waters, mixed, tol 1e-5, 1x RTX PRO 6000 Blackwell (README.md:448)",
         }
-        if nn is not None:
-            line["nn_guess"] = nn
+        if args.nn:
+            line["learned_guess"] = train_info
+            line["plain_cg"] = plain
+            line["nn_over_plain_cg"] = {p: ns_per_day(ms_max) / v["value"] for p, v in plain.items()}
         if args.cpu_baseline:
             r = cpu_reference(3, 1, budget_s=40.0)
             line["cpu_baseline"] = {"value": r["value"], "unit": "ns/day", "cores": r["cores"], "kind": "port",
@@ -273,46 +271,57 @@ def run_engine(args) -> None:
         dist.destroy_process_group()
 
 
-def run_nn_guess(s, pos, H, rank, args, torch) -> dict:
-    """The learned guess on the same workload: plain-solver MD writes (features, converged dipoles),
-    the model trains on the GPU, then graph-replayed MD starts every CG from its prediction (the
-    unfused start: one more field sweep per step than the fused mu4 start)."""
-    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
-    from pgm_jax_b200.learned import GuessModel, collect, guess_errors
-    from pgm_jax_b200.md import RigidMD
-
-    st = settings()
-    ff = PGMForceField(s, H, MDSettings(**{**st.__dict__, "predictor": "nn"}), device=torch.cuda.current_device())
-    md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=11 + rank)
-    t0 = time.perf_counter()
-    train = collect(md, 24)
-    held = collect(md, 4)
-    model = GuessModel(seed=0)
-    before = guess_errors(model, held)
-    model.train(train, iters=600, batch=32768, lr=2e-3)
-    after = guess_errors(model, held)
-    t_train = time.perf_counter() - t0
-    model.install(ff)
-    for _ in range(3):
-        md.step()
-    md.capture()
-    md.run(3)
-    md.stream.synchronize()
-    steps = max(10, min(args.steps, 200))
+def timed_replays(md, steps: int, torch) -> tuple:
+    """(ms per step, mean CG iterations) of `steps` graph replays, CUDA events on the MD stream."""
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    it_sum = torch.zeros((), dtype=torch.int64, device=ff.device)
+    it_sum = torch.zeros((), dtype=torch.int64, device=md.ff.device)
     ev0.record(md.stream)
     for _ in range(steps):
         md.run(1)
         with torch.cuda.stream(md.stream):
-            it_sum += ff._iters[0].to(torch.int64)
+            it_sum += md.result.iterations[0].to(torch.int64)
     ev1.record(md.stream)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / steps
-    return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "cg_iters_per_step": float(it_sum.item()) / steps,
-            "steps": steps, "guess_rms_e_nm": {"untrained_linear_extrapolation": before["linear"], "trained": after["model"]},
-            "train_frames": 24, "train_samples": int(train["inv"].shape[0]), "train_seconds": t_train,
-            "start": "unfused: field sweep for b, features + model, residual sweep (the mu4 start is one fused sweep)"}
+    torch.cuda.synchronize(md.ff.device)
+    return ev0.elapsed_time(ev1) / steps, float(it_sum.item()) / steps
+
+
+def train_guess(md, ff, frames: int = 24, held_frames: int = 4, iters: int = 600) -> dict:
+    """Plain-solver MD (mu4 until a model is installed) writes (features, mu* - mu4 guess) pairs;
+    the model trains on the GPU and is installed; guess errors on held-out frames."""
+    from pgm_jax_b200.learned import GuessModel, collect, guess_errors
+
+    t0 = time.perf_counter()
+    train = collect(md, frames)
+    held = collect(md, held_frames)
+    model = GuessModel(seed=0, device=ff.device.index)
+    before = guess_errors(model, held)
+    model.train(train, iters=iters, batch=32768, lr=2e-3)
+    after = guess_errors(model, held)
+    model.install(ff)
+    return {"train_frames": frames, "train_pairs": int(train["inv"].shape[0]), "adam_steps": iters,
+            "seconds": time.perf_counter() - t0,
+            "guess_rms_e_nm_held_out": {"mu1": before["mu1"], "mu4": before["mu4"], "mu4_plus_model": after["model"]},
+            "start": "x0 = mu4 + the model's correction, fused start (one field sweep, as mu4)"}
+
+
+def run_plain(s, pos, H, rank, predictor, args, torch) -> dict:
+    """The same MD with plain CG from `predictor`, graph-replayed and timed like the headline."""
+    from pgm_jax_b200.forcefield import PGMForceField
+    from pgm_jax_b200.md import RigidMD
+
+    ff = PGMForceField(s, H, settings(predictor=predictor), device=torch.cuda.current_device())
+    md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
+    for _ in range(max(1, args.warmup) + 4):
+        md.step()
+    md.capture()
+    md.run(3)
+    md.stream.synchronize()
+    steps = max(10, min(args.steps, 300))
+    ms, n_it = timed_replays(md, steps, torch)
+    del md
+    return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "cg_iters_per_step": n_it, "steps": steps,
+            "predictor": {"mu1": "previous step's dipoles", "mu4": "4 mu1 - 6 mu2 + 4 mu3 - mu4 (the reference's default)"}[
+                predictor]}
 
 
 def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
@@ -376,7 +385,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--no-nn", dest="nn", action="store_false", help="skip the learned-guess comparison")
+    ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

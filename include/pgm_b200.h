@@ -55,8 +55,9 @@ typedef struct {
     int pme_order;      /* 4, 6 or 8 (PMESettings.order) */
     double dipole_tol;  /* max|alpha r| / mean|alpha b| (Induction.tol) */
     int max_iter;       /* Induction.max_iter */
-    int predictor;      /* 0 "none", 3 "mu3", 4 "mu4" (Induction.predictor); 5 the learned guess
-                           (pgm_set_nn_model; mu4 until a model is set) */
+    int predictor;      /* 0 "none", 3 "mu3", 4 "mu4" (Induction.predictor); 1 the previous step's
+                           dipoles; 5 mu4 + the learned correction (pgm_set_nn_model; mu4 until
+                           a model is set) */
     int fused;          /* Induction.fused */
     int norm_refresh;   /* Induction.norm_refresh */
     double peek;        /* Induction.peek */
@@ -172,8 +173,9 @@ long long pgm_launches_per_iteration(const PgmHandle *h);
  * gather in one kernel), 1 the PME spread, 2 the five FFT/convolution passes, 3 the energy/force
  * pass, 4 the row build, 5 the first FFT pass alone, 6 a spread followed by the first FFT pass,
  * 7 the row field alone, 8 the PME gather + operator assembly alone, 9 a whole operator sweep as
- * the solver runs it (spread, row field beside the FFT chain, gather).  The last pgm_compute's
- * position array must still be valid. */
+ * the solver runs it (spread, row field beside the FFT chain, gather), 10 the learned guess's
+ * channel pass, 11 its feature pass, 12 its model.  The last pgm_compute's position (and, for 10,
+ * induction history) arrays must still be valid. */
 PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, double *ms_per_launch);
 
 /* In-cutoff pairs (both rows of every pair) of the last step's row build. */
@@ -181,21 +183,24 @@ long long pgm_row_pairs(PgmHandle *h);
 
 /* ------------------------------------------------------------------ learned initial guess
  * No counterpart in the reference (its guesses are the mu3 / mu4 / ls predictors,
- * forcefield.py:1917-2008).  A message-passing model on the short-range graph predicts the
- * converged dipoles from the permanent field b (of this step and the last) and the last two steps'
- * dipoles; with predictor 5
- * the solve starts from that prediction (an unfused start: the field sweep for b, the features, the
- * model, the residual sweep) and CG iterates to the same tolerance.
- * Features per atom: 16 rotation invariants (float, (N, 16)) and 27 vector channels (float,
- * (N, 27, 3)): alpha (b - b_prev), mu_{n-1}, mu_{n-2} and their radial-basis neighbour sums over edges r < the
- * graph cutoff, plain and projected on the edge direction.  The model (pgm_nn_param_count() floats,
- * device) is the MLP of pgm_nn_predict. */
+ * forcefield.py:1917-2008).  A message-passing model on the short-range graph (edges r < the graph
+ * cutoff) predicts the correction mu* - x4 to the mu4 extrapolation x4 of the converged dipoles,
+ * from the change of the graph's permanent field since the last step and the last steps' dipoles.
+ * With predictor 5 the solve starts from x4 + the prediction, with mu4's fused start (one field
+ * sweep), and CG iterates to the same tolerance; the untrained (zero) model is mu4.
+ * Per-atom channels (N, 12) floats: c0 = alpha (b - b_prev) (b: the real-space field of charges and
+ * permanent dipoles over the graph), c1 = mu1 - mu2, c2 = x4 - mu1, mu1.  Features: 16 rotation
+ * invariants (float, (N, 16)) and 27 vector channels (float, (N, 27, 3)): c0..c2 and their
+ * radial-basis sums over the graph, plain and projected on the edge direction.  The model
+ * (pgm_nn_param_count() floats, device) is the MLP of pgm_nn_predict; sigma is the scale of the
+ * per-step changes in the invariants [e nm]. */
 PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff);
-/* Features at a geometry: hist (4, N, 3) device (newest first, as PgmInduction.hist); b_prev (N, 3)
- * the permanent field of the previous step or NULL (channel 0 is then alpha b instead of
- * alpha (b - b_prev)); b_out (N, 3) receives this step's permanent field (or NULL); inv, vec device. */
+/* Features at a geometry: hist (4, N, 3) device (newest first, as PgmInduction.hist); bl_prev (N, 4)
+ * floats, the graph's permanent field of the previous step, or NULL (c0 = 0); bl_out (N, 4)
+ * receives this step's; inv, vec device.  Uses the sigma and graph cutoff of pgm_set_nn_model
+ * (before any: 2e-4 e nm and 0.5 nm). */
 PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist,
-                          const double *b_prev, double *b_out, float *inv, float *vec);
+                          const float *bl_prev, float *bl_out, float *inv, float *vec);
 int pgm_nn_param_count(void);
 /* mu (n, 3) = sum_c c_c(inv) vec_c with c = MLP(inv): BF16 tensor cores, FP32 accumulation. */
 PgmStatus pgm_nn_predict(void *stream, const float *weights, const float *inv, const float *vec, int n, float *mu);

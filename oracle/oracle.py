@@ -96,7 +96,7 @@ class Oracle:
         )
         st = dict(settings)
         elec = st.get("elec", "qpi")
-        pred = {"none": 0, "mu3": 3, "mu4": 4}[st.get("predictor", "mu4")]
+        pred = {"none": 0, "mu1": 1, "mu3": 3, "mu4": 4}[st.get("predictor", "mu4")]
         K = st["pme_grid"]
         self._set = _Set(
             int("p" in elec), int("i" in elec), int(st.get("vdw", "lj") == "lj"), int(st.get("lj_lrc", True)),

@@ -616,9 +616,10 @@ static void solve(ctx_t *C, const double *q, const double *pdip, double *mu, dou
     const double *al = C->sys->alpha;
     double *x0 = calloc(m, sizeof(double)), *r0 = malloc(sizeof(double) * m), *b = malloc(sizeof(double) * m),
            *dd = malloc(sizeof(double) * m), *Ax = malloc(sizeof(double) * m);
-    static const double c4[4] = {4.0, -6.0, 4.0, -1.0}, c3[3] = {3.0, -3.0, 1.0};
-    int K = s->predictor == 4 ? 4 : (s->predictor == 3 ? 3 : 0);
-    const double *cc = K == 4 ? c4 : c3;
+    /* mu3 / mu4 extrapolations (forcefield.py:605); predictor 1 = the previous step's dipoles */
+    static const double c4[4] = {4.0, -6.0, 4.0, -1.0}, c3[3] = {3.0, -3.0, 1.0}, c1[1] = {1.0};
+    int K = s->predictor == 4 ? 4 : (s->predictor == 3 ? 3 : (s->predictor == 1 ? 1 : 0));
+    const double *cc = K == 4 ? c4 : (K == 3 ? c3 : c1);
     int have = K > 0 && *count >= K;
     if (have)
         for (int j = 0; j < K; ++j)

@@ -104,8 +104,8 @@ struct EngineBase {
                         const double *mu, double *energy, double *forces, double *virial, uint32_t *status) = 0;
   virtual void set_capacity(int mc) = 0;
   virtual void set_nn(const float *w, float sigma, float rg) = 0;
-  virtual void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const double *bprev,
-                           double *b_out, float *inv, float *vec) = 0;
+  virtual void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const float *bl_prev,
+                           float *bl_out, float *inv, float *vec) = 0;
   virtual void set_list_capacity(int c) = 0;
   virtual int list_capacity() const = 0;
   virtual long long list_rebuilds() = 0;
@@ -113,6 +113,7 @@ struct EngineBase {
   virtual int max_count() = 0;
   virtual long long launches_per_iteration() const = 0;
   virtual double profile(cudaStream_t st, int which, int reps) = 0;
+  virtual bool has_hist() const = 0;
   virtual long long row_pairs() = 0;
   int nt = 0, nsys = 0;
   double *host_scratch = nullptr;  // device block of pgm_compute_host (allocated on first use)
@@ -174,10 +175,12 @@ struct Engine : EngineBase {
   DBuf<T> Q, Phi, Ginf;
   DBuf<pgm::c2<T>> C, tw;
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
-  DBuf<float> nn_w, nn_inv, nn_vec, nn_mu;  // learned guess: model and per-atom features
-  bool nn_on = false, nn_bprev_ok = false;
-  DBuf<pgm::v4<T>> nn_bprev;
-  float nn_sigma = 0.02f, nn_rg = 0.5f;
+  DBuf<float> nn_w, nn_inv, nn_vec, nn_mu, nn_chan;  // learned guess: model and per-atom features
+  bool nn_on = false;
+  const double *last_hist = nullptr;  // the history of the last predictor solve (profiling)
+  DBuf<float4> nn_bl;  // the graph's permanent field of the last solve (for the change channel)
+  DBuf<int> nn_valid;  // nn_bl holds a previous step
+  float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
   int *h_any = nullptr;
   const double *last_pos = nullptr;
   cudaStream_t side = nullptr, aux = nullptr, aux_b = nullptr;
@@ -435,7 +438,8 @@ struct Engine : EngineBase {
     CK(cudaMemset(Q.p, 0, sizeof(T) * rgrid));
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
     nn_w.alloc(pgmnn::NN_NPARAM); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
-    nn_mu.alloc((size_t)nt * 3); nn_bprev.alloc(nt);
+    nn_mu.alloc((size_t)nt * 3); nn_chan.alloc((size_t)nt * pgm::NN_CHAN); nn_bl.alloc(nt); nn_valid.alloc(1);
+    CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
     CK(cudaMallocHost(&h_any, sizeof(int)));
     CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&aux_b, cudaStreamNonBlocking));
@@ -510,25 +514,28 @@ struct Engine : EngineBase {
 
   void set_nn(const float *w, float sigma, float rg) override {
     nn_on = w != nullptr;
-    nn_bprev_ok = false;
     if (w) CK(cudaMemcpy(nn_w.p, w, sizeof(float) * pgmnn::NN_NPARAM, cudaMemcpyDeviceToDevice));
+    CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
     nn_sigma = sigma;
     nn_rg = rg;
   }
 
-  // Features of the learned guess at a geometry (rows, the permanent field b, the history).
-  void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const double *bprev,
-                   double *b_out, float *inv, float *vec) override {
+  // The model's inputs at a geometry: rows, then the graph's permanent field (written to bl_out;
+  // its change from bl_prev, when given, is a channel) and the history channels.
+  void nn_inputs(cudaStream_t st, pgm::Dev<T> &a, const double *hist, const float4 *bl_prev, const int *valid, float4 *bl_out,
+                 float *inv, float *vec, int *set_valid) {
+    pgm::k_nn_chan<T><<<nwblk, 256, 0, st>>>(a, hist, bl_prev, valid, nn_rg, bl_out, nn_chan.p); check_launch();
+    pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, nn_chan.p, nn_sigma, nn_rg, inv, vec, set_valid); check_launch();
+  }
+
+  void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const float *bl_prev,
+                   float *bl_out, float *inv, float *vec) override {
     launches = 0;
     CK(cudaMemsetAsync(d_status.p, 0, sizeof(unsigned) * nsys, st));
     pgm::Dev<T> a = dev(pos, nullptr, 0, forces_tmp.p, d_status.p);
     prepare(st, a, box);
-    pgm::k_total_dipoles<T><<<grid1(nt), 256, 0, st>>>(a, nullptr); check_launch();
-    sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
-    if (bprev) { pgm::k_vec_from_f64<T><<<grid1(nt), 256, 0, st>>>(nt, bprev, nn_bprev.p); check_launch(); }
-    pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, hist, bprev ? nn_bprev.p : nullptr, nn_sigma, nn_rg, inv, vec);
-    check_launch();
-    if (b_out) { pgm::k_store_vec<T><<<grid1(nt), 256, 0, st>>>(a, Bv.p, b_out); check_launch(); }
+    nn_inputs(st, a, hist, reinterpret_cast<const float4 *>(bl_prev), nullptr, reinterpret_cast<float4 *>(bl_out), inv, vec,
+              nullptr);
   }
 
   void set_capacity(int c) override {
@@ -544,6 +551,7 @@ struct Engine : EngineBase {
   // Average duration [ms] of one launch of a kernel of the last step, re-run `reps` times on the
   // state that step left (rows, vectors, grids): 0 the CG matvec (rows + PME gather), 1 the spread,
   // 2 the FFT/convolution chain (five passes), 3 the energy/force pass, 4 the row build.
+  bool has_hist() const override { return last_hist != nullptr; }
   double profile(cudaStream_t st, int which, int reps) override {
     pgm::Dev<T> a = dev(nullptr, nullptr, 0, forces_tmp.p, d_status.p);
     a.pos = last_pos;
@@ -573,8 +581,14 @@ struct Engine : EngineBase {
           });
       } else if (which == 7) pgm::k_rowfield<T, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, Fv.p);
       else if (which == 8) pgm::k_rowmat<T, P, false, 1, 0, false><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
-      else {  // 9: a whole operator sweep with the row/PME overlap
+      else if (which == 9) {  // a whole operator sweep with the row/PME overlap
         sweep<false, false, 0, 1>(st, a, Pv.p, AP.p);
+      } else if (which == 10) {  // the learned guess's channel pass (rewrites the same graph field)
+        pgm::k_nn_chan<T><<<nwblk, 256, 0, st>>>(a, last_hist, nn_bl.p, nullptr, nn_rg, nn_bl.p, nn_chan.p);
+      } else if (which == 11) {
+        pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, nn_chan.p, nn_sigma, nn_rg, nn_inv.p, nn_vec.p, nullptr);
+      } else {  // 12: the model
+        CK(pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st));
       }
     };
     long long l0 = launches;
@@ -706,37 +720,33 @@ struct Engine : EngineBase {
   // The induced-dipole solve (forcefield.py:1917-2008 and 1714-1821).  mode 0: predictor start
   // and history push (compute); mode 1: plain start from ind->mu, no push (energy).
   void solve(cudaStream_t st, pgm::Dev<T> &a, PgmInduction *ind, int mode, double *mu_out, int32_t *iters, double *resid) {
-    // predictor 5 ("nn"): the learned guess from the permanent field and the last two dipoles,
-    // for systems with two steps of history (unfused start); without a model, mu4
+    // predictor 5 ("nn"): the mu4 extrapolation plus the learned correction, for systems with four
+    // steps of history, with mu4's (fused) start; without a model, mu4.  Predictor 1: the previous
+    // step's dipoles.
     const bool use_nn = mode == 0 && set.predictor == 5 && nn_on;
-    const int pred = set.predictor == 5 ? (nn_on ? 0 : 4) : set.predictor;
-    const int K = pred == 4 ? 4 : (pred == 3 ? 3 : 0);
-    const double c4[4] = {4.0, -6.0, 4.0, -1.0}, c3[4] = {3.0, -3.0, 1.0, 0.0}, c0[4] = {0, 0, 0, 0};
-    const double *cc = K == 4 ? c4 : (K == 3 ? c3 : c0);
+    const int pred = set.predictor == 5 ? 4 : set.predictor;
+    const int K = pred == 4 ? 4 : (pred == 3 ? 3 : (pred == 1 ? 1 : 0));
+    const double c4[4] = {4.0, -6.0, 4.0, -1.0}, c3[4] = {3.0, -3.0, 1.0, 0.0}, c1[4] = {1.0, 0, 0, 0}, c0[4] = {0, 0, 0, 0};
+    const double *cc = K == 4 ? c4 : (K == 3 ? c3 : (K == 1 ? c1 : c0));
     pgm::k_cg_setup<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, mode == 0 ? ind->count : nullptr, ind->norm,
-                                                    mode == 0 ? (use_nn ? 2 : K) : 0, use_nn ? 0 : set.fused,
-                                                    std::max(1, set.norm_refresh), mode);
+                                                    mode == 0 ? K : 0, set.fused, std::max(1, set.norm_refresh), mode);
     check_launch();
     if (mode == 1) {
       // x0 = ind->mu with the plain start: X = mu, have = 1
       pgm::k_energy_start<T><<<grid1(nt), 256, 0, st>>>(a, ind->mu);
       check_launch();
     } else {
-      pgm::k_start1<T><<<grid1(nt), 256, 0, st>>>(a, ind->hist, K, cc[0], cc[1], cc[2], cc[3]);
+      last_hist = ind->hist;
+      if (use_nn) {
+        nn_inputs(st, a, ind->hist, nn_bl.p, nn_valid.p, nn_bl.p, nn_inv.p, nn_vec.p, nn_valid.p);
+        cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st);
+        if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
+        ++launches;
+      }
+      pgm::k_start1<T><<<grid1(nt), 256, 0, st>>>(a, ind->hist, K, cc[0], cc[1], cc[2], cc[3], use_nn ? nn_mu.p : nullptr);
       check_launch();
     }
     sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
-    if (use_nn) {
-      pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, ind->hist, nn_bprev_ok ? nn_bprev.p : nullptr, nn_sigma, nn_rg, nn_inv.p,
-                                                    nn_vec.p);
-      check_launch();
-      pgm::k_copy_vec<T><<<grid1(nt), 256, 0, st>>>(nt, Bv.p, nn_bprev.p); check_launch();  // b of this step for the next
-      nn_bprev_ok = true;
-      cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st);
-      if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
-      ++launches;
-      pgm::k_nn_set_x<T><<<grid1(nt), 256, 0, st>>>(a, nn_mu.p); check_launch();
-    }
     pgm::k_start2<T><<<ntblk, 256, 0, st>>>(a); check_launch();
     sweep<false, false, 2, 1>(st, a, X.p, AP.p);
     pgm::k_start3<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
@@ -885,8 +895,8 @@ PgmStatus pgm_create(const PgmSettings *s, const PgmSystemDesc *systems, int n, 
   if (s->precision < 0 || s->precision > 1) return fail(PGM_ERR_INVALID, "precision must be 0 (mixed) or 1 (double)");
   if (!(s->cutoff > 0) || !(s->ewald_beta > 0)) return fail(PGM_ERR_INVALID, "cutoff and ewald_beta must be positive");
   if (s->pme_order != 4 && s->pme_order != 6 && s->pme_order != 8) return fail(PGM_ERR_UNSUPPORTED, "pme_order must be 4, 6 or 8");
-  if (s->predictor != 0 && s->predictor != 3 && s->predictor != 4 && s->predictor != 5)
-    return fail(PGM_ERR_INVALID, "predictor must be 0 (none), 3 (mu3), 4 (mu4) or 5 (learned guess)");
+  if (s->predictor != 0 && s->predictor != 1 && s->predictor != 3 && s->predictor != 4 && s->predictor != 5)
+    return fail(PGM_ERR_INVALID, "predictor must be 0 (none), 1 (previous step), 3 (mu3), 4 (mu4) or 5 (learned guess)");
   if (s->max_iter < 0) return fail(PGM_ERR_INVALID, "max_iter must be >= 0");
   for (int i = 0; i < n; ++i) {
     const PgmSystemDesc &d = systems[i];
@@ -1065,11 +1075,11 @@ PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, floa
 }
 
 PgmStatus pgm_nn_features(PgmHandle *h, void *stream, const double *pos, const double *box, const double *hist,
-                          const double *b_prev, double *b_out, float *inv, float *vec) {
-  if (!h || !pos || !box || !hist || !inv || !vec) return fail(PGM_ERR_INVALID, "null argument");
+                          const float *bl_prev, float *bl_out, float *inv, float *vec) {
+  if (!h || !pos || !box || !hist || !bl_out || !inv || !vec) return fail(PGM_ERR_INVALID, "null argument");
   try {
     CK(cudaSetDevice(h->device));
-    h->eng->nn_features((cudaStream_t)stream, pos, box, hist, b_prev, b_out, inv, vec);
+    h->eng->nn_features((cudaStream_t)stream, pos, box, hist, bl_prev, bl_out, inv, vec);
     return PGM_OK;
   } catch (CudaError &e) {
     return fail(PGM_ERR_CUDA, e.msg);
@@ -1128,7 +1138,8 @@ long long pgm_last_launch_count(const PgmHandle *h) { return h ? h->eng->launche
 long long pgm_launches_per_iteration(const PgmHandle *h) { return h ? h->eng->launches_per_iteration() : -1; }
 
 PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, double *ms_per_launch) {
-  if (!h || !ms_per_launch || reps <= 0 || which < 0 || which > 9) return fail(PGM_ERR_INVALID, "bad argument");
+  if (!h || !ms_per_launch || reps <= 0 || which < 0 || which > 12) return fail(PGM_ERR_INVALID, "bad argument");
+  if (which == 10 && !h->eng->has_hist()) return fail(PGM_ERR_INVALID, "no solve with a history has run");
   if (!static_cast<bool>(h->eng)) return fail(PGM_ERR_INVALID, "no engine");
   try {
     CK(cudaSetDevice(h->device));

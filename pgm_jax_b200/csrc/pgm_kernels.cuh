@@ -1070,21 +1070,78 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
 }
 
 // ------------------------------------------------------------------ learned guess: features
-// One warp per atom over its pair row, edges with r < rg (the short-range graph): vector channels
-// (e nm) v0 = alpha_i (b_i - b_prev,i) (the change of the permanent field since the last step; b
-// itself without bprev), v1 = mu_{n-1,i}, v2 = mu_{n-2,i}, and for each of them and 4 radial
-// bases phi_k(r) = exp(-((r - 0.1 (k + 1) nm) / 0.1 nm)^2) (cos(pi r / rg) + 1) / 2 the aggregates
-// A_ck = sum_j phi_k v_c,j and D_ck = sum_j phi_k (v_c,j . u) u (u = x / r); 16 rotation invariants
-// for the MLP (pgm_nn.cu).  The model mixes the 27 channels: the prediction turns with the system.
+// The model predicts the correction delta = mu* - x4 to the mu4 extrapolation x4 = 4 mu1 - 6 mu2 +
+// 4 mu3 - mu4 (mu_j the converged dipoles j steps back), so the untrained model (zero output) is the
+// reference's mu4 predictor, and the solver keeps its fused one-sweep start: everything the model
+// sees is known before the step's first field sweep.
+//
+// Step 1, one warp per atom over its pair row, edges r < rg (the short-range graph): the permanent
+// field of the graph, b_i = -sum_k [(-q_k G1 - G2 (p_k . x)) x + G1 p_k] (the real-space row field
+// of charges and permanent dipoles, restricted to the graph), and three per-atom channel vectors
+// (e nm): c0 = alpha_i (b_i - b_prev,i) (zero when there is no previous b), c1 = mu1 - mu2,
+// c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
+// NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
+constexpr int NN_CHAN = 12;
 template <typename T>
-__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *hist, const v4<T> *bprev, float sigma, float rg,
-                                                     float *inv, float *vec) {
+__global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, const float4 *bl_prev, const int *valid,
+                                                 float rg, float4 *bl_out, float *chan) {
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
   if (i >= S.atom0 + S.natom) return;
+  float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+  int n = min(a.rn[i], a.mc);
+  size_t base = (size_t)i * a.mc;
+  for (int t = lane; t < n; t += 32) {
+    size_t o = base + t;
+    float x = float(a.rx[o]), y = float(a.ry[o]), z = float(a.rz[o]);
+    if (x * x + y * y + z * z >= rg * rg) continue;
+    int k = a.rk[o];
+    float g1 = float(a.rg1[o]), g2 = float(a.rg2[o]);
+    double4 pk = a.pperm[k];
+    float px = float(pk.x), py = float(pk.y), pz = float(pk.z);
+    float c = -float(a.q[k]) * g1 - g2 * (px * x + py * y + pz * z);
+    f0 += c * x + g1 * px;
+    f1 += c * y + g1 * py;
+    f2 += c * z + g1 * pz;
+  }
+  f0 = -warp_sum<float>(f0); f1 = -warp_sum<float>(f1); f2 = -warp_sum<float>(f2);
+  if (lane >= 3) return;
+  // lanes 0..2 write one component each
+  const float fb = lane == 0 ? f0 : (lane == 1 ? f1 : f2);
+  const float *bp = bl_prev ? reinterpret_cast<const float *>(bl_prev + i) : nullptr;
+  const bool have_prev = bp && (!valid || *valid);
+  const float db = have_prev ? fb - bp[lane] : 0.f;
   const size_t st = (size_t)a.nt * 3;
+  double m1 = hist[3 * (size_t)i + lane], m2 = hist[st + 3 * (size_t)i + lane], m3 = hist[2 * st + 3 * (size_t)i + lane],
+         m4 = hist[3 * st + 3 * (size_t)i + lane];
+  double x4 = 4.0 * m1 - 6.0 * m2 + 4.0 * m3 - m4;
+  __syncwarp(0x7);
+  reinterpret_cast<float *>(bl_out + i)[lane] = fb;
+  if (lane == 0) reinterpret_cast<float *>(bl_out + i)[3] = 0.f;
+  float *C = chan + (size_t)i * NN_CHAN;
+  C[lane] = float(a.alpha[i]) * db;
+  C[3 + lane] = float(m1 - m2);
+  C[6 + lane] = float(x4 - m1);
+  C[9 + lane] = float(m1);
+}
+
+// Step 2, one warp per atom over the same edges: vector channels (NN_CH = 27) v0..v2 = the atom's own
+// c0..c2 and, for each c and 4 radial bases phi_k(r) = exp(-((r - 0.1 (k + 1) nm) / 0.1 nm)^2)
+// (cos(pi r / rg) + 1) / 2, the aggregates A_ck = sum_j phi_k c_j and D_ck = sum_j phi_k (c_j . u) u
+// (u = x / r); 16 rotation invariants (asinh of magnitudes and dot products over the change scale
+// sigma, |mu1| over 0.02 e nm, alpha, radius).  The model mixes the 27 channels, so the predicted
+// correction turns with the system.  Sets *valid (the next step has a previous b).
+template <typename T>
+__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan, float sigma, float rg, float *inv, float *vec,
+                                                     int *valid) {
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (valid && blockIdx.x == 0 && threadIdx.x == 0) *valid = 1;  // read by the previous kernel only
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
   float acc[2][3][4][3];
 #pragma unroll
   for (int q = 0; q < 2; ++q)
@@ -1110,12 +1167,9 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *his
       float d = (r - 0.1f * (k + 1)) * 10.f;
       phi[k] = expf(-d * d) * fc;
     }
-    v4<T> bj = a.B[j];
-    if (bprev) { v4<T> q = bprev[j]; bj.x -= q.x; bj.y -= q.y; bj.z -= q.z; }
-    float aj = float(a.alpha[j]);
-    float v[3][3] = {{aj * float(bj.x), aj * float(bj.y), aj * float(bj.z)},
-                     {float(hist[3 * j]), float(hist[3 * j + 1]), float(hist[3 * j + 2])},
-                     {float(hist[st + 3 * j]), float(hist[st + 3 * j + 1]), float(hist[st + 3 * j + 2])}};
+    const float4 *cj = reinterpret_cast<const float4 *>(chan + (size_t)j * NN_CHAN);
+    float4 c01 = cj[0], c12 = cj[1], c2m = cj[2];
+    float v[3][3] = {{c01.x, c01.y, c01.z}, {c01.w, c12.x, c12.y}, {c12.z, c12.w, c2m.x}};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       float pr = v[c][0] * u[0] + v[c][1] * u[1] + v[c][2] * u[2];
@@ -1137,12 +1191,9 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *his
 #pragma unroll
         for (int x = 0; x < 3; ++x) acc[q][c][k][x] = warp_sum<float>(acc[q][c][k][x]);
   if (lane != 0) return;
-  v4<T> bi = a.B[i];
-  if (bprev) { v4<T> q = bprev[i]; bi.x -= q.x; bi.y -= q.y; bi.z -= q.z; }
-  float ai = float(a.alpha[i]);
-  float self[3][3] = {{ai * float(bi.x), ai * float(bi.y), ai * float(bi.z)},
-                      {float(hist[3 * i]), float(hist[3 * i + 1]), float(hist[3 * i + 2])},
-                      {float(hist[st + 3 * i]), float(hist[st + 3 * i + 1]), float(hist[st + 3 * i + 2])}};
+  const float *ci = chan + (size_t)i * NN_CHAN;
+  float self[3][3] = {{ci[0], ci[1], ci[2]}, {ci[3], ci[4], ci[5]}, {ci[6], ci[7], ci[8]}};
+  const float m1[3] = {ci[9], ci[10], ci[11]};
   float *V = vec + (size_t)i * pgmnn::NN_CH * 3;
   for (int c = 0; c < 3; ++c)
     for (int x = 0; x < 3; ++x) V[3 * c + x] = self[c][x];
@@ -1153,17 +1204,17 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const double *his
   auto dot = [](const float *p, const float *q) { return p[0] * q[0] + p[1] * q[1] + p[2] * q[2]; };
   float is = 1.f / sigma, is2 = is * is;
   float *F = inv + (size_t)i * pgmnn::NN_IN;
-  F[0] = ai * 1e3f;
+  F[0] = float(a.alpha[i]) * 1e3f;
   F[1] = float(a.radius[i]) / 0.06f;
-  F[2] = sqrtf(dot(self[0], self[0])) * is;
-  F[3] = sqrtf(dot(self[1], self[1])) * is;
-  F[4] = sqrtf(dot(self[2], self[2])) * is;
-  F[5] = dot(self[0], self[1]) * is2;
-  F[6] = dot(self[1], self[2]) * is2;
-  F[7] = dot(self[0], self[2]) * is2;
+  F[2] = asinhf(sqrtf(dot(self[0], self[0])) * is);
+  F[3] = sqrtf(dot(m1, m1)) * 50.f;
+  F[4] = asinhf(sqrtf(dot(self[1], self[1])) * is);
+  F[5] = asinhf(sqrtf(dot(self[2], self[2])) * is);
+  F[6] = asinhf(dot(self[0], self[1]) * is2);
+  F[7] = asinhf(dot(self[0], self[2]) * is2);
   for (int k = 0; k < 4; ++k) {
-    F[8 + k] = sqrtf(dot(acc[0][0][k], acc[0][0][k])) * is;
-    F[12 + k] = sqrtf(dot(acc[0][1][k], acc[0][1][k])) * is;
+    F[8 + k] = asinhf(sqrtf(dot(acc[0][0][k], acc[0][0][k])) * is);
+    F[12 + k] = asinhf(sqrtf(dot(acc[0][1][k], acc[0][1][k])) * is);
   }
 }
 
@@ -1182,22 +1233,11 @@ __global__ void k_vec_from_f64(int n, const double *src, v4<T> *dst) {
   dst[i] = d;
 }
 
-// x0 = the model's prediction for the systems with a history (count >= 2).
-template <typename T>
-__global__ void k_nn_set_x(Dev<T> a, const float *mu) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nt) return;
-  if (!a.cg[a.sysid[i]].have) return;
-  v4<T> x;
-  x.x = T(mu[3 * i]); x.y = T(mu[3 * i + 1]); x.z = T(mu[3 * i + 2]); x.w = T(0);
-  a.X[i] = x;
-}
-
 // ------------------------------------------------------------------ CG
 // Start, step 1 (thread per atom): the predictor guess x0h = sum c_j hist_j (forcefield.py:605,
 // 1956-1958) and the dipoles of the first field sweep: p + x0h (fused start) or p (plain).
 template <typename T>
-__global__ void k_start1(Dev<T> a, const double *hist, int K, double c0, double c1, double c2, double c3) {
+__global__ void k_start1(Dev<T> a, const double *hist, int K, double c0, double c1, double c2, double c3, const float *xnn) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   int s = a.sysid[i];
@@ -1207,6 +1247,8 @@ __global__ void k_start1(Dev<T> a, const double *hist, int K, double c0, double 
     const double cc[4] = {c0, c1, c2, c3};
     for (int j = 0; j < K; ++j)
       for (int c = 0; c < 3; ++c) x0[c] += cc[j] * hist[((size_t)j * a.nt + i) * 3 + c];
+    if (xnn)  // the learned correction to the extrapolation
+      for (int c = 0; c < 3; ++c) x0[c] += double(xnn[3 * (size_t)i + c]);
   }
   double4 p = a.pperm[i];
   v4<T> d, x;

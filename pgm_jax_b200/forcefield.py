@@ -25,7 +25,9 @@ from . import _lib
 from .systems import System, grid_size
 
 ELEC_LEVELS = {"q": 0, "qp": 1, "qi": 2, "qpi": 3}
-PREDICTORS = {"none": 0, "mu3": 3, "mu4": 4, "nn": 5}  # "nn": the learned guess (learned.py), mu4 until installed
+# "mu1": the previous step's dipoles (the plain-CG start the learned guess is measured against);
+# "nn": mu4 plus the learned correction (learned.py), mu4 until a model is installed
+PREDICTORS = {"none": 0, "mu1": 1, "mu3": 3, "mu4": 4, "nn": 5}
 
 # The settings of MDSettings that this engine implements, with the reference's defaults
 # (forcefield.py:142-516).  Other reference settings (iEL, IPS, DE / GVDW, split rows, the local

@@ -1,16 +1,18 @@
 """The learned initial guess of the induced-dipole solve: data, training and use.
 
 A message-passing model on the short-range graph (edges r < 0.5 nm taken from the pair rows)
-predicts the converged induced dipoles of a step from the permanent field b (of that step and the
-previous one: the change alpha (b_n - b_{n-1}) is its response channel) and the dipoles of the two
-previous steps; the engine's solver starts CG from the prediction (predictor
-"nn", an unfused start) and iterates to the same tolerance, so the plain solver judges the guess.
+predicts the correction mu* - x4 from the mu4 extrapolation x4 = 4 mu1 - 6 mu2 + 4 mu3 - mu4 to the
+converged induced dipoles mu* of a step, from the change of the graph's permanent field since the
+last step (the real-space field of charges and permanent dipoles over the graph edges) and the last
+steps' dipoles.  With predictor "nn" the engine's solver starts CG from x4 + the prediction with
+mu4's fused start (one field sweep, as the reference's mu4 predictor) and iterates to the same
+tolerance, so the plain solver judges the guess; the untrained (zero) model is mu4 exactly.
 The model (csrc/pgm_nn.cu): 16 rotation invariants -> MLP 64 -> 64 (SiLU) -> 27 coefficients that
-mix 27 vector channels per atom (csrc/pgm_kernels.cuh k_nn_features), so the prediction rotates
-with the system.  Training runs on the GPU with the project's BF16 tensor-core forward/backward
-kernels and Adam; the data are (features, converged dipoles) pairs written while the plain solver
-runs MD.  The reference has no counterpart (pgm_jax/md/forcefield.py:1917-2008 has the mu3, mu4
-and least-squares predictors only).
+mix 27 vector channels per atom (csrc/pgm_kernels.cuh k_nn_chan, k_nn_features), so the prediction
+rotates with the system.  Training runs on the GPU with the project's BF16 tensor-core
+forward/backward kernels and Adam; the data are (features, mu* - x4) pairs written while the plain
+solver runs MD.  The reference has no counterpart (pgm_jax/md/forcefield.py:1917-2008 has the mu3,
+mu4 and least-squares predictors only).
 """
 
 from __future__ import annotations
@@ -23,20 +25,18 @@ import torch
 from . import _lib
 
 N_IN, N_HID, N_OUT, N_CH = 16, 64, 32, 27
-SIGMA = 0.02  # e nm, scale of the invariants
+SIGMA = 2e-4  # e nm, scale of the per-step changes in the invariants and the loss
 GRAPH_CUTOFF = 0.5  # nm
 
 
 def init_weights(seed: int = 0) -> np.ndarray:
-    """Flat FP32 weights (w1, b1, w2, b2, w3, b3): small random layers and an output bias that makes
-    the untrained model the linear extrapolation 2 mu_{n-1} - mu_{n-2}."""
+    """Flat FP32 weights (w1, b1, w2, b2, w3, b3): small random hidden layers and a zero output
+    layer, so the untrained model predicts no correction (the guess is mu4)."""
     rng = np.random.default_rng(seed)
     w1 = rng.normal(scale=1.0 / np.sqrt(N_IN), size=(N_IN, N_HID))
     w2 = rng.normal(scale=1.0 / np.sqrt(N_HID), size=(N_HID, N_HID))
-    w3 = np.zeros((N_HID, N_OUT))  # the untrained model is exactly the extrapolation
-    b3 = np.zeros(N_OUT)
-    b3[1], b3[2] = 2.0, -1.0
-    flat = np.concatenate([w1.ravel(), np.zeros(N_HID), w2.ravel(), np.zeros(N_HID), w3.ravel(), b3]).astype(np.float32)
+    flat = np.concatenate([w1.ravel(), np.zeros(N_HID), w2.ravel(), np.zeros(N_HID), np.zeros(N_HID * N_OUT),
+                           np.zeros(N_OUT)]).astype(np.float32)
     assert flat.size == _lib.load().pgm_nn_param_count()
     return flat
 
@@ -45,17 +45,19 @@ def _p(t: torch.Tensor):
     return C.c_void_p(t.data_ptr())
 
 
-def features(ff, pos: torch.Tensor, boxes: torch.Tensor, hist: torch.Tensor, b_prev: torch.Tensor | None = None):
-    """Invariants (N, 16), vector channels (N, 27, 3) and the permanent field b (N, 3) at a geometry.
+def features(ff, pos: torch.Tensor, boxes: torch.Tensor, hist: torch.Tensor, bl_prev: torch.Tensor | None = None):
+    """Invariants (N, 16), vector channels (N, 27, 3) and the graph's permanent field (N, 4) at a
+    geometry, with the history hist (4, N, 3) of the solve there.
 
-    b_prev: the previous step's b (then channel 0 is alpha (b - b_prev), as in the solver)."""
+    bl_prev: the previous step's graph field (else the field-change channel is zero).  Uses the
+    installed sigma and graph cutoff (GuessModel.install) or the defaults."""
     n = ff.n
     inv = torch.empty((n, N_IN), dtype=torch.float32, device=ff.device)
     vec = torch.empty((n, N_CH, 3), dtype=torch.float32, device=ff.device)
-    b = torch.empty((n, 3), dtype=torch.float64, device=ff.device)
+    bl = torch.empty((n, 4), dtype=torch.float32, device=ff.device)
     _lib.check(ff._lib.pgm_nn_features(ff._h, ff._stream(), _p(pos), _p(boxes), _p(hist),
-                                       None if b_prev is None else _p(b_prev), _p(b), _p(inv), _p(vec)))
-    return inv, vec, b
+                                       None if bl_prev is None else _p(bl_prev), _p(bl), _p(inv), _p(vec)))
+    return inv, vec, bl
 
 
 class GuessModel:
@@ -116,11 +118,12 @@ class GuessModel:
 
 
 def collect(md, steps: int, every: int = 1) -> dict:
-    """Run `steps` MD steps with the plain solver and keep (features, converged dipoles) of every
-    `every`-th step (once the history holds two steps)."""
+    """Run `steps` MD steps with the plain solver and keep, for every `every`-th step once the
+    history holds four steps, the features and the target mu* - x4 (device tensors; "prev" holds
+    mu1 - x4, for the previous-step guess's error)."""
     ff = md.ff
-    keep = {"inv": [], "vec": [], "target": []}
-    b_prev = None
+    keep = {"inv": [], "vec": [], "target": [], "prev": []}
+    bl_prev = None
     for k in range(steps):
         md.stream.synchronize()
         count = int(md.ind.count.min())
@@ -128,20 +131,24 @@ def collect(md, steps: int, every: int = 1) -> dict:
             hist = md.ind.hist.clone()
         md.step()
         with torch.cuda.stream(md.stream):
-            inv, vec, b = features(ff, md.pos, md.box, hist, b_prev)
+            inv, vec, bl = features(ff, md.pos, md.box, hist, bl_prev)
+            x4 = 4.0 * hist[0] - 6.0 * hist[1] + 4.0 * hist[2] - hist[3]
+            target = (md.ind.mu - x4).to(torch.float32)
+            prev = (hist[0] - x4).to(torch.float32)
         md.stream.synchronize()
-        if count >= 2 and b_prev is not None and k % every == 0:
+        if count >= 4 and bl_prev is not None and k % every == 0:
             keep["inv"].append(inv)
             keep["vec"].append(vec)
-            keep["target"].append(md.ind.mu.to(torch.float32).clone())
-        b_prev = b
+            keep["target"].append(target)
+            keep["prev"].append(prev)
+        bl_prev = bl
     return {k: torch.cat(v) for k, v in keep.items()}
 
 
 def guess_errors(model: GuessModel, data: dict) -> dict:
-    """RMS error (e nm) of the model's guess and of the linear extrapolation 2 mu1 - mu2 on data."""
-    mu = model.predict(data["inv"], data["vec"])
-    lin = 2.0 * data["vec"][:, 1] - data["vec"][:, 2]
+    """RMS error (e nm) of the guesses on data: mu4 + the model's correction, mu4, and the previous
+    step's dipoles."""
+    pred = model.predict(data["inv"], data["vec"])
     t = data["target"]
-    rms = lambda x: float(torch.sqrt(torch.mean((x - t) ** 2)))  # noqa: E731
-    return {"model": rms(mu), "linear": rms(lin), "target_rms": float(torch.sqrt(torch.mean(t * t)))}
+    rms = lambda x: float(torch.sqrt(torch.mean(x * x)))  # noqa: E731
+    return {"model": rms(pred - t), "mu4": rms(t), "mu1": rms(data["prev"] - t)}

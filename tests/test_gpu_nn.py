@@ -1,5 +1,5 @@
 """The learned initial guess on the GPU: tensor-core kernels against the NumPy model, equivariance
-of the features, and what a trained model gains over the untrained (linear extrapolation) guess."""
+of the features, and what a trained model gains over the untrained guess (mu4)."""
 
 import numpy as np
 import pytest
@@ -40,7 +40,8 @@ def test_tensor_core_gradient_matches_numpy():
 
 
 def test_features_turn_with_the_system():
-    """A 90-degree turn of a cubic box: invariants unchanged, vector channels turned."""
+    """A 90-degree turn of a cubic box: invariants unchanged, vector channels and the graph field
+    turned, for a first geometry and a displaced second one (the field-change channel nonzero)."""
     from pgm_jax_b200.forcefield import MDSettings, PGMForceField
     from pgm_jax_b200.learned import features
     from pgm_jax_b200.systems import water_box
@@ -51,20 +52,27 @@ def test_features_turn_with_the_system():
     rng = np.random.default_rng(2)
     hist = rng.normal(scale=0.01, size=(4, s.n, 3))
     R = np.array([[0.0, -1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
-    pos_r = (pos @ R.T) % 1.25
-    inv0, vec0, b0 = features(ff, _dev(pos, torch.float64), _dev(H[None], torch.float64), _dev(hist, torch.float64))
-    inv1, vec1, b1 = features(ff, _dev(pos_r, torch.float64), _dev(H[None], torch.float64), _dev(hist @ R.T, torch.float64))
-    assert np.abs(b0.cpu().numpy() @ R.T - b1.cpu().numpy()).max() <= 1e-8 * float(b0.abs().max())
-    inv0, inv1 = inv0.cpu().numpy(), inv1.cpu().numpy()
-    assert np.abs(inv0 - inv1).max() <= 1e-4 * max(1.0, np.abs(inv0).max())
-    v0, v1 = vec0.cpu().numpy(), vec1.cpu().numpy()
+    dx = rng.normal(scale=2e-3, size=pos.shape)
+    Hd = _dev(H[None], torch.float64)
+    out = []
+    for turn in (np.eye(3), R):
+        p0 = _dev((pos @ turn.T) % 1.25, torch.float64)
+        p1 = _dev(((pos + dx) @ turn.T) % 1.25, torch.float64)
+        hd = _dev(hist @ turn.T, torch.float64)
+        _, _, bl0 = features(ff, p0, Hd, hd)
+        inv, vec, bl1 = features(ff, p1, Hd, hd, bl0)
+        out.append((bl0.cpu().numpy()[:, :3], inv.cpu().numpy(), vec.cpu().numpy()))
+    (b0, inv0, v0), (b1, inv1, v1) = out
+    assert np.abs(b0 @ R.T - b1).max() <= 1e-5 * np.abs(b0).max()
+    assert np.abs(v0[:, 0]).max() > 1e-3 * np.abs(v0[:, 1]).max()  # the field changed
+    assert np.abs(inv0 - inv1).max() <= 1e-3 * max(1.0, np.abs(inv0).max())
     assert np.abs(v0 @ R.T - v1).max() <= 1e-4 * np.abs(v0).max()
 
 
-def test_trained_guess_beats_extrapolation_and_solves_to_tolerance():
-    """Plain-solver MD writes (features, converged dipoles); a few hundred GPU Adam steps train the
-    model; on later frames its guess is closer than 2 mu1 - mu2, and MD started from it converges to
-    the same tolerance."""
+def test_trained_guess_beats_mu4_and_solves_to_tolerance():
+    """Plain-solver MD writes (features, mu* - mu4 guess); GPU Adam steps train the model; on later
+    frames mu4 + its correction is closer to mu* than mu4 (and mu4 than the previous step's dipoles),
+    and MD started from it converges to the same tolerance."""
     from pgm_jax_b200.forcefield import MDSettings, PGMForceField
     from pgm_jax_b200.learned import GuessModel, collect, guess_errors
     from pgm_jax_b200.md import RigidMD
@@ -74,14 +82,16 @@ def test_trained_guess_beats_extrapolation_and_solves_to_tolerance():
     kw = dict(precision="mixed", cutoff=0.7, ewald_beta=5.0, pme_grid=(32, 32, 32), dipole_tol=1e-6, max_iter=100)
     ff = PGMForceField(s, H, MDSettings(predictor="nn", **kw))
     md = RigidMD(ff, pos, H, temperature=300.0, dt_fs=1.0, gamma_ps=5.0, seed=2)
-    train = collect(md, 60)
-    held = collect(md, 12)
+    train = collect(md, 64)
+    held = collect(md, 16)
     model = GuessModel(seed=0)
     before = guess_errors(model, held)
     model.train(train, iters=800, batch=8192, lr=2e-3)
     after = guess_errors(model, held)
-    assert abs(before["model"] - before["linear"]) <= 1e-3 * before["linear"]  # untrained = extrapolation
-    assert after["model"] < 0.97 * before["linear"], (before, after)  # the trained model gains on unseen frames
+    print("guess rms", before, after)
+    assert before["model"] == before["mu4"]  # the untrained model adds nothing
+    assert before["mu4"] < before["mu1"]
+    assert after["model"] < 0.9 * before["mu4"], (before, after)  # the trained model gains on unseen frames
     model.install(ff)
     its = []
     for _ in range(8):

@@ -122,13 +122,14 @@ def test_energy_and_fixed_mu_paths(box):
     assert abs(float(Ef[0]) - ref["total"]) <= 1e-10 * abs(ref["total"])
 
 
-@pytest.mark.parametrize("prec", ["double", "mixed"])
-def test_predictor_steps_match_oracle(small_box_system, prec):
-    """Six steps with the mu4 predictor and the fused start (history, count, norm carried)."""
+@pytest.mark.parametrize("prec,pred", [("double", "mu4"), ("mixed", "mu4"), ("double", "mu1")])
+def test_predictor_steps_match_oracle(small_box_system, prec, pred):
+    """Six steps with a predictor (mu4, or mu1: the previous step's dipoles) and the fused start
+    (history, count, norm carried)."""
     s, pos, H = small_box_system
-    st = dict(SMALL_BOX_SETTINGS, dipole_tol=1e-8, norm_refresh=5)
+    st = dict(SMALL_BOX_SETTINGS, dipole_tol=1e-8, norm_refresh=5, predictor=pred)
     o = O.Oracle(s, st)
-    ff = ff_for(s, H, prec, dipole_tol=1e-8, norm_refresh=5)
+    ff = ff_for(s, H, prec, dipole_tol=1e-8, norm_refresh=5, predictor=pred)
     ind_o = o.init_induction()
     ind_g = ff.init_induction()
     rng = np.random.default_rng(1)
