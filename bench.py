@@ -50,7 +50,22 @@ CONFIG = {
     "solver": "CG from mu4 + the learned correction (fused start); plain CG from mu1 and mu4 beside it",
     "l2": "working set larger than L2: pair rows 8 x 4 B x 12288 x capacity = 164 MB (126 MB L2)",
     "seeds": {"positions": 0, "velocities_thermostat": 1},
+    "equilibration": "1000 steps of 1 fs at gamma 20/ps from the lattice start, before training and timing",
 }
+
+
+EQUIL_STEPS, EQUIL_GAMMA = 1000, 20.0  # relaxation of the lattice start before any data or timing
+
+
+def equilibrate(md, steps: int = EQUIL_STEPS) -> None:
+    """Relax the lattice start (random orientations) with direct steps under a strong thermostat
+    (gamma 20 / ps, then back to the run's gamma), outside any timed region."""
+    g = md.gamma
+    md.gamma = EQUIL_GAMMA
+    for _ in range(steps):
+        md.step()
+    md.gamma = g
+    md.stream.synchronize()
 
 
 def settings(precision="mixed", predictor="mu4"):
@@ -196,6 +211,7 @@ def run_engine(args) -> None:
     ff = PGMForceField(s, H, settings(predictor="nn" if args.nn else "mu4"), device=local)
     md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
     lib = ff._lib
+    equilibrate(md)
     train_info = train_guess(md, ff) if args.nn else None  # plain-solver MD writes the data; GPU training
     # warm-up: direct steps (rows sized), then capture and replay
     for _ in range(max(1, args.warmup)):
@@ -210,8 +226,10 @@ def run_engine(args) -> None:
         dist.barrier()
     torch.cuda.synchronize(dev)
     clk = Clocks(local)
-    ms, n_it = timed_replays(md, args.steps, torch)
+    builds0 = int(lib.pgm_list_rebuilds(ff._h))
+    ms, n_it = timed_replays(md, args.steps, torch, label="timed_md")
     clocks = clk.stop()
+    rebuilds = int(lib.pgm_list_rebuilds(ff._h)) - builds0
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if ws > 1:
         dist.barrier()
@@ -243,7 +261,7 @@ def run_engine(args) -> None:
             "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic", "config": CONFIG, "cg_iters_per_step": n_it, "cg_iters_first_step": it0,
-            "status": status, "gpu_launches": int(round(launches)),
+            "status": status, "gpu_launches": int(round(launches)), "list_rebuilds_per_step": rebuilds / args.steps,
             "clocks": clocks,
             "roofline": {
                 "bound": "hbm", "kernel": "k_rowfield (CG matvec row stream: k, x, y, z, G1, G2 per pair)",
@@ -271,21 +289,26 @@ def run_engine(args) -> None:
         dist.destroy_process_group()
 
 
-def timed_replays(md, steps: int, torch) -> tuple:
-    """(ms per step, mean CG iterations) of `steps` graph replays, CUDA events on the MD stream."""
+def timed_replays(md, steps: int, torch, label: str | None = None) -> tuple:
+    """(ms per step, mean CG iterations) of `steps` graph replays, CUDA events on the MD stream;
+    `label` names an NVTX range around them (a profiler can restrict its capture to it)."""
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     it_sum = torch.zeros((), dtype=torch.int64, device=md.ff.device)
+    if label:
+        torch.cuda.nvtx.range_push(label)
     ev0.record(md.stream)
     for _ in range(steps):
         md.run(1)
         with torch.cuda.stream(md.stream):
             it_sum += md.result.iterations[0].to(torch.int64)
     ev1.record(md.stream)
+    if label:
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize(md.ff.device)
     return ev0.elapsed_time(ev1) / steps, float(it_sum.item()) / steps
 
 
-def train_guess(md, ff, frames: int = 24, held_frames: int = 4, iters: int = 600) -> dict:
+def train_guess(md, ff, frames: int = 64, held_frames: int = 8, iters: int = 2000) -> dict:
     """Plain-solver MD (mu4 until a model is installed) writes (features, mu* - mu4 guess) pairs;
     the model trains on the GPU and is installed; guess errors on held-out frames."""
     from pgm_jax_b200.learned import GuessModel, collect, guess_errors
@@ -311,6 +334,7 @@ def run_plain(s, pos, H, rank, predictor, args, torch) -> dict:
 
     ff = PGMForceField(s, H, settings(predictor=predictor), device=torch.cuda.current_device())
     md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
+    equilibrate(md)
     for _ in range(max(1, args.warmup) + 4):
         md.step()
     md.capture()
@@ -361,11 +385,13 @@ def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
         for _ in range(2):
             one()
         md.stream.synchronize()
+        torch.cuda.nvtx.range_push("e2e_md")  # direct launches: a profiler's launch list can use this range
         t0 = time.perf_counter()
         for _ in range(steps):
             one()
         md.stream.synchronize()
         ms = (time.perf_counter() - t0) * 1e3 / steps
+        torch.cuda.nvtx.range_pop()
     b = 8 * n * 3
     h2d = b + 9 * 8 * S + 5 * b + 4 * S + 8 * S + b  # positions, box, mu + hist, count, norm; forces back to the integrator
     d2h = b + b + 5 * b + 4 * S + 8 * S + 8 * (3 + 9 + 1) * S + 8 * S  # positions out; forces, state, energy, virial...

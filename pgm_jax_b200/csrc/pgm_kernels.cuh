@@ -58,6 +58,12 @@ struct Dev {
   int *rn, *rnsp, *rk;
   T *rx, *ry, *rz, *rg0, *rg1, *rg2, *rg3;
   int *max_count;
+  // the learned guess's graph (row entries with r^2 < nn_rg2): row slots [atom][nn_emax] and
+  // counts, written by the row build when nn_es is set (a count above nn_emax: scan the row)
+  uint16_t *nn_es;
+  int *nn_ne;
+  int nn_emax;
+  float nn_rg2;
   // vectors
   v4<T> *X, *R, *Z, *P, *AP, *B, *D;
   v4<T> *F;  // row field of a sweep (computed concurrently with the PME chain)
@@ -338,17 +344,23 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 // G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] (forcefield.py:1314-1338, kernels.py:76-118).
 template <typename T>
 __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, double x, double y, double z, size_t base, int &count,
-                                         int lane) {
+                                         int lane, int i, int &ecount) {
+  const unsigned lt = (1u << lane) - 1u;
   unsigned bal = __ballot_sync(0xffffffffu, keep);
-  if (keep) {
-    int slot = count + __popc(bal & ((1u << lane) - 1u));
-    if (slot < a.mc) {
-      size_t o = base + slot;
-      a.rk[o] = j;
-      a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
-    }
+  const int slot = count + __popc(bal & lt);
+  if (keep && slot < a.mc) {
+    size_t o = base + slot;
+    a.rk[o] = j;
+    a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
   }
   count += __popc(bal);
+  if (a.nn_es) {  // graph edges of the learned guess: the slots of the short entries
+    bool sh = keep && slot < a.mc && float(x * x + y * y + z * z) < a.nn_rg2;
+    unsigned eb = __ballot_sync(0xffffffffu, sh);
+    int at = ecount + __popc(eb & lt);
+    if (sh && at < a.nn_emax) a.nn_es[(size_t)i * a.nn_emax + at] = (uint16_t)slot;
+    ecount += __popc(eb);
+  }
 }
 
 template <typename T>
@@ -367,7 +379,7 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
   double4 pi = a.pos4[i];
   double rc2 = a.cutoff * a.cutoff;
   size_t base = (size_t)i * a.mc;
-  int count = 0;
+  int count = 0, ecount = 0;
   int mf = a.molfirst[i], me = a.molend[i];
   for (int j0 = mf; j0 < me; j0 += 32) {
     int j = j0 + lane;
@@ -379,7 +391,7 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount);
   }
   int nsp = count;
   int mi = (int)pi.w;
@@ -415,11 +427,12 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount);
   }
   if (lane == 0) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
+    if (a.nn_es) a.nn_ne[i] = ecount;
     if (count > a.mc) atomicOr(&a.status[s], 0x1u);
     atomicMax(a.max_count, count);
   }
@@ -1082,30 +1095,97 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
 // c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
 // NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
 constexpr int NN_CHAN = 12;
+constexpr int NN_EBUF = 64;  // per-warp staging of compacted graph edges (two rounds of 32)
+
+// Scans atom i's pair row 32 entries at a time (16-byte vector loads in FP32) and hands every edge
+// with r < rg to `edge(k, x, y, z, o)` with all lanes busy: the passing entries of a round are
+// compacted (ballot + prefix) into the warp's shared buffer and consumed 32 at a time, so the
+// per-edge work runs on full warps although only a fifth of the row is inside the graph cutoff.
+template <typename T, typename F>
+__device__ __forceinline__ void graph_edges(const Dev<T> &a, int i, float rg, float4 *buf, int *bo, F &&edge) {
+  const int lane = threadIdx.x & 31;
+  const int n = min(a.rn[i], a.mc);
+  const size_t base = (size_t)i * a.mc;
+  const float rg2 = rg * rg;
+  int cnt = 0;
+  auto flush = [&](int m) {  // consume buf[0, m) (m <= 32), one edge per lane
+    __syncwarp();
+    if (lane < m) {
+      float4 e = buf[lane];
+      edge(__float_as_int(e.w), e.x, e.y, e.z, bo[lane]);
+    }
+    __syncwarp();
+  };
+  for (int t0 = 0; t0 < n; t0 += 32) {
+    const int t = t0 + lane;
+    float x = 0.f, y = 0.f, z = 0.f;
+    int k = 0;
+    bool pass = false;
+    if (t < n) {
+      size_t o = base + t;
+      x = float(a.rx[o]); y = float(a.ry[o]); z = float(a.rz[o]);
+      pass = x * x + y * y + z * z < rg2;
+      if (pass) k = a.rk[o];
+    }
+    unsigned m = __ballot_sync(0xffffffffu, pass);
+    int at = cnt + __popc(m & ((1u << lane) - 1u));
+    if (pass) { buf[at] = make_float4(x, y, z, __int_as_float(k)); bo[at] = t; }
+    cnt += __popc(m);
+    if (cnt >= 32) {
+      flush(32);
+      if (lane < cnt - 32) { buf[lane] = buf[32 + lane]; bo[lane] = bo[32 + lane]; }
+      __syncwarp();  // the moved entries are read before the next round writes past them
+      cnt -= 32;
+    }
+  }
+  if (cnt > 0) flush(cnt);
+}
+
+// The graph edges of atom i: the row build's slot list when it holds them all, else the scan.
+template <typename T, typename F>
+__device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, float rg, float4 *buf, int *bo, F &&edge) {
+  const int ne = a.nn_es ? a.nn_ne[i] : a.nn_emax + 1;
+  if (ne > a.nn_emax) {
+    graph_edges(a, i, rg, buf, bo, edge);
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  const size_t base = (size_t)i * a.mc;
+  const uint16_t *es = a.nn_es + (size_t)i * a.nn_emax;
+  for (int e = lane; e < ne; e += 32) {
+    const int t = es[e];
+    const size_t o = base + t;
+    edge(a.rk[o], float(a.rx[o]), float(a.ry[o]), float(a.rz[o]), t);
+  }
+}
+
+// Step 1, one warp per atom over the graph edges of its pair row (r < rg): the permanent field of
+// the graph, b_i = -sum_k [(-q_k G1 - G2 (p_k . x)) x + G1 p_k] (the real-space row field of
+// charges and permanent dipoles, restricted to the graph), and three per-atom channel vectors
+// (e nm): c0 = alpha_i (b_i - b_prev,i) (zero when there is no previous b), c1 = mu1 - mu2,
+// c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
+// NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
 template <typename T>
 __global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, const float4 *bl_prev, const int *valid,
                                                  float rg, float4 *bl_out, float *chan) {
+  __shared__ float4 ebuf[WARPS_PER_BLOCK][NN_EBUF];
+  __shared__ int eoff[WARPS_PER_BLOCK][NN_EBUF];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
   if (i >= S.atom0 + S.natom) return;
   float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-  int n = min(a.rn[i], a.mc);
-  size_t base = (size_t)i * a.mc;
-  for (int t = lane; t < n; t += 32) {
-    size_t o = base + t;
-    float x = float(a.rx[o]), y = float(a.ry[o]), z = float(a.rz[o]);
-    if (x * x + y * y + z * z >= rg * rg) continue;
-    int k = a.rk[o];
-    float g1 = float(a.rg1[o]), g2 = float(a.rg2[o]);
+  const size_t base = (size_t)i * a.mc;
+  for_graph_edges(a, i, rg, ebuf[warp], eoff[warp], [&](int k, float x, float y, float z, int t) {
+    float g1 = float(a.rg1[base + t]), g2 = float(a.rg2[base + t]);
     double4 pk = a.pperm[k];
     float px = float(pk.x), py = float(pk.y), pz = float(pk.z);
     float c = -float(a.q[k]) * g1 - g2 * (px * x + py * y + pz * z);
     f0 += c * x + g1 * px;
     f1 += c * y + g1 * py;
     f2 += c * z + g1 * pz;
-  }
+  });
   f0 = -warp_sum<float>(f0); f1 = -warp_sum<float>(f1); f2 = -warp_sum<float>(f2);
   if (lane >= 3) return;
   // lanes 0..2 write one component each
@@ -1117,7 +1197,6 @@ __global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, c
   double m1 = hist[3 * (size_t)i + lane], m2 = hist[st + 3 * (size_t)i + lane], m3 = hist[2 * st + 3 * (size_t)i + lane],
          m4 = hist[3 * st + 3 * (size_t)i + lane];
   double x4 = 4.0 * m1 - 6.0 * m2 + 4.0 * m3 - m4;
-  __syncwarp(0x7);
   reinterpret_cast<float *>(bl_out + i)[lane] = fb;
   if (lane == 0) reinterpret_cast<float *>(bl_out + i)[3] = 0.f;
   float *C = chan + (size_t)i * NN_CHAN;
@@ -1132,33 +1211,41 @@ __global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, c
 // (cos(pi r / rg) + 1) / 2, the aggregates A_ck = sum_j phi_k c_j and D_ck = sum_j phi_k (c_j . u) u
 // (u = x / r); 16 rotation invariants (asinh of magnitudes and dot products over the change scale
 // sigma, |mu1| over 0.02 e nm, alpha, radius).  The model mixes the 27 channels, so the predicted
-// correction turns with the system.  Sets *valid (the next step has a previous b).
-template <typename T>
-__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan, float sigma, float rg, float *inv, float *vec,
-                                                     int *valid) {
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (valid && blockIdx.x == 0 && threadIdx.x == 0) *valid = 1;  // read by the previous kernel only
-  int s = a.wb_sys[blockIdx.x];
-  int i = a.wb_atom0[blockIdx.x] + warp;
-  const SysInfo &S = a.sys[s];
-  if (i >= S.atom0 + S.natom) return;
-  float acc[2][3][4][3];
+// correction turns with the system.  The A and the D sums are two passes over the edges (36 sums
+// live at a time, for occupancy).  Sets *valid (the next step has a previous b).
+// One halving step of a transposing warp reduction: lanes with bit (N/2) set keep the upper half of
+// their N values and receive the partner's upper half, the others the lower halves.
+template <int N>
+__device__ __forceinline__ void transpose_step(float (&v)[32], int lane) {
+  const bool up = lane & (N / 2);
 #pragma unroll
-  for (int q = 0; q < 2; ++q)
+  for (int j = 0; j < N / 2; ++j) {
+    float send = up ? v[j] : v[j + N / 2];
+    float keep = up ? v[j + N / 2] : v[j];
+    v[j] = keep + __shfl_xor_sync(0xffffffffu, send, N / 2);
+  }
+}
+// Warp sums of 32 values per lane in 31 shuffles: lane l returns the total of v[l].
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
+  const int lane = threadIdx.x & 31;
+  transpose_step<32>(v, lane);
+  transpose_step<16>(v, lane);
+  transpose_step<8>(v, lane);
+  transpose_step<4>(v, lane);
+  transpose_step<2>(v, lane);
+  return v[0];
+}
+
+// The 36 sums of one kind (Q = 0: A, 1: D) over the graph edges, value o = (c * 4 + k) * 3 + x;
+// returns on lane l the total of value l (l < 32) and in tail[0..3] the totals of values 32..35.
+template <int Q, typename T>
+__device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const float *chan, float rg, float4 *ebuf, int *eoff,
+                                              float (&tail)[4]) {
+  float acc[36];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-#pragma unroll
-        for (int x = 0; x < 3; ++x) acc[q][c][k][x] = 0.f;
-  int n = min(a.rn[i], a.mc);
-  size_t base = (size_t)i * a.mc;
-  for (int t = lane; t < n; t += 32) {
-    size_t o = base + t;
-    float x = float(a.rx[o]), y = float(a.ry[o]), z = float(a.rz[o]);
+  for (int o = 0; o < 36; ++o) acc[o] = 0.f;
+  for_graph_edges(a, i, rg, ebuf, eoff, [&](int j, float x, float y, float z, int) {
     float r = sqrtf(x * x + y * y + z * z);
-    if (r >= rg) continue;
-    int j = a.rk[o];
     float ir = 1.f / r, u[3] = {x * ir, y * ir, z * ir};
     float fc = 0.5f * (cospif(r / rg) + 1.f);
     float phi[4];
@@ -1172,50 +1259,67 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan
     float v[3][3] = {{c01.x, c01.y, c01.z}, {c01.w, c12.x, c12.y}, {c12.z, c12.w, c2m.x}};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      float pr = v[c][0] * u[0] + v[c][1] * u[1] + v[c][2] * u[2];
+      float w[3];
+      if (Q == 0) {
+        w[0] = v[c][0]; w[1] = v[c][1]; w[2] = v[c][2];
+      } else {
+        float pr = v[c][0] * u[0] + v[c][1] * u[1] + v[c][2] * u[2];
+        w[0] = pr * u[0]; w[1] = pr * u[1]; w[2] = pr * u[2];
+      }
 #pragma unroll
       for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int xx = 0; xx < 3; ++xx) {
-          acc[0][c][k][xx] += phi[k] * v[c][xx];
-          acc[1][c][k][xx] += phi[k] * pr * u[xx];
-        }
+        for (int xx = 0; xx < 3; ++xx) acc[(c * 4 + k) * 3 + xx] += phi[k] * w[xx];
     }
-  }
+  });
 #pragma unroll
-  for (int q = 0; q < 2; ++q)
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-#pragma unroll
-        for (int x = 0; x < 3; ++x) acc[q][c][k][x] = warp_sum<float>(acc[q][c][k][x]);
+  for (int o = 0; o < 4; ++o) tail[o] = warp_sum<float>(acc[32 + o]);
+  float (&head)[32] = *reinterpret_cast<float (*)[32]>(acc);
+  return warp_transpose_sum(head);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan, float sigma, float rg, float *inv, float *vec,
+                                                     int *valid) {
+  __shared__ float4 ebuf[WARPS_PER_BLOCK][NN_EBUF];
+  __shared__ int eoff[WARPS_PER_BLOCK][NN_EBUF];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (valid && blockIdx.x == 0 && threadIdx.x == 0) *valid = 1;  // read by the previous kernel only
+  int s = a.wb_sys[blockIdx.x];
+  int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
+  float *V = vec + (size_t)i * pgmnn::NN_CH * 3;
+  float *F = inv + (size_t)i * pgmnn::NN_IN;
+  const float is = 1.f / sigma, is2 = is * is;
+  float tail[4];
+  // A sums: lane l holds value l; |A_0k| and |A_1k| (values 3k.. and 12 + 3k..) for the invariants
+  float mine = nn_aggregate<0>(a, i, chan, rg, ebuf[warp], eoff[warp], tail);
+  V[9 + lane] = mine;
+  if (lane < 4) V[9 + 32 + lane] = tail[lane];
+  float sq = mine * mine;
+  float n2 = sq + __shfl_down_sync(0xffffffffu, sq, 1) + __shfl_down_sync(0xffffffffu, sq, 2);
+  if (lane < 24 && lane % 3 == 0) F[(lane < 12 ? 8 : 12) + (lane % 12) / 3] = asinhf(sqrtf(n2) * is);
+  // D sums
+  mine = nn_aggregate<1>(a, i, chan, rg, ebuf[warp], eoff[warp], tail);
+  V[45 + lane] = mine;
+  if (lane < 4) V[45 + 32 + lane] = tail[lane];
   if (lane != 0) return;
   const float *ci = chan + (size_t)i * NN_CHAN;
   float self[3][3] = {{ci[0], ci[1], ci[2]}, {ci[3], ci[4], ci[5]}, {ci[6], ci[7], ci[8]}};
   const float m1[3] = {ci[9], ci[10], ci[11]};
-  float *V = vec + (size_t)i * pgmnn::NN_CH * 3;
   for (int c = 0; c < 3; ++c)
     for (int x = 0; x < 3; ++x) V[3 * c + x] = self[c][x];
-  for (int q = 0; q < 2; ++q)
-    for (int c = 0; c < 3; ++c)
-      for (int k = 0; k < 4; ++k)
-        for (int x = 0; x < 3; ++x) V[3 * (3 + q * 12 + c * 4 + k) + x] = acc[q][c][k][x];
   auto dot = [](const float *p, const float *q) { return p[0] * q[0] + p[1] * q[1] + p[2] * q[2]; };
-  float is = 1.f / sigma, is2 = is * is;
-  float *F = inv + (size_t)i * pgmnn::NN_IN;
+  auto norm3 = [](const float *p) { return sqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]); };
   F[0] = float(a.alpha[i]) * 1e3f;
   F[1] = float(a.radius[i]) / 0.06f;
-  F[2] = asinhf(sqrtf(dot(self[0], self[0])) * is);
-  F[3] = sqrtf(dot(m1, m1)) * 50.f;
-  F[4] = asinhf(sqrtf(dot(self[1], self[1])) * is);
-  F[5] = asinhf(sqrtf(dot(self[2], self[2])) * is);
+  F[2] = asinhf(norm3(self[0]) * is);
+  F[3] = norm3(m1) * 50.f;
+  F[4] = asinhf(norm3(self[1]) * is);
+  F[5] = asinhf(norm3(self[2]) * is);
   F[6] = asinhf(dot(self[0], self[1]) * is2);
   F[7] = asinhf(dot(self[0], self[2]) * is2);
-  for (int k = 0; k < 4; ++k) {
-    F[8 + k] = asinhf(sqrtf(dot(acc[0][0][k], acc[0][0][k])) * is);
-    F[12 + k] = asinhf(sqrtf(dot(acc[0][1][k], acc[0][1][k])) * is);
-  }
 }
 
 template <typename T>

@@ -6,8 +6,9 @@
 //
 // Model: h1 = silu(x W1 + b1), h2 = silu(h1 W2 + b2), c = h2 W3 + b3 (x: NN_IN invariants, hidden
 // NN_HID, c: NN_OUT coefficients, the first NN_CH used); mu = sum_c c_c v_c over the atom's vector
-// channels.  Weights: an FP32 master array; each CTA converts them to BF16 in shared memory.  A CTA
-// of 4 warps runs a tile of 64 samples through all layers (each warp 16 rows).
+// channels.  Weights: an FP32 master array; each CTA converts them to BF16 in shared memory.  In
+// training a CTA of 4 warps runs a tile of 64 samples through all layers (each warp 16 rows); in
+// inference each warp runs its own 16 samples.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <mma.h>
@@ -102,13 +103,35 @@ __device__ void weight_grad(Smem &s, const __nv_bfloat16 *A, const __nv_bfloat16
   }
 }
 
-__device__ void load_weights(Smem &s, const NNWeights &w) {
-  for (int t = threadIdx.x; t < NN_IN * NN_HID; t += blockDim.x) s.w1[t] = __float2bfloat16(w.w1[t]);
-  for (int t = threadIdx.x; t < NN_HID * NN_HID; t += blockDim.x) s.w2[t] = __float2bfloat16(w.w2[t]);
-  for (int t = threadIdx.x; t < NN_HID * NN_OUT; t += blockDim.x) s.w3[t] = __float2bfloat16(w.w3[t]);
-  for (int t = threadIdx.x; t < NN_HID; t += blockDim.x) { s.b1[t] = w.b1[t]; s.b2[t] = w.b2[t]; }
-  for (int t = threadIdx.x; t < NN_OUT; t += blockDim.x) s.b3[t] = w.b3[t];
+// FP32 -> BF16 of n floats (n a multiple of 4 * THREADS; 16-byte aligned source), 16-byte loads,
+// all of a thread's loads issued before the first conversion.
+template <int N>
+__device__ __forceinline__ void stage_bf16(const float *src, __nv_bfloat16 *dst) {
+  static_assert(N % (4 * THREADS) == 0, "whole float4 rounds");
+  const float4 *s4 = reinterpret_cast<const float4 *>(src);
+  __nv_bfloat162 *d2 = reinterpret_cast<__nv_bfloat162 *>(dst);
+  float4 v[N / (4 * THREADS)];
+#pragma unroll
+  for (int k = 0; k < N / (4 * THREADS); ++k) v[k] = s4[threadIdx.x + k * THREADS];
+#pragma unroll
+  for (int k = 0; k < N / (4 * THREADS); ++k) {
+    int t = threadIdx.x + k * THREADS;
+    d2[2 * t] = __floats2bfloat162_rn(v[k].x, v[k].y);
+    d2[2 * t + 1] = __floats2bfloat162_rn(v[k].z, v[k].w);
+  }
 }
+
+// The weights into shared memory (BF16 matrices, FP32 biases); blockDim.x == THREADS.
+__device__ void stage_weights(const NNWeights &w, __nv_bfloat16 *w1, __nv_bfloat16 *w2, __nv_bfloat16 *w3, float *b1, float *b2,
+                              float *b3) {
+  stage_bf16<NN_IN * NN_HID>(w.w1, w1);
+  stage_bf16<NN_HID * NN_HID>(w.w2, w2);
+  stage_bf16<NN_HID * NN_OUT>(w.w3, w3);
+  for (int t = threadIdx.x; t < NN_HID; t += blockDim.x) { b1[t] = w.b1[t]; b2[t] = w.b2[t]; }
+  for (int t = threadIdx.x; t < NN_OUT; t += blockDim.x) b3[t] = w.b3[t];
+}
+
+__device__ void load_weights(Smem &s, const NNWeights &w) { stage_weights(w, s.w1, s.w2, s.w3, s.b1, s.b2, s.b3); }
 
 __device__ void load_x(Smem &s, const float *inv, int n0, int n) {
   for (int t = threadIdx.x; t < TILE * NN_IN; t += blockDim.x) {
@@ -142,21 +165,51 @@ __device__ void forward_tile(Smem &s) {
   __syncthreads();
 }
 
+// Inference: every warp runs its own 16 samples through the layers (warp-synchronous, no block
+// barrier after the weights are staged), in a small shared-memory footprint so that several CTAs
+// share an SM.  Same rounding points as the training forward.
+constexpr int FWD_ROWS = 16;
+struct FwdSmem {
+  __nv_bfloat16 w1[NN_IN * NN_HID], w2[NN_HID * NN_HID], w3[NN_HID * NN_OUT];
+  __nv_bfloat16 x[THREADS / 32][FWD_ROWS * NN_IN], act[THREADS / 32][FWD_ROWS * NN_HID];
+  float z[THREADS / 32][FWD_ROWS * NN_HID];
+  float b1[NN_HID], b2[NN_HID], b3[NN_OUT];
+};
+
 __global__ void __launch_bounds__(THREADS) k_forward(NNWeights w, const float *inv, const float *vec, int n, float *mu) {
-  extern __shared__ __align__(128) unsigned char raw[];
-  Smem &s = *reinterpret_cast<Smem *>(raw);
-  load_weights(s, w);
-  int n0 = blockIdx.x * TILE;
-  load_x(s, inv, n0, n);
+  __shared__ __align__(128) FwdSmem s;
+  stage_weights(w, s.w1, s.w2, s.w3, s.b1, s.b2, s.b3);
   __syncthreads();
-  forward_tile(s);
-  for (int t = threadIdx.x; t < TILE * 3; t += blockDim.x) {
-    int r = t / 3, a = t - 3 * r, i = n0 + r;
-    if (i >= n) continue;
-    const float *v = vec + (size_t)i * NN_CH * 3;
-    float acc = 0.f;
-    for (int c = 0; c < NN_CH; ++c) acc += s.out[r * NN_OUT + c] * v[3 * c + a];
-    mu[3 * (size_t)i + a] = acc;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __nv_bfloat16 *x = s.x[warp], *act = s.act[warp];
+  float *z = s.z[warp];
+  for (int tile = blockIdx.x * (THREADS / 32) + warp; tile * FWD_ROWS < n; tile += gridDim.x * (THREADS / 32)) {
+    const int r0 = tile * FWD_ROWS;
+    for (int t = lane; t < FWD_ROWS * NN_IN; t += 32) {
+      int i = r0 + t / NN_IN;
+      x[t] = __float2bfloat16(i < n ? inv[(size_t)r0 * NN_IN + t] : 0.f);
+    }
+    __syncwarp();
+    warp_gemm<NN_HID, NN_IN>(x, NN_IN, s.w1, NN_HID, z, NN_HID);
+    __syncwarp();
+    for (int t = lane; t < FWD_ROWS * NN_HID; t += 32) act[t] = __float2bfloat16(silu(z[t] + s.b1[t % NN_HID]));
+    __syncwarp();
+    warp_gemm<NN_HID, NN_HID>(act, NN_HID, s.w2, NN_HID, z, NN_HID);
+    __syncwarp();
+    for (int t = lane; t < FWD_ROWS * NN_HID; t += 32) act[t] = __float2bfloat16(silu(z[t] + s.b2[t % NN_HID]));
+    __syncwarp();
+    warp_gemm<NN_OUT, NN_HID>(act, NN_HID, s.w3, NN_OUT, z, NN_OUT);
+    __syncwarp();
+    for (int t = lane; t < FWD_ROWS * 3; t += 32) {
+      int r = t / 3, a = t - 3 * r, i = r0 + r;
+      if (i >= n) continue;
+      const float *v = vec + (size_t)i * NN_CH * 3;
+      float acc = 0.f;
+#pragma unroll
+      for (int c = 0; c < NN_CH; ++c) acc += (z[r * NN_OUT + c] + s.b3[c]) * v[3 * c + a];  // all loads in flight
+      mu[3 * (size_t)i + a] = acc;
+    }
+    __syncwarp();
   }
 }
 
@@ -179,6 +232,7 @@ __global__ void __launch_bounds__(THREADS) k_train(NNWeights w, NNWeights g, con
     if (i < n) {
       const float *v = vec + (size_t)i * NN_CH * 3;
       float mu = 0.f;
+#pragma unroll
       for (int c = 0; c < NN_CH; ++c) mu += s.out[r * NN_OUT + c] * v[3 * c + a];
       e = mu - target[3 * (size_t)i + a];
       lsum += inv_scale * e * e;
@@ -262,9 +316,7 @@ size_t smem_bytes() { return sizeof(Smem); }
 cudaError_t set_attrs() {
   static bool done = false;
   if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+  cudaError_t e = cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e == cudaSuccess) done = true;
   return e;
 }
@@ -273,7 +325,8 @@ cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *
   cudaError_t e = set_attrs();
   if (e != cudaSuccess) return e;
   if (n <= 0) return cudaSuccess;
-  k_forward<<<(n + TILE - 1) / TILE, THREADS, sizeof(Smem), st>>>(nn_view(const_cast<float *>(flat)), inv, vec, n, mu);
+  const int tiles = (n + FWD_ROWS - 1) / FWD_ROWS, per = THREADS / 32;
+  k_forward<<<(tiles + per - 1) / per, THREADS, 0, st>>>(nn_view(const_cast<float *>(flat)), inv, vec, n, mu);
   return cudaGetLastError();
 }
 
