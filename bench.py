@@ -385,6 +385,7 @@ def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
         for _ in range(2):
             one()
         md.stream.synchronize()
+        builds0 = int(lib.pgm_list_rebuilds(ff._h))
         torch.cuda.nvtx.range_push("e2e_md")  # direct launches: a profiler's launch list can use this range
         t0 = time.perf_counter()
         for _ in range(steps):
@@ -392,10 +393,12 @@ def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
         md.stream.synchronize()
         ms = (time.perf_counter() - t0) * 1e3 / steps
         torch.cuda.nvtx.range_pop()
+        rebuilds = (int(lib.pgm_list_rebuilds(ff._h)) - builds0) / steps
     b = 8 * n * 3
     h2d = b + 9 * 8 * S + 5 * b + 4 * S + 8 * S + b  # positions, box, mu + hist, count, norm; forces back to the integrator
     d2h = b + b + 5 * b + 4 * S + 8 * S + 8 * (3 + 9 + 1) * S + 8 * S  # positions out; forces, state, energy, virial...
-    return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "steps": steps, "h2d_bytes_per_step": h2d,
+    return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "steps": steps, "list_rebuilds_per_step": rebuilds,
+            "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h,
             "path": "pgm_compute_host (C ABI, pinned host buffers: positions in; forces, energies, virial, induction "
             "state out) with the rigid-body kernels on the GPU; wall clock around the loop"}

@@ -708,6 +708,35 @@ __device__ __forceinline__ c2<T> *fft_lines(c2<T> *x, c2<T> *y, int Lrt, int nl,
   else return fft_run_ct<T, L, 0, 1>(x, y, nl, ld, tw, sign);
 }
 
+// Global -> shared staging of `total` elements by the FFT_THREADS threads of a pass: with a
+// compile-time bound N every load of a thread is issued before its first store (the passes are
+// latency-bound; one L2 round trip instead of one per element); N = 0: a plain loop.
+template <int N, typename Get, typename Put>
+__device__ __forceinline__ void staged_copy(int total, Get &&get, Put &&put) {
+  if constexpr (N > 0) {
+    constexpr int PER = (N + FFT_THREADS - 1) / FFT_THREADS;
+    using V = decltype(get(0));
+    V v[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      int t = threadIdx.x + j * FFT_THREADS;
+      if (t < total) v[j] = get(t);
+    }
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      int t = threadIdx.x + j * FFT_THREADS;
+      if (t < total) put(t, v[j]);
+    }
+  } else {
+    for (int t = threadIdx.x; t < total; t += blockDim.x) put(t, get(t));
+  }
+}
+
+template <typename T>
+struct c2pair {
+  c2<T> a, b;
+};
+
 // A launch of an FFT pass covers a group of systems with the same mesh length along the pass's
 // axis: block -> (group member g, tile) by the tile prefix gtile0 (ng + 1 entries).
 __device__ __forceinline__ int group_member(const int *gtile0, int ng, int b) {
@@ -737,11 +766,12 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, co
   c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
   T *Q = a.Q + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];  // twiddles in shared memory
-  for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
-    int rl = t / K3, k = t - rl * K3;
-    T *dst = reinterpret_cast<T *>(&x[(rl >> 1) * K3 + k]);
-    dst[rl & 1] = Q[t];
-  }
+  staged_copy<2 * FFT_PAIRS * L>(
+      2 * np * K3, [&](int t) { return Q[t]; },
+      [&](int t, T v) {
+        int rl = t / K3, k = t - rl * K3;
+        reinterpret_cast<T *>(&x[(rl >> 1) * K3 + k])[rl & 1] = v;
+      });
   __syncthreads();
   c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, -1);
   c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
@@ -772,17 +802,24 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
   c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
   const c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
   for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];
-  for (int t = threadIdx.x; t < np * K3; t += blockDim.x) {
-    int cl = t / K3, m = t - cl * K3;
-    bool up = m > K3 / 2;
-    int mm = up ? K3 - m : m;
-    c2<T> A = C[(size_t)(2 * cl) * K3h + mm], Bv = C[(size_t)(2 * cl + 1) * K3h + mm];
-    if (mm == 0 || 2 * mm == K3) { A.y = T(0); Bv.y = T(0); }
-    if (up) { A.y = -A.y; Bv.y = -Bv.y; }
-    c2<T> Z;
-    Z.x = A.x - Bv.y; Z.y = A.y + Bv.x;
-    x[cl * K3 + m] = Z;
-  }
+  staged_copy<FFT_PAIRS * L>(
+      np * K3,
+      [&](int t) {
+        int cl = t / K3, m = t - cl * K3;
+        int mm = m > K3 / 2 ? K3 - m : m;
+        return c2pair<T>{C[(size_t)(2 * cl) * K3h + mm], C[(size_t)(2 * cl + 1) * K3h + mm]};
+      },
+      [&](int t, c2pair<T> p) {
+        int cl = t / K3, m = t - cl * K3;
+        bool up = m > K3 / 2;
+        int mm = up ? K3 - m : m;
+        c2<T> A = p.a, Bv = p.b;
+        if (mm == 0 || 2 * mm == K3) { A.y = T(0); Bv.y = T(0); }
+        if (up) { A.y = -A.y; Bv.y = -Bv.y; }
+        c2<T> Z;
+        Z.x = A.x - Bv.y; Z.y = A.y + Bv.x;
+        x[cl * K3 + m] = Z;
+      });
   __syncthreads();
   c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, +1);
   T *Phi = a.Phi + S.rgrid0 + (size_t)l0 * K3;
@@ -808,17 +845,23 @@ __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const 
   c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_TILE * ld, *tws = y + FFT_TILE * ld;
   c2<T> *C = a.C + S.cgrid0;
   for (int t = threadIdx.x; t < K2; t += blockDim.x) tws[t] = a.tw[S.tw[1] + t];
-  for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
-    int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
-    int col = c0 + c;
-    c2<T> v;
-    v.x = T(0); v.y = T(0);
-    if (col < ncol) {
-      int k1 = col / K3h, m3 = col - k1 * K3h;
-      v = C[((size_t)k1 * K2 + k2) * K3h + m3];
-    }
-    x[c * ld + k2] = v;
-  }
+  staged_copy<L * FFT_TILE>(
+      K2 * FFT_TILE,
+      [&](int t) {
+        int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
+        int col = c0 + c;
+        c2<T> v;
+        v.x = T(0); v.y = T(0);
+        if (col < ncol) {
+          int k1 = col / K3h, m3 = col - k1 * K3h;
+          v = C[((size_t)k1 * K2 + k2) * K3h + m3];
+        }
+        return v;
+      },
+      [&](int t, c2<T> v) {
+        int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
+        x[c * ld + k2] = v;
+      });
   __syncthreads();
   c2<T> *res = fft_lines<T, L>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], tws, sign);
   for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
@@ -850,25 +893,46 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
   c2<T> *C = a.C + S.cgrid0;
   const size_t rs = (size_t)ncol;
   for (int t = threadIdx.x; t < K1; t += blockDim.x) tws[t] = a.tw[S.tw[0] + t];
-  for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
-    int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
-    int col = c0 + c;
-    c2<T> v;
-    v.x = T(0); v.y = T(0);
-    if (col < ncol) v = C[k1 * rs + col];
-    x[c * ld + k1] = v;
-  }
+  const T *G = a.Ginf + S.cgrid0;
+  // the influence values of this tile are staged beside the grid columns (their loads in flight
+  // with the grid's); y holds them until the first transform overwrites it
+  T *gst = reinterpret_cast<T *>(y);
+  staged_copy<L * FFT_TILE>(
+      K1 * FFT_TILE,
+      [&](int t) {
+        int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
+        int col = c0 + c;
+        c2pair<T> v;
+        v.a.x = T(0); v.a.y = T(0); v.b.x = T(0); v.b.y = T(0);
+        if (col < ncol) { v.a = C[k1 * rs + col]; v.b.x = G[k1 * rs + col]; }
+        return v;
+      },
+      [&](int t, c2pair<T> v) {
+        int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
+        x[c * ld + k1] = v.a;
+        gst[t] = v.b.x;
+      });
   __syncthreads();
+  T gvr[(L * FFT_TILE + FFT_THREADS - 1) / FFT_THREADS > 0 ? (L * FFT_TILE + FFT_THREADS - 1) / FFT_THREADS : 1];
+  if constexpr (L > 0) {
+#pragma unroll
+    for (int j = 0; j < (L * FFT_TILE + FFT_THREADS - 1) / FFT_THREADS; ++j) {
+      int t = threadIdx.x + j * FFT_THREADS;
+      gvr[j] = t < K1 * FFT_TILE ? gst[t] : T(0);
+    }
+    __syncthreads();  // y is the transform's scratch from here
+  }
   c2<T> *res = fft_lines<T, L>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], tws, -1);
   c2<T> *oth = res == x ? y : x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const BoxInfo &B = a.box[s];
-  const T *G = a.Ginf + S.cgrid0;
-  for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
+#pragma unroll
+  for (int j = 0; j < (L > 0 ? (L * FFT_TILE + FFT_THREADS - 1) / FFT_THREADS : 1); ++j) {
+   for (int t = threadIdx.x + j * FFT_THREADS; t < K1 * FFT_TILE; t += (L > 0 ? K1 * FFT_TILE : (int)blockDim.x)) {
     int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
     int col = c0 + c;
     if (col >= ncol) continue;
-    T gv = G[k1 * rs + col];
+    T gv = L > 0 ? gvr[j] : G[k1 * rs + col];
     c2<T> F = res[c * ld + k1];
     if (ENERGY && gv != T(0)) {
       int k2 = col / K3h, m3 = col - k2 * K3h;
@@ -893,6 +957,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
     T g2 = T(2) * gv;
     F.x *= g2; F.y *= g2;
     res[c * ld + k1] = F;
+   }
   }
   if (ENERGY) {
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
