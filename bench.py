@@ -68,6 +68,11 @@ def equilibrate(md, steps: int = EQUIL_STEPS) -> None:
     md.stream.synchronize()
 
 
+# DRAM bytes of one k_rowfield<float, 0, 1> launch (read + write) from an ncu capture of this
+# workload (profiles/k_rowfield_water4096.txt), with the pair count it had; scaled by pairs.
+ROWFIELD_NCU_DRAM_BYTES, ROWFIELD_NCU_PAIRS = 93.654784e6 + 3.39328e6, 3.745e6
+
+
 def settings(precision="mixed", predictor="mu4"):
     from pgm_jax_b200.forcefield import MDSettings
 
@@ -266,7 +271,8 @@ def run_engine(args) -> None:
             "roofline": {
                 "bound": "hbm", "kernel": "k_rowfield (CG matvec row stream: k, x, y, z, G1, G2 per pair)",
                 "achieved": mv_gbs, "peak": peak, "unit": "GB/s", "frac": mv_gbs / peak, "peak_kind": peak_kind,
-                "traffic": None, "bytes_per_launch": mv_bytes, "ms_per_launch": kt["row_field"],
+                "traffic": ROWFIELD_NCU_DRAM_BYTES * pairs / ROWFIELD_NCU_PAIRS, "traffic_unit": "bytes per launch (ncu)",
+                "bytes_per_launch": mv_bytes, "ms_per_launch": kt["row_field"],
                 "step_bytes": step_bytes, "step_gbs": step_bytes / (ms_max * 1e-3) / 1e9,
                 "step_frac": step_bytes / (ms_max * 1e-3) / 1e9 / peak,
             },
