@@ -413,6 +413,133 @@ def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
 from ctypes import byref, c_double as C_double, c_void_p as C_void_p  # noqa: E402
 
 
+# ----------------------------------------------------------------------------- other workloads
+def batch_workload():
+    """16 boxes of uneven sizes (4 each of 216 / 512 / 1000 / 2197 waters, edges 1.86 / 2.48 / 3.10 /
+    4.04 nm, PME 32^3 / 48^3 / 64^3 / 72^3) at 298 K plus 32 REMD replicas of 512 waters (2.483 nm,
+    48^3) on a geometric 280-400 K ladder, all in one engine."""
+    from pgm_jax_b200.remd import geometric_ladder
+    from pgm_jax_b200.systems import water_box
+
+    boxes, grids, temps = [], [], []
+    for k, (n, L, K) in enumerate([(6, 1.86, 32), (8, 2.48, 48), (10, 3.10, 64), (13, 4.04, 72)]):
+        for r in range(4):
+            boxes.append(water_box(n, L, seed=100 + 4 * k + r))
+            grids.append((K, K, K))
+            temps.append(TEMP)
+    ladder = geometric_ladder(280.0, 400.0, 32)
+    for r in range(32):
+        boxes.append(water_box(8, 2.483, seed=200 + r))
+        grids.append((48, 48, 48))
+    temps += list(ladder)
+    return boxes, grids, np.array(temps), ladder
+
+
+def make_md(boxes, grids, temps, predictor, rank, torch, gamma=GAMMA):
+    from pgm_jax_b200.forcefield import PGMForceField
+    from pgm_jax_b200.md import RigidMD
+
+    ff = PGMForceField([b[0] for b in boxes], [b[2] for b in boxes], settings(predictor=predictor), pme_grids=grids,
+                       device=torch.cuda.current_device())
+    md = RigidMD(ff, np.concatenate([b[1] for b in boxes]), np.stack([b[2] for b in boxes]), temperature=temps, dt_fs=DT_FS,
+                 gamma_ps=gamma, seed=1 + rank)
+    return ff, md
+
+
+def run_workload(args) -> None:
+    """--workload batch: the uneven boxes + REMD replicas in one launch, exchanges every 100 steps
+    inside the timed region.  --workload water32768: 32,768 waters (9.93 nm, PME 192^3), the learned
+    guess (trained on the 4096-water workload) against plain CG from mu1 and mu4."""
+    import torch
+
+    from pgm_jax_b200.remd import ReplicaExchange, RigidReplicas
+    from pgm_jax_b200.systems import water_box
+
+    torch.cuda.set_device(0)
+    line = {"metric": METRIC, "unit": "ns/day", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "dtype": "f32+f64", "workload": args.workload}
+    if args.workload == "batch":
+        boxes, grids, temps, ladder = batch_workload()
+        ff, md = make_md(boxes, grids, temps, "mu4", 0, torch)
+        equilibrate(md, 500)
+        rex = ReplicaExchange(RigidReplicas(md, systems=range(16, 48)), ladder, seed=1)
+        md.step()
+        md.capture()
+        md.run(5)
+        md.stream.synchronize()
+        blocks = max(1, args.steps // 100)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        it_sum = torch.zeros(ff.nsys, dtype=torch.int64, device=ff.device)
+        clk = Clocks(0)
+        ev0.record(md.stream)
+        for _ in range(blocks):
+            for _ in range(100):
+                md.run(1)
+                with torch.cuda.stream(md.stream):
+                    it_sum += md.result.iterations.to(torch.int64)
+            rex.exchange()  # host: energies of the replicas, Metropolis, temperatures, momenta
+        ev1.record(md.stream)
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        steps = 100 * blocks
+        ms = ev0.elapsed_time(ev1) / steps
+        its = it_sum.cpu().numpy() / steps
+        line.update({
+            "value": ns_per_day(ms), "ms_per_step": ms, "steps": steps, "systems": ff.nsys, "atoms": ff.n,
+            "system_ns_per_day": ns_per_day(ms) * ff.nsys, "atom_steps_per_s": ff.n * 1e3 / ms,
+            "cg_iters_per_step_mean": float(its.mean()), "cg_iters_per_step_max": float(its.max()),
+            "exchange_acceptance": rex.stats.neighbour_acceptance().tolist(), "exchanges": rex.stats.n_exchanges,
+            "status_any": int(md.result.status.max()), "clocks": clocks, "row_capacity": ff.capacity,
+            "config": {"workload": "4 x (216 @ 1.86 nm, 32^3; 512 @ 2.48 nm, 48^3; 1000 @ 3.10 nm, 64^3; 2197 @ 4.04 nm, "
+                       "72^3) at 298 K + 32 x 512 waters REMD 280-400 K (geometric), one engine, mixed, CG 1e-6 from mu4, "
+                       "Langevin 2/ps, dt 1 fs, exchanges every 100 steps (timed)", "equilibration": "500 steps at 20/ps"},
+        })
+    else:  # water32768
+        from pgm_jax_b200.forcefield import PGMForceField
+        from pgm_jax_b200.md import RigidMD
+
+        s4, p4, H4 = water_box(N_SIDE, EDGE_NM, seed=0)
+        ff4 = PGMForceField(s4, H4, settings(predictor="nn"), device=0)
+        md4 = RigidMD(ff4, p4, H4, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1)
+        equilibrate(md4)
+        from pgm_jax_b200.learned import GuessModel, collect, guess_errors
+
+        train = collect(md4, 64)
+        model = GuessModel(seed=0)
+        model.train(train, iters=2000, batch=32768, lr=2e-3)
+        del md4, ff4
+        big = [water_box(32, 9.93, seed=0)]
+        arms = {}
+        for pred in ("nn", "mu1", "mu4"):
+            ff, md = make_md(big, [(192, 192, 192)], [TEMP], pred, 0, torch)
+            equilibrate(md, 300)
+            info = None
+            if pred == "nn":
+                held = collect(md, 6)
+                info = guess_errors(model, held)
+                model.install(ff)
+            for _ in range(4):
+                md.step()
+            md.capture()
+            md.run(3)
+            md.stream.synchronize()
+            ms, n_it = timed_replays(md, max(10, min(args.steps, 200)), torch)
+            arms[pred] = {"value": ns_per_day(ms), "ms_per_step": ms, "cg_iters_per_step": n_it}
+            if info:
+                arms[pred]["guess_rms_e_nm_held_out"] = info
+            pairs = int(ff._lib.pgm_row_pairs(ff._h))
+            arms[pred]["step_bytes"] = bytes_per_step(ff.n, pairs, n_it, 192)
+            arms[pred]["step_frac_of_hbm"] = arms[pred]["step_bytes"] / (ms * 1e-3) / 1e9 / peaks()[0]
+            del md, ff
+        line.update({"value": arms["nn"]["value"], "ms_per_step": arms["nn"]["ms_per_step"],
+                     "cg_iters_per_step": arms["nn"]["cg_iters_per_step"], "arms": arms, "atoms": 98304,
+                     "nn_over_plain_cg": {p: arms["nn"]["value"] / arms[p]["value"] for p in ("mu1", "mu4")},
+                     "config": {"workload": "32768 rigid pGM3P-25 waters, 9.93 nm, PME 192^3 o6, rc 0.9 nm, Langevin 298 K "
+                                "2/ps, dt 1 fs, mixed, CG 1e-6; model trained on 64 frames of the 4096-water workload",
+                                "equilibration": "300 steps at 20/ps per arm"}})
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -421,11 +548,15 @@ def main() -> None:
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
+    ap.add_argument("--workload", default="water4096", choices=["water4096", "batch", "water32768"],
+                    help="water4096: the headline; the others print their own line (one GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "water4096":
+        run_workload(args)
     else:
         run_engine(args)
 

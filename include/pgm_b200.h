@@ -260,6 +260,9 @@ PgmStatus pgm_rigid_end_step(PgmRigid *r, void *stream, double dt, const double 
                              double *angmom);
 /* Kinetic energy per system (device, n_systems). */
 PgmStatus pgm_rigid_kinetic(PgmRigid *r, void *stream, const double *mom, const double *angmom, double *ke);
+/* Momenta and angular momenta of each system's molecules times factor[system] (device,
+ * n_systems): the sqrt(T_new / T_old) rescaling of a replica exchange (pgm_jax/md/remd.py:571-611). */
+PgmStatus pgm_rigid_scale_momenta(PgmRigid *r, void *stream, const double *factor, double *mom, double *angmom);
 const char *pgm_rigid_last_error(void);
 
 /* Stream capture of engine calls into a replayable CUDA graph (exec is a cudaGraphExec_t). */

@@ -173,6 +173,18 @@ __global__ void k_md_kinetic(MDDev d, const double *P, const double *L, double *
   atomicAdd(&ke[d.msys[m]], e);
 }
 
+// Momenta (linear and angular) of every molecule times the factor of its system (replica
+// exchange: sqrt(T_new / T_old) for a configuration that changes temperature, remd.py:571-611).
+__global__ void k_md_scale(MDDev d, const double *factor, double *P, double *L) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= d.nmol) return;
+  double f = factor[d.msys[m]];
+  for (int c = 0; c < 3; ++c) {
+    P[3 * m + c] *= f;
+    L[3 * m + c] *= f;
+  }
+}
+
 thread_local std::string g_md_err;
 
 }  // namespace
@@ -270,6 +282,13 @@ PgmStatus pgm_rigid_kinetic(PgmRigid *r, void *stream, const double *mom, const 
   if (!r || !mom || !angmom || !ke) return PGM_ERR_INVALID;
   MDCK(cudaMemsetAsync(ke, 0, sizeof(double) * r->nsys, (cudaStream_t)stream));
   k_md_kinetic<<<(r->nmol + 127) / 128, 128, 0, (cudaStream_t)stream>>>(r->dev(), mom, angmom, ke);
+  MDCK(cudaGetLastError());
+  return PGM_OK;
+}
+
+PgmStatus pgm_rigid_scale_momenta(PgmRigid *r, void *stream, const double *factor, double *mom, double *angmom) {
+  if (!r || !factor || !mom || !angmom) return PGM_ERR_INVALID;
+  k_md_scale<<<(r->nmol + 127) / 128, 128, 0, (cudaStream_t)stream>>>(r->dev(), factor, mom, angmom);
   MDCK(cudaGetLastError());
   return PGM_OK;
 }

@@ -190,6 +190,21 @@ class RigidMD:
                 self._step_enqueue()
             self.step_count += 1
 
+    def set_temperatures(self, temps) -> None:
+        """Thermostat temperature of every system [K] (written in place: captured steps see it)."""
+        temps = np.broadcast_to(np.asarray(temps, float), (self.ff.nsys,)).copy()
+        self.temps = temps
+        with torch.cuda.stream(self.stream):
+            self.kT.copy_(torch.tensor(KB * temps, dtype=torch.float64), non_blocking=False)
+
+    def scale_momenta(self, factors) -> None:
+        """Linear and angular momenta of every system's molecules times its factor (on the MD stream)."""
+        f = torch.tensor(np.broadcast_to(np.asarray(factors, float), (self.ff.nsys,)).copy(), dtype=torch.float64,
+                         device=self.dev)
+        with torch.cuda.stream(self.stream):
+            _lib.check(self._lib.pgm_rigid_scale_momenta(self._h, self._stream(), _p(f), _p(self.mom), _p(self.angmom)))
+        self.stream.synchronize()
+
     def kinetic(self) -> np.ndarray:
         ke = torch.zeros(self.ff.nsys, dtype=torch.float64, device=self.dev)
         self.stream.wait_stream(torch.cuda.current_stream(self.dev))
