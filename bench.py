@@ -494,6 +494,43 @@ def run_workload(args) -> None:
                        "72^3) at 298 K + 32 x 512 waters REMD 280-400 K (geometric), one engine, mixed, CG 1e-6 from mu4, "
                        "Langevin 2/ps, dt 1 fs, exchanges every 100 steps (timed)", "equilibration": "500 steps at 20/ps"},
         })
+    elif args.workload == "pimd":
+        from pgm_jax_b200.forcefield import MDSettings
+        from pgm_jax_b200.pimd import PIMD
+
+        s, pos, H = water_box(11, 3.13, seed=0, n_water=1024)
+        st = MDSettings(precision="mixed", cutoff=0.9, ewald_beta=4.0, pme_grid=(64, 64, 64), pme_order=6, dipole_tol=TOL,
+                        max_iter=100, predictor="mu4")
+        pm = PIMD(s, pos, H, st, beads=32, temperature=300.0, dt_fs=0.5, mode="pimd", seed=1)
+        for _ in range(5):
+            pm.step()
+        pm.capture()
+        pm.run(200)  # relaxation of the lattice start (captured steps)
+        pm.stream.synchronize()
+        steps = max(10, min(args.steps, 200))
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        it_sum = torch.zeros(32, dtype=torch.int64, device=pm.dev)
+        clk = Clocks(0)
+        ev0.record(pm.stream)
+        for _ in range(steps):
+            pm.run(1)
+            with torch.cuda.stream(pm.stream):
+                it_sum += pm.result.iterations.to(torch.int64)
+        ev1.record(pm.stream)
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        ms = ev0.elapsed_time(ev1) / steps
+        est = pm.estimators()
+        line.update({
+            "value": 86.4 * 0.5 / ms, "ms_per_step": ms, "steps": steps, "beads": 32, "atoms": 3072, "bead_atoms": 98304,
+            "cg_iters_per_step_mean": float(it_sum.float().mean().item()) / steps, "clocks": clocks,
+            "t_centroid_K": est["t_centroid"], "t_internal_modes_K": float(np.mean(est["t_modes"][1:])),
+            "kinetic_prim_per_atom_kjmol": est["prim"] / 3072, "kinetic_cv_per_atom_kjmol": est["cv"] / 3072,
+            "status_any": int(pm.result.status.max()),
+            "config": {"workload": "PIMD 32 beads x 1024 flexible pGM waters (q-TIP4P/F intramolecular), 3.13 nm, PME 64^3 o6, "
+                       "rc 0.9 nm, 300 K PILE-L (tau_centroid 0.2 ps), dt 0.5 fs, mixed, CG 1e-6 from mu4 per bead, "
+                       "all beads in one engine", "equilibration": "205 steps from the lattice + free ring polymer start"},
+        })
     else:  # water32768
         from pgm_jax_b200.forcefield import PGMForceField
         from pgm_jax_b200.md import RigidMD
@@ -548,7 +585,7 @@ def main() -> None:
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
-    ap.add_argument("--workload", default="water4096", choices=["water4096", "batch", "water32768"],
+    ap.add_argument("--workload", default="water4096", choices=["water4096", "batch", "water32768", "pimd"],
                     help="water4096: the headline; the others print their own line (one GPU)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -265,6 +265,28 @@ PgmStatus pgm_rigid_kinetic(PgmRigid *r, void *stream, const double *mom, const 
 PgmStatus pgm_rigid_scale_momenta(PgmRigid *r, void *stream, const double *factor, double *mom, double *angmom);
 const char *pgm_rigid_last_error(void);
 
+/* ------------------------------------------------------------------ path-integral MD
+ * The ring-polymer integrator around the batched force field (pgm_jax/md/pimd.py:484-700): the P
+ * beads are the systems of one engine batch, positions / momenta / forces bead-major (atom i of
+ * bead k at k N + i, (P N, 3) doubles).  A step: pgm_pimd_kick(dt/2), pgm_pimd_free_thermostat
+ * (Cayley A(dt/2), PILE-L O(dt), A(dt/2) in normal modes), the force call on all beads (+
+ * pgm_water_bonded for flexible water), pgm_pimd_kick(dt/2). */
+/* mom += h forces over n3 = 3 P N doubles. */
+PgmStatus pgm_pimd_kick(void *stream, long long n3, double h, const double *forces, double *mom);
+/* A O A in normal modes (pimd.py:222-296, 411-440): C (P, P) row-major normal-mode matrix
+ * (C[j][l], bead j, mode l), omega (P,) mode frequencies [rad/ps], gamma (P,) frictions [1/ps]
+ * (all 0: RPMD), mass (N,) [amu], kT_P = P kB T [kJ/mol]; the noise is drawn from (seed, *counter),
+ * and the device counter advances by one.  1 <= P <= 32.  All pointers device. */
+PgmStatus pgm_pimd_free_thermostat(void *stream, int beads, int n_atoms, const double *C, const double *omega, const double *gamma,
+                                   const double *mass, double dt, double kT_P, uint64_t seed, uint64_t *counter, double *pos,
+                                   double *mom);
+/* q-TIP4P/F intramolecular water term (pgm_jax/models/water.py:33-69) for molecules O, H, H at
+ * first_atom[m]: params (host, 5) = D [kJ/mol], alpha [1/nm], r_eq [nm], k_theta [kJ/mol/rad^2],
+ * theta_eq [rad]; forces += its forces; energy[mol_system[m]] += its energy (energy may be NULL). */
+PgmStatus pgm_water_bonded(void *stream, int n_mol, const int32_t *first_atom, const int32_t *mol_system, const double *pos,
+                           const double *params, double *forces, double *energy);
+const char *pgm_pimd_last_error(void);
+
 /* Stream capture of engine calls into a replayable CUDA graph (exec is a cudaGraphExec_t). */
 PgmStatus pgm_graph_begin(void *stream);
 PgmStatus pgm_graph_end(void *stream, void **exec_out);

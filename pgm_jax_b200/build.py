@@ -8,7 +8,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libpgm_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", n) for n in ("pgm_api.cu", "pgm_md.cu", "pgm_static.cu", "pgm_nn.cu")]
+SOURCES = [os.path.join(HERE, "csrc", n) for n in ("pgm_api.cu", "pgm_md.cu", "pgm_static.cu", "pgm_nn.cu", "pgm_pimd.cu")]
 DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "pgm_device.cuh"),
     os.path.join(HERE, "csrc", "pgm_kernels.cuh"),

@@ -118,12 +118,14 @@ def water_geometry(r: float = 0.09572, theta_deg: float = 104.52) -> np.ndarray:
     return np.array([[0, 0, 0], [r * np.sin(t), r * np.cos(t), 0], [-r * np.sin(t), r * np.cos(t), 0]])
 
 
-def water_box(n_side: int, edge_nm: float, seed: int = 0, jitter: float = 0.01, mol: Molecule | None = None):
+def water_box(n_side: int, edge_nm: float, seed: int = 0, jitter: float = 0.01, mol: Molecule | None = None,
+              n_water: int | None = None):
     """Return (System, positions (3 n^3, 3) [nm], box (3, 3) [nm]) of a jittered lattice of waters.
 
     Orientations are the Q factor of a Gaussian 3x3 matrix from np.random.default_rng(seed), as in
     toy.water_lattice (toy.py:107-141); each molecule is centred on its cell centre plus Gaussian
-    jitter of `jitter` nm (as toy.small_box, toy.py:173).
+    jitter of `jitter` nm (as toy.small_box, toy.py:173).  n_water < n^3: that many sites of the
+    lattice, chosen at random (seeded), the others left empty.
     """
     rng = np.random.default_rng(seed)
     w = water_geometry()
@@ -136,8 +138,13 @@ def water_box(n_side: int, edge_nm: float, seed: int = 0, jitter: float = 0.01, 
                 Q = np.linalg.qr(rng.normal(size=(3, 3)))[0]
                 c = (np.array([i, j, k]) + 0.5) * sp + rng.normal(scale=jitter, size=3)
                 pos.append(w @ Q.T + c)
+    nw = n_side**3
+    if n_water is not None and n_water < nw:
+        keep = np.sort(rng.choice(nw, size=n_water, replace=False))
+        pos = [pos[k] for k in keep]
+        nw = n_water
     m = pgm3p25_water() if mol is None else mol
-    return System([m] * n_side**3), np.concatenate(pos), np.eye(3) * edge_nm
+    return System([m] * nw), np.concatenate(pos), np.eye(3) * edge_nm
 
 
 # ----------------------------------------------------------------------------- toy systems
