@@ -73,11 +73,14 @@ def equilibrate(md, steps: int = EQUIL_STEPS) -> None:
 ROWFIELD_NCU_DRAM_BYTES, ROWFIELD_NCU_PAIRS = 93.654784e6 + 3.39328e6, 3.745e6
 
 
+SPLIT: dict = {}  # --elec-cutoff: split rows (elec_cutoff, ewald_beta for it; the 96^3 mesh fits its spacing)
+
+
 def settings(precision="mixed", predictor="mu4"):
     from pgm_jax_b200.forcefield import MDSettings
 
-    return MDSettings(precision=precision, cutoff=0.9, ewald_beta=4.0, pme_grid=(GRID, GRID, GRID), pme_order=6,
-                      dipole_tol=TOL, max_iter=100, predictor=predictor)
+    return MDSettings(precision=precision, cutoff=0.9, ewald_beta=SPLIT.get("ewald_beta", 4.0), pme_grid=(GRID, GRID, GRID),
+                      pme_order=6, dipole_tol=TOL, max_iter=100, predictor=predictor, elec_cutoff=SPLIT.get("elec_cutoff"))
 
 
 def ns_per_day(ms_per_step: float) -> float:
@@ -608,9 +611,17 @@ def main() -> None:
     ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
     ap.add_argument("--workload", default="water4096", choices=["water4096", "batch", "water32768", "pimd"],
                     help="water4096: the headline; the others print their own line (one GPU)")
+    ap.add_argument("--elec-cutoff", type=float, default=None,
+                    help="split rows: electrostatics cutoff [nm] below the 0.9 nm LJ cutoff (Ewald coefficient for it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.elec_cutoff:
+        from pgm_jax_b200.forcefield import elec_cutoff_settings
+
+        SPLIT.update(elec_cutoff_settings(args.elec_cutoff))
+        CONFIG["workload"] += f"; split rows: electrostatics {args.elec_cutoff} nm, beta {SPLIT['ewald_beta']:.4f}/nm"
+        CONFIG["elec_cutoff_nm"] = args.elec_cutoff
     if args.impl == "reference":
         run_reference(args)
     elif args.workload != "water4096":

@@ -65,6 +65,12 @@ typedef struct {
     double skin;        /* Verlet skin of the engine's candidate list [nm] (NeighborList.skin); clipped so
                            that cutoff + skin fits the smallest box, 0: rebuilt every step */
     int list_capacity;  /* candidates kept per atom; 0: sized from the density */
+    double elec_cutoff; /* electrostatics cutoff [nm] (Cutoffs.elec_cutoff); 0 or = cutoff: one cutoff.
+                           Below cutoff (with vdw "lj") the rows are split (forcefield.py:44-58,
+                           1197-1238): [0, elec_capacity) pairs inside elec_cutoff, then the pairs
+                           between elec_cutoff and cutoff with a nonzero LJ term; the field sweeps
+                           stream the first part only.  ewald_beta and the mesh must suit it. */
+    int elec_capacity;  /* split rows: electrostatic pairs kept per row (0: from the density) */
 } PgmSettings;
 
 /* One system of the batch: topology and parameters (host arrays, copied at creation). */
@@ -146,6 +152,11 @@ int pgm_row_capacity(const PgmHandle *h);
 
 /* Candidates kept per atom in the engine's Verlet list (rounded up to a multiple of 32; 0:
  * automatic); the list is rebuilt at the next call. */
+/* Split rows: the electrostatic part of the row capacity (PGM_ERR_INVALID without split rows) and
+ * the largest van der Waals part of the last row build. */
+PgmStatus pgm_set_elec_capacity(PgmHandle *h, int capacity);
+int pgm_elec_capacity(const PgmHandle *h);
+int pgm_max_vdw_count(PgmHandle *h);
 PgmStatus pgm_set_list_capacity(PgmHandle *h, int capacity);
 int pgm_list_capacity(const PgmHandle *h);
 /* Steps since creation at which the candidate list was rebuilt (host counter of calls that found

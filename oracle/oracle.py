@@ -34,7 +34,7 @@ class _Set(C.Structure):
     _fields_ = [
         ("perm", _i), ("induce", _i), ("lj", _i), ("lj_lrc", _i), ("cutoff", _d), ("beta", _d), ("K", _i * 3),
         ("order", _i), ("tol", _d), ("max_iter", _i), ("predictor", _i), ("fused", _i), ("norm_refresh", _i),
-        ("peek", _d), ("nthreads", _i),
+        ("peek", _d), ("nthreads", _i), ("elec_cutoff", _d),
     ]
 
 
@@ -103,6 +103,7 @@ class Oracle:
             float(st.get("cutoff", 0.9)), float(st.get("ewald_beta", 4.0)), (_i * 3)(*K), int(st.get("pme_order", 6)),
             float(st.get("dipole_tol", 1e-5)), int(st.get("max_iter", 50)), pred, int(st.get("fused", True)),
             int(st.get("norm_refresh", 1000)), float(st.get("peek", 0.65)), int(nthreads),
+            float(st.get("elec_cutoff") or 0.0),
         )
 
     def init_induction(self) -> dict:

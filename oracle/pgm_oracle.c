@@ -402,6 +402,7 @@ typedef struct {
     double *x;          /* (pairs, 3) x_i - x_k, minimum image */
     double *G;          /* (pairs, 4) */
     double *wv;         /* van der Waals weight: 0 intramolecular, 1 otherwise */
+    unsigned char *we;  /* 1: inside the electrostatics cutoff (split rows, forcefield.py:1197-1238) */
 } rows_t;
 
 static int *atom_mol(const pgmo_system *sys) {
@@ -437,6 +438,9 @@ static void build_rows(const pgmo_system *sys, const pgmo_settings *s, const dou
     R->x = malloc(sizeof(double) * 3 * (np ? np : 1));
     R->G = malloc(sizeof(double) * 4 * (np ? np : 1));
     R->wv = malloc(sizeof(double) * (np ? np : 1));
+    R->we = malloc(np ? np : 1);
+    const double rce = (s->elec_cutoff > 0.0 && s->elec_cutoff < s->cutoff) ? s->elec_cutoff : s->cutoff;
+    const double rce2 = rce * rce;
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < n; ++i) {
         long long o = R->start[i];
@@ -454,6 +458,7 @@ static void build_rows(const pgmo_system *sys, const pgmo_settings *s, const dou
                 double a = 1.0 / sqrt(2.0 * (sys->radius[i] * sys->radius[i] + sys->radius[k] * sys->radius[k]));
                 pair_kernels(a, s->beta, sqrt(r2), R->G + 4 * o);
                 R->wv[o] = pass == 0 ? 0.0 : 1.0;
+                R->we[o] = r2 < rce2;
                 ++o;
             }
     }
@@ -467,6 +472,7 @@ static void free_rows(rows_t *R) {
     free(R->x);
     free(R->G);
     free(R->wv);
+    free(R->we);
 }
 
 /* sum_k de_ik/dd_i (forcefield.py:1395-1402), q may be NULL. */
@@ -475,6 +481,7 @@ static void row_field(const rows_t *R, int n, const double *q, const double *d, 
     for (int i = 0; i < n; ++i) {
         double f[3] = {0, 0, 0};
         for (long long o = R->start[i]; o < R->start[i + 1]; ++o) {
+            if (!R->we[o]) continue;
             int k = R->k[o];
             const double *x = R->x + 3 * o, *G = R->G + 4 * o, *dk = d + 3 * k;
             double dkx = dk[0] * x[0] + dk[1] * x[1] + dk[2] * x[2];
@@ -710,7 +717,9 @@ static void energy_forces(ctx_t *C, const double *pos, const double *H, const do
             double qi = sys->q[i];
             for (long long o = C->R.start[i]; o < C->R.start[i + 1]; ++o) {
                 int k = C->R.k[o];
-                const double *x = C->R.x + 3 * o, *G = C->R.G + 4 * o, *dk = d + 3 * k;
+                const double *x = C->R.x + 3 * o, *dk = d + 3 * k;
+                /* beyond the electrostatics cutoff only the van der Waals term (split rows) */
+                const double G0[4] = {0, 0, 0, 0}, *G = C->R.we[o] ? C->R.G + 4 * o : G0;
                 double qk = sys->q[k];
                 double dix = di[0] * x[0] + di[1] * x[1] + di[2] * x[2];
                 double dkx = dk[0] * x[0] + dk[1] * x[1] + dk[2] * x[2];

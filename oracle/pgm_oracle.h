@@ -48,6 +48,7 @@ typedef struct {
     int norm_refresh;
     double peek;
     int nthreads;          /* OpenMP threads (0: default) */
+    double elec_cutoff;    /* electrostatics cutoff [nm] (0 or >= cutoff: the pair cutoff; forcefield.py:44-58) */
 } pgmo_settings;
 
 typedef struct {

@@ -18,7 +18,7 @@ _pu = C.POINTER(C.c_uint32)
 # every symbol the header declares (tests check the library exports them)
 EXPORTS = (
     "pgm_create", "pgm_destroy", "pgm_compute", "pgm_compute_host", "pgm_energy", "pgm_energy_fixed_mu", "pgm_field",
-    "pgm_set_row_capacity", "pgm_row_capacity", "pgm_set_list_capacity", "pgm_list_capacity", "pgm_list_rebuilds", "pgm_max_row_count", "pgm_num_atoms", "pgm_num_systems",
+    "pgm_set_row_capacity", "pgm_row_capacity", "pgm_set_elec_capacity", "pgm_elec_capacity", "pgm_max_vdw_count", "pgm_set_list_capacity", "pgm_list_capacity", "pgm_list_rebuilds", "pgm_max_row_count", "pgm_num_atoms", "pgm_num_systems",
     "pgm_last_error", "pgm_last_launch_count", "pgm_launches_per_iteration", "pgm_profile_kernel", "pgm_row_pairs", "pgm_rigid_create", "pgm_rigid_destroy",
     "pgm_rigid_begin_step", "pgm_rigid_set_step", "pgm_rigid_end_step", "pgm_rigid_kinetic", "pgm_rigid_scale_momenta", "pgm_rigid_last_error", "pgm_pimd_kick",
     "pgm_pimd_free_thermostat", "pgm_water_bonded", "pgm_pimd_last_error", "pgm_graph_begin",
@@ -39,7 +39,8 @@ class PgmSettings(C.Structure):
         ("elec", C.c_int), ("vdw", C.c_int), ("lj_lrc", C.c_int), ("precision", C.c_int), ("cutoff", C.c_double),
         ("ewald_beta", C.c_double), ("pme_order", C.c_int), ("dipole_tol", C.c_double), ("max_iter", C.c_int),
         ("predictor", C.c_int), ("fused", C.c_int), ("norm_refresh", C.c_int), ("peek", C.c_double),
-        ("row_capacity", C.c_int), ("skin", C.c_double), ("list_capacity", C.c_int),
+        ("row_capacity", C.c_int), ("skin", C.c_double), ("list_capacity", C.c_int), ("elec_cutoff", C.c_double),
+        ("elec_capacity", C.c_int),
     ]
 
 
@@ -85,6 +86,10 @@ def load(path: str | None = None):
     lib.pgm_field.argtypes = [H, vp, vp, vp, C.c_int, vp, vp]
     lib.pgm_set_row_capacity.argtypes = [H, C.c_int]
     lib.pgm_row_capacity.argtypes = [H]
+    lib.pgm_set_elec_capacity.argtypes = [H, C.c_int]
+    lib.pgm_set_elec_capacity.restype = C.c_int
+    lib.pgm_elec_capacity.argtypes = [H]
+    lib.pgm_max_vdw_count.argtypes = [H]
     lib.pgm_set_list_capacity.argtypes = [H, C.c_int]
     lib.pgm_set_list_capacity.restype = C.c_int
     lib.pgm_list_capacity.argtypes = [H]

@@ -103,6 +103,9 @@ struct EngineBase {
   virtual void fixed_mu(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width,
                         const double *mu, double *energy, double *forces, double *virial, uint32_t *status) = 0;
   virtual void set_capacity(int mc) = 0;
+  virtual bool set_elec_capacity(int c) = 0;
+  virtual int elec_capacity() const = 0;
+  virtual int max_vdw_count() = 0;
   virtual void set_nn(const float *w, float sigma, float rg) = 0;
   virtual void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const float *bl_prev,
                            float *bl_out, float *inv, float *vec) = 0;
@@ -148,6 +151,11 @@ struct Engine : EngineBase {
   PgmSettings set;
   std::vector<pgm::SysInfo> hsys;
   int nmol_total = 0, ncell = 0, ncov = 0, mc = 0, mc_auto = 0, cc = 0, cc_auto = 0;
+  // split rows (elec_cutoff < cutoff): electrostatic part [0, mce) of every row, LJ part [mce, mc)
+  double rc_e = 0.0;
+  bool split = false;
+  int mce = 0, mce_auto = 0;
+  DBuf<int> rnv;
   double skin = 0.0;
   long long rgrid = 0, cgrid = 0;
   std::vector<std::unique_ptr<FftGroup>> gx, gy, gz;
@@ -233,6 +241,7 @@ struct Engine : EngineBase {
     a.rn = rn.p; a.rnsp = rnsp.p; a.rk = rk.p;
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
     a.max_count = dmax.p;
+    a.mce = mce; a.rnv = split ? rnv.p : nullptr; a.rce2 = rc_e * rc_e;
     a.nn_es = nn_es.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
     a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p; a.F = Fv.p;
     a.Q = Q.p; a.Phi = Phi.p; a.Ginf = Ginf.p; a.C = C.p; a.tw = tw.p; a.bmod = bmod.p;
@@ -364,6 +373,16 @@ struct Engine : EngineBase {
     double sphere = 4.0 / 3.0 * M_PI * std::pow(set.cutoff, 3) * rho_max;
     mc_auto = std::max(32, (int)std::ceil((sphere * 1.25 + 16.0) / 32.0) * 32);
     mc = set.row_capacity > 0 ? ((set.row_capacity + 31) / 32) * 32 : mc_auto;
+    rc_e = (set.elec_cutoff > 0 && set.elec_cutoff < set.cutoff && set.vdw) ? set.elec_cutoff : set.cutoff;
+    split = rc_e < set.cutoff;
+    if (split) {
+      double se = 4.0 / 3.0 * M_PI * std::pow(rc_e, 3) * rho_max;
+      mce_auto = std::max(32, (int)std::ceil((se * 1.25 + 16.0) / 32.0) * 32);
+      mce = set.elec_capacity > 0 ? ((set.elec_capacity + 31) / 32) * 32 : mce_auto;
+      mc = std::max(mc, mce + 32);
+    } else {
+      mce = mc;
+    }
     // Verlet skin: cutoff + skin must stay within half of every box (minimum image)
     double halfmin = 1e300;
     for (int si = 0; si < n; ++si) {
@@ -436,7 +455,8 @@ struct Engine : EngineBase {
     CK(cudaMemset(cell_count.p, 0, sizeof(int) * ncell));
     CK(cudaMemset(nb_builds.p, 0, sizeof(long long)));
     { int one = 1; CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice)); }
-    rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(1); dany.alloc(1);
+    rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(2); dany.alloc(1);
+    if (split) rnv.alloc(nt);
     alloc_rows();
     Q.alloc(rgrid); Phi.alloc(rgrid); Ginf.alloc(cgrid); C.alloc(cgrid);
     CK(cudaMemset(Q.p, 0, sizeof(T) * rgrid));
@@ -545,12 +565,29 @@ struct Engine : EngineBase {
 
   void set_capacity(int c) override {
     int want = c > 0 ? ((c + 31) / 32) * 32 : mc_auto;
+    if (split) want = std::max(want, mce + 32);
     if (want != mc) {
       mc = want;
+      if (!split) mce = mc;
       alloc_rows();
     }
   }
   int capacity() const override { return mc; }
+  bool set_elec_capacity(int c) override {
+    if (!split) return false;
+    mce = c > 0 ? ((c + 31) / 32) * 32 : mce_auto;
+    if (mc < mce + 32) {
+      mc = mce + 32;
+      alloc_rows();
+    }
+    return true;
+  }
+  int elec_capacity() const override { return mce; }
+  int max_vdw_count() override {
+    int v[2] = {0, 0};
+    CK(cudaMemcpy(v, dmax.p, sizeof(v), cudaMemcpyDeviceToHost));
+    return v[1];
+  }
   long long launches_per_iteration() const override { return per_iter; }
 
   // Average duration [ms] of one launch of a kernel of the last step, re-run `reps` times on the
@@ -618,7 +655,7 @@ struct Engine : EngineBase {
     std::vector<int> h(nt);
     CK(cudaMemcpy(h.data(), rn.p, sizeof(int) * nt, cudaMemcpyDeviceToHost));
     long long t = 0;
-    for (int v : h) t += std::min(v, mc);
+    for (int v : h) t += std::min(v, mce);
     return t;
   }
   int max_count() override {
@@ -638,7 +675,7 @@ struct Engine : EngineBase {
   // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
   // cell list, rows, influence function.
   void prepare(cudaStream_t st, pgm::Dev<T> &a, const double *boxes) {
-    CK(cudaMemsetAsync(dmax.p, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(dmax.p, 0, 2 * sizeof(int), st));
     pgm::k_box<T><<<grid1(nsys, 64), 64, 0, st>>>(a, boxes); check_launch();
     pgm::k_prep<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
     pgm::k_mol<T><<<grid1(nmol_total), 256, 0, st>>>(a); check_launch();
@@ -903,6 +940,10 @@ PgmStatus pgm_create(const PgmSettings *s, const PgmSystemDesc *systems, int n, 
   if (s->predictor != 0 && s->predictor != 1 && s->predictor != 3 && s->predictor != 4 && s->predictor != 5)
     return fail(PGM_ERR_INVALID, "predictor must be 0 (none), 1 (previous step), 3 (mu3), 4 (mu4) or 5 (learned guess)");
   if (s->max_iter < 0) return fail(PGM_ERR_INVALID, "max_iter must be >= 0");
+  if (s->elec_cutoff < 0 || s->elec_cutoff > s->cutoff)
+    return fail(PGM_ERR_INVALID, "elec_cutoff must be 0 (none) or in (0, cutoff]");
+  if (s->elec_capacity != 0 && !(s->elec_cutoff > 0 && s->elec_cutoff < s->cutoff && s->vdw))
+    return fail(PGM_ERR_INVALID, "elec_capacity applies only to split rows (elec_cutoff < cutoff with a van der Waals term)");
   for (int i = 0; i < n; ++i) {
     const PgmSystemDesc &d = systems[i];
     if (d.n_atoms <= 0 || d.n_mol <= 0 || !d.mol_start || !d.q || !d.radius || !d.alpha || !d.lj_rmin_half || !d.lj_sqrt_eps ||
@@ -1121,6 +1162,27 @@ long long pgm_list_rebuilds(PgmHandle *h) {
   if (!h) return -1;
   try {
     return h->eng->list_rebuilds();
+  } catch (CudaError &e) {
+    g_err = e.msg;
+    return -1;
+  }
+}
+
+PgmStatus pgm_set_elec_capacity(PgmHandle *h, int capacity) {
+  if (!h || capacity < 0) return fail(PGM_ERR_INVALID, "bad argument");
+  try {
+    CK(cudaSetDevice(h->device));
+    if (!h->eng->set_elec_capacity(capacity)) return fail(PGM_ERR_INVALID, "elec_capacity applies only to split rows");
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+int pgm_elec_capacity(const PgmHandle *h) { return h ? h->eng->elec_capacity() : -1; }
+int pgm_max_vdw_count(PgmHandle *h) {
+  if (!h) return -1;
+  try {
+    return h->eng->max_vdw_count();
   } catch (CudaError &e) {
     g_err = e.msg;
     return -1;

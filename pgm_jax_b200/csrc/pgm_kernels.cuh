@@ -57,7 +57,12 @@ struct Dev {
   // rows
   int *rn, *rnsp, *rk;
   T *rx, *ry, *rz, *rg0, *rg1, *rg2, *rg3;
-  int *max_count;
+  int *max_count;  // [0] largest electrostatic (or only) part, [1] largest van der Waals part
+  // split rows: the electrostatic part of a row is [0, mce), the van der Waals part [mce, mc) with
+  // its counts in rnv (null: one cutoff, mce == mc); rce2 = elec_cutoff^2
+  int mce;
+  int *rnv;
+  double rce2;
   // the learned guess's graph (row entries with r^2 < nn_rg2): row slots [atom][nn_emax] and
   // counts, written by the row build when nn_es is set (a count above nn_emax: scan the row)
   uint16_t *nn_es;
@@ -344,18 +349,34 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 // G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] (forcefield.py:1314-1338, kernels.py:76-118).
 template <typename T>
 __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, double x, double y, double z, size_t base, int &count,
-                                         int lane, int i, int &ecount) {
+                                         int lane, int i, int &ecount, int &vcount, bool special) {
   const unsigned lt = (1u << lane) - 1u;
+  const double r2 = x * x + y * y + z * z;
+  bool kv = false;
+  if (a.rnv && keep && !(r2 < a.rce2)) {  // split rows: beyond elec_cutoff only pairs with an LJ term stay
+    kv = !special && j >= 0 && a.seps[i] * a.seps[j] != T(0);  // molecule partners have LJ weight 0
+    keep = false;
+  }
   unsigned bal = __ballot_sync(0xffffffffu, keep);
   const int slot = count + __popc(bal & lt);
-  if (keep && slot < a.mc) {
+  if (keep && slot < a.mce) {
     size_t o = base + slot;
     a.rk[o] = j;
     a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
   }
   count += __popc(bal);
+  if (a.rnv) {
+    unsigned bv = __ballot_sync(0xffffffffu, kv);
+    const int sv = vcount + __popc(bv & lt);
+    if (kv && sv < a.mc - a.mce) {
+      size_t o = base + a.mce + sv;
+      a.rk[o] = j;
+      a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
+    }
+    vcount += __popc(bv);
+  }
   if (a.nn_es) {  // graph edges of the learned guess: the slots of the short entries
-    bool sh = keep && slot < a.mc && float(x * x + y * y + z * z) < a.nn_rg2;
+    bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
     unsigned eb = __ballot_sync(0xffffffffu, sh);
     int at = ecount + __popc(eb & lt);
     if (sh && at < a.nn_emax) a.nn_es[(size_t)i * a.nn_emax + at] = (uint16_t)slot;
@@ -379,7 +400,7 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
   double4 pi = a.pos4[i];
   double rc2 = a.cutoff * a.cutoff;
   size_t base = (size_t)i * a.mc;
-  int count = 0, ecount = 0;
+  int count = 0, ecount = 0, vcount = 0;
   int mf = a.molfirst[i], me = a.molend[i];
   for (int j0 = mf; j0 < me; j0 += 32) {
     int j = j0 + lane;
@@ -391,7 +412,7 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, true);
   }
   int nsp = count;
   int mi = (int)pi.w;
@@ -427,14 +448,19 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, false);
   }
   if (lane == 0) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
     if (a.nn_es) a.nn_ne[i] = ecount;
-    if (count > a.mc) atomicOr(&a.status[s], 0x1u);
+    if (count > a.mce) atomicOr(&a.status[s], 0x1u);
     atomicMax(a.max_count, count);
+    if (a.rnv) {
+      a.rnv[i] = vcount;
+      if (vcount > a.mc - a.mce) atomicOr(&a.status[s], 0x1u);
+      atomicMax(a.max_count + 1, vcount);
+    }
   }
 }
 
@@ -442,7 +468,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_row_kernels(Dev<T> a) {
   size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   int i = (int)(t / a.mc), slot = (int)(t - (size_t)i * a.mc);
-  if (i >= a.nt || slot >= min(a.rn[i], a.mc)) return;
+  if (i >= a.nt || slot >= min(a.rn[i], a.mce)) return;
   size_t o = (size_t)i * a.mc + slot;
   T x = a.rx[o], y = a.ry[o], z = a.rz[o];
   int k = a.rk[o];
@@ -995,7 +1021,7 @@ __global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restr
   if (i >= S.atom0 + S.natom) return;
   if (ACT == 1 && !a.cg[s].active) return;
   if (ACT == 2 && !a.cg[s].sweep2) return;
-  int n = min(a.rn[i], a.mc);
+  int n = min(a.rn[i], a.mce);
   size_t base = (size_t)i * a.mc;
   T f0 = 0, f1 = 0, f2 = 0;
   auto pair = [&](int k, T x, T y, T z, T g1, T g2) {
@@ -1049,7 +1075,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
   if (ACT == 2 && !a.cg[s].sweep2) return;
   double dotv = 0.0;
   if (valid) {
-    int n = ROWS ? min(a.rn[i], a.mc) : 0;
+    int n = ROWS ? min(a.rn[i], a.mce) : 0;
     size_t base = (size_t)i * a.mc;
     T f0 = 0, f1 = 0, f2 = 0;
     auto pair = [&](int k, T x, T y, T z, T g1, T g2) {
@@ -1169,7 +1195,7 @@ constexpr int NN_EBUF = 64;  // per-warp staging of compacted graph edges (two r
 template <typename T, typename F>
 __device__ __forceinline__ void graph_edges(const Dev<T> &a, int i, float rg, float4 *buf, int *bo, F &&edge) {
   const int lane = threadIdx.x & 31;
-  const int n = min(a.rn[i], a.mc);
+  const int n = min(a.rn[i], a.mce);
   const size_t base = (size_t)i * a.mc;
   const float rg2 = rg * rg;
   int cnt = 0;
@@ -1688,7 +1714,7 @@ __global__ void __launch_bounds__(256) k_forces(Dev<T> a, const double *mu) {
     const BoxInfo &B = a.box[s];
     v4<T> di = a.D[i];
     T qi = a.q[i], rhi = a.rminh[i], sei = a.seps[i];
-    int n = min(a.rn[i], a.mc), nsp = a.rnsp[i];
+    int n = min(a.rn[i], a.mce), nsp = a.rnsp[i];
     size_t base = (size_t)i * a.mc;
     T gx0 = 0, gx1 = 0, gx2 = 0, gl0 = 0, gl1 = 0, gl2 = 0, fd0 = 0, fd1 = 0, fd2 = 0;
     T ee = 0, el = 0;
@@ -1725,6 +1751,24 @@ __global__ void __launch_bounds__(256) k_forces(Dev<T> a, const double *mu) {
       w[0] += kx * x; w[1] += kx * y; w[2] += kx * z;
       w[3] += ky * x; w[4] += ky * y; w[5] += ky * z;
       w[6] += kz * x; w[7] += kz * y; w[8] += kz * z;
+    }
+    if (a.rnv) {  // split rows: the LJ pairs between elec_cutoff and cutoff
+      const int nv = min(a.rnv[i], a.mc - a.mce);
+      for (int t = lane; t < nv; t += 32) {
+        size_t o = base + a.mce + t;
+        int k = a.rk[o];
+        T x = a.rx[o], y = a.ry[o], z = a.rz[o];
+        T rm = rhi + a.rminh[k], ep = sei * a.seps[k];
+        T r2 = x * x + y * y + z * z;
+        T s2 = rm * rm / r2, s6 = s2 * s2 * s2;
+        el += ep * (s6 * s6 - T(2) * s6);
+        T dl = ep * T(12) * (s6 - s6 * s6) / r2;
+        gl0 += dl * x; gl1 += dl * y; gl2 += dl * z;
+        T kx = dl * x, ky = dl * y, kz = dl * z;
+        w[0] += kx * x; w[1] += kx * y; w[2] += kx * z;
+        w[3] += ky * x; w[4] += ky * y; w[5] += ky * z;
+        w[6] += kz * x; w[7] += kz * y; w[8] += kz * z;
+      }
     }
     // reciprocal gradients of the atom
     int4 b = a.base[i];

@@ -18,6 +18,8 @@ import ctypes as C
 import dataclasses as _dc
 from typing import NamedTuple
 
+import math
+
 import numpy as np
 import torch
 
@@ -34,7 +36,7 @@ PREDICTORS = {"none": 0, "mu1": 1, "mu3": 3, "mu4": 4, "nn": 5}
 # preconditioner, the "ls" predictor, differentiable solves) are outside this path.
 _OUT_OF_SCOPE = {
     "iel", "iel_iter", "iel_order", "iel_kappa", "iel_alpha", "iel_precond", "iel_omega", "iel_shadow", "long_range",
-    "ips_order", "ips_boundary", "de_alpha", "de_beta", "gvdw_rep", "elec_cutoff", "local_cut", "local_niter",
+    "ips_order", "ips_boundary", "de_alpha", "de_beta", "gvdw_rep", "local_cut", "local_niter",
     "extrap_order", "extrap_steps", "differentiable", "adjoint_tol", "neighbor_list",
 }
 
@@ -47,6 +49,7 @@ class MDSettings:
     vdw: str = "lj"
     lj_lrc: bool = True
     cutoff: float = 0.9
+    elec_cutoff: float | None = None  # < cutoff with vdw "lj": split rows (forcefield.py:44-58)
     skin: float = 0.1
     ewald_beta: float = 4.0
     pme_grid: tuple | None = None
@@ -80,6 +83,12 @@ class MDSettings:
             raise ValueError(f"precision {self.precision!r} (mixed | double)")
         if not (self.cutoff > 0):
             raise ValueError("cutoff must be positive")
+        if self.elec_cutoff is not None and not (0 < self.elec_cutoff <= self.cutoff):
+            raise ValueError("elec_cutoff must be in (0, cutoff] (or None)")
+
+    @property
+    def split_rows(self) -> bool:
+        return self.elec_cutoff is not None and self.elec_cutoff < self.cutoff and self.vdw != "none"
 
     @property
     def has_induction(self) -> bool:
@@ -88,6 +97,37 @@ class MDSettings:
     @property
     def perm_dipoles(self) -> bool:
         return "p" in self.elec
+
+
+DSUM_TOL = 3.95e-8  # Amber-convention direct-sum tolerance of the default pair 0.9 nm / 4.0 nm^-1
+
+
+def ewald_beta_for(elec_cutoff: float, dsum_tol: float = DSUM_TOL) -> float:
+    """Ewald coefficient [1/nm] with erfc(beta rc) / rc_A = dsum_tol, rc_A the cutoff in Angstrom,
+    by bisection (forcefield.py:523-567): 0.9 nm -> 4.0, 0.7 nm -> 5.19 nm^-1."""
+    rc = float(elec_cutoff)
+    if not rc > 0.0:
+        raise ValueError(f"elec_cutoff must be positive, got {elec_cutoff}")
+    f = lambda b: math.erfc(b * rc) / (10.0 * rc) - dsum_tol  # noqa: E731
+    if not (dsum_tol > 0.0 and f(0.0) > 0.0):
+        raise ValueError(f"dsum_tol must be in (0, 1/rc_A) = (0, {1.0 / (10.0 * rc):.3g}), got {dsum_tol}")
+    lo, hi = 0.0, 1.0
+    while f(hi) > 0.0:
+        hi *= 2.0
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        if f(mid) > 0.0:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def elec_cutoff_settings(elec_cutoff: float, dsum_tol: float = DSUM_TOL, exponent: float = 1.6) -> dict:
+    """MDSettings arguments for a shorter electrostatics cutoff (forcefield.py:570-601): the Ewald
+    coefficient for it and the PME spacing 0.08 nm (4.0 / beta)^exponent."""
+    b = ewald_beta_for(elec_cutoff, dsum_tol)
+    return {"elec_cutoff": float(elec_cutoff), "ewald_beta": b, "pme_spacing": 0.08 * (4.0 / b) ** exponent}
 
 
 @_dc.dataclass
@@ -138,7 +178,9 @@ class PGMForceField:
     """
 
     def __init__(self, system, H, settings: MDSettings = MDSettings(), row_capacity: int | None = None, device: int = 0,
-                 pme_grids=None) -> None:
+                 pme_grids=None, elec_capacity: int | None = None) -> None:
+        if elec_capacity is not None and not settings.split_rows:
+            raise ValueError("elec_capacity applies only to split rows (elec_cutoff < cutoff with a van der Waals term)")
         self.systems = list(system) if isinstance(system, (list, tuple)) else [system]
         boxes = [np.asarray(h, float) for h in H] if isinstance(H, (list, tuple)) else [np.asarray(H, float)] * len(self.systems)
         if len(boxes) != len(self.systems):
@@ -157,6 +199,7 @@ class PGMForceField:
             int(settings.precision == "double"), float(settings.cutoff), float(settings.ewald_beta), int(settings.pme_order),
             float(settings.dipole_tol), int(settings.max_iter), PREDICTORS[settings.predictor], int(settings.fused),
             int(settings.norm_refresh), float(settings.peek), int(row_capacity or 0), float(settings.skin), 0,
+            float(settings.elec_cutoff or 0.0), int(elec_capacity or 0),
         )
         descs = (_lib.PgmSystemDesc * self.nsys)()
         self._keep = []
@@ -223,12 +266,29 @@ class PGMForceField:
     def set_capacity(self, mc: int) -> None:
         _lib.check(self._lib.pgm_set_row_capacity(self._h, int(mc)))
 
+    @property
+    def elec_capacity(self) -> int:
+        """Split rows: electrostatic pairs kept per row (else the row capacity)."""
+        return int(self._lib.pgm_elec_capacity(self._h))
+
+    def set_elec_capacity(self, c: int) -> None:
+        _lib.check(self._lib.pgm_set_elec_capacity(self._h, int(c)))
+
     def size_rows(self, pos, H, idx=None, factor: float = 1.2) -> int:
-        """Set the capacity from the largest row at pos, with half the head-room `factor` gives (forcefield.py:1269)."""
+        """Set the capacity from the largest row at pos, with half the head-room `factor` gives (forcefield.py:1269);
+        with split rows both parts."""
+        grow = lambda c: int(np.ceil((c * (1.0 + 0.5 * (factor - 1.0)) + 8) / 8.0) * 8)  # noqa: E731
         self.set_capacity(max(self.capacity, 1024))
+        if self.s.split_rows:
+            self.set_elec_capacity(max(self.elec_capacity, 512))
         self.compute(pos, H, idx, self.init_induction())
         c = int(self._lib.pgm_max_row_count(self._h))
-        self.set_capacity(int(np.ceil((c * (1.0 + 0.5 * (factor - 1.0)) + 8) / 8.0) * 8))
+        if self.s.split_rows:
+            v = int(self._lib.pgm_max_vdw_count(self._h))
+            self.set_elec_capacity(grow(c))
+            self.set_capacity(self.elec_capacity + grow(v))
+        else:
+            self.set_capacity(grow(c))
         return self.capacity
 
     @property
@@ -244,7 +304,13 @@ class PGMForceField:
         return int(self._lib.pgm_list_rebuilds(self._h))
 
     def grow_rows(self, old: int) -> None:
-        """Widen the rows by at least 8 after an overflow at capacity `old` (forcefield.py:1286)."""
+        """Widen the rows by at least 8 after an overflow at capacity `old` (forcefield.py:1286); with
+        split rows each part to the largest count of the last build + 8."""
+        if self.s.split_rows:
+            e, v = int(self._lib.pgm_max_row_count(self._h)), int(self._lib.pgm_max_vdw_count(self._h))
+            self.set_elec_capacity(max(self.elec_capacity, e + 8))
+            self.set_capacity(max(self.capacity, self.elec_capacity + v + 8, int(old) + 8))
+            return
         self.set_capacity(max(self.capacity, int(old) + 8))
 
     def fit_rows(self, caps) -> None:

@@ -220,3 +220,37 @@ def test_cg_max_iter_status(box):
     ff = ff_for(s, H, "double", max_iter=3)
     res = ff.compute(pos, H)
     assert int(res.iterations[0]) == 3 and int(res.status[0]) & 0x2
+
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_split_rows_match_oracle(small_box_system, prec):
+    """elec_cutoff 0.45 < cutoff 0.6 (split rows): the field sweeps stream only the electrostatic
+    part of every row, the LJ term keeps every pair; energies, forces, dipoles and iterations as the
+    oracle's split rows, and an overflow of either part is reported and recovered by grow_rows."""
+    s, pos, H = small_box_system
+    st = dict(SMALL_BOX_SETTINGS, dipole_tol=1e-8, elec_cutoff=0.45)
+    ro = O.Oracle(s, st).compute(pos, H)
+    ff = ff_for(s, H, prec, dipole_tol=1e-8, elec_cutoff=0.45)
+    rg = ff.compute(pos, H)
+    assert int(rg.status[0]) == 0
+    e = float(rg.energy["total"][0])
+    assert abs(e - ro["energy"]["total"]) <= (1e-10 if prec == "double" else 1e-6) * abs(ro["energy"]["total"])
+    assert rms_rel(rg.forces.cpu().numpy(), ro["forces"]) <= (1e-9 if prec == "double" else 1e-5)
+    assert rms_rel(rg.induction.mu.cpu().numpy(), ro["mu"]) <= (1e-9 if prec == "double" else 1e-5)
+    if prec == "double":
+        assert int(rg.iterations[0]) == ro["iterations"]
+        full = ff_for(s, H, prec, dipole_tol=1e-8)
+        full.compute(pos, H)
+        assert int(full._lib.pgm_row_pairs(full._h)) > int(ff._lib.pgm_row_pairs(ff._h))  # fewer pairs streamed
+        # overflow of the LJ part, then recovery
+        small = ff_for(s, H, prec, dipole_tol=1e-8, elec_cutoff=0.45)
+        small.set_capacity(small.elec_capacity + 32)
+        e_cap = small.elec_capacity
+        small.set_elec_capacity(32)
+        r1 = small.compute(pos, H)
+        if int(small._lib.pgm_max_row_count(small._h)) > 32:
+            assert int(r1.status[0]) & 0x1
+        small.grow_rows(small.capacity)
+        r2 = small.compute(pos, H)
+        assert int(r2.status[0]) == 0 and small.elec_capacity >= 32 and e_cap > 0
+        assert abs(float(r2.energy["total"][0]) - ro["energy"]["total"]) <= 1e-10 * abs(ro["energy"]["total"])

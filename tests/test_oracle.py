@@ -116,3 +116,22 @@ def test_oracle_forces_without_permanent_dipoles_are_pure_charge(small_box_syste
         d[a, k] = h
         fd = -(o.energy_fixed_mu(pos + d, H, r["mu"])["total"] - o.energy_fixed_mu(pos - d, H, r["mu"])["total"]) / (2 * h)
         assert abs(fd - r["forces"][a, k]) < 1e-5 * max(1.0, abs(fd))
+
+
+def test_oracle_split_rows(small):
+    """Split rows (elec_cutoff < cutoff, forcefield.py:44-58): elec_cutoff = cutoff changes nothing;
+    below it the LJ term keeps every pair inside the cutoff and the forces stay the central
+    differences of the energy."""
+    s, pos, H, o, r = small
+    same = O.Oracle(s, dict(SMALL_BOX_SETTINGS, elec_cutoff=SMALL_BOX_SETTINGS["cutoff"])).compute(pos, H)
+    assert same["energy"]["total"] == r["energy"]["total"] and np.array_equal(same["forces"], r["forces"])
+    os_ = O.Oracle(s, dict(SMALL_BOX_SETTINGS, elec_cutoff=0.45))
+    rs = os_.compute(pos, H)
+    assert abs(rs["energy"]["vdw"] - r["energy"]["vdw"]) <= 1e-12 * abs(r["energy"]["vdw"])
+    assert abs(rs["energy"]["elec"] - r["energy"]["elec"]) > 1e-6 * abs(r["energy"]["elec"])
+    h = 1e-6
+    for a, k in [(0, 0), (40, 2)]:
+        d = np.zeros_like(pos)
+        d[a, k] = h
+        fd = -(os_.energy_fixed_mu(pos + d, H, rs["mu"])["total"] - os_.energy_fixed_mu(pos - d, H, rs["mu"])["total"]) / (2 * h)
+        assert abs(fd - rs["forces"][a, k]) < 1e-5 * max(1.0, abs(fd)), (a, k, fd, rs["forces"][a, k])
