@@ -107,14 +107,19 @@ class Clocks:
 
     def __init__(self, index: int) -> None:
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+        q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
+        self.window = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
                                        "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+
+    def mark(self, t0: float, t1: float) -> None:
+        """The timed region's wall-clock window (samples outside it are dropped when some fall inside)."""
+        self.window = (t0, t1)
 
     def stop(self) -> dict:
         if self.p is None:
@@ -126,8 +131,21 @@ class Clocks:
             self.p.kill()
         self.f.flush()
         self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        rows = [[c.strip() for c in r.split(",")] for r in self.f.read().strip().splitlines() if r.count(",") >= 9]
         os.unlink(self.f.name)
+        if self.window and rows:
+            import datetime
+
+            def when(r):
+                try:
+                    return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    return None
+
+            inside = [r for r in rows if when(r) is not None and self.window[0] <= when(r) <= self.window[1]]
+            if inside:
+                rows = inside
+        rows = [r[1:] for r in rows]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
@@ -226,25 +244,31 @@ def run_engine(args) -> None:
         md.step()
     md.stream.synchronize()
     md.capture()
-    md.run(max(3, args.warmup))
+    md.run(3)
     md.stream.synchronize()
     it0 = int(md.result.iterations[0])
+    builds0 = int(lib.pgm_list_rebuilds(ff._h))
+    # the clock sampler starts while warm-up replays keep the GPU busy, so that the timed region
+    # begins on a loaded GPU at its running clocks (not after an idle gap)
+    clk = Clocks(local)
+    md.run(max(3, args.warmup) + 200)
     # timed region: K graph replays between CUDA events on the MD stream; clocks sampled meanwhile
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    clk = Clocks(local)
-    builds0 = int(lib.pgm_list_rebuilds(ff._h))
+    t_wall = time.time()
     ms, n_it = timed_replays(md, args.steps, torch, label="timed_md")
+    clk.mark(t_wall, time.time())
     clocks = clk.stop()
-    rebuilds = int(lib.pgm_list_rebuilds(ff._h)) - builds0
+    rebuilds = int(lib.pgm_list_rebuilds(ff._h)) - builds0  # over the last warm-up replays and the timed ones
+    rebuilds_steps = args.steps + max(3, args.warmup) + 200
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if ws > 1:
         dist.barrier()
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     status = int(md.result.status[0])
-    launches = args.steps * (md.launches_outside_loop + n_it * md.launches_per_iteration)
+    launches = args.steps * (md.launches_outside_loop + max(n_it, md.unrolled_iterations) * md.launches_per_iteration)
     # the dominant kernel: the CG matvec, timed alone with CUDA events on the MD stream
     pairs = int(lib.pgm_row_pairs(ff._h))
     kt = {}
@@ -270,7 +294,7 @@ def run_engine(args) -> None:
             "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic", "config": CONFIG, "cg_iters_per_step": n_it, "cg_iters_first_step": it0,
-            "status": status, "gpu_launches": int(round(launches)), "list_rebuilds_per_step": rebuilds / args.steps,
+            "status": status, "gpu_launches": int(round(launches)), "list_rebuilds_per_step": rebuilds / rebuilds_steps,
             "clocks": clocks,
             "roofline": {
                 "bound": "hbm", "kernel": "k_rowfield (CG matvec row stream: k, x, y, z, G1, G2 per pair)",
@@ -495,6 +519,9 @@ def run_workload(args) -> None:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         it_sum = torch.zeros(ff.nsys, dtype=torch.int64, device=ff.device)
         clk = Clocks(0)
+        md.run(50)  # the GPU stays loaded while the sampler starts
+        torch.cuda.synchronize()
+        t_wall = time.time()
         ev0.record(md.stream)
         for _ in range(blocks):
             for _ in range(100):
@@ -504,6 +531,7 @@ def run_workload(args) -> None:
             rex.exchange()  # host: energies of the replicas, Metropolis, temperatures, momenta
         ev1.record(md.stream)
         torch.cuda.synchronize()
+        clk.mark(t_wall, time.time())
         clocks = clk.stop()
         steps = 100 * blocks
         ms = ev0.elapsed_time(ev1) / steps
@@ -535,6 +563,9 @@ def run_workload(args) -> None:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         it_sum = torch.zeros(32, dtype=torch.int64, device=pm.dev)
         clk = Clocks(0)
+        pm.run(30)  # the GPU stays loaded while the sampler starts
+        torch.cuda.synchronize()
+        t_wall = time.time()
         ev0.record(pm.stream)
         for _ in range(steps):
             pm.run(1)
@@ -542,6 +573,7 @@ def run_workload(args) -> None:
                 it_sum += pm.result.iterations.to(torch.int64)
         ev1.record(pm.stream)
         torch.cuda.synchronize()
+        clk.mark(t_wall, time.time())
         clocks = clk.stop()
         ms = ev0.elapsed_time(ev1) / steps
         est = pm.estimators()

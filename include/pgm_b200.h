@@ -178,6 +178,9 @@ const char *pgm_last_error(void);
  * and the kernels of one CG iteration (launch accounting). */
 long long pgm_last_launch_count(const PgmHandle *h);
 long long pgm_launches_per_iteration(const PgmHandle *h);
+/* CG iterations of a captured solve that run as plain graph nodes ahead of its conditional while
+ * node (from the iteration count of the last host-driven solve; 0: all in the while node). */
+int pgm_unrolled_iterations(const PgmHandle *h);
 
 /* Average duration [ms] of one launch of a kernel of the last pgm_compute, re-run `reps` times on
  * `stream` between CUDA events on the state that step left: 0 the CG matvec (row field + PME

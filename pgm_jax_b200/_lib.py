@@ -19,7 +19,7 @@ _pu = C.POINTER(C.c_uint32)
 EXPORTS = (
     "pgm_create", "pgm_destroy", "pgm_compute", "pgm_compute_host", "pgm_energy", "pgm_energy_fixed_mu", "pgm_field",
     "pgm_set_row_capacity", "pgm_row_capacity", "pgm_set_elec_capacity", "pgm_elec_capacity", "pgm_max_vdw_count", "pgm_set_list_capacity", "pgm_list_capacity", "pgm_list_rebuilds", "pgm_max_row_count", "pgm_num_atoms", "pgm_num_systems",
-    "pgm_last_error", "pgm_last_launch_count", "pgm_launches_per_iteration", "pgm_profile_kernel", "pgm_row_pairs", "pgm_rigid_create", "pgm_rigid_destroy",
+    "pgm_last_error", "pgm_last_launch_count", "pgm_launches_per_iteration", "pgm_unrolled_iterations", "pgm_profile_kernel", "pgm_row_pairs", "pgm_rigid_create", "pgm_rigid_destroy",
     "pgm_rigid_begin_step", "pgm_rigid_set_step", "pgm_rigid_end_step", "pgm_rigid_kinetic", "pgm_rigid_scale_momenta", "pgm_rigid_last_error", "pgm_pimd_kick",
     "pgm_pimd_free_thermostat", "pgm_water_bonded", "pgm_pimd_last_error", "pgm_graph_begin",
     "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
@@ -96,6 +96,7 @@ def load(path: str | None = None):
     lib.pgm_list_rebuilds.argtypes = [H]
     lib.pgm_list_rebuilds.restype = C.c_longlong
     lib.pgm_max_row_count.argtypes = [H]
+    lib.pgm_unrolled_iterations.argtypes = [H]
     lib.pgm_num_atoms.argtypes = [H]
     lib.pgm_num_systems.argtypes = [H]
     lib.pgm_last_launch_count.argtypes = [H]

@@ -122,6 +122,7 @@ struct EngineBase {
   double *host_scratch = nullptr;  // device block of pgm_compute_host (allocated on first use)
   size_t host_scratch_bytes = 0;
   long long launches = 0;
+  int unrolled = 0;  // CG iterations unrolled in front of the while node of the last capture
 };
 
 // Mesh lengths with a compiled FFT plan (others run the runtime-length kernels).
@@ -185,6 +186,7 @@ struct Engine : EngineBase {
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
   DBuf<float> nn_w, nn_inv, nn_vec, nn_mu, nn_chan;  // learned guess: model and per-atom features
   bool nn_on = false;
+  int last_iters = 0;  // CG iterations of the last host-driven solve (sizes the unrolled part of a capture)
   const double *last_hist = nullptr;  // the history of the last predictor solve (profiling)
   DBuf<float4> nn_bl;  // the graph's permanent field of the last solve (for the change channel)
   DBuf<int> nn_valid;  // nn_bl holds a previous step
@@ -509,31 +511,32 @@ struct Engine : EngineBase {
   void fft_chain(cudaStream_t st, pgm::Dev<T> &a, int act, bool energy) {
     for (auto &g : gx)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
-        check_launch();
+        launch_pdl(pgm::k_fft_x_fwd<T, decltype(Lc)::value>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a, (const int *)g->sys.p,
+                   (const int *)g->tile0.p, g->ng, act);
       });
     for (auto &g : gy)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, -1);
-        check_launch();
+        launch_pdl(pgm::k_fft_y<T, decltype(Lc)::value>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a, (const int *)g->sys.p,
+                   (const int *)g->tile0.p, g->ng, act, -1);
       });
     for (auto &g : gz)
       with_fft_len(g->K, [&](auto Lc) {
         if (energy)
-          pgm::k_fft_z_conv<T, decltype(Lc)::value, true><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
+          launch_pdl(pgm::k_fft_z_conv<T, decltype(Lc)::value, true>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a,
+                     (const int *)g->sys.p, (const int *)g->tile0.p, g->ng, act);
         else
-          pgm::k_fft_z_conv<T, decltype(Lc)::value, false><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
-        check_launch();
+          launch_pdl(pgm::k_fft_z_conv<T, decltype(Lc)::value, false>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a,
+                     (const int *)g->sys.p, (const int *)g->tile0.p, g->ng, act);
       });
     for (auto &g : gy)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_y<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act, +1);
-        check_launch();
+        launch_pdl(pgm::k_fft_y<T, decltype(Lc)::value>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a, (const int *)g->sys.p,
+                   (const int *)g->tile0.p, g->ng, act, +1);
       });
     for (auto &g : gx)
       with_fft_len(g->K, [&](auto Lc) {
-        pgm::k_fft_x_inv<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, act);
-        check_launch();
+        launch_pdl(pgm::k_fft_x_inv<T, decltype(Lc)::value>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a, (const int *)g->sys.p,
+                   (const int *)g->tile0.p, g->ng, act);
       });
   }
 
@@ -672,6 +675,25 @@ struct Engine : EngineBase {
 
   int grid1(int n, int b = 256) { return (n + b - 1) / b; }
 
+  // Launch with programmatic stream serialization: the kernel (which begins with pdl_enter()) is
+  // scheduled while its predecessor drains, so the per-kernel launch gap of the CG loop overlaps
+  // the previous kernel's tail; after a non-kernel node the attribute has no effect.
+  template <typename... KArgs, typename... Args>
+  void launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k, args...));
+    ++launches;
+  }
+
   // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
   // cell list, rows, influence function.
   void prepare(cudaStream_t st, pgm::Dev<T> &a, const double *boxes) {
@@ -712,7 +734,7 @@ struct Engine : EngineBase {
   // Reciprocal-space potential phi of the grid spread from `vin` (with charges if WITH_Q).
   template <bool WITH_Q, bool UPDATE_P, int ACT, bool ENERGY>
   void pme(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin) {
-    CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // the spread accumulates into a cleared grid
+    // Q is zero here: cleared at creation and, after every spread, by the forward k2 FFT pass
     pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
     fft_chain(st, a, ACT, ENERGY);
   }
@@ -725,17 +747,17 @@ struct Engine : EngineBase {
     if (!overlap) {
       // one stream: the row field runs between the spread and the first FFT pass, while the L2
       // still processes the spread's atomic adds, then the FFTs and the PME gather
-      CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // the spread accumulates into a cleared grid
+      // Q is zero here: cleared at creation and, after every spread, by the forward k2 FFT pass
       pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
-      pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, st>>>(a, UPDATE_P ? Pv.p : vin, Fv.p); check_launch();
+      const pgm::v4<T> *dv = UPDATE_P ? Pv.p : vin;
+      launch_pdl(pgm::k_rowfield<T, WITH_Q, ACT>, nwblk, 256, 0, st, a, dv, Fv.p);
       fft_chain(st, a, ACT, false);
-      pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false><<<nwblk, 256, 0, st>>>(a, UPDATE_P ? Pv.p : vin, out); check_launch();
+      launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false>, nwblk, 256, 0, st, a, dv, out);
       return;
     }
     // the loop body is captured as a sequence of its own: it forks to its own stream
     cudaStream_t ax = in_body ? aux_b : aux;
     cudaEvent_t ef = in_body ? ev_fork_b : ev_fork, ej = in_body ? ev_join_b : ev_join;
-    CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));
     pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
     CK(cudaEventRecord(ef, st));
     CK(cudaStreamWaitEvent(ax, ef, 0));
@@ -749,8 +771,8 @@ struct Engine : EngineBase {
   // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check.
   void iteration(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
     sweep<false, true, 1, 1>(st, a, Pv.p, AP.p);
-    pgm::k_cg_update<T><<<ntblk, 256, 0, st>>>(a); check_launch();
-    pgm::k_cg_check<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, cond, use_cond); check_launch();
+    launch_pdl(pgm::k_cg_update<T>, ntblk, 256, 0, st, a);
+    launch_pdl(pgm::k_cg_check, 1, 256, 0, st, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, cond, use_cond);
   }
 
   bool any_active(cudaStream_t st) {
@@ -797,15 +819,21 @@ struct Engine : EngineBase {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
     if (cs == cudaStreamCaptureStatusActive) {
-      // captured: a conditional while node whose body is one CG iteration; the body's last kernel
-      // sets the condition to "some system still iterating" (bounded by max_iter on the device)
+      // captured: the first U iterations as plain kernel nodes (their kernels skip systems that
+      // have converged; U = the iterations of the last host-driven solve - 2), then a conditional
+      // while node whose body is one CG iteration.  The last check before the node and the body's
+      // last kernel set the condition to "some system still iterating" (max_iter on the device).
       cudaGraph_t g;
       const cudaGraphNode_t *deps = nullptr;
       size_t nd = 0;
       unsigned long long id;
       CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+      const int U = std::max(0, std::min(last_iters - 2, set.max_iter));
       cudaGraphConditionalHandle cond;
-      CK(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+      CK(cudaGraphConditionalHandleCreate(&cond, g, U > 0 ? 0 : 1, cudaGraphCondAssignDefault));
+      for (int k = 0; k < U; ++k) iteration(st, a, cond, k == U - 1 ? 1 : 0);
+      unrolled = U;
+      if (U > 0) CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
       cudaGraphNodeParams np = {};
       np.type = cudaGraphNodeTypeConditional;
       np.conditional.handle = cond;
@@ -831,12 +859,14 @@ struct Engine : EngineBase {
       per_iter = launches - l0;
       CK(cudaStreamEndCapture(side, &body));
     } else {
-      for (int it = 0; it < set.max_iter; ++it) {
+      int it = 0;
+      for (; it < set.max_iter; ++it) {
         if (!any_active(st)) break;
         long long l0 = launches;
         iteration(st, a, 0, 0);
         per_iter = launches - l0;
       }
+      last_iters = it;
     }
     pgm::k_cg_finish<T><<<grid1(nt), 256, 0, st>>>(a, mu_out, mode == 0 ? ind->hist : nullptr, mode == 0); check_launch();
     pgm::k_cg_state_out<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, ind->count, ind->norm, iters, resid, a.status, mode == 0,
@@ -1203,6 +1233,7 @@ int pgm_num_atoms(const PgmHandle *h) { return h ? h->eng->nt : -1; }
 int pgm_num_systems(const PgmHandle *h) { return h ? h->eng->nsys : -1; }
 long long pgm_last_launch_count(const PgmHandle *h) { return h ? h->eng->launches : -1; }
 long long pgm_launches_per_iteration(const PgmHandle *h) { return h ? h->eng->launches_per_iteration() : -1; }
+int pgm_unrolled_iterations(const PgmHandle *h) { return h ? h->eng->unrolled : -1; }
 
 PgmStatus pgm_profile_kernel(PgmHandle *h, void *stream, int which, int reps, double *ms_per_launch) {
   if (!h || !ms_per_launch || reps <= 0 || which < 0 || which > 12) return fail(PGM_ERR_INVALID, "bad argument");

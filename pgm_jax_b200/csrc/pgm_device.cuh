@@ -159,6 +159,12 @@ __device__ __forceinline__ void bspline(T f, T *th, T *dth, T *d2th) {
   }
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may be
+// scheduled as its predecessor in the stream drains (its blocks trigger the launch when they exit);
+// it waits here for the predecessor's completion (its memory visible) before touching any data.
+// Without the launch attribute the instruction is a no-op.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -518,6 +518,7 @@ __global__ void k_influence(Dev<T> a, long long total) {
 // UPDATE_P the CG direction is first advanced, p = z + beta p (forcefield.py:1812), and spread.
 template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT>
 __global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
+  pdl_enter();
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
@@ -780,6 +781,7 @@ __device__ __forceinline__ bool pass_active(const Dev<T> &a, int s, int act) {
 // length-K3 FFT, untangled.
 template <typename T, int L>
 __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
+  pdl_enter();
   extern __shared__ unsigned char smem_raw[];
   int g = group_member(gtile0, ng, blockIdx.x);
   int s = gsys[g];
@@ -816,6 +818,7 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, co
 // k3 pass, half complex -> real (the inverse of k_fft_x_fwd, unnormalised): writes phi.
 template <typename T, int L>
 __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
+  pdl_enter();
   extern __shared__ unsigned char smem_raw[];
   int g = group_member(gtile0, ng, blockIdx.x);
   int s = gsys[g];
@@ -860,6 +863,7 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
 // column index, each a line over k2 with stride K3h.
 template <typename T, int L>
 __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act, int sign) {
+  pdl_enter();
   extern __shared__ unsigned char smem_raw[];
   int g = group_member(gtile0, ng, blockIdx.x);
   int s = gsys[g];
@@ -889,6 +893,16 @@ __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const 
         x[c * ld + k2] = v;
       });
   __syncthreads();
+  if (sign < 0) {
+    // the real grid of this system was consumed by the k3 pass: clear this CTA's share of it for
+    // the next spread (no separate memset between the sweeps)
+    const size_t nq = (size_t)S.K[0] * S.K[1] * S.K[2];
+    const int ntile = gtile0[g + 1] - gtile0[g];
+    const size_t per = (nq + ntile - 1) / ntile, q0 = (size_t)(blockIdx.x - gtile0[g]) * per;
+    const size_t q1 = q0 + per < nq ? q0 + per : nq;
+    T *Qs = a.Q + S.rgrid0;
+    for (size_t t = q0 + threadIdx.x; t < q1; t += blockDim.x) Qs[t] = T(0);
+  }
   c2<T> *res = fft_lines<T, L>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], tws, sign);
   for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
     int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
@@ -906,6 +920,7 @@ __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const 
 // (pme.py:390-411) and the influence part of the virial are accumulated.
 template <typename T, int L, bool ENERGY>
 __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
+  pdl_enter();
   extern __shared__ unsigned char smem_raw[];
   __shared__ double red[7][8];
   int g = group_member(gtile0, ng, blockIdx.x);
@@ -1014,6 +1029,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
 // The row part alone: F_i = sum_k de_ik/dd_i, one warp per atom (runs beside the PME chain).
 template <typename T, bool WITH_Q, int ACT>
 __global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ F) {
+  pdl_enter();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
@@ -1039,8 +1055,10 @@ __global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restr
                  *z4 = reinterpret_cast<const float4 *>(a.rz + base), *p4 = reinterpret_cast<const float4 *>(a.rg1 + base),
                  *q4 = reinterpret_cast<const float4 *>(a.rg2 + base);
     for (int t4 = lane; 4 * t4 < n; t4 += 32) {
-      int4 kk = k4[t4];
-      float4 xx = x4[t4], yy = y4[t4], zz = z4[t4], g1 = p4[t4], g2 = q4[t4];
+      // streaming loads (evict first): the 90+ MB of rows pass through L2 once per sweep and must
+      // not push out the PME grids that the FFT passes read next
+      int4 kk = __ldcs(k4 + t4);
+      float4 xx = __ldcs(x4 + t4), yy = __ldcs(y4 + t4), zz = __ldcs(z4 + t4), g1 = __ldcs(p4 + t4), g2 = __ldcs(q4 + t4);
       int t = 4 * t4;
       pair(kk.x, xx.x, yy.x, zz.x, g1.x, g2.x);
       if (t + 1 < n) pair(kk.y, xx.y, yy.y, zz.y, g1.y, g2.y);
@@ -1064,6 +1082,7 @@ __global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restr
 // ROWS: the row sum is computed here; otherwise it is read from a.F (k_rowfield).
 template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true>
 __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
+  pdl_enter();
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
   __shared__ double red[WARPS_PER_BLOCK];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1562,6 +1581,7 @@ __global__ void k_cg_begin(CGSys *cg, int nsys, double tol, int max_iter, int *a
 // z'.(r' - r), r'.z', max|z'| (forcefield.py:1802-1814).
 template <typename T>
 __global__ void k_cg_update(Dev<T> a) {
+  pdl_enter();
   __shared__ double red[2][THREADS_PER_BLOCK / 32];
   __shared__ unsigned long long mx[THREADS_PER_BLOCK / 32];
   int s = a.tb_sys[blockIdx.x];
@@ -1607,6 +1627,7 @@ __global__ void k_cg_update(Dev<T> a) {
 // still iterating.
 __global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *any, cudaGraphConditionalHandle cond,
                            int use_cond) {
+  pdl_enter();
   __shared__ int act;
   if (threadIdx.x == 0) act = 0;
   __syncthreads();

@@ -178,8 +178,11 @@ class RigidMD:
             raise
         _lib.check(self._lib.pgm_graph_end(st, C.byref(ex)))
         self._graph = ex
-        self.launches_outside_loop = self.ff.last_launch_count() + 2 - int(self._lib.pgm_launches_per_iteration(self.ff._h))
         self.launches_per_iteration = int(self._lib.pgm_launches_per_iteration(self.ff._h))
+        self.unrolled_iterations = int(self._lib.pgm_unrolled_iterations(self.ff._h))
+        # launches of a replay: these + max(unrolled, CG iterations) x launches_per_iteration
+        self.launches_outside_loop = (self.ff.last_launch_count() + 2
+                                      - (1 + self.unrolled_iterations) * self.launches_per_iteration)
 
     def run(self, n: int) -> None:
         """n steps: graph replays when captured, else direct launches."""
