@@ -196,8 +196,10 @@ struct Engine : EngineBase {
   float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
   int *h_any = nullptr;
   const double *last_pos = nullptr;
-  cudaStream_t side = nullptr, aux = nullptr, aux_b = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork_b = nullptr, ev_join_b = nullptr;
+  cudaStream_t side = nullptr, aux = nullptr, aux_b = nullptr, nn_st = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork_b = nullptr, ev_join_b = nullptr, ev_nn_fork = nullptr,
+              ev_nn_join = nullptr;
+  bool nn_forked = false;  // the learned guess of this step runs on nn_st (joined before the solve's start)
   bool in_body = false;  // enqueueing the CG while-loop body (its own capture sequence)
   bool overlap = false;  // row field on a second stream beside the FFT chain (slower on B200 at 12k atoms)
   long long per_iter = 0;
@@ -211,6 +213,9 @@ struct Engine : EngineBase {
     if (ev_join) cudaEventDestroy(ev_join);
     if (ev_fork_b) cudaEventDestroy(ev_fork_b);
     if (ev_join_b) cudaEventDestroy(ev_join_b);
+    if (nn_st) cudaStreamDestroy(nn_st);
+    if (ev_nn_fork) cudaEventDestroy(ev_nn_fork);
+    if (ev_nn_join) cudaEventDestroy(ev_nn_join);
   }
 
   pgm::Dev<T> dev(const double *pos, const int32_t *idx, int idx_width, double *forces, unsigned *status) {
@@ -474,6 +479,9 @@ struct Engine : EngineBase {
     CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_fork_b, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join_b, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&nn_st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_nn_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_nn_join, cudaEventDisableTiming));
     set_smem();
   }
 
@@ -696,7 +704,20 @@ struct Engine : EngineBase {
 
   // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
   // cell list, rows, influence function.
-  void prepare(cudaStream_t st, pgm::Dev<T> &a, const double *boxes) {
+  // The learned guess's inputs and prediction for this step's rows: forked onto nn_st after the
+  // row build, beside the row kernels and the influence function; solve() joins it.
+  void nn_fork(cudaStream_t st, pgm::Dev<T> &a, const double *hist) {
+    CK(cudaEventRecord(ev_nn_fork, st));
+    CK(cudaStreamWaitEvent(nn_st, ev_nn_fork, 0));
+    nn_inputs(nn_st, a, hist, nn_bl.p, nn_valid.p, nn_bl.p, nn_inv.p, nn_vec.p, nn_valid.p);
+    cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, nn_st);
+    if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
+    ++launches;
+    CK(cudaEventRecord(ev_nn_join, nn_st));
+    nn_forked = true;
+  }
+
+  void prepare(cudaStream_t st, pgm::Dev<T> &a, const double *boxes, const double *nn_hist = nullptr) {
     CK(cudaMemsetAsync(dmax.p, 0, 2 * sizeof(int), st));
     pgm::k_box<T><<<grid1(nsys, 64), 64, 0, st>>>(a, boxes); check_launch();
     pgm::k_prep<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
@@ -711,6 +732,7 @@ struct Engine : EngineBase {
       pgm::k_nb_lower<<<1, 1, 0, st>>>(nb_flag.p, nb_builds.p); check_launch();
     }
     pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a); check_launch();
+    if (nn_hist) nn_fork(st, a, nn_hist);
     pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a); check_launch();
     pgm::k_influence<T><<<std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st>>>(a, cgrid); check_launch();
   }
@@ -801,11 +823,10 @@ struct Engine : EngineBase {
       check_launch();
     } else {
       last_hist = ind->hist;
+      if (use_nn && !nn_forked) nn_fork(st, a, ind->hist);
       if (use_nn) {
-        nn_inputs(st, a, ind->hist, nn_bl.p, nn_valid.p, nn_bl.p, nn_inv.p, nn_vec.p, nn_valid.p);
-        cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st);
-        if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
-        ++launches;
+        CK(cudaStreamWaitEvent(st, ev_nn_join, 0));  // the prediction, computed beside the row kernels
+        nn_forked = false;
       }
       pgm::k_start1<T><<<grid1(nt), 256, 0, st>>>(a, ind->hist, K, cc[0], cc[1], cc[2], cc[3], use_nn ? nn_mu.p : nullptr);
       check_launch();
@@ -894,7 +915,8 @@ struct Engine : EngineBase {
     CK(cudaMemsetAsync(status, 0, sizeof(unsigned) * nsys, st));
     pgm::Dev<T> a = dev(pos, idx, idx_width, forces, status);
     last_pos = pos;
-    prepare(st, a, box);
+    nn_forked = false;
+    prepare(st, a, box, a.induce && set.predictor == 5 && nn_on ? ind->hist : nullptr);
     double *mu = ind->mu;
     if (a.induce) {
       solve(st, a, ind, 0, mu, out->iterations, out->residual);

@@ -1287,8 +1287,15 @@ __global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, c
   if (i >= S.atom0 + S.natom) return;
   float f0 = 0.f, f1 = 0.f, f2 = 0.f;
   const size_t base = (size_t)i * a.mc;
-  for_graph_edges(a, i, rg, ebuf[warp], eoff[warp], [&](int k, float x, float y, float z, int t) {
-    float g1 = float(a.rg1[base + t]), g2 = float(a.rg2[base + t]);
+  const float Ri = float(a.radius[i]), beta = float(a.beta);
+  for_graph_edges(a, i, rg, ebuf[warp], eoff[warp], [&](int k, float x, float y, float z, int) {
+    // the pair kernels G1, G2 of the edge, evaluated here (not read from the rows) so that this
+    // pass can run beside the row-kernel evaluation
+    const float Rk = float(a.radius[k]), r = sqrtf(x * x + y * y + z * z);
+    float A[4], Bb[4];
+    erf_kernels<float>(rsqrtf(2.f * (Ri * Ri + Rk * Rk)), r, A);
+    erf_kernels<float>(beta, r, Bb);
+    const float g1 = A[1] - Bb[1], g2 = A[2] - Bb[2];
     double4 pk = a.pperm[k];
     float px = float(pk.x), py = float(pk.y), pz = float(pk.z);
     float c = -float(a.q[k]) * g1 - g2 * (px * x + py * y + pz * z);
