@@ -171,6 +171,7 @@ struct Engine : EngineBase {
   DBuf<int> wb_sys, wb_atom0, tb_sys, tb_atom0;
   DBuf<int> sysid, molid, molfirst, molend, mol_start, cov_start, cov_j, cov_i_flat, cov_j_flat;
   DBuf<T> q, radius, alpha, ialpha, rminh, seps;
+  DBuf<pgm::v4<T>> qls;
   DBuf<double> mass, cov_c, cov_c_flat, bmod;
   DBuf<int4> base;
   DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D, Fv;
@@ -234,6 +235,7 @@ struct Engine : EngineBase {
     a.wb_sys = wb_sys.p; a.wb_atom0 = wb_atom0.p; a.tb_sys = tb_sys.p; a.tb_atom0 = tb_atom0.p;
     a.sysid = sysid.p; a.molid = molid.p; a.molfirst = molfirst.p; a.molend = molend.p; a.mol_start = mol_start.p;
     a.q = q.p; a.radius = radius.p; a.alpha = alpha.p; a.ialpha = ialpha.p; a.rminh = rminh.p; a.seps = seps.p;
+    a.qls = qls.p;
     a.mass = mass.p;
     a.cov_start = cov_start.p; a.cov_j = cov_j.p; a.cov_i_flat = cov_i_flat.p; a.cov_j_flat = cov_j_flat.p;
     a.cov_c = cov_c.p; a.cov_c_flat = cov_c_flat.p;
@@ -453,6 +455,13 @@ struct Engine : EngineBase {
     mol_start.upload(h_molstart); cov_start.upload(h_covstart); cov_j.upload(h_covj);
     cov_i_flat.upload(h_covi_flat); cov_j_flat.upload(h_covj_flat);
     q.upload(h_q); radius.upload(h_rad); alpha.upload(h_al); ialpha.upload(h_ial); rminh.upload(h_rh); seps.upload(h_se);
+    {
+      std::vector<pgm::v4<T>> h_qls(nt);
+      for (int k = 0; k < nt; ++k) {
+        h_qls[k].x = h_q[k]; h_qls[k].y = h_rh[k]; h_qls[k].z = h_se[k]; h_qls[k].w = T(0);
+      }
+      qls.upload(h_qls);
+    }
     mass.upload(h_mass); cov_c.upload(h_covc); cov_c_flat.upload(h_covc_flat); bmod.upload(h_bmod);
     tw.upload(h_tw);
     base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt); Fv.alloc(nt);

@@ -42,6 +42,7 @@ struct Dev {
   // atoms
   const int *sysid, *molid, *molfirst, *molend, *mol_start;
   const T *q, *radius, *alpha, *ialpha, *rminh, *seps;
+  const v4<T> *qls;  // per atom (q, R*/2, sqrt(eps), 0): one load per partner in the force pass
   const double *mass;
   const int *cov_start, *cov_j, *cov_i_flat, *cov_j_flat;
   const double *cov_c, *cov_c_flat;
@@ -1747,13 +1748,10 @@ __global__ void __launch_bounds__(256) k_forces(Dev<T> a, const double *mu) {
     T gx0 = 0, gx1 = 0, gx2 = 0, gl0 = 0, gl1 = 0, gl2 = 0, fd0 = 0, fd1 = 0, fd2 = 0;
     T ee = 0, el = 0;
     T w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int t = lane; t < n; t += 32) {
-      size_t o = base + t;
-      int k = a.rk[o];
-      T x = a.rx[o], y = a.ry[o], z = a.rz[o];
-      T G0 = a.rg0[o], G1 = a.rg1[o], G2 = a.rg2[o], G3 = a.rg3[o];
+    auto pair = [&](int k, T x, T y, T z, T G0, T G1, T G2, T G3, int t) {
       v4<T> dk = a.D[k];
-      T qk = a.q[k];
+      v4<T> pk = a.qls[k];  // q, R*/2, sqrt(eps) of the partner in one load
+      T qk = pk.x;
       T dix = di.x * x + di.y * y + di.z * z;
       T dkx = dk.x * x + dk.y * y + dk.z * z;
       T didk = di.x * dk.x + di.y * dk.y + di.z * dk.z;
@@ -1766,8 +1764,9 @@ __global__ void __launch_bounds__(256) k_forces(Dev<T> a, const double *mu) {
       T c = -qk * G1 - G2 * dkx;
       fd0 += c * x + G1 * dk.x; fd1 += c * y + G1 * dk.y; fd2 += c * z + G1 * dk.z;
       T kx = T(KE) * gxv, ky = T(KE) * gyv, kz = T(KE) * gzv;
-      if (a.lj && t >= nsp) {
-        T rm = rhi + a.rminh[k], ep = sei * a.seps[k];
+      T ep = sei * pk.z;
+      if (a.lj && t >= nsp && ep != T(0)) {  // LJ: not for molecule partners, nor pairs without an LJ term
+        T rm = rhi + pk.y;
         T r2 = x * x + y * y + z * z;
         T s2 = rm * rm / r2, s6 = s2 * s2 * s2;
         el += ep * (s6 * s6 - T(2) * s6);
@@ -1779,6 +1778,29 @@ __global__ void __launch_bounds__(256) k_forces(Dev<T> a, const double *mu) {
       w[0] += kx * x; w[1] += kx * y; w[2] += kx * z;
       w[3] += ky * x; w[4] += ky * y; w[5] += ky * z;
       w[6] += kz * x; w[7] += kz * y; w[8] += kz * z;
+    };
+    if constexpr (sizeof(T) == 4) {
+      // 16-byte loads of four consecutive entries of every row array
+      const int4 *k4 = reinterpret_cast<const int4 *>(a.rk + base);
+      const float4 *x4 = reinterpret_cast<const float4 *>(a.rx + base), *y4 = reinterpret_cast<const float4 *>(a.ry + base),
+                   *z4 = reinterpret_cast<const float4 *>(a.rz + base), *h0 = reinterpret_cast<const float4 *>(a.rg0 + base),
+                   *h1 = reinterpret_cast<const float4 *>(a.rg1 + base), *h2 = reinterpret_cast<const float4 *>(a.rg2 + base),
+                   *h3 = reinterpret_cast<const float4 *>(a.rg3 + base);
+      for (int t4 = lane; 4 * t4 < n; t4 += 32) {
+        int4 kk = __ldcs(k4 + t4);
+        float4 xx = __ldcs(x4 + t4), yy = __ldcs(y4 + t4), zz = __ldcs(z4 + t4);
+        float4 a0 = __ldcs(h0 + t4), a1 = __ldcs(h1 + t4), a2 = __ldcs(h2 + t4), a3 = __ldcs(h3 + t4);
+        int t = 4 * t4;
+        pair(kk.x, xx.x, yy.x, zz.x, a0.x, a1.x, a2.x, a3.x, t);
+        if (t + 1 < n) pair(kk.y, xx.y, yy.y, zz.y, a0.y, a1.y, a2.y, a3.y, t + 1);
+        if (t + 2 < n) pair(kk.z, xx.z, yy.z, zz.z, a0.z, a1.z, a2.z, a3.z, t + 2);
+        if (t + 3 < n) pair(kk.w, xx.w, yy.w, zz.w, a0.w, a1.w, a2.w, a3.w, t + 3);
+      }
+    } else {
+      for (int t = lane; t < n; t += 32) {
+        size_t o = base + t;
+        pair(a.rk[o], a.rx[o], a.ry[o], a.rz[o], a.rg0[o], a.rg1[o], a.rg2[o], a.rg3[o], t);
+      }
     }
     if (a.rnv) {  // split rows: the LJ pairs between elec_cutoff and cutoff
       const int nv = min(a.rnv[i], a.mc - a.mce);
