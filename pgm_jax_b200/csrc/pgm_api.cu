@@ -202,7 +202,7 @@ struct Engine : EngineBase {
               ev_nn_join = nullptr;
   bool nn_forked = false;  // the learned guess of this step runs on nn_st (joined before the solve's start)
   bool in_body = false;  // enqueueing the CG while-loop body (its own capture sequence)
-  bool overlap = false;  // row field on a second stream beside the FFT chain (slower on B200 at 12k atoms)
+  bool overlap = true;  // row field on a second stream beside the FFT chain
   long long per_iter = 0;
 
   ~Engine() {
