@@ -500,6 +500,7 @@ def run_workload(args) -> None:
     guess (trained on the 4096-water workload) against plain CG from mu1 and mu4."""
     import torch
 
+    from pgm_jax_b200 import _lib
     from pgm_jax_b200.remd import ReplicaExchange, RigidReplicas
     from pgm_jax_b200.systems import water_box
 
@@ -623,6 +624,13 @@ def run_workload(args) -> None:
             pairs = int(ff._lib.pgm_row_pairs(ff._h))
             arms[pred]["step_bytes"] = bytes_per_step(ff.n, pairs, n_it, 192)
             arms[pred]["step_frac_of_hbm"] = arms[pred]["step_bytes"] / (ms * 1e-3) / 1e9 / peaks()[0]
+            if pred == "mu4":  # the matvec's row stream at a size far above L2 (720 MB of rows per sweep)
+                v = C_double()
+                _lib.check(ff._lib.pgm_profile_kernel(ff._h, C_void_p(md.stream.cuda_stream), 7, 20, byref(v)))
+                mv_bytes = 24.0 * pairs + 32.0 * ff.n
+                arms[pred]["row_field_roofline"] = {"kernel": "k_rowfield", "bytes_per_launch": mv_bytes, "ms_per_launch": v.value,
+                                                    "achieved_gbs": mv_bytes / (v.value * 1e-3) / 1e9,
+                                                    "frac": mv_bytes / (v.value * 1e-3) / 1e9 / peaks()[0], "peak_gbs": peaks()[0]}
             del md, ff
         line.update({"value": arms["nn"]["value"], "ms_per_step": arms["nn"]["ms_per_step"],
                      "cg_iters_per_step": arms["nn"]["cg_iters_per_step"], "arms": arms, "atoms": 98304,
