@@ -1729,7 +1729,7 @@ __global__ void k_energy_start(Dev<T> a, const double *mu) {
 // virial sum g (x) x - gx (x) off; then the PME gradients of the atom: dU/dd and dU/dr through the
 // spline derivatives (the autodiff of pme.py:390-411 written out).
 template <typename T, int P>
-__global__ void __launch_bounds__(256) k_forces(Dev<T> a, const double *mu) {
+__global__ void __launch_bounds__(256, 3) k_forces(Dev<T> a, const double *mu) {
   __shared__ T sh[WARPS_PER_BLOCK][3][3][P];
   __shared__ double red[WARPS_PER_BLOCK][16];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
