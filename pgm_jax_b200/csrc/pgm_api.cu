@@ -123,6 +123,7 @@ struct EngineBase {
   size_t host_scratch_bytes = 0;
   long long launches = 0;
   int unrolled = 0;  // CG iterations unrolled in front of the while node of the last capture
+  long long generation = 0;  // bumped when device buffers are reallocated (captured graphs go stale)
 };
 
 // Mesh lengths with a compiled FFT plan (others run the runtime-length kernels).
@@ -495,6 +496,7 @@ struct Engine : EngineBase {
   }
 
   void alloc_rows() {
+    ++generation;
     size_t m = (size_t)nt * mc;
     rk.alloc(m); rx.alloc(m); ry.alloc(m); rz.alloc(m); rg0.alloc(m); rg1.alloc(m); rg2.alloc(m); rg3.alloc(m);
   }
@@ -558,6 +560,7 @@ struct Engine : EngineBase {
   }
 
   void set_nn(const float *w, float sigma, float rg) override {
+    ++generation;  // a captured step depends on whether a model is set, and on sigma and rg
     nn_on = w != nullptr;
     if (w) CK(cudaMemcpy(nn_w.p, w, sizeof(float) * pgmnn::NN_NPARAM, cudaMemcpyDeviceToDevice));
     CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
@@ -596,6 +599,7 @@ struct Engine : EngineBase {
   bool set_elec_capacity(int c) override {
     if (!split) return false;
     mce = c > 0 ? ((c + 31) / 32) * 32 : mce_auto;
+    ++generation;
     if (mc < mce + 32) {
       mc = mce + 32;
       alloc_rows();
@@ -751,6 +755,7 @@ struct Engine : EngineBase {
     if (want != cc) {
       cc = want;
       cand.alloc((size_t)nt * cc);
+      ++generation;
     }
     int one = 1;
     CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice));
@@ -980,6 +985,16 @@ struct Engine : EngineBase {
 struct PgmHandle {
   std::unique_ptr<EngineBase> eng;
   int device = 0;
+  // pgm_compute_host: its own stream and, from the second call on, the force call replayed as a
+  // captured graph (no host round trip per CG iteration) while the device buffers stay the same
+  cudaStream_t host_stream = nullptr;
+  cudaGraphExec_t host_graph = nullptr;
+  long long host_graph_gen = -1;
+  int host_calls = 0;
+  ~PgmHandle() {
+    if (host_graph) cudaGraphExecDestroy(host_graph);
+    if (host_stream) cudaStreamDestroy(host_stream);
+  }
 };
 
 static PgmStatus fail(PgmStatus s, const std::string &m) {
@@ -1099,13 +1114,15 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
       e->host_scratch_bytes = 0;
       CK(cudaMalloc(&e->host_scratch, bytes));
       e->host_scratch_bytes = bytes;
+      ++e->generation;
     }
+    if (!h->host_stream) CK(cudaStreamCreateWithFlags(&h->host_stream, cudaStreamNonBlocking));
     d = e->host_scratch;
     double *dpos = d, *dbox = dpos + n3, *dmu = dbox + 9 * ns, *dhist = dmu + n3, *dnorm = dhist + 4 * n3, *den = dnorm + ns,
            *dF = den + 3 * ns, *dvir = dF + n3, *dres = dvir + 9 * ns;
     int32_t *dcount = reinterpret_cast<int32_t *>(dres + ns), *dit = dcount + ns;
     uint32_t *dst = reinterpret_cast<uint32_t *>(dit + ns);
-    cudaStream_t st = 0;
+    cudaStream_t st = h->host_stream;
     CK(cudaMemcpyAsync(dpos, pos, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dbox, box, sizeof(double) * 9 * ns, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dmu, ind->mu, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
@@ -1114,7 +1131,31 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
     CK(cudaMemcpyAsync(dcount, ind->count, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
     PgmInduction di{dmu, dhist, dcount, dnorm};
     PgmOutputs dout{den, dF, dvir, dit, dres, dst};
-    e->compute(st, dpos, dbox, nullptr, 0, &di, &dout);
+    if (h->host_graph && h->host_graph_gen != e->generation) {
+      cudaGraphExecDestroy(h->host_graph);
+      h->host_graph = nullptr;
+    }
+    if (!h->host_graph && h->host_calls > 0) {
+      // capture once (the first call ran directly and sized the unrolled CG iterations)
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+      try {
+        e->compute(st, dpos, dbox, nullptr, 0, &di, &dout);
+      } catch (...) {
+        cudaGraph_t junk;
+        cudaStreamEndCapture(st, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        throw;
+      }
+      cudaGraph_t g;
+      CK(cudaStreamEndCapture(st, &g));
+      cudaError_t ie = cudaGraphInstantiate(&h->host_graph, g, 0);
+      cudaGraphDestroy(g);
+      CK(ie);
+      h->host_graph_gen = e->generation;
+    }
+    if (h->host_graph) CK(cudaGraphLaunch(h->host_graph, st));
+    else e->compute(st, dpos, dbox, nullptr, 0, &di, &dout);
+    ++h->host_calls;
     CK(cudaMemcpyAsync(ind->mu, dmu, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(ind->hist, dhist, sizeof(double) * 4 * n3, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(ind->norm, dnorm, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));

@@ -254,3 +254,45 @@ def test_split_rows_match_oracle(small_box_system, prec):
         r2 = small.compute(pos, H)
         assert int(r2.status[0]) == 0 and small.elec_capacity >= 32 and e_cap > 0
         assert abs(float(r2.energy["total"][0]) - ro["energy"]["total"]) <= 1e-10 * abs(ro["energy"]["total"])
+
+
+def test_compute_host_matches_device_calls():
+    """pgm_compute_host (host buffers; from the second call a replayed captured graph) gives the
+    device path's energies, forces and dipole history over consecutive steps, also after the row
+    capacity changed (the captured graph is rebuilt)."""
+    import ctypes as C
+
+    from pgm_jax_b200 import _lib
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(4, 1.25, seed=9)
+    kw = dict(cutoff=0.6, ewald_beta=5.0, pme_grid=(32, 32, 32), dipole_tol=1e-7, max_iter=100)
+    fd = ff_for(s, H, "mixed", **kw)
+    fh = ff_for(s, H, "mixed", **kw)
+    ind_d = fd.init_induction()
+    n = s.n
+    mu, hist = np.zeros((n, 3)), np.zeros((4, n, 3))
+    cnt, norm = np.zeros(1, np.int32), np.ones(1)
+    E, F, V = np.zeros((1, 3)), np.zeros((n, 3)), np.zeros((1, 3, 3))
+    it, res, stt = np.zeros(1, np.int32), np.zeros(1), np.zeros(1, np.int32)
+    p = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    ind = _lib.PgmInduction(p(mu).value, p(hist).value, p(cnt).value, p(norm).value)
+    out = _lib.PgmOutputs(p(E).value, p(F).value, p(V).value, p(it).value, p(res).value, p(stt).value)
+    rng = np.random.default_rng(3)
+    x = pos.copy()
+    hb = np.ascontiguousarray(H[None])
+    for step in range(7):
+        if step == 4:
+            fh.set_capacity(fh.capacity + 32)
+            fd.set_capacity(fd.capacity + 32)
+        x = x + rng.normal(scale=2e-4, size=x.shape)
+        xc = np.ascontiguousarray(x)
+        _lib.check(fh._lib.pgm_compute_host(fh._h, p(xc), p(hb), C.byref(ind), C.byref(out)))
+        rd = fd.compute(x, H, None, ind_d)
+        ind_d = rd.induction
+        assert stt[0] == 0
+        # mixed precision: the two handles differ only by the order of FP32 atomic additions
+        assert abs(E[0, 2] - float(rd.energy["total"][0])) <= 1e-7 * abs(E[0, 2]), step
+        assert np.abs(F - rd.forces.cpu().numpy()).max() <= 1e-5 * np.abs(F).max(), step
+        assert np.abs(hist - ind_d.hist.cpu().numpy()).max() <= 1e-5 * np.abs(hist).max(), step
+        assert abs(int(it[0]) - int(rd.iterations[0])) <= 1 and int(cnt[0]) == int(ind_d.count[0]) == step + 1
