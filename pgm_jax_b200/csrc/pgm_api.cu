@@ -182,6 +182,7 @@ struct Engine : EngineBase {
   DBuf<int> cand, ncand, nb_flag;
   DBuf<long long> nb_builds;
   DBuf<int> rn, rnsp, rk, dmax, dany;
+  DBuf<unsigned> cg_done;  // blocks of the fused CG update that have finished (the last one checks)
   DBuf<T> rx, ry, rz, rg0, rg1, rg2, rg3;
   DBuf<T> Q, Phi, Ginf;
   DBuf<pgm::c2<T>> C, tw;
@@ -472,7 +473,8 @@ struct Engine : EngineBase {
     CK(cudaMemset(cell_count.p, 0, sizeof(int) * ncell));
     CK(cudaMemset(nb_builds.p, 0, sizeof(long long)));
     { int one = 1; CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice)); }
-    rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(2); dany.alloc(1);
+    rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(2); dany.alloc(1); cg_done.alloc(1);
+    CK(cudaMemset(cg_done.p, 0, sizeof(unsigned)));
     if (split) rnv.alloc(nt);
     alloc_rows();
     Q.alloc(rgrid); Phi.alloc(rgrid); Ginf.alloc(cgrid); C.alloc(cgrid);
@@ -807,8 +809,8 @@ struct Engine : EngineBase {
   // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check.
   void iteration(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
     sweep<false, true, 1, 1>(st, a, Pv.p, AP.p);
-    launch_pdl(pgm::k_cg_update<T>, ntblk, 256, 0, st, a);
-    launch_pdl(pgm::k_cg_check, 1, 256, 0, st, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, cond, use_cond);
+    launch_pdl(pgm::k_cg_update_check<T>, ntblk, 256, 0, st, a, nsys, set.dipole_tol, set.max_iter, dany.p, cond, use_cond,
+               cg_done.p);
   }
 
   bool any_active(cudaStream_t st) {

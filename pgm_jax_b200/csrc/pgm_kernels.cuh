@@ -1587,14 +1587,15 @@ __global__ void k_cg_begin(CGSys *cg, int nsys, double tol, int max_iter, int *a
 
 // One CG update (thread per atom): x += a p, r' = r - a Ap, z' = alpha r', and the sums of
 // z'.(r' - r), r'.z', max|z'| (forcefield.py:1802-1814).
+// One CG update (thread per atom): x += st p, r -= st Ap, z = alpha r (Jacobi), with the block
+// partials of z.(r_new - r), r.z and max|z| added to the system's accumulators.
 template <typename T>
-__global__ void k_cg_update(Dev<T> a) {
-  pdl_enter();
+__device__ __forceinline__ void cg_update_body(Dev<T> &a) {
   __shared__ double red[2][THREADS_PER_BLOCK / 32];
   __shared__ unsigned long long mx[THREADS_PER_BLOCK / 32];
   int s = a.tb_sys[blockIdx.x];
   CGSys &G = a.cg[s];
-  if (!G.active) return;
+  if (!G.active) return;  // the block's system has converged
   int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
   const SysInfo &S = a.sys[s];
   double num = 0, rzn = 0, m = 0;
@@ -1630,12 +1631,15 @@ __global__ void k_cg_update(Dev<T> a) {
   }
 }
 
-// Per-system scalars after an update: beta (Polak-Ribiere), r.z, err, iteration count and the
-// loop condition err > tol and it < max_iter (forcefield.py:1798-1816).  *any = some system
-// still iterating.
-__global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *any, cudaGraphConditionalHandle cond,
-                           int use_cond) {
+template <typename T>
+__global__ void k_cg_update(Dev<T> a) {
   pdl_enter();
+  cg_update_body(a);
+}
+
+// The per-system scalars after an update (the body of k_cg_check, run by one block).
+__device__ __forceinline__ void cg_check_body(CGSys *cg, int nsys, double tol, int max_iter, int *any,
+                                              cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ int act;
   if (threadIdx.x == 0) act = 0;
   __syncthreads();
@@ -1656,6 +1660,33 @@ __global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *a
     *any = act;
     if (use_cond) cudaGraphSetConditional(cond, act ? 1u : 0u);  // the captured while loop of the solve
   }
+}
+
+// k_cg_update and k_cg_check in one launch: every block adds its partial sums, and the block that
+// finishes last (a counter after a memory fence) evaluates the per-system scalars and the loop
+// condition, then resets the counter for the next iteration.
+template <typename T>
+__global__ void k_cg_update_check(Dev<T> a, int nsys, double tol, int max_iter, int *any, cudaGraphConditionalHandle cond,
+                                  int use_cond, unsigned *done) {
+  pdl_enter();
+  cg_update_body(a);
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's partial sums are visible before it is counted
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  cg_check_body(a.cg, nsys, tol, max_iter, any, cond, use_cond);
+  if (threadIdx.x == 0) *done = 0u;
+}
+
+__global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *any, cudaGraphConditionalHandle cond,
+                           int use_cond) {
+  pdl_enter();
+  cg_check_body(cg, nsys, tol, max_iter, any, cond, use_cond);
 }
 
 // After the loop: the peek step mu = x + peek alpha r (forcefield.py:1819-1820), the dipoles
