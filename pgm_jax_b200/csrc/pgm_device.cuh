@@ -12,9 +12,9 @@ constexpr double PI = 3.14159265358979323846;
 constexpr int WARPS_PER_BLOCK = 8;       // warp-per-atom kernels: 8 atoms per block
 constexpr int THREADS_PER_BLOCK = 256;   // thread-per-atom kernels: 256 atoms per block
 constexpr int MAX_STAGES = 10;           // FFT stages per axis
-constexpr int FFT_TILE = 8;              // lines per CTA in the strided FFT passes
-constexpr int FFT_PAIRS = 4;             // complex lines (= 2x real lines) per CTA in the k3 pass
-constexpr int FFT_THREADS = 128;         // threads per CTA of the FFT passes (many small CTAs: latency)
+constexpr int FFT_TILE = 16;             // lines per CTA in the strided FFT passes
+constexpr int FFT_PAIRS = 8;             // complex lines (= 2x real lines) per CTA in the k3 pass
+constexpr int FFT_THREADS = 256;         // threads per CTA of the FFT passes (<= the passes' launch bounds)
 
 template <typename T> struct Vec4;
 template <> struct Vec4<float> { using type = float4; };

@@ -765,6 +765,8 @@ struct c2pair {
   c2<T> a, b;
 };
 
+static_assert(FFT_THREADS <= 256, "the FFT passes are compiled for at most 256 threads per CTA");
+
 // A launch of an FFT pass covers a group of systems with the same mesh length along the pass's
 // axis: block -> (group member g, tile) by the tile prefix gtile0 (ng + 1 entries).
 __device__ __forceinline__ int group_member(const int *gtile0, int ng, int b) {
