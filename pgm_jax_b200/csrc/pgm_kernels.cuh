@@ -1057,16 +1057,29 @@ __global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restr
     const float4 *x4 = reinterpret_cast<const float4 *>(a.rx + base), *y4 = reinterpret_cast<const float4 *>(a.ry + base),
                  *z4 = reinterpret_cast<const float4 *>(a.rz + base), *p4 = reinterpret_cast<const float4 *>(a.rg1 + base),
                  *q4 = reinterpret_cast<const float4 *>(a.rg2 + base);
+    // streaming loads (evict first): the 90+ MB of rows pass through L2 once per sweep and must
+    // not push out the PME grids that the FFT passes read next.  The next group of four entries
+    // is loaded before the current one is used (two groups of row data in flight per lane).
+    int4 kk = make_int4(0, 0, 0, 0);
+    float4 xx = make_float4(0, 0, 0, 0), yy = xx, zz = xx, g1 = xx, g2 = xx;
+    if (4 * lane < n) {
+      kk = __ldcs(k4 + lane);
+      xx = __ldcs(x4 + lane); yy = __ldcs(y4 + lane); zz = __ldcs(z4 + lane); g1 = __ldcs(p4 + lane); g2 = __ldcs(q4 + lane);
+    }
     for (int t4 = lane; 4 * t4 < n; t4 += 32) {
-      // streaming loads (evict first): the 90+ MB of rows pass through L2 once per sweep and must
-      // not push out the PME grids that the FFT passes read next
-      int4 kk = __ldcs(k4 + t4);
-      float4 xx = __ldcs(x4 + t4), yy = __ldcs(y4 + t4), zz = __ldcs(z4 + t4), g1 = __ldcs(p4 + t4), g2 = __ldcs(q4 + t4);
+      const int t4n = t4 + 32;
+      int4 kn = make_int4(0, 0, 0, 0);
+      float4 xn = make_float4(0, 0, 0, 0), yn = xn, zn = xn, g1n = xn, g2n = xn;
+      if (4 * t4n < n) {
+        kn = __ldcs(k4 + t4n);
+        xn = __ldcs(x4 + t4n); yn = __ldcs(y4 + t4n); zn = __ldcs(z4 + t4n); g1n = __ldcs(p4 + t4n); g2n = __ldcs(q4 + t4n);
+      }
       int t = 4 * t4;
       pair(kk.x, xx.x, yy.x, zz.x, g1.x, g2.x);
       if (t + 1 < n) pair(kk.y, xx.y, yy.y, zz.y, g1.y, g2.y);
       if (t + 2 < n) pair(kk.z, xx.z, yy.z, zz.z, g1.z, g2.z);
       if (t + 3 < n) pair(kk.w, xx.w, yy.w, zz.w, g1.w, g2.w);
+      kk = kn; xx = xn; yy = yn; zz = zn; g1 = g1n; g2 = g2n;
     }
   } else {
     for (int t = lane; t < n; t += 32) {
