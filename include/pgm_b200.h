@@ -204,7 +204,7 @@ long long pgm_row_pairs(PgmHandle *h);
  * sweep), and CG iterates to the same tolerance; the untrained (zero) model is mu4.
  * Per-atom channels (N, 12) floats: c0 = alpha (b - b_prev) (b: the real-space field of charges and
  * permanent dipoles over the graph), c1 = mu1 - mu2, c2 = x4 - mu1, mu1.  Features: 16 rotation
- * invariants (float, (N, 16)) and 27 vector channels (float, (N, 27, 3)): c0..c2 and their
+ * invariants (float, (N, 16)) and 15 vector channels (float, (N, 15, 3)): c0..c2 and their
  * radial-basis sums over the graph, plain and projected on the edge direction.  The model
  * (pgm_nn_param_count() floats, device) is the MLP of pgm_nn_predict; sigma is the scale of the
  * per-step changes in the invariants [e nm]. */

@@ -1,7 +1,7 @@
 """NumPy restatement of the learned-guess model and its gradient -- TEST INFRASTRUCTURE.
 
 The same MLP as pgm_jax_b200/csrc/pgm_nn.cu (16 invariants -> 64 -> 64 SiLU -> 32 coefficients,
-mu = sum_c c_c v_c over 27 vector channels), with the BF16 roundings at the points where the
+mu = sum_c c_c v_c over 15 vector channels), with the BF16 roundings at the points where the
 tensor-core kernels round (inputs, weights, hidden activations, backpropagated errors), in float64
 otherwise; and the exact float64 model for finite-difference checks.  Only tests use it.
 """
@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
-N_IN, N_HID, N_OUT, N_CH = 16, 64, 32, 27
+N_IN, N_HID, N_OUT, N_CH = 16, 64, 32, 15
 
 
 def bf16(x: np.ndarray) -> np.ndarray:

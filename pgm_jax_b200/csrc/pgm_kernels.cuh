@@ -1339,13 +1339,13 @@ __global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, c
   C[9 + lane] = float(m1);
 }
 
-// Step 2, one warp per atom over the same edges: vector channels (NN_CH = 27) v0..v2 = the atom's own
-// c0..c2 and, for each c and 4 radial bases phi_k(r) = exp(-((r - 0.1 (k + 1) nm) / 0.1 nm)^2)
+// Step 2, one warp per atom over the same edges: vector channels (NN_CH = 15) v0..v2 = the atom's own
+// c0..c2 and, for each c and 2 radial bases phi_k(r) = exp(-((r - (0.15 + 0.2 k) nm) / 0.15 nm)^2)
 // (cos(pi r / rg) + 1) / 2, the aggregates A_ck = sum_j phi_k c_j and D_ck = sum_j phi_k (c_j . u) u
-// (u = x / r); 16 rotation invariants (asinh of magnitudes and dot products over the change scale
-// sigma, |mu1| over 0.02 e nm, alpha, radius).  The model mixes the 27 channels, so the predicted
-// correction turns with the system.  The A and the D sums are two passes over the edges (36 sums
-// live at a time, for occupancy).  Sets *valid (the next step has a previous b).
+// (u = x / r), 36 sums in one pass over the edges with a transposing warp reduction; 16 rotation
+// invariants (asinh of magnitudes and dot products over the change scale sigma, |mu1| over
+// 0.02 e nm, alpha, radius).  The model mixes the 15 channels, so the predicted correction turns
+// with the system.  Sets *valid (the next step has a previous b).
 // One halving step of a transposing warp reduction: lanes with bit (N/2) set keep the upper half of
 // their N values and receive the partner's upper half, the others the lower halves.
 template <int N>
@@ -1369,9 +1369,10 @@ __device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
   return v[0];
 }
 
-// The 36 sums of one kind (Q = 0: A, 1: D) over the graph edges, value o = (c * 4 + k) * 3 + x;
-// returns on lane l the total of value l (l < 32) and in tail[0..3] the totals of values 32..35.
-template <int Q, typename T>
+// The 36 sums over the graph edges in one pass, value o = ((q * 3 + c) * 2 + k) * 3 + x for the
+// plain (q = 0: A) and projected (q = 1: D) sums of channel c with radial basis k; returns on lane l
+// the total of value l (l < 32) and in tail[0..3] the totals of values 32..35.
+template <typename T>
 __device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const float *chan, float rg, float4 *ebuf, int *eoff,
                                               float (&tail)[4]) {
   float acc[36];
@@ -1381,10 +1382,10 @@ __device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const floa
     float r = sqrtf(x * x + y * y + z * z);
     float ir = 1.f / r, u[3] = {x * ir, y * ir, z * ir};
     float fc = 0.5f * (cospif(r / rg) + 1.f);
-    float phi[4];
+    float phi[2];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      float d = (r - 0.1f * (k + 1)) * 10.f;
+    for (int k = 0; k < 2; ++k) {
+      float d = (r - (0.15f + 0.2f * k)) * (1.f / 0.15f);
       phi[k] = expf(-d * d) * fc;
     }
     const float4 *cj = reinterpret_cast<const float4 *>(chan + (size_t)j * NN_CHAN);
@@ -1392,17 +1393,14 @@ __device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const floa
     float v[3][3] = {{c01.x, c01.y, c01.z}, {c01.w, c12.x, c12.y}, {c12.z, c12.w, c2m.x}};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      float w[3];
-      if (Q == 0) {
-        w[0] = v[c][0]; w[1] = v[c][1]; w[2] = v[c][2];
-      } else {
-        float pr = v[c][0] * u[0] + v[c][1] * u[1] + v[c][2] * u[2];
-        w[0] = pr * u[0]; w[1] = pr * u[1]; w[2] = pr * u[2];
-      }
+      float pr = v[c][0] * u[0] + v[c][1] * u[1] + v[c][2] * u[2];
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
+      for (int k = 0; k < 2; ++k)
 #pragma unroll
-        for (int xx = 0; xx < 3; ++xx) acc[(c * 4 + k) * 3 + xx] += phi[k] * w[xx];
+        for (int xx = 0; xx < 3; ++xx) {
+          acc[(c * 2 + k) * 3 + xx] += phi[k] * v[c][xx];
+          acc[18 + (c * 2 + k) * 3 + xx] += phi[k] * pr * u[xx];
+        }
     }
   });
 #pragma unroll
@@ -1426,17 +1424,13 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan
   float *F = inv + (size_t)i * pgmnn::NN_IN;
   const float is = 1.f / sigma, is2 = is * is;
   float tail[4];
-  // A sums: lane l holds value l; |A_0k| and |A_1k| (values 3k.. and 12 + 3k..) for the invariants
-  float mine = nn_aggregate<0>(a, i, chan, rg, ebuf[warp], eoff[warp], tail);
+  // lane l holds value l; the norms of the first eight (c, k) groups of three for the invariants
+  float mine = nn_aggregate(a, i, chan, rg, ebuf[warp], eoff[warp], tail);
   V[9 + lane] = mine;
   if (lane < 4) V[9 + 32 + lane] = tail[lane];
   float sq = mine * mine;
   float n2 = sq + __shfl_down_sync(0xffffffffu, sq, 1) + __shfl_down_sync(0xffffffffu, sq, 2);
-  if (lane < 24 && lane % 3 == 0) F[(lane < 12 ? 8 : 12) + (lane % 12) / 3] = asinhf(sqrtf(n2) * is);
-  // D sums
-  mine = nn_aggregate<1>(a, i, chan, rg, ebuf[warp], eoff[warp], tail);
-  V[45 + lane] = mine;
-  if (lane < 4) V[45 + 32 + lane] = tail[lane];
+  if (lane < 24 && lane % 3 == 0) F[8 + lane / 3] = asinhf(sqrtf(n2) * is);
   if (lane != 0) return;
   const float *ci = chan + (size_t)i * NN_CHAN;
   float self[3][3] = {{ci[0], ci[1], ci[2]}, {ci[3], ci[4], ci[5]}, {ci[6], ci[7], ci[8]}};

@@ -7,7 +7,7 @@ namespace pgmnn {
 constexpr int NN_IN = 16;   // rotation invariants per atom
 constexpr int NN_HID = 64;  // hidden width (2 layers)
 constexpr int NN_OUT = 32;  // coefficient outputs (the first NN_CH used)
-constexpr int NN_CH = 27;   // vector channels per atom
+constexpr int NN_CH = 15;   // vector channels per atom
 constexpr int NN_NPARAM = NN_IN * NN_HID + NN_HID + NN_HID * NN_HID + NN_HID + NN_HID * NN_OUT + NN_OUT;
 
 // Views into one flat FP32 array, in this order: w1 (IN x HID), b1, w2 (HID x HID), b2,

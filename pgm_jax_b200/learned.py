@@ -7,8 +7,8 @@ last step (the real-space field of charges and permanent dipoles over the graph 
 steps' dipoles.  With predictor "nn" the engine's solver starts CG from x4 + the prediction with
 mu4's fused start (one field sweep, as the reference's mu4 predictor) and iterates to the same
 tolerance, so the plain solver judges the guess; the untrained (zero) model is mu4 exactly.
-The model (csrc/pgm_nn.cu): 16 rotation invariants -> MLP 64 -> 64 (SiLU) -> 27 coefficients that
-mix 27 vector channels per atom (csrc/pgm_kernels.cuh k_nn_chan, k_nn_features), so the prediction
+The model (csrc/pgm_nn.cu): 16 rotation invariants -> MLP 64 -> 64 (SiLU) -> 15 coefficients that
+mix 15 vector channels per atom (csrc/pgm_kernels.cuh k_nn_chan, k_nn_features), so the prediction
 rotates with the system.  Training runs on the GPU with the project's BF16 tensor-core
 forward/backward kernels and Adam; the data are (features, mu* - x4) pairs written while the plain
 solver runs MD.  The reference has no counterpart (pgm_jax/md/forcefield.py:1917-2008 has the mu3,
@@ -24,7 +24,7 @@ import torch
 
 from . import _lib
 
-N_IN, N_HID, N_OUT, N_CH = 16, 64, 32, 27
+N_IN, N_HID, N_OUT, N_CH = 16, 64, 32, 15
 SIGMA = 2e-4  # e nm, scale of the per-step changes in the invariants and the loss
 GRAPH_CUTOFF = 0.5  # nm
 
@@ -46,7 +46,7 @@ def _p(t: torch.Tensor):
 
 
 def features(ff, pos: torch.Tensor, boxes: torch.Tensor, hist: torch.Tensor, bl_prev: torch.Tensor | None = None):
-    """Invariants (N, 16), vector channels (N, 27, 3) and the graph's permanent field (N, 4) at a
+    """Invariants (N, 16), vector channels (N, 15, 3) and the graph's permanent field (N, 4) at a
     geometry, with the history hist (4, N, 3) of the solve there.
 
     bl_prev: the previous step's graph field (else the field-change channel is zero).  Uses the
