@@ -203,8 +203,9 @@ struct Engine : EngineBase {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork_b = nullptr, ev_join_b = nullptr, ev_nn_fork = nullptr,
               ev_nn_join = nullptr;
   bool nn_forked = false;  // the learned guess of this step runs on nn_st (joined before the solve's start)
-  bool in_body = false;  // enqueueing the CG while-loop body (its own capture sequence)
+  bool in_body = false;  // enqueueing the body of a conditional node (its own capture sequence)
   bool overlap = true;  // row field on a second stream beside the FFT chain
+  int prio_hi = 0;      // the device's highest stream priority (the learned guess's kernels)
   long long per_iter = 0;
 
   ~Engine() {
@@ -491,7 +492,9 @@ struct Engine : EngineBase {
     CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_fork_b, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join_b, cudaEventDisableTiming));
-    CK(cudaStreamCreateWithFlags(&nn_st, cudaStreamNonBlocking));
+    int prio_lo = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CK(cudaStreamCreateWithPriority(&nn_st, cudaStreamNonBlocking, prio_hi));
     CK(cudaEventCreateWithFlags(&ev_nn_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_nn_join, cudaEventDisableTiming));
     set_smem();
@@ -574,8 +577,9 @@ struct Engine : EngineBase {
   // its change from bl_prev, when given, is a channel) and the history channels.
   void nn_inputs(cudaStream_t st, pgm::Dev<T> &a, const double *hist, const float4 *bl_prev, const int *valid, float4 *bl_out,
                  float *inv, float *vec, int *set_valid) {
-    pgm::k_nn_chan<T><<<nwblk, 256, 0, st>>>(a, hist, bl_prev, valid, nn_rg, bl_out, nn_chan.p); check_launch();
-    pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, nn_chan.p, nn_sigma, nn_rg, inv, vec, set_valid); check_launch();
+    launch_prio(pgm::k_nn_chan<T>, nwblk, 256, 0, st, prio_hi, a, hist, bl_prev, valid, nn_rg, bl_out, nn_chan.p);
+    launch_prio(pgm::k_nn_features<T>, nwblk, 256, 0, st, prio_hi, a, (const float *)nn_chan.p, nn_sigma, nn_rg, inv, vec,
+                set_valid);
   }
 
   void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const float *bl_prev,
@@ -717,6 +721,24 @@ struct Engine : EngineBase {
     ++launches;
   }
 
+  // A launch at scheduling priority prio (a node attribute when captured: the block scheduler
+  // dispatches its blocks ahead of those of concurrent lower-priority kernels).
+  template <typename... KArgs, typename... Args>
+  void launch_prio(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st, int prio, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributePriority;
+    at[0].val.priority = prio;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k, args...));
+    ++launches;
+  }
+
   // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
   // cell list, rows, influence function.
   // The learned guess's inputs and prediction for this step's rows: forked onto nn_st after the
@@ -725,7 +747,7 @@ struct Engine : EngineBase {
     CK(cudaEventRecord(ev_nn_fork, st));
     CK(cudaStreamWaitEvent(nn_st, ev_nn_fork, 0));
     nn_inputs(nn_st, a, hist, nn_bl.p, nn_valid.p, nn_bl.p, nn_inv.p, nn_vec.p, nn_valid.p);
-    cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, nn_st);
+    cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, nn_st, prio_hi);
     if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
     ++launches;
     CK(cudaEventRecord(ev_nn_join, nn_st));
@@ -813,6 +835,41 @@ struct Engine : EngineBase {
                cg_done.p);
   }
 
+  // Adds a conditional node (IF or WHILE on `cond`) after the capture's current dependencies of
+  // st, captures body(stream) into the node's body graph (on the side stream, with the sweep's
+  // fork on aux_b), and makes the node the capture's new dependency.
+  template <typename F>
+  void conditional_node(cudaStream_t st, cudaGraphConditionalHandle cond, cudaGraphConditionalNodeType type, F &&body) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    unsigned long long id;
+    CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t bg = np.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    if (!side) CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCaptureToGraph(side, bg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    in_body = true;
+    try {
+      body(side);
+    } catch (...) {
+      in_body = false;
+      cudaGraph_t junk;
+      cudaStreamEndCapture(side, &junk);
+      throw;
+    }
+    in_body = false;
+    CK(cudaStreamEndCapture(side, &bg));
+  }
+
   bool any_active(cudaStream_t st) {
     CK(cudaMemcpyAsync(h_any, dany.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -830,8 +887,23 @@ struct Engine : EngineBase {
     const int K = pred == 4 ? 4 : (pred == 3 ? 3 : (pred == 1 ? 1 : 0));
     const double c4[4] = {4.0, -6.0, 4.0, -1.0}, c3[4] = {3.0, -3.0, 1.0, 0.0}, c1[4] = {1.0, 0, 0, 0}, c0[4] = {0, 0, 0, 0};
     const double *cc = K == 4 ? c4 : (K == 3 ? c3 : (K == 1 ? c1 : c0));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    const bool captured = cs == cudaStreamCaptureStatusActive;
+    // captured: the plain start's second sweep sits in a conditional IF node whose condition
+    // k_cg_setup raises when some system takes the plain start (else the node's kernels are skipped)
+    cudaGraphConditionalHandle cond2 = 0;
+    if (captured) {
+      cudaGraph_t g;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t nd = 0;
+      unsigned long long id;
+      CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+      CK(cudaGraphConditionalHandleCreate(&cond2, g, 0, cudaGraphCondAssignDefault));
+    }
     pgm::k_cg_setup<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, mode == 0 ? ind->count : nullptr, ind->norm,
-                                                    mode == 0 ? K : 0, set.fused, std::max(1, set.norm_refresh), mode);
+                                                    mode == 0 ? K : 0, set.fused, std::max(1, set.norm_refresh), mode, cond2,
+                                                    captured ? 1 : 0);
     check_launch();
     if (mode == 1) {
       // x0 = ind->mu with the plain start: X = mu, have = 1
@@ -849,13 +921,15 @@ struct Engine : EngineBase {
     }
     sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
     pgm::k_start2<T><<<ntblk, 256, 0, st>>>(a); check_launch();
-    sweep<false, false, 2, 1>(st, a, X.p, AP.p);
-    pgm::k_start3<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
+    auto plain_start = [&](cudaStream_t s2) {
+      sweep<false, false, 2, 1>(s2, a, X.p, AP.p);
+      pgm::k_start3<T><<<grid1(nt), 256, 0, s2>>>(a); check_launch();
+    };
+    if (captured) conditional_node(st, cond2, cudaGraphCondTypeIf, plain_start);
+    else plain_start(st);
     pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
     pgm::k_cg_begin<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p); check_launch();
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    CK(cudaStreamIsCapturing(st, &cs));
-    if (cs == cudaStreamCaptureStatusActive) {
+    if (captured) {
       // captured: the first U iterations as plain kernel nodes (their kernels skip systems that
       // have converged; U = the iterations of the last host-driven solve - 2), then a conditional
       // while node whose body is one CG iteration.  The last check before the node and the body's
@@ -870,31 +944,11 @@ struct Engine : EngineBase {
       CK(cudaGraphConditionalHandleCreate(&cond, g, U > 0 ? 0 : 1, cudaGraphCondAssignDefault));
       for (int k = 0; k < U; ++k) iteration(st, a, cond, k == U - 1 ? 1 : 0);
       unrolled = U;
-      if (U > 0) CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
-      cudaGraphNodeParams np = {};
-      np.type = cudaGraphNodeTypeConditional;
-      np.conditional.handle = cond;
-      np.conditional.type = cudaGraphCondTypeWhile;
-      np.conditional.size = 1;
-      cudaGraphNode_t node;
-      CK(cudaGraphAddNode(&node, g, deps, nd, &np));
-      cudaGraph_t body = np.conditional.phGraph_out[0];
-      CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
-      if (!side) CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-      CK(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-      long long l0 = launches;
-      in_body = true;
-      try {
-        iteration(side, a, cond, 1);
-      } catch (...) {
-        in_body = false;
-        cudaGraph_t junk;
-        cudaStreamEndCapture(side, &junk);
-        throw;
-      }
-      in_body = false;
-      per_iter = launches - l0;
-      CK(cudaStreamEndCapture(side, &body));
+      conditional_node(st, cond, cudaGraphCondTypeWhile, [&](cudaStream_t s2) {
+        long long l0 = launches;
+        iteration(s2, a, cond, 1);
+        per_iter = launches - l0;
+      });
     } else {
       int it = 0;
       for (; it < set.max_iter; ++it) {
@@ -1150,7 +1204,7 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
       }
       cudaGraph_t g;
       CK(cudaStreamEndCapture(st, &g));
-      cudaError_t ie = cudaGraphInstantiate(&h->host_graph, g, 0);
+      cudaError_t ie = cudaGraphInstantiateWithFlags(&h->host_graph, g, cudaGraphInstantiateFlagUseNodePriority);
       cudaGraphDestroy(g);
       CK(ie);
       h->host_graph_gen = e->generation;

@@ -1737,7 +1737,7 @@ __global__ void k_cg_state_out(const CGSys *cg, int nsys, int32_t *count, double
 // mode 0: history predictor (compute); mode 1: the guess is the state's mu, plain start (energy,
 // forcefield.py:2606-2612).
 __global__ void k_cg_setup(CGSys *cg, int nsys, const int32_t *count, const double *norm, int K, int fused, int refresh,
-                           int mode) {
+                           int mode, cudaGraphConditionalHandle plain, int use_cond) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   CGSys &G = cg[s];
@@ -1745,6 +1745,7 @@ __global__ void k_cg_setup(CGSys *cg, int nsys, const int32_t *count, const doub
   G.have = mode == 1 ? 1 : (K > 0 && c >= K);
   G.fused = mode == 0 && G.have && fused && (c % refresh) != 0;
   G.sweep2 = !G.fused;
+  if (use_cond && G.sweep2) cudaGraphSetConditional(plain, 1u);  // the plain start's sweep runs (default 0)
   G.active = 0;
   G.norm = G.fused ? norm[s] : 1.0;
   G.acc_abs = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0; G.acc_num = 0;

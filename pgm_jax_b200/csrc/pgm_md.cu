@@ -40,12 +40,13 @@ __device__ __forceinline__ void quat_rot(const double *q, double R[9]) {
 // Free rotation about body axis k for time t: L rotates by -phi about e_k, q <- q (x) exp(phi/2 e_k).
 __device__ __forceinline__ void rotate_axis(int k, double t, const double *I, double *L, double *q) {
   double phi = t * L[k] / I[k];
-  double c = cos(phi), s = sin(phi);
+  double sh, ch;
+  sincos(0.5 * phi, &sh, &ch);
+  const double c = 1.0 - 2.0 * sh * sh, s = 2.0 * sh * ch;  // cos phi, sin phi by the double-angle identities
   int a = (k + 1) % 3, b = (k + 2) % 3;
   double La = L[a], Lb = L[b];
   L[a] = c * La + s * Lb;
   L[b] = -s * La + c * Lb;
-  double ch = cos(0.5 * phi), sh = sin(0.5 * phi);
   double e[3] = {0, 0, 0};
   e[k] = sh;
   double w = q[0], x = q[1], y = q[2], z = q[3];
@@ -79,9 +80,10 @@ __device__ __forceinline__ void normals(unsigned long long seed, unsigned long l
   unsigned long long h2 = mix64(h);
   double u1 = ((h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
   double u2 = ((h2 >> 11) + 0.5) * (1.0 / 9007199254740992.0);
-  double r = sqrt(-2.0 * log(u1));
-  g0 = r * cospi(2.0 * u2);
-  g1 = r * sinpi(2.0 * u2);
+  double r = sqrt(-2.0 * log(u1)), sn, cs;
+  sincospi(2.0 * u2, &sn, &cs);
+  g0 = r * cs;
+  g1 = r * sn;
 }
 
 // Half kick of P and L from the atom forces.
@@ -305,7 +307,7 @@ PgmStatus pgm_graph_end(void *stream, void **exec_out) {
   cudaGraph_t g;
   MDCK(cudaStreamEndCapture((cudaStream_t)stream, &g));
   cudaGraphExec_t ex;
-  MDCK(cudaGraphInstantiate(&ex, g, 0));
+  MDCK(cudaGraphInstantiateWithFlags(&ex, g, cudaGraphInstantiateFlagUseNodePriority));  // kernels keep their launch priority
   MDCK(cudaGraphDestroy(g));
   *exec_out = (void *)ex;
   return PGM_OK;

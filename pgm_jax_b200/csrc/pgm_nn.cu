@@ -8,7 +8,7 @@
 // NN_HID, c: NN_OUT coefficients, the first NN_CH used); mu = sum_c c_c v_c over the atom's vector
 // channels.  Weights: an FP32 master array; each CTA converts them to BF16 in shared memory.  In
 // training a CTA of 4 warps runs a tile of 64 samples through all layers (each warp 16 rows); in
-// inference each warp runs its own 16 samples.
+// inference a CTA runs 16 samples, each warp a 16-column slice of every layer.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <mma.h>
@@ -165,51 +165,86 @@ __device__ void forward_tile(Smem &s) {
   __syncthreads();
 }
 
-// Inference: every warp runs its own 16 samples through the layers (warp-synchronous, no block
-// barrier after the weights are staged), in a small shared-memory footprint so that several CTAs
-// share an SM.  Same rounding points as the training forward.
+// Inference: a CTA of 4 warps runs 16 samples at a time through the layers with the output columns
+// split across the warps (layers 1 and 2: 16 hidden columns per warp; layer 3: the 16 coefficient
+// columns that the channel mix uses, its K = 64 split in four and the partial products summed in
+// shared memory), so that a sample's chain of dependent tensor-core steps is a quarter of a whole
+// layer stack.  Same rounding points as the training forward (BF16 operands, FP32 accumulation).
 constexpr int FWD_ROWS = 16;
+constexpr int FWD_WARPS = THREADS / 32;
+static_assert(NN_HID == 16 * FWD_WARPS && NN_CH <= 16, "one 16-column slice of each layer per warp");
 struct FwdSmem {
   __nv_bfloat16 w1[NN_IN * NN_HID], w2[NN_HID * NN_HID], w3[NN_HID * NN_OUT];
-  __nv_bfloat16 x[THREADS / 32][FWD_ROWS * NN_IN], act[THREADS / 32][FWD_ROWS * NN_HID];
-  float z[THREADS / 32][FWD_ROWS * NN_HID];
+  __nv_bfloat16 x[FWD_ROWS * NN_IN], a1[FWD_ROWS * NN_HID], a2[FWD_ROWS * NN_HID];
+  float z[FWD_ROWS * NN_HID];            // layer outputs before the activation
+  float zp[FWD_WARPS][FWD_ROWS * 16];    // layer-3 partial products
   float b1[NN_HID], b2[NN_HID], b3[NN_OUT];
 };
+
+// One warp's 16 x 16 slice: C (ldc) = A[16 x K] (lda) B[K x 16] (ldb), FP32 accumulation.
+template <int K>
+__device__ __forceinline__ void warp_slice(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int ldb, float *C, int ldc) {
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+  wmma::fill_fragment(acc, 0.0f);
+#pragma unroll
+  for (int k = 0; k < K; k += 16) {
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> fa;
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> fb;
+    wmma::load_matrix_sync(fa, A + k, lda);
+    wmma::load_matrix_sync(fb, B + k * ldb, ldb);
+    wmma::mma_sync(acc, fa, fb, acc);
+  }
+  wmma::store_matrix_sync(C, acc, ldc, wmma::mem_row_major);
+}
 
 __global__ void __launch_bounds__(THREADS) k_forward(NNWeights w, const float *inv, const float *vec, int n, float *mu) {
   __shared__ __align__(128) FwdSmem s;
   stage_weights(w, s.w1, s.w2, s.w3, s.b1, s.b2, s.b3);
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __nv_bfloat16 *x = s.x[warp], *act = s.act[warp];
-  float *z = s.z[warp];
-  for (int tile = blockIdx.x * (THREADS / 32) + warp; tile * FWD_ROWS < n; tile += gridDim.x * (THREADS / 32)) {
-    const int r0 = tile * FWD_ROWS;
-    for (int t = lane; t < FWD_ROWS * NN_IN; t += 32) {
-      int i = r0 + t / NN_IN;
-      x[t] = __float2bfloat16(i < n ? inv[(size_t)r0 * NN_IN + t] : 0.f);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, c0 = 16 * warp;
+  for (int r0 = blockIdx.x * FWD_ROWS; r0 < n; r0 += gridDim.x * FWD_ROWS) {
+    // the channel vectors of the mix (threads 0..47: row t / 3, component t % 3) in flight
+    // through the layers
+    float v[NN_CH];
+    const int mr = threadIdx.x / 3, ma = threadIdx.x - 3 * mr, mi = r0 + mr;
+    const bool mixer = threadIdx.x < FWD_ROWS * 3 && mi < n;
+    if (mixer) {
+      const float *vp = vec + (size_t)mi * NN_CH * 3 + ma;
+#pragma unroll
+      for (int c = 0; c < NN_CH; ++c) v[c] = vp[3 * c];
     }
+    for (int t = threadIdx.x; t < FWD_ROWS * NN_IN; t += THREADS) {
+      int i = r0 + t / NN_IN;
+      s.x[t] = __float2bfloat16(i < n ? inv[(size_t)r0 * NN_IN + t] : 0.f);
+    }
+    __syncthreads();  // x (and, on the first tile, the weights)
+    warp_slice<NN_IN>(s.x, NN_IN, s.w1 + c0, NN_HID, s.z + c0, NN_HID);
     __syncwarp();
-    warp_gemm<NN_HID, NN_IN>(x, NN_IN, s.w1, NN_HID, z, NN_HID);
+    for (int e = lane; e < FWD_ROWS * 16; e += 32) {
+      int r = e >> 4, c = c0 + (e & 15);
+      s.a1[r * NN_HID + c] = __float2bfloat16(silu(s.z[r * NN_HID + c] + s.b1[c]));
+    }
+    __syncthreads();  // a1 complete
+    warp_slice<NN_HID>(s.a1, NN_HID, s.w2 + c0, NN_HID, s.z + c0, NN_HID);
     __syncwarp();
-    for (int t = lane; t < FWD_ROWS * NN_HID; t += 32) act[t] = __float2bfloat16(silu(z[t] + s.b1[t % NN_HID]));
-    __syncwarp();
-    warp_gemm<NN_HID, NN_HID>(act, NN_HID, s.w2, NN_HID, z, NN_HID);
-    __syncwarp();
-    for (int t = lane; t < FWD_ROWS * NN_HID; t += 32) act[t] = __float2bfloat16(silu(z[t] + s.b2[t % NN_HID]));
-    __syncwarp();
-    warp_gemm<NN_OUT, NN_HID>(act, NN_HID, s.w3, NN_OUT, z, NN_OUT);
-    __syncwarp();
-    for (int t = lane; t < FWD_ROWS * 3; t += 32) {
-      int r = t / 3, a = t - 3 * r, i = r0 + r;
-      if (i >= n) continue;
-      const float *v = vec + (size_t)i * NN_CH * 3;
+    for (int e = lane; e < FWD_ROWS * 16; e += 32) {
+      int r = e >> 4, c = c0 + (e & 15);
+      s.a2[r * NN_HID + c] = __float2bfloat16(silu(s.z[r * NN_HID + c] + s.b2[c]));
+    }
+    __syncthreads();  // a2 complete
+    // layer 3, coefficient columns 0..15: this warp's 16 rows of K
+    warp_slice<16>(s.a2 + c0, NN_HID, s.w3 + c0 * NN_OUT, NN_OUT, s.zp[warp], 16);
+    __syncthreads();
+    if (mixer) {
       float acc = 0.f;
 #pragma unroll
-      for (int c = 0; c < NN_CH; ++c) acc += (z[r * NN_OUT + c] + s.b3[c]) * v[3 * c + a];  // all loads in flight
-      mu[3 * (size_t)i + a] = acc;
+      for (int c = 0; c < NN_CH; ++c) {
+        const int e = mr * 16 + c;
+        const float coef = ((s.zp[0][e] + s.zp[1][e]) + (s.zp[2][e] + s.zp[3][e])) + s.b3[c];
+        acc += coef * v[c];
+      }
+      mu[3 * (size_t)mi + ma] = acc;
     }
-    __syncwarp();
+    __syncthreads();  // x, z and zp are rewritten by the next tile
   }
 }
 
@@ -321,13 +356,22 @@ cudaError_t set_attrs() {
   return e;
 }
 
-cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *vec, int n, float *mu, cudaStream_t st) {
+cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *vec, int n, float *mu, cudaStream_t st,
+                              int priority) {
   cudaError_t e = set_attrs();
   if (e != cudaSuccess) return e;
   if (n <= 0) return cudaSuccess;
-  const int tiles = (n + FWD_ROWS - 1) / FWD_ROWS, per = THREADS / 32;
-  k_forward<<<(tiles + per - 1) / per, THREADS, 0, st>>>(nn_view(const_cast<float *>(flat)), inv, vec, n, mu);
-  return cudaGetLastError();
+  const int tiles = (n + FWD_ROWS - 1) / FWD_ROWS;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tiles);  // one 16-sample tile per CTA (about 24 KB of shared memory each)
+  cfg.blockDim = dim3(THREADS);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributePriority;
+  at[0].val.priority = priority;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_forward, nn_view(const_cast<float *>(flat)), inv, vec, n, mu);
 }
 
 thread_local std::string g_nn_err;
@@ -340,7 +384,7 @@ int pgm_nn_param_count(void) { return pgmnn::NN_NPARAM; }
 
 PgmStatus pgm_nn_predict(void *stream, const float *weights, const float *inv, const float *vec, int n, float *mu) {
   if (!weights || !inv || !vec || !mu || n < 0) return PGM_ERR_INVALID;
-  cudaError_t e = pgmnn::nn_predict_launch(weights, inv, vec, n, mu, (cudaStream_t)stream);
+  cudaError_t e = pgmnn::nn_predict_launch(weights, inv, vec, n, mu, (cudaStream_t)stream, 0);
   if (e != cudaSuccess) {
     pgmnn::g_nn_err = cudaGetErrorString(e);
     return PGM_ERR_CUDA;

@@ -29,6 +29,6 @@ inline __host__ __device__ NNWeights nn_view(float *flat) {
 
 // mu (n, 3) FP32 = the model's prediction from invariants inv (n, NN_IN) and channels vec
 // (n, NN_CH, 3); launched on `st` (used by the engine's solver start).
-cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *vec, int n, float *mu, cudaStream_t st);
+cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *vec, int n, float *mu, cudaStream_t st, int priority = 0);
 
 }  // namespace pgmnn
