@@ -160,7 +160,7 @@ struct Engine : EngineBase {
   DBuf<int> rnv;
   double skin = 0.0;
   long long rgrid = 0, cgrid = 0;
-  std::vector<std::unique_ptr<FftGroup>> gx, gy, gz;
+  std::vector<std::unique_ptr<FftGroup>> gx, gy, gz, gp;  // k3, k2, k1 passes; plane passes (k3 + k2)
   int nwblk = 0, ntblk = 0;
   std::vector<int> natoms;
 
@@ -415,18 +415,30 @@ struct Engine : EngineBase {
     nwblk = (int)wbs.size();
     ntblk = (int)tbs.size();
     wb_sys.upload(wbs); wb_atom0.upload(wba); tb_sys.upload(tbs); tb_atom0.upload(tba);
+    // plane passes for the systems whose K2 = K3 mesh has a compiled plan and whose plane (two
+    // regions + the twiddles) fits in a CTA's shared memory; the others run the k3 and k2 passes
+    int cur_dev = 0, smem_optin = 0;
+    CK(cudaGetDevice(&cur_dev));
+    CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, cur_dev));
+    auto plane_ok = [&](const pgm::SysInfo &S) {
+      const int L = S.K[1];
+      if (L != S.K[2] || L > 128 || L % 8 != 0) return false;
+      bool compiled = false;
+      with_fft_len(L, [&](auto Lc) { compiled = decltype(Lc)::value != 0; });
+      return compiled && plane_smem(L) <= (size_t)smem_optin;
+    };
     // FFT launch groups per axis: systems with the same mesh length share one launch
     auto groups = [&](int axis, std::vector<std::unique_ptr<FftGroup>> &out) {
       std::vector<int> Ks;
       for (auto &S : hsys)
-        if (std::find(Ks.begin(), Ks.end(), S.K[axis]) == Ks.end()) Ks.push_back(S.K[axis]);
+        if ((axis == 0 || !plane_ok(S)) && std::find(Ks.begin(), Ks.end(), S.K[axis]) == Ks.end()) Ks.push_back(S.K[axis]);
       for (int K : Ks) {
         std::unique_ptr<FftGroup> g(new FftGroup());
         g->K = K;
         std::vector<int> gs, gt{0};
         for (int si = 0; si < n; ++si) {
           const pgm::SysInfo &S = hsys[si];
-          if (S.K[axis] != K) continue;
+          if (S.K[axis] != K || (axis != 0 && plane_ok(S))) continue;
           int tiles = axis == 2 ? (S.K[0] * S.K[1] + 2 * pgm::FFT_PAIRS - 1) / (2 * pgm::FFT_PAIRS)
                     : axis == 1 ? (S.K[0] * S.K3h + pgm::FFT_TILE - 1) / pgm::FFT_TILE
                                 : (S.K[1] * S.K3h + pgm::FFT_TILE - 1) / pgm::FFT_TILE;
@@ -445,6 +457,27 @@ struct Engine : EngineBase {
     groups(2, gx);
     groups(1, gy);
     groups(0, gz);
+    {
+      std::vector<int> Ls;
+      for (auto &S : hsys)
+        if (plane_ok(S) && std::find(Ls.begin(), Ls.end(), S.K[1]) == Ls.end()) Ls.push_back(S.K[1]);
+      for (int L : Ls) {
+        std::unique_ptr<FftGroup> g(new FftGroup());
+        g->K = L;
+        std::vector<int> gs, gt{0};
+        for (int si = 0; si < n; ++si) {
+          if (!plane_ok(hsys[si]) || hsys[si].K[1] != L) continue;
+          gs.push_back(si);
+          gt.push_back(gt.back() + hsys[si].K[0]);  // one CTA per k1 plane
+        }
+        g->ng = (int)gs.size();
+        g->ntiles = gt.back();
+        g->smem = plane_smem(L);
+        g->sys.upload(gs);
+        g->tile0.upload(gt);
+        gp.push_back(std::move(g));
+      }
+    }
     d_sys.upload(hsys);
     d_box.alloc(n);
     CK(cudaMemset(d_box.p, 0, sizeof(pgm::BoxInfo) * n));
@@ -506,12 +539,29 @@ struct Engine : EngineBase {
     rk.alloc(m); rx.alloc(m); ry.alloc(m); rz.alloc(m); rg0.alloc(m); rg1.alloc(m); rg2.alloc(m); rg3.alloc(m);
   }
 
+  static size_t plane_smem(int L) { return (size_t)(2 * pgm::plane_region(L) + L) * sizeof(pgm::c2<T>); }
+
+  // Plane-pass lengths: the compiled plans up to 128 (a 192 plane does not fit in shared memory).
+  template <typename F>
+  static void with_plane_len(int L, F &&f) {
+    with_fft_len(L, [&](auto Lc) {
+      constexpr int Lv = decltype(Lc)::value;
+      if constexpr (Lv > 0 && Lv <= 128) f(Lc);
+    });
+  }
+
   template <typename K>
   void smem_attr(K kern, size_t bytes) {
     if (bytes > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   }
 
   void set_smem() {
+    for (auto &g : gp)
+      with_plane_len(g->K, [&](auto Lc) {
+        constexpr int L = decltype(Lc)::value;
+        smem_attr(pgm::k_fft_plane_fwd<T, L>, g->smem);
+        smem_attr(pgm::k_fft_plane_inv<T, L>, g->smem);
+      });
     for (auto &g : gx)
       with_fft_len(g->K, [&](auto Lc) {
         constexpr int L = decltype(Lc)::value;
@@ -531,8 +581,19 @@ struct Engine : EngineBase {
       });
   }
 
-  // The five passes of one reciprocal-space convolution (r2c, k2, k1 with G, k2, c2r).
+  // The forward plane passes (k3 + k2 per k1 plane) of the systems that have them.
+  void plane_fwd(cudaStream_t st, pgm::Dev<T> &a, int act) {
+    for (auto &g : gp)
+      with_plane_len(g->K, [&](auto Lc) {
+        launch_pdl(pgm::k_fft_plane_fwd<T, decltype(Lc)::value>, g->ntiles, pgm::PLANE_THREADS, g->smem, st, a,
+                   (const int *)g->sys.p, (const int *)g->tile0.p, g->ng, act);
+      });
+  }
+
+  // The passes of one reciprocal-space convolution: r2c (k3) and k2 -- one plane pass where the
+  // mesh has it --, k1 with G, k2 and c2r (k3).
   void fft_chain(cudaStream_t st, pgm::Dev<T> &a, int act, bool energy) {
+    plane_fwd(st, a, act);
     for (auto &g : gx)
       with_fft_len(g->K, [&](auto Lc) {
         launch_pdl(pgm::k_fft_x_fwd<T, decltype(Lc)::value>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a, (const int *)g->sys.p,
@@ -561,6 +622,11 @@ struct Engine : EngineBase {
       with_fft_len(g->K, [&](auto Lc) {
         launch_pdl(pgm::k_fft_x_inv<T, decltype(Lc)::value>, g->ntiles, pgm::FFT_THREADS, g->smem, st, a, (const int *)g->sys.p,
                    (const int *)g->tile0.p, g->ng, act);
+      });
+    for (auto &g : gp)
+      with_plane_len(g->K, [&](auto Lc) {
+        launch_pdl(pgm::k_fft_plane_inv<T, decltype(Lc)::value>, g->ntiles, pgm::PLANE_THREADS, g->smem, st, a,
+                   (const int *)g->sys.p, (const int *)g->tile0.p, g->ng, act);
       });
   }
 
@@ -622,7 +688,7 @@ struct Engine : EngineBase {
 
   // Average duration [ms] of one launch of a kernel of the last step, re-run `reps` times on the
   // state that step left (rows, vectors, grids): 0 the CG matvec (rows + PME gather), 1 the spread,
-  // 2 the FFT/convolution chain (five passes), 3 the energy/force pass, 4 the row build.
+  // 2 the FFT/convolution chain, 3 the energy/force pass, 4 the row build.
   bool has_hist() const override { return last_hist != nullptr; }
   double profile(cudaStream_t st, int which, int reps) override {
     pgm::Dev<T> a = dev(nullptr, nullptr, 0, forces_tmp.p, d_status.p);
@@ -640,13 +706,9 @@ struct Engine : EngineBase {
         pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
         pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a);
       }
-      else if (which == 5) {
-        for (auto &g : gx)
-          with_fft_len(g->K, [&](auto Lc) {
-            pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
-          });
-      } else if (which == 6) {
-        pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
+      else if (which == 5 || which == 6) {  // the first FFT pass (plane or k3), after the spread with 6
+        if (which == 6) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
+        plane_fwd(st, a, 0);
         for (auto &g : gx)
           with_fft_len(g->K, [&](auto Lc) {
             pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);

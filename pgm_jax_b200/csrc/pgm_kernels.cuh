@@ -917,6 +917,140 @@ __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const 
   }
 }
 
+// ---- plane passes (meshes with K2 = K3 = L): one CTA per k1 plane runs the k3 and k2 passes in
+// shared memory, in two regions of plane_region(L) complex elements each (the L/2 packed k3-lines
+// of the real plane, or the L/2 + 1 k2-columns padded to L + 1).  The same arithmetic as
+// k_fft_x_fwd followed by k_fft_y(-1), and as k_fft_y(+1) followed by k_fft_x_inv, with one grid
+// round trip and one launch instead of two.
+constexpr int PLANE_THREADS = 512;
+__host__ __device__ constexpr int plane_region(int L) { return (L / 2 + 1) * (L + 1); }
+
+template <typename T, int L>
+__global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane_fwd(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
+  static_assert(L > 0 && L % 8 == 0, "compile-time plane length");
+  pdl_enter();
+  extern __shared__ unsigned char smem_raw[];
+  const int g = group_member(gtile0, ng, blockIdx.x);
+  const int s = gsys[g];
+  if (!pass_active(a, s, act)) return;
+  const SysInfo &S = a.sys[s];
+  constexpr int K = L, Kh = L / 2 + 1, NP = L / 2, LD = L + 1, REG = plane_region(L), Q4 = L / 4;
+  const int k1 = blockIdx.x - gtile0[g];
+  c2<T> *A = reinterpret_cast<c2<T> *>(smem_raw), *B = A + REG, *tws = B + REG;
+  for (int t = threadIdx.x; t < K; t += PLANE_THREADS) tws[t] = a.tw[S.tw[2] + t];  // K2 = K3: one table
+  // rows 2cl and 2cl + 1 of the plane (K x K reals, rows k2) packed as complex line cl, four
+  // columns per thread and load; each thread clears what it read (Q is zero for the next spread)
+  using V = v4<T>;
+  V *Qp = reinterpret_cast<V *>(a.Q + S.rgrid0 + (size_t)k1 * K * K);
+  constexpr int NV = NP * Q4, PER = (NV + PLANE_THREADS - 1) / PLANE_THREADS;
+  V lo[PER], hi[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int t = threadIdx.x + j * PLANE_THREADS;
+    if (t < NV) {
+      const int cl = t / Q4, q = t - cl * Q4;
+      lo[j] = Qp[(2 * cl) * Q4 + q];
+      hi[j] = Qp[(2 * cl + 1) * Q4 + q];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int t = threadIdx.x + j * PLANE_THREADS;
+    if (t < NV) {
+      const int cl = t / Q4, q = t - cl * Q4;
+      c2<T> *d = A + cl * K + 4 * q;
+      d[0].x = lo[j].x; d[0].y = hi[j].x;
+      d[1].x = lo[j].y; d[1].y = hi[j].y;
+      d[2].x = lo[j].z; d[2].y = hi[j].z;
+      d[3].x = lo[j].w; d[3].y = hi[j].w;
+      V z;
+      z.x = T(0); z.y = T(0); z.z = T(0); z.w = T(0);
+      Qp[(2 * cl) * Q4 + q] = z;
+      Qp[(2 * cl + 1) * Q4 + q] = z;
+    }
+  }
+  __syncthreads();
+  c2<T> *res = fft_lines<T, L>(A, B, K, NP, K, S.rad[2], S.nst[2], tws, -1);
+  c2<T> *col = res == A ? B : A;
+  // untangle line cl into rows 2cl, 2cl + 1 (m3 = 0..K/2), stored as k2-columns
+  for (int t = threadIdx.x; t < NP * Kh; t += PLANE_THREADS) {
+    const int cl = t / Kh, m = t - cl * Kh;
+    const c2<T> Z = res[cl * K + m], W = res[cl * K + (m == 0 ? 0 : K - m)];
+    c2<T> X0, X1;
+    X0.x = T(0.5) * (Z.x + W.x); X0.y = T(0.5) * (Z.y - W.y);
+    const T dx = Z.x - W.x, dy = Z.y + W.y;  // (Z - conj W) / (2 i)
+    X1.x = T(0.5) * dy; X1.y = -T(0.5) * dx;
+    col[m * LD + 2 * cl] = X0;
+    col[m * LD + 2 * cl + 1] = X1;
+  }
+  __syncthreads();
+  c2<T> *res2 = fft_lines<T, L>(col, res, K, Kh, LD, S.rad[1], S.nst[1], tws, -1);
+  c2<T> *C = a.C + S.cgrid0 + (size_t)k1 * K * Kh;
+  for (int t = threadIdx.x; t < K * Kh; t += PLANE_THREADS) {
+    const int k2 = t / Kh, m3 = t - k2 * Kh;
+    C[t] = res2[m3 * LD + k2];
+  }
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane_inv(Dev<T> a, const int *gsys, const int *gtile0, int ng, int act) {
+  static_assert(L > 0 && L % 8 == 0, "compile-time plane length");
+  pdl_enter();
+  extern __shared__ unsigned char smem_raw[];
+  const int g = group_member(gtile0, ng, blockIdx.x);
+  const int s = gsys[g];
+  if (!pass_active(a, s, act)) return;
+  const SysInfo &S = a.sys[s];
+  constexpr int K = L, Kh = L / 2 + 1, NP = L / 2, LD = L + 1, REG = plane_region(L), Q4 = L / 4;
+  const int k1 = blockIdx.x - gtile0[g];
+  c2<T> *A = reinterpret_cast<c2<T> *>(smem_raw), *B = A + REG, *tws = B + REG;
+  for (int t = threadIdx.x; t < K; t += PLANE_THREADS) tws[t] = a.tw[S.tw[2] + t];
+  const c2<T> *C = a.C + S.cgrid0 + (size_t)k1 * K * Kh;
+  constexpr int NC = K * Kh, PER = (NC + PLANE_THREADS - 1) / PLANE_THREADS;
+  c2<T> v[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int t = threadIdx.x + j * PLANE_THREADS;
+    if (t < NC) v[j] = C[t];
+  }
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int t = threadIdx.x + j * PLANE_THREADS;
+    if (t < NC) {
+      const int k2 = t / Kh, m3 = t - k2 * Kh;
+      A[m3 * LD + k2] = v[j];
+    }
+  }
+  __syncthreads();
+  c2<T> *res = fft_lines<T, L>(A, B, K, Kh, LD, S.rad[1], S.nst[1], tws, +1);
+  c2<T> *lin = res == A ? B : A;
+  // rows 2cl, 2cl + 1 back into complex line cl (z = a + i b) over the full k3 range (Hermitian)
+  for (int t = threadIdx.x; t < NP * K; t += PLANE_THREADS) {
+    const int cl = t / K, m = t - cl * K;
+    const bool up = m > K / 2;
+    const int mm = up ? K - m : m;
+    c2<T> X0 = res[mm * LD + 2 * cl], X1 = res[mm * LD + 2 * cl + 1];
+    if (mm == 0 || 2 * mm == K) { X0.y = T(0); X1.y = T(0); }
+    if (up) { X0.y = -X0.y; X1.y = -X1.y; }
+    c2<T> Z;
+    Z.x = X0.x - X1.y; Z.y = X0.y + X1.x;
+    lin[cl * K + m] = Z;
+  }
+  __syncthreads();
+  c2<T> *res2 = fft_lines<T, L>(lin, res, K, NP, K, S.rad[2], S.nst[2], tws, +1);
+  using V = v4<T>;
+  V *Pp = reinterpret_cast<V *>(a.Phi + S.rgrid0 + (size_t)k1 * K * K);
+  for (int t = threadIdx.x; t < NP * Q4; t += PLANE_THREADS) {
+    const int cl = t / Q4, q = t - cl * Q4;
+    const c2<T> *z = res2 + cl * K + 4 * q;
+    V r0, r1;
+    r0.x = z[0].x; r0.y = z[1].x; r0.z = z[2].x; r0.w = z[3].x;
+    r1.x = z[0].y; r1.y = z[1].y; r1.z = z[2].y; r1.w = z[3].y;
+    Pp[(2 * cl) * Q4 + q] = r0;
+    Pp[(2 * cl + 1) * Q4 + q] = r1;
+  }
+}
+
 // k1 pass with the convolution: FFT_TILE consecutive columns c = k2 K3h + m3 (contiguous in
 // memory), forward FFT along k1, multiply by 2 G(m) (phi = dE/dQ = 2 K^3 irfft(G F[Q]),
 // pme.py:370-376), inverse FFT.  With ENERGY the reciprocal energy sum w3 G |F|^2
