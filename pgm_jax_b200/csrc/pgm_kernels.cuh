@@ -603,9 +603,11 @@ __device__ __forceinline__ c2<T> cmul(c2<T> a, c2<T> b) {
   return r;
 }
 
-// Radix plan of a length-L transform: radix 4 first, then 2, 3, 5 (constexpr and runtime).
+// Compile-time radix plan of a length-L transform: radix 8 first, then 4, 2, 3, 5 (the runtime
+// plans of the host use 4, 2, 3, 5).
 __host__ __device__ constexpr int fft_nst(int L) {
   int n = 0;
+  while (L % 8 == 0) { L /= 8; ++n; }
   while (L % 4 == 0) { L /= 4; ++n; }
   while (L % 2 == 0) { L /= 2; ++n; }
   while (L % 3 == 0) { L /= 3; ++n; }
@@ -614,6 +616,7 @@ __host__ __device__ constexpr int fft_nst(int L) {
 }
 __host__ __device__ constexpr int fft_radix(int L, int st) {
   int n = 0;
+  while (L % 8 == 0) { if (n == st) return 8; L /= 8; ++n; }
   while (L % 4 == 0) { if (n == st) return 4; L /= 4; ++n; }
   while (L % 2 == 0) { if (n == st) return 2; L /= 2; ++n; }
   while (L % 3 == 0) { if (n == st) return 3; L /= 3; ++n; }
@@ -621,11 +624,27 @@ __host__ __device__ constexpr int fft_radix(int L, int st) {
   return 1;
 }
 
-// R-point DFT in registers, sign -1 forward / +1 inverse.
+// R-point DFT in registers, sign -1 forward / +1 inverse: X_k = sum_n v_n w^(n k), w = exp(sign 2 pi i / R).
 template <typename T, int R>
 __device__ __forceinline__ void butterfly(c2<T> *v, T sg) {
   c2<T> o[R];
-  if constexpr (R == 2) {
+  if constexpr (R == 8) {
+    // two 4-point DFTs of the even and odd points, X_k = E_k + w^k O_k, X_(k+4) = E_k - w^k O_k
+    c2<T> e[4] = {v[0], v[2], v[4], v[6]}, d[4] = {v[1], v[3], v[5], v[7]};
+    butterfly<T, 4>(e, sg);
+    butterfly<T, 4>(d, sg);
+    const T h = T(0.70710678118654752440);
+    c2<T> t[4];
+    t[0] = d[0];
+    t[1].x = h * (d[1].x - sg * d[1].y); t[1].y = h * (d[1].y + sg * d[1].x);
+    t[2].x = -sg * d[2].y; t[2].y = sg * d[2].x;
+    t[3].x = -h * (d[3].x + sg * d[3].y); t[3].y = h * (sg * d[3].x - d[3].y);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      o[k].x = e[k].x + t[k].x; o[k].y = e[k].y + t[k].y;
+      o[k + 4].x = e[k].x - t[k].x; o[k + 4].y = e[k].y - t[k].y;
+    }
+  } else if constexpr (R == 2) {
     o[0].x = v[0].x + v[1].x; o[0].y = v[0].y + v[1].y;
     o[1].x = v[0].x - v[1].x; o[1].y = v[0].y - v[1].y;
   } else if constexpr (R == 4) {

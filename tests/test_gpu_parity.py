@@ -51,6 +51,27 @@ def test_field_of_charges_and_dipoles(box, prec):
     assert np.abs(got0 - ref0).max() <= tol * np.abs(ref0).max()
 
 
+@pytest.mark.parametrize("grid", [(32, 32, 32), (36, 48, 48), (32, 32, 48), (30, 36, 32)])
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_field_through_every_fft_route(box, grid, prec):
+    """The field sweep on meshes that take each route of the reciprocal-space chain: the plane
+    passes (K2 = K3 with a compiled plan: 32^3 and 36 x 48^2), separate k3 and k2 passes with compiled
+    plans (32 x 32 x 48), and the runtime-length passes (30 x 36 x 32), against the oracle.  The
+    oracle transforms the full spectrum, the engine (as pme.py:370-376) the rfft half: on this
+    triclinic box the influence function is not mirror-symmetric on the Nyquist planes, which
+    separates the two by up to ~2e-10 of the field on the coarse 30 x 36 x 32 mesh (white-noise
+    grids: 7e-12), hence 1e-9 for FP64 here."""
+    s, pos, H, _, _ = box
+    st = dict(SMALL_BOX_SETTINGS, pme_grid=grid)
+    o = O.Oracle(s, st)
+    rng = np.random.default_rng(5)
+    d = rng.normal(scale=0.01, size=(s.n, 3))
+    ref = o.field(pos, H, s.q, d)
+    got = ff_for(s, H, prec, pme_grid=grid).field(pos, H, d, charges=True).cpu().numpy()
+    tol = 1e-9 if prec == "double" else 2e-6
+    assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), np.abs(got - ref).max() / np.abs(ref).max()
+
+
 def test_compute_double_matches_golden(box, golden_small_box):
     """FP64 engine: ff_small_box energies, forces, dipoles, iterations, virial (reference golden)."""
     s, pos, H, o, r = box
