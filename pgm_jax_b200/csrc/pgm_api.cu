@@ -193,7 +193,7 @@ struct Engine : EngineBase {
   const double *last_hist = nullptr;  // the history of the last predictor solve (profiling)
   DBuf<float4> nn_bl;  // the graph's permanent field of the last solve (for the change channel)
   DBuf<int> nn_valid;  // nn_bl holds a previous step
-  DBuf<uint16_t> nn_es;  // the graph's row slots per atom (learned guess)
+  DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by the row build)
   DBuf<int> nn_ne;
   static constexpr int NN_EMAX = 128;
   float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
@@ -254,7 +254,7 @@ struct Engine : EngineBase {
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
     a.max_count = dmax.p;
     a.mce = mce; a.rnv = split ? rnv.p : nullptr; a.rce2 = rc_e * rc_e;
-    a.nn_es = nn_es.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
+    a.nn_e4 = nn_e4.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
     a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p; a.F = Fv.p;
     a.Q = Q.p; a.Phi = Phi.p; a.Ginf = Ginf.p; a.C = C.p; a.tw = tw.p; a.bmod = bmod.p;
     a.forces = forces; a.dEdd = dEdd.p;
@@ -516,7 +516,7 @@ struct Engine : EngineBase {
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
     nn_w.alloc(pgmnn::NN_NPARAM); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
     nn_mu.alloc((size_t)nt * 3); nn_chan.alloc((size_t)nt * pgm::NN_CHAN); nn_bl.alloc(nt); nn_valid.alloc(1);
-    if (set.predictor == 5) { nn_es.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
+    if (set.predictor == 5) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
     CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
     CK(cudaMallocHost(&h_any, sizeof(int)));
     CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));

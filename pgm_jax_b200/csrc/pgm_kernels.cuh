@@ -64,9 +64,10 @@ struct Dev {
   int mce;
   int *rnv;
   double rce2;
-  // the learned guess's graph (row entries with r^2 < nn_rg2): row slots [atom][nn_emax] and
-  // counts, written by the row build when nn_es is set (a count above nn_emax: scan the row)
-  uint16_t *nn_es;
+  // the learned guess's graph (the row entries with float(r^2) < nn_rg2): per atom up to nn_emax
+  // edges (x, y, z, partner bits) in row order and the count, written by the row build when
+  // nn_e4 is set (a count above nn_emax: the consumers scan the row)
+  float4 *nn_e4;
   int *nn_ne;
   int nn_emax;
   float nn_rg2;
@@ -376,17 +377,17 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
     }
     vcount += __popc(bv);
   }
-  if (a.nn_es) {  // graph edges of the learned guess: the slots of the short entries
-    bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
-    unsigned eb = __ballot_sync(0xffffffffu, sh);
-    int at = ecount + __popc(eb & lt);
-    if (sh && at < a.nn_emax) a.nn_es[(size_t)i * a.nn_emax + at] = (uint16_t)slot;
+  if (a.nn_e4) {  // the learned guess's graph edges: the short entries, with their displacement
+    const bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
+    const unsigned eb = __ballot_sync(0xffffffffu, sh);
+    const int at = ecount + __popc(eb & lt);
+    if (sh && at < a.nn_emax) a.nn_e4[(size_t)i * a.nn_emax + at] = make_float4(float(x), float(y), float(z), __int_as_float(j));
     ecount += __popc(eb);
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
+__global__ void __launch_bounds__(256, 5) k_rows(Dev<T> a) {
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int blk = blockIdx.x;
   int s = a.wb_sys[blk];
@@ -454,7 +455,7 @@ __global__ void __launch_bounds__(256) k_rows(Dev<T> a) {
   if (lane == 0) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
-    if (a.nn_es) a.nn_ne[i] = ecount;
+    if (a.nn_e4) a.nn_ne[i] = ecount;
     if (count > a.mce) atomicOr(&a.status[s], 0x1u);
     atomicMax(a.max_count, count);
     if (a.rnv) {
@@ -1374,67 +1375,27 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
 // c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
 // NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
 constexpr int NN_CHAN = 12;
-constexpr int NN_EBUF = 64;  // per-warp staging of compacted graph edges (two rounds of 32)
-
-// Scans atom i's pair row 32 entries at a time (16-byte vector loads in FP32) and hands every edge
-// with r < rg to `edge(k, x, y, z, o)` with all lanes busy: the passing entries of a round are
-// compacted (ballot + prefix) into the warp's shared buffer and consumed 32 at a time, so the
-// per-edge work runs on full warps although only a fifth of the row is inside the graph cutoff.
+// The graph edges of atom i: from the list the row build wrote, one edge per lane and round, or,
+// when the list overflowed (or there is none), by a scan of the row (each edge on the lane that
+// reads it).
 template <typename T, typename F>
-__device__ __forceinline__ void graph_edges(const Dev<T> &a, int i, float rg, float4 *buf, int *bo, F &&edge) {
+__device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, F &&edge) {
   const int lane = threadIdx.x & 31;
-  const int n = min(a.rn[i], a.mce);
-  const size_t base = (size_t)i * a.mc;
-  const float rg2 = rg * rg;
-  int cnt = 0;
-  auto flush = [&](int m) {  // consume buf[0, m) (m <= 32), one edge per lane
-    __syncwarp();
-    if (lane < m) {
-      float4 e = buf[lane];
-      edge(__float_as_int(e.w), e.x, e.y, e.z, bo[lane]);
-    }
-    __syncwarp();
-  };
-  for (int t0 = 0; t0 < n; t0 += 32) {
-    const int t = t0 + lane;
-    float x = 0.f, y = 0.f, z = 0.f;
-    int k = 0;
-    bool pass = false;
-    if (t < n) {
-      size_t o = base + t;
-      x = float(a.rx[o]); y = float(a.ry[o]); z = float(a.rz[o]);
-      pass = x * x + y * y + z * z < rg2;
-      if (pass) k = a.rk[o];
-    }
-    unsigned m = __ballot_sync(0xffffffffu, pass);
-    int at = cnt + __popc(m & ((1u << lane) - 1u));
-    if (pass) { buf[at] = make_float4(x, y, z, __int_as_float(k)); bo[at] = t; }
-    cnt += __popc(m);
-    if (cnt >= 32) {
-      flush(32);
-      if (lane < cnt - 32) { buf[lane] = buf[32 + lane]; bo[lane] = bo[32 + lane]; }
-      __syncwarp();  // the moved entries are read before the next round writes past them
-      cnt -= 32;
-    }
-  }
-  if (cnt > 0) flush(cnt);
-}
-
-// The graph edges of atom i: the row build's slot list when it holds them all, else the scan.
-template <typename T, typename F>
-__device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, float rg, float4 *buf, int *bo, F &&edge) {
-  const int ne = a.nn_es ? a.nn_ne[i] : a.nn_emax + 1;
+  const int ne = a.nn_e4 ? a.nn_ne[i] : a.nn_emax + 1;
   if (ne > a.nn_emax) {
-    graph_edges(a, i, rg, buf, bo, edge);
+    const int n = min(a.rn[i], a.mce);
+    const size_t base = (size_t)i * a.mc;
+    for (int t = lane; t < n; t += 32) {
+      const size_t o = base + t;
+      const double x = a.rx[o], y = a.ry[o], z = a.rz[o];
+      if (float(x * x + y * y + z * z) < a.nn_rg2) edge(a.rk[o], float(x), float(y), float(z), t);
+    }
     return;
   }
-  const int lane = threadIdx.x & 31;
-  const size_t base = (size_t)i * a.mc;
-  const uint16_t *es = a.nn_es + (size_t)i * a.nn_emax;
+  const float4 *list = a.nn_e4 + (size_t)i * a.nn_emax;
   for (int e = lane; e < ne; e += 32) {
-    const int t = es[e];
-    const size_t o = base + t;
-    edge(a.rk[o], float(a.rx[o]), float(a.ry[o]), float(a.rz[o]), t);
+    const float4 v = list[e];
+    edge(__float_as_int(v.w), v.x, v.y, v.z, e);
   }
 }
 
@@ -1447,17 +1408,15 @@ __device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, float rg
 template <typename T>
 __global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, const float4 *bl_prev, const int *valid,
                                                  float rg, float4 *bl_out, float *chan) {
-  __shared__ float4 ebuf[WARPS_PER_BLOCK][NN_EBUF];
-  __shared__ int eoff[WARPS_PER_BLOCK][NN_EBUF];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
   if (i >= S.atom0 + S.natom) return;
+  (void)rg;  // the graph radius is a.nn_rg2 here
   float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-  const size_t base = (size_t)i * a.mc;
   const float Ri = float(a.radius[i]), beta = float(a.beta);
-  for_graph_edges(a, i, rg, ebuf[warp], eoff[warp], [&](int k, float x, float y, float z, int) {
+  for_graph_edges(a, i, [&](int k, float x, float y, float z, int) {
     // the pair kernels G1, G2 of the edge, evaluated here (not read from the rows) so that this
     // pass can run beside the row-kernel evaluation
     const float Rk = float(a.radius[k]), r = sqrtf(x * x + y * y + z * z);
@@ -1526,12 +1485,11 @@ __device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
 // plain (q = 0: A) and projected (q = 1: D) sums of channel c with radial basis k; returns on lane l
 // the total of value l (l < 32) and in tail[0..3] the totals of values 32..35.
 template <typename T>
-__device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const float *chan, float rg, float4 *ebuf, int *eoff,
-                                              float (&tail)[4]) {
+__device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const float *chan, float rg, float (&tail)[4]) {
   float acc[36];
 #pragma unroll
   for (int o = 0; o < 36; ++o) acc[o] = 0.f;
-  for_graph_edges(a, i, rg, ebuf, eoff, [&](int j, float x, float y, float z, int) {
+  for_graph_edges(a, i, [&](int j, float x, float y, float z, int) {
     float r = sqrtf(x * x + y * y + z * z);
     float ir = 1.f / r, u[3] = {x * ir, y * ir, z * ir};
     float fc = 0.5f * (cospif(r / rg) + 1.f);
@@ -1565,8 +1523,6 @@ __device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const floa
 template <typename T>
 __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan, float sigma, float rg, float *inv, float *vec,
                                                      int *valid) {
-  __shared__ float4 ebuf[WARPS_PER_BLOCK][NN_EBUF];
-  __shared__ int eoff[WARPS_PER_BLOCK][NN_EBUF];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (valid && blockIdx.x == 0 && threadIdx.x == 0) *valid = 1;  // read by the previous kernel only
   int s = a.wb_sys[blockIdx.x];
@@ -1578,7 +1534,7 @@ __global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan
   const float is = 1.f / sigma, is2 = is * is;
   float tail[4];
   // lane l holds value l; the norms of the first eight (c, k) groups of three for the invariants
-  float mine = nn_aggregate(a, i, chan, rg, ebuf[warp], eoff[warp], tail);
+  float mine = nn_aggregate(a, i, chan, rg, tail);
   V[9 + lane] = mine;
   if (lane < 4) V[9 + 32 + lane] = tail[lane];
   float sq = mine * mine;
