@@ -817,23 +817,22 @@ struct Engine : EngineBase {
   }
 
   void prepare(cudaStream_t st, pgm::Dev<T> &a, const double *boxes, const double *nn_hist = nullptr) {
-    CK(cudaMemsetAsync(dmax.p, 0, 2 * sizeof(int), st));
-    pgm::k_box<T><<<grid1(nsys, 64), 64, 0, st>>>(a, boxes); check_launch();
-    pgm::k_prep<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
-    pgm::k_mol<T><<<grid1(nmol_total), 256, 0, st>>>(a); check_launch();
+    launch_pdl(pgm::k_box<T>, grid1(nsys, 64), 64, 0, st, a, boxes);
+    launch_pdl(pgm::k_prep<T>, grid1(nt), 256, 0, st, a);
+    launch_pdl(pgm::k_mol<T>, grid1(nmol_total), 256, 0, st, a);
     if (!a.idx) {  // the Verlet candidate list, rebuilt on the device when the flag is up
-      pgm::k_cell_assign<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
-      pgm::k_scan_cells<<<1, 1024, 0, st>>>(cell_count.p, cell_start.p, ncell, nb_flag.p); check_launch();
-      pgm::k_scatter<T><<<grid1(nt), 256, 0, st>>>(a); check_launch();
-      pgm::k_cand<T><<<nwblk, 256, 0, st>>>(a); check_launch();
-      pgm::k_nb_finish<<<std::max(1, std::min(1024, grid1(ncell))), 256, 0, st>>>(cell_count.p, ncell, nb_flag.p, nb_builds.p);
-      check_launch();
-      pgm::k_nb_lower<<<1, 1, 0, st>>>(nb_flag.p, nb_builds.p); check_launch();
+      launch_pdl(pgm::k_cell_assign<T>, grid1(nt), 256, 0, st, a);
+      launch_pdl(pgm::k_scan_cells, 1, 1024, 0, st, (const int *)cell_count.p, cell_start.p, ncell, (const int *)nb_flag.p);
+      launch_pdl(pgm::k_scatter<T>, grid1(nt), 256, 0, st, a);
+      launch_pdl(pgm::k_cand<T>, nwblk, 256, 0, st, a);
+      launch_pdl(pgm::k_nb_finish, std::max(1, std::min(1024, grid1(ncell))), 256, 0, st, cell_count.p, ncell, nb_flag.p,
+                 nb_builds.p);
+      launch_pdl(pgm::k_nb_lower, 1, 1, 0, st, nb_flag.p, nb_builds.p);
     }
-    pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a); check_launch();
+    launch_pdl(pgm::k_rows<T>, nwblk, 256, 0, st, a);
     if (nn_hist) nn_fork(st, a, nn_hist);
-    pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a); check_launch();
-    pgm::k_influence<T><<<std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st>>>(a, cgrid); check_launch();
+    launch_pdl(pgm::k_row_kernels<T>, (int)(((size_t)nt * mc + 255) / 256), 256, 0, st, a);
+    launch_pdl(pgm::k_influence<T>, (int)std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st, a, (long long)cgrid);
   }
 
   void set_list_capacity(int c) override {
@@ -857,7 +856,7 @@ struct Engine : EngineBase {
   template <bool WITH_Q, bool UPDATE_P, int ACT, bool ENERGY>
   void pme(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin) {
     // Q is zero here: cleared at creation and, after every spread, by the forward k2 FFT pass
-    pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
+    launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
     fft_chain(st, a, ACT, ENERGY);
   }
 
@@ -880,7 +879,7 @@ struct Engine : EngineBase {
     // the loop body is captured as a sequence of its own: it forks to its own stream
     cudaStream_t ax = in_body ? aux_b : aux;
     cudaEvent_t ef = in_body ? ev_fork_b : ev_fork, ej = in_body ? ev_join_b : ev_join;
-    pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
+    launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
     CK(cudaEventRecord(ef, st));
     CK(cudaStreamWaitEvent(ax, ef, 0));
     pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, ax>>>(a, vin, Fv.p); check_launch();
@@ -963,10 +962,8 @@ struct Engine : EngineBase {
       CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
       CK(cudaGraphConditionalHandleCreate(&cond2, g, 0, cudaGraphCondAssignDefault));
     }
-    pgm::k_cg_setup<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, mode == 0 ? ind->count : nullptr, ind->norm,
-                                                    mode == 0 ? K : 0, set.fused, std::max(1, set.norm_refresh), mode, cond2,
-                                                    captured ? 1 : 0);
-    check_launch();
+    launch_pdl(pgm::k_cg_setup, grid1(nsys, 64), 64, 0, st, d_cg.p, nsys, mode == 0 ? (const int32_t *)ind->count : nullptr,
+               (const double *)ind->norm, mode == 0 ? K : 0, set.fused, std::max(1, set.norm_refresh), mode, cond2, captured ? 1 : 0);
     if (mode == 1) {
       // x0 = ind->mu with the plain start: X = mu, have = 1
       pgm::k_energy_start<T><<<grid1(nt), 256, 0, st>>>(a, ind->mu);
@@ -982,15 +979,15 @@ struct Engine : EngineBase {
       check_launch();
     }
     sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
-    pgm::k_start2<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+    launch_pdl(pgm::k_start2<T>, ntblk, 256, 0, st, a);
     auto plain_start = [&](cudaStream_t s2) {
       sweep<false, false, 2, 1>(s2, a, X.p, AP.p);
-      pgm::k_start3<T><<<grid1(nt), 256, 0, s2>>>(a); check_launch();
+      launch_pdl(pgm::k_start3<T>, grid1(nt), 256, 0, s2, a);
     };
     if (captured) conditional_node(st, cond2, cudaGraphCondTypeIf, plain_start);
     else plain_start(st);
     pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
-    pgm::k_cg_begin<<<1, 256, 0, st>>>(d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p); check_launch();
+    launch_pdl(pgm::k_cg_begin, 1, 256, 0, st, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p);
     if (captured) {
       // captured: the first U iterations as plain kernel nodes (their kernels skip systems that
       // have converged; U = the iterations of the last host-driven solve - 2), then a conditional
@@ -1021,22 +1018,20 @@ struct Engine : EngineBase {
       }
       last_iters = it;
     }
-    pgm::k_cg_finish<T><<<grid1(nt), 256, 0, st>>>(a, mu_out, mode == 0 ? ind->hist : nullptr, mode == 0); check_launch();
-    pgm::k_cg_state_out<<<grid1(nsys, 64), 64, 0, st>>>(d_cg.p, nsys, ind->count, ind->norm, iters, resid, a.status, mode == 0,
-                                                        set.dipole_tol);
-    check_launch();
+    launch_pdl(pgm::k_cg_finish<T>, grid1(nt), 256, 0, st, a, mu_out, mode == 0 ? ind->hist : nullptr, mode == 0 ? 1 : 0);
+    launch_pdl(pgm::k_cg_state_out, grid1(nsys, 64), 64, 0, st, (const pgm::CGSys *)d_cg.p, nsys, ind->count, ind->norm, iters,
+               resid, a.status, mode == 0 ? 1 : 0, set.dipole_tol);
   }
 
   // Energies, forces and virial at fixed mu (forcefield.py:2362-2430).
   void energy_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, double *energy, double *virial) {
-    CK(cudaMemsetAsync(d_eacc.p, 0, sizeof(pgm::EnergyAcc) * nsys, st));
-    pgm::k_total_dipoles<T><<<grid1(nt), 256, 0, st>>>(a, mu); check_launch();
+    launch_pdl(pgm::k_total_dipoles<T>, grid1(nt), 256, 0, st, a, mu);
     pme<true, false, 0, true>(st, a, D.p);
-    pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, mu); check_launch();
-    if (ncov) { pgm::k_cov_forces<T><<<grid1(ncov), 256, 0, st>>>(a); check_launch(); }
-    pgm::k_energy_finish<<<grid1(nsys, 64), 64, 0, st>>>(d_sys.p, d_box.p, d_eacc.p, nsys, set.ewald_beta, a.c_self, set.cutoff,
-                                                         set.vdw == 1, set.lj_lrc, a.induce, energy, virial, a.status);
-    check_launch();
+    launch_pdl(pgm::k_forces<T, P>, nwblk, 256, 0, st, a, mu);
+    if (ncov) launch_pdl(pgm::k_cov_forces<T>, grid1(ncov), 256, 0, st, a);
+    launch_pdl(pgm::k_energy_finish, grid1(nsys, 64), 64, 0, st, (const pgm::SysInfo *)d_sys.p, (const pgm::BoxInfo *)d_box.p,
+               (const pgm::EnergyAcc *)d_eacc.p, nsys, set.ewald_beta, a.c_self, set.cutoff, set.vdw == 1, set.lj_lrc, a.induce, energy,
+               virial, a.status);
   }
 
   void compute(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width, PgmInduction *ind,
@@ -1044,8 +1039,7 @@ struct Engine : EngineBase {
     launches = 0;
     unsigned *status = out->status ? out->status : d_status.p;
     double *forces = out->forces ? out->forces : forces_tmp.p;
-    CK(cudaMemsetAsync(status, 0, sizeof(unsigned) * nsys, st));
-    pgm::Dev<T> a = dev(pos, idx, idx_width, forces, status);
+    pgm::Dev<T> a = dev(pos, idx, idx_width, forces, status);  // k_box zeroes the status words
     last_pos = pos;
     nn_forked = false;
     prepare(st, a, box, a.induce && set.predictor == 5 && nn_on ? ind->hist : nullptr);

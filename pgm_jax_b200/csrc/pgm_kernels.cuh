@@ -87,7 +87,9 @@ struct Dev {
 // ------------------------------------------------------------------ box and per-atom set-up
 template <typename T>
 __global__ void k_box(Dev<T> a, const double *boxes) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) { a.max_count[0] = 0; a.max_count[1] = 0; }  // the step's largest row counts start here
   if (s >= a.nsys) return;
   const double *H = boxes + 9 * s;
   BoxInfo &B = a.box[s];
@@ -117,13 +119,14 @@ __global__ void k_box(Dev<T> a, const double *boxes) {
   double mc = 0.5 * fmin(H[0], fmin(H[4], H[8]));
   if (a.cutoff > mc) bad = 1;
   B.bad = bad;
-  if (bad) atomicOr(&a.status[s], 0x8u);
+  a.status[s] = bad ? 0x8u : 0u;  // the step's status word starts here
 }
 
 // Fractional coordinates, spline base and offset (pme.py:269-304), permanent dipoles
 // (forcefield.py:1032-1042) and the cell of every atom.
 template <typename T>
 __global__ void k_prep(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   int s = a.sysid[i];
@@ -179,6 +182,7 @@ __global__ void k_prep(Dev<T> a) {
 // Cell of every atom (only when the candidate list is rebuilt).
 template <typename T>
 __global__ void k_cell_assign(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   if (!*a.nb_flag) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
@@ -205,6 +209,7 @@ __global__ void k_cell_assign(Dev<T> a) {
 // atom), for the molecular virial.
 template <typename T>
 __global__ void k_mol(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= a.nmol) return;
   int i0 = a.mol_start[m], i1 = a.mol_start[m + 1];
@@ -225,6 +230,7 @@ __global__ void k_mol(Dev<T> a) {
 
 // Exclusive scan of the cell counts of all systems (one block).
 __global__ void k_scan_cells(const int *count, int *start, int n, const int *flag) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   if (!*flag) return;
   __shared__ int part[1024];
   __shared__ int carry;
@@ -251,6 +257,7 @@ __global__ void k_scan_cells(const int *count, int *start, int n, const int *fla
 
 template <typename T>
 __global__ void k_scatter(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   if (!*a.nb_flag) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
@@ -266,6 +273,7 @@ __global__ void k_scatter(Dev<T> a) {
 // md/neighbors.py:169-304, rebuilt when an atom moved more than skin / 2).
 template <typename T>
 __global__ void __launch_bounds__(256) k_cand(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   if (!*a.nb_flag) return;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
@@ -335,10 +343,12 @@ __global__ void __launch_bounds__(256) k_cand(Dev<T> a) {
 
 // End of a rebuild: clear the cell counts for the next one, count it, lower the flag.
 __global__ void k_nb_finish(int *cell_count, int ncell, int *flag, long long *builds) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   if (!*flag) return;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) cell_count[c] = 0;
 }
 __global__ void k_nb_lower(int *flag, long long *builds) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   if (*flag) { *flag = 0; *builds += 1; }
 }
 
@@ -388,6 +398,7 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
 
 template <typename T>
 __global__ void __launch_bounds__(256, 5) k_rows(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int blk = blockIdx.x;
   int s = a.wb_sys[blk];
@@ -468,6 +479,7 @@ __global__ void __launch_bounds__(256, 5) k_rows(Dev<T> a) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_row_kernels(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   int i = (int)(t / a.mc), slot = (int)(t - (size_t)i * a.mc);
   if (i >= a.nt || slot >= min(a.rn[i], a.mce)) return;
@@ -488,6 +500,7 @@ __global__ void __launch_bounds__(256) k_row_kernels(Dev<T> a) {
 // on the half spectrum, computed in FP64, stored in T; recomputed only when the box changed.
 template <typename T>
 __global__ void k_influence(Dev<T> a, long long total) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
     int s = 0;
     while (s + 1 < a.nsys && a.sys[s + 1].cgrid0 <= g) ++s;
@@ -1604,6 +1617,7 @@ __global__ void k_start1(Dev<T> a, const double *hist, int K, double c0, double 
 // mean|alpha b| and, without history, x0 = alpha b (forcefield.py:1960-1997).
 template <typename T>
 __global__ void k_start2(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   __shared__ double red[THREADS_PER_BLOCK / 32];
   int s = a.tb_sys[blockIdx.x];
   int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
@@ -1640,6 +1654,7 @@ __global__ void k_start2(Dev<T> a) {
 // Start, step 3 (plain start only): r0 = b - A x0.
 template <typename T>
 __global__ void k_start3(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   int s = a.sysid[i];
@@ -1685,6 +1700,7 @@ __global__ void k_cg_init(Dev<T> a) {
 
 // Per-system scalars after the start: norm, r.z, err, active; *any = some system iterates.
 __global__ void k_cg_begin(CGSys *cg, int nsys, double tol, int max_iter, int *any) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   __shared__ int act;
   if (threadIdx.x == 0) act = 0;
   __syncthreads();
@@ -1811,6 +1827,7 @@ __global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *a
 // in FP64, the history push (forcefield.py:2005-2007) and mu + p for the energy pass.
 template <typename T>
 __global__ void k_cg_finish(Dev<T> a, double *mu, double *hist, int push) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   v4<T> x = a.X[i], r = a.R[i];
@@ -1833,6 +1850,7 @@ __global__ void k_cg_finish(Dev<T> a, double *mu, double *hist, int push) {
 
 __global__ void k_cg_state_out(const CGSys *cg, int nsys, int32_t *count, double *norm, int32_t *iters, double *resid,
                                unsigned *status, int push, double tol) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   const CGSys &G = cg[s];
@@ -1847,6 +1865,7 @@ __global__ void k_cg_state_out(const CGSys *cg, int nsys, int32_t *count, double
 // forcefield.py:2606-2612).
 __global__ void k_cg_setup(CGSys *cg, int nsys, const int32_t *count, const double *norm, int K, int fused, int refresh,
                            int mode, cudaGraphConditionalHandle plain, int use_cond) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   CGSys &G = cg[s];
@@ -1863,6 +1882,7 @@ __global__ void k_cg_setup(CGSys *cg, int nsys, const int32_t *count, const doub
 // Energy-only start: x0 = the state's mu, first sweep at d = p.
 template <typename T>
 __global__ void k_energy_start(Dev<T> a, const double *mu) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   double4 p = a.pperm[i];
@@ -1880,6 +1900,7 @@ __global__ void k_energy_start(Dev<T> a, const double *mu) {
 // spline derivatives (the autodiff of pme.py:390-411 written out).
 template <typename T, int P>
 __global__ void __launch_bounds__(256, 3) k_forces(Dev<T> a, const double *mu) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   __shared__ T sh[WARPS_PER_BLOCK][3][3][P];
   __shared__ double red[WARPS_PER_BLOCK][16];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -2063,6 +2084,7 @@ __global__ void __launch_bounds__(256, 3) k_forces(Dev<T> a, const double *mu) {
 // (the vector-Jacobian product of forcefield.py:2412).  One thread per covalent dipole.
 template <typename T>
 __global__ void k_cov_forces(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= a.ncov || !a.perm) return;
   int i = a.cov_i_flat[m], j = a.cov_j_flat[m];
@@ -2083,6 +2105,7 @@ __global__ void k_cov_forces(Dev<T> a) {
 // E_elec = KE [rows/2 + U_rec + U_self + U_bg + U_pol], E_vdw = rows/2 + tail.
 __global__ void k_energy_finish(const SysInfo *sys, const BoxInfo *box, const EnergyAcc *E, int nsys, double beta, double c_self,
                                 double cutoff, int lj, int lj_lrc, int induce, double *energy, double *virial, unsigned *status) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   const EnergyAcc &e = E[s];
@@ -2115,7 +2138,11 @@ __global__ void k_energy_finish(const SysInfo *sys, const BoxInfo *box, const En
 // d = p + mu (energy pass), in T.
 template <typename T>
 __global__ void k_total_dipoles(Dev<T> a, const double *mu) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // the energy accumulators of the pass start at zero
+  constexpr int NACC = sizeof(EnergyAcc) / sizeof(double);
+  for (int t = i; t < NACC * a.nsys; t += gridDim.x * blockDim.x) reinterpret_cast<double *>(a.eacc)[t] = 0.0;
   if (i >= a.nt) return;
   double4 p = a.pperm[i];
   double m0 = mu ? mu[3 * i] : 0.0, m1 = mu ? mu[3 * i + 1] : 0.0, m2 = mu ? mu[3 * i + 2] : 0.0;
@@ -2127,6 +2154,7 @@ __global__ void k_total_dipoles(Dev<T> a, const double *mu) {
 // Copy of a (N, 3) FP64 array into v4<T> (pgm_field input).
 template <typename T>
 __global__ void k_load_vec(Dev<T> a, const double *v, v4<T> *out) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   v4<T> d;
@@ -2136,6 +2164,7 @@ __global__ void k_load_vec(Dev<T> a, const double *v, v4<T> *out) {
 
 template <typename T>
 __global__ void k_store_vec(Dev<T> a, const v4<T> *in, double *v) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   v4<T> d = in[i];

@@ -108,6 +108,7 @@ __device__ __forceinline__ void half_kick(const MDDev &d, int m, double dt, cons
 __global__ void k_md_begin(MDDev d, double dt, double gamma, const double *kT, unsigned long long seed,
                            const unsigned long long *counter, const double *F, double *X, double *Q, double *P, double *L,
                            double *pos, const double *box) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent: the forces are complete
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= d.nmol) return;
   unsigned long long step = *counter;
@@ -153,6 +154,7 @@ __global__ void k_md_begin(MDDev d, double dt, double gamma, const double *kT, u
 
 __global__ void k_md_end(MDDev d, double dt, const double *F, const double *Q, double *P, double *L,
                          unsigned long long *counter) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent: the forces are complete
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0) *counter += 1;  // the Langevin noise counter of the next step
   if (m >= d.nmol) return;
@@ -207,6 +209,22 @@ struct PgmRigid {
       return PGM_ERR_CUDA;                                          \
     }                                                               \
   } while (0)
+
+// A launch with programmatic stream serialization: the kernel may be scheduled while its
+// predecessor drains and waits (griddepcontrol.wait) for its completion before touching data.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_dependent(void (*k)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
 
 extern "C" {
 
@@ -266,17 +284,16 @@ PgmStatus pgm_rigid_begin_step(PgmRigid *r, void *stream, double dt, double gamm
                                const double *forces, double *com, double *quat, double *mom, double *angmom, double *pos,
                                const double *box) {
   if (!r || !com || !quat || !mom || !angmom || !pos || !box || (gamma > 0 && !kT)) return PGM_ERR_INVALID;
-  k_md_begin<<<(r->nmol + 127) / 128, 128, 0, (cudaStream_t)stream>>>(r->dev(), dt, gamma, kT, seed, r->counter, forces, com,
-                                                                     quat, mom, angmom, pos, box);
-  MDCK(cudaGetLastError());
+  MDCK(launch_dependent(k_md_begin, (r->nmol + 127) / 128, 128, (cudaStream_t)stream, r->dev(), dt, gamma, kT, seed,
+                        (const unsigned long long *)r->counter, forces, com, quat, mom, angmom, pos, box));
   return PGM_OK;
 }
 
 PgmStatus pgm_rigid_end_step(PgmRigid *r, void *stream, double dt, const double *forces, const double *quat, double *mom,
                              double *angmom) {
   if (!r || !forces || !quat || !mom || !angmom) return PGM_ERR_INVALID;
-  k_md_end<<<(r->nmol + 127) / 128, 128, 0, (cudaStream_t)stream>>>(r->dev(), dt, forces, quat, mom, angmom, r->counter);
-  MDCK(cudaGetLastError());
+  MDCK(launch_dependent(k_md_end, (r->nmol + 127) / 128, 128, (cudaStream_t)stream, r->dev(), dt, forces, quat, mom, angmom,
+                        r->counter));
   return PGM_OK;
 }
 
