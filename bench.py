@@ -285,6 +285,14 @@ def run_engine(args) -> None:
     # end to end: the force call through the C ABI with host buffers (positions in, forces out and
     # the induction state in and out every step), the integrator on the GPU
     e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
+    # three MD steps launched directly (the CG loop driven from the host), untimed, in their own
+    # NVTX range: a profiler cannot see the kernels of graphs with conditional nodes
+    with torch.cuda.stream(md.stream):
+        torch.cuda.nvtx.range_push("direct_md")
+        for _ in range(3):
+            md.step()
+        md.stream.synchronize()
+        torch.cuda.nvtx.range_pop()
     acc = accuracy_vs_fp64(s, H, md, torch)
     # plain CG on the same workload: from the previous step's dipoles and from mu4
     plain = {p: run_plain(s, pos, H, rank, p, args, torch) for p in (("mu1", "mu4") if args.nn else ())}
@@ -440,7 +448,7 @@ def run_e2e(md, ff, steps, torch, lib, _lib) -> dict:
             one()
         md.stream.synchronize()
         builds0 = int(lib.pgm_list_rebuilds(ff._h))
-        torch.cuda.nvtx.range_push("e2e_md")  # direct launches: a profiler's launch list can use this range
+        torch.cuda.nvtx.range_push("e2e_md")
         t0 = time.perf_counter()
         for _ in range(steps):
             one()
