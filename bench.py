@@ -284,7 +284,6 @@ def run_engine(args) -> None:
     step_bytes = bytes_per_step(ff.n, pairs, n_it, GRID)
     # end to end: the force call through the C ABI with host buffers (positions in, forces out and
     # the induction state in and out every step), the integrator on the GPU
-    e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
     # three MD steps launched directly (the CG loop driven from the host), untimed, in their own
     # NVTX range: a profiler cannot see the kernels of graphs with conditional nodes
     with torch.cuda.stream(md.stream):
@@ -293,6 +292,7 @@ def run_engine(args) -> None:
             md.step()
         md.stream.synchronize()
         torch.cuda.nvtx.range_pop()
+    e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
     acc = accuracy_vs_fp64(s, H, md, torch)
     # plain CG on the same workload: from the previous step's dipoles and from mu4
     plain = {p: run_plain(s, pos, H, rank, p, args, torch) for p in (("mu1", "mu4") if args.nn else ())}
