@@ -886,7 +886,8 @@ struct Engine : EngineBase {
     CK(cudaEventRecord(ej, ax));
     fft_chain(st, a, ACT, false);
     CK(cudaStreamWaitEvent(st, ej, 0));
-    pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false><<<nwblk, 256, 0, st>>>(a, vin, out); check_launch();
+    // a programmatic dependent of the last FFT pass; griddepcontrol.wait also covers the joined row field
+    launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false>, nwblk, 256, 0, st, a, vin, out);
   }
 
   // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check.
@@ -975,8 +976,8 @@ struct Engine : EngineBase {
         CK(cudaStreamWaitEvent(st, ev_nn_join, 0));  // the prediction, computed beside the row kernels
         nn_forked = false;
       }
-      pgm::k_start1<T><<<grid1(nt), 256, 0, st>>>(a, ind->hist, K, cc[0], cc[1], cc[2], cc[3], use_nn ? nn_mu.p : nullptr);
-      check_launch();
+      launch_pdl(pgm::k_start1<T>, grid1(nt), 256, 0, st, a, (const double *)ind->hist, K, cc[0], cc[1], cc[2], cc[3],
+                 use_nn ? (const float *)nn_mu.p : nullptr);
     }
     sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
     launch_pdl(pgm::k_start2<T>, ntblk, 256, 0, st, a);

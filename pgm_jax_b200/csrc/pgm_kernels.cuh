@@ -1591,6 +1591,7 @@ __global__ void k_vec_from_f64(int n, const double *src, v4<T> *dst) {
 // 1956-1958) and the dipoles of the first field sweep: p + x0h (fused start) or p (plain).
 template <typename T>
 __global__ void k_start1(Dev<T> a, const double *hist, int K, double c0, double c1, double c2, double c3, const float *xnn) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   int s = a.sysid[i];
