@@ -1323,17 +1323,47 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
     const T *phi = a.Phi + S.rgrid0;
     const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2];
     T g0 = 0, g1 = 0, g2 = 0;
-    for (int p = lane; p < P * P * P; p += 32) {
-      int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
-      int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
-      int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
-      int i3 = b.z + j3; if (i3 >= K3) i3 -= K3;
-      T ph = phi[((size_t)i1 * K2 + i2) * K3 + i3];
-      T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2], t3 = sh[warp][0][2][j3];
-      T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2], u3 = sh[warp][1][2][j3];
-      g0 += ph * u1 * t2 * t3;
-      g1 += ph * t1 * u2 * t3;
-      g2 += ph * t1 * t2 * u3;
+    bool vec = false;
+    if constexpr (sizeof(T) == 4) vec = (K3 & 3) == 0 && (S.rgrid0 & 3) == 0;
+    if (vec) {
+      // 16-byte loads: along k3 the P points of a stencil row fall into ng aligned groups of 4;
+      // one work item per (stencil row, group)
+      const int g0i = b.z >> 2, ng = ((b.z + P - 1) >> 2) - g0i + 1, K34 = K3 >> 2;
+      for (int sl = lane; sl < P * P * ng; sl += 32) {
+        const int r = sl / ng, gi = sl - r * ng;
+        const int j1 = r / P, j2 = r - j1 * P;
+        int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
+        int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
+        const int g = g0i + gi, gp = g >= K34 ? g - K34 : g;
+        const float4 ph4 = reinterpret_cast<const float4 *>(phi + ((size_t)i1 * K2 + i2) * K3)[gp];
+        const T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2];
+        const T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2];
+        const T A0 = u1 * t2, A1 = t1 * u2, A2 = t1 * t2;
+        const float pv[4] = {ph4.x, ph4.y, ph4.z, ph4.w};
+#pragma unroll
+        for (int el = 0; el < 4; ++el) {
+          const int j3 = 4 * g + el - b.z;
+          if (j3 >= 0 && j3 < P) {
+            const T ph = T(pv[el]), t3 = sh[warp][0][2][j3], u3 = sh[warp][1][2][j3];
+            g0 += ph * A0 * t3;
+            g1 += ph * A1 * t3;
+            g2 += ph * A2 * u3;
+          }
+        }
+      }
+    } else {
+      for (int p = lane; p < P * P * P; p += 32) {
+        int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
+        int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
+        int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
+        int i3 = b.z + j3; if (i3 >= K3) i3 -= K3;
+        T ph = phi[((size_t)i1 * K2 + i2) * K3 + i3];
+        T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2], t3 = sh[warp][0][2][j3];
+        T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2], u3 = sh[warp][1][2][j3];
+        g0 += ph * u1 * t2 * t3;
+        g1 += ph * t1 * u2 * t3;
+        g2 += ph * t1 * t2 * u3;
+      }
     }
     if (ROWS) { f0 = warp_sum<T>(f0); f1 = warp_sum<T>(f1); f2 = warp_sum<T>(f2); }
     g0 = warp_sum<T>(g0); g1 = warp_sum<T>(g1); g2 = warp_sum<T>(g2);
