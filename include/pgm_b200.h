@@ -125,7 +125,12 @@ PgmStatus pgm_destroy(PgmHandle *h);
 PgmStatus pgm_compute(PgmHandle *h, void *stream, const double *pos, const double *box, const int32_t *idx,
                       int idx_width, PgmInduction *ind, PgmOutputs *out);
 
-/* pgm_compute with host pointers (copies in and out; ind arrays and out arrays on the host). */
+/* pgm_compute with host pointers (copies in and out; ind arrays and out arrays on the host).
+ * ind == NULL keeps the induction state on the device, in the handle: each call starts from the
+ * state the previous pgm_compute_host call left (empty before the first: no history, count 0), and
+ * only positions, box and the outputs cross the host link -- the layout of a host MD engine that
+ * owns the coordinates but not the solver's state (the reference keeps InductionState in device
+ * arrays).  A call with ind set loads that state and leaves it (updated) in the handle too. */
 PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, PgmInduction *ind, PgmOutputs *out);
 
 /* PGMForceField.energy (forcefield.py:2562): energy only, CG started from ind->mu (plain start), no

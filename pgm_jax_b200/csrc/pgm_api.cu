@@ -1209,7 +1209,7 @@ PgmStatus pgm_compute(PgmHandle *h, void *stream, const double *pos, const doubl
 }
 
 PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, PgmInduction *ind, PgmOutputs *out) {
-  if (!h || !pos || !box || !ind || !out || !ind->mu || !ind->hist || !ind->count || !ind->norm)
+  if (!h || !pos || !box || !out || (ind && (!ind->mu || !ind->hist || !ind->count || !ind->norm)))
     return fail(PGM_ERR_INVALID, "null argument");
   EngineBase *e = h->eng.get();
   size_t n3 = (size_t)3 * e->nt, ns = e->nsys;
@@ -1221,15 +1221,17 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
     size_t nd = n3 + 9 * ns + n3 + 4 * n3 + ns + 3 * ns + n3 + 9 * ns + ns;
     size_t ni = 3 * ns;
     size_t bytes = sizeof(double) * nd + sizeof(int32_t) * ni;
+    if (!h->host_stream) CK(cudaStreamCreateWithFlags(&h->host_stream, cudaStreamNonBlocking));
     if (e->host_scratch_bytes < bytes) {
       if (e->host_scratch) cudaFree(e->host_scratch);
       e->host_scratch = nullptr;
       e->host_scratch_bytes = 0;
       CK(cudaMalloc(&e->host_scratch, bytes));
+      // a device-resident induction state starts empty (cleared on the stream of the calls)
+      CK(cudaMemsetAsync(e->host_scratch, 0, bytes, h->host_stream));
       e->host_scratch_bytes = bytes;
       ++e->generation;
     }
-    if (!h->host_stream) CK(cudaStreamCreateWithFlags(&h->host_stream, cudaStreamNonBlocking));
     d = e->host_scratch;
     double *dpos = d, *dbox = dpos + n3, *dmu = dbox + 9 * ns, *dhist = dmu + n3, *dnorm = dhist + 4 * n3, *den = dnorm + ns,
            *dF = den + 3 * ns, *dvir = dF + n3, *dres = dvir + 9 * ns;
@@ -1238,10 +1240,12 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
     cudaStream_t st = h->host_stream;
     CK(cudaMemcpyAsync(dpos, pos, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dbox, box, sizeof(double) * 9 * ns, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dmu, ind->mu, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dhist, ind->hist, sizeof(double) * 4 * n3, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dnorm, ind->norm, sizeof(double) * ns, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(dcount, ind->count, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
+    if (ind) {  // else the state the previous call left in the handle's block
+      CK(cudaMemcpyAsync(dmu, ind->mu, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(dhist, ind->hist, sizeof(double) * 4 * n3, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(dnorm, ind->norm, sizeof(double) * ns, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(dcount, ind->count, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
+    }
     PgmInduction di{dmu, dhist, dcount, dnorm};
     PgmOutputs dout{den, dF, dvir, dit, dres, dst};
     if (h->host_graph && h->host_graph_gen != e->generation) {
@@ -1269,10 +1273,12 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
     if (h->host_graph) CK(cudaGraphLaunch(h->host_graph, st));
     else e->compute(st, dpos, dbox, nullptr, 0, &di, &dout);
     ++h->host_calls;
-    CK(cudaMemcpyAsync(ind->mu, dmu, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ind->hist, dhist, sizeof(double) * 4 * n3, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ind->norm, dnorm, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ind->count, dcount, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, st));
+    if (ind) {
+      CK(cudaMemcpyAsync(ind->mu, dmu, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(ind->hist, dhist, sizeof(double) * 4 * n3, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(ind->norm, dnorm, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(ind->count, dcount, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, st));
+    }
     if (out->energy) CK(cudaMemcpyAsync(out->energy, den, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, st));
     if (out->forces) CK(cudaMemcpyAsync(out->forces, dF, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));
     if (out->virial) CK(cudaMemcpyAsync(out->virial, dvir, sizeof(double) * 9 * ns, cudaMemcpyDeviceToHost, st));

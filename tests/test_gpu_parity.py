@@ -277,6 +277,56 @@ def test_split_rows_match_oracle(small_box_system, prec):
         assert abs(float(r2.energy["total"][0]) - ro["energy"]["total"]) <= 1e-10 * abs(ro["energy"]["total"])
 
 
+def test_compute_host_with_the_state_on_the_device():
+    """pgm_compute_host with ind = NULL (the induction state kept in the handle, only positions in
+    and outputs out) gives, step after step, what the same call with the state in host buffers
+    gives, and switching between the two continues from the handle's state."""
+    import ctypes as C
+
+    from pgm_jax_b200 import _lib
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(4, 1.25, seed=11)
+    kw = dict(cutoff=0.6, ewald_beta=5.0, pme_grid=(32, 32, 32), dipole_tol=1e-7, max_iter=100)
+    fa = ff_for(s, H, "mixed", **kw)  # state on the device
+    fb = ff_for(s, H, "mixed", **kw)  # state in host buffers
+    n = s.n
+    p = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+
+    def outputs():
+        arrs = [np.zeros((1, 3)), np.zeros((n, 3)), np.zeros((1, 3, 3)), np.zeros(1, np.int32), np.zeros(1),
+                np.zeros(1, np.int32)]
+        return arrs, _lib.PgmOutputs(*[p(a).value for a in arrs])
+
+    arrs_a, outa = outputs()  # the arrays stay referenced: the library writes into them
+    arrs_b, outb = outputs()
+    Ea, Fa, _va, ita, _ra, sta = arrs_a
+    Eb, Fb, _vb, itb, _rb, stb = arrs_b
+    mu, hist = np.zeros((n, 3)), np.zeros((4, n, 3))
+    cnt, norm = np.zeros(1, np.int32), np.ones(1)
+    ind = _lib.PgmInduction(p(mu).value, p(hist).value, p(cnt).value, p(norm).value)
+    rng = np.random.default_rng(5)
+    x = pos.copy()
+    hb = np.ascontiguousarray(H[None])
+    for step in range(6):
+        x = x + rng.normal(scale=2e-4, size=x.shape)
+        xc = np.ascontiguousarray(x)
+        # at step 3 the device-state handle is given the host state from before this step (the
+        # values it holds itself): it loads it and carries on from it
+        ia = None
+        if step == 3:
+            mu_b, hist_b, cnt_b, norm_b = mu.copy(), hist.copy(), cnt.copy(), norm.copy()
+            ind_prev = _lib.PgmInduction(p(mu_b).value, p(hist_b).value, p(cnt_b).value, p(norm_b).value)
+            ia = C.byref(ind_prev)
+        _lib.check(fb._lib.pgm_compute_host(fb._h, p(xc), p(hb), C.byref(ind), C.byref(outb)))
+        _lib.check(fa._lib.pgm_compute_host(fa._h, p(xc), p(hb), ia, C.byref(outa)))
+        assert sta[0] == 0 and stb[0] == 0
+        # mixed precision: the two handles differ only by the order of FP32 atomic additions
+        assert abs(Ea[0, 2] - Eb[0, 2]) <= 1e-7 * abs(Eb[0, 2]), step
+        assert np.abs(Fa - Fb).max() <= 1e-5 * np.abs(Fb).max(), step
+        assert abs(int(ita[0]) - int(itb[0])) <= 1, step
+
+
 def test_compute_host_matches_device_calls():
     """pgm_compute_host (host buffers; from the second call a replayed captured graph) gives the
     device path's energies, forces and dipole history over consecutive steps, also after the row
