@@ -397,7 +397,7 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, 5) k_rows(Dev<T> a) {
+__global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int blk = blockIdx.x;
