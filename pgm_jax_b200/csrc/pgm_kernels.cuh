@@ -1449,7 +1449,7 @@ __device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, F &&edge
 // c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
 // NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
 template <typename T>
-__global__ void __launch_bounds__(256) k_nn_chan(Dev<T> a, const double *hist, const float4 *bl_prev, const int *valid,
+__global__ void __launch_bounds__(256, 8) k_nn_chan(Dev<T> a, const double *hist, const float4 *bl_prev, const int *valid,
                                                  float rg, float4 *bl_out, float *chan) {
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int s = a.wb_sys[blockIdx.x];
@@ -1564,7 +1564,7 @@ __device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const floa
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_nn_features(Dev<T> a, const float *chan, float sigma, float rg, float *inv, float *vec,
+__global__ void __launch_bounds__(256, 4) k_nn_features(Dev<T> a, const float *chan, float sigma, float rg, float *inv, float *vec,
                                                      int *valid) {
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (valid && blockIdx.x == 0 && threadIdx.x == 0) *valid = 1;  // read by the previous kernel only
