@@ -188,6 +188,7 @@ struct Engine : EngineBase {
   DBuf<pgm::c2<T>> C, tw;
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
   DBuf<float> nn_w, nn_inv, nn_vec, nn_mu, nn_chan;  // learned guess: model and per-atom features
+  DBuf<__nv_bfloat16> nn_wb;  // the model's weight matrices in BF16 (converted when the model is set)
   bool nn_on = false;
   int last_iters = 0;  // CG iterations of the last host-driven solve (sizes the unrolled part of a capture)
   const double *last_hist = nullptr;  // the history of the last predictor solve (profiling)
@@ -514,7 +515,7 @@ struct Engine : EngineBase {
     Q.alloc(rgrid); Phi.alloc(rgrid); Ginf.alloc(cgrid); C.alloc(cgrid);
     CK(cudaMemset(Q.p, 0, sizeof(T) * rgrid));
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
-    nn_w.alloc(pgmnn::NN_NPARAM); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
+    nn_w.alloc(pgmnn::NN_NPARAM); nn_wb.alloc(pgmnn::NN_WB_ELEMS); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
     nn_mu.alloc((size_t)nt * 3); nn_chan.alloc((size_t)nt * pgm::NN_CHAN); nn_bl.alloc(nt); nn_valid.alloc(1);
     if (set.predictor == 5) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
     CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
@@ -633,7 +634,11 @@ struct Engine : EngineBase {
   void set_nn(const float *w, float sigma, float rg) override {
     ++generation;  // a captured step depends on whether a model is set, and on sigma and rg
     nn_on = w != nullptr;
-    if (w) CK(cudaMemcpy(nn_w.p, w, sizeof(float) * pgmnn::NN_NPARAM, cudaMemcpyDeviceToDevice));
+    if (w) {
+      CK(cudaMemcpy(nn_w.p, w, sizeof(float) * pgmnn::NN_NPARAM, cudaMemcpyDeviceToDevice));
+      CK(pgmnn::nn_weights_bf16(nn_w.p, nn_wb.p, 0));  // the matrices as the inference kernel reads them
+      CK(cudaDeviceSynchronize());
+    }
     CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
     nn_sigma = sigma;
     nn_rg = rg;
@@ -722,7 +727,7 @@ struct Engine : EngineBase {
       } else if (which == 11) {
         pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, nn_chan.p, nn_sigma, nn_rg, nn_inv.p, nn_vec.p, nullptr);
       } else {  // 12: the model
-        CK(pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st));
+        CK(pgmnn::nn_predict_launch(nn_w.p, nn_wb.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st));
       }
     };
     long long l0 = launches;
@@ -809,7 +814,7 @@ struct Engine : EngineBase {
     CK(cudaEventRecord(ev_nn_fork, st));
     CK(cudaStreamWaitEvent(nn_st, ev_nn_fork, 0));
     nn_inputs(nn_st, a, hist, nn_bl.p, nn_valid.p, nn_bl.p, nn_inv.p, nn_vec.p, nn_valid.p);
-    cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, nn_st, prio_hi);
+    cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_wb.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, nn_st, prio_hi);
     if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
     ++launches;
     CK(cudaEventRecord(ev_nn_join, nn_st));

@@ -169,38 +169,59 @@ __device__ void forward_tile(Smem &s) {
 // split across the warps (layers 1 and 2: 16 hidden columns per warp; layer 3: the 16 coefficient
 // columns that the channel mix uses, its K = 64 split in four and the partial products summed in
 // shared memory), so that a sample's chain of dependent tensor-core steps is a quarter of a whole
-// layer stack.  Same rounding points as the training forward (BF16 operands, FP32 accumulation).
+// layer stack.  The weights come as BF16 matrices in global memory (converted once, k_to_bf16):
+// each warp loads its six B fragments straight from there (L2), with no staging and no barrier.
+// Same rounding points as the training forward (BF16 operands, FP32 accumulation).
 constexpr int FWD_ROWS = 16;
 constexpr int FWD_WARPS = THREADS / 32;
 static_assert(NN_HID == 16 * FWD_WARPS && NN_CH <= 16, "one 16-column slice of each layer per warp");
 struct FwdSmem {
-  __nv_bfloat16 w1[NN_IN * NN_HID], w2[NN_HID * NN_HID], w3[NN_HID * NN_OUT];
   __nv_bfloat16 x[FWD_ROWS * NN_IN], a1[FWD_ROWS * NN_HID], a2[FWD_ROWS * NN_HID];
   float z[FWD_ROWS * NN_HID];            // layer outputs before the activation
   float zp[FWD_WARPS][FWD_ROWS * 16];    // layer-3 partial products
-  float b1[NN_HID], b2[NN_HID], b3[NN_OUT];
 };
 
-// One warp's 16 x 16 slice: C (ldc) = A[16 x K] (lda) B[K x 16] (ldb), FP32 accumulation.
-template <int K>
-__device__ __forceinline__ void warp_slice(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int ldb, float *C, int ldc) {
+using FragB = wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major>;
+
+// C (16 x 16, ldc) = A[16 x 16 K] (lda) times the K / 16 B fragments fb.
+template <int KS>
+__device__ __forceinline__ void warp_slice(const __nv_bfloat16 *A, int lda, const FragB (&fb)[KS], float *C, int ldc) {
   wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
   wmma::fill_fragment(acc, 0.0f);
 #pragma unroll
-  for (int k = 0; k < K; k += 16) {
+  for (int k = 0; k < KS; ++k) {
     wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> fa;
-    wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> fb;
-    wmma::load_matrix_sync(fa, A + k, lda);
-    wmma::load_matrix_sync(fb, B + k * ldb, ldb);
-    wmma::mma_sync(acc, fa, fb, acc);
+    wmma::load_matrix_sync(fa, A + 16 * k, lda);
+    wmma::mma_sync(acc, fa, fb[k], acc);
   }
   wmma::store_matrix_sync(C, acc, ldc, wmma::mem_row_major);
 }
 
-__global__ void __launch_bounds__(THREADS) k_forward(NNWeights w, const float *inv, const float *vec, int n, float *mu) {
+// BF16 copies of the three weight matrices of the flat FP32 array, packed: W1 | W2 | W3.
+constexpr int NN_WB = NN_WB_ELEMS;
+__global__ void k_to_bf16(NNWeights w, __nv_bfloat16 *out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NN_WB) return;
+  float v;
+  if (t < NN_IN * NN_HID) v = w.w1[t];
+  else if (t < NN_IN * NN_HID + NN_HID * NN_HID) v = w.w2[t - NN_IN * NN_HID];
+  else v = w.w3[t - NN_IN * NN_HID - NN_HID * NN_HID];
+  out[t] = __float2bfloat16(v);
+}
+
+__global__ void __launch_bounds__(THREADS) k_forward(NNWeights w, const __nv_bfloat16 *wb, const float *inv, const float *vec,
+                                                     int n, float *mu) {
   __shared__ __align__(128) FwdSmem s;
-  stage_weights(w, s.w1, s.w2, s.w3, s.b1, s.b2, s.b3);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, c0 = 16 * warp;
+  const __nv_bfloat16 *W1 = wb, *W2 = W1 + NN_IN * NN_HID, *W3 = W2 + NN_HID * NN_HID;
+  // this warp's B fragments: layer 1 columns c0.., layer 2 columns c0.. (four K steps), layer 3
+  // rows c0.. of the first 16 columns
+  FragB f1[1], f2[NN_HID / 16], f3[1];
+  wmma::load_matrix_sync(f1[0], W1 + c0, NN_HID);
+#pragma unroll
+  for (int k = 0; k < NN_HID / 16; ++k) wmma::load_matrix_sync(f2[k], W2 + 16 * k * NN_HID + c0, NN_HID);
+  wmma::load_matrix_sync(f3[0], W3 + c0 * NN_OUT, NN_OUT);
+  const float b1 = w.b1[c0 + (lane & 15)], b2 = w.b2[c0 + (lane & 15)];
   for (int r0 = blockIdx.x * FWD_ROWS; r0 < n; r0 += gridDim.x * FWD_ROWS) {
     // the channel vectors of the mix (threads 0..47: row t / 3, component t % 3) in flight
     // through the layers
@@ -216,30 +237,30 @@ __global__ void __launch_bounds__(THREADS) k_forward(NNWeights w, const float *i
       int i = r0 + t / NN_IN;
       s.x[t] = __float2bfloat16(i < n ? inv[(size_t)r0 * NN_IN + t] : 0.f);
     }
-    __syncthreads();  // x (and, on the first tile, the weights)
-    warp_slice<NN_IN>(s.x, NN_IN, s.w1 + c0, NN_HID, s.z + c0, NN_HID);
+    __syncthreads();  // x
+    warp_slice<1>(s.x, NN_IN, f1, s.z + c0, NN_HID);
     __syncwarp();
-    for (int e = lane; e < FWD_ROWS * 16; e += 32) {
+    for (int e = lane; e < FWD_ROWS * 16; e += 32) {  // column c0 + (e & 15) == c0 + (lane & 15)
       int r = e >> 4, c = c0 + (e & 15);
-      s.a1[r * NN_HID + c] = __float2bfloat16(silu(s.z[r * NN_HID + c] + s.b1[c]));
+      s.a1[r * NN_HID + c] = __float2bfloat16(silu(s.z[r * NN_HID + c] + b1));
     }
     __syncthreads();  // a1 complete
-    warp_slice<NN_HID>(s.a1, NN_HID, s.w2 + c0, NN_HID, s.z + c0, NN_HID);
+    warp_slice<NN_HID / 16>(s.a1, NN_HID, f2, s.z + c0, NN_HID);
     __syncwarp();
     for (int e = lane; e < FWD_ROWS * 16; e += 32) {
       int r = e >> 4, c = c0 + (e & 15);
-      s.a2[r * NN_HID + c] = __float2bfloat16(silu(s.z[r * NN_HID + c] + s.b2[c]));
+      s.a2[r * NN_HID + c] = __float2bfloat16(silu(s.z[r * NN_HID + c] + b2));
     }
     __syncthreads();  // a2 complete
     // layer 3, coefficient columns 0..15: this warp's 16 rows of K
-    warp_slice<16>(s.a2 + c0, NN_HID, s.w3 + c0 * NN_OUT, NN_OUT, s.zp[warp], 16);
+    warp_slice<1>(s.a2 + c0, NN_HID, f3, s.zp[warp], 16);
     __syncthreads();
     if (mixer) {
       float acc = 0.f;
 #pragma unroll
       for (int c = 0; c < NN_CH; ++c) {
         const int e = mr * 16 + c;
-        const float coef = ((s.zp[0][e] + s.zp[1][e]) + (s.zp[2][e] + s.zp[3][e])) + s.b3[c];
+        const float coef = ((s.zp[0][e] + s.zp[1][e]) + (s.zp[2][e] + s.zp[3][e])) + w.b3[c];
         acc += coef * v[c];
       }
       mu[3 * (size_t)mi + ma] = acc;
@@ -356,14 +377,17 @@ cudaError_t set_attrs() {
   return e;
 }
 
-cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *vec, int n, float *mu, cudaStream_t st,
-                              int priority) {
-  cudaError_t e = set_attrs();
-  if (e != cudaSuccess) return e;
+cudaError_t nn_weights_bf16(const float *flat, __nv_bfloat16 *wb, cudaStream_t st) {
+  k_to_bf16<<<(NN_WB + 255) / 256, 256, 0, st>>>(nn_view(const_cast<float *>(flat)), wb);
+  return cudaGetLastError();
+}
+
+cudaError_t nn_predict_launch(const float *flat, const __nv_bfloat16 *wb, const float *inv, const float *vec, int n, float *mu,
+                              cudaStream_t st, int priority) {
   if (n <= 0) return cudaSuccess;
   const int tiles = (n + FWD_ROWS - 1) / FWD_ROWS;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(tiles);  // one 16-sample tile per CTA (about 24 KB of shared memory each)
+  cfg.gridDim = dim3(tiles);  // one 16-sample tile per CTA
   cfg.blockDim = dim3(THREADS);
   cfg.stream = st;
   cudaLaunchAttribute at[1];
@@ -371,7 +395,7 @@ cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *
   at[0].val.priority = priority;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_forward, nn_view(const_cast<float *>(flat)), inv, vec, n, mu);
+  return cudaLaunchKernelEx(&cfg, k_forward, nn_view(const_cast<float *>(flat)), wb, inv, vec, n, mu);
 }
 
 thread_local std::string g_nn_err;
@@ -384,7 +408,16 @@ int pgm_nn_param_count(void) { return pgmnn::NN_NPARAM; }
 
 PgmStatus pgm_nn_predict(void *stream, const float *weights, const float *inv, const float *vec, int n, float *mu) {
   if (!weights || !inv || !vec || !mu || n < 0) return PGM_ERR_INVALID;
-  cudaError_t e = pgmnn::nn_predict_launch(weights, inv, vec, n, mu, (cudaStream_t)stream, 0);
+  // the BF16 weight copy in stream-ordered memory, converted and released on the caller's stream
+  cudaStream_t st = (cudaStream_t)stream;
+  __nv_bfloat16 *wb = nullptr;
+  cudaError_t e = cudaMallocAsync(&wb, sizeof(__nv_bfloat16) * pgmnn::NN_WB, st);
+  if (e == cudaSuccess) e = pgmnn::nn_weights_bf16(weights, wb, st);
+  if (e == cudaSuccess) e = pgmnn::nn_predict_launch(weights, wb, inv, vec, n, mu, st, 0);
+  if (wb) {
+    cudaError_t f = cudaFreeAsync(wb, st);
+    if (e == cudaSuccess) e = f;
+  }
   if (e != cudaSuccess) {
     pgmnn::g_nn_err = cudaGetErrorString(e);
     return PGM_ERR_CUDA;

@@ -1,5 +1,6 @@
 // pgm_nn.cuh -- sizes and weight layout of the learned initial guess (pgm_nn.cu).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 namespace pgmnn {
@@ -27,8 +28,14 @@ inline __host__ __device__ NNWeights nn_view(float *flat) {
   return w;
 }
 
+// BF16 copies of the weight matrices (W1 | W2 | W3, NN_WB elements) from the flat FP32 array.
+constexpr int NN_WB_ELEMS = NN_IN * NN_HID + NN_HID * NN_HID + NN_HID * NN_OUT;
+cudaError_t nn_weights_bf16(const float *flat, __nv_bfloat16 *wb, cudaStream_t st);
+
 // mu (n, 3) FP32 = the model's prediction from invariants inv (n, NN_IN) and channels vec
-// (n, NN_CH, 3); launched on `st` (used by the engine's solver start).
-cudaError_t nn_predict_launch(const float *flat, const float *inv, const float *vec, int n, float *mu, cudaStream_t st, int priority = 0);
+// (n, NN_CH, 3), with the biases from the flat FP32 array and the matrices from their BF16 copy
+// wb; launched on `st` (used by the engine's solver start).
+cudaError_t nn_predict_launch(const float *flat, const __nv_bfloat16 *wb, const float *inv, const float *vec, int n, float *mu,
+                              cudaStream_t st, int priority = 0);
 
 }  // namespace pgmnn
