@@ -6,7 +6,7 @@ converged induced dipoles mu* of a step, from the change of the graph's permanen
 last step (the real-space field of charges and permanent dipoles over the graph edges) and the last
 steps' dipoles.  With predictor "nn" the engine's solver starts CG from x4 + the prediction with
 mu4's fused start (one field sweep, as the reference's mu4 predictor) and iterates to the same
-tolerance, so the plain solver judges the guess; the untrained (zero) model is mu4 exactly.
+tolerance, so a poor guess costs iterations, never accuracy; the untrained (zero) model is mu4 exactly.
 The model (csrc/pgm_nn.cu): 16 rotation invariants -> MLP 64 -> 64 (SiLU) -> 15 coefficients that
 mix 15 vector channels per atom (csrc/pgm_kernels.cuh k_nn_chan, k_nn_features), so the prediction
 rotates with the system.  Training runs on the GPU with the project's BF16 tensor-core
