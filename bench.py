@@ -565,6 +565,45 @@ def run_workload(args) -> None:
                        "72^3) at 298 K + 32 x 512 waters REMD 280-400 K (geometric), one engine, mixed, CG 1e-6 from mu4, "
                        "Langevin 2/ps, dt 1 fs, exchanges every 100 steps (timed)", "equilibration": "500 steps at 20/ps"},
         })
+    elif args.workload == "npt":
+        from pgm_jax_b200.barostat import MonteCarloBarostat
+        from pgm_jax_b200.forcefield import PGMForceField
+        from pgm_jax_b200.md import RigidMD
+
+        s, pos, H = water_box(N_SIDE, EDGE_NM, seed=0)
+        ff = PGMForceField(s, H, settings(predictor="mu4"), device=0)
+        md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1)
+        equilibrate(md)
+        for _ in range(4):
+            md.step()
+        md.capture()
+        baro = MonteCarloBarostat(md, pressure=1.0, every=100, seed=1)
+        baro.run(400)  # warm-up: the step size adapts, the first moves are made
+        md.stream.synchronize()
+        V0 = float(baro.volumes()[0])
+        tries0, acc0 = int(baro.total_tries[0]), int(baro.total_accepted[0])
+        steps = max(200, (min(args.steps, 2000) // 100) * 100)
+        clk = Clocks(0)
+        md.run(50)  # the GPU stays loaded while the sampler starts
+        torch.cuda.synchronize()
+        # wall clock: the volume moves return to the host (the accept decision), so events on the
+        # MD stream alone would miss the host's part
+        t0 = time.perf_counter()
+        baro.run(steps)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        clk.mark(t0, t1)
+        clocks = clk.stop()
+        ms = (t1 - t0) * 1e3 / steps
+        line.update({
+            "value": ns_per_day(ms), "ms_per_step": ms, "steps": steps, "clocks": clocks,
+            "volume_moves": int(baro.total_tries[0]) - tries0, "accepted": int(baro.total_accepted[0]) - acc0,
+            "volume_nm3": [V0, float(baro.volumes()[0])], "dv_nm3": float(baro.dv[0]),
+            "status_any": int(md.ff._status.max()),
+            "config": {"workload": "4096 rigid pGM3P-25 waters, NPT 1 bar / 298 K: the bench MD (mu4 start, mixed, CG 1e-6) "
+                       "with an isotropic Monte Carlo volume move every 100 steps", "timing": "wall clock over the steps "
+                       "and the moves (each move: one trial energy, and the forces again when accepted)"},
+        })
     elif args.workload == "pimd":
         from pgm_jax_b200.forcefield import MDSettings
         from pgm_jax_b200.pimd import PIMD
@@ -667,7 +706,7 @@ def main() -> None:
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
-    ap.add_argument("--workload", default="water4096", choices=["water4096", "batch", "water32768", "pimd"],
+    ap.add_argument("--workload", default="water4096", choices=["water4096", "batch", "water32768", "pimd", "npt"],
                     help="water4096: the headline; the others print their own line (one GPU)")
     ap.add_argument("--elec-cutoff", type=float, default=None,
                     help="split rows: electrostatics cutoff [nm] below the 0.9 nm LJ cutoff (Ewald coefficient for it)")
