@@ -299,6 +299,19 @@ PgmStatus pgm_pimd_kick(void *stream, long long n3, double h, const double *forc
 PgmStatus pgm_pimd_free_thermostat(void *stream, int beads, int n_atoms, const double *C, const double *omega, const double *gamma,
                                    const double *mass, double dt, double kT_P, uint64_t seed, uint64_t *counter, double *pos,
                                    double *mom);
+/* PILE-G (pimd.py:411-440 with the Bussi step of thermostats.py:279-335): the rescaling factor of
+ * the ring polymer's centroid for an O step of length dt [ps] with time constant tau [ps], from the
+ * centroid kinetic energy of mom at kT_P with N_f = 3 n_atoms degrees of freedom; random numbers
+ * from (seed, *counter) (the counter is not advanced).  work: 4 device doubles, written as
+ * [K, alpha, R1, S] (the kinetic energy, the factor, the normal and the chi^2(N_f - 1) draws). */
+PgmStatus pgm_pimd_centroid_bussi(void *stream, int beads, int n_atoms, const double *C, const double *mass, double dt, double kT_P,
+                                  double tau, uint64_t seed, const uint64_t *counter, const double *mom, double *work);
+/* pgm_pimd_free_thermostat with the centroid mode multiplied by *centroid_scale (device; the
+ * factor pgm_pimd_centroid_bussi left in work[1]) in place of its Langevin step (its friction
+ * should be 0); centroid_scale NULL: pgm_pimd_free_thermostat. */
+PgmStatus pgm_pimd_free_thermostat_scaled(void *stream, int beads, int n_atoms, const double *C, const double *omega,
+                                          const double *gamma, const double *mass, double dt, double kT_P, uint64_t seed,
+                                          uint64_t *counter, double *pos, double *mom, const double *centroid_scale);
 /* q-TIP4P/F intramolecular water term (pgm_jax/models/water.py:33-69) for molecules O, H, H at
  * first_atom[m]: params (host, 5) = D [kJ/mol], alpha [1/nm], r_eq [nm], k_theta [kJ/mol/rad^2],
  * theta_eq [rad]; forces += its forces; energy[mol_system[m]] += its energy (energy may be NULL). */

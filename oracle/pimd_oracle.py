@@ -1,8 +1,8 @@
 """NumPy restatement of the ring-polymer integrator pieces and the q-TIP4P/F water term -- TEST
 INFRASTRUCTURE (only tests use it).
 
-The free ring-polymer step in normal modes with the Cayley propagator and the PILE-L thermostat
-(pgm_jax/md/pimd.py:238-282, 411-440, 651-670), and the q-TIP4P/F intramolecular energy
+The free ring-polymer step in normal modes with the Cayley propagator, the PILE-L thermostat and
+PILE-G's Bussi factor (pgm_jax/md/pimd.py:238-282, 411-440, 651-670; thermostats.py:279-335), and the q-TIP4P/F intramolecular energy
 (pgm_jax/models/water.py:38-69) with forces by central differences.
 """
 
@@ -33,6 +33,35 @@ def free_step(q, p, C, omega, mass, dt):
     qn, pn = cayley(qn, pn, w, m, 0.5 * dt)
     qn, pn = cayley(qn, pn, w, m, 0.5 * dt)
     return np.einsum("jl,lnc->jnc", C, qn), np.einsum("jl,lnc->jnc", C, pn)
+
+
+def free_step_centroid_scaled(q, p, C, omega, mass, dt, alpha):
+    """A(dt/2), the centroid momentum times alpha (PILE-G's Bussi rescaling, no other friction),
+    A(dt/2), in normal modes (pimd.py:411-440)."""
+    qn = np.einsum("jl,jnc->lnc", C, q)
+    pn = np.einsum("jl,jnc->lnc", C, p)
+    w = np.asarray(omega)[:, None, None]
+    m = np.asarray(mass)[None, :, None]
+    qn, pn = cayley(qn, pn, w, m, 0.5 * dt)
+    pn[0] *= alpha
+    qn, pn = cayley(qn, pn, w, m, 0.5 * dt)
+    return np.einsum("jl,lnc->jnc", C, qn), np.einsum("jl,lnc->jnc", C, pn)
+
+
+def centroid_kinetic(p, C, mass):
+    """Kinetic energy of the ring polymer's centroid mode: sum p~0^2 / (2 m), p~0 = sum_j C[j][0] p_j."""
+    p0 = np.einsum("j,jnc->nc", C[:, 0], p)
+    return float(0.5 * np.sum(p0 * p0 / np.asarray(mass)[:, None]))
+
+
+def bussi_factor(K, kT, dof, h, tau, r1, S):
+    """Bussi's rescaling factor for a step h given the draws R1 ~ N(0,1), S ~ chi^2(dof - 1)
+    (thermostats.py:320-334)."""
+    K = max(K, 1e-30)
+    c = math.exp(-h / tau)
+    f = 0.5 * dof * kT / (dof * K)
+    a2 = c + (1.0 - c) * f * (r1 * r1 + S) + 2.0 * r1 * math.sqrt(c * (1.0 - c) * f)
+    return math.copysign(math.sqrt(max(a2, 0.0)), r1 + math.sqrt(c / ((1.0 - c) * f)))
 
 
 def qtip4pf_energy(R, D, alpha, r_eq, k_theta, theta_eq_rad):

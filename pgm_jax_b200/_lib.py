@@ -21,7 +21,8 @@ EXPORTS = (
     "pgm_set_row_capacity", "pgm_row_capacity", "pgm_set_elec_capacity", "pgm_elec_capacity", "pgm_max_vdw_count", "pgm_set_list_capacity", "pgm_list_capacity", "pgm_list_rebuilds", "pgm_max_row_count", "pgm_num_atoms", "pgm_num_systems",
     "pgm_last_error", "pgm_last_launch_count", "pgm_launches_per_iteration", "pgm_unrolled_iterations", "pgm_profile_kernel", "pgm_row_pairs", "pgm_rigid_create", "pgm_rigid_destroy",
     "pgm_rigid_begin_step", "pgm_rigid_set_step", "pgm_rigid_end_step", "pgm_rigid_kinetic", "pgm_rigid_scale_momenta", "pgm_rigid_last_error", "pgm_pimd_kick",
-    "pgm_pimd_free_thermostat", "pgm_water_bonded", "pgm_pimd_last_error", "pgm_graph_begin",
+    "pgm_pimd_free_thermostat", "pgm_pimd_centroid_bussi", "pgm_pimd_free_thermostat_scaled", "pgm_water_bonded",
+    "pgm_pimd_last_error", "pgm_graph_begin",
     "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
     "pgm_set_nn_model", "pgm_nn_features", "pgm_nn_param_count", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam",
     "pgm_nn_last_error",
@@ -118,9 +119,14 @@ def load(path: str | None = None):
     lib.pgm_pimd_kick.argtypes = [vp, C.c_longlong, C.c_double, vp, vp]
     lib.pgm_pimd_free_thermostat.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, C.c_double, C.c_uint64, vp, vp,
                                              vp]
+    lib.pgm_pimd_centroid_bussi.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_double, C.c_double, C.c_double, C.c_uint64, vp, vp,
+                                            vp]
+    lib.pgm_pimd_free_thermostat_scaled.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, C.c_double, C.c_uint64,
+                                                    vp, vp, vp, vp]
     lib.pgm_water_bonded.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp]
     lib.pgm_pimd_last_error.restype = C.c_char_p
-    for n in ("pgm_pimd_kick", "pgm_pimd_free_thermostat", "pgm_water_bonded"):
+    for n in ("pgm_pimd_kick", "pgm_pimd_free_thermostat", "pgm_pimd_centroid_bussi", "pgm_pimd_free_thermostat_scaled",
+              "pgm_water_bonded"):
         getattr(lib, n).restype = C.c_int
     lib.pgm_rigid_last_error.restype = C.c_char_p
     lib.pgm_field_static.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_double, C.c_double, vp, C.c_int, C.c_int, vp, vp]

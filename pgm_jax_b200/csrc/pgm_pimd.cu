@@ -74,7 +74,73 @@ struct PimdArgs {
   double dt, kTP;
   unsigned long long seed;
   unsigned long long *counter;
+  const double *cscale;  // PILE-G: the centroid's Bussi factor (null: none)
 };
+
+// One uniform in (0, 1) per (seed, step, stream index) (the hash of normal01).
+__device__ __forceinline__ double uniform01(unsigned long long seed, unsigned long long step, unsigned long long idx) {
+  unsigned long long h = mix64(seed ^ mix64(step * 0x100000001B3ull + idx));
+  return ((h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// Stream indices of the Bussi draws, above those of the per-(atom, component, mode) Langevin noise.
+constexpr unsigned long long BUSSI_STREAM = 1ull << 48;
+
+// PILE-G, step 1: the centroid kinetic energy K = sum_i,c p~0(i, c)^2 / (2 m_i) of the ring
+// polymer, p~0 = sum_j C[j][0] p_j (one thread per atom component, block sums, one atomic each).
+__global__ void k_centroid_ke(int P, int N, const double *C, const double *mass, const double *p, double *K) {
+  __shared__ double red[8];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (t < 3LL * N) {
+    const int i = (int)(t / 3);
+    double p0 = 0.0;
+    for (int j = 0; j < P; ++j) p0 += C[j * P] * p[(size_t)j * 3 * N + t];
+    e = 0.5 * p0 * p0 / mass[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w];
+    atomicAdd(K, v);
+  }
+}
+
+// PILE-G, step 2 (one thread): Bussi's exact rescaling factor (thermostats.py:279-335) for an O
+// step of length h with time constant tau, from K = work[0] at kT with N_f = dof:
+//   alpha^2 = c + (1 - c) f (R1^2 + S) + 2 R1 sqrt(c (1 - c) f),  f = K0 / (N_f K) = kT / (2 K),
+// c = exp(-h / tau), R1 ~ N(0, 1), S ~ chi^2(N_f - 1) = 2 Gamma((N_f - 1) / 2), alpha with the
+// sign of R1 + sqrt(c / ((1 - c) f)).  The Gamma variate by Marsaglia and Tsang's method (ACM TOMS
+// 26, 363 (2000)), shape k = (N_f - 1) / 2 >= 1, at most 64 proposals (then its mode).
+// work: [K, alpha, R1, S].
+__global__ void k_bussi(double dof, double kT, double h, double tau, unsigned long long seed, const unsigned long long *counter,
+                        double *work) {
+  const unsigned long long step = *counter;
+  const double K = fmax(work[0], 1e-30);
+  const double c = exp(-h / tau), f = kT / (2.0 * K);
+  const double r1 = normal01(seed, step, BUSSI_STREAM);
+  const double k = 0.5 * (dof - 1.0), d = k - 1.0 / 3.0, cc = 1.0 / sqrt(9.0 * d);
+  double g = d;
+  for (int it = 0; it < 64; ++it) {
+    const double x = normal01(seed, step, BUSSI_STREAM + 1 + 2 * it);
+    double v = 1.0 + cc * x;
+    if (v <= 0.0) continue;
+    v = v * v * v;
+    const double u = uniform01(seed, step, BUSSI_STREAM + 2 + 2 * it);
+    if (log(u) < 0.5 * x * x + d - d * v + d * log(v)) {
+      g = d * v;
+      break;
+    }
+  }
+  const double S = 2.0 * g;
+  const double a2 = c + (1.0 - c) * f * (r1 * r1 + S) + 2.0 * r1 * sqrt(c * (1.0 - c) * f);
+  const double sg = (r1 + sqrt(c / ((1.0 - c) * f))) < 0.0 ? -1.0 : 1.0;
+  work[1] = sg * sqrt(fmax(a2, 0.0));
+  work[2] = r1;
+  work[3] = S;
+}
 
 __global__ void __launch_bounds__(256) k_pimd_aoa(PimdArgs A, double *q, double *p) {
   const int lane = threadIdx.x & 31;
@@ -96,7 +162,9 @@ __global__ void __launch_bounds__(256) k_pimd_aoa(PimdArgs A, double *q, double 
     const double m = A.mass[i], wl = A.omega[lane], h = 0.5 * A.dt;
     cayley(wl, m, h, qn, pn);
     const double g = A.gamma[lane];
-    if (g > 0.0) {
+    if (lane == 0 && A.cscale) {
+      pn *= *A.cscale;  // PILE-G: the centroid rescaled by Bussi's factor
+    } else if (g > 0.0) {
       const double cc = exp(-g * A.dt);
       const unsigned long long step = *A.counter;
       const double xi = normal01(A.seed, step, ((unsigned long long)off * 32ull + lane));
@@ -178,10 +246,31 @@ PgmStatus pgm_pimd_kick(void *stream, long long n3, double h, const double *forc
 PgmStatus pgm_pimd_free_thermostat(void *stream, int beads, int n_atoms, const double *C, const double *omega, const double *gamma,
                                    const double *mass, double dt, double kT_P, uint64_t seed, uint64_t *counter, double *pos,
                                    double *mom) {
+  return pgm_pimd_free_thermostat_scaled(stream, beads, n_atoms, C, omega, gamma, mass, dt, kT_P, seed, counter, pos, mom, nullptr);
+}
+
+PgmStatus pgm_pimd_centroid_bussi(void *stream, int beads, int n_atoms, const double *C, const double *mass, double dt, double kT_P,
+                                  double tau, uint64_t seed, const uint64_t *counter, const double *mom, double *work) {
+  if (beads < 1 || beads > 32 || n_atoms < 1 || !C || !mass || !counter || !mom || !work || !(tau > 0.0) || !(dt > 0.0))
+    return PGM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  PCK(cudaMemsetAsync(work, 0, sizeof(double), st));
+  const long long n3 = 3LL * n_atoms;
+  k_centroid_ke<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(beads, n_atoms, C, mass, mom, work);
+  PCK(cudaGetLastError());
+  k_bussi<<<1, 1, 0, st>>>(3.0 * n_atoms, kT_P, dt, tau, seed, reinterpret_cast<const unsigned long long *>(counter), work);
+  PCK(cudaGetLastError());
+  return PGM_OK;
+}
+
+PgmStatus pgm_pimd_free_thermostat_scaled(void *stream, int beads, int n_atoms, const double *C, const double *omega,
+                                          const double *gamma, const double *mass, double dt, double kT_P, uint64_t seed,
+                                          uint64_t *counter, double *pos, double *mom, const double *centroid_scale) {
   if (beads < 1 || beads > 32 || n_atoms < 0 || !C || !omega || !gamma || !mass || !counter || !pos || !mom)
     return PGM_ERR_INVALID;
   if (n_atoms == 0) return PGM_OK;
-  PimdArgs A{beads, n_atoms, C, omega, gamma, mass, dt, kT_P, seed, reinterpret_cast<unsigned long long *>(counter)};
+  PimdArgs A{beads, n_atoms, C, omega, gamma, mass, dt, kT_P, seed, reinterpret_cast<unsigned long long *>(counter),
+             centroid_scale};
   const long long warps = 3LL * n_atoms;
   k_pimd_aoa<<<(unsigned)((warps + 7) / 8), 256, 0, (cudaStream_t)stream>>>(A, pos, mom);
   PCK(cudaGetLastError());

@@ -70,18 +70,22 @@ class RingPolymer:
         return 0.5 * self.omega_P**2 * mass * np.sum(d * d, axis=(0, 2))
 
 
-def frictions(ring: RingPolymer, mode: str = "pimd", tau_centroid: float = 0.2, lam: float | None = None) -> np.ndarray:
+def frictions(ring: RingPolymer, mode: str = "pimd", tau_centroid: float = 0.2, lam: float | None = None,
+              centroid: str = "l") -> np.ndarray:
     """Friction of every mode [1/ps] (PILEStep, pimd.py:375-397): 2 lam omega_l on the internal
-    modes (lam 1 for "pimd", 1/2 for "trpmd"), 1/tau_centroid on the centroid for "pimd", none for
+    modes (lam 1 for "pimd", 1/2 for "trpmd"), 1/tau_centroid on the centroid for "pimd" with the
+    Langevin centroid (PILE-L, centroid "l"), 0 with Bussi's (PILE-G, centroid "g"), none for
     "rpmd"."""
     mode = mode.lower()
     if mode not in ("pimd", "trpmd", "rpmd"):
         raise ValueError(f"mode: 'pimd' | 'trpmd' | 'rpmd', not {mode!r}")
+    if centroid not in ("l", "g"):
+        raise ValueError(f"centroid thermostat must be 'l' (Langevin) or 'g' (Bussi), not {centroid!r}")
     if tau_centroid <= 0:
         raise ValueError("tau_centroid must be > 0")
     lam = (0.5 if mode == "trpmd" else 1.0) if lam is None else float(lam)
     g = 2.0 * lam * ring.omega
-    g[0] = 1.0 / tau_centroid if mode == "pimd" else 0.0
+    g[0] = 1.0 / tau_centroid if (mode == "pimd" and centroid == "l") else 0.0
     if mode == "rpmd":
         g[:] = 0.0
     return g
@@ -96,13 +100,14 @@ class PIMD:
 
     system, pos (N, 3) [nm], H (3, 3) [nm]; settings an MDSettings (pme_grid etc.); beads P <= 32.
     The beads start on the free ring polymer around `pos` (seeded) with momenta at P kB T.
-    mode "pimd" (PILE-L), "trpmd" or "rpmd" (no thermostat).  Water molecules (3 atoms: O, H, H)
+    mode "pimd" (PILE-L, or PILE-G with centroid="g": Bussi's rescaling of the centroid with time
+    constant tau_centroid), "trpmd" or "rpmd" (no thermostat).  Water molecules (3 atoms: O, H, H)
     get the q-TIP4P/F intramolecular term.
     """
 
     def __init__(self, system, pos, H, settings: MDSettings, beads: int = 32, temperature: float = 300.0, dt_fs: float = 0.5,
                  mode: str = "pimd", tau_centroid: float = 0.2, lam: float | None = None, seed: int = 1, device: int = 0,
-                 pme_grid=None, bonded: dict | None = QTIP4PF) -> None:
+                 pme_grid=None, bonded: dict | None = QTIP4PF, centroid: str = "l") -> None:
         if not 1 <= int(beads) <= 32:
             raise ValueError("1 <= beads <= 32")
         self.P = int(beads)
@@ -131,7 +136,10 @@ class PIMD:
         self.forces = torch.zeros_like(self.q)
         self.C = t(self.ring.C)
         self.omega = t(self.ring.omega)
-        self.gamma = t(frictions(self.ring, mode, tau_centroid, lam))
+        self.gamma = t(frictions(self.ring, mode, tau_centroid, lam, centroid))
+        self.tau0 = float(tau_centroid)
+        self.centroid_bussi = mode == "pimd" and centroid == "g"
+        self.bussi_work = torch.zeros(4, dtype=torch.float64, device=self.dev)  # K, alpha, R1, S of the last step
         self.mass = t(self.mass_np)
         self.counter = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.ind = self.ff.init_induction()
@@ -168,8 +176,14 @@ class PIMD:
         n3 = 3 * self.P * self.n
         with torch.cuda.stream(self.stream):
             _lib.check(lib.pgm_pimd_kick(st, n3, h, _p(self.forces), _p(self.p)))
-            _lib.check(lib.pgm_pimd_free_thermostat(st, self.P, self.n, _p(self.C), _p(self.omega), _p(self.gamma), _p(self.mass),
-                                                    self.dt, self.ring.kT_P, self.seed, _p(self.counter), _p(self.q), _p(self.p)))
+            scale = None
+            if self.centroid_bussi:  # PILE-G: the centroid's Bussi factor from the momenta before the O step
+                _lib.check(lib.pgm_pimd_centroid_bussi(st, self.P, self.n, _p(self.C), _p(self.mass), self.dt, self.ring.kT_P,
+                                                       self.tau0, self.seed, _p(self.counter), _p(self.p), _p(self.bussi_work)))
+                scale = C.c_void_p(self.bussi_work.data_ptr() + 8)
+            _lib.check(lib.pgm_pimd_free_thermostat_scaled(st, self.P, self.n, _p(self.C), _p(self.omega), _p(self.gamma),
+                                                           _p(self.mass), self.dt, self.ring.kT_P, self.seed, _p(self.counter),
+                                                           _p(self.q), _p(self.p), scale))
             self._forces()
             _lib.check(lib.pgm_pimd_kick(st, n3, h, _p(self.forces), _p(self.p)))
 

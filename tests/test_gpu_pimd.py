@@ -44,6 +44,48 @@ def test_free_step_matches_numpy():
         assert int(cnt.item()) == 1
 
 
+def test_pile_g_centroid_factor_and_scaled_free_step():
+    """PILE-G on the device: the centroid kinetic energy and Bussi factor equal the restatement for
+    the draws the kernel reports, and the free step with the centroid rescaled equals the NumPy one."""
+    from pgm_jax_b200 import _lib
+    from pgm_jax_b200.pimd import RingPolymer
+
+    lib = _lib.load()
+    P, n, dt, tau = 8, 37, 0.0005, 0.2
+    ring = RingPolymer(P, 300.0)
+    rng = np.random.default_rng(11)
+    q, p = rng.normal(scale=0.01, size=(P, n, 3)), rng.normal(size=(P, n, 3))
+    m = rng.uniform(1, 16, size=n)
+    dq, dp = _t(q.reshape(-1, 3)), _t(p.reshape(-1, 3))
+    cnt = torch.full((1,), 7, dtype=torch.int64, device="cuda")
+    work = torch.zeros(4, dtype=torch.float64, device="cuda")
+    keep = [_t(ring.C), _t(ring.omega), _t(np.zeros(P)), _t(m)]
+    _lib.check(lib.pgm_pimd_centroid_bussi(None, P, n, _p(keep[0]), _p(keep[3]), dt, ring.kT_P, tau, 5, _p(cnt), _p(dp), _p(work)))
+    torch.cuda.synchronize()
+    K, alpha, r1, S = work.cpu().numpy()
+    assert abs(K - PO.centroid_kinetic(p, ring.C, m)) <= 1e-12 * K
+    assert S > 0 and abs(alpha - PO.bussi_factor(K, ring.kT_P, 3 * n, dt, tau, r1, S)) <= 1e-13
+    _lib.check(lib.pgm_pimd_free_thermostat_scaled(None, P, n, *[_p(k) for k in keep], dt, ring.kT_P, 5, _p(cnt), _p(dq), _p(dp),
+                                                   C.c_void_p(work.data_ptr() + 8)))
+    torch.cuda.synchronize()
+    qr, pr = PO.free_step_centroid_scaled(q, p, ring.C, ring.omega, m, dt, alpha)
+    assert np.abs(dq.cpu().numpy().reshape(P, n, 3) - qr).max() <= 1e-13
+    assert np.abs(dp.cpu().numpy().reshape(P, n, 3) - pr).max() <= 1e-11 * np.abs(pr).max()
+    assert int(cnt.item()) == 8
+    # the device draws: R1 ~ N(0, 1) and S ~ chi^2(3n - 1) over many steps
+    r1s, ss = [], []
+    for step in range(400):
+        cnt.fill_(1000 + step)
+        _lib.check(lib.pgm_pimd_centroid_bussi(None, P, n, _p(keep[0]), _p(keep[3]), dt, ring.kT_P, tau, 5, _p(cnt), _p(dp),
+                                               _p(work)))
+        w = work.cpu().numpy()
+        r1s.append(w[2]); ss.append(w[3])
+    r1s, ss = np.array(r1s), np.array(ss)
+    dof1 = 3 * n - 1
+    assert abs(r1s.mean()) < 4 / np.sqrt(len(r1s)) and abs(r1s.std() - 1) < 0.15
+    assert abs(ss.mean() - dof1) < 4 * np.sqrt(2 * dof1 / len(ss)) and abs(ss.var() / (2 * dof1) - 1) < 0.3
+
+
 def test_water_bonded_forces():
     from pgm_jax_b200 import _lib
     from pgm_jax_b200.pimd import QTIP4PF
@@ -70,7 +112,7 @@ def test_water_bonded_forces():
     assert np.allclose(e.cpu().numpy(), E, rtol=1e-12)
 
 
-def _pimd(mode, P, prec, seed=1, dt_fs=0.25, n_side=3, edge=0.95):
+def _pimd(mode, P, prec, seed=1, dt_fs=0.25, n_side=3, edge=0.95, centroid="l"):
     from pgm_jax_b200.forcefield import MDSettings
     from pgm_jax_b200.pimd import PIMD
     from pgm_jax_b200.systems import water_box
@@ -78,7 +120,7 @@ def _pimd(mode, P, prec, seed=1, dt_fs=0.25, n_side=3, edge=0.95):
     s, pos, H = water_box(n_side, edge, seed=seed)
     st = MDSettings(precision=prec, cutoff=0.45, ewald_beta=7.0, pme_grid=(32, 32, 32), dipole_tol=1e-10 if prec == "double" else 1e-6,
                     max_iter=200)
-    return PIMD(s, pos, H, st, beads=P, temperature=300.0, dt_fs=dt_fs, mode=mode, seed=seed)
+    return PIMD(s, pos, H, st, beads=P, temperature=300.0, dt_fs=dt_fs, mode=mode, seed=seed, centroid=centroid)
 
 
 def test_rpmd_conserves_the_ring_polymer_hamiltonian_and_graphs_replay_steps():
@@ -126,3 +168,21 @@ def test_pile_holds_internal_modes_at_temperature():
     internal = t[:, 1:].mean()
     assert abs(internal / 300.0 - 1.0) < 0.05, t.mean(0)
     assert not int(pm.result.status.max()) & 0x6
+
+
+def test_pile_g_holds_every_mode_at_temperature():
+    """PILE-G: Bussi's centroid rescaling (tight, tau 0.01 ps, against the heat the relaxing lattice
+    start releases) and the internal modes' Langevin keep the centroid and the internal modes near T
+    once the start has relaxed (0.4 ps)."""
+    pm = _pimd("pimd", 8, "mixed", dt_fs=0.5, n_side=4, edge=1.25, centroid="g")
+    pm.tau0 = 0.01
+    pm.capture()
+    pm.run(800)
+    t = []
+    for _ in range(60):
+        pm.run(5)
+        t.append(pm.estimators()["t_modes"])
+    t = np.array(t)
+    assert abs(t[:, 1:].mean() / 300.0 - 1.0) < 0.05, t.mean(0)
+    assert abs(t[:, 0].mean() / 300.0 - 1.0) < 0.1, t[:, 0].mean()
+    assert float(pm.bussi_work[1]) > 0 and not int(pm.result.status.max()) & 0x6

@@ -39,6 +39,24 @@ def test_frictions():
     assert np.all(frictions(ring, "rpmd") == 0)
     with pytest.raises(ValueError):
         frictions(ring, "nve")
+    g = frictions(ring, "pimd", 0.2, centroid="g")  # PILE-G: the centroid is Bussi's, not Langevin's
+    assert g[0] == 0 and np.allclose(g[1:], 2 * ring.omega[1:])
+    with pytest.raises(ValueError):
+        frictions(ring, "pimd", centroid="x")
+
+
+def test_bussi_factor_keeps_the_canonical_kinetic_energy():
+    """With exact draws, K alpha^2 has mean c K + (1 - c) K0 (Bussi's relaxation toward K0 = N_f kT / 2)."""
+    import pimd_oracle as PO
+
+    rng = np.random.default_rng(0)
+    dof, kT, h, tau, K = 300.0, 2.5, 0.0005, 0.2, 500.0
+    K0 = 0.5 * dof * kT
+    a = np.array([PO.bussi_factor(K, kT, dof, h, tau, rng.normal(), rng.chisquare(dof - 1)) for _ in range(100000)])
+    c = np.exp(-h / tau)
+    mean = np.mean(K * a * a)
+    assert abs(mean - (c * K + (1 - c) * K0)) < 4 * np.std(K * a * a) / np.sqrt(len(a))
+    assert np.all(a > 0)  # far from K = 0 the factor keeps its sign
 
 
 def test_oracle_free_step_conserves_every_mode():
