@@ -1796,13 +1796,7 @@ __device__ __forceinline__ void cg_update_body(Dev<T> &a) {
   }
 }
 
-template <typename T>
-__global__ void k_cg_update(Dev<T> a) {
-  pdl_enter();
-  cg_update_body(a);
-}
-
-// The per-system scalars after an update (the body of k_cg_check, run by one block).
+// The per-system scalars after an update (run by the last block of k_cg_update_check).
 __device__ __forceinline__ void cg_check_body(CGSys *cg, int nsys, double tol, int max_iter, int *any,
                                               cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ int act;
@@ -1827,7 +1821,7 @@ __device__ __forceinline__ void cg_check_body(CGSys *cg, int nsys, double tol, i
   }
 }
 
-// k_cg_update and k_cg_check in one launch: every block adds its partial sums, and the block that
+// The CG update and the per-system check in one launch: every block adds its partial sums, and the block that
 // finishes last (a counter after a memory fence) evaluates the per-system scalars and the loop
 // condition, then resets the counter for the next iteration.
 template <typename T>
@@ -1846,12 +1840,6 @@ __global__ void k_cg_update_check(Dev<T> a, int nsys, double tol, int max_iter, 
   __threadfence();
   cg_check_body(a.cg, nsys, tol, max_iter, any, cond, use_cond);
   if (threadIdx.x == 0) *done = 0u;
-}
-
-__global__ void k_cg_check(CGSys *cg, int nsys, double tol, int max_iter, int *any, cudaGraphConditionalHandle cond,
-                           int use_cond) {
-  pdl_enter();
-  cg_check_body(cg, nsys, tol, max_iter, any, cond, use_cond);
 }
 
 // After the loop: the peek step mu = x + peek alpha r (forcefield.py:1819-1820), the dipoles
