@@ -180,7 +180,7 @@ def cpu_reference(steps: int, warmup: int, budget_s: float = 120.0):
     times, iters = [], []
     t_start = time.perf_counter()
     n = 0
-    while n < max(1, steps):
+    while len(times) < max(1, steps):  # min(warmup, 1) untimed steps, then the timed ones (time-boxed)
         x = x + rng.normal(scale=2e-4, size=x.shape)  # a moving geometry, so the predictor works as in MD
         t0 = time.perf_counter()
         r = o.compute(x, H, ind)
