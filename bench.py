@@ -1,18 +1,19 @@
 """Benchmark: pGM rigid-water MD on the B200 engine, ns/day and CG iterations per step, with the
 learned initial guess against plain CG.
 
-Workload (one GPU): 4096 pGM3P-25 waters (12,288 atoms) on a seeded jittered 16^3 lattice in a
-4.966 nm cubic box, cutoff 0.9 nm, Ewald 4.0 / nm, PME 96^3 order 6, mixed precision (FP32 pair /
-PME / CG vectors, FP64 reductions), Langevin NVT 298 K with gamma 2 / ps, dt 1 fs, CG to max|alpha
-r| / mean|alpha b| <= 1e-6.  A step is one captured CUDA graph: rigid-body kick/drift/Langevin, the
-force call (rows, PME, CG as a device-side while loop, energy / forces / virial), closing kick.
+Headline workload (one GPU): 32,768 pGM3P-25 waters (98,304 atoms) on a seeded jittered 32^3
+lattice in a 9.93 nm cubic box, cutoff 0.9 nm, Ewald 4.0 / nm, PME 192^3 order 6, mixed precision
+(FP32 pair / PME / CG vectors, FP64 reductions), Langevin NVT 298 K with gamma 2 / ps, dt 1 fs, CG to
+max|alpha r| / mean|alpha b| <= 1e-6.  A step is one captured CUDA graph: rigid-body kick/drift/
+Langevin, the force call (rows, PME, CG as a device-side while loop, energy / forces / virial),
+closing kick.  `--workload water4096` runs the same line on 4,096 waters (4.966 nm, PME 96^3).
 
-The headline run starts every solve from the learned guess (mu4 + the model's correction, fused
-start): plain-solver MD on the same workload writes the training pairs, the model trains on the GPU
-(outside the timed region), then the timed MD uses it.  Beside it, the same MD with plain CG from
-the previous step's dipoles (mu1) and from the reference's default mu4 predictor.
+The headline run starts every solve from the learned guess: plain-solver MD on the 4,096-water box
+writes the training pairs, the model trains on the GPU (outside the timed region), then the timed
+MD uses it.  Beside it, the same MD with plain CG from the previous step's dipoles (mu1) and from
+the reference's default mu4 predictor.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
 
 With N > 1 (torchrun, one process per GPU) every rank runs its own independent replica (the path
 has no exchange step: replicas only); value = total ns/day over the ranks, time = max over ranks.
@@ -36,33 +37,50 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_SIDE, EDGE_NM, GRID = 16, 4.966, 96
 DT_FS, GAMMA, TEMP, TOL = 1.0, 2.0, 298.0, 1e-6
 METRIC = "ns/day & CG iters/step on 1 B200: NN-guess vs plain CG at residual≤1e-6"
-CONFIG = {
-    "workload": "4096 rigid pGM3P-25 waters, 4.966 nm box, PME 96^3 o6, rc 0.9 nm, beta 4.0/nm, Langevin 298 K "
-    "gamma 2/ps, dt 1 fs, mixed precision, CG tol 1e-6 from the learned guess",
-    "atoms": 12288,
-    "pme_grid": [GRID, GRID, GRID],
-    "cutoff_nm": 0.9,
-    "dt_fs": DT_FS,
-    "cg_tol": TOL,
-    "solver": "CG from mu4 + the learned correction (fused start); plain CG from mu1 and mu4 beside it",
-    "l2": "working set larger than L2: pair rows 8 x 4 B x 12288 x capacity = 164 MB (126 MB L2)",
-    "seeds": {"positions": 0, "velocities_thermostat": 1},
-    "equilibration": "1000 steps of 1 fs at gamma 20/ps from the lattice start, before training and timing",
+
+# water boxes of the MD line: lattice side, box edge [nm], PME mesh
+BOXES = {
+    "water32768": {"n_side": 32, "edge": 9.93, "grid": 192, "atoms": 98304,
+                   "equil_steps": 500, "published": None},
+    "water4096": {"n_side": 16, "edge": 4.966, "grid": 96, "atoms": 12288, "equil_steps": 1000,
+                  "published": "44 ns/day, 4096 waters, mixed, tol 1e-5, 1x RTX PRO 6000 Blackwell (README.md:448)"},
 }
+W = dict(BOXES["water32768"], name="water32768")  # the workload of this run (set from --workload)
+TRAIN_BOX = "water4096"  # the learned guess trains on pairs written by the plain solver on this box
 
 
-EQUIL_STEPS, EQUIL_GAMMA = 1000, 20.0  # relaxation of the lattice start before any data or timing
+def config() -> dict:
+    n_w = W["atoms"] // 3
+    K = W["grid"]
+    return {
+        "workload": f"{n_w} rigid pGM3P-25 waters, {W['edge']} nm box, PME {K}^3 o6, rc 0.9 nm, beta 4.0/nm, Langevin "
+        "298 K gamma 2/ps, dt 1 fs, mixed precision, CG tol 1e-6 from the learned guess (trained on 4096-water frames)",
+        "atoms": W["atoms"],
+        "pme_grid": [K, K, K],
+        "cutoff_nm": 0.9,
+        "dt_fs": DT_FS,
+        "cg_tol": TOL,
+        "solver": "CG from mu4 + the learned correction (fused start); plain CG from mu1 and mu4 beside it",
+        "l2": f"working set larger than L2: pair rows 8 x 4 B x {W['atoms']} x capacity "
+        f"= {8 * 4 * W['atoms'] * 416 / 1e6:.0f} MB (126 MB L2)",
+        "seeds": {"positions": 0, "velocities_thermostat": 1},
+        "equilibration": f"{W['equil_steps']} steps of 1 fs at gamma 20/ps from the lattice start, before timing",
+        **({"split_rows": f"electrostatics {SPLIT['elec_cutoff']} nm, beta {SPLIT['ewald_beta']:.4f}/nm, LJ 0.9 nm"}
+           if SPLIT else {}),
+    }
 
 
-def equilibrate(md, steps: int = EQUIL_STEPS) -> None:
+EQUIL_GAMMA = 20.0  # relaxation of the lattice start before any data or timing
+
+
+def equilibrate(md, steps: int | None = None) -> None:
     """Relax the lattice start (random orientations) with direct steps under a strong thermostat
     (gamma 20 / ps, then back to the run's gamma), outside any timed region."""
     g = md.gamma
     md.gamma = EQUIL_GAMMA
-    for _ in range(steps):
+    for _ in range(W["equil_steps"] if steps is None else steps):
         md.step()
     md.gamma = g
     md.stream.synchronize()
@@ -73,14 +91,21 @@ def equilibrate(md, steps: int = EQUIL_STEPS) -> None:
 ROWFIELD_NCU_DRAM_BYTES, ROWFIELD_NCU_PAIRS = 93.654784e6 + 3.39328e6, 3.745e6
 
 
-SPLIT: dict = {}  # --elec-cutoff: split rows (elec_cutoff, ewald_beta for it; the 96^3 mesh fits its spacing)
+SPLIT: dict = {}  # --elec-cutoff: split rows (elec_cutoff, ewald_beta for it; the meshes fit its spacing)
 
 
-def settings(precision="mixed", predictor="mu4"):
+def settings(precision="mixed", predictor="mu4", grid=None):
     from pgm_jax_b200.forcefield import MDSettings
 
-    return MDSettings(precision=precision, cutoff=0.9, ewald_beta=SPLIT.get("ewald_beta", 4.0), pme_grid=(GRID, GRID, GRID),
+    K = W["grid"] if grid is None else grid
+    return MDSettings(precision=precision, cutoff=0.9, ewald_beta=SPLIT.get("ewald_beta", 4.0), pme_grid=(K, K, K),
                       pme_order=6, dipole_tol=TOL, max_iter=100, predictor=predictor, elec_cutoff=SPLIT.get("elec_cutoff"))
+
+
+def headline_box(seed: int = 0):
+    from pgm_jax_b200.systems import water_box
+
+    return water_box(W["n_side"], W["edge"], seed=seed)
 
 
 def ns_per_day(ms_per_step: float) -> float:
@@ -163,31 +188,40 @@ def dist_env():
     return ws, rank, local
 
 
+def drift_frames(s, pos, seed: int = 1):
+    """Frames of a smooth trajectory for the CPU leg: every molecule translated at a Maxwell velocity
+    (298 K) by 1 fs per frame, so that the predictor extrapolates a smooth history as in MD."""
+    rng = np.random.default_rng(seed)
+    mw = float(s.masses[s.mol == 0].sum())  # every molecule of the box is a water
+    v = rng.normal(scale=np.sqrt(0.0083144626 * TEMP / mw), size=(s.nmol, 3))[s.mol]  # nm/ps
+    return lambda k: pos + v * (k * DT_FS * 1e-3)
+
+
 def cpu_reference(steps: int, warmup: int, budget_s: float = 120.0):
-    """The FP64 CPU oracle (restatement of the reference's algorithm) on the same workload."""
+    """The FP64 CPU oracle (restatement of the reference's algorithm) on the same workload: the
+    first four frames of a smooth trajectory fill the predictor's history untimed, then up to
+    `steps` force steps are timed, time-boxed to `budget_s`."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O  # noqa: E402  (the checker; this is the reference arm / CPU baseline)
 
-    from pgm_jax_b200.systems import water_box
-
-    s, pos, H = water_box(N_SIDE, EDGE_NM, seed=0)
-    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(GRID, GRID, GRID), pme_order=6, dipole_tol=TOL, max_iter=100)
+    s, pos, H = headline_box()
+    K = W["grid"]
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(K, K, K), pme_order=6, dipole_tol=TOL, max_iter=100)
     cores = os.cpu_count() or 1
     o = O.Oracle(s, st, nthreads=cores)
     ind = o.init_induction()
-    rng = np.random.default_rng(1)
-    x = pos.copy()
+    frame = drift_frames(s, pos)
+    n_fill = 4  # mu4 extrapolates once the history holds four steps (forcefield.py:1917-2008)
     times, iters = [], []
     t_start = time.perf_counter()
-    n = 0
-    while len(times) < max(1, steps):  # min(warmup, 1) untimed steps, then the timed ones (time-boxed)
-        x = x + rng.normal(scale=2e-4, size=x.shape)  # a moving geometry, so the predictor works as in MD
+    k = 0
+    while len(times) < max(1, steps):
         t0 = time.perf_counter()
-        r = o.compute(x, H, ind)
+        r = o.compute(frame(k), H, ind)
         dt = time.perf_counter() - t0
         ind = r["induction"]
-        n += 1
-        if n > min(warmup, 1):
+        k += 1
+        if k > n_fill:
             times.append(dt)
             iters.append(r["iterations"])
         if time.perf_counter() - t_start > budget_s and times:
@@ -196,8 +230,9 @@ def cpu_reference(steps: int, warmup: int, budget_s: float = 120.0):
     return {
         "value": ns_per_day(ms), "ms_per_step": ms, "cores": cores, "steps_timed": len(times),
         "cg_iters_per_step": float(np.mean(iters)),
-        "sample": f"{len(times)} force steps of the 4096-water workload (FP64 oracle, {cores} threads, after "
-        f"{min(warmup, 1)} untimed); the rigid-body integrator's cost (<1%) is not included",
+        "sample": f"{len(times)} force steps of the {W['atoms'] // 3}-water workload (FP64 oracle, {cores} threads, "
+        f"mu4 predictor, CG 1e-6) on a smooth drift trajectory, after {n_fill} untimed steps that fill the history; "
+        "the rigid-body integrator's cost (<1%) is not included",
     }
 
 
@@ -208,9 +243,9 @@ def run_reference(args) -> None:
     r = cpu_reference(args.steps, args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "ns/day", "n_gpus": args.gpus,
-        "steps": r["steps_timed"], "warmup": min(args.warmup, 1), "ms_per_step": r["ms_per_step"],
+        "steps": r["steps_timed"], "warmup": 4, "ms_per_step": r["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": CONFIG, "cg_iters_per_step": r["cg_iters_per_step"],
+        "config": config(), "cg_iters_per_step": r["cg_iters_per_step"],
         "cpu_baseline": {"value": r["value"], "unit": "ns/day", "cores": r["cores"], "kind": "port", "sample": r["sample"]},
         "e2e": {"value": r["value"], "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (JAX) is not installable here (no jax/jax_md wheels, no network); its algorithm is "
@@ -219,26 +254,56 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def train_guess(rank: int, torch) -> tuple:
+    """Plain-solver MD on the 4,096-water box writes (features, mu* - mu4 guess) pairs; the model
+    trains on the GPU.  Returns the model and what was trained."""
+    from pgm_jax_b200.forcefield import PGMForceField
+    from pgm_jax_b200.learned import GuessModel, collect
+    from pgm_jax_b200.md import RigidMD
+    from pgm_jax_b200.systems import water_box
+
+    t0 = time.perf_counter()
+    B = BOXES[TRAIN_BOX]
+    s, pos, H = water_box(B["n_side"], B["edge"], seed=0)
+    ff = PGMForceField(s, H, settings(predictor="nn", grid=B["grid"]), device=torch.cuda.current_device())
+    md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
+    equilibrate(md, B["equil_steps"])
+    frames, iters = 64, 2000
+    train = collect(md, frames)
+    model = GuessModel(seed=0, device=torch.cuda.current_device())
+    model.train(train, iters=iters, batch=32768, lr=2e-3)
+    info = {"train_box": f"{B['atoms'] // 3} waters, {B['edge']} nm, PME {B['grid']}^3", "train_frames": frames,
+            "train_pairs": int(train["inv"].shape[0]), "adam_steps": iters, "seconds": time.perf_counter() - t0}
+    del md, ff, train
+    return model, info
+
+
 def run_engine(args) -> None:
     import torch
     import torch.distributed as dist
 
     from pgm_jax_b200 import _lib
     from pgm_jax_b200.forcefield import PGMForceField
+    from pgm_jax_b200.learned import collect, guess_errors
     from pgm_jax_b200.md import RigidMD
-    from pgm_jax_b200.systems import water_box
 
     ws, rank, local = dist_env()
     if ws > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    s, pos, H = water_box(N_SIDE, EDGE_NM, seed=0)
+    model, train_info = train_guess(rank, torch) if args.nn else (None, None)
+    s, pos, H = headline_box()
     ff = PGMForceField(s, H, settings(predictor="nn" if args.nn else "mu4"), device=local)
     md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
     lib = ff._lib
     equilibrate(md)
-    train_info = train_guess(md, ff) if args.nn else None  # plain-solver MD writes the data; GPU training
+    if args.nn:  # held-out frames of this box (plain solver: the model is not installed yet)
+        held = collect(md, 6)
+        train_info["guess_rms_e_nm_held_out"] = guess_errors(model, held)
+        train_info["start"] = "x0 = mu4 + the model's correction, fused start (one field sweep, as mu4)"
+        del held
+        model.install(ff)
     # warm-up: direct steps (rows sized), then capture and replay
     for _ in range(max(1, args.warmup)):
         md.step()
@@ -251,7 +316,8 @@ def run_engine(args) -> None:
     # the clock sampler starts while warm-up replays keep the GPU busy, so that the timed region
     # begins on a loaded GPU at its running clocks (not after an idle gap)
     clk = Clocks(local)
-    md.run(max(3, args.warmup) + 200)
+    n_pre = max(3, args.warmup) + 50
+    md.run(n_pre)
     # timed region: K graph replays between CUDA events on the MD stream; clocks sampled meanwhile
     if ws > 1:
         dist.barrier()
@@ -261,7 +327,7 @@ def run_engine(args) -> None:
     clk.mark(t_wall, time.time())
     clocks = clk.stop()
     rebuilds = int(lib.pgm_list_rebuilds(ff._h)) - builds0  # over the last warm-up replays and the timed ones
-    rebuilds_steps = args.steps + max(3, args.warmup) + 200
+    rebuilds_steps = args.steps + n_pre
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if ws > 1:
         dist.barrier()
@@ -281,9 +347,7 @@ def run_engine(args) -> None:
     peak, peak_kind = peaks()
     mv_bytes = 24.0 * pairs + 32.0 * ff.n  # rows (k, x, y, z, G1, G2) + the dipole vector in and out
     mv_gbs = mv_bytes / (kt["row_field"] * 1e-3) / 1e9
-    step_bytes = bytes_per_step(ff.n, pairs, n_it, GRID)
-    # end to end: the force call through the C ABI with host buffers (positions in, forces out and
-    # the induction state in and out every step), the integrator on the GPU
+    step_bytes = bytes_per_step(ff.n, pairs, n_it, W["grid"])
     # three MD steps launched directly (the CG loop driven from the host), untimed, in their own
     # NVTX range: a profiler cannot see the kernels of graphs with conditional nodes
     with torch.cuda.stream(md.stream):
@@ -292,17 +356,22 @@ def run_engine(args) -> None:
             md.step()
         md.stream.synchronize()
         torch.cuda.nvtx.range_pop()
+    # end to end: the force call through the C ABI with host buffers (positions in, forces out; the
+    # induction state on the device, or copied in and out every step), the integrator on the GPU
     e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
     e2e_host_state = run_e2e(md, ff, args.steps, torch, lib, _lib, state_on_device=False)
-    acc = accuracy_vs_fp64(s, H, md, torch)
+    final = {"pos": md.pos.cpu().numpy(), "box": md.box[0].cpu().numpy(),
+             "ind": {k: getattr(md.ind, k).cpu().numpy() for k in ("mu", "hist", "count", "norm")}}
+    del md
     # plain CG on the same workload: from the previous step's dipoles and from mu4
     plain = {p: run_plain(s, pos, H, rank, p, args, torch) for p in (("mu1", "mu4") if args.nn else ())}
+    acc = accuracy_vs_oracle(s, final, torch) if (rank == 0 and args.cpu_baseline) else None
     value = ws * ns_per_day(ms_max)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic", "config": CONFIG, "cg_iters_per_step": n_it, "cg_iters_first_step": it0,
+            "data": "synthetic", "config": config(), "cg_iters_per_step": n_it, "cg_iters_first_step": it0,
             "status": status, "gpu_launches": int(round(launches)), "list_rebuilds_per_step": rebuilds / rebuilds_steps,
             "clocks": clocks,
             "roofline": {
@@ -313,45 +382,64 @@ def run_engine(args) -> None:
                 "step_bytes": step_bytes, "step_gbs": step_bytes / (ms_max * 1e-3) / 1e9,
                 "step_frac": step_bytes / (ms_max * 1e-3) / 1e9 / peak,
             },
-            "kernel_ms": kt, "pairs": pairs, "row_capacity": ff.capacity, "accuracy_vs_fp64": acc,
+            "kernel_ms": kt, "pairs": pairs, "row_capacity": ff.capacity, "accuracy_vs_oracle": acc,
             "e2e": e2e,
             "e2e_host_state": {k: e2e_host_state[k] for k in ("value", "unit", "ms_per_step", "h2d_bytes_per_step",
                                                               "d2h_bytes_per_step", "path")},
-            "published_reference": "44 ns/day, 4096 waters, mixed, tol 1e-5, 1x RTX PRO 6000 Blackwell (README.md:448)",
+            "published_reference": W["published"],
         }
         if args.nn:
             line["learned_guess"] = train_info
             line["plain_cg"] = plain
             line["nn_over_plain_cg"] = {p: ns_per_day(ms_max) / v["value"] for p, v in plain.items()}
         if args.cpu_baseline:
-            r = cpu_reference(3, 1, budget_s=40.0)
+            r = cpu_reference(2, 1, budget_s=30.0)
             line["cpu_baseline"] = {"value": r["value"], "unit": "ns/day", "cores": r["cores"], "kind": "port",
                                     "sample": r["sample"]}
         print(json.dumps(line), flush=True)
-    del md
+    del ff
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def accuracy_vs_fp64(s, H, md, torch) -> dict:
-    """Mixed precision (the timed path, CG 1e-6) against the FP64 engine (CG 1e-10) at the MD's
-    current coordinates, both started from the same converged dipoles' history-free plain start."""
-    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+def accuracy_vs_oracle(s, final: dict, torch, grid=None, label: str = "the final MD frame") -> dict:
+    """Mixed precision (the timed path: FP32 kernels, FP64 reductions, CG 1e-6) and the FP64 engine
+    (CG 1e-8) against the FP64 oracle (CG 1e-8) at the same coordinates, all three started from the
+    MD's induction state at that frame (mu4 from its history)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402  (the checker)
 
-    md.stream.synchronize()
-    pos = md.pos.clone()
+    from pgm_jax_b200.forcefield import InductionState, MDSettings, PGMForceField
+
+    pos, H, ind = final["pos"], final["box"], final["ind"]
     dev = torch.cuda.current_device()
-    st = settings()
-    mixed = PGMForceField(s, H, MDSettings(**{**st.__dict__, "predictor": "none"}), device=dev).compute(pos, H)
-    ref = PGMForceField(s, H, MDSettings(**{**st.__dict__, "predictor": "none", "precision": "double", "dipole_tol": 1e-10}),
-                        device=dev).compute(pos, H)
-    rms = lambda a, b: float(torch.sqrt(torch.mean((a - b) ** 2)) / torch.sqrt(torch.mean(b**2)))  # noqa: E731
-    e_m, e_r = float(mixed.energy["total"][0]), float(ref.energy["total"][0])
-    return {"energy_rel": abs(e_m - e_r) / abs(e_r), "forces_rms_rel": rms(mixed.forces, ref.forces),
-            "mu_rms_rel": rms(mixed.induction.mu, ref.induction.mu), "fp64_energy_kjmol": e_r,
-            "note": "mixed (FP32 kernels, FP64 reductions, CG 1e-6) vs FP64 engine (CG 1e-10) at the final MD frame; "
-            "the FP64 engine matches the FP64 oracle in the parity tests"}
+    st = settings(grid=grid)
+    K = st.pme_grid
+    t0 = time.perf_counter()
+    o = O.Oracle(s, dict(cutoff=0.9, ewald_beta=4.0, pme_grid=K, pme_order=6, dipole_tol=1e-8, max_iter=100),
+                 nthreads=os.cpu_count() or 1)
+    ref = o.compute(pos, H, {k: (np.array(v) if k in ("mu", "hist") else (int(v[0]) if k == "count" else float(v[0])))
+                             for k, v in ind.items()})
+    t_oracle = time.perf_counter() - t0
+
+    def engine(prec, tol):
+        ff = PGMForceField(s, H, MDSettings(**{**st.__dict__, "predictor": "mu4", "precision": prec, "dipole_tol": tol}),
+                           device=dev)
+        st_in = InductionState(*(torch.as_tensor(ind[k], device=ff.device) for k in ("mu", "hist", "count", "norm")))
+        return ff.compute(pos, H, None, st_in)
+
+    rms = lambda a, b: float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b**2)))  # noqa: E731
+    out = {"frame": label, "oracle_energy_kjmol": ref["energy"]["total"], "oracle_iterations": ref["iterations"],
+           "oracle_seconds": t_oracle}
+    for name, prec, tol in (("mixed_tol1e-6", "mixed", TOL), ("fp64_tol1e-8", "double", 1e-8)):
+        r = engine(prec, tol)
+        e = float(r.energy["total"][0])
+        out[name] = {"energy_rel": abs(e - ref["energy"]["total"]) / abs(ref["energy"]["total"]),
+                     "forces_rms_rel": rms(r.forces.cpu().numpy(), ref["forces"]),
+                     "mu_rms_rel": rms(r.induction.mu.cpu().numpy(), ref["mu"]), "iterations": int(r.iterations[0])}
+        del r
+    return out
 
 
 def timed_replays(md, steps: int, torch, label: str | None = None) -> tuple:
@@ -373,25 +461,6 @@ def timed_replays(md, steps: int, torch, label: str | None = None) -> tuple:
     return ev0.elapsed_time(ev1) / steps, float(it_sum.item()) / steps
 
 
-def train_guess(md, ff, frames: int = 64, held_frames: int = 8, iters: int = 2000) -> dict:
-    """Plain-solver MD (mu4 until a model is installed) writes (features, mu* - mu4 guess) pairs;
-    the model trains on the GPU and is installed; guess errors on held-out frames."""
-    from pgm_jax_b200.learned import GuessModel, collect, guess_errors
-
-    t0 = time.perf_counter()
-    train = collect(md, frames)
-    held = collect(md, held_frames)
-    model = GuessModel(seed=0, device=ff.device.index)
-    before = guess_errors(model, held)
-    model.train(train, iters=iters, batch=32768, lr=2e-3)
-    after = guess_errors(model, held)
-    model.install(ff)
-    return {"train_frames": frames, "train_pairs": int(train["inv"].shape[0]), "adam_steps": iters,
-            "seconds": time.perf_counter() - t0,
-            "guess_rms_e_nm_held_out": {"mu1": before["mu1"], "mu4": before["mu4"], "mu4_plus_model": after["model"]},
-            "start": "x0 = mu4 + the model's correction, fused start (one field sweep, as mu4)"}
-
-
 def run_plain(s, pos, H, rank, predictor, args, torch) -> dict:
     """The same MD with plain CG from `predictor`, graph-replayed and timed like the headline."""
     from pgm_jax_b200.forcefield import PGMForceField
@@ -407,7 +476,7 @@ def run_plain(s, pos, H, rank, predictor, args, torch) -> dict:
     md.stream.synchronize()
     steps = max(10, min(args.steps, 300))
     ms, n_it = timed_replays(md, steps, torch)
-    del md
+    del md, ff
     return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "cg_iters_per_step": n_it, "steps": steps,
             "predictor": {"mu1": "previous step's dipoles", "mu4": "4 mu1 - 6 mu2 + 4 mu3 - mu4 (the reference's default)"}[
                 predictor]}
@@ -501,6 +570,16 @@ def batch_workload():
     return boxes, grids, np.array(temps), ladder
 
 
+def system_frame(md, k: int) -> dict:
+    """Positions, box and induction state of system k of a batched MD (host arrays)."""
+    md.stream.synchronize()
+    o = md.ff.offsets
+    sl = slice(int(o[k]), int(o[k + 1]))
+    return {"pos": md.pos[sl].cpu().numpy(), "box": md.box[k].cpu().numpy(),
+            "ind": {"mu": md.ind.mu[sl].cpu().numpy(), "hist": md.ind.hist[:, sl].cpu().numpy(),
+                    "count": md.ind.count[k:k + 1].cpu().numpy(), "norm": md.ind.norm[k:k + 1].cpu().numpy()}}
+
+
 def make_md(boxes, grids, temps, predictor, rank, torch, gamma=GAMMA):
     from pgm_jax_b200.forcefield import PGMForceField
     from pgm_jax_b200.md import RigidMD
@@ -514,8 +593,8 @@ def make_md(boxes, grids, temps, predictor, rank, torch, gamma=GAMMA):
 
 def run_workload(args) -> None:
     """--workload batch: the uneven boxes + REMD replicas in one launch, exchanges every 100 steps
-    inside the timed region.  --workload water32768: 32,768 waters (9.93 nm, PME 192^3), the learned
-    guess (trained on the 4096-water workload) against plain CG from mu1 and mu4."""
+    inside the timed region.  --workload npt: the 4,096-water MD with Monte Carlo volume moves.
+    --workload pimd: 32 beads x 1,024 flexible waters."""
     import torch
 
     from pgm_jax_b200 import _lib
@@ -561,6 +640,8 @@ def run_workload(args) -> None:
             "cg_iters_per_step_mean": float(its.mean()), "cg_iters_per_step_max": float(its.max()),
             "exchange_acceptance": rex.stats.neighbour_acceptance().tolist(), "exchanges": rex.stats.n_exchanges,
             "status_any": int(md.result.status.max()), "clocks": clocks, "row_capacity": ff.capacity,
+            "accuracy_vs_oracle": accuracy_vs_oracle(boxes[12][0], system_frame(md, 12), torch, grid=72,
+                                                     label="the final frame of the first 2197-water box (72^3)"),
             "config": {"workload": "4 x (216 @ 1.86 nm, 32^3; 512 @ 2.48 nm, 48^3; 1000 @ 3.10 nm, 64^3; 2197 @ 4.04 nm, "
                        "72^3) at 298 K + 32 x 512 waters REMD 280-400 K (geometric), one engine, mixed, CG 1e-6 from mu4, "
                        "Langevin 2/ps, dt 1 fs, exchanges every 100 steps (timed)", "equilibration": "500 steps at 20/ps"},
@@ -570,10 +651,11 @@ def run_workload(args) -> None:
         from pgm_jax_b200.forcefield import PGMForceField
         from pgm_jax_b200.md import RigidMD
 
-        s, pos, H = water_box(N_SIDE, EDGE_NM, seed=0)
-        ff = PGMForceField(s, H, settings(predictor="mu4"), device=0)
+        B = BOXES["water4096"]
+        s, pos, H = water_box(B["n_side"], B["edge"], seed=0)
+        ff = PGMForceField(s, H, settings(predictor="mu4", grid=B["grid"]), device=0)
         md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1)
-        equilibrate(md)
+        equilibrate(md, B["equil_steps"])
         for _ in range(4):
             md.step()
         md.capture()
@@ -635,6 +717,10 @@ def run_workload(args) -> None:
         clocks = clk.stop()
         ms = ev0.elapsed_time(ev1) / steps
         est = pm.estimators()
+        bead0 = {"pos": pm.q[: pm.n].cpu().numpy(), "box": pm.box[0].cpu().numpy(),
+                 "ind": {"mu": pm.ind.mu[: pm.n].cpu().numpy(), "hist": pm.ind.hist[:, : pm.n].cpu().numpy(),
+                         "count": pm.ind.count[:1].cpu().numpy(), "norm": pm.ind.norm[:1].cpu().numpy()}}
+        line["accuracy_vs_oracle"] = accuracy_vs_oracle(s, bead0, torch, grid=64, label="bead 0 of the final frame")
         line.update({
             "value": 86.4 * 0.5 / ms, "ms_per_step": ms, "steps": steps, "beads": 32, "atoms": 3072, "bead_atoms": 98304,
             "cg_iters_per_step_mean": float(it_sum.float().mean().item()) / steps, "clocks": clocks,
@@ -645,56 +731,6 @@ def run_workload(args) -> None:
                        "rc 0.9 nm, 300 K PILE-L (tau_centroid 0.2 ps), dt 0.5 fs, mixed, CG 1e-6 from mu4 per bead, "
                        "all beads in one engine", "equilibration": "805 steps from the lattice + free ring polymer start"},
         })
-    else:  # water32768
-        from pgm_jax_b200.forcefield import PGMForceField
-        from pgm_jax_b200.md import RigidMD
-
-        s4, p4, H4 = water_box(N_SIDE, EDGE_NM, seed=0)
-        ff4 = PGMForceField(s4, H4, settings(predictor="nn"), device=0)
-        md4 = RigidMD(ff4, p4, H4, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1)
-        equilibrate(md4)
-        from pgm_jax_b200.learned import GuessModel, collect, guess_errors
-
-        train = collect(md4, 64)
-        model = GuessModel(seed=0)
-        model.train(train, iters=2000, batch=32768, lr=2e-3)
-        del md4, ff4
-        big = [water_box(32, 9.93, seed=0)]
-        arms = {}
-        for pred in ("nn", "mu1", "mu4"):
-            ff, md = make_md(big, [(192, 192, 192)], [TEMP], pred, 0, torch)
-            equilibrate(md, 300)
-            info = None
-            if pred == "nn":
-                held = collect(md, 6)
-                info = guess_errors(model, held)
-                model.install(ff)
-            for _ in range(4):
-                md.step()
-            md.capture()
-            md.run(3)
-            md.stream.synchronize()
-            ms, n_it = timed_replays(md, max(10, min(args.steps, 200)), torch)
-            arms[pred] = {"value": ns_per_day(ms), "ms_per_step": ms, "cg_iters_per_step": n_it}
-            if info:
-                arms[pred]["guess_rms_e_nm_held_out"] = info
-            pairs = int(ff._lib.pgm_row_pairs(ff._h))
-            arms[pred]["step_bytes"] = bytes_per_step(ff.n, pairs, n_it, 192)
-            arms[pred]["step_frac_of_hbm"] = arms[pred]["step_bytes"] / (ms * 1e-3) / 1e9 / peaks()[0]
-            if pred == "mu4":  # the matvec's row stream at a size far above L2 (720 MB of rows per sweep)
-                v = C_double()
-                _lib.check(ff._lib.pgm_profile_kernel(ff._h, C_void_p(md.stream.cuda_stream), 7, 20, byref(v)))
-                mv_bytes = 24.0 * pairs + 32.0 * ff.n
-                arms[pred]["row_field_roofline"] = {"kernel": "k_rowfield", "bytes_per_launch": mv_bytes, "ms_per_launch": v.value,
-                                                    "achieved_gbs": mv_bytes / (v.value * 1e-3) / 1e9,
-                                                    "frac": mv_bytes / (v.value * 1e-3) / 1e9 / peaks()[0], "peak_gbs": peaks()[0]}
-            del md, ff
-        line.update({"value": arms["nn"]["value"], "ms_per_step": arms["nn"]["ms_per_step"],
-                     "cg_iters_per_step": arms["nn"]["cg_iters_per_step"], "arms": arms, "atoms": 98304,
-                     "nn_over_plain_cg": {p: arms["nn"]["value"] / arms[p]["value"] for p in ("mu1", "mu4")},
-                     "config": {"workload": "32768 rigid pGM3P-25 waters, 9.93 nm, PME 192^3 o6, rc 0.9 nm, Langevin 298 K "
-                                "2/ps, dt 1 fs, mixed, CG 1e-6; model trained on 64 frames of the 4096-water workload",
-                                "equilibration": "300 steps at 20/ps per arm"}})
     print(json.dumps(line), flush=True)
 
 
@@ -706,8 +742,9 @@ def main() -> None:
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
-    ap.add_argument("--workload", default="water4096", choices=["water4096", "batch", "water32768", "pimd", "npt"],
-                    help="water4096: the headline; the others print their own line (one GPU)")
+    ap.add_argument("--workload", default="water32768", choices=["water32768", "water4096", "batch", "pimd", "npt"],
+                    help="water32768: the headline; water4096 the same line on the smaller box; the others print "
+                    "their own line (one GPU)")
     ap.add_argument("--elec-cutoff", type=float, default=None,
                     help="split rows: electrostatics cutoff [nm] below the 0.9 nm LJ cutoff (Ewald coefficient for it)")
     args = ap.parse_args()
@@ -717,11 +754,12 @@ def main() -> None:
         from pgm_jax_b200.forcefield import elec_cutoff_settings
 
         SPLIT.update(elec_cutoff_settings(args.elec_cutoff))
-        CONFIG["workload"] += f"; split rows: electrostatics {args.elec_cutoff} nm, beta {SPLIT['ewald_beta']:.4f}/nm"
-        CONFIG["elec_cutoff_nm"] = args.elec_cutoff
+    if args.workload in BOXES:
+        W.clear()
+        W.update(BOXES[args.workload], name=args.workload)
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload != "water4096":
+    elif args.workload not in BOXES:
         run_workload(args)
     else:
         run_engine(args)

@@ -243,7 +243,13 @@ const char *pgm_nn_last_error(void);
  * PGM_STATIC_MAX_GRID, order 4, 6 or 8; larger inputs return PGM_ERR_UNSUPPORTED with a message in
  * pgm_static_last_error().  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (other streams or threads at the same time) race on it. */
+ * calls that overlap on the GPU (other streams or threads at the same time) race on it.
+ * The stream must belong to the current device (PGM_ERR_INVALID otherwise); a CUDA error left
+ * pending by an earlier launch is reported (PGM_ERR_CUDA) and not cleared.  The box must be lower
+ * triangular with a positive diagonal and the cutoff at most half its smallest diagonal element:
+ * the box is on the device, so this is checked there and any other box gives a NaN field.  Pairs
+ * are taken by minimum image within the cutoff; pgm_field's rows also keep the pairs of one
+ * molecule beyond the cutoff, so the two differ for a molecule larger than the cutoff. */
 #define PGM_STATIC_MAX_ATOMS 4096
 #define PGM_STATIC_MAX_K 64
 #define PGM_STATIC_MAX_GRID 32768

@@ -3,8 +3,8 @@
  *
  * A plain FP64 restatement, with OpenMP over atoms, of the per-step pGM electrostatics of
  * pGM-JAX.  Every function names the reference code it follows.  The structure is deliberately
- * simple (brute-force minimum-image pair search, a recursive mixed-radix FFT): it is a checker and
- * a CPU baseline, not a fast implementation.
+ * plain (a cell-list pair search with the reference's minimum image, a recursive mixed-radix FFT,
+ * OpenMP over atoms, grid slabs and FFT lines): it is a checker and a CPU baseline.
  */
 #include "pgm_oracle.h"
 
@@ -129,8 +129,22 @@ static void bspline_moduli(int K, int order, double *mod) {
         if (mod[m] < 1e-7) mod[m] = 0.5 * (mod[(m - 1 + K) % K] + mod[(m + 1) % K]);
 }
 
-/* ------------------------------------------------------------------ FFT (plain recursive mixed radix) */
-static void fft_rec(double complex *x, int n, int stride, double complex *out, int sign) {
+/* ------------------------------------------------------------------ FFT (recursive mixed radix) */
+/* w[j] = exp(sign 2 pi i j / L), j < L: the twiddles of every sub-transform of a length-L line. */
+static double complex *twiddles(int L, int sign) {
+    double complex *w = malloc(sizeof(double complex) * L);
+    for (int j = 0; j < L; ++j) {
+        double ang = sign * 2.0 * M_PI * (double)j / L;
+        w[j] = cos(ang) + I * sin(ang);
+    }
+    return w;
+}
+
+/* Decimation in time by the smallest prime factor p of n: p sub-transforms of length n / p of the
+ * strided input, then the p-point butterflies.  w is the twiddle table of the full line length
+ * (wstep = L / n), work holds 2 n values (this level's sub-transforms and the levels below). */
+static void fft_rec(const double complex *x, int n, int stride, double complex *out, const double complex *w, int wstep,
+                    double complex *work) {
     if (n == 1) {
         out[0] = x[0];
         return;
@@ -139,54 +153,56 @@ static void fft_rec(double complex *x, int n, int stride, double complex *out, i
     while (p * p <= n && n % p) ++p;
     if (n % p) p = n; /* prime */
     int m = n / p;
-    double complex *sub = malloc(sizeof(double complex) * n);
-    for (int r = 0; r < p; ++r) fft_rec(x + r * stride, m, stride * p, sub + r * m, sign);
+    double complex *sub = work;
+    for (int r = 0; r < p; ++r) fft_rec(x + r * stride, m, stride * p, sub + r * m, w, wstep * p, work + n);
     for (int k = 0; k < m; ++k)
         for (int s2 = 0; s2 < p; ++s2) {
             int kk = k + m * s2;
             double complex acc = 0;
-            for (int r = 0; r < p; ++r) {
-                double ang = sign * 2.0 * M_PI * (double)((long long)r * kk % n) / n;
-                acc += sub[r * m + k] * (cos(ang) + I * sin(ang));
-            }
+            for (int r = 0; r < p; ++r) acc += sub[r * m + k] * w[(size_t)((long long)r * kk % n) * wstep];
             out[kk] = acc;
         }
-    free(sub);
 }
 
 /* In-place unnormalised 3D DFT, sign -1 forward, +1 backward, grid [K0][K1][K2]. */
 static void fft3d(double complex *g, const int K[3], int sign, int nth) {
     int K0 = K[0], K1 = K[1], K2 = K[2];
     (void)nth;
+    double complex *w0 = twiddles(K0, sign), *w1 = twiddles(K1, sign), *w2 = twiddles(K2, sign);
 #pragma omp parallel
     {
         int L = K0 > K1 ? (K0 > K2 ? K0 : K2) : (K1 > K2 ? K1 : K2);
         double complex *in = malloc(sizeof(double complex) * L), *out = malloc(sizeof(double complex) * L);
+        double complex *work = malloc(sizeof(double complex) * 2 * L);
 #pragma omp for collapse(2)
         for (int a = 0; a < K0; ++a)
             for (int b = 0; b < K1; ++b) {
                 double complex *line = g + ((size_t)a * K1 + b) * K2;
                 memcpy(in, line, sizeof(double complex) * K2);
-                fft_rec(in, K2, 1, out, sign);
+                fft_rec(in, K2, 1, out, w2, 1, work);
                 memcpy(line, out, sizeof(double complex) * K2);
             }
 #pragma omp for collapse(2)
         for (int a = 0; a < K0; ++a)
             for (int c = 0; c < K2; ++c) {
                 for (int b = 0; b < K1; ++b) in[b] = g[((size_t)a * K1 + b) * K2 + c];
-                fft_rec(in, K1, 1, out, sign);
+                fft_rec(in, K1, 1, out, w1, 1, work);
                 for (int b = 0; b < K1; ++b) g[((size_t)a * K1 + b) * K2 + c] = out[b];
             }
 #pragma omp for collapse(2)
         for (int b = 0; b < K1; ++b)
             for (int c = 0; c < K2; ++c) {
                 for (int a = 0; a < K0; ++a) in[a] = g[((size_t)a * K1 + b) * K2 + c];
-                fft_rec(in, K0, 1, out, sign);
+                fft_rec(in, K0, 1, out, w0, 1, work);
                 for (int a = 0; a < K0; ++a) g[((size_t)a * K1 + b) * K2 + c] = out[a];
             }
         free(in);
         free(out);
+        free(work);
     }
+    free(w0);
+    free(w1);
+    free(w2);
 }
 
 /* ------------------------------------------------------------------ PME (md/pme.py:175-411) */
@@ -277,30 +293,50 @@ static inline size_t pme_index(const pme_t *P, int i, int k1, int k2, int k3) {
     return ((size_t)i1 * P->K[1] + i2) * P->K[2] + i3;
 }
 
-/* Spread q and d (pme.py:306-337), transform, return E_rec = sum G |F[Q]|^2 [e^2/nm] and leave
- * phi = dE/dQ = 2 Re IDFT(G F[Q]) (pme.py:370-376) in the real part of the grid. */
-static double pme_energy_phi(pme_t *P, const double *q, const double *d, int n) {
+/* Spread q and d on the grid (pme.py:306-337).  Each thread owns a slab of k1 planes and adds, in
+ * atom order, the stencil points that fall in it, so every grid value is the same ordered sum as
+ * in a serial loop over the atoms.  q may be NULL. */
+static void pme_spread(pme_t *P, const double *q, const double *d, int n) {
     int p = P->p;
     size_t ng = (size_t)P->K[0] * P->K[1] * P->K[2];
     memset(P->grid, 0, sizeof(double complex) * ng);
-    for (int i = 0; i < n; ++i) {
-        double e[3];
-        for (int a = 0; a < 3; ++a)
-            e[a] = d[i * 3 + 0] * P->escale[0 * 3 + a] + d[i * 3 + 1] * P->escale[1 * 3 + a] +
-                   d[i * 3 + 2] * P->escale[2 * 3 + a];
-        const double *t1 = P->th + (size_t)(i * 3 + 0) * p, *t2 = P->th + (size_t)(i * 3 + 1) * p,
-                     *t3 = P->th + (size_t)(i * 3 + 2) * p;
-        const double *d1 = P->dth + (size_t)(i * 3 + 0) * p, *d2 = P->dth + (size_t)(i * 3 + 1) * p,
-                     *d3 = P->dth + (size_t)(i * 3 + 2) * p;
-        double qi = q ? q[i] : 0.0;
-        for (int a = 0; a < p; ++a)
-            for (int b = 0; b < p; ++b)
-                for (int c = 0; c < p; ++c) {
-                    double v = qi * t1[a] * t2[b] * t3[c] + e[0] * d1[a] * t2[b] * t3[c] +
-                               e[1] * t1[a] * d2[b] * t3[c] + e[2] * t1[a] * t2[b] * d3[c];
-                    P->grid[pme_index(P, i, a, b, c)] += v;
-                }
+#pragma omp parallel
+    {
+        int nt = 1, t = 0;
+#ifdef _OPENMP
+        nt = omp_get_num_threads();
+        t = omp_get_thread_num();
+#endif
+        int lo = (int)((long long)P->K[0] * t / nt), hi = (int)((long long)P->K[0] * (t + 1) / nt);
+        for (int i = 0; i < n; ++i) {
+            double e[3];
+            for (int a = 0; a < 3; ++a)
+                e[a] = d[i * 3 + 0] * P->escale[0 * 3 + a] + d[i * 3 + 1] * P->escale[1 * 3 + a] +
+                       d[i * 3 + 2] * P->escale[2 * 3 + a];
+            const double *t1 = P->th + (size_t)(i * 3 + 0) * p, *t2 = P->th + (size_t)(i * 3 + 1) * p,
+                         *t3 = P->th + (size_t)(i * 3 + 2) * p;
+            const double *d1 = P->dth + (size_t)(i * 3 + 0) * p, *d2 = P->dth + (size_t)(i * 3 + 1) * p,
+                         *d3 = P->dth + (size_t)(i * 3 + 2) * p;
+            double qi = q ? q[i] : 0.0;
+            for (int a = 0; a < p; ++a) {
+                int i1 = (P->base[i * 3 + 0] + a) % P->K[0];
+                if (i1 < lo || i1 >= hi) continue;
+                for (int b = 0; b < p; ++b)
+                    for (int c = 0; c < p; ++c) {
+                        double v = qi * t1[a] * t2[b] * t3[c] + e[0] * d1[a] * t2[b] * t3[c] +
+                                   e[1] * t1[a] * d2[b] * t3[c] + e[2] * t1[a] * t2[b] * d3[c];
+                        P->grid[pme_index(P, i, a, b, c)] += v;
+                    }
+            }
+        }
     }
+}
+
+/* Spread q and d (pme.py:306-337), transform, return E_rec = sum G |F[Q]|^2 [e^2/nm] and leave
+ * phi = dE/dQ = 2 Re IDFT(G F[Q]) (pme.py:370-376) in the real part of the grid. */
+static double pme_energy_phi(pme_t *P, const double *q, const double *d, int n) {
+    size_t ng = (size_t)P->K[0] * P->K[1] * P->K[2];
+    pme_spread(P, q, d, n);
     fft3d(P->grid, P->K, -1, 0);
     double E = 0.0;
     for (size_t m = 0; m < ng; ++m) {
@@ -351,24 +387,7 @@ static void pme_gather(const pme_t *P, int i, double qi, const double d[3], doub
  * 1/|m*|^2)] (strain derivative of pme.py:243-267 at fixed fractional coordinates).  Needs the
  * forward transform: called on a fresh spread. */
 static void pme_influence_virial(pme_t *P, const double *q, const double *d, int n, double W[9]) {
-    int p = P->p;
-    size_t ng = (size_t)P->K[0] * P->K[1] * P->K[2];
-    memset(P->grid, 0, sizeof(double complex) * ng);
-    for (int i = 0; i < n; ++i) {
-        double e[3];
-        for (int a = 0; a < 3; ++a)
-            e[a] = d[i * 3 + 0] * P->escale[0 * 3 + a] + d[i * 3 + 1] * P->escale[1 * 3 + a] +
-                   d[i * 3 + 2] * P->escale[2 * 3 + a];
-        const double *t1 = P->th + (size_t)(i * 3 + 0) * p, *t2 = P->th + (size_t)(i * 3 + 1) * p,
-                     *t3 = P->th + (size_t)(i * 3 + 2) * p;
-        const double *d1 = P->dth + (size_t)(i * 3 + 0) * p, *d2 = P->dth + (size_t)(i * 3 + 1) * p,
-                     *d3 = P->dth + (size_t)(i * 3 + 2) * p;
-        for (int a = 0; a < p; ++a)
-            for (int b = 0; b < p; ++b)
-                for (int c = 0; c < p; ++c)
-                    P->grid[pme_index(P, i, a, b, c)] += q[i] * t1[a] * t2[b] * t3[c] + e[0] * d1[a] * t2[b] * t3[c] +
-                                                         e[1] * t1[a] * d2[b] * t3[c] + e[2] * t1[a] * t2[b] * d3[c];
-    }
+    pme_spread(P, q, d, n);
     fft3d(P->grid, P->K, -1, 0);
     int K0 = P->K[0], K1 = P->K[1], K2 = P->K[2];
     double acc[9] = {0};
@@ -412,6 +431,77 @@ static int *atom_mol(const pgmo_system *sys) {
     return m;
 }
 
+/* Candidate partners of atoms: the atoms of the 27 cells around an atom's cell in fractional
+ * coordinates, cells at least one cutoff high across their planes (the grid has at least 3 cells
+ * along every axis; otherwise every atom is a candidate).  A pair inside the cutoff under the
+ * minimum image has an image whose fractional separation is below rc / h_a along every axis
+ * (h_a the box height across the planes of axis a), so it lies in a neighbouring cell. */
+typedef struct {
+    int nc[3];
+    int *start, *atoms, *cell;  /* (cells + 1), (n) atoms by cell in index order, (n) cell of each atom */
+} cells_t;
+
+static int cells_init(cells_t *L, const double *pos, const double *H, int n, double rc) {
+    double Hi[9];
+    inv3(H, Hi);
+    long long ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        double h = 1.0 / sqrt(Hi[0 * 3 + a] * Hi[0 * 3 + a] + Hi[1 * 3 + a] * Hi[1 * 3 + a] + Hi[2 * 3 + a] * Hi[2 * 3 + a]);
+        L->nc[a] = (int)floor(h / rc);
+        if (L->nc[a] < 3 || n < 4096) return 0;
+        if (L->nc[a] > 256) L->nc[a] = 256;
+        ncell *= L->nc[a];
+    }
+    L->cell = malloc(sizeof(int) * n);
+    L->start = calloc(ncell + 1, sizeof(int));
+    L->atoms = malloc(sizeof(int) * n);
+    for (int i = 0; i < n; ++i) {
+        int c[3];
+        for (int a = 0; a < 3; ++a) {
+            double u = pos[i * 3] * Hi[a] + pos[i * 3 + 1] * Hi[3 + a] + pos[i * 3 + 2] * Hi[6 + a];
+            c[a] = (int)floor((u - floor(u)) * L->nc[a]);
+            if (c[a] >= L->nc[a]) c[a] = L->nc[a] - 1;
+            if (c[a] < 0) c[a] = 0;
+        }
+        L->cell[i] = (c[0] * L->nc[1] + c[1]) * L->nc[2] + c[2];
+        L->start[L->cell[i] + 1]++;
+    }
+    for (long long c = 0; c < ncell; ++c) L->start[c + 1] += L->start[c];
+    int *fill = malloc(sizeof(int) * ncell);
+    memcpy(fill, L->start, sizeof(int) * ncell);
+    for (int i = 0; i < n; ++i) L->atoms[fill[L->cell[i]]++] = i;
+    free(fill);
+    return 1;
+}
+
+static int cmp_int(const void *a, const void *b) {
+    int x = *(const int *)a, y = *(const int *)b;
+    return (x > y) - (x < y);
+}
+
+/* The candidates of atom i in ascending index order (i itself excluded); returns their number. */
+static int candidates(const cells_t *L, int use_cells, int n, int i, int *out) {
+    int m = 0;
+    if (!use_cells) {
+        for (int k = 0; k < n; ++k)
+            if (k != i) out[m++] = k;
+        return m;
+    }
+    int c = L->cell[i];
+    int c2 = c % L->nc[2], c1 = (c / L->nc[2]) % L->nc[1], c0 = c / (L->nc[1] * L->nc[2]);
+    for (int d0 = -1; d0 <= 1; ++d0)
+        for (int d1 = -1; d1 <= 1; ++d1)
+            for (int d2 = -1; d2 <= 1; ++d2) {
+                int e0 = (c0 + d0 + L->nc[0]) % L->nc[0], e1 = (c1 + d1 + L->nc[1]) % L->nc[1],
+                    e2 = (c2 + d2 + L->nc[2]) % L->nc[2];
+                int cc = (e0 * L->nc[1] + e1) * L->nc[2] + e2;
+                for (int t = L->start[cc]; t < L->start[cc + 1]; ++t)
+                    if (L->atoms[t] != i) out[m++] = L->atoms[t];
+            }
+    qsort(out, m, sizeof(int), cmp_int);
+    return m;
+}
+
 /* Every atom's row: its molecule partners (the rigid special table, topology.py:161-178, vdW
  * weight 0) then every other atom inside the cutoff (vdW weight 1), all masked to r < rc. */
 static void build_rows(const pgmo_system *sys, const pgmo_settings *s, const double *pos, const double *H,
@@ -419,18 +509,41 @@ static void build_rows(const pgmo_system *sys, const pgmo_settings *s, const dou
     int n = sys->n;
     int *mol = atom_mol(sys);
     double rc2 = s->cutoff * s->cutoff;
+    cells_t L;
+    int use_cells = cells_init(&L, pos, H, n, s->cutoff);
+    int maxc = n;
+    if (use_cells) {  /* the largest 27-cell neighbourhood */
+        maxc = 0;
+        for (int i = 0; i < n; ++i) {
+            int c = L.cell[i], m = 0;
+            int c2 = c % L.nc[2], c1 = (c / L.nc[2]) % L.nc[1], c0 = c / (L.nc[1] * L.nc[2]);
+            for (int d0 = -1; d0 <= 1; ++d0)
+                for (int d1 = -1; d1 <= 1; ++d1)
+                    for (int d2 = -1; d2 <= 1; ++d2) {
+                        int cc = (((c0 + d0 + L.nc[0]) % L.nc[0]) * L.nc[1] + (c1 + d1 + L.nc[1]) % L.nc[1]) * L.nc[2] +
+                                 (c2 + d2 + L.nc[2]) % L.nc[2];
+                        m += L.start[cc + 1] - L.start[cc];
+                    }
+            if (m > maxc) maxc = m;
+        }
+    }
     R->start = calloc(n + 1, sizeof(long long));
     int *cnt = calloc(n, sizeof(int));
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int i = 0; i < n; ++i) {
-        int c = 0;
-        for (int k = 0; k < n; ++k) {
-            if (k == i) continue;
-            double x[3] = {pos[i * 3] - pos[k * 3], pos[i * 3 + 1] - pos[k * 3 + 1], pos[i * 3 + 2] - pos[k * 3 + 2]};
-            min_image(x, H);
-            if (x[0] * x[0] + x[1] * x[1] + x[2] * x[2] < rc2) ++c;
+#pragma omp parallel
+    {
+        int *cand = malloc(sizeof(int) * (maxc + 1));
+#pragma omp for schedule(dynamic, 16)
+        for (int i = 0; i < n; ++i) {
+            int nc = candidates(&L, use_cells, n, i, cand), c = 0;
+            for (int t = 0; t < nc; ++t) {
+                int k = cand[t];
+                double x[3] = {pos[i * 3] - pos[k * 3], pos[i * 3 + 1] - pos[k * 3 + 1], pos[i * 3 + 2] - pos[k * 3 + 2]};
+                min_image(x, H);
+                if (x[0] * x[0] + x[1] * x[1] + x[2] * x[2] < rc2) ++c;
+            }
+            cnt[i] = c;
         }
-        cnt[i] = c;
+        free(cand);
     }
     for (int i = 0; i < n; ++i) R->start[i + 1] = R->start[i] + cnt[i];
     long long np = R->start[n];
@@ -441,26 +554,38 @@ static void build_rows(const pgmo_system *sys, const pgmo_settings *s, const dou
     R->we = malloc(np ? np : 1);
     const double rce = (s->elec_cutoff > 0.0 && s->elec_cutoff < s->cutoff) ? s->elec_cutoff : s->cutoff;
     const double rce2 = rce * rce;
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int i = 0; i < n; ++i) {
-        long long o = R->start[i];
-        int mi = mol[i];
-        /* specials first (same molecule, sorted), then the others in index order */
-        for (int pass = 0; pass < 2; ++pass)
-            for (int k = 0; k < n; ++k) {
-                if (k == i || ((mol[k] == mi) != (pass == 0))) continue;
-                double x[3] = {pos[i * 3] - pos[k * 3], pos[i * 3 + 1] - pos[k * 3 + 1], pos[i * 3 + 2] - pos[k * 3 + 2]};
-                min_image(x, H);
-                double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
-                if (r2 >= rc2) continue;
-                R->k[o] = k;
-                memcpy(R->x + 3 * o, x, sizeof(x));
-                double a = 1.0 / sqrt(2.0 * (sys->radius[i] * sys->radius[i] + sys->radius[k] * sys->radius[k]));
-                pair_kernels(a, s->beta, sqrt(r2), R->G + 4 * o);
-                R->wv[o] = pass == 0 ? 0.0 : 1.0;
-                R->we[o] = r2 < rce2;
-                ++o;
-            }
+#pragma omp parallel
+    {
+        int *cand = malloc(sizeof(int) * (maxc + 1));
+#pragma omp for schedule(dynamic, 16)
+        for (int i = 0; i < n; ++i) {
+            long long o = R->start[i];
+            int mi = mol[i];
+            int nc = candidates(&L, use_cells, n, i, cand);
+            /* specials first (same molecule, sorted), then the others in index order */
+            for (int pass = 0; pass < 2; ++pass)
+                for (int t = 0; t < nc; ++t) {
+                    int k = cand[t];
+                    if ((mol[k] == mi) != (pass == 0)) continue;
+                    double x[3] = {pos[i * 3] - pos[k * 3], pos[i * 3 + 1] - pos[k * 3 + 1], pos[i * 3 + 2] - pos[k * 3 + 2]};
+                    min_image(x, H);
+                    double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+                    if (r2 >= rc2) continue;
+                    R->k[o] = k;
+                    memcpy(R->x + 3 * o, x, sizeof(x));
+                    double a = 1.0 / sqrt(2.0 * (sys->radius[i] * sys->radius[i] + sys->radius[k] * sys->radius[k]));
+                    pair_kernels(a, s->beta, sqrt(r2), R->G + 4 * o);
+                    R->wv[o] = pass == 0 ? 0.0 : 1.0;
+                    R->we[o] = r2 < rce2;
+                    ++o;
+                }
+        }
+        free(cand);
+    }
+    if (use_cells) {
+        free(L.cell);
+        free(L.start);
+        free(L.atoms);
     }
     free(cnt);
     free(mol);

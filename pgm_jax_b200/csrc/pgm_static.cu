@@ -8,6 +8,13 @@
 // smooth PME, self term) for ONE small system in FP64, with every intermediate (the PME grids and
 // the box values) in the file-scope array g_field_scratch below instead of buffers of a handle.
 //
+// Pairs are taken by minimum image within the cutoff.  pgm_field's rows also keep every pair of
+// atoms of one molecule, however far apart; the two agree for molecules smaller than the cutoff
+// (water), and differ for a molecule whose atoms lie further apart than the cutoff.  The box must
+// be the handle path's: lower triangular with a positive diagonal, the cutoff at most half of its
+// smallest diagonal element; for any other box every field value is NaN (the box is on the device,
+// so the check runs there).  The stream must belong to the current device.
+//
 // Limits (checked, PGM_ERR_UNSUPPORTED beyond them): at most PGM_STATIC_MAX_ATOMS atoms, mesh sizes
 // K <= PGM_STATIC_MAX_K per axis with K1 K2 K3 <= PGM_STATIC_MAX_GRID points, spline order 4, 6 or 8.
 // The array (2 complex FP64 grids + 64 doubles, 1 MB) is held by every GPU that loads the library
@@ -24,7 +31,7 @@
 
 namespace {
 
-constexpr int SCR_BOX = 64;  // doubles at the end of the array: H, H^-1, volume
+constexpr int SCR_BOX = 64;  // doubles at the end of the array: H, H^-1, volume, box flag
 constexpr size_t SCR_DOUBLES = 4 * (size_t)PGM_STATIC_MAX_GRID + SCR_BOX;
 
 // Grids A and B (complex, ping-pong of the 3D DFT) followed by the box block.
@@ -46,7 +53,7 @@ struct StaticArgs {
   int with_q;
   double *field;
   double2 *A, *B;  // complex grids in the scratch array
-  double *bx;      // box block: H (9), H^-1 (9), volume (1)
+  double *bx;      // box block: H (9), H^-1 (9), volume (1), unusable-box flag (1)
 };
 
 __global__ void ks_box_and_clear(StaticArgs s) {
@@ -62,6 +69,12 @@ __global__ void ks_box_and_clear(StaticArgs s) {
     Hi[6] = (H[3] * H[7] - H[4] * H[6]) / d; Hi[7] = (H[1] * H[6] - H[0] * H[7]) / d; Hi[8] = (H[0] * H[4] - H[1] * H[3]) / d;
     for (int k = 0; k < 9; ++k) s.bx[k] = H[k];
     s.bx[18] = fabs(d);
+    // the minimum image below needs the handle path's box: lower triangular, positive diagonal,
+    // the cutoff at most half the smallest diagonal element; otherwise the field is NaN
+    int bad = (fabs(H[1]) > 1e-12 * fabs(H[0])) || (fabs(H[2]) > 1e-12 * fabs(H[0])) ||
+              (fabs(H[5]) > 1e-12 * fabs(H[0])) || !(H[0] > 0 && H[4] > 0 && H[8] > 0) ||
+              !(s.cutoff <= 0.5 * fmin(H[0], fmin(H[4], H[8])));
+    s.bx[19] = bad ? 1.0 : 0.0;
   }
 }
 
@@ -223,6 +236,10 @@ __global__ void ks_field(StaticArgs s, const double2 *phi) {
   if (lane == 0) {
     const double *Hi = s.bx + 9;
     const int K[3] = {s.K1, s.K2, s.K3};
+    if (s.bx[19] != 0.0) {  // a box the minimum image cannot serve: no value rather than a wrong one
+      for (int bb = 0; bb < 3; ++bb) s.field[3 * i + bb] = nan("");
+      return;
+    }
     for (int bb = 0; bb < 3; ++bb) {
       double rec = g[0] * Hi[bb * 3 + 0] * K[0] + g[1] * Hi[bb * 3 + 1] * K[1] + g[2] * Hi[bb * 3 + 2] * K[2];
       s.field[3 * i + bb] = -(f[bb] + rec - s.c_self * s.d[3 * i + bb]);
@@ -230,21 +247,31 @@ __global__ void ks_field(StaticArgs s, const double2 *phi) {
   }
 }
 
+// Every launch is checked as it is made, so an error is this call's own (a pending error of an
+// earlier launch was refused on entry).
 template <int P>
 cudaError_t run_static(StaticArgs s, cudaStream_t st) {
   int ng = s.K1 * s.K2 * s.K3;
   int gb = (ng + 255) / 256;
-  ks_box_and_clear<<<gb, 256, 0, st>>>(s);
-  ks_spread<P><<<(s.n + 127) / 128, 128, 0, st>>>(s);
-  ks_dft<<<gb, 256, 0, st>>>(s, s.A, s.B, 2, -1);
-  ks_dft<<<gb, 256, 0, st>>>(s, s.B, s.A, 1, -1);
-  ks_dft<<<gb, 256, 0, st>>>(s, s.A, s.B, 0, -1);
-  ks_convolve<P><<<gb, 256, 0, st>>>(s, s.B);
-  ks_dft<<<gb, 256, 0, st>>>(s, s.B, s.A, 0, +1);
-  ks_dft<<<gb, 256, 0, st>>>(s, s.A, s.B, 1, +1);
-  ks_dft<<<gb, 256, 0, st>>>(s, s.B, s.A, 2, +1);
-  ks_field<P><<<(s.n * 32 + 255) / 256, 256, 0, st>>>(s, s.A);
-  return cudaGetLastError();
+  cudaError_t e;
+#define PGM_STATIC_LAUNCH(...) \
+  do {                         \
+    __VA_ARGS__;               \
+    e = cudaGetLastError();    \
+    if (e != cudaSuccess) return e; \
+  } while (0)
+  PGM_STATIC_LAUNCH(ks_box_and_clear<<<gb, 256, 0, st>>>(s));
+  PGM_STATIC_LAUNCH(ks_spread<P><<<(s.n + 127) / 128, 128, 0, st>>>(s));
+  PGM_STATIC_LAUNCH(ks_dft<<<gb, 256, 0, st>>>(s, s.A, s.B, 2, -1));
+  PGM_STATIC_LAUNCH(ks_dft<<<gb, 256, 0, st>>>(s, s.B, s.A, 1, -1));
+  PGM_STATIC_LAUNCH(ks_dft<<<gb, 256, 0, st>>>(s, s.A, s.B, 0, -1));
+  PGM_STATIC_LAUNCH(ks_convolve<P><<<gb, 256, 0, st>>>(s, s.B));
+  PGM_STATIC_LAUNCH(ks_dft<<<gb, 256, 0, st>>>(s, s.B, s.A, 0, +1));
+  PGM_STATIC_LAUNCH(ks_dft<<<gb, 256, 0, st>>>(s, s.A, s.B, 1, +1));
+  PGM_STATIC_LAUNCH(ks_dft<<<gb, 256, 0, st>>>(s, s.B, s.A, 2, +1));
+  PGM_STATIC_LAUNCH(ks_field<P><<<(s.n * 32 + 255) / 256, 256, 0, st>>>(s, s.A));
+#undef PGM_STATIC_LAUNCH
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -267,10 +294,19 @@ PgmStatus pgm_field_static(void *stream, int n_atoms, const double *pos, const d
                                          " with at most " + std::to_string(PGM_STATIC_MAX_GRID) + " points");
   if (pme_order != 4 && pme_order != 6 && pme_order != 8) return serr(PGM_ERR_UNSUPPORTED, "pme_order must be 4, 6 or 8");
   if (!(cutoff > 0) || !(ewald_beta > 0)) return serr(PGM_ERR_INVALID, "cutoff and ewald_beta must be positive");
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess)  // left by an earlier launch of the caller: not cleared here, not blamed on this call
+    return serr(PGM_ERR_CUDA, std::string("pgm_field_static: an earlier CUDA error is pending: ") + cudaGetErrorString(e));
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return serr(PGM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= 64) return serr(PGM_ERR_UNSUPPORTED, "device index above 63");
+  int sdev = dev;
+  e = cudaStreamGetDevice((cudaStream_t)stream, &sdev);
+  if (e != cudaSuccess) return serr(PGM_ERR_CUDA, std::string("cudaStreamGetDevice: ") + cudaGetErrorString(e));
+  if (sdev != dev)  // the scratch address below belongs to the current device
+    return serr(PGM_ERR_INVALID, "pgm_field_static: the stream belongs to device " + std::to_string(sdev) +
+                                     ", the current device is " + std::to_string(dev));
   double *base = nullptr;
   {
     // set-up, once per device with that device current: the device address of the array

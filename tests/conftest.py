@@ -28,6 +28,25 @@ def golden_small_box():
     return dict(np.load(os.path.join(GOLDEN, "ff_small_box.npz")))
 
 
+# Settings of the reference's regression case ff_pgm3p25_512 (regression_cases.py:291-307): the
+# MDSettings defaults; the 0.08 nm spacing gives a 30^3 mesh on the 2.72 nm truncated octahedron
+PGM3P25_512_SETTINGS = dict(
+    cutoff=0.9, ewald_beta=4.0, pme_grid=(30, 30, 30), pme_order=6, lj_lrc=True, dipole_tol=1e-5, max_iter=50
+)
+
+
+@pytest.fixture(scope="session")
+def golden_pgm3p25_512():
+    return dict(np.load(os.path.join(GOLDEN, "ff_pgm3p25_512.npz")))
+
+
+@pytest.fixture(scope="session")
+def pgm3p25_512_system():
+    from pgm_jax_b200.systems import System, pgm3p25_water
+
+    return System([pgm3p25_water()] * 512)
+
+
 @pytest.fixture(scope="session")
 def small_box_system():
     from pgm_jax_b200.systems import small_box

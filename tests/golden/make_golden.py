@@ -1,16 +1,27 @@
-"""Write tests/golden/*.npz from the reference's own regression golden files.
+"""Write tests/golden/*.npz from the reference's own regression golden files and example frame.
 
-Run in a container where the reference is mounted (it is not needed afterwards):
+Run once in a container where a checkout of pGM-JAX is available (it is not needed afterwards);
+the checkout's root is the one required argument:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the pGM-JAX checkout>
 
-Source: tests/regression/golden/ff_small_box.npz of pGM-JAX (case `ff_small_box`,
+ff_small_box.npz -- from tests/regression/golden/ff_small_box.npz of pGM-JAX (case `ff_small_box`,
 tests/regression/regression_cases.py:240-276): the MD force field on the 114-atom triclinic
 water/methanol box of pgm_jax/models/toy.py:143 small_box(0), cutoff 0.6 nm, skin 0.05, Ewald 6.0/nm,
 PME 32^3 order 6, LJ tail, tol 1e-10, max_iter 500, recorded in float64 and in mixed precision.
 The inputs (positions, box) are regenerated here by pgm_jax_b200.systems.small_box(0) from the same
 numpy seed and stored next to the outputs, so that the tests need neither the reference nor numpy's
 generator to stay stable.
+
+ff_pgm3p25_512.npz -- from tests/regression/golden/ff_pgm3p25_512.npz of pGM-JAX (case
+`ff_pgm3p25_512`, regression_cases.py:291-307): 512 pGM3P-25 waters of examples/water512, default
+MDSettings (cutoff 0.9 nm, Ewald 4.0/nm, order 6, spacing 0.08 nm -> 30^3 on this box, tol 1e-5,
+mu4) in float64 and mixed precision.  The frame is examples/water512/pgm3p25_512.rst7 (an Amber
+NetCDF restart: coordinates and velocities in Angstrom and Angstrom/ps -- velocities scaled by the
+variable's scale_factor as pgm_jax/md/io.py:54-70 reads them -- and a truncated-octahedron cell,
+27.201 A, 109.47 deg), turned into the lower-triangular box of pgm_jax/md/box.py:291-314
+(box_from_cell) and nm as the regression case does.  The velocities are stored for the 10-step NVE
+install check of tests/test_water512.py (step-10 Epot -2114884.256504 kJ/mol, T 291.356783 K).
 """
 
 import os
@@ -23,17 +34,52 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from pgm_jax_b200.systems import small_box  # noqa: E402
 
+KEYS = ("energy.elec", "energy.vdw", "energy.total", "forces", "mu", "iterations", "residual", "strain")
+
+
+def box_from_cell(lengths, angles) -> np.ndarray:
+    """Lattice vectors as rows, a along x, b in the xy plane (the Amber / PDB convention)."""
+    a, b, c = (float(x) for x in lengths)
+    al, be, ga = np.radians(np.asarray(angles, float))
+    cx = c * np.cos(be)
+    cy = c * (np.cos(al) - np.cos(be) * np.cos(ga)) / np.sin(ga)
+    return np.array([[a, 0.0, 0.0], [b * np.cos(ga), b * np.sin(ga), 0.0], [cx, cy, np.sqrt(c * c - cx * cx - cy * cy)]])
+
+
+def water512_frame(ref: str):
+    """(positions [nm], velocities [nm/ps], box [nm]) of examples/water512/pgm3p25_512.rst7."""
+    from scipy.io import netcdf_file
+
+    f = netcdf_file(os.path.join(ref, "examples", "water512", "pgm3p25_512.rst7"), "r", mmap=False)
+    v = f.variables
+    xyz = np.array(v["coordinates"][:], float).reshape(-1, 3)
+    vel = np.array(v["velocities"][:], float).reshape(-1, 3) * float(getattr(v["velocities"], "scale_factor", 20.455))
+    H = box_from_cell(np.array(v["cell_lengths"][:], float), np.array(v["cell_angles"][:], float))
+    return xyz * 0.1, vel * 0.1, H * 0.1
+
 
 def main(ref: str) -> None:
-    g = np.load(os.path.join(ref, "tests", "regression", "golden", "ff_small_box.npz"))
+    gdir = os.path.join(ref, "tests", "regression", "golden")
+    g = np.load(os.path.join(gdir, "ff_small_box.npz"))
     _, pos, H = small_box(0)
     out = {"pos": pos, "box": H}
     for tag in ("double", "mixed"):
-        for k in ("energy.elec", "energy.vdw", "energy.total", "forces", "mu", "iterations", "residual", "strain"):
+        for k in KEYS:
             out[f"{tag}.{k}"] = g[f"{tag}.{k}"]
     np.savez_compressed(os.path.join(HERE, "ff_small_box.npz"), **out)
     print("wrote", os.path.join(HERE, "ff_small_box.npz"), sorted(out))
 
+    g = np.load(os.path.join(gdir, "ff_pgm3p25_512.npz"))
+    pos, vel, H = water512_frame(ref)
+    out = {"pos": pos, "vel": vel, "box": H}
+    for tag in ("double", "mixed"):
+        for k in KEYS:
+            out[f"{tag}.{k}"] = g[f"{tag}.{k}"]
+    np.savez_compressed(os.path.join(HERE, "ff_pgm3p25_512.npz"), **out)
+    print("wrote", os.path.join(HERE, "ff_pgm3p25_512.npz"), sorted(out))
+
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(sys.argv[1])

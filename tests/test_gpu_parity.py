@@ -367,3 +367,76 @@ def test_compute_host_matches_device_calls():
         assert np.abs(F - rd.forces.cpu().numpy()).max() <= 1e-5 * np.abs(F).max(), step
         assert np.abs(hist - ind_d.hist.cpu().numpy()).max() <= 1e-5 * np.abs(hist).max(), step
         assert abs(int(it[0]) - int(rd.iterations[0])) <= 1 and int(cnt[0]) == int(ind_d.count[0]) == step + 1
+
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_pgm3p25_512_matches_reference_golden(pgm3p25_512_system, golden_pgm3p25_512, prec):
+    """The reference's ff_pgm3p25_512 regression point (examples/water512 frame, truncated
+    octahedron, default settings, 30^3 mesh): FP64 against its float64 record (energy 1e-9, forces
+    1e-8 RMS, iterations equal, virial 1e-6); mixed precision against its mixed record (energy
+    1e-6, forces and dipoles 1e-5 RMS relative)."""
+    from conftest import PGM3P25_512_SETTINGS
+
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+
+    g = golden_pgm3p25_512
+    ff = PGMForceField(pgm3p25_512_system, g["box"], MDSettings(precision=prec, **PGM3P25_512_SETTINGS))
+    res = ff.compute(g["pos"], g["box"], None, ff.init_induction())
+    assert int(res.status[0]) == 0
+    tol_e = 1e-9 if prec == "double" else 1e-6
+    for k in ("elec", "vdw", "total"):
+        ref = float(g[f"{prec}.energy.{k}"])
+        assert abs(float(res.energy[k][0]) - ref) <= tol_e * abs(ref), (k, float(res.energy[k][0]), ref)
+    tol = 1e-8 if prec == "double" else 1e-5
+    assert rms_rel(res.forces.cpu().numpy(), g[f"{prec}.forces"]) <= tol
+    assert rms_rel(res.induction.mu.cpu().numpy(), g[f"{prec}.mu"]) <= tol
+    if prec == "double":
+        assert int(res.iterations[0]) == int(g["double.iterations"])
+        W = g["double.strain"]
+        assert np.abs(res.virial[0].cpu().numpy() - W).max() <= 1e-6 * np.abs(W).max()
+    else:
+        assert abs(int(res.iterations[0]) - int(g["mixed.iterations"])) <= 1
+
+
+@pytest.mark.parametrize("grid", [(64, 64, 64), (72, 72, 72), (96, 96, 96), (192, 192, 192), (64, 96, 72)])
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_field_on_the_workload_meshes(grid, prec):
+    """The field sweep on the mesh lengths of the benchmark workloads: 64^3 and 72^3 (the uneven
+    boxes and the path-integral beads), 96^3 (4,096 waters) and 192^3 (32,768 waters: K > 128 takes
+    the five-pass chain), and a mixed 64 x 96 x 72 mesh (the separate passes, each axis's compiled
+    plan), against the oracle's full-spectrum FFT on 512 pGM3P-25 waters."""
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(8, 2.483, seed=2)
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=grid, pme_order=6, dipole_tol=1e-8, max_iter=100)
+    rng = np.random.default_rng(7)
+    d = rng.normal(scale=0.01, size=(s.n, 3))
+    ref = O.Oracle(s, st).field(pos, H, s.q, d)
+    got = PGMForceField(s, H, MDSettings(precision=prec, **st)).field(pos, H, d, charges=True).cpu().numpy()
+    tol = 1e-9 if prec == "double" else 2e-6
+    assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), np.abs(got - ref).max() / np.abs(ref).max()
+
+
+def test_water4096_frame_matches_oracle():
+    """The 4,096-water benchmark frame (12,288 atoms, 4.966 nm box, PME 96^3, cutoff 0.9 nm,
+    Ewald 4.0/nm) as a single point at tol 1e-8: the FP64 engine against the oracle (energy 1e-9,
+    forces 1e-8 RMS, iterations equal, virial 1e-7); mixed precision at tol 1e-6 against the same
+    oracle point (energy 1e-6, forces and dipoles 1e-5 RMS)."""
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(16, 4.966, seed=0)
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(96, 96, 96), pme_order=6, dipole_tol=1e-8, max_iter=100)
+    r = O.Oracle(s, st).compute(pos, H)
+    g = PGMForceField(s, H, MDSettings(precision="double", **st)).compute(pos, H)
+    assert int(g.status[0]) == 0
+    assert abs(float(g.energy["total"][0]) - r["energy"]["total"]) <= 1e-9 * abs(r["energy"]["total"])
+    assert rms_rel(g.forces.cpu().numpy(), r["forces"]) <= 1e-8
+    assert rms_rel(g.induction.mu.cpu().numpy(), r["mu"]) <= 1e-8
+    assert int(g.iterations[0]) == r["iterations"]
+    assert np.abs(g.virial[0].cpu().numpy() - r["virial"]).max() <= 1e-7 * np.abs(r["virial"]).max()
+    m = PGMForceField(s, H, MDSettings(precision="mixed", **dict(st, dipole_tol=1e-6))).compute(pos, H)
+    assert abs(float(m.energy["total"][0]) - r["energy"]["total"]) <= 1e-6 * abs(r["energy"]["total"])
+    assert rms_rel(m.forces.cpu().numpy(), r["forces"]) <= 1e-5
+    assert rms_rel(m.induction.mu.cpu().numpy(), r["mu"]) <= 1e-5

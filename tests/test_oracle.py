@@ -135,3 +135,25 @@ def test_oracle_split_rows(small):
         d[a, k] = h
         fd = -(os_.energy_fixed_mu(pos + d, H, rs["mu"])["total"] - os_.energy_fixed_mu(pos - d, H, rs["mu"])["total"]) / (2 * h)
         assert abs(fd - rs["forces"][a, k]) < 1e-5 * max(1.0, abs(fd)), (a, k, fd, rs["forces"][a, k])
+
+
+def test_oracle_matches_reference_golden_pgm3p25_512(pgm3p25_512_system, golden_pgm3p25_512):
+    """512 pGM3P-25 waters of the reference's examples/water512 frame at the default settings
+    (regression case ff_pgm3p25_512): the parameters, the truncated-octahedron box and the 30^3
+    mesh of every pGM3P-25 workload, pinned to the reference's float64 output."""
+    from conftest import PGM3P25_512_SETTINGS
+
+    from pgm_jax_b200.systems import grid_size
+
+    g = golden_pgm3p25_512
+    assert grid_size(g["box"], 0.08) == PGM3P25_512_SETTINGS["pme_grid"]
+    r = O.Oracle(pgm3p25_512_system, PGM3P25_512_SETTINGS).compute(g["pos"], g["box"])
+    for k in ("elec", "vdw", "total"):
+        ref = float(g[f"double.energy.{k}"])
+        assert abs(r["energy"][k] - ref) <= 1e-10 * abs(ref), (k, r["energy"][k], ref)
+    assert r["iterations"] == int(g["double.iterations"])
+    F, mu = g["double.forces"], g["double.mu"]
+    assert np.sqrt(np.sum((r["forces"] - F) ** 2) / np.sum(F**2)) <= 1e-8
+    assert np.sqrt(np.sum((r["mu"] - mu) ** 2) / np.sum(mu**2)) <= 1e-8
+    W = g["double.strain"]
+    assert np.abs(r["virial"] - W).max() <= 1e-6 * np.abs(W).max()

@@ -68,3 +68,25 @@ def test_static_field_rejects_oversized_inputs():
     grid_c = (C.c_int * 3)(16, 16, 16)
     rc = lib.pgm_field_static(None, 5000, _p(z), _p(box), _p(r), _p(r), 0.4, 6.0, grid_c, 6, 1, _p(z), _p(z))
     assert rc == 4 and b"n_atoms" in lib.pgm_static_last_error()
+
+
+def test_static_field_box_too_small_for_the_cutoff_gives_nan():
+    """A box whose half height is below the cutoff cannot be served by the minimum image: the
+    field is NaN (not a silently wrong value), and the next valid call is correct again."""
+    from pgm_jax_b200 import _lib
+    from pgm_jax_b200.systems import small_box
+
+    s, pos, H = small_box(0)
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    f64 = lambda a: torch.tensor(np.ascontiguousarray(a, float), dtype=torch.float64, device=dev)  # noqa: E731
+    x, box, q, rad = f64(pos), f64(H), f64(s.q), f64(s.radius)
+    d = f64(np.random.default_rng(2).normal(scale=0.01, size=(s.n, 3)))
+    grid_c = (C.c_int * 3)(32, 32, 32)
+    out = torch.zeros((s.n, 3), dtype=torch.float64, device=dev)
+    cutoff = 0.6 * float(np.min(np.diag(H)))  # above half the smallest diagonal element
+    rc = lib.pgm_field_static(None, s.n, _p(x), _p(box), _p(q), _p(rad), cutoff, 6.0, grid_c, 6, 1, _p(d), _p(out))
+    assert rc == 0, lib.pgm_static_last_error().decode()
+    assert torch.isnan(out).all()
+    rc = lib.pgm_field_static(None, s.n, _p(x), _p(box), _p(q), _p(rad), 0.6, 6.0, grid_c, 6, 1, _p(d), _p(out))
+    assert rc == 0 and torch.isfinite(out).all()
