@@ -271,10 +271,12 @@ PgmStatus pgm_rigid_create(int n_mol, const int32_t *mol_start, const int32_t *m
                            const double *body, const double *inertia, int device, PgmRigid **out);
 PgmStatus pgm_rigid_destroy(PgmRigid *r);
 
-/* Kick (with the forces of the previous step; NULL: none), drift, Langevin (gamma [1/ps] > 0, kT
- * [kJ/mol] per system, device; the noise is drawn from (seed, the handle's step counter)), drift;
- * writes the atom positions pos (N, 3) for the next force call.  box (n_systems, 3, 3) keeps the
- * centres in the box. */
+/* Kick (with the forces of the previous step; NULL: none), then with gamma [1/ps] > 0: half drift,
+ * Langevin (kT [kJ/mol] per system, device; the noise is drawn from (seed, the handle's step
+ * counter)), half drift; with gamma = 0 (NVE): one drift of dt (the reference's velocity Verlet,
+ * integrate.py:743-761).  A drift moves the centres and turns the bodies by the free-rotor splitting
+ * (axes 3, 2, 1, 2, 3).  Writes the atom positions pos (N, 3) for the next force call.  box
+ * (n_systems, 3, 3) keeps the centres in the box. */
 PgmStatus pgm_rigid_begin_step(PgmRigid *r, void *stream, double dt, double gamma, const double *kT, uint64_t seed,
                                const double *forces, double *com, double *quat, double *mom, double *angmom, double *pos,
                                const double *box);

@@ -3,12 +3,15 @@
 // O-step of md/thermostats.py:195-240).
 //
 // Rigid bodies: centre of mass X, orientation quaternion q (body -> space), COM momentum P and
-// body-frame angular momentum L; atoms at X + R(q) b_i with b_i in the principal frame.  One step
-// is B A O A (forces) B: half kicks of P and L (torque rotated into the body frame), half drifts of
-// X and of the free rotor by the symplectic splitting of Dullweber, Leimkuhler and McLachlan
-// (J. Chem. Phys. 107, 5840 (1997): rotations about body axes 3, 2, 1, 2, 3), and the Langevin
-// step P <- c P + sqrt((1 - c^2) M kT) xi, L_k <- c L_k + sqrt((1 - c^2) I_k kT) xi with
-// c = exp(-gamma dt) (gamma = 0: NVE).  One thread per molecule; FP64 throughout.
+// body-frame angular momentum L; atoms at X + R(q) b_i with b_i in the principal frame.  With
+// Langevin friction (gamma > 0) one step is B A O A (forces) B; in NVE (gamma = 0) it is B A
+// (forces) B with one drift of the full step, as integrate.py:743-761.  B: half kicks of P and L
+// (torque rotated into the body frame).  A: the drift of X and the free rotor by exact rotations
+// about the principal axes 3, 2, 1, 2, 3 (half, half, full, half, half) -- the splitting of
+// Dullweber, Leimkuhler and McLachlan (J. Chem. Phys. 107, 5840 (1997)), in quaternion form the
+// NO_SQUISH integrator of Miller et al. (J. Chem. Phys. 116, 8649 (2002)) that the reference runs.
+// O: P <- c P + sqrt((1 - c^2) M kT) xi, L_k <- c L_k + sqrt((1 - c^2) I_k kT) xi with
+// c = exp(-gamma dt).  One thread per molecule; FP64 throughout.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -119,9 +122,9 @@ __global__ void k_md_begin(MDDev d, double dt, double gamma, const double *kT, u
   double R[9];
   quat_rot(q, R);
   if (F) half_kick(d, m, dt, F, R, p, l);
-  for (int c = 0; c < 3; ++c) x[c] += 0.5 * dt * p[c] / M;
-  free_rotor(0.5 * dt, I, l, q);
-  if (gamma > 0) {
+  if (gamma > 0) {  // A(dt/2) O A(dt/2)
+    for (int c = 0; c < 3; ++c) x[c] += 0.5 * dt * p[c] / M;
+    free_rotor(0.5 * dt, I, l, q);
     double c = exp(-gamma * dt), t = kT[d.msys[m]];
     double g[6];
     normals(seed, step, m, 0, g[0], g[1]);
@@ -130,9 +133,12 @@ __global__ void k_md_begin(MDDev d, double dt, double gamma, const double *kT, u
     double sp = sqrt((1 - c * c) * M * t);
     for (int k = 0; k < 3; ++k) p[k] = c * p[k] + sp * g[k];
     for (int k = 0; k < 3; ++k) l[k] = c * l[k] + sqrt((1 - c * c) * I[k] * t) * g[3 + k];
+    for (int c = 0; c < 3; ++c) x[c] += 0.5 * dt * p[c] / M;
+    free_rotor(0.5 * dt, I, l, q);
+  } else {  // NVE: A(dt)
+    for (int c = 0; c < 3; ++c) x[c] += dt * p[c] / M;
+    free_rotor(dt, I, l, q);
   }
-  for (int c = 0; c < 3; ++c) x[c] += 0.5 * dt * p[c] / M;
-  free_rotor(0.5 * dt, I, l, q);
   // keep the centre of mass in the box (sequential reduction by the lattice vectors)
   const double *H = box + 9 * d.msys[m];
   for (int c = 2; c >= 0; --c) {

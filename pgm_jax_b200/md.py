@@ -2,8 +2,8 @@
 
 The role of the reference's rigid-body engine (pgm_jax/md/simulation.py:55 Simulation with
 md/integrate.py:743-761 _step and md/thermostats.py:195-240 Langevin): one step is
-B A O A (forces) B on rigid bodies, run by the engine's kernels (csrc/pgm_md.cu), with the force
-call in between.  A step is captured once into a CUDA graph (the CG loop as a device-side while
+B A O A (forces) B on rigid bodies (B A (forces) B in NVE), run by the engine's kernels
+(csrc/pgm_md.cu), with the force call in between.  A step is captured once into a CUDA graph (the CG loop as a device-side while
 node) and replayed, so a step never returns to the host.
 
 Units: nm, ps, amu, kJ/mol, K.
@@ -23,7 +23,7 @@ KB = 0.0083144626181532  # kJ/mol/K (pgm_jax/units.py:16)
 
 
 def _quat_from_matrix(R: np.ndarray) -> np.ndarray:
-    """Unit quaternion (w, x, y, z) of a proper rotation matrix (Shepperd's method)."""
+    """Unit quaternion (w, x, y, z), w >= 0, of a proper rotation matrix (Shepperd's method)."""
     t = np.trace(R)
     if t > 0:
         s = np.sqrt(t + 1.0) * 2
@@ -38,40 +38,77 @@ def _quat_from_matrix(R: np.ndarray) -> np.ndarray:
         s = np.sqrt(1.0 + R[2, 2] - R[0, 0] - R[1, 1]) * 2
         q = [(R[1, 0] - R[0, 1]) / s, (R[0, 2] + R[2, 0]) / s, (R[1, 2] + R[2, 1]) / s, 0.25 * s]
     q = np.asarray(q)
-    return q / np.linalg.norm(q)
+    return q / np.linalg.norm(q) * (1.0 if q[0] >= 0 else -1.0)
 
 
 def rigid_bodies(system, pos: np.ndarray, H: np.ndarray):
     """Centres of mass, quaternions, principal-frame coordinates and principal moments of every molecule.
 
-    Molecules are made whole from their first atom (minimum image).  Returns (com (M, 3), quat (M, 4),
-    body (N, 3), inertia (M, 3)).
+    As pgm_jax/md/rigid.py:126-205: molecules are made whole (every atom at the minimum image of the
+    first); the instances of one Molecule object share the principal frame of the first instance
+    (moments ascending, a proper frame), and every instance's orientation is the Kabsch fit of that
+    template to it.  Returns (com (M, 3), quat (M, 4), body (N, 3), inertia (M, 3)).
     """
     pos = np.asarray(pos, float)
+    H = np.asarray(H, float)
+    Hinv = np.linalg.inv(H)
     M = system.nmol
     com = np.zeros((M, 3))
     quat = np.zeros((M, 4))
     body = np.zeros((system.n, 3))
     inertia = np.zeros((M, 3))
+    templates = {}
     for m in range(M):
         a0, a1 = system.mol_start[m], system.mol_start[m + 1]
-        x = pos[a0:a1] - pos[a0]
-        for c in (2, 1, 0):
-            n = np.round(x[:, c] / H[c, c])
-            x = x - n[:, None] * H[c][None, :]
-        x = x + pos[a0]
+        d = pos[a0:a1] - pos[a0]
+        for _ in range(2):  # a second pass catches what a skewed box leaves after one rounding
+            d = d - np.round(d @ Hinv) @ H
+        x = pos[a0] + d
         w = system.masses[a0:a1]
         c = (w[:, None] * x).sum(0) / w.sum()
-        d = x - c
-        Itens = np.sum(w[:, None, None] * ((d * d).sum(1)[:, None, None] * np.eye(3) - d[:, :, None] * d[:, None, :]), 0)
-        ev, V = np.linalg.eigh(Itens)
-        if np.linalg.det(V) < 0:
-            V[:, 2] = -V[:, 2]
+        y = x - c
+        key = id(system.molecules[m])
+        if key not in templates:
+            Itens = np.sum(w[:, None, None] * ((y * y).sum(1)[:, None, None] * np.eye(3) - y[:, :, None] * y[:, None, :]), 0)
+            ev, V = np.linalg.eigh(Itens)
+            if np.linalg.det(V) < 0:
+                V[:, 0] = -V[:, 0]
+            templates[key] = (y @ V, ev)
+        b, ev = templates[key]
+        U, _, Vt = np.linalg.svd(b.T @ y)  # Kabsch: y ~ b @ R.T
+        dd = np.sign(np.linalg.det(Vt.T @ U.T))
+        R = Vt.T @ np.diag([1.0, 1.0, dd]) @ U.T
         com[m] = c
-        quat[m] = _quat_from_matrix(V)
-        body[a0:a1] = d @ V
+        quat[m] = _quat_from_matrix(R)
+        body[a0:a1] = b
         inertia[m] = ev
     return com, quat, body, inertia
+
+
+def rigid_momenta(system, pos: np.ndarray, com: np.ndarray, quat: np.ndarray, vel: np.ndarray):
+    """Linear momenta P (M, 3) and body-frame angular momenta L (M, 3) of the rigid part of atom
+    velocities (rigid.py:235-265): P_k = sum m v, L_k = R_k^T sum m (r - X_k) x v, r the atoms of
+    the bodies."""
+    m = np.asarray(system.masses, float)
+    mol = np.asarray(system.mol)
+    P = np.zeros((system.nmol, 3))
+    np.add.at(P, mol, m[:, None] * vel)
+    L = np.zeros((system.nmol, 3))
+    np.add.at(L, mol, m[:, None] * np.cross(pos - com[mol], vel))
+    w, x, y, z = quat.T
+    Rm = np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)], -1),
+        np.stack([2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)], -1),
+        np.stack([2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1),
+    ], -2)
+    return P, np.einsum("kji,kj->ki", Rm, L)
+
+
+def _rot(q: np.ndarray) -> np.ndarray:
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
 
 
 class RigidMD:
@@ -80,10 +117,14 @@ class RigidMD:
         md = RigidMD(ff, pos, H, temperature=298.0, dt_fs=1.0, gamma_ps=2.0, seed=1)
         md.run(100)                      # steps (graph replays)
         md.temperature(), md.energy()
+
+    Momenta are drawn at `temperature` (seeded, no net momentum), or, with `velocities` (N, 3)
+    [nm/ps], taken from the rigid part of those atom velocities.  NVE (gamma_ps = 0) is the
+    reference's velocity Verlet: kick, one drift of dt, forces, kick.
     """
 
     def __init__(self, ff: PGMForceField, pos, H, temperature=298.0, dt_fs: float = 1.0, gamma_ps: float = 0.0,
-                 seed: int = 1, velocity_seed: int | None = None) -> None:
+                 seed: int = 1, velocity_seed: int | None = None, velocities=None) -> None:
         self.ff = ff
         self.dev = ff.device
         self.dt = dt_fs * 1e-3
@@ -118,6 +159,14 @@ class RigidMD:
         for k in range(ff.nsys):  # no net momentum per system
             sel = msys == k
             P[sel] -= P[sel].mean(0)
+        if velocities is not None:  # the rigid part of given atom velocities [nm/ps] (Simulation(velocities=...))
+            vel = np.asarray(velocities, float).reshape(ff.n, 3)
+            for k, sy in enumerate(systems):
+                sl = slice(int(ff.offsets[k]), int(ff.offsets[k + 1]))
+                sel = msys == k
+                R = np.stack([np.asarray(_rot(q)) for q in quat[sel]])
+                bpos = com[sel][sy.mol] + np.einsum("nij,nj->ni", R[sy.mol], body[sl])
+                P[sel], L[sel] = rigid_momenta(sy, bpos, com[sel], quat[sel], vel[sl])
         t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=self.dev)  # noqa: E731
         self.com, self.quat, self.mom, self.angmom = t(com), t(quat), t(P), t(L)
         self.box = t(boxes)

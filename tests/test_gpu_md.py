@@ -63,3 +63,30 @@ def test_langevin_reaches_temperature():
         md.run(10)
         temps.append(md.temperature()[0])
     assert 240.0 < np.mean(temps[10:]) < 360.0, temps
+
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_water512_install_check(pgm3p25_512_system, golden_pgm3p25_512, prec):
+    """The reference's install check (tests/test_water512.py): 10 NVE steps of 1 fs from
+    examples/water512 (512 pGM3P-25 waters with the file's velocities) at the run_md defaults
+    (cutoff 0.9 nm, Ewald 4.0 / nm, PME 48^3 order 8, LJ tail, tol 1e-5, mu4).  Step-10 potential
+    energy -2114884.256504 kJ/mol within 1e-9 (FP64) or 1e-6 (mixed), temperature 291.356783 K
+    within 1e-6 (1e-5 mixed), total energy between steps 5 and 10 within 0.5 kJ/mol."""
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.md import RigidMD
+
+    g = golden_pgm3p25_512
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(48, 48, 48), pme_order=8, lj_lrc=True, dipole_tol=1e-5, max_iter=50)
+    ff = PGMForceField(pgm3p25_512_system, g["box"], MDSettings(precision=prec, **st))
+    md = RigidMD(ff, g["pos"], g["box"], temperature=298.0, dt_fs=1.0, gamma_ps=0.0, velocities=g["vel"])
+    etot = []
+    for _ in range(10):
+        md.step()
+        e = md.energy()
+        etot.append(e["total"][0] + e["kinetic"][0])
+    epot, T = md.energy()["total"][0], md.temperature()[0]
+    rtol_e, rtol_t = (1e-9, 1e-6) if prec == "double" else (1e-6, 1e-5)
+    assert abs(epot - -2114884.256504) <= rtol_e * 2114884.256504, epot
+    assert abs(T - 291.356783) <= rtol_t * 291.356783, T
+    assert abs(etot[9] - etot[4]) < 0.5
+    assert int(md.result.status[0]) == 0

@@ -383,10 +383,12 @@ def test_pgm3p25_512_matches_reference_golden(pgm3p25_512_system, golden_pgm3p25
     ff = PGMForceField(pgm3p25_512_system, g["box"], MDSettings(precision=prec, **PGM3P25_512_SETTINGS))
     res = ff.compute(g["pos"], g["box"], None, ff.init_induction())
     assert int(res.status[0]) == 0
-    tol_e = 1e-9 if prec == "double" else 1e-6
+    # mixed: the FP32 LJ pair sum carries ~1e-6 of the van der Waals term (the reference's own mixed
+    # record is 5e-7 from its float64 one), so that component is held to 1e-5 as on the small box
+    tol_e = {"elec": 1e-9, "vdw": 1e-9, "total": 1e-9} if prec == "double" else {"elec": 1e-6, "vdw": 1e-5, "total": 1e-6}
     for k in ("elec", "vdw", "total"):
         ref = float(g[f"{prec}.energy.{k}"])
-        assert abs(float(res.energy[k][0]) - ref) <= tol_e * abs(ref), (k, float(res.energy[k][0]), ref)
+        assert abs(float(res.energy[k][0]) - ref) <= tol_e[k] * abs(ref), (k, float(res.energy[k][0]), ref)
     tol = 1e-8 if prec == "double" else 1e-5
     assert rms_rel(res.forces.cpu().numpy(), g[f"{prec}.forces"]) <= tol
     assert rms_rel(res.induction.mu.cpu().numpy(), g[f"{prec}.mu"]) <= tol
