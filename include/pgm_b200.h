@@ -214,6 +214,40 @@ long long pgm_row_pairs(PgmHandle *h);
  * (pgm_nn_param_count() floats, device) is the MLP of pgm_nn_predict; sigma is the scale of the
  * per-step changes in the invariants [e nm]. */
 PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff);
+/* ------------------------------------------------------------------ autotuner
+ * No counterpart in the reference (XLA chooses its own fusions).  The kernel variants of a handle:
+ * rowfield_lanes, the lanes that share one neighbour row in the CG matvec's row stream (32: a warp
+ * per atom; 16, 8: two or four atoms per warp); forces_blocks_per_sm, the minimum resident blocks of
+ * 256 threads the force pass is compiled for (2, 3, 4: registers against warps).  Unless fixed by
+ * pgm_set_tuning, the first pgm_compute that is not being captured times every variant on its own
+ * rows (CUDA events on its stream, the mean of 10 launches after one) and keeps the fastest;
+ * handles of the same precision, order, atoms, row capacity and grid size in one process share the
+ * result (from_cache).  Every variant computes the same sums (in another order of addition). */
+typedef struct {
+    int rowfield_lanes;        /* 32, 16 or 8 (default 32 before tuning) */
+    int forces_blocks_per_sm;  /* 2, 3 or 4 (default 3) */
+    double rowfield_ms[3];     /* timed launches: 32, 16, 8 lanes [ms] */
+    double forces_ms[3];       /* timed launches: 2, 3, 4 blocks per SM [ms] */
+    int tuned;                 /* 1 once timed (or taken from the cache) */
+    int from_cache;
+} PgmTuning;
+PgmStatus pgm_tuning(PgmHandle *h, PgmTuning *out);
+/* Fix the variants (0 leaves one as it is; both 0: autotune again at the next direct step). */
+PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm);
+/* Time the variants now on the last step's rows (synchronises the stream). */
+PgmStatus pgm_autotune(PgmHandle *h, void *stream);
+
+/* The learned guess's fallback (no counterpart in the reference, whose solver has no learned
+ * guess): with predictor 5 every solve starts from x4 + the model's correction with the fused start,
+ * whose residual r0 is known before the first CG iteration at no extra cost.  When max|alpha r0| /
+ * norm exceeds `factor` times the running mean of the same quantity for starts from the plain
+ * extrapolation x4 (recorded from the solves without the model and from every fallback), that
+ * system restarts from x4: r0 += A delta, one operator sweep of the correction delta (captured in a
+ * conditional node that runs only then).  factor 0 turns the check off; default 2. */
+PgmStatus pgm_set_nn_fallback(PgmHandle *h, double factor);
+/* Per system (host arrays of n_systems, either may be NULL): the number of fallbacks so far and the
+ * recorded mean start residual of the extrapolation (-1 before the first record). */
+PgmStatus pgm_nn_fallback_stats(PgmHandle *h, long long *fallbacks, double *ref_err);
 /* Features at a geometry: hist (4, N, 3) device (newest first, as PgmInduction.hist); bl_prev (N, 4)
  * floats, the graph's permanent field of the previous step, or NULL (c0 = 0); bl_out (N, 4)
  * receives this step's; inv, vec device.  Uses the sigma and graph cutoff of pgm_set_nn_model

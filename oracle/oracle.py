@@ -35,6 +35,8 @@ class _Set(C.Structure):
         ("perm", _i), ("induce", _i), ("lj", _i), ("lj_lrc", _i), ("cutoff", _d), ("beta", _d), ("K", _i * 3),
         ("order", _i), ("tol", _d), ("max_iter", _i), ("predictor", _i), ("fused", _i), ("norm_refresh", _i),
         ("peek", _d), ("nthreads", _i), ("elec_cutoff", _d),
+        ("iel", _i), ("iel_order", _i), ("iel_kappa", _d), ("iel_alpha", _d), ("iel_omega", _d), ("iel_precond", _i),
+        ("iel_iter", _i), ("iel_shadow", _i),
     ]
 
 
@@ -60,7 +62,8 @@ def lib():
         if not os.path.exists(LIB):
             build()
         _lib = C.CDLL(LIB)
-        for name in ("pgmo_compute", "pgmo_energy_fixed_mu", "pgmo_field", "pgmo_perm_dipoles"):
+        for name in ("pgmo_compute", "pgmo_energy_fixed_mu", "pgmo_field", "pgmo_perm_dipoles", "pgmo_compute_iel",
+                     "pgmo_iel_len"):
             getattr(_lib, name).restype = _i
         _lib.pgmo_erf_kernels.restype = None
         _lib.pgmo_bspline.restype = None
@@ -104,15 +107,25 @@ class Oracle:
             float(st.get("dipole_tol", 1e-5)), int(st.get("max_iter", 50)), pred, int(st.get("fused", True)),
             int(st.get("norm_refresh", 1000)), float(st.get("peek", 0.65)), int(nthreads),
             float(st.get("elec_cutoff") or 0.0),
+            {"none": 0, "0scf": 1, "scf": 2}[st.get("iel", "none")], int(st.get("iel_order", 7)),
+            float("nan") if st.get("iel_kappa") is None else float(st["iel_kappa"]),
+            float("nan") if st.get("iel_alpha") is None else float(st["iel_alpha"]), float(st.get("iel_omega", 1.0)),
+            {"jacobi": 0, "block": 1}[st.get("iel_precond", "block")], int(st.get("iel_iter", 1)),
+            int(st.get("iel_shadow", True)),
         )
+        self.iel = st.get("iel", "none") != "none"
 
     def init_induction(self) -> dict:
         n = self.sys.n
-        return {"mu": np.zeros((n, 3)), "hist": np.zeros((4, n, 3)), "count": 0, "norm": 1.0}
+        ind = {"mu": np.zeros((n, 3)), "hist": np.zeros((4, n, 3)), "count": 0, "norm": 1.0}
+        if self.iel:
+            ind["xl"] = np.zeros((lib().pgmo_iel_len(self._set.iel_order), n, 3))
+        return ind
 
     def compute(self, pos, H, ind: dict | None = None) -> dict:
         """One step: returns energy dict, forces, mu, iterations, residual, virial, and the new state."""
-        ind = self.init_induction() if ind is None else {k: (np.array(v) if k in ("mu", "hist") else v) for k, v in ind.items()}
+        ind = self.init_induction() if ind is None else {k: (np.array(v) if k in ("mu", "hist", "xl") else v)
+                                                          for k, v in ind.items()}
         pos = np.ascontiguousarray(pos, float)
         H = np.ascontiguousarray(H, float)
         mu = np.ascontiguousarray(ind["mu"], float)
@@ -121,8 +134,13 @@ class Oracle:
         nrm = C.c_double(float(ind["norm"]))
         F = np.zeros((self.sys.n, 3))
         r = _Res()
-        rc = lib().pgmo_compute(C.byref(self._s), C.byref(self._set), _p(pos), _p(H), _p(mu), _p(hist), C.byref(cnt),
-                                C.byref(nrm), _p(F), C.byref(r))
+        if self.iel:
+            xl = np.ascontiguousarray(ind["xl"], float)
+            rc = lib().pgmo_compute_iel(C.byref(self._s), C.byref(self._set), _p(pos), _p(H), _p(mu), _p(hist),
+                                        C.byref(cnt), C.byref(nrm), _p(xl), _p(F), C.byref(r))
+        else:
+            rc = lib().pgmo_compute(C.byref(self._s), C.byref(self._set), _p(pos), _p(H), _p(mu), _p(hist), C.byref(cnt),
+                                    C.byref(nrm), _p(F), C.byref(r))
         if rc != 0:
             raise RuntimeError(f"oracle compute failed ({rc})")
         return {
@@ -133,7 +151,8 @@ class Oracle:
             "residual": r.residual,
             "virial": np.array(r.virial[:]).reshape(3, 3),
             "pairs": r.pairs,
-            "induction": {"mu": mu, "hist": hist, "count": cnt.value, "norm": nrm.value},
+            "induction": dict({"mu": mu, "hist": hist, "count": cnt.value, "norm": nrm.value},
+                              **({"xl": xl} if self.iel else {})),
         }
 
     def energy_fixed_mu(self, pos, H, mu) -> dict:

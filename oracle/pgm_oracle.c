@@ -17,6 +17,8 @@
 #endif
 
 #define KE 138.935458 /* kJ mol^-1 nm e^-2, pgm_jax/units.py:31 */
+
+static int set_threads(const pgmo_settings *s);
 #define SQRT_PI 1.7724538509055160273
 
 /* ------------------------------------------------------------------ box helpers (md/box.py) */
@@ -693,7 +695,7 @@ static double dot(const double *a, const double *b, int m) {
 
 /* Jacobi PCG with the Polak-Ribiere beta, pmemd-pgm's max-norm test and the peek step
  * (forcefield.py:1714-1821). */
-static void cg(ctx_t *C, double *x, double *r, double norm, int *iters, double *resid) {
+static void cg_to(ctx_t *C, double *x, double *r, double norm, double tol, int max_iter, int *iters, double *resid) {
     const pgmo_settings *s = C->s;
     int n = C->sys->n, m = 3 * n;
     const double *al = C->sys->alpha;
@@ -706,7 +708,7 @@ static void cg(ctx_t *C, double *x, double *r, double norm, int *iters, double *
     for (int i = 0; i < m; ++i) err = fmax(err, fabs(al[i / 3] * r[i]));
     err /= norm;
     int it = 0;
-    while (err > s->tol && it < s->max_iter) {
+    while (err > tol && it < max_iter) {
         apply_A(C, p, Ap);
         double pAp = dot(p, Ap, m);
         double a = rz / fmax(pAp, 1e-300);
@@ -738,6 +740,10 @@ static void cg(ctx_t *C, double *x, double *r, double norm, int *iters, double *
     free(p);
     free(Ap);
     free(rn);
+}
+
+static void cg(ctx_t *C, double *x, double *r, double norm, int *iters, double *resid) {
+    cg_to(C, x, r, norm, C->s->tol, C->s->max_iter, iters, resid);
 }
 
 /* Initial guess and residual, fused or plain, then CG; pushes the history (forcefield.py:1917-2008). */
@@ -823,7 +829,7 @@ static void com_offsets(const pgmo_system *sys, const double *pos, const double 
  * non-pair terms (2011-2045), the covalent-frame pull-back (2362-2430), the strain derivative of the
  * same energy (608-662, 2628-2695) written out analytically. */
 static void energy_forces(ctx_t *C, const double *pos, const double *H, const double *mu, const double *pdip,
-                          double *forces, pgmo_result *res) {
+                          double *forces, pgmo_result *res, const double *delta, const int *blk, double keep_blk) {
     const pgmo_system *sys = C->sys;
     const pgmo_settings *s = C->s;
     int n = sys->n;
@@ -857,6 +863,19 @@ static void energy_forces(ctx_t *C, const double *pos, const double *H, const do
                     double cross = di[j] * dkx + dk[j] * dix;
                     g[j] = radial * x[j] + qi * G[1] * dk[j] - qk * G[1] * di[j] - G[2] * cross;
                     gx[j] += g[j];
+                }
+                if (delta) {
+                    /* iEL/0-SCF shadow energy: minus the pair terms of the dipoles delta alone
+                     * (forcefield.py:2316-2330); inside a preconditioner block scaled by 1 - 1/omega */
+                    double w = (blk && blk[i] >= 0 && blk[i] == blk[k]) ? keep_blk : 1.0;
+                    const double Di[3] = {w * delta[3 * i], w * delta[3 * i + 1], w * delta[3 * i + 2]};
+                    const double *Dk = delta + 3 * k;
+                    double Dix = Di[0] * x[0] + Di[1] * x[1] + Di[2] * x[2];
+                    double Dkx = Dk[0] * x[0] + Dk[1] * x[1] + Dk[2] * x[2];
+                    double DiDk = Di[0] * Dk[0] + Di[1] * Dk[1] + Di[2] * Dk[2];
+                    e += G[2] * Dix * Dkx - G[1] * DiDk;
+                    double rad2 = -G[3] * Dix * Dkx + G[2] * DiDk;
+                    for (int j = 0; j < 3; ++j) gx[j] += rad2 * x[j] + G[2] * (Di[j] * Dkx + Dk[j] * Dix);
                 }
                 se_t += e;
                 double c = -qk * G[1] - G[2] * dkx;
@@ -917,6 +936,18 @@ static void energy_forces(ctx_t *C, const double *pos, const double *H, const do
     double Wi[9] = {0};
     pme_influence_virial(&C->P, sys->q, d, n, Wi);
     for (int k = 0; k < 9; ++k) W[k] += Wr[k] + KE * Wi[k];
+    /* shadow energy: minus the reciprocal energy of delta alone; its position gradient at fixed delta
+     * (the strain derivative stays the fixed-mu one of strain_derivative, forcefield.py:2628) */
+    double Erec_d = 0.0;
+    if (delta) {
+        Erec_d = pme_energy_phi(&C->P, NULL, delta, n);
+#pragma omp parallel for
+        for (int i = 0; i < n; ++i) {
+            double gd[3], gr[3];
+            pme_gather(&C->P, i, 0.0, delta + 3 * i, gd, gr);
+            for (int j = 0; j < 3; ++j) forces[3 * i + j] += KE * gr[j];
+        }
+    }
     /* covalent-dipole frames: p_i = sum c unit(r_j - r_i) pulled back (vjp of forcefield.py:1032-1042) */
     for (int m = 0; m < (s->perm ? sys->ncov : 0); ++m) {
         int i = sys->cov_i[m], j = sys->cov_j[m];
@@ -942,8 +973,17 @@ static void energy_forces(ctx_t *C, const double *pos, const double *H, const do
     }
     double vol = fabs(det3(H));
     double uself = -(s->beta / SQRT_PI) * q2 - 0.5 * C->c_self * d2;
+    if (delta) { /* forcefield.py:2037-2042 */
+        double dd2 = 0.0, dda = 0.0;
+        for (int i = 0; i < n; ++i)
+            for (int a = 0; a < 3; ++a) {
+                dd2 += delta[3 * i + a] * delta[3 * i + a];
+                dda += delta[3 * i + a] * delta[3 * i + a] / (2.0 * sys->alpha[i]);
+            }
+        uself += 0.5 * C->c_self * dd2 - (1.0 - 1.0 / s->iel_omega) * dda;
+    }
     double ubg = -M_PI * qs * qs / (2.0 * vol * s->beta * s->beta);
-    double e_elec = 0.5 * KE * se + KE * (Erec + uself + ubg + upol);
+    double e_elec = 0.5 * KE * se + KE * (Erec - Erec_d + uself + ubg + upol);
     double tail = (s->lj && s->lj_lrc) ? lj_tail(sys, vol, s->cutoff) : 0.0;
     double e_vdw = 0.5 * sl + tail;
     for (int a = 0; a < 3; ++a) W[a * 3 + a] += -KE * ubg - 2.0 * tail;
@@ -955,6 +995,214 @@ static void energy_forces(ctx_t *C, const double *pos, const double *H, const do
     free(d);
     free(dEdd);
     free(off);
+}
+
+/* ------------------------------------------------------------------ extended-Lagrangian dipoles */
+/* Dissipative extended-Lagrangian Verlet coefficients (kappa, a, c_0..c_K) of Niklasson et al.,
+ * J. Chem. Phys. 130, 214109 (2009), the table of forcefield.py:667-676. */
+static const struct {
+    int K;
+    double kappa, a;
+    double c[10];
+} XL[] = {
+    {0, 1.0, 0.0, {0}},
+    {3, 1.69, 0.150, {-2, 3, 0, -1}},
+    {4, 1.75, 0.057, {-3, 6, -2, -2, 1}},
+    {5, 1.82, 0.018, {-6, 14, -8, -3, 4, -1}},
+    {6, 1.84, 0.0055, {-14, 36, -27, -2, 12, -6, 1}},
+    {7, 1.86, 0.0016, {-36, 99, -88, 11, 32, -25, 8, -1}},
+    {8, 1.88, 0.00044, {-99, 286, -286, 78, 78, -90, 42, -10, 1}},
+    {9, 1.89, 0.00012, {-286, 858, -936, 364, 168, -300, 184, -63, 12, -1}},
+};
+
+static int xl_row(int order) {
+    for (int r = 0; r < (int)(sizeof(XL) / sizeof(XL[0])); ++r)
+        if (XL[r].K == order) return r;
+    return -1;
+}
+
+/* Auxiliary dipoles kept: x_{n+1} and x_n ... x_{n-K} after a step, at least 3 (forcefield.py:1476-1479). */
+int pgmo_iel_len(int order) {
+    int nc = order == 0 ? 1 : order + 1;
+    return nc + 1 > 3 ? nc + 1 : 3;
+}
+
+/* Block of every atom for the block preconditioner: molecules of 2..8 atoms (forcefield.py:1487-1517),
+ * -1 elsewhere. */
+static int *iel_blocks(const pgmo_system *sys) {
+    int *b = malloc(sizeof(int) * sys->n);
+    int nb = 0;
+    for (int m = 0; m < sys->nmol; ++m) {
+        int sz = sys->mol_start[m + 1] - sys->mol_start[m];
+        int id = (sz >= 2 && sz <= 8) ? nb++ : -1;
+        for (int i = sys->mol_start[m]; i < sys->mol_start[m + 1]; ++i) b[i] = id;
+    }
+    return b;
+}
+
+/* delta = M^-1 r per block, M = diag(1/alpha) + sum of the same-molecule row tensors G1 I - G2 x x^T
+ * (forcefield.py:1530-1556), by Gaussian elimination with partial pivoting; alpha r outside blocks. */
+static void block_solve(ctx_t *C, const int *blk, const double *r, double *d) {
+    const pgmo_system *sys = C->sys;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int m = 0; m < sys->nmol; ++m) {
+        int i0 = sys->mol_start[m], i1 = sys->mol_start[m + 1], nb = i1 - i0, N = 3 * nb;
+        if (blk[i0] < 0) {
+            for (int i = i0; i < i1; ++i)
+                for (int a = 0; a < 3; ++a) d[3 * i + a] = sys->alpha[i] * r[3 * i + a];
+            continue;
+        }
+        double M[24][25];
+        for (int u = 0; u < N; ++u)
+            for (int v = 0; v <= N; ++v) M[u][v] = 0.0;
+        for (int i = i0; i < i1; ++i) {
+            int li = i - i0;
+            for (int a = 0; a < 3; ++a) {
+                M[3 * li + a][3 * li + a] += 1.0 / sys->alpha[i];
+                M[3 * li + a][N] = r[3 * i + a];
+            }
+            for (long long o = C->R.start[i]; o < C->R.start[i + 1]; ++o) {
+                int k = C->R.k[o];
+                if (k < i0 || k >= i1 || !C->R.we[o]) continue;
+                const double *x = C->R.x + 3 * o, *G = C->R.G + 4 * o;
+                int lk = k - i0;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        M[3 * li + a][3 * lk + b] += (a == b ? G[1] : 0.0) - G[2] * x[a] * x[b];
+            }
+        }
+        for (int c = 0; c < N; ++c) {
+            int pr = c;
+            for (int u = c + 1; u < N; ++u)
+                if (fabs(M[u][c]) > fabs(M[pr][c])) pr = u;
+            if (pr != c)
+                for (int v = 0; v <= N; ++v) {
+                    double t = M[c][v];
+                    M[c][v] = M[pr][v];
+                    M[pr][v] = t;
+                }
+            for (int u = c + 1; u < N; ++u) {
+                double f = M[u][c] / M[c][c];
+                for (int v = c; v <= N; ++v) M[u][v] -= f * M[c][v];
+            }
+        }
+        for (int c = N - 1; c >= 0; --c) {
+            double acc = M[c][N];
+            for (int v = c + 1; v < N; ++v) acc -= M[c][v] * M[v][N];
+            M[c][N] = acc / M[c][c];
+        }
+        for (int i = i0; i < i1; ++i)
+            for (int a = 0; a < 3; ++a) d[3 * i + a] = M[3 * (i - i0) + a][N];
+    }
+}
+
+/* One iEL step (forcefield.py:1558-1650): the warm-up steps solve to tol (from mu or alpha b on the
+ * first, from x after), the others take x = xl[0] and either the 0-SCF update mu = x + omega delta,
+ * delta = alpha r(x) or M^-1 r(x), r(x) = field(q, p + x) - x / alpha (one field sweep, no CG), or
+ * ("scf") iel_iter CG iterations from x; then x_{n+1} = 2 x_n - x_{n-1} + kappa (mu - x_n)
+ * + a sum_k c_k x_{n-k}.  delta_out: the shadow displacement (0 in the warm-up). */
+static void solve_iel(ctx_t *C, const double *q, const double *pdip, const int *blk, double *mu, double *hist, int *count,
+                      double *normp, double *xl, int *iters, double *resid, double *delta_out) {
+    const pgmo_settings *s = C->s;
+    int n = C->sys->n, m = 3 * n;
+    const double *al = C->sys->alpha;
+    int row = xl_row(s->iel_order);
+    double kap = isnan(s->iel_kappa) ? XL[row].kappa : s->iel_kappa;
+    double a = isnan(s->iel_alpha) ? XL[row].a : s->iel_alpha;
+    int nc = s->iel_order == 0 ? 1 : s->iel_order + 1, K1 = pgmo_iel_len(s->iel_order);
+    int first = *count == 0, warm = *count < (s->iel_order > 2 ? s->iel_order : 2) + 1;
+    double *x = xl, *r0 = malloc(sizeof(double) * m), *b = malloc(sizeof(double) * m), *Ax = malloc(sizeof(double) * m),
+           *dd = malloc(sizeof(double) * m), *d = calloc(m, sizeof(double));
+    double norm;
+    *iters = 0;
+    if (warm) {
+        field(C, q, pdip, b);
+        double sab = 0.0;
+        int any = 0;
+        for (int i = 0; i < m; ++i) {
+            sab += fabs(al[i / 3] * b[i]);
+            any |= mu[i] != 0.0;
+        }
+        norm = sab / m + 1e-300;
+        for (int i = 0; i < m; ++i) dd[i] = first ? (any ? mu[i] : al[i / 3] * b[i]) : x[i];
+        apply_A(C, dd, Ax);
+        for (int i = 0; i < m; ++i) r0[i] = b[i] - Ax[i];
+        cg_to(C, dd, r0, norm, s->tol, s->max_iter, iters, resid);
+        memcpy(mu, dd, sizeof(double) * m);
+    } else {
+        for (int i = 0; i < m; ++i) dd[i] = pdip[i] + x[i];
+        field(C, q, dd, r0);
+        for (int i = 0; i < m; ++i) r0[i] -= x[i] / al[i / 3];
+        norm = *normp;
+        if (s->iel == 1) {
+            if (s->iel_precond == 1) block_solve(C, blk, r0, d);
+            else
+                for (int i = 0; i < m; ++i) d[i] = al[i / 3] * r0[i];
+            double mx = 0.0;
+            for (int i = 0; i < m; ++i) {
+                d[i] *= s->iel_omega;
+                mu[i] = x[i] + d[i];
+                mx = fmax(mx, fabs(d[i]));
+            }
+            *resid = mx / norm;
+        } else {
+            memcpy(dd, x, sizeof(double) * m);
+            int k = s->iel_iter;
+            cg_to(C, dd, r0, norm, k > 0 ? 0.0 : s->tol, k > 0 ? k : s->max_iter, iters, resid);
+            memcpy(mu, dd, sizeof(double) * m);
+            for (int i = 0; i < m; ++i) d[i] = mu[i] - x[i];
+        }
+    }
+    /* Xh: every entry mu on the first step, xl with xl[0] = mu in the warm-up, else xl */
+    double *Xh = malloc(sizeof(double) * (size_t)K1 * m);
+    for (int j = 0; j < K1; ++j)
+        memcpy(Xh + (size_t)j * m, first ? mu : (j == 0 && warm ? mu : xl + (size_t)j * m), sizeof(double) * m);
+    for (int i = 0; i < m; ++i) {
+        double v = 2.0 * Xh[i] - Xh[m + i] + (warm ? 0.0 : kap * d[i]);
+        if (a != 0.0)
+            for (int k = 0; k < nc; ++k) v += a * XL[row].c[k] * Xh[(size_t)k * m + i];
+        xl[i] = v;
+    }
+    for (int j = 1; j < K1; ++j) memcpy(xl + (size_t)j * m, Xh + (size_t)(j - 1) * m, sizeof(double) * m);
+    memmove(hist + m, hist, sizeof(double) * 3 * m);
+    memcpy(hist, mu, sizeof(double) * m);
+    *count += 1;
+    *normp = norm;
+    for (int i = 0; i < m; ++i) delta_out[i] = (warm || s->iel != 1) ? 0.0 : d[i];
+    free(Xh);
+    free(r0);
+    free(b);
+    free(Ax);
+    free(dd);
+    free(d);
+}
+
+int pgmo_compute_iel(const pgmo_system *sys, const pgmo_settings *s, const double *pos, const double *H, double *mu,
+                     double *hist, int *count, double *norm, double *xl, double *forces, pgmo_result *res) {
+    if (xl_row(s->iel_order) < 0 || s->iel < 1 || s->iel > 2 || !(s->iel_omega > 0)) return 1;
+    set_threads(s);
+    ctx_t C;
+    ctx_init(&C, sys, s, pos, H);
+    int n = sys->n;
+    double *p = calloc(3 * n, sizeof(double)), *delta = calloc(3 * n, sizeof(double));
+    int *blk = s->iel_precond == 1 ? iel_blocks(sys) : NULL;
+    if (s->perm) perm_dipoles_impl(sys, pos, H, p);
+    res->iterations = 0;
+    res->residual = 0.0;
+    int shadow = 0;
+    if (s->induce) {
+        int warm = *count < (s->iel_order > 2 ? s->iel_order : 2) + 1;
+        solve_iel(&C, sys->q, p, blk, mu, hist, count, norm, xl, &res->iterations, &res->residual, delta);
+        shadow = s->iel == 1 && s->iel_shadow && !warm;
+    } else {
+        memset(mu, 0, sizeof(double) * 3 * n);
+    }
+    energy_forces(&C, pos, H, mu, p, forces, res, shadow ? delta : NULL, blk, 1.0 - 1.0 / s->iel_omega);
+    free(p);
+    free(delta);
+    free(blk);
+    ctx_free(&C);
+    return 0;
 }
 
 static int set_threads(const pgmo_settings *s) {
@@ -979,7 +1227,7 @@ int pgmo_compute(const pgmo_system *sys, const pgmo_settings *s, const double *p
         solve(&C, sys->q, p, mu, hist, count, norm, &res->iterations, &res->residual);
     else
         memset(mu, 0, sizeof(double) * 3 * n);
-    energy_forces(&C, pos, H, mu, p, forces, res);
+    energy_forces(&C, pos, H, mu, p, forces, res, NULL, NULL, 1.0);
     free(p);
     ctx_free(&C);
     return 0;
@@ -994,7 +1242,7 @@ int pgmo_energy_fixed_mu(const pgmo_system *sys, const pgmo_settings *s, const d
     double *p = calloc(3 * n, sizeof(double)), *f = malloc(sizeof(double) * 3 * n);
     if (s->perm) perm_dipoles_impl(sys, pos, H, p);
     pgmo_result r;
-    energy_forces(&C, pos, H, mu, p, f, &r);
+    energy_forces(&C, pos, H, mu, p, f, &r, NULL, NULL, 1.0);
     out[0] = r.elec;
     out[1] = r.vdw;
     out[2] = r.total;

@@ -49,6 +49,15 @@ typedef struct {
     double peek;
     int nthreads;          /* OpenMP threads (0: default) */
     double elec_cutoff;    /* electrostatics cutoff [nm] (0 or >= cutoff: the pair cutoff; forcefield.py:44-58) */
+    /* extended-Lagrangian dipoles (forcefield.py:246-282 ExtendedLagrangian, 1452-1650) */
+    int iel;               /* 0 none, 1 "0scf", 2 "scf" */
+    int iel_order;         /* Niklasson dissipation order K: 0, 3..9 */
+    double iel_kappa;      /* NaN: the table's value for K */
+    double iel_alpha;      /* NaN: the table's value for K */
+    double iel_omega;      /* 0scf: mu = x + omega delta */
+    int iel_precond;       /* 0 jacobi, 1 block (molecules of 2..8 atoms) */
+    int iel_iter;          /* scf: CG iterations per step (0: to tol) */
+    int iel_shadow;        /* 0scf: energy and forces of the shadow potential */
 } pgmo_settings;
 
 typedef struct {
@@ -65,6 +74,12 @@ int pgmo_compute(const pgmo_system *sys, const pgmo_settings *s, const double *p
                  double *mu, double *hist, int *count, double *norm, double *forces, pgmo_result *res);
 
 /* Energy at fixed induced dipoles mu (PGMForceField.energy_fixed_mu, forcefield.py:2249). */
+/* iEL step: as pgmo_compute with the auxiliary dipoles xl (K1, n, 3), K1 = pgmo_iel_len(order),
+ * newest first (updated in place); the warm-up steps (count < max(K, 2) + 1) solve to tol. */
+int pgmo_compute_iel(const pgmo_system *sys, const pgmo_settings *s, const double *pos, const double *H, double *mu,
+                     double *hist, int *count, double *norm, double *xl, double *forces, pgmo_result *res);
+int pgmo_iel_len(int order);
+
 int pgmo_energy_fixed_mu(const pgmo_system *sys, const pgmo_settings *s, const double *pos, const double *H,
                          const double *mu, double out[3]);
 

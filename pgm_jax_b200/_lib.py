@@ -25,7 +25,7 @@ EXPORTS = (
     "pgm_pimd_last_error", "pgm_graph_begin",
     "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
     "pgm_set_nn_model", "pgm_nn_features", "pgm_nn_param_count", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam",
-    "pgm_nn_last_error",
+    "pgm_nn_last_error", "pgm_set_nn_fallback", "pgm_nn_fallback_stats", "pgm_tuning", "pgm_set_tuning", "pgm_autotune",
 )
 
 STATUS_ROW_OVERFLOW = 0x1
@@ -33,6 +33,13 @@ STATUS_CG_MAXITER = 0x2
 STATUS_NONFINITE = 0x4
 STATUS_BAD_BOX = 0x8
 STATUS_LIST_OVERFLOW = 0x10
+
+
+class PgmTuning(C.Structure):
+    _fields_ = [
+        ("rowfield_lanes", C.c_int), ("forces_blocks_per_sm", C.c_int), ("rowfield_ms", C.c_double * 3),
+        ("forces_ms", C.c_double * 3), ("tuned", C.c_int), ("from_cache", C.c_int),
+    ]
 
 
 class PgmSettings(C.Structure):
@@ -138,7 +145,15 @@ def load(path: str | None = None):
     lib.pgm_nn_loss_grad.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_float, vp, vp]
     lib.pgm_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
     lib.pgm_nn_last_error.restype = C.c_char_p
-    for n in ("pgm_set_nn_model", "pgm_nn_features", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam"):
+    lib.pgm_tuning.argtypes = [H, C.POINTER(PgmTuning)]
+    lib.pgm_set_tuning.argtypes = [H, C.c_int, C.c_int]
+    lib.pgm_autotune.argtypes = [H, vp]
+    for n in ("pgm_tuning", "pgm_set_tuning", "pgm_autotune"):
+        getattr(lib, n).restype = C.c_int
+    lib.pgm_set_nn_fallback.argtypes = [H, C.c_double]
+    lib.pgm_nn_fallback_stats.argtypes = [H, vp, vp]
+    for n in ("pgm_set_nn_model", "pgm_nn_features", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam",
+              "pgm_set_nn_fallback", "pgm_nn_fallback_stats"):
         getattr(lib, n).restype = C.c_int
     lib.pgm_graph_begin.argtypes = [vp]
     lib.pgm_graph_end.argtypes = [vp, C.POINTER(vp)]

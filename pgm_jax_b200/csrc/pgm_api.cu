@@ -4,6 +4,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -107,6 +110,11 @@ struct EngineBase {
   virtual int elec_capacity() const = 0;
   virtual int max_vdw_count() = 0;
   virtual void set_nn(const float *w, float sigma, float rg) = 0;
+  virtual void set_nn_fallback(double factor) = 0;
+  virtual void set_tuning(int rowfield_lanes, int forces_blocks) = 0;
+  virtual void autotune(cudaStream_t st) = 0;
+  virtual PgmTuning tuning() const = 0;
+  virtual void nn_fallback_stats(long long *fallbacks, double *ref_err) = 0;
   virtual void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const float *bl_prev,
                            float *bl_out, float *inv, float *vec) = 0;
   virtual void set_list_capacity(int c) = 0;
@@ -147,6 +155,18 @@ struct FftGroup {
   size_t smem = 0;
   DBuf<int> sys, tile0;
 };
+
+// Autotuner choices, shared by the handles of one process with the same precision, spline
+// order, atoms, row capacity and grid size (timed once per such shape).
+struct TuneKey {
+  int tsize, order, nt, mc;
+  long long rgrid;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(tsize, order, nt, mc, rgrid) < std::tie(o.tsize, o.order, o.nt, o.mc, o.rgrid);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, PgmTuning> g_tune_cache;
 
 template <typename T, int P>
 struct Engine : EngineBase {
@@ -190,6 +210,10 @@ struct Engine : EngineBase {
   DBuf<float> nn_w, nn_inv, nn_vec, nn_mu, nn_chan;  // learned guess: model and per-atom features
   DBuf<__nv_bfloat16> nn_wb;  // the model's weight matrices in BF16 (converted when the model is set)
   bool nn_on = false;
+  PgmTuning tune{};          // kernel variants in use (autotuned at the first direct step unless fixed)
+  bool tune_fixed = false;
+  double nn_fb_factor = 2.0;  // learned guess: fall back to x4 when its start residual is above this x the record
+  DBuf<int> dfb;              // some system falls back (the host-driven solve reads it)
   int last_iters = 0;  // CG iterations of the last host-driven solve (sizes the unrolled part of a capture)
   const double *last_hist = nullptr;  // the history of the last predictor solve (profiling)
   DBuf<float4> nn_bl;  // the graph's permanent field of the last solve (for the change channel)
@@ -508,7 +532,7 @@ struct Engine : EngineBase {
     CK(cudaMemset(cell_count.p, 0, sizeof(int) * ncell));
     CK(cudaMemset(nb_builds.p, 0, sizeof(long long)));
     { int one = 1; CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice)); }
-    rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(2); dany.alloc(1); cg_done.alloc(1);
+    rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(2); dany.alloc(1); cg_done.alloc(1); dfb.alloc(1);
     CK(cudaMemset(cg_done.p, 0, sizeof(unsigned)));
     if (split) rnv.alloc(nt);
     alloc_rows();
@@ -631,6 +655,113 @@ struct Engine : EngineBase {
       });
   }
 
+  // ---------------------------------------------------------------- autotuner
+  // The tuned kernels: the CG matvec's row stream k_rowfield (lanes per row 32 / 16 / 8: how a
+  // neighbour row is split over a warp) and the force pass k_forces (at least 2 / 3 / 4 blocks of
+  // 256 threads per SM: registers against resident warps).
+  template <bool WITH_Q, int ACT>
+  void rowfield(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin, pgm::v4<T> *out, bool pdl, int lpr = 0) {
+    auto go = [&](auto L) {
+      constexpr int LPR = decltype(L)::value;
+      if (pdl) {
+        launch_pdl(pgm::k_rowfield<T, WITH_Q, ACT, LPR>, nwblk, 8 * LPR, 0, st, a, vin, out);
+      } else {
+        pgm::k_rowfield<T, WITH_Q, ACT, LPR><<<nwblk, 8 * LPR, 0, st>>>(a, vin, out);
+        check_launch();
+      }
+    };
+    const int l = lpr ? lpr : tune.rowfield_lanes;
+    if (l == 16) go(std::integral_constant<int, 16>{});
+    else if (l == 8) go(std::integral_constant<int, 8>{});
+    else go(std::integral_constant<int, 32>{});
+  }
+  void forces_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, bool pdl, int minb = 0) {
+    auto go = [&](auto B) {
+      constexpr int MINB = decltype(B)::value;
+      if (pdl) {
+        launch_pdl(pgm::k_forces<T, P, MINB>, nwblk, 256, 0, st, a, mu);
+      } else {
+        pgm::k_forces<T, P, MINB><<<nwblk, 256, 0, st>>>(a, mu);
+        check_launch();
+      }
+    };
+    const int b = minb ? minb : tune.forces_blocks_per_sm;
+    if (b == 2) go(std::integral_constant<int, 2>{});
+    else if (b == 4) go(std::integral_constant<int, 4>{});
+    else go(std::integral_constant<int, 3>{});
+  }
+  void set_tuning(int lanes, int blocks) override {
+    ++generation;  // captured steps hold the old variants
+    tune_fixed = lanes > 0 || blocks > 0;
+    if (lanes > 0) tune.rowfield_lanes = lanes;
+    if (blocks > 0) tune.forces_blocks_per_sm = blocks;
+    if (!tune_fixed) tune.tuned = 0;  // autotune again at the next direct step
+  }
+  PgmTuning tuning() const override { return tune; }
+  // Times every variant on this handle's rows (the last step's geometry; CUDA events on st, a
+  // warm-up launch and the mean of 10) and keeps the fastest of each kernel.  Writes only scratch
+  // buffers: the last call's outputs are untouched.
+  void autotune(cudaStream_t st) override {
+    const TuneKey key{(int)sizeof(T), P, nt, mc, rgrid};
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        tune = it->second;
+        tune.from_cache = 1;
+        ++generation;
+        return;
+      }
+    }
+    pgm::Dev<T> a = dev(nullptr, nullptr, 0, forces_tmp.p, d_status.p);
+    a.pos = last_pos;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const long long l0 = launches;
+    auto time = [&](auto &&launch) {
+      launch();
+      CK(cudaEventRecord(e0, st));
+      for (int r = 0; r < 10; ++r) launch();
+      CK(cudaEventRecord(e1, st));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      return ms / 10.0;
+    };
+    const int lanes[3] = {32, 16, 8}, blocks[3] = {2, 3, 4};
+    int bl = 0, bb = 0;
+    for (int v = 0; v < 3; ++v) {
+      tune.rowfield_ms[v] = time([&] { rowfield<false, 0>(st, a, X.p, Fv.p, false, lanes[v]); });
+      tune.forces_ms[v] = time([&] { forces_pass(st, a, nullptr, false, blocks[v]); });
+      if (tune.rowfield_ms[v] < tune.rowfield_ms[bl]) bl = v;
+      if (tune.forces_ms[v] < tune.forces_ms[bb]) bb = v;
+    }
+    launches = l0;
+    CK(cudaEventDestroy(e0));
+    CK(cudaEventDestroy(e1));
+    tune.rowfield_lanes = lanes[bl];
+    tune.forces_blocks_per_sm = blocks[bb];
+    tune.tuned = 1;
+    tune.from_cache = 0;
+    ++generation;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = tune;
+  }
+
+  void set_nn_fallback(double factor) override {
+    ++generation;  // a captured step holds the fallback node only when the check is on
+    nn_fb_factor = factor;
+  }
+  void nn_fallback_stats(long long *fallbacks, double *ref_err) override {
+    std::vector<pgm::CGSys> h(nsys);
+    CK(cudaMemcpy(h.data(), d_cg.p, sizeof(pgm::CGSys) * nsys, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < nsys; ++k) {
+      if (fallbacks) fallbacks[k] = h[k].fallbacks;
+      if (ref_err) ref_err[k] = h[k].ref_n > 0 ? h[k].ref_err : -1.0;
+    }
+  }
+
   void set_nn(const float *w, float sigma, float rg) override {
     ++generation;  // a captured step depends on whether a model is set, and on sigma and rg
     nn_on = w != nullptr;
@@ -706,7 +837,7 @@ struct Engine : EngineBase {
       else if (which == 1) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
       else if (which == 2) {
         fft_chain(st, a, 0, false);
-      } else if (which == 3) pgm::k_forces<T, P><<<nwblk, 256, 0, st>>>(a, nullptr);
+      } else if (which == 3) forces_pass(st, a, nullptr, false);
       else if (which == 4) {
         pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
         pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a);
@@ -718,7 +849,7 @@ struct Engine : EngineBase {
           with_fft_len(g->K, [&](auto Lc) {
             pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
           });
-      } else if (which == 7) pgm::k_rowfield<T, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, Fv.p);
+      } else if (which == 7) rowfield<false, 0>(st, a, Pv.p, Fv.p, false);
       else if (which == 8) pgm::k_rowmat<T, P, false, 1, 0, false><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
       else if (which == 9) {  // a whole operator sweep with the row/PME overlap
         sweep<false, false, 0, 1>(st, a, Pv.p, AP.p);
@@ -876,7 +1007,7 @@ struct Engine : EngineBase {
       // Q is zero here: cleared at creation and, after every spread, by the forward k2 FFT pass
       pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
       const pgm::v4<T> *dv = UPDATE_P ? Pv.p : vin;
-      launch_pdl(pgm::k_rowfield<T, WITH_Q, ACT>, nwblk, 256, 0, st, a, dv, Fv.p);
+      rowfield<WITH_Q, ACT>(st, a, dv, Fv.p, true);
       fft_chain(st, a, ACT, false);
       launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false>, nwblk, 256, 0, st, a, dv, out);
       return;
@@ -887,7 +1018,7 @@ struct Engine : EngineBase {
     launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
     CK(cudaEventRecord(ef, st));
     CK(cudaStreamWaitEvent(ax, ef, 0));
-    pgm::k_rowfield<T, WITH_Q, ACT><<<nwblk, 256, 0, ax>>>(a, vin, Fv.p); check_launch();
+    rowfield<WITH_Q, ACT>(ax, a, vin, Fv.p, false);
     CK(cudaEventRecord(ej, ax));
     fft_chain(st, a, ACT, false);
     CK(cudaStreamWaitEvent(st, ej, 0));
@@ -959,7 +1090,11 @@ struct Engine : EngineBase {
     const bool captured = cs == cudaStreamCaptureStatusActive;
     // captured: the plain start's second sweep sits in a conditional IF node whose condition
     // k_cg_setup raises when some system takes the plain start (else the node's kernels are skipped)
-    cudaGraphConditionalHandle cond2 = 0;
+    // the learned guess's check: its start residual against the record of the extrapolation's
+    // (k_cg_begin); a fallback restarts those systems from x4 with one operator sweep, captured in
+    // a conditional IF node that runs only when some system falls back
+    const bool check_nn = use_nn && nn_fb_factor > 0.0;
+    cudaGraphConditionalHandle cond2 = 0, condfb = 0;
     if (captured) {
       cudaGraph_t g;
       const cudaGraphNode_t *deps = nullptr;
@@ -967,9 +1102,11 @@ struct Engine : EngineBase {
       unsigned long long id;
       CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
       CK(cudaGraphConditionalHandleCreate(&cond2, g, 0, cudaGraphCondAssignDefault));
+      if (check_nn) CK(cudaGraphConditionalHandleCreate(&condfb, g, 0, cudaGraphCondAssignDefault));
     }
     launch_pdl(pgm::k_cg_setup, grid1(nsys, 64), 64, 0, st, d_cg.p, nsys, mode == 0 ? (const int32_t *)ind->count : nullptr,
-               (const double *)ind->norm, mode == 0 ? K : 0, set.fused, std::max(1, set.norm_refresh), mode, cond2, captured ? 1 : 0);
+               (const double *)ind->norm, mode == 0 ? K : 0, set.fused, std::max(1, set.norm_refresh), mode, cond2, captured ? 1 : 0,
+               use_nn ? 1 : 0);
     if (mode == 1) {
       // x0 = ind->mu with the plain start: X = mu, have = 1
       pgm::k_energy_start<T><<<grid1(nt), 256, 0, st>>>(a, ind->mu);
@@ -993,7 +1130,26 @@ struct Engine : EngineBase {
     if (captured) conditional_node(st, cond2, cudaGraphCondTypeIf, plain_start);
     else plain_start(st);
     pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
-    launch_pdl(pgm::k_cg_begin, 1, 256, 0, st, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p);
+    launch_pdl(pgm::k_cg_begin, 1, 256, 0, st, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p,
+               mode == 0 && set.predictor == 5 ? nn_fb_factor : 0.0, 0, condfb, captured && check_nn ? 1 : 0, dfb.p);
+    if (check_nn) {
+      auto fallback = [&](cudaStream_t s2) {
+        launch_pdl(pgm::k_fb_prep<T>, grid1(nt), 256, 0, s2, a, (const float *)nn_mu.p);
+        sweep<false, false, 3, 1>(s2, a, D.p, AP.p);  // A delta
+        launch_pdl(pgm::k_cg_init<T, true>, ntblk, 256, 0, s2, a, (const float *)nn_mu.p);
+        launch_pdl(pgm::k_cg_begin, 1, 256, 0, s2, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, nn_fb_factor, 1,
+                   condfb, 0, (int *)nullptr);
+      };
+      if (captured) {
+        conditional_node(st, condfb, cudaGraphCondTypeIf, fallback);
+      } else {
+        int h = 0;
+        CK(cudaMemcpyAsync(h_any, dfb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        h = *h_any;
+        if (h) fallback(st);
+      }
+    }
     if (captured) {
       // captured: the first U iterations as plain kernel nodes (their kernels skip systems that
       // have converged; U = the iterations of the last host-driven solve - 2), then a conditional
@@ -1033,7 +1189,7 @@ struct Engine : EngineBase {
   void energy_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, double *energy, double *virial) {
     launch_pdl(pgm::k_total_dipoles<T>, grid1(nt), 256, 0, st, a, mu);
     pme<true, false, 0, true>(st, a, D.p);
-    launch_pdl(pgm::k_forces<T, P>, nwblk, 256, 0, st, a, mu);
+    forces_pass(st, a, mu, true);
     if (ncov) launch_pdl(pgm::k_cov_forces<T>, grid1(ncov), 256, 0, st, a);
     launch_pdl(pgm::k_energy_finish, grid1(nsys, 64), 64, 0, st, (const pgm::SysInfo *)d_sys.p, (const pgm::BoxInfo *)d_box.p,
                (const pgm::EnergyAcc *)d_eacc.p, nsys, set.ewald_beta, a.c_self, set.cutoff, set.vdw == 1, set.lj_lrc, a.induce, energy,
@@ -1058,6 +1214,11 @@ struct Engine : EngineBase {
       if (out->residual) CK(cudaMemsetAsync(out->residual, 0, sizeof(double) * nsys, st));
     }
     energy_pass(st, a, mu, out->energy ? out->energy : energy_tmp.p, out->virial);
+    if (!tune.tuned && !tune_fixed) {  // the first direct step: time the kernel variants on its rows
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      CK(cudaStreamIsCapturing(st, &cs));
+      if (cs == cudaStreamCaptureStatusNone) autotune(st);
+    }
   }
 
   void energy(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width, PgmInduction *ind,
@@ -1340,6 +1501,48 @@ PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, floa
   try {
     CK(cudaSetDevice(h->device));
     h->eng->set_nn(weights, sigma, graph_cutoff);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_tuning(PgmHandle *h, PgmTuning *out) {
+  if (!h || !out) return fail(PGM_ERR_INVALID, "null argument");
+  *out = h->eng->tuning();
+  return PGM_OK;
+}
+
+PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm) {
+  if (!h || !(rowfield_lanes == 0 || rowfield_lanes == 8 || rowfield_lanes == 16 || rowfield_lanes == 32) ||
+      !(forces_blocks_per_sm == 0 || (forces_blocks_per_sm >= 2 && forces_blocks_per_sm <= 4)))
+    return fail(PGM_ERR_INVALID, "rowfield_lanes 0, 8, 16 or 32; forces_blocks_per_sm 0, 2, 3 or 4");
+  h->eng->set_tuning(rowfield_lanes, forces_blocks_per_sm);
+  return PGM_OK;
+}
+
+PgmStatus pgm_autotune(PgmHandle *h, void *stream) {
+  if (!h) return fail(PGM_ERR_INVALID, "null handle");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->autotune((cudaStream_t)stream);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_set_nn_fallback(PgmHandle *h, double factor) {
+  if (!h || !(factor >= 0)) return fail(PGM_ERR_INVALID, "bad argument");
+  h->eng->set_nn_fallback(factor);
+  return PGM_OK;
+}
+
+PgmStatus pgm_nn_fallback_stats(PgmHandle *h, long long *fallbacks, double *ref_err) {
+  if (!h) return fail(PGM_ERR_INVALID, "null handle");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->nn_fallback_stats(fallbacks, ref_err);
     return PGM_OK;
   } catch (CudaError &e) {
     return fail(PGM_ERR_CUDA, e.msg);

@@ -69,6 +69,13 @@ struct CGSys {
   int n3;               // 3 x atoms of the system (the mean of mean|alpha b|)
   double acc_pap, acc_rz, acc_num, acc_abs;
   unsigned long long acc_max;  // non-negative doubles compare as their bit patterns
+  // learned guess: nn = this solve starts from x4 + the model's correction; fallback = its start
+  // residual was worse than the record of the extrapolation's, so the solve restarts from x4.
+  // Kept across solves: ref_err, the running mean of the extrapolation's start residual
+  // max|alpha r0| / norm (plain starts, and every fallback), ref_n its samples, fallbacks the count.
+  int nn, fallback, ref_n, pad_;
+  double ref_err;
+  long long fallbacks;
 };
 
 // Per-system accumulators of the energy pass.

@@ -542,6 +542,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restric
   if (i >= S.atom0 + S.natom) return;
   if (ACT == 1 && !a.cg[s].active) return;
   if (ACT == 2 && !a.cg[s].sweep2) return;
+  if (ACT == 3 && !a.cg[s].fallback) return;
   v4<T> d;
   if (UPDATE_P) {
     v4<T> z = a.Z[i], p = a.P[i];
@@ -810,7 +811,7 @@ __device__ __forceinline__ int group_member(const int *gtile0, int ng, int b) {
 
 template <typename T>
 __device__ __forceinline__ bool pass_active(const Dev<T> &a, int s, int act) {
-  return act == 0 || (act == 1 && a.cg[s].active) || (act == 2 && a.cg[s].sweep2);
+  return act == 0 || (act == 1 && a.cg[s].active) || (act == 2 && a.cg[s].sweep2) || (act == 3 && a.cg[s].fallback);
 }
 
 // k3 pass, real -> half complex: two real lines packed as one complex line (z = a + i b), one
@@ -1196,19 +1197,26 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
 // (pme.py:378-388), then by MODE:
 //   0 FIELD  out = -(s - c_self d)                       (forcefield.py:1428-1433)
 //   1 OPER   out = d / alpha + s - c_self d, and p.Ap    (forcefield.py:1694-1712, 1806-1807)
-// The row part alone: F_i = sum_k de_ik/dd_i, one warp per atom (runs beside the PME chain).
-template <typename T, bool WITH_Q, int ACT>
-__global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ F) {
+// The row part alone: F_i = sum_k de_ik/dd_i (runs beside the PME chain).  LPR lanes per row
+// (32: a warp per atom; 16 or 8: two or four atoms per warp, each row split over fewer lanes, more
+// rows in flight per warp), 8 atoms per block of 8 LPR threads either way -- the autotuner's choice
+// (Engine::autotune).  The lane partial sums are combined by a butterfly within each LPR group,
+// so the variants differ only in the order of the row's additions.
+template <typename T, bool WITH_Q, int ACT, int LPR = 32>
+__global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ F) {
+  static_assert(LPR == 32 || LPR == 16 || LPR == 8, "lanes per row");
   pdl_enter();
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = threadIdx.x / LPR, lane = threadIdx.x % LPR;
   int s = a.wb_sys[blockIdx.x];
-  int i = a.wb_atom0[blockIdx.x] + warp;
+  int i = a.wb_atom0[blockIdx.x] + sub;
   const SysInfo &S = a.sys[s];
-  if (i >= S.atom0 + S.natom) return;
-  if (ACT == 1 && !a.cg[s].active) return;
+  if (ACT == 1 && !a.cg[s].active) return;  // uniform over the block
   if (ACT == 2 && !a.cg[s].sweep2) return;
-  int n = min(a.rn[i], a.mce);
-  size_t base = (size_t)i * a.mc;
+  if (ACT == 3 && !a.cg[s].fallback) return;
+  const bool valid = i < S.atom0 + S.natom;
+  if (LPR == 32 && !valid) return;  // uniform over the warp
+  int n = valid ? min(a.rn[i], a.mce) : 0;
+  size_t base = (size_t)(valid ? i : 0) * a.mc;
   T f0 = 0, f1 = 0, f2 = 0;
   auto pair = [&](int k, T x, T y, T z, T g1, T g2) {
     v4<T> dk = D[k];
@@ -1233,8 +1241,8 @@ __global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restr
       kk = __ldcs(k4 + lane);
       xx = __ldcs(x4 + lane); yy = __ldcs(y4 + lane); zz = __ldcs(z4 + lane); g1 = __ldcs(p4 + lane); g2 = __ldcs(q4 + lane);
     }
-    for (int t4 = lane; 4 * t4 < n; t4 += 32) {
-      const int t4n = t4 + 32;
+    for (int t4 = lane; 4 * t4 < n; t4 += LPR) {
+      const int t4n = t4 + LPR;
       int4 kn = make_int4(0, 0, 0, 0);
       float4 xn = make_float4(0, 0, 0, 0), yn = xn, zn = xn, g1n = xn, g2n = xn;
       if (4 * t4n < n) {
@@ -1249,13 +1257,19 @@ __global__ void __launch_bounds__(256) k_rowfield(Dev<T> a, const v4<T> *__restr
       kk = kn; xx = xn; yy = yn; zz = zn; g1 = g1n; g2 = g2n;
     }
   } else {
-    for (int t = lane; t < n; t += 32) {
+    for (int t = lane; t < n; t += LPR) {
       size_t o = base + t;
       pair(a.rk[o], a.rx[o], a.ry[o], a.rz[o], a.rg1[o], a.rg2[o]);
     }
   }
-  f0 = warp_sum<T>(f0); f1 = warp_sum<T>(f1); f2 = warp_sum<T>(f2);
-  if (lane == 0) {
+  // every lane of the warp takes part in the butterfly (a row past the system's end adds zeros)
+#pragma unroll
+  for (int o = LPR / 2; o > 0; o >>= 1) {
+    f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+  }
+  if (valid && lane == 0) {
     v4<T> o;
     o.x = f0; o.y = f1; o.z = f2; o.w = T(0);
     F[i] = o;
@@ -1275,6 +1289,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
   bool valid = i < S.atom0 + S.natom;
   if (ACT == 1 && !a.cg[s].active) return;   // uniform over the block
   if (ACT == 2 && !a.cg[s].sweep2) return;
+  if (ACT == 3 && !a.cg[s].fallback) return;
   double dotv = 0.0;
   if (valid) {
     int n = ROWS ? min(a.rn[i], a.mce) : 0;
@@ -1696,15 +1711,26 @@ __global__ void k_start3(Dev<T> a) {
 }
 
 // CG initialisation: z = alpha r, p = z, r.z and max|alpha r| (forcefield.py:1796-1819).
-template <typename T>
-__global__ void k_cg_init(Dev<T> a) {
+// FB (the learned guess's fallback, systems with the flag only): first back to the extrapolation,
+// x = x4 = x - delta and r0 = b - A x4 = r0 + A delta (A delta in AP).
+template <typename T, bool FB = false>
+__global__ void k_cg_init(Dev<T> a, const float *delta = nullptr) {
   __shared__ double red[THREADS_PER_BLOCK / 32];
   __shared__ unsigned long long mx[THREADS_PER_BLOCK / 32];
+  if (FB) pdl_enter();  // launched as a programmatic dependent of the fallback sweep
   int s = a.tb_sys[blockIdx.x];
+  if (FB && !a.cg[s].fallback) return;  // uniform over the block
   int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
   const SysInfo &S = a.sys[s];
   double rz = 0, m = 0;
   if (i < S.atom0 + S.natom) {
+    if (FB) {
+      v4<T> r = a.R[i], ad = a.AP[i], x = a.X[i];
+      r.x += ad.x; r.y += ad.y; r.z += ad.z;
+      x.x -= T(delta[3 * (size_t)i]); x.y -= T(delta[3 * (size_t)i + 1]); x.z -= T(delta[3 * (size_t)i + 2]);
+      a.R[i] = r;
+      a.X[i] = x;
+    }
     v4<T> r = a.R[i];
     T al = a.alpha[i];
     v4<T> z;
@@ -1730,24 +1756,59 @@ __global__ void k_cg_init(Dev<T> a) {
 }
 
 // Per-system scalars after the start: norm, r.z, err, active; *any = some system iterates.
-__global__ void k_cg_begin(CGSys *cg, int nsys, double tol, int max_iter, int *any) {
+// The learned guess's check (fb_factor > 0, pass 0): a system that started from x4 + the model's
+// correction falls back to x4 when its start residual err exceeds fb_factor times the running
+// mean of the extrapolation's (raising the fallback node's condition, *fb_any); a system that
+// started from the extrapolation itself adds its err to that mean.  Pass 1 (after the fallback
+// sweep) re-evaluates the fallback systems, adds their (extrapolation) err to the mean and counts
+// the fallback; *any covers every system.
+__global__ void k_cg_begin(CGSys *cg, int nsys, double tol, int max_iter, int *any, double fb_factor = 0.0, int pass = 0,
+                           cudaGraphConditionalHandle fbcond = 0, int use_cond = 0, int *fb_any = nullptr) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
-  __shared__ int act;
-  if (threadIdx.x == 0) act = 0;
+  __shared__ int act, fb;
+  if (threadIdx.x == 0) { act = 0; fb = 0; }
   __syncthreads();
+  constexpr double W = 0.1;  // weight of a new sample in the running mean
   for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
     CGSys &G = cg[s];
-    if (!G.fused) G.norm = G.acc_abs / G.n3 + 1e-300;
-    G.rz = G.acc_rz;
-    G.err = __longlong_as_double((long long)G.acc_max) / G.norm;
-    G.beta = 0.0;
-    G.it = 0;
-    G.active = (G.err > tol) && (max_iter > 0);
-    G.acc_abs = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0; G.acc_num = 0;
+    if (pass == 0 || G.fallback) {
+      if (!G.fused) G.norm = G.acc_abs / G.n3 + 1e-300;
+      G.rz = G.acc_rz;
+      G.err = __longlong_as_double((long long)G.acc_max) / G.norm;
+      G.beta = 0.0;
+      G.it = 0;
+      G.active = (G.err > tol) && (max_iter > 0);
+      G.acc_abs = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0; G.acc_num = 0;
+      const bool record = (pass == 1) || (fb_factor > 0.0 && G.have && !G.nn);
+      if (pass == 0 && fb_factor > 0.0 && G.nn && G.ref_n > 0 && G.err > fb_factor * G.ref_err) {
+        G.fallback = 1;
+        atomicOr(&fb, 1);
+      } else if (record) {
+        G.ref_err = G.ref_n == 0 ? G.err : (1.0 - W) * G.ref_err + W * G.err;
+        G.ref_n += 1;
+        if (pass == 1) G.fallbacks += 1;
+      }
+    }
     if (G.active) atomicOr(&act, 1);
   }
   __syncthreads();
-  if (threadIdx.x == 0) *any = act;
+  if (threadIdx.x == 0) {
+    *any = act;
+    if (pass == 0 && fb_any) *fb_any = fb;
+    if (pass == 0 && use_cond && fb) cudaGraphSetConditional(fbcond, 1u);  // the fallback node runs (default 0)
+  }
+}
+
+// Fallback, step 1: the model's correction delta of every fallback system's atoms as the dipoles
+// of one operator sweep (A delta).
+template <typename T>
+__global__ void k_fb_prep(Dev<T> a, const float *delta) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt || !a.cg[a.sysid[i]].fallback) return;
+  v4<T> d;
+  d.x = T(delta[3 * (size_t)i]); d.y = T(delta[3 * (size_t)i + 1]); d.z = T(delta[3 * (size_t)i + 2]); d.w = T(0);
+  a.D[i] = d;
 }
 
 // One CG update (thread per atom): x += a p, r' = r - a Ap, z' = alpha r', and the sums of
@@ -1883,13 +1944,15 @@ __global__ void k_cg_state_out(const CGSys *cg, int nsys, int32_t *count, double
 // mode 0: history predictor (compute); mode 1: the guess is the state's mu, plain start (energy,
 // forcefield.py:2606-2612).
 __global__ void k_cg_setup(CGSys *cg, int nsys, const int32_t *count, const double *norm, int K, int fused, int refresh,
-                           int mode, cudaGraphConditionalHandle plain, int use_cond) {
+                           int mode, cudaGraphConditionalHandle plain, int use_cond, int use_nn = 0) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   CGSys &G = cg[s];
   int c = count ? count[s] : 0;
   G.have = mode == 1 ? 1 : (K > 0 && c >= K);
+  G.nn = use_nn && G.have;  // k_start1 adds the model's correction to the extrapolation
+  G.fallback = 0;
   G.fused = mode == 0 && G.have && fused && (c % refresh) != 0;
   G.sweep2 = !G.fused;
   if (use_cond && G.sweep2) cudaGraphSetConditional(plain, 1u);  // the plain start's sweep runs (default 0)
@@ -1917,8 +1980,8 @@ __global__ void k_energy_start(Dev<T> a, const double *mu) {
 // kernels G0..G3 (forcefield.py:2294-2360), LJ rows, the row field at (q, d) (dE/dd), the pair
 // virial sum g (x) x - gx (x) off; then the PME gradients of the atom: dU/dd and dU/dr through the
 // spline derivatives (the autodiff of pme.py:390-411 written out).
-template <typename T, int P>
-__global__ void __launch_bounds__(256, 3) k_forces(Dev<T> a, const double *mu) {
+template <typename T, int P, int MINB = 3>
+__global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
   __shared__ T sh[WARPS_PER_BLOCK][3][3][P];
   __shared__ double red[WARPS_PER_BLOCK][16];

@@ -433,3 +433,33 @@ class PGMForceField:
     def last_launch_count(self) -> int:
         """Kernels launched by the last call."""
         return int(self._lib.pgm_last_launch_count(self._h))
+
+    def set_nn_fallback(self, factor: float) -> None:
+        """Learned guess (predictor "nn"): restart a solve from the mu4 extrapolation when the start
+        residual of the learned guess is above `factor` times the recorded mean of the extrapolation's
+        (0: never; default 2)."""
+        _lib.check(self._lib.pgm_set_nn_fallback(self._h, float(factor)))
+
+    def nn_fallback_stats(self) -> dict:
+        """Per system: fallbacks so far and the recorded mean start residual of the extrapolation."""
+        fb = np.zeros(self.nsys, np.int64)
+        ref = np.zeros(self.nsys)
+        _lib.check(self._lib.pgm_nn_fallback_stats(self._h, C.c_void_p(fb.ctypes.data), C.c_void_p(ref.ctypes.data)))
+        return {"fallbacks": fb, "ref_err": ref}
+
+    def tuning(self) -> dict:
+        """The kernel variants in use and the autotuner's timings (pgm_tuning)."""
+        t = _lib.PgmTuning()
+        _lib.check(self._lib.pgm_tuning(self._h, C.byref(t)))
+        return {"rowfield_lanes": t.rowfield_lanes, "forces_blocks_per_sm": t.forces_blocks_per_sm,
+                "rowfield_ms": list(t.rowfield_ms), "forces_ms": list(t.forces_ms), "tuned": bool(t.tuned),
+                "from_cache": bool(t.from_cache)}
+
+    def set_tuning(self, rowfield_lanes: int = 0, forces_blocks_per_sm: int = 0) -> None:
+        """Fix the kernel variants (0 keeps one; both 0: autotune again at the next direct step)."""
+        _lib.check(self._lib.pgm_set_tuning(self._h, int(rowfield_lanes), int(forces_blocks_per_sm)))
+
+    def autotune(self) -> dict:
+        """Time the kernel variants now on the last step's rows; returns tuning()."""
+        _lib.check(self._lib.pgm_autotune(self._h, self._stream()))
+        return self.tuning()

@@ -213,8 +213,12 @@ class RigidMD:
         self.step_count += 1
 
     def capture(self) -> None:
-        """Capture one step into a CUDA graph (CG loop as a device-side while node)."""
+        """Capture one step into a CUDA graph (CG loop as a device-side while node); a graph captured
+        before is released."""
         self.stream.synchronize()
+        if self._graph is not None:
+            _lib.check(self._lib.pgm_graph_destroy(self._graph))
+            self._graph = None
         st = self._stream()
         _lib.check(self._lib.pgm_graph_begin(st))
         ex = C.c_void_p()

@@ -52,3 +52,15 @@ def small_box_system():
     from pgm_jax_b200.systems import small_box
 
     return small_box(0)
+
+
+# Settings of the reference's regression case iel_point (regression_cases.py:334-352)
+IEL_POINT_SETTINGS = dict(
+    cutoff=0.6, ewald_beta=6.0, pme_grid=(48, 48, 48), pme_order=8, lj_lrc=True, dipole_tol=1e-10, max_iter=200,
+    iel="0scf", iel_precond="block",
+)
+
+
+@pytest.fixture(scope="session")
+def golden_iel_point():
+    return dict(np.load(os.path.join(GOLDEN, "iel_point.npz")))

@@ -13,6 +13,11 @@ The inputs (positions, box) are regenerated here by pgm_jax_b200.systems.small_b
 numpy seed and stored next to the outputs, so that the tests need neither the reference nor numpy's
 generator to stay stable.
 
+iel_point.npz -- from tests/regression/golden/iel_point.npz (case `iel_point`,
+regression_cases.py:334-352): the iEL/0-SCF force field (block preconditioner) at small_box(1),
+cutoff 0.6 nm, Ewald 6.0/nm, PME 48^3 order 8, float64, tol 1e-10, max_iter 200, from a fresh
+solver state (the warm-up solve to tol); inputs regenerated by small_box(1) as above.
+
 ff_pgm3p25_512.npz -- from tests/regression/golden/ff_pgm3p25_512.npz of pGM-JAX (case
 `ff_pgm3p25_512`, regression_cases.py:291-307): 512 pGM3P-25 waters of examples/water512, default
 MDSettings (cutoff 0.9 nm, Ewald 4.0/nm, order 6, spacing 0.08 nm -> 30^3 on this box, tol 1e-5,
@@ -68,6 +73,14 @@ def main(ref: str) -> None:
             out[f"{tag}.{k}"] = g[f"{tag}.{k}"]
     np.savez_compressed(os.path.join(HERE, "ff_small_box.npz"), **out)
     print("wrote", os.path.join(HERE, "ff_small_box.npz"), sorted(out))
+
+    g = np.load(os.path.join(gdir, "iel_point.npz"))
+    _, pos, H = small_box(1)
+    out = {"pos": pos, "box": H}
+    for k in KEYS:
+        out[f"sp.{k}"] = g[f"sp.{k}"]
+    np.savez_compressed(os.path.join(HERE, "iel_point.npz"), **out)
+    print("wrote", os.path.join(HERE, "iel_point.npz"), sorted(out))
 
     g = np.load(os.path.join(gdir, "ff_pgm3p25_512.npz"))
     pos, vel, H = water512_frame(ref)

@@ -69,33 +69,96 @@ def test_features_turn_with_the_system():
     assert np.abs(v0 @ R.T - v1).max() <= 1e-4 * np.abs(v0).max()
 
 
-def test_trained_guess_beats_mu4_and_solves_to_tolerance():
-    """Plain-solver MD writes (features, mu* - mu4 guess); GPU Adam steps train the model; on later
-    frames mu4 + its correction is closer to mu* than mu4 (and mu4 than the previous step's dipoles),
-    and MD started from it converges to the same tolerance."""
+def _same_positions(md, steps, ffs, captured=False):
+    """Run `steps` MD steps of md (the learned guess; launched directly, or replayed from a captured
+    graph) and solve every other force field in `ffs` (each with its own solver state, started from
+    md's) at the same positions: per step CG iterations of md and of each of ffs."""
+    import torch
+
+    md.stream.synchronize()
+    states = {k: md.ind.clone() for k in ffs}
+    its = {"md": []}
+    its.update({k: [] for k in ffs})
+    if captured:
+        md.capture()
+    for _ in range(steps):
+        if captured:
+            md.run(1)
+        else:
+            md.step()
+        md.stream.synchronize()
+        its["md"].append(int(md.result.iterations[0]))
+        assert float(md.result.residual[0]) <= md.ff.s.dipole_tol and not int(md.result.status[0]) & 0x2
+        pos = md.pos.clone()
+        for k, ff in ffs.items():
+            r = ff.compute(pos, md.box[0].cpu().numpy(), None, states[k])
+            states[k] = r.induction
+            its[k].append(int(r.iterations[0]))
+        torch.cuda.synchronize()
+    return {k: np.array(v) for k, v in its.items()}
+
+
+def _learned_md(prec="mixed", tol=1e-6):
     from pgm_jax_b200.forcefield import MDSettings, PGMForceField
-    from pgm_jax_b200.learned import GuessModel, collect, guess_errors
     from pgm_jax_b200.md import RigidMD
     from pgm_jax_b200.systems import water_box
 
     s, pos, H = water_box(5, 1.55, seed=6)
-    kw = dict(precision="mixed", cutoff=0.7, ewald_beta=5.0, pme_grid=(32, 32, 32), dipole_tol=1e-6, max_iter=100)
+    kw = dict(precision=prec, cutoff=0.7, ewald_beta=5.0, pme_grid=(32, 32, 32), dipole_tol=tol, max_iter=100)
     ff = PGMForceField(s, H, MDSettings(predictor="nn", **kw))
     md = RigidMD(ff, pos, H, temperature=300.0, dt_fs=1.0, gamma_ps=5.0, seed=2)
+    others = {p: PGMForceField(s, H, MDSettings(predictor=p, **kw)) for p in ("mu4", "mu1")}
+    return s, H, ff, md, others
+
+
+def test_trained_guess_saves_iterations_over_mu4_and_mu1():
+    """Plain-solver MD writes (features, mu* - mu4 guess); GPU Adam steps train the model; on later
+    frames mu4 + its correction is closer to mu* than mu4 (and mu4 than the previous step's
+    dipoles), and on held-out MD with the model the solver needs fewer CG iterations than plain CG
+    from mu4 and from the previous step's dipoles, solved at the same positions from the same
+    history, all to the same tolerance."""
+    from pgm_jax_b200.learned import GuessModel, collect, guess_errors
+
+    s, H, ff, md, others = _learned_md()
     train = collect(md, 64)
     held = collect(md, 16)
     model = GuessModel(seed=0)
     before = guess_errors(model, held)
-    model.train(train, iters=800, batch=8192, lr=2e-3)
+    model.train(train, iters=2000, batch=8192, lr=2e-3)
     after = guess_errors(model, held)
     print("guess rms", before, after)
     assert before["model"] == before["mu4"]  # the untrained model adds nothing
     assert before["mu4"] < before["mu1"]
     assert after["model"] < 0.9 * before["mu4"], (before, after)  # the trained model gains on unseen frames
     model.install(ff)
-    its = []
-    for _ in range(8):
+    its = _same_positions(md, 40, others, captured=True)
+    print("iterations per step", {k: float(v.mean()) for k, v in its.items()})
+    assert its["md"].mean() < its["mu4"].mean() < its["mu1"].mean(), {k: float(v.mean()) for k, v in its.items()}
+    assert int(ff.nn_fallback_stats()["fallbacks"][0]) <= 4  # the trained model is rarely worse than mu4
+
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_bad_model_falls_back_to_mu4(prec):
+    """A model with random output weights (its corrections several times the mu4 guess's error):
+    every solve's start residual is above twice the record of mu4's, so every step falls back to
+    x4 with one extra operator sweep, and needs at most one CG iteration more than mu4 at the same
+    positions from the same history; the solution meets the tolerance."""
+    from pgm_jax_b200.learned import N_HID, N_OUT, GuessModel, init_weights
+
+    s, H, ff, md, others = _learned_md(prec, tol=1e-7)
+    for _ in range(12):  # plain mu4 starts (no model yet) record the extrapolation's start residual
         md.step()
-        its.append(int(ff._iters[0]))
-        assert float(ff._resid[0]) <= 1e-6 and not int(ff._status[0]) & 0x2
-    assert np.mean(its) > 0
+    md.stream.synchronize()
+    assert ff.nn_fallback_stats()["ref_err"][0] > 0
+    w = init_weights(0)
+    rng = np.random.default_rng(9)
+    w[-(N_HID * N_OUT + N_OUT):] = rng.normal(scale=0.5, size=N_HID * N_OUT + N_OUT)  # output layer
+    GuessModel(w).install(ff)
+    its = _same_positions(md, 3, {"mu4": others["mu4"]})  # host-driven solves
+    its2 = _same_positions(md, 3, {"mu4": others["mu4"]}, captured=True)  # the fallback as a conditional node
+    st = ff.nn_fallback_stats()
+    assert int(st["fallbacks"][0]) == 6, st
+    assert np.all(its["md"] <= its["mu4"] + 1) and np.all(its2["md"] <= its2["mu4"] + 1), (its, its2)
+    ff.set_nn_fallback(0.0)  # without the check the bad guess costs iterations
+    its_off = _same_positions(md, 4, {"mu4": others["mu4"]}, captured=True)
+    assert its_off["md"].mean() > its_off["mu4"].mean() + 1, its_off
