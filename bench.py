@@ -360,6 +360,9 @@ def run_engine(args) -> None:
     # induction state on the device, or copied in and out every step), the integrator on the GPU
     e2e = run_e2e(md, ff, args.steps, torch, lib, _lib)
     e2e_host_state = run_e2e(md, ff, args.steps, torch, lib, _lib, state_on_device=False)
+    tuning = ff.tuning()
+    if args.nn:
+        train_info["fallbacks_in_run"] = int(ff.nn_fallback_stats()["fallbacks"][0])
     final = {"pos": md.pos.cpu().numpy(), "box": md.box[0].cpu().numpy(),
              "ind": {k: getattr(md.ind, k).cpu().numpy() for k in ("mu", "hist", "count", "norm")}}
     del md
@@ -383,6 +386,7 @@ def run_engine(args) -> None:
                 "step_frac": step_bytes / (ms_max * 1e-3) / 1e9 / peak,
             },
             "kernel_ms": kt, "pairs": pairs, "row_capacity": ff.capacity, "accuracy_vs_oracle": acc,
+            "tuning": tuning,
             "e2e": e2e,
             "e2e_host_state": {k: e2e_host_state[k] for k in ("value", "unit", "ms_per_step", "h2d_bytes_per_step",
                                                               "d2h_bytes_per_step", "path")},

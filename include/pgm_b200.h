@@ -71,6 +71,24 @@ typedef struct {
                            between elec_cutoff and cutoff with a nonzero LJ term; the field sweeps
                            stream the first part only.  ewald_beta and the mesh must suit it. */
     int elec_capacity;  /* split rows: electrostatic pairs kept per row (0: from the density) */
+    /* Extended-Lagrangian induced dipoles (Induction.iel, forcefield.py:246-282, 1452-1650): the
+       auxiliary dipoles PgmInduction.xl follow Niklasson's dissipative Verlet
+       x_{n+1} = 2 x_n - x_{n-1} + kappa (mu_n - x_n) + a sum_k c_k x_{n-k}; the first
+       max(order, 2) + 1 steps solve to dipole_tol, later ones start from x = xl[0]. */
+    int iel;            /* 0 "none" (the predictor + CG above), 1 "0scf" (mu = x + omega delta, delta =
+                           alpha r(x) or M^-1 r(x), one field sweep, no CG), 2 "scf" (iel_iter CG
+                           iterations from x; 0: to dipole_tol) */
+    int iel_order;      /* dissipation order K: 0 or 3..9 (the reference's default is 7) */
+    int iel_custom;     /* 1: iel_kappa and iel_alpha below; 0: Niklasson's values for the order */
+    double iel_kappa;   /* kappa = (omega dt)^2 of the auxiliary dipoles' harmonic coupling */
+    double iel_alpha;   /* dissipation strength a */
+    double iel_omega;   /* 0scf: mu = x + omega delta (0 is read as 1) */
+    int iel_precond;    /* 0scf: 0 "block" (M = 1/alpha + the rows inside molecules of 2..8 atoms),
+                           1 "jacobi" (delta = alpha r) */
+    int iel_iter;       /* scf: CG iterations per step (0: to dipole_tol) */
+    int iel_no_shadow;  /* 0scf: 0 the energy and forces of the shadow potential U(R, x + delta) -
+                           U_es(0, delta) (the reference's default, exact and conserved); 1 the
+                           fixed-dipole energy and forces at mu */
 } PgmSettings;
 
 /* One system of the batch: topology and parameters (host arrays, copied at creation). */
@@ -98,6 +116,8 @@ typedef struct {
     double *hist;    /* (4, N, 3) dipoles of the last steps, newest first */
     int32_t *count;  /* (n_systems) steps recorded */
     double *norm;    /* (n_systems) mean|alpha b| of the last unfused step */
+    double *xl;      /* iel only: (pgm_iel_len(order), N, 3) auxiliary dipoles, newest first
+                        (InductionState.xl); NULL otherwise */
 } PgmInduction;
 
 /* Outputs of a step (Result, forcefield.py:716-746), device pointers; any may be NULL. */
@@ -111,6 +131,10 @@ typedef struct {
 } PgmOutputs;
 
 typedef struct PgmHandle PgmHandle;
+
+/* Auxiliary dipoles kept by an iEL state of this order: x_{n+1} and x_n ... x_{n-K}, at least 3
+ * (PGMForceField.xl_len, forcefield.py:1476-1479). */
+int pgm_iel_len(int order);
 
 /* PGMForceField.__init__ (forcefield.py:868): settings and the systems of the batch. */
 PgmStatus pgm_create(const PgmSettings *settings, const PgmSystemDesc *systems, int n_systems, int device,

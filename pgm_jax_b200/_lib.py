@@ -26,6 +26,7 @@ EXPORTS = (
     "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
     "pgm_set_nn_model", "pgm_nn_features", "pgm_nn_param_count", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam",
     "pgm_nn_last_error", "pgm_set_nn_fallback", "pgm_nn_fallback_stats", "pgm_tuning", "pgm_set_tuning", "pgm_autotune",
+    "pgm_iel_len",
 )
 
 STATUS_ROW_OVERFLOW = 0x1
@@ -48,7 +49,9 @@ class PgmSettings(C.Structure):
         ("ewald_beta", C.c_double), ("pme_order", C.c_int), ("dipole_tol", C.c_double), ("max_iter", C.c_int),
         ("predictor", C.c_int), ("fused", C.c_int), ("norm_refresh", C.c_int), ("peek", C.c_double),
         ("row_capacity", C.c_int), ("skin", C.c_double), ("list_capacity", C.c_int), ("elec_cutoff", C.c_double),
-        ("elec_capacity", C.c_int),
+        ("elec_capacity", C.c_int), ("iel", C.c_int), ("iel_order", C.c_int), ("iel_custom", C.c_int),
+        ("iel_kappa", C.c_double), ("iel_alpha", C.c_double), ("iel_omega", C.c_double), ("iel_precond", C.c_int),
+        ("iel_iter", C.c_int), ("iel_no_shadow", C.c_int),
     ]
 
 
@@ -61,7 +64,7 @@ class PgmSystemDesc(C.Structure):
 
 
 class PgmInduction(C.Structure):
-    _fields_ = [("mu", C.c_void_p), ("hist", C.c_void_p), ("count", C.c_void_p), ("norm", C.c_void_p)]
+    _fields_ = [("mu", C.c_void_p), ("hist", C.c_void_p), ("count", C.c_void_p), ("norm", C.c_void_p), ("xl", C.c_void_p)]
 
 
 class PgmOutputs(C.Structure):
@@ -145,6 +148,8 @@ def load(path: str | None = None):
     lib.pgm_nn_loss_grad.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_float, vp, vp]
     lib.pgm_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
     lib.pgm_nn_last_error.restype = C.c_char_p
+    lib.pgm_iel_len.argtypes = [C.c_int]
+    lib.pgm_iel_len.restype = C.c_int
     lib.pgm_tuning.argtypes = [H, C.POINTER(PgmTuning)]
     lib.pgm_set_tuning.argtypes = [H, C.c_int, C.c_int]
     lib.pgm_autotune.argtypes = [H, vp]

@@ -127,6 +127,7 @@ struct EngineBase {
   virtual bool has_hist() const = 0;
   virtual long long row_pairs() = 0;
   int nt = 0, nsys = 0;
+  int iel_len = 0;  // auxiliary dipoles kept by an iEL state (0: no iEL)
   double *host_scratch = nullptr;  // device block of pgm_compute_host (allocated on first use)
   size_t host_scratch_bytes = 0;
   long long launches = 0;
@@ -210,6 +211,14 @@ struct Engine : EngineBase {
   DBuf<float> nn_w, nn_inv, nn_vec, nn_mu, nn_chan;  // learned guess: model and per-atom features
   DBuf<__nv_bfloat16> nn_wb;  // the model's weight matrices in BF16 (converted when the model is set)
   bool nn_on = false;
+  // extended-Lagrangian dipoles: the recurrence's coefficients, delta, the reciprocal potential of
+  // delta alone and its energy accumulators (shadow potential)
+  pgm::IelCoef iel_co{};
+  int iel_warmup = 0;
+  bool iel_shadow = false;
+  DBuf<pgm::v4<T>> Dl;
+  DBuf<T> Phi2;
+  DBuf<pgm::EnergyAcc> d_eacc2;
   PgmTuning tune{};          // kernel variants in use (autotuned at the first direct step unless fixed)
   bool tune_fixed = false;
   double nn_fb_factor = 2.0;  // learned guess: fall back to x4 when its start residual is above this x the record
@@ -283,6 +292,10 @@ struct Engine : EngineBase {
     a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p; a.F = Fv.p;
     a.Q = Q.p; a.Phi = Phi.p; a.Ginf = Ginf.p; a.C = C.p; a.tw = tw.p; a.bmod = bmod.p;
     a.forces = forces; a.dEdd = dEdd.p;
+    a.Dl = Dl.p; a.Phi2 = Phi2.p;
+    const double om = set.iel_omega > 0 ? set.iel_omega : 1.0;
+    a.iel_keep = 1.0 - 1.0 / om;
+    a.iel_keep_on = set.iel == 1 && set.iel_precond == 0;
     return a;
   }
 
@@ -533,6 +546,36 @@ struct Engine : EngineBase {
     CK(cudaMemset(nb_builds.p, 0, sizeof(long long)));
     { int one = 1; CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice)); }
     rn.alloc(nt); rnsp.alloc(nt); dmax.alloc(2); dany.alloc(1); cg_done.alloc(1); dfb.alloc(1);
+    if (set.iel) {  // extended-Lagrangian dipoles: Niklasson's coefficients for the order
+      static const struct { int K; double kappa, a; double c[10]; } xl_table[] = {
+          {0, 1.0, 0.0, {0}},
+          {3, 1.69, 0.150, {-2, 3, 0, -1}},
+          {4, 1.75, 0.057, {-3, 6, -2, -2, 1}},
+          {5, 1.82, 0.018, {-6, 14, -8, -3, 4, -1}},
+          {6, 1.84, 0.0055, {-14, 36, -27, -2, 12, -6, 1}},
+          {7, 1.86, 0.0016, {-36, 99, -88, 11, 32, -25, 8, -1}},
+          {8, 1.88, 0.00044, {-99, 286, -286, 78, 78, -90, 42, -10, 1}},
+          {9, 1.89, 0.00012, {-286, 858, -936, 364, 168, -300, 184, -63, 12, -1}},
+      };
+      int row = -1;
+      for (int r = 0; r < 8; ++r)
+        if (xl_table[r].K == set.iel_order) row = r;
+      iel_co.kappa = set.iel_custom ? set.iel_kappa : xl_table[row].kappa;
+      iel_co.a = set.iel_custom ? set.iel_alpha : xl_table[row].a;
+      iel_co.nc = set.iel_order == 0 ? 1 : set.iel_order + 1;
+      for (int k = 0; k < iel_co.nc; ++k) iel_co.c[k] = xl_table[row].c[k];
+      iel_co.K1 = pgm_iel_len(set.iel_order);
+      iel_co.zscf = set.iel == 1;
+      iel_len = iel_co.K1;
+      iel_warmup = std::max(set.iel_order, 2) + 1;
+      iel_shadow = set.iel == 1 && !set.iel_no_shadow;
+      Dl.alloc(nt);
+      CK(cudaMemset(Dl.p, 0, sizeof(pgm::v4<T>) * nt));
+      if (iel_shadow) {
+        Phi2.alloc(rgrid);
+        d_eacc2.alloc(nsys);
+      }
+    }
     CK(cudaMemset(cg_done.p, 0, sizeof(unsigned)));
     if (split) rnv.alloc(nt);
     alloc_rows();
@@ -675,10 +718,12 @@ struct Engine : EngineBase {
     else if (l == 8) go(std::integral_constant<int, 8>{});
     else go(std::integral_constant<int, 32>{});
   }
-  void forces_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, bool pdl, int minb = 0) {
+  void forces_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, bool pdl, int minb = 0, bool shadow = false) {
     auto go = [&](auto B) {
       constexpr int MINB = decltype(B)::value;
-      if (pdl) {
+      if (shadow) {  // iEL/0-SCF: the shadow potential's energy and forces
+        launch_pdl(pgm::k_forces<T, P, MINB, true>, nwblk, 256, 0, st, a, mu);
+      } else if (pdl) {
         launch_pdl(pgm::k_forces<T, P, MINB>, nwblk, 256, 0, st, a, mu);
       } else {
         pgm::k_forces<T, P, MINB><<<nwblk, 256, 0, st>>>(a, mu);
@@ -1186,14 +1231,88 @@ struct Engine : EngineBase {
   }
 
   // Energies, forces and virial at fixed mu (forcefield.py:2362-2430).
-  void energy_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, double *energy, double *virial) {
+  void energy_pass(cudaStream_t st, pgm::Dev<T> &a, const double *mu, double *energy, double *virial, bool shadow = false) {
     launch_pdl(pgm::k_total_dipoles<T>, grid1(nt), 256, 0, st, a, mu);
+    if (shadow) {
+      // the reciprocal energy and potential of delta alone (zero outside extended steps), into
+      // Phi2 and the second accumulators
+      CK(cudaMemsetAsync(d_eacc2.p, 0, sizeof(pgm::EnergyAcc) * nsys, st));
+      pgm::Dev<T> a2 = a;
+      a2.Phi = Phi2.p;
+      a2.eacc = d_eacc2.p;
+      pme<false, false, 0, true>(st, a2, Dl.p);
+    }
     pme<true, false, 0, true>(st, a, D.p);
-    forces_pass(st, a, mu, true);
+    forces_pass(st, a, mu, true, 0, shadow);
     if (ncov) launch_pdl(pgm::k_cov_forces<T>, grid1(ncov), 256, 0, st, a);
     launch_pdl(pgm::k_energy_finish, grid1(nsys, 64), 64, 0, st, (const pgm::SysInfo *)d_sys.p, (const pgm::BoxInfo *)d_box.p,
                (const pgm::EnergyAcc *)d_eacc.p, nsys, set.ewald_beta, a.c_self, set.cutoff, set.vdw == 1, set.lj_lrc, a.induce, energy,
-               virial, a.status);
+               virial, a.status, shadow ? (const pgm::EnergyAcc *)d_eacc2.p : (const pgm::EnergyAcc *)nullptr,
+               set.iel_omega > 0 ? set.iel_omega : 1.0);
+  }
+
+  // The extended-Lagrangian step (forcefield.py:1558-1650) on the solver's kernels: per system a
+  // warm-up solve to tol (plain start) or an extended step from x = xl[0] (fused start), then the
+  // 0-SCF update or the CG iterations, the history push and the auxiliary dipoles' recurrence.
+  void solve_iel(cudaStream_t st, pgm::Dev<T> &a, PgmInduction *ind, double *mu_out, int32_t *iters, double *resid) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    const bool captured = cs == cudaStreamCaptureStatusActive;
+    cudaGraphConditionalHandle cond2 = 0, cond = 0;
+    int U = 0;
+    if (captured) {
+      cudaGraph_t g;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t nd = 0;
+      unsigned long long id;
+      CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+      CK(cudaGraphConditionalHandleCreate(&cond2, g, 0, cudaGraphCondAssignDefault));
+      U = std::max(0, std::min(last_iters - 2, set.max_iter));
+      CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    }
+    launch_pdl(pgm::k_iel_setup, nsys, 256, 0, st, d_cg.p, (const pgm::SysInfo *)d_sys.p, nsys, (const int32_t *)ind->count,
+               (const double *)ind->norm, (const double *)ind->mu, iel_warmup, set.iel, set.iel_iter, cond2, captured ? 1 : 0);
+    launch_pdl(pgm::k_iel_start1<T>, grid1(nt), 256, 0, st, a, (const double *)ind->xl, (const double *)ind->mu);
+    sweep<true, false, 0, 0>(st, a, D.p, Bv.p);
+    launch_pdl(pgm::k_start2<T>, ntblk, 256, 0, st, a);
+    auto plain_start = [&](cudaStream_t s2) {
+      sweep<false, false, 2, 1>(s2, a, X.p, AP.p);
+      launch_pdl(pgm::k_start3<T>, grid1(nt), 256, 0, s2, a);
+    };
+    if (captured) conditional_node(st, cond2, cudaGraphCondTypeIf, plain_start);
+    else plain_start(st);
+    pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+    launch_pdl(pgm::k_cg_begin, 1, 256, 0, st, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, 0.0, 0,
+               (cudaGraphConditionalHandle)0, 0, (int *)nullptr);
+    if (set.iel == 1) {
+      const double om = set.iel_omega > 0 ? set.iel_omega : 1.0;
+      launch_pdl(pgm::k_iel_delta<T>, grid1(nmol_total, 128), 128, 0, st, a, (const double *)ind->xl, om,
+                 set.iel_precond == 0 ? 1 : 0, mu_out, Dl.p);
+      launch_pdl(pgm::k_iel_begin, 1, 256, 0, st, d_cg.p, nsys, dany.p, 1, cond, (captured && U == 0) ? 1 : 0);
+    } else if (captured && U == 0) {
+      launch_pdl(pgm::k_iel_begin, 1, 256, 0, st, d_cg.p, nsys, dany.p, 0, cond, 1);  // the loop's condition only
+    }
+    if (captured) {
+      for (int k = 0; k < U; ++k) iteration(st, a, cond, k == U - 1 ? 1 : 0);
+      unrolled = U;
+      conditional_node(st, cond, cudaGraphCondTypeWhile, [&](cudaStream_t s2) {
+        long long l0 = launches;
+        iteration(s2, a, cond, 1);
+        per_iter = launches - l0;
+      });
+    } else {
+      int it = 0;
+      for (; it < set.max_iter; ++it) {
+        if (!any_active(st)) break;
+        long long l0 = launches;
+        iteration(st, a, 0, 0);
+        per_iter = launches - l0;
+      }
+      last_iters = it;
+    }
+    launch_pdl(pgm::k_iel_finish<T>, grid1(nt), 256, 0, st, a, mu_out, ind->hist, ind->xl, iel_co);
+    launch_pdl(pgm::k_cg_state_out, grid1(nsys, 64), 64, 0, st, (const pgm::CGSys *)d_cg.p, nsys, ind->count, ind->norm, iters,
+               resid, a.status, 1, set.dipole_tol);
   }
 
   void compute(cudaStream_t st, const double *pos, const double *box, const int32_t *idx, int idx_width, PgmInduction *ind,
@@ -1206,14 +1325,17 @@ struct Engine : EngineBase {
     nn_forked = false;
     prepare(st, a, box, a.induce && set.predictor == 5 && nn_on ? ind->hist : nullptr);
     double *mu = ind->mu;
-    if (a.induce) {
+    if (a.induce && set.iel) {
+      if (!ind->xl) throw CudaError{"iel: PgmInduction.xl (the auxiliary dipoles) is required"};
+      solve_iel(st, a, ind, mu, out->iterations, out->residual);
+    } else if (a.induce) {
       solve(st, a, ind, 0, mu, out->iterations, out->residual);
     } else {
       CK(cudaMemsetAsync(mu, 0, sizeof(double) * 3 * nt, st));
       if (out->iterations) CK(cudaMemsetAsync(out->iterations, 0, sizeof(int32_t) * nsys, st));
       if (out->residual) CK(cudaMemsetAsync(out->residual, 0, sizeof(double) * nsys, st));
     }
-    energy_pass(st, a, mu, out->energy ? out->energy : energy_tmp.p, out->virial);
+    energy_pass(st, a, mu, out->energy ? out->energy : energy_tmp.p, out->virial, a.induce && iel_shadow);
     if (!tune.tuned && !tune_fixed) {  // the first direct step: time the kernel variants on its rows
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
       CK(cudaStreamIsCapturing(st, &cs));
@@ -1285,8 +1407,18 @@ extern "C" {
 
 const char *pgm_last_error(void) { return g_err.c_str(); }
 
+int pgm_iel_len(int order) {
+  const int nc = order == 0 ? 1 : order + 1;
+  return std::max(nc + 1, 3);
+}
+
 PgmStatus pgm_create(const PgmSettings *s, const PgmSystemDesc *systems, int n, int device, PgmHandle **out) {
   if (!s || !systems || n <= 0 || !out) return fail(PGM_ERR_INVALID, "null argument or no systems");
+  if (s->iel < 0 || s->iel > 2) return fail(PGM_ERR_INVALID, "iel must be 0 (none), 1 (0scf) or 2 (scf)");
+  if (s->iel && !(s->iel_order == 0 || (s->iel_order >= 3 && s->iel_order <= 9)))
+    return fail(PGM_ERR_INVALID, "iel_order must be 0 or 3..9");
+  if (s->iel && (s->iel_omega < 0 || s->iel_iter < 0 || s->iel_precond < 0 || s->iel_precond > 1))
+    return fail(PGM_ERR_INVALID, "iel_omega >= 0, iel_iter >= 0, iel_precond 0 (block) or 1 (jacobi)");
   if (s->elec < 0 || s->elec > 3) return fail(PGM_ERR_INVALID, "elec must be 0..3 (q, qp, qi, qpi)");
   if (s->vdw < 0 || s->vdw > 1) return fail(PGM_ERR_INVALID, "vdw must be 0 (none) or 1 (lj)");
   if (s->precision < 0 || s->precision > 1) return fail(PGM_ERR_INVALID, "precision must be 0 (mixed) or 1 (double)");
@@ -1364,6 +1496,7 @@ PgmStatus pgm_compute(PgmHandle *h, void *stream, const double *pos, const doubl
                       PgmInduction *ind, PgmOutputs *out) {
   if (!h || !pos || !box || !ind || !out || !ind->mu) return fail(PGM_ERR_INVALID, "null argument");
   if (h->eng && (h->eng->nt > 0) && (!ind->hist || !ind->count || !ind->norm)) return fail(PGM_ERR_INVALID, "induction state incomplete");
+  if (h->eng->iel_len && !ind->xl) return fail(PGM_ERR_INVALID, "iel: PgmInduction.xl (the auxiliary dipoles) is required");
   if (idx && idx_width <= 0) return fail(PGM_ERR_INVALID, "idx_width must be positive with idx");
   try {
     CK(cudaSetDevice(h->device));
@@ -1378,13 +1511,14 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
   if (!h || !pos || !box || !out || (ind && (!ind->mu || !ind->hist || !ind->count || !ind->norm)))
     return fail(PGM_ERR_INVALID, "null argument");
   EngineBase *e = h->eng.get();
-  size_t n3 = (size_t)3 * e->nt, ns = e->nsys;
+  if (ind && e->iel_len && !ind->xl) return fail(PGM_ERR_INVALID, "iel: PgmInduction.xl is required");
+  size_t n3 = (size_t)3 * e->nt, ns = e->nsys, nxl = (size_t)e->iel_len * n3;
   double *d = nullptr;
   try {
     CK(cudaSetDevice(h->device));
     // one device block, kept by the handle: pos, box, mu, hist, norm, energy, forces, virial,
-    // residual | count, iterations, status
-    size_t nd = n3 + 9 * ns + n3 + 4 * n3 + ns + 3 * ns + n3 + 9 * ns + ns;
+    // residual, (iEL) xl | count, iterations, status
+    size_t nd = n3 + 9 * ns + n3 + 4 * n3 + ns + 3 * ns + n3 + 9 * ns + ns + nxl;
     size_t ni = 3 * ns;
     size_t bytes = sizeof(double) * nd + sizeof(int32_t) * ni;
     if (!h->host_stream) CK(cudaStreamCreateWithFlags(&h->host_stream, cudaStreamNonBlocking));
@@ -1401,7 +1535,8 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
     d = e->host_scratch;
     double *dpos = d, *dbox = dpos + n3, *dmu = dbox + 9 * ns, *dhist = dmu + n3, *dnorm = dhist + 4 * n3, *den = dnorm + ns,
            *dF = den + 3 * ns, *dvir = dF + n3, *dres = dvir + 9 * ns;
-    int32_t *dcount = reinterpret_cast<int32_t *>(dres + ns), *dit = dcount + ns;
+    double *dxl = dres + ns;
+    int32_t *dcount = reinterpret_cast<int32_t *>(dxl + nxl), *dit = dcount + ns;
     uint32_t *dst = reinterpret_cast<uint32_t *>(dit + ns);
     cudaStream_t st = h->host_stream;
     CK(cudaMemcpyAsync(dpos, pos, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
@@ -1411,8 +1546,9 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
       CK(cudaMemcpyAsync(dhist, ind->hist, sizeof(double) * 4 * n3, cudaMemcpyHostToDevice, st));
       CK(cudaMemcpyAsync(dnorm, ind->norm, sizeof(double) * ns, cudaMemcpyHostToDevice, st));
       CK(cudaMemcpyAsync(dcount, ind->count, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
+      if (nxl) CK(cudaMemcpyAsync(dxl, ind->xl, sizeof(double) * nxl, cudaMemcpyHostToDevice, st));
     }
-    PgmInduction di{dmu, dhist, dcount, dnorm};
+    PgmInduction di{dmu, dhist, dcount, dnorm, nxl ? dxl : nullptr};
     PgmOutputs dout{den, dF, dvir, dit, dres, dst};
     if (h->host_graph && h->host_graph_gen != e->generation) {
       cudaGraphExecDestroy(h->host_graph);
@@ -1444,6 +1580,7 @@ PgmStatus pgm_compute_host(PgmHandle *h, const double *pos, const double *box, P
       CK(cudaMemcpyAsync(ind->hist, dhist, sizeof(double) * 4 * n3, cudaMemcpyDeviceToHost, st));
       CK(cudaMemcpyAsync(ind->norm, dnorm, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
       CK(cudaMemcpyAsync(ind->count, dcount, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, st));
+      if (nxl) CK(cudaMemcpyAsync(ind->xl, dxl, sizeof(double) * nxl, cudaMemcpyDeviceToHost, st));
     }
     if (out->energy) CK(cudaMemcpyAsync(out->energy, den, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, st));
     if (out->forces) CK(cudaMemcpyAsync(out->forces, dF, sizeof(double) * n3, cudaMemcpyDeviceToHost, st));

@@ -76,11 +76,17 @@ struct CGSys {
   int nn, fallback, ref_n, pad_;
   double ref_err;
   long long fallbacks;
+  // extended-Lagrangian dipoles: iel_ext = this step is an extended (0-SCF or SCF-from-x) step,
+  // iel_first = the first step of the run; tol_s / maxit_s override the solver's tolerance and
+  // iteration limit for this system (tol_s < 0, maxit_s < 0: the settings').
+  int iel_ext, iel_first, maxit_s, pad2_;
+  double tol_s;
 };
 
 // Per-system accumulators of the energy pass.
 struct EnergyAcc {
   double e_pair, e_lj, e_rec, d2, upol;
+  double dd2, dda;      // iEL/0-SCF shadow energy: sum |delta|^2 and sum |delta|^2 / (2 alpha)
   double vir[9];        // pair + reciprocal (positional and dipolar) parts [kJ/mol]
   double vinf[7];       // influence-function part: E then xx, yy, zz, xy, xz, yz [e^2/nm]
 };

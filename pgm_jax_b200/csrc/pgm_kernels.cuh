@@ -71,6 +71,12 @@ struct Dev {
   int *nn_ne;
   int nn_emax;
   float nn_rg2;
+  // iEL/0-SCF shadow energy: delta (Dl) and the reciprocal potential of delta alone (Phi2);
+  // iel_keep = 1 - 1/omega for pairs inside a preconditioner block when iel_keep_on
+  const v4<T> *Dl;
+  const T *Phi2;
+  double iel_keep;
+  int iel_keep_on;
   // vectors
   v4<T> *X, *R, *Z, *P, *AP, *B, *D;
   v4<T> *F;  // row field of a sweep (computed concurrently with the PME chain)
@@ -1777,7 +1783,7 @@ __global__ void k_cg_begin(CGSys *cg, int nsys, double tol, int max_iter, int *a
       G.err = __longlong_as_double((long long)G.acc_max) / G.norm;
       G.beta = 0.0;
       G.it = 0;
-      G.active = (G.err > tol) && (max_iter > 0);
+      G.active = (G.err > (G.tol_s >= 0.0 ? G.tol_s : tol)) && ((G.maxit_s >= 0 ? G.maxit_s : max_iter) > 0);
       G.acc_abs = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0; G.acc_num = 0;
       const bool record = (pass == 1) || (fb_factor > 0.0 && G.have && !G.nn);
       if (pass == 0 && fb_factor > 0.0 && G.nn && G.ref_n > 0 && G.err > fb_factor * G.ref_err) {
@@ -1870,7 +1876,7 @@ __device__ __forceinline__ void cg_check_body(CGSys *cg, int nsys, double tol, i
       G.rz = G.acc_rz;
       G.err = __longlong_as_double((long long)G.acc_max) / G.norm;
       G.it += 1;
-      G.active = (G.err > tol) && (G.it < max_iter);
+      G.active = (G.err > (G.tol_s >= 0.0 ? G.tol_s : tol)) && (G.it < (G.maxit_s >= 0 ? G.maxit_s : max_iter));
     }
     G.acc_num = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0;
     if (G.active) atomicOr(&act, 1);
@@ -1937,7 +1943,7 @@ __global__ void k_cg_state_out(const CGSys *cg, int nsys, int32_t *count, double
   if (push) { count[s] += 1; norm[s] = G.norm; }
   if (iters) iters[s] = G.it;
   if (resid) resid[s] = G.err;
-  if (G.err > tol) atomicOr(&status[s], 0x2u);
+  if (G.err > tol && !G.iel_ext) atomicOr(&status[s], 0x2u);  // an extended iEL step stops short of tol by design
 }
 
 // Per-system start of a solve: which predictor start applies (forcefield.py:1951-1966).
@@ -1953,6 +1959,7 @@ __global__ void k_cg_setup(CGSys *cg, int nsys, const int32_t *count, const doub
   G.have = mode == 1 ? 1 : (K > 0 && c >= K);
   G.nn = use_nn && G.have;  // k_start1 adds the model's correction to the extrapolation
   G.fallback = 0;
+  G.iel_ext = 0; G.iel_first = 0; G.maxit_s = -1; G.tol_s = -1.0;
   G.fused = mode == 0 && G.have && fused && (c % refresh) != 0;
   G.sweep2 = !G.fused;
   if (use_cond && G.sweep2) cudaGraphSetConditional(plain, 1u);  // the plain start's sweep runs (default 0)
@@ -1975,12 +1982,233 @@ __global__ void k_energy_start(Dev<T> a, const double *mu) {
   a.X[i] = x;
 }
 
+// ------------------------------------------------------------------ extended-Lagrangian dipoles
+// iEL (forcefield.py:1452-1650, Niklasson's dissipative extended-Lagrangian Verlet): the
+// auxiliary dipoles xl (K1, N, 3) FP64, newest first; warm-up steps (count < warmup) solve to tol,
+// extended steps take x = xl[0]: 0-SCF mu = x + omega delta (no CG), SCF iel_iter CG iterations
+// (to tol with 0) from x.
+
+// Per system: first / warm-up / extended, the start the shared solver machinery takes (plain with
+// its second sweep in the warm-up, fused from x otherwise), whether the first step starts from a
+// given mu (any nonzero dipole of the system: one block per system), and the overrides of tol and
+// max_iter (SCF with a set number of iterations: tol 0).
+__global__ void k_iel_setup(CGSys *cg, const SysInfo *sys, int nsys, const int32_t *count, const double *norm, const double *mu,
+                            int warmup, int scheme, int iel_iter, cudaGraphConditionalHandle plain, int use_cond) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
+  int s = blockIdx.x;
+  if (s >= nsys) return;
+  const SysInfo &S = sys[s];
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  const int c = count[s];
+  if (c == 0)
+    for (int t = threadIdx.x; t < 3 * S.natom; t += blockDim.x)
+      if (mu[3 * (size_t)S.atom0 + t] != 0.0) any = 1;
+  __syncthreads();
+  if (threadIdx.x) return;
+  CGSys &G = cg[s];
+  const int warm = c < warmup;
+  G.iel_first = c == 0;
+  G.iel_ext = !warm;
+  G.have = c == 0 ? any : 1;
+  G.nn = 0;
+  G.fallback = 0;
+  G.fused = !warm;
+  G.sweep2 = warm;
+  if (use_cond && warm) cudaGraphSetConditional(plain, 1u);  // the plain start's sweep runs (default 0)
+  G.active = 0;
+  G.norm = warm ? 1.0 : norm[s];
+  G.tol_s = -1.0;
+  G.maxit_s = -1;
+  if (!warm && scheme == 2 && iel_iter > 0) { G.tol_s = 0.0; G.maxit_s = iel_iter; }
+  G.acc_abs = 0; G.acc_rz = 0; G.acc_max = 0; G.acc_pap = 0; G.acc_num = 0;
+}
+
+// The start's first sweep: x0 = xl[0] (the first step: the given mu, or 0 and then alpha b), the
+// dipoles p + x0 of the fused start or p of the plain one.
+template <typename T>
+__global__ void k_iel_start1(Dev<T> a, const double *xl, const double *mu) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  const CGSys &G = a.cg[a.sysid[i]];
+  double x0[3] = {0, 0, 0};
+  for (int c = 0; c < 3; ++c) x0[c] = G.iel_first ? (G.have ? mu[3 * (size_t)i + c] : 0.0) : xl[3 * (size_t)i + c];
+  double4 p = a.pperm[i];
+  v4<T> d, x;
+  if (G.fused) { d.x = T(p.x + x0[0]); d.y = T(p.y + x0[1]); d.z = T(p.z + x0[2]); }
+  else { d.x = T(p.x); d.y = T(p.y); d.z = T(p.z); }
+  d.w = T(0);
+  x.x = T(x0[0]); x.y = T(x0[1]); x.z = T(x0[2]); x.w = T(0);
+  a.D[i] = d;
+  a.X[i] = x;
+}
+
+// Solve M d = r for one molecule's block in FP64 (Gaussian elimination, partial pivoting), M =
+// diag(1/alpha) + the same-molecule row tensors G1 I - G2 x x^T (forcefield.py:1530-1556).
+template <typename T>
+__device__ void iel_block_solve(const Dev<T> &a, int i0, int nb, double (*M)[25], double *d) {
+  const int N = 3 * nb;
+  for (int u = 0; u < N; ++u)
+    for (int v = 0; v <= N; ++v) M[u][v] = 0.0;
+  for (int li = 0; li < nb; ++li) {
+    const int i = i0 + li;
+    const v4<T> r = a.R[i];
+    const double ia = 1.0 / double(a.alpha[i]);
+    const double rr[3] = {double(r.x), double(r.y), double(r.z)};
+    for (int c = 0; c < 3; ++c) { M[3 * li + c][3 * li + c] += ia; M[3 * li + c][N] = rr[c]; }
+    const int nsp = a.rnsp[i];  // molecule partners first in every row
+    const size_t base = (size_t)i * a.mc;
+    for (int t = 0; t < nsp; ++t) {
+      const int k = a.rk[base + t];
+      const int lk = k - i0;
+      if (lk < 0 || lk >= nb) continue;
+      const double x[3] = {double(a.rx[base + t]), double(a.ry[base + t]), double(a.rz[base + t])};
+      const double g1 = double(a.rg1[base + t]), g2 = double(a.rg2[base + t]);
+      for (int u = 0; u < 3; ++u)
+        for (int v = 0; v < 3; ++v) M[3 * li + u][3 * lk + v] += (u == v ? g1 : 0.0) - g2 * x[u] * x[v];
+    }
+  }
+  for (int c = 0; c < N; ++c) {
+    int pr = c;
+    for (int u = c + 1; u < N; ++u)
+      if (fabs(M[u][c]) > fabs(M[pr][c])) pr = u;
+    if (pr != c)
+      for (int v = 0; v <= N; ++v) { double t = M[c][v]; M[c][v] = M[pr][v]; M[pr][v] = t; }
+    for (int u = c + 1; u < N; ++u) {
+      const double f = M[u][c] / M[c][c];
+      for (int v = c; v <= N; ++v) M[u][v] -= f * M[c][v];
+    }
+  }
+  for (int c = N - 1; c >= 0; --c) {
+    double acc = M[c][N];
+    for (int v = c + 1; v < N; ++v) acc -= M[c][v] * d[v];
+    d[c] = acc / M[c][c];
+  }
+}
+
+// 0-SCF, one thread per molecule: for the extended systems delta = omega alpha r (Jacobi, and for
+// molecules outside 2..8 atoms) or omega M^-1 r (block), mu = x + delta in FP64 (x = xl[0]), delta
+// in Dl for the shadow energy, and max|delta| for the residual; zero delta elsewhere.
+template <typename T>
+__global__ void k_iel_delta(Dev<T> a, const double *xl, double omega, int block, double *mu, v4<T> *Dl) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.nmol) return;
+  const int i0 = a.mol_start[m], nb = a.mol_start[m + 1] - i0;
+  CGSys &G = a.cg[a.sysid[i0]];
+  if (!G.iel_ext) {
+    for (int i = i0; i < i0 + nb; ++i) Dl[i] = v4<T>{T(0), T(0), T(0), T(0)};
+    return;
+  }
+  double d[24];
+  double M[24][25];
+  if (block && nb >= 2 && nb <= 8) {
+    iel_block_solve(a, i0, nb, M, d);
+  } else {
+    for (int li = 0; li < nb && li < 8; ++li) {
+      const v4<T> r = a.R[i0 + li];
+      const double al = double(a.alpha[i0 + li]);
+      d[3 * li] = al * double(r.x); d[3 * li + 1] = al * double(r.y); d[3 * li + 2] = al * double(r.z);
+    }
+  }
+  double mx = 0.0;
+  for (int li = 0; li < nb; ++li) {
+    const int i = i0 + li;
+    double dl[3];
+    if (li < 8) {
+      for (int c = 0; c < 3; ++c) dl[c] = omega * d[3 * li + c];
+    } else {  // molecules above 8 atoms: Jacobi, atom by atom
+      const v4<T> r = a.R[i];
+      const double al = double(a.alpha[i]);
+      dl[0] = omega * al * double(r.x); dl[1] = omega * al * double(r.y); dl[2] = omega * al * double(r.z);
+    }
+    for (int c = 0; c < 3; ++c) {
+      mu[3 * (size_t)i + c] = xl[3 * (size_t)i + c] + dl[c];
+      mx = fmax(mx, fabs(dl[c]));
+    }
+    Dl[i] = v4<T>{T(dl[0]), T(dl[1]), T(dl[2]), T(0)};
+  }
+  atomicMax(&G.acc_max, (unsigned long long)__double_as_longlong(mx));
+}
+
+// After the start (zscf: and the 0-SCF update): the extended 0-SCF systems' residual max|delta| /
+// norm and no CG; *any over the systems that still iterate (warm-up solves, SCF from x), which
+// with use_cond is also the captured loop's condition.
+__global__ void k_iel_begin(CGSys *cg, int nsys, int *any, int zscf, cudaGraphConditionalHandle cond, int use_cond) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
+  __shared__ int act;
+  if (threadIdx.x == 0) act = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+    CGSys &G = cg[s];
+    if (zscf && G.iel_ext) {
+      G.err = __longlong_as_double((long long)G.acc_max) / G.norm;
+      G.active = 0;
+      G.acc_max = 0;
+    }
+    if (G.active) atomicOr(&act, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *any = act;
+    if (use_cond) cudaGraphSetConditional(cond, act ? 1u : 0u);
+  }
+}
+
+// After the solve: mu (the CG result with the peek step; 0-SCF extended systems: already written),
+// the history push, and the auxiliary dipoles' step x_{n+1} = 2 Xh[0] - Xh[1] + kappa dx + a sum_k
+// c_k Xh[k] with Xh = (mu, mu, ...) on the first step, xl with Xh[0] = mu in the warm-up, xl after,
+// dx = mu - x on extended steps (0 in the warm-up); xl becomes (x_{n+1}, Xh[0], ..., Xh[K1 - 2]).
+struct IelCoef {
+  double kappa, a, c[10];
+  int nc, K1, zscf;
+};
+template <typename T>
+__global__ void k_iel_finish(Dev<T> a, double *mu, double *hist, double *xl, IelCoef co) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  const CGSys &G = a.cg[a.sysid[i]];
+  const size_t st = (size_t)a.nt * 3;
+  double m[3];
+  if (G.iel_ext && co.zscf) {
+    for (int c = 0; c < 3; ++c) m[c] = mu[3 * (size_t)i + c];
+  } else {
+    v4<T> x = a.X[i], r = a.R[i];
+    const T al = a.alpha[i], pk = T(a.peek);
+    if (a.peek != 0.0) { x.x += pk * r.x * al; x.y += pk * r.y * al; x.z += pk * r.z * al; }
+    m[0] = double(x.x); m[1] = double(x.y); m[2] = double(x.z);
+    for (int c = 0; c < 3; ++c) mu[3 * (size_t)i + c] = m[c];
+  }
+  for (int c = 0; c < 3; ++c) {
+    const size_t o = (size_t)3 * i + c;
+    hist[3 * st + o] = hist[2 * st + o];
+    hist[2 * st + o] = hist[st + o];
+    hist[st + o] = hist[o];
+    hist[o] = m[c];
+    double X[12];
+    for (int j = 0; j < co.K1; ++j) X[j] = G.iel_first ? m[c] : ((j == 0 && !G.iel_ext) ? m[c] : xl[j * st + o]);
+    double v = 2.0 * X[0] - X[1] + (G.iel_ext ? co.kappa * (m[c] - X[0]) : 0.0);
+    if (co.a != 0.0)
+      for (int k = 0; k < co.nc; ++k) v += co.a * co.c[k] * X[k];
+    xl[o] = v;
+    for (int j = 1; j < co.K1; ++j) xl[j * st + o] = X[j - 1];
+  }
+}
+
 // ------------------------------------------------------------------ energy, forces, virial
 // One warp per atom over its row: pair energies and their row gradients with the analytic
 // kernels G0..G3 (forcefield.py:2294-2360), LJ rows, the row field at (q, d) (dE/dd), the pair
 // virial sum g (x) x - gx (x) off; then the PME gradients of the atom: dU/dd and dU/dr through the
 // spline derivatives (the autodiff of pme.py:390-411 written out).
-template <typename T, int P, int MINB = 3>
+// SHADOW (iEL/0-SCF, forcefield.py:2011-2045, 2294-2360): the energy is the shadow potential's,
+// minus the pair and reciprocal energies of the dipoles Dl = delta alone (inside a molecule of 2..8
+// atoms with the block preconditioner, the i-side delta scaled by a.iel_keep = 1 - 1/omega); their
+// position gradients at fixed delta go to the forces, not to the virial (the fixed-mu strain
+// derivative); the sums of |delta|^2 and |delta|^2 / (2 alpha) go to the energy accumulators.
+template <typename T, int P, int MINB = 3, bool SHADOW = false>
 __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
   __shared__ T sh[WARPS_PER_BLOCK][3][3][P];
@@ -2001,8 +2229,27 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
     T gx0 = 0, gx1 = 0, gx2 = 0, gl0 = 0, gl1 = 0, gl2 = 0, fd0 = 0, fd1 = 0, fd2 = 0;
     T ee = 0, el = 0;
     T w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    T gs0 = 0, gs1 = 0, gs2 = 0;  // SHADOW: gradient of the delta-delta pair terms (forces only)
+    v4<T> Dli = v4<T>{T(0), T(0), T(0), T(0)};
+    bool blk_i = false;
+    if constexpr (SHADOW) {
+      Dli = a.Dl[i];
+      const int msz = a.molend[i] - a.molfirst[i];
+      blk_i = a.iel_keep_on && msz >= 2 && msz <= 8;
+    }
     auto pair = [&](int k, T x, T y, T z, T G0, T G1, T G2, T G3, int t) {
       v4<T> dk = a.D[k];
+      if constexpr (SHADOW) {
+        const v4<T> Dk = a.Dl[k];
+        const T wb = (blk_i && t < nsp) ? T(a.iel_keep) : T(1);  // molecule partners come first in a row
+        const T Dix = wb * (Dli.x * x + Dli.y * y + Dli.z * z), Dkx = Dk.x * x + Dk.y * y + Dk.z * z;
+        const T DiDk = wb * (Dli.x * Dk.x + Dli.y * Dk.y + Dli.z * Dk.z);
+        ee += G2 * Dix * Dkx - G1 * DiDk;
+        const T rad2 = -G3 * Dix * Dkx + G2 * DiDk;
+        gs0 += rad2 * x + G2 * (wb * Dli.x * Dkx + Dk.x * Dix);
+        gs1 += rad2 * y + G2 * (wb * Dli.y * Dkx + Dk.y * Dix);
+        gs2 += rad2 * z + G2 * (wb * Dli.z * Dkx + Dk.z * Dix);
+      }
       v4<T> pk = a.qls[k];  // q, R*/2, sqrt(eps) of the partner in one load
       T qk = pk.x;
       T dix = di.x * x + di.y * y + di.z * z;
@@ -2094,6 +2341,30 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
     const T *phi = a.Phi + S.rgrid0;
     const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2];
     T ge0 = 0, ge1 = 0, ge2 = 0, gw0 = 0, gw1 = 0, gw2 = 0;
+    if constexpr (SHADOW) {  // d/dr of the reciprocal energy of delta alone (its potential in Phi2)
+      const T f0 = Dli.x * es[0] + Dli.y * es[3] + Dli.z * es[6];
+      const T f1 = Dli.x * es[1] + Dli.y * es[4] + Dli.z * es[7];
+      const T f2 = Dli.x * es[2] + Dli.y * es[5] + Dli.z * es[8];
+      const T *phi2 = a.Phi2 + S.rgrid0;
+      T h0 = 0, h1 = 0, h2 = 0;
+      for (int p = lane; p < P * P * P; p += 32) {
+        int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
+        int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
+        int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
+        int i3 = b.z + j3; if (i3 >= K3) i3 -= K3;
+        T ph = phi2[((size_t)i1 * K2 + i2) * K3 + i3];
+        T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2], t3 = sh[warp][0][2][j3];
+        T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2], u3 = sh[warp][1][2][j3];
+        T v1 = sh[warp][2][0][j1], v2 = sh[warp][2][1][j2], v3 = sh[warp][2][2][j3];
+        h0 += ph * (f0 * v1 * t2 * t3 + f1 * u1 * u2 * t3 + f2 * u1 * t2 * u3);
+        h1 += ph * (f0 * u1 * u2 * t3 + f1 * t1 * v2 * t3 + f2 * t1 * u2 * u3);
+        h2 += ph * (f0 * u1 * t2 * u3 + f1 * t1 * u2 * u3 + f2 * t1 * t2 * v3);
+      }
+      // the pair part is KE (gx + gs); the reciprocal part of -U_rec(0, delta) enters with a minus sign
+      gs0 = gs0 - h0 * es[0] - h1 * es[1] - h2 * es[2];
+      gs1 = gs1 - h0 * es[3] - h1 * es[4] - h2 * es[5];
+      gs2 = gs2 - h0 * es[6] - h1 * es[7] - h2 * es[8];
+    }
     for (int p = lane; p < P * P * P; p += 32) {
       int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
       int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
@@ -2115,6 +2386,7 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
 #pragma unroll
     for (int k = 0; k < 24; ++k) red_in[k] = warp_sum<T>(red_in[k]);
     T w7 = warp_sum<T>(w[7]), w8 = warp_sum<T>(w[8]);
+    if constexpr (SHADOW) { gs0 = warp_sum<T>(gs0); gs1 = warp_sum<T>(gs1); gs2 = warp_sum<T>(gs2); }
     if (lane == 0) {
       double gd[3], gr[3];
       for (int bb = 0; bb < 3; ++bb) {
@@ -2129,9 +2401,15 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
       double ofs[3] = {of.x, of.y, of.z};
       double cs = a.c_self;
       double dE[3];
+      const double gsh[3] = {double(gs0), double(gs1), double(gs2)};
       for (int c = 0; c < 3; ++c) {
-        a.forces[3 * i + c] = -(KE * gx[c] + gl[c] + KE * gr[c]);
+        a.forces[3 * i + c] = -(KE * gx[c] + gl[c] + KE * gr[c] + (SHADOW ? KE * gsh[c] : 0.0));
         dE[c] = KE * (fd[c] + gd[c] - cs * d3[c]);
+      }
+      if constexpr (SHADOW) {
+        const double dl2 = double(Dli.x) * double(Dli.x) + double(Dli.y) * double(Dli.y) + double(Dli.z) * double(Dli.z);
+        vals[13] = dl2;
+        vals[14] = dl2 / (2.0 * double(a.alpha[i]));
       }
       a.dEdd[i] = make_double4(dE[0], dE[1], dE[2], 0);
       vals[0] = double(red_in[9]);
@@ -2149,15 +2427,17 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
           vals[4 + aa * 3 + bb] = 0.5 * wsum[aa * 3 + bb] - (KE * gx[aa] + gl[aa]) * ofs[bb] - KE * (gr[aa] * ofs[bb] + gd[aa] * d3[bb]);
     }
   }
+  constexpr int NV = SHADOW ? 15 : 13;
   if (lane == 0)
-    for (int k = 0; k < 13; ++k) red[warp][k] = vals[k];
+    for (int k = 0; k < NV; ++k) red[warp][k] = vals[k];
   __syncthreads();
-  if (threadIdx.x < 13) {
+  if (threadIdx.x < NV) {
     double v = 0;
     for (int w2 = 0; w2 < WARPS_PER_BLOCK; ++w2) v += red[w2][threadIdx.x];
     EnergyAcc &E = a.eacc[s];
     double *dst = threadIdx.x == 0 ? &E.e_pair : threadIdx.x == 1 ? &E.e_lj : threadIdx.x == 2 ? &E.d2
-                  : threadIdx.x == 3 ? &E.upol : &E.vir[threadIdx.x - 4];
+                  : threadIdx.x == 3 ? &E.upol : threadIdx.x == 13 ? &E.dd2 : threadIdx.x == 14 ? &E.dda
+                  : &E.vir[threadIdx.x - 4];
     atomicAdd(dst, v);
   }
 }
@@ -2186,7 +2466,8 @@ __global__ void k_cov_forces(Dev<T> a) {
 // Energies and virial of every system (forcefield.py:2011-2045, 2420-2430, lj.py:87-114):
 // E_elec = KE [rows/2 + U_rec + U_self + U_bg + U_pol], E_vdw = rows/2 + tail.
 __global__ void k_energy_finish(const SysInfo *sys, const BoxInfo *box, const EnergyAcc *E, int nsys, double beta, double c_self,
-                                double cutoff, int lj, int lj_lrc, int induce, double *energy, double *virial, unsigned *status) {
+                                double cutoff, int lj, int lj_lrc, int induce, double *energy, double *virial, unsigned *status,
+                                const EnergyAcc *E2 = nullptr, double omega = 1.0) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
@@ -2194,9 +2475,14 @@ __global__ void k_energy_finish(const SysInfo *sys, const BoxInfo *box, const En
   const SysInfo &S = sys[s];
   double vol = box[s].vol;
   double uself = -(beta / SQRT_PI) * S.sum_q2 - 0.5 * c_self * e.d2;
+  double urec_delta = 0.0;
+  if (E2) {  // iEL/0-SCF shadow energy (forcefield.py:2037-2042)
+    uself += 0.5 * c_self * e.dd2 - (1.0 - 1.0 / omega) * e.dda;
+    urec_delta = E2[s].vinf[0];
+  }
   double ubg = -PI * S.sum_q * S.sum_q / (2.0 * vol * beta * beta);
   double upol = induce ? e.upol : 0.0;
-  double elec = 0.5 * KE * e.e_pair + KE * (e.vinf[0] + uself + ubg + upol);
+  double elec = 0.5 * KE * e.e_pair + KE * (e.vinf[0] - urec_delta + uself + ubg + upol);
   double tail = (lj && lj_lrc) ? -2.0 * PI * S.tail_sb / (3.0 * vol * cutoff * cutoff * cutoff) : 0.0;
   double vdw = 0.5 * e.e_lj + tail;
   if (energy) {

@@ -32,10 +32,10 @@ ELEC_LEVELS = {"q": 0, "qp": 1, "qi": 2, "qpi": 3}
 PREDICTORS = {"none": 0, "mu1": 1, "mu3": 3, "mu4": 4, "nn": 5}
 
 # The settings of MDSettings that this engine implements, with the reference's defaults
-# (forcefield.py:142-516).  Other reference settings (iEL, IPS, DE / GVDW, split rows, the local
-# preconditioner, the "ls" predictor, differentiable solves) are outside this path.
+# (forcefield.py:142-516).  Other reference settings (IPS, DE / GVDW, the local preconditioner, the
+# "ls" predictor, differentiable solves) are outside this path.
 _OUT_OF_SCOPE = {
-    "iel", "iel_iter", "iel_order", "iel_kappa", "iel_alpha", "iel_precond", "iel_omega", "iel_shadow", "long_range",
+    "long_range",
     "ips_order", "ips_boundary", "de_alpha", "de_beta", "gvdw_rep", "local_cut", "local_niter",
     "extrap_order", "extrap_steps", "differentiable", "adjoint_tol", "neighbor_list",
 }
@@ -62,6 +62,15 @@ class MDSettings:
     norm_refresh: int = 1000
     peek: float = 0.65
     precision: str = "mixed"
+    # extended-Lagrangian dipoles (ExtendedLagrangian, forcefield.py:246-282)
+    iel: str = "none"
+    iel_iter: int = 1
+    iel_order: int = 7
+    iel_kappa: float | None = None
+    iel_alpha: float | None = None
+    iel_precond: str = "block"
+    iel_omega: float = 1.0
+    iel_shadow: bool = True
 
     def replace(self, **changes) -> MDSettings:
         """Return a copy with settings changed (TypeError for unknown names, as forcefield.py:480)."""
@@ -85,6 +94,14 @@ class MDSettings:
             raise ValueError("cutoff must be positive")
         if self.elec_cutoff is not None and not (0 < self.elec_cutoff <= self.cutoff):
             raise ValueError("elec_cutoff must be in (0, cutoff] (or None)")
+        if self.iel not in ("none", "0scf", "scf"):
+            raise ValueError(f"iel {self.iel!r} (none | 0scf | scf)")
+        if self.iel_order not in (0, 3, 4, 5, 6, 7, 8, 9):
+            raise ValueError("iel_order must be 0 or 3..9")
+        if self.iel_precond not in ("block", "jacobi"):
+            raise ValueError(f"iel_precond {self.iel_precond!r} (block | jacobi)")
+        if not (self.iel_omega > 0) or self.iel_iter < 0:
+            raise ValueError("iel_omega must be positive and iel_iter >= 0")
 
     @property
     def split_rows(self) -> bool:
@@ -98,6 +115,11 @@ class MDSettings:
     def perm_dipoles(self) -> bool:
         return "p" in self.elec
 
+
+# (kappa, a) of Niklasson et al., J. Chem. Phys. 130, 214109 (2009), by dissipation order (the
+# defaults when only one of iel_kappa / iel_alpha is given; forcefield.py:667-676)
+_XL_TABLE = {0: (1.0, 0.0), 3: (1.69, 0.150), 4: (1.75, 0.057), 5: (1.82, 0.018), 6: (1.84, 0.0055), 7: (1.86, 0.0016),
+             8: (1.88, 0.00044), 9: (1.89, 0.00012)}
 
 DSUM_TOL = 3.95e-8  # Amber-convention direct-sum tolerance of the default pair 0.9 nm / 4.0 nm^-1
 
@@ -138,9 +160,15 @@ class InductionState:
     hist: torch.Tensor   # (4, N, 3) float64, newest first
     count: torch.Tensor  # (S,) int32
     norm: torch.Tensor   # (S,) float64
+    xl: torch.Tensor | None = None  # iEL: (pgm_iel_len(order), N, 3) float64 auxiliary dipoles, newest first
 
     def clone(self) -> InductionState:
-        return InductionState(self.mu.clone(), self.hist.clone(), self.count.clone(), self.norm.clone())
+        return InductionState(self.mu.clone(), self.hist.clone(), self.count.clone(), self.norm.clone(),
+                              None if self.xl is None else self.xl.clone())
+
+    def _c(self):
+        return _lib.PgmInduction(self.mu.data_ptr(), self.hist.data_ptr(), self.count.data_ptr(), self.norm.data_ptr(),
+                                 None if self.xl is None else self.xl.data_ptr())
 
 
 class Result(NamedTuple):
@@ -200,6 +228,12 @@ class PGMForceField:
             float(settings.dipole_tol), int(settings.max_iter), PREDICTORS[settings.predictor], int(settings.fused),
             int(settings.norm_refresh), float(settings.peek), int(row_capacity or 0), float(settings.skin), 0,
             float(settings.elec_cutoff or 0.0), int(elec_capacity or 0),
+            {"none": 0, "0scf": 1, "scf": 2}[settings.iel], int(settings.iel_order),
+            int(settings.iel_kappa is not None or settings.iel_alpha is not None),
+            float(settings.iel_kappa if settings.iel_kappa is not None else _XL_TABLE[settings.iel_order][0]),
+            float(settings.iel_alpha if settings.iel_alpha is not None else _XL_TABLE[settings.iel_order][1]),
+            float(settings.iel_omega), 0 if settings.iel_precond == "block" else 1, int(settings.iel_iter),
+            int(not settings.iel_shadow),
         )
         descs = (_lib.PgmSystemDesc * self.nsys)()
         self._keep = []
@@ -251,11 +285,15 @@ class PGMForceField:
     def init_induction(self) -> InductionState:
         """A fresh solver state: zero dipoles and history, normaliser 1 (forcefield.py:1436-1450)."""
         dev = self.device
+        xl = None
+        if self.s.iel != "none":
+            xl = torch.zeros((self._lib.pgm_iel_len(int(self.s.iel_order)), self.n, 3), dtype=torch.float64, device=dev)
         return InductionState(
             torch.zeros((self.n, 3), dtype=torch.float64, device=dev),
             torch.zeros((4, self.n, 3), dtype=torch.float64, device=dev),
             torch.zeros(self.nsys, dtype=torch.int32, device=dev),
             torch.ones(self.nsys, dtype=torch.float64, device=dev),
+            xl,
         )
 
     @property
@@ -368,7 +406,7 @@ class PGMForceField:
         b = self._boxes(H)
         it, w = self._idx(idx)
         F = torch.empty((self.n, 3), dtype=torch.float64, device=self.device)
-        di = _lib.PgmInduction(ind.mu.data_ptr(), ind.hist.data_ptr(), ind.count.data_ptr(), ind.norm.data_ptr())
+        di = ind._c()
         E, V, I, R, Sst = self._energy.clone(), self._virial.clone(), self._iters.clone(), self._resid.clone(), self._status.clone()
         out = _lib.PgmOutputs(E.data_ptr(), F.data_ptr(), V.data_ptr(), I.data_ptr(), R.data_ptr(), Sst.data_ptr())
         _lib.check(self._lib.pgm_compute(self._h, self._stream(), _ptr(x), _ptr(b), _ptr(it), w, C.byref(di), C.byref(out)))
@@ -382,7 +420,7 @@ class PGMForceField:
         energy, virial, iterations, residual and status of the Result are this instance's buffers,
         overwritten by the next call.
         """
-        di = _lib.PgmInduction(ind.mu.data_ptr(), ind.hist.data_ptr(), ind.count.data_ptr(), ind.norm.data_ptr())
+        di = ind._c()
         out = _lib.PgmOutputs(self._energy.data_ptr(), forces.data_ptr(), self._virial.data_ptr(), self._iters.data_ptr(),
                               self._resid.data_ptr(), self._status.data_ptr())
         _lib.check(self._lib.pgm_compute(self._h, self._stream(), _ptr(pos), _ptr(boxes), None, 0, C.byref(di), C.byref(out)))
@@ -399,7 +437,7 @@ class PGMForceField:
         x = _f64(pos, self.device)
         b = self._boxes(H)
         it, w = self._idx(idx)
-        di = _lib.PgmInduction(ind.mu.data_ptr(), ind.hist.data_ptr(), ind.count.data_ptr(), ind.norm.data_ptr())
+        di = ind._c()
         E, I, Sst = self._energy.clone(), self._iters.clone(), self._status.clone()
         _lib.check(self._lib.pgm_energy(self._h, self._stream(), _ptr(x), _ptr(b), _ptr(it), w, C.byref(di), _ptr(E), _ptr(I),
                                         _ptr(Sst)))

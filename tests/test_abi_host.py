@@ -38,8 +38,11 @@ def test_settings_mirror_the_reference_names_and_errors():
     assert s.replace(dipole_tol=1e-6).dipole_tol == 1e-6
     with pytest.raises(TypeError):
         s.replace(nonsense=1)
+    assert s.replace(iel="0scf").iel == "0scf"  # extended-Lagrangian dipoles are in this engine
     with pytest.raises(ValueError):
-        s.replace(iel="0scf")
+        s.replace(long_range="ips")  # a reference setting outside this path
+    with pytest.raises(ValueError):
+        s.replace(iel="xl")
     with pytest.raises(ValueError):
         MDSettings(elec="qq")
 

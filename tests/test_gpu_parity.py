@@ -374,7 +374,7 @@ def test_pgm3p25_512_matches_reference_golden(pgm3p25_512_system, golden_pgm3p25
     """The reference's ff_pgm3p25_512 regression point (examples/water512 frame, truncated
     octahedron, default settings, 30^3 mesh): FP64 against its float64 record (energy 1e-9, forces
     1e-8 RMS, iterations equal, virial 1e-6); mixed precision against its mixed record (energy
-    1e-6, forces and dipoles 1e-5 RMS relative)."""
+    1e-6) and its float64 record (forces and dipoles 1e-5 RMS relative; 2e-5 against its mixed one)."""
     from conftest import PGM3P25_512_SETTINGS
 
     from pgm_jax_b200.forcefield import MDSettings, PGMForceField
@@ -390,8 +390,13 @@ def test_pgm3p25_512_matches_reference_golden(pgm3p25_512_system, golden_pgm3p25
         ref = float(g[f"{prec}.energy.{k}"])
         assert abs(float(res.energy[k][0]) - ref) <= tol_e[k] * abs(ref), (k, float(res.energy[k][0]), ref)
     tol = 1e-8 if prec == "double" else 1e-5
-    assert rms_rel(res.forces.cpu().numpy(), g[f"{prec}.forces"]) <= tol
-    assert rms_rel(res.induction.mu.cpu().numpy(), g[f"{prec}.mu"]) <= tol
+    # FP32 kernels against the float64 record; against the reference's own mixed record (its FP32
+    # path's rounding added to ours) at twice that
+    assert rms_rel(res.forces.cpu().numpy(), g["double.forces"]) <= tol
+    assert rms_rel(res.induction.mu.cpu().numpy(), g["double.mu"]) <= tol
+    if prec == "mixed":
+        assert rms_rel(res.forces.cpu().numpy(), g["mixed.forces"]) <= 2 * tol
+        assert rms_rel(res.induction.mu.cpu().numpy(), g["mixed.mu"]) <= 2 * tol
     if prec == "double":
         assert int(res.iterations[0]) == int(g["double.iterations"])
         W = g["double.strain"]
