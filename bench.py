@@ -749,6 +749,8 @@ def main() -> None:
     ap.add_argument("--workload", default="water32768", choices=["water32768", "water4096", "batch", "pimd", "npt"],
                     help="water32768: the headline; water4096 the same line on the smaller box; the others print "
                     "their own line (one GPU)")
+    ap.add_argument("--equil-steps", type=int, default=None,
+                    help="relaxation steps of the lattice start before timing (default: the workload's)")
     ap.add_argument("--elec-cutoff", type=float, default=None,
                     help="split rows: electrostatics cutoff [nm] below the 0.9 nm LJ cutoff (Ewald coefficient for it)")
     args = ap.parse_args()
@@ -761,6 +763,8 @@ def main() -> None:
     if args.workload in BOXES:
         W.clear()
         W.update(BOXES[args.workload], name=args.workload)
+        if args.equil_steps is not None:
+            W["equil_steps"] = args.equil_steps
     if args.impl == "reference":
         run_reference(args)
     elif args.workload not in BOXES:

@@ -242,7 +242,8 @@ PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, floa
  * No counterpart in the reference (XLA chooses its own fusions).  The kernel variants of a handle:
  * rowfield_lanes, the lanes that share one neighbour row in the CG matvec's row stream (32: a warp
  * per atom; 16, 8: two or four atoms per warp); forces_blocks_per_sm, the minimum resident blocks of
- * 256 threads the force pass is compiled for (2, 3, 4: registers against warps).  Unless fixed by
+ * 256 threads the force pass is compiled for (2, 3, 4: registers against warps); sweep_early, the
+ * order of the CG sweep's concurrent parts.  Unless fixed by
  * pgm_set_tuning, the first pgm_compute that is not being captured times every variant on its own
  * rows (CUDA events on its stream, the mean of 10 launches after one) and keeps the fastest;
  * handles of the same precision, order, atoms, row capacity and grid size in one process share the
@@ -254,10 +255,15 @@ typedef struct {
     double forces_ms[3];       /* timed launches: 2, 3, 4 blocks per SM [ms] */
     int tuned;                 /* 1 once timed (or taken from the cache) */
     int from_cache;
+    int sweep_early;           /* the CG direction's sweep: 0 the row field forked after the spread
+                                  (on p), 1 at the start of the sweep (on z; the rows of p = z +
+                                  beta p_prev combined in the gather) */
+    double sweep_ms[2];        /* timed sweeps of the two schedules [ms] */
 } PgmTuning;
 PgmStatus pgm_tuning(PgmHandle *h, PgmTuning *out);
-/* Fix the variants (0 leaves one as it is; both 0: autotune again at the next direct step). */
-PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm);
+/* Fix the variants (0, or -1 for sweep_early, leaves one as it is; all so: autotune again at the
+ * next direct step). */
+PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm, int sweep_early);
 /* Time the variants now on the last step's rows (synchronises the stream). */
 PgmStatus pgm_autotune(PgmHandle *h, void *stream);
 
@@ -288,6 +294,17 @@ PgmStatus pgm_nn_loss_grad(void *stream, const float *weights, const float *inv,
 PgmStatus pgm_nn_adam(void *stream, float *weights, float *grad, float *m, float *v, float lr, float beta1, float beta2,
                       float eps, int step);
 const char *pgm_nn_last_error(void);
+
+/* ------------------------------------------------------------------ tcgen05 dense layers
+ * No counterpart in the reference (its learned models run through XLA).  C = act(A W^T + bias) on
+ * the 5th-generation tensor cores: A (M, lda) BF16 with the first K of every row used (lda a
+ * multiple of 8), W (N, K) BF16, bias N floats or NULL, C (M, ldc) FP32 (out_f32) or BF16; act 0
+ * none, 1 SiLU; BF16 products accumulated in FP32 (tensor memory).  Compiled (K, N): (16, 64),
+ * (64, 64), (64, 128), (80, 64), (64, 32), (128, 16); others return PGM_ERR_UNSUPPORTED.  *err
+ * (device int) is set when a tile's wait for its MMAs gave up (it is never expected to). */
+PgmStatus pgm_tc_gemm(void *stream, int K, int N, int act, int out_f32, const void *A, int lda, int M, const void *W,
+                      const float *bias, void *C, int ldc, int *err);
+const char *pgm_tc_last_error(void);
 
 /* ------------------------------------------------------------------ allocation-free field
  * pgm_field_static has no counterpart in the reference.  It is for callers that must not allocate

@@ -26,7 +26,7 @@ EXPORTS = (
     "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
     "pgm_set_nn_model", "pgm_nn_features", "pgm_nn_param_count", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam",
     "pgm_nn_last_error", "pgm_set_nn_fallback", "pgm_nn_fallback_stats", "pgm_tuning", "pgm_set_tuning", "pgm_autotune",
-    "pgm_iel_len",
+    "pgm_iel_len", "pgm_tc_gemm", "pgm_tc_last_error",
 )
 
 STATUS_ROW_OVERFLOW = 0x1
@@ -39,7 +39,8 @@ STATUS_LIST_OVERFLOW = 0x10
 class PgmTuning(C.Structure):
     _fields_ = [
         ("rowfield_lanes", C.c_int), ("forces_blocks_per_sm", C.c_int), ("rowfield_ms", C.c_double * 3),
-        ("forces_ms", C.c_double * 3), ("tuned", C.c_int), ("from_cache", C.c_int),
+        ("forces_ms", C.c_double * 3), ("tuned", C.c_int), ("from_cache", C.c_int), ("sweep_early", C.c_int),
+        ("sweep_ms", C.c_double * 2),
     ]
 
 
@@ -148,10 +149,13 @@ def load(path: str | None = None):
     lib.pgm_nn_loss_grad.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_float, vp, vp]
     lib.pgm_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
     lib.pgm_nn_last_error.restype = C.c_char_p
+    lib.pgm_tc_gemm.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp]
+    lib.pgm_tc_gemm.restype = C.c_int
+    lib.pgm_tc_last_error.restype = C.c_char_p
     lib.pgm_iel_len.argtypes = [C.c_int]
     lib.pgm_iel_len.restype = C.c_int
     lib.pgm_tuning.argtypes = [H, C.POINTER(PgmTuning)]
-    lib.pgm_set_tuning.argtypes = [H, C.c_int, C.c_int]
+    lib.pgm_set_tuning.argtypes = [H, C.c_int, C.c_int, C.c_int]
     lib.pgm_autotune.argtypes = [H, vp]
     for n in ("pgm_tuning", "pgm_set_tuning", "pgm_autotune"):
         getattr(lib, n).restype = C.c_int

@@ -8,11 +8,13 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libpgm_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", n) for n in ("pgm_api.cu", "pgm_md.cu", "pgm_static.cu", "pgm_nn.cu", "pgm_pimd.cu")]
+SOURCES = [os.path.join(HERE, "csrc", n)
+           for n in ("pgm_api.cu", "pgm_md.cu", "pgm_static.cu", "pgm_nn.cu", "pgm_pimd.cu", "pgm_mpnn.cu")]
 DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "pgm_device.cuh"),
     os.path.join(HERE, "csrc", "pgm_kernels.cuh"),
     os.path.join(HERE, "csrc", "pgm_nn.cuh"),
+    os.path.join(HERE, "csrc", "pgm_tc.cuh"),
     os.path.join(os.path.dirname(HERE), "include", "pgm_b200.h"),
 ]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc")

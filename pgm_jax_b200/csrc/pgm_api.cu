@@ -111,7 +111,7 @@ struct EngineBase {
   virtual int max_vdw_count() = 0;
   virtual void set_nn(const float *w, float sigma, float rg) = 0;
   virtual void set_nn_fallback(double factor) = 0;
-  virtual void set_tuning(int rowfield_lanes, int forces_blocks) = 0;
+  virtual void set_tuning(int rowfield_lanes, int forces_blocks, int sweep_early) = 0;
   virtual void autotune(cudaStream_t st) = 0;
   virtual PgmTuning tuning() const = 0;
   virtual void nn_fallback_stats(long long *fallbacks, double *ref_err) = 0;
@@ -196,7 +196,7 @@ struct Engine : EngineBase {
   DBuf<pgm::v4<T>> qls;
   DBuf<double> mass, cov_c, cov_c_flat, bmod;
   DBuf<int4> base;
-  DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D, Fv;
+  DBuf<pgm::v4<T>> frac, X, R, Z, Pv, AP, Bv, D, Fv, Fpv;
   DBuf<double4> pperm, off, dEdd;
   DBuf<int> cell_of, slot_of, cell_count, cell_start, cell_atoms;
   DBuf<double4> spos, pos_ref, pos4;
@@ -219,7 +219,7 @@ struct Engine : EngineBase {
   DBuf<pgm::v4<T>> Dl;
   DBuf<T> Phi2;
   DBuf<pgm::EnergyAcc> d_eacc2;
-  PgmTuning tune{};          // kernel variants in use (autotuned at the first direct step unless fixed)
+  PgmTuning tune{32, 3};     // kernel variants in use (autotuned at the first direct step unless fixed)
   bool tune_fixed = false;
   double nn_fb_factor = 2.0;  // learned guess: fall back to x4 when its start residual is above this x the record
   DBuf<int> dfb;              // some system falls back (the host-driven solve reads it)
@@ -289,7 +289,7 @@ struct Engine : EngineBase {
     a.max_count = dmax.p;
     a.mce = mce; a.rnv = split ? rnv.p : nullptr; a.rce2 = rc_e * rc_e;
     a.nn_e4 = nn_e4.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
-    a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p; a.F = Fv.p;
+    a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p; a.F = Fv.p; a.Fp = Fpv.p;
     a.Q = Q.p; a.Phi = Phi.p; a.Ginf = Ginf.p; a.C = C.p; a.tw = tw.p; a.bmod = bmod.p;
     a.forces = forces; a.dEdd = dEdd.p;
     a.Dl = Dl.p; a.Phi2 = Phi2.p;
@@ -538,7 +538,7 @@ struct Engine : EngineBase {
     }
     mass.upload(h_mass); cov_c.upload(h_covc); cov_c_flat.upload(h_covc_flat); bmod.upload(h_bmod);
     tw.upload(h_tw);
-    base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt); Fv.alloc(nt);
+    base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt); Fv.alloc(nt); Fpv.alloc(nt);
     pperm.alloc(nt); off.alloc(nt); dEdd.alloc(nt);
     cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt); spos.alloc(nt);
     pos_ref.alloc(nt); pos4.alloc(nt); ncand.alloc(nt); cand.alloc((size_t)nt * cc); nb_flag.alloc(1); nb_builds.alloc(1);
@@ -735,11 +735,12 @@ struct Engine : EngineBase {
     else if (b == 4) go(std::integral_constant<int, 4>{});
     else go(std::integral_constant<int, 3>{});
   }
-  void set_tuning(int lanes, int blocks) override {
+  void set_tuning(int lanes, int blocks, int early) override {
     ++generation;  // captured steps hold the old variants
-    tune_fixed = lanes > 0 || blocks > 0;
+    tune_fixed = lanes > 0 || blocks > 0 || early >= 0;
     if (lanes > 0) tune.rowfield_lanes = lanes;
     if (blocks > 0) tune.forces_blocks_per_sm = blocks;
+    if (early >= 0) tune.sweep_early = early;
     if (!tune_fixed) tune.tuned = 0;  // autotune again at the next direct step
   }
   PgmTuning tuning() const override { return tune; }
@@ -782,6 +783,17 @@ struct Engine : EngineBase {
       if (tune.rowfield_ms[v] < tune.rowfield_ms[bl]) bl = v;
       if (tune.forces_ms[v] < tune.forces_ms[bb]) bb = v;
     }
+    tune.rowfield_lanes = lanes[bl];
+    // the CG direction's sweep (spread with the update of p, FFT chain, row field, gather) with the
+    // row field forked after the spread or at the start of the sweep (on z)
+    if (overlap) {
+      for (int v = 0; v < 2; ++v) {
+        tune.sweep_early = v;
+        tune.sweep_ms[v] = time([&] { sweep<false, true, 0, 1>(st, a, Pv.p, AP.p); });
+      }
+      tune.sweep_early = tune.sweep_ms[1] < tune.sweep_ms[0] ? 1 : 0;
+    }
+    CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // leave the spread grid cleared
     launches = l0;
     CK(cudaEventDestroy(e0));
     CK(cudaEventDestroy(e1));
@@ -1060,6 +1072,19 @@ struct Engine : EngineBase {
     // the loop body is captured as a sequence of its own: it forks to its own stream
     cudaStream_t ax = in_body ? aux_b : aux;
     cudaEvent_t ef = in_body ? ev_fork_b : ev_fork, ej = in_body ? ev_join_b : ev_join;
+    if (tune.sweep_early) {
+      // the row field starts with the sweep, beside the spread and the FFT chain; for a CG
+      // direction it takes z (the rows of p = z + beta p_prev are combined in the gather)
+      CK(cudaEventRecord(ef, st));
+      CK(cudaStreamWaitEvent(ax, ef, 0));
+      rowfield<WITH_Q, ACT>(ax, a, UPDATE_P ? Z.p : vin, Fv.p, false);
+      CK(cudaEventRecord(ej, ax));
+      launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
+      fft_chain(st, a, ACT, false);
+      CK(cudaStreamWaitEvent(st, ej, 0));
+      launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false, UPDATE_P>, nwblk, 256, 0, st, a, vin, out);
+      return;
+    }
     launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
     CK(cudaEventRecord(ef, st));
     CK(cudaStreamWaitEvent(ax, ef, 0));
@@ -1650,11 +1675,12 @@ PgmStatus pgm_tuning(PgmHandle *h, PgmTuning *out) {
   return PGM_OK;
 }
 
-PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm) {
+PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm, int sweep_early) {
   if (!h || !(rowfield_lanes == 0 || rowfield_lanes == 8 || rowfield_lanes == 16 || rowfield_lanes == 32) ||
-      !(forces_blocks_per_sm == 0 || (forces_blocks_per_sm >= 2 && forces_blocks_per_sm <= 4)))
-    return fail(PGM_ERR_INVALID, "rowfield_lanes 0, 8, 16 or 32; forces_blocks_per_sm 0, 2, 3 or 4");
-  h->eng->set_tuning(rowfield_lanes, forces_blocks_per_sm);
+      !(forces_blocks_per_sm == 0 || (forces_blocks_per_sm >= 2 && forces_blocks_per_sm <= 4)) || sweep_early < -1 ||
+      sweep_early > 1)
+    return fail(PGM_ERR_INVALID, "rowfield_lanes 0, 8, 16 or 32; forces_blocks_per_sm 0, 2, 3 or 4; sweep_early -1, 0 or 1");
+  h->eng->set_tuning(rowfield_lanes, forces_blocks_per_sm, sweep_early);
   return PGM_OK;
 }
 

@@ -80,6 +80,7 @@ struct Dev {
   // vectors
   v4<T> *X, *R, *Z, *P, *AP, *B, *D;
   v4<T> *F;  // row field of a sweep (computed concurrently with the PME chain)
+  v4<T> *Fp; // the early-fork schedule: row field of the previous CG direction
   // grids
   T *Q, *Phi, *Ginf;
   c2<T> *C;
@@ -1282,8 +1283,10 @@ __global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__r
   }
 }
 
-// ROWS: the row sum is computed here; otherwise it is read from a.F (k_rowfield).
-template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true>
+// ROWS: the row sum is computed here; otherwise it is read from a.F (k_rowfield).  COMBINE (the
+// CG direction's sweep with the row field started before the spread): a.F holds the rows of
+// z, and the rows of p = z + beta p_prev are a.F + beta a.Fp (a.Fp: those of p_prev, rewritten).
+template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true, bool COMBINE = false>
 __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
   pdl_enter();
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
@@ -1390,6 +1393,14 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
     g0 = warp_sum<T>(g0); g1 = warp_sum<T>(g1); g2 = warp_sum<T>(g2);
     if (lane == 0) {
       if (!ROWS) { v4<T> fr = a.F[i]; f0 = fr.x; f1 = fr.y; f2 = fr.z; }
+      if (COMBINE) {
+        const double beta = a.cg[s].beta;
+        if (beta != 0.0) {
+          const v4<T> fp = a.Fp[i];
+          f0 += T(beta) * fp.x; f1 += T(beta) * fp.y; f2 += T(beta) * fp.z;
+        }
+        a.Fp[i] = v4<T>{f0, f1, f2, T(0)};
+      }
       // dU/dd_b = sum_a g_a Hinv[b][a] K_a
       T es[9];
 #pragma unroll

@@ -1,0 +1,191 @@
+// pgm_tc.cuh -- dense layers of the learned guess on the 5th-generation tensor cores (sm_100a).
+//
+// C[M x N] = act(A[M x K] W[N x K]^T + bias): BF16 operands, FP32 accumulation in tensor memory.
+// One CTA of 128 threads per 128-row tile of A: the tile and W are staged in shared memory in the
+// K-major layout without swizzle (8-row x 16-byte core matrices, the two core matrices of one
+// instruction's K = 16 adjacent: leading byte offset 128, stride byte offset (K / 8) x 128), one
+// elected thread issues K / 16 tcgen05.mma (kind::f16, M = 128, N) into a TMEM accumulator of
+// 128 lanes x N columns and commits them to an mbarrier; every warp then reads its 32 lanes with
+// tcgen05.ld, adds the bias, applies the activation and stores its rows.
+//
+// Waits are bounded: a wait on the MMAs' mbarrier that has not completed after a fixed number of
+// tries sets *err, waits once more (bounded) and still frees the tensor memory before returning.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pgmtc {
+
+constexpr int TM = 128;       // rows of A per tile (the MMA's M)
+constexpr int THREADS = 128;  // four warps: warp w reads TMEM lanes 32 w .. 32 w + 31
+
+// Activations of the epilogue.
+constexpr int ACT_NONE = 0, ACT_SILU = 1;
+
+// Shared-memory matrix descriptor of a K-major, unswizzled operand (sm_100 descriptor version 1):
+// start address, leading byte offset (between the two core matrices adjacent in K), stride byte
+// offset (between core matrices adjacent in M or N), all in 16-byte units.
+__host__ __device__ constexpr uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator, BF16 A and B, both K-major,
+// dense, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Byte offset of element (r, k) of an R x K BF16 operand in that layout.
+__host__ __device__ constexpr int tile_off(int r, int k, int K) {
+  return (r >> 3) * (K >> 3) * 128 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// Tensor-memory columns for an N-column accumulator: a power of two, at least 32.
+__host__ __device__ constexpr int tmem_cols(int N) { return N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256; }
+
+// Shared memory of a tile: A (TM x K), W (N x K), the mbarrier and the TMEM address.
+__host__ __device__ constexpr size_t smem_bytes(int K, int N) {
+  return (size_t)TM * K * 2 + (size_t)N * K * 2 + 64;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Waits for phase `parity` of an mbarrier with at most `tries` polls; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int tries) {
+  for (int t = 0; t < tries; ++t) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <typename OutT>
+__device__ __forceinline__ void store_val(OutT *p, float v);
+template <>
+__device__ __forceinline__ void store_val<float>(float *p, float v) { *p = v; }
+template <>
+__device__ __forceinline__ void store_val<__nv_bfloat16>(__nv_bfloat16 *p, float v) { *p = __float2bfloat16(v); }
+
+// C = act(A W^T + bias) for one 128-row tile per CTA.  A: M rows of lda BF16 (the first K used),
+// 16-byte aligned rows; W: N x K BF16 (K contiguous); bias: N floats or null; C: M rows of ldc.
+// K: a multiple of 16 up to 256; N: a multiple of 16 up to 256.
+template <int K, int N, int ACT, typename OutT>
+__global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__restrict__ A, int lda, int M,
+                                                     const __nv_bfloat16 *__restrict__ W, const float *__restrict__ bias,
+                                                     OutT *__restrict__ C, int ldc, int *err) {
+  static_assert(K % 16 == 0 && K >= 16 && K <= 256, "K: a multiple of 16 up to 256");
+  static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N: a multiple of 16 up to 256");
+  constexpr int NCOL = tmem_cols(N);
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sA = smem, *sW = smem + (size_t)TM * K * 2;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sW + (size_t)N * K * 2);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * TM;
+
+  if (warp == 0) {  // the accumulator's columns (one warp allocates and frees)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(NCOL));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  // stage the tile of A (rows past M as zeros) and W, 16 bytes (8 values of one core-matrix row) at a time
+  constexpr int KC = K / 8;
+  for (int c = tid; c < TM * KC; c += THREADS) {
+    const int r = c / KC, kc = c - r * KC;
+    int4 v = make_int4(0, 0, 0, 0);
+    if (m0 + r < M) v = *reinterpret_cast<const int4 *>(A + (size_t)(m0 + r) * lda + 8 * kc);
+    *reinterpret_cast<int4 *>(sA + tile_off(r, 8 * kc, K)) = v;
+  }
+  for (int c = tid; c < N * KC; c += THREADS) {
+    const int r = c / KC, kc = c - r * KC;
+    *reinterpret_cast<int4 *>(sW + tile_off(r, 8 * kc, K)) = *reinterpret_cast<const int4 *>(W + (size_t)r * K + 8 * kc);
+  }
+  // the tensor core reads shared memory through the async proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  if (tid == 0) {
+    const uint32_t a0 = smem_u32(sA), w0 = smem_u32(sW), id = idesc_bf16(TM, N);
+#pragma unroll
+    for (int ks = 0; ks < K / 16; ++ks) {
+      const uint64_t da = smem_desc(a0 + 256 * ks, 128, (K / 8) * 128);
+      const uint64_t dw = smem_desc(w0 + 256 * ks, 128, (K / 8) * 128);
+      const uint32_t acc = ks > 0 ? 1u : 0u;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "setp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+          "l"(da), "l"(dw), "r"(id), "r"(acc));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+  }
+  __syncwarp();
+  bool ok = mbar_wait(smem_u32(bar), 0, 1 << 22);
+  if (!ok) {
+    if (lane == 0) atomicExch(err, 1);
+    mbar_wait(smem_u32(bar), 0, 1 << 22);  // the MMAs in flight, once more, before the memory is freed
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  if (ok) {
+    const int row = m0 + 32 * warp + lane;
+    const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+          "[%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+            "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          float x = __uint_as_float(v[j]) + (bias ? bias[c0 + j] : 0.0f);
+          if (ACT == ACT_SILU) x = x / (1.0f + __expf(-x));
+          store_val<OutT>(C + (size_t)row * ldc + c0 + j, x);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL));
+}
+
+// Launch: ceil(M / 128) CTAs of 128 threads with the tile's shared memory.
+template <int K, int N, int ACT, typename OutT>
+cudaError_t gemm(const __nv_bfloat16 *A, int lda, int M, const __nv_bfloat16 *W, const float *bias, OutT *C, int ldc, int *err,
+                 cudaStream_t st) {
+  if (M <= 0) return cudaSuccess;
+  const size_t sm = smem_bytes(K, N);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<K, N, ACT, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_tc_gemm<K, N, ACT, OutT><<<(M + TM - 1) / TM, THREADS, sm, st>>>(A, lda, M, W, bias, C, ldc, err);
+  return cudaGetLastError();
+}
+
+}  // namespace pgmtc

@@ -490,12 +490,12 @@ class PGMForceField:
         t = _lib.PgmTuning()
         _lib.check(self._lib.pgm_tuning(self._h, C.byref(t)))
         return {"rowfield_lanes": t.rowfield_lanes, "forces_blocks_per_sm": t.forces_blocks_per_sm,
-                "rowfield_ms": list(t.rowfield_ms), "forces_ms": list(t.forces_ms), "tuned": bool(t.tuned),
-                "from_cache": bool(t.from_cache)}
+                "sweep_early": t.sweep_early, "rowfield_ms": list(t.rowfield_ms), "forces_ms": list(t.forces_ms),
+                "sweep_ms": list(t.sweep_ms), "tuned": bool(t.tuned), "from_cache": bool(t.from_cache)}
 
-    def set_tuning(self, rowfield_lanes: int = 0, forces_blocks_per_sm: int = 0) -> None:
-        """Fix the kernel variants (0 keeps one; both 0: autotune again at the next direct step)."""
-        _lib.check(self._lib.pgm_set_tuning(self._h, int(rowfield_lanes), int(forces_blocks_per_sm)))
+    def set_tuning(self, rowfield_lanes: int = 0, forces_blocks_per_sm: int = 0, sweep_early: int = -1) -> None:
+        """Fix the kernel variants (0 / -1 keeps one; all so: autotune again at the next direct step)."""
+        _lib.check(self._lib.pgm_set_tuning(self._h, int(rowfield_lanes), int(forces_blocks_per_sm), int(sweep_early)))
 
     def autotune(self) -> dict:
         """Time the kernel variants now on the last step's rows; returns tuning()."""

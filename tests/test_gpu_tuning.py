@@ -1,13 +1,15 @@
 """The autotuner's kernel variants (GPU): every choice of lanes per row in the CG matvec's row
-stream and of blocks per SM in the force pass computes the same step (FP64: only the order of the
-row additions changes), and the first direct step of a handle times them and keeps the fastest."""
+stream, of blocks per SM in the force pass and of the order of the CG sweep's concurrent parts (the
+row field of p, or of z combined with the previous direction's) computes the same step (FP64: only
+the order of additions changes), and the first direct step of a handle times them and keeps the
+fastest."""
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [(32, 3), (16, 2), (8, 4), (16, 3), (8, 2), (32, 4)]
+VARIANTS = [(32, 3, 0), (16, 2, 1), (8, 4, 0), (16, 3, 1), (8, 2, 1), (32, 4, 1)]
 
 
 def _box():
@@ -24,12 +26,12 @@ def test_every_variant_computes_the_same_step(prec):
 
     s, pos, H, st = _box()
     out = []
-    for lanes, blocks in VARIANTS:
+    for lanes, blocks, early in VARIANTS:
         ff = PGMForceField(s, H, MDSettings(precision=prec, **st))
-        ff.set_tuning(lanes, blocks)
+        ff.set_tuning(lanes, blocks, early)
         r = ff.compute(pos, H)
         t = ff.tuning()
-        assert (t["rowfield_lanes"], t["forces_blocks_per_sm"]) == (lanes, blocks) and not t["tuned"]
+        assert (t["rowfield_lanes"], t["forces_blocks_per_sm"], t["sweep_early"]) == (lanes, blocks, early) and not t["tuned"]
         out.append((float(r.energy["total"][0]), r.forces.cpu().numpy(), r.induction.mu.cpu().numpy(), int(r.iterations[0])))
     e0, f0, m0, i0 = out[0]
     tol = 1e-12 if prec == "double" else 1e-6
@@ -49,7 +51,8 @@ def test_first_direct_step_autotunes():
     ff.compute(pos, H)
     t = ff.tuning()
     assert t["tuned"] and t["rowfield_lanes"] in (32, 16, 8) and t["forces_blocks_per_sm"] in (2, 3, 4)
-    assert all(ms > 0 for ms in t["rowfield_ms"] + t["forces_ms"])
+    assert all(ms > 0 for ms in t["rowfield_ms"] + t["forces_ms"] + t["sweep_ms"])
+    assert t["sweep_early"] == (1 if t["sweep_ms"][1] < t["sweep_ms"][0] else 0)
     assert t["rowfield_ms"][[32, 16, 8].index(t["rowfield_lanes"])] == min(t["rowfield_ms"])
     # a second handle of the same shape takes the choice from the cache
     ff2 = PGMForceField(s, H, MDSettings(precision="mixed", **st))
