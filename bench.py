@@ -254,11 +254,12 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def train_guess(rank: int, torch) -> tuple:
-    """Plain-solver MD on the 4,096-water box writes (features, mu* - mu4 guess) pairs; the model
-    trains on the GPU.  Returns the model and what was trained."""
+def train_guess(rank: int, torch, kind: str) -> tuple:
+    """Plain-solver MD on the 4,096-water box writes (features, mu* - mu4 guess) pairs -- frame by
+    frame with the graph for the message-passing model; the model trains on the GPU.  Returns the
+    model and what was trained."""
     from pgm_jax_b200.forcefield import PGMForceField
-    from pgm_jax_b200.learned import GuessModel, collect
+    from pgm_jax_b200.learned import GuessModel, MPNNModel, collect, collect_frames
     from pgm_jax_b200.md import RigidMD
     from pgm_jax_b200.systems import water_box
 
@@ -268,12 +269,24 @@ def train_guess(rank: int, torch) -> tuple:
     ff = PGMForceField(s, H, settings(predictor="nn", grid=B["grid"]), device=torch.cuda.current_device())
     md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
     equilibrate(md, B["equil_steps"])
-    frames, iters = 64, 2000
-    train = collect(md, frames)
-    model = GuessModel(seed=0, device=torch.cuda.current_device())
-    model.train(train, iters=iters, batch=32768, lr=2e-3)
-    info = {"train_box": f"{B['atoms'] // 3} waters, {B['edge']} nm, PME {B['grid']}^3", "train_frames": frames,
-            "train_pairs": int(train["inv"].shape[0]), "adam_steps": iters, "seconds": time.perf_counter() - t0}
+    frames = 64
+    if kind == "mpnn":
+        iters = 2000
+        train = collect_frames(md, frames)
+        model = MPNNModel(seed=0, device=torch.cuda.current_device())
+        model.train(train, iters=iters, lr=2e-3)
+        pairs = sum(int(f["inv"].shape[0]) for f in train)
+        what = ("2-layer message-passing model on the 0.5 nm graph (64 hidden, 8 radial x 8 message features; "
+                "tcgen05 BF16 dense layers, FP32 accumulation), one frame per Adam step")
+    else:
+        iters = 2000
+        train = collect(md, frames)
+        model = GuessModel(seed=0, device=torch.cuda.current_device())
+        model.train(train, iters=iters, batch=32768, lr=2e-3)
+        pairs = int(train["inv"].shape[0])
+        what = "per-atom MLP 16 -> 64 -> 64 -> 32 on radial-basis features of the 0.5 nm graph (WMMA BF16)"
+    info = {"model": what, "train_box": f"{B['atoms'] // 3} waters, {B['edge']} nm, PME {B['grid']}^3",
+            "train_frames": frames, "train_pairs": pairs, "adam_steps": iters, "seconds": time.perf_counter() - t0}
     del md, ff, train
     return model, info
 
@@ -292,15 +305,21 @@ def run_engine(args) -> None:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    model, train_info = train_guess(rank, torch) if args.nn else (None, None)
+    model, train_info = train_guess(rank, torch, args.model) if args.nn else (None, None)
     s, pos, H = headline_box()
     ff = PGMForceField(s, H, settings(predictor="nn" if args.nn else "mu4"), device=local)
     md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
     lib = ff._lib
     equilibrate(md)
     if args.nn:  # held-out frames of this box (plain solver: the model is not installed yet)
-        held = collect(md, 6)
-        train_info["guess_rms_e_nm_held_out"] = guess_errors(model, held)
+        if args.model == "mpnn":
+            from pgm_jax_b200.learned import collect_frames, frame_errors
+
+            held = collect_frames(md, 6)
+            train_info["guess_rms_e_nm_held_out"] = frame_errors(model, held)
+        else:
+            held = collect(md, 6)
+            train_info["guess_rms_e_nm_held_out"] = guess_errors(model, held)
         train_info["start"] = "x0 = mu4 + the model's correction, fused start (one field sweep, as mu4)"
         del held
         model.install(ff)
@@ -746,6 +765,8 @@ def main() -> None:
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
+    ap.add_argument("--model", default="mpnn", choices=["mpnn", "mlp"],
+                    help="the learned guess: the 2-layer message-passing model or the per-atom MLP")
     ap.add_argument("--workload", default="water32768", choices=["water32768", "water4096", "batch", "pimd", "npt"],
                     help="water32768: the headline; water4096 the same line on the smaller box; the others print "
                     "their own line (one GPU)")

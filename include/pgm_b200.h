@@ -295,6 +295,38 @@ PgmStatus pgm_nn_adam(void *stream, float *weights, float *grad, float *m, float
                       float eps, int step);
 const char *pgm_nn_last_error(void);
 
+/* ------------------------------------------------------------------ message-passing guess
+ * No counterpart in the reference.  The 2-layer message-passing model of the learned guess on the
+ * graph of the row entries closer than graph_cutoff (pgm_mpnn.cu): h0 = SiLU(W0 inv + b0) (16 ->
+ * 64); per layer g = W_g h (64 = 8 radial x 8 features), messages a_i[f] = sum over the graph of
+ * sum_r phi_r(d_ij) g_j[8 r + f] (phi_r: 8 Gaussians times a cosine cutoff), h += W_b SiLU(W_a
+ * [h; a; 0] + b_a) + b_b (80 -> 64 -> 64); c = W_o h + b_o (16); mu = sigma sum_c c_c v_c over the
+ * 15 vector channels.  BF16 weights and activations, FP32 accumulation on the tcgen05 tensor
+ * cores.  Weights: pgm_mpnn_param_count() FP32 (W0, b0, then per layer Wg, Wa, ba, Wb, bb, then
+ * Wo, bo; matrices out x in, row-major). */
+int pgm_mpnn_param_count(void);
+/* Use it as the learned guess of predictor 5 (weights device FP32; NULL: no model). */
+PgmStatus pgm_set_mpnn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff);
+/* The graph of the last step with predictor 5: edges (N, emax) float4 (x_i - x_j, y, z, partner j
+ * as the bits of an int32) and counts (N) (a count above emax: the first emax kept). */
+PgmStatus pgm_nn_graph(PgmHandle *h, void *stream, void *edges, int *counts, int emax);
+/* Device workspace of pgm_mpnn_predict (train 0) or pgm_mpnn_loss_grad (train 1) for n atoms [bytes]. */
+long long pgm_mpnn_work_bytes(int n, int train);
+/* Prediction mu (n, 3) from invariants inv (n, 16), channels vec (n, 15, 3) and a symmetric graph
+ * (edges (n, emax), counts (n) as pgm_nn_graph writes). */
+PgmStatus pgm_mpnn_predict(void *stream, const float *weights, const float *inv, const float *vec, const void *edges,
+                           const int *ecount, int emax, int n, float sigma, float graph_cutoff, void *work, float *mu);
+/* Training: loss += scale sum |mu - target|^2 (double, device) and grad += dloss/dweights (FP32,
+ * device), the forward and activation gradients on the tensor cores, the weight gradients as FP32
+ * sums over the atoms. */
+PgmStatus pgm_mpnn_loss_grad(void *stream, const float *weights, const float *inv, const float *vec, const float *target,
+                             const void *edges, const int *ecount, int emax, int n, float sigma, float graph_cutoff,
+                             float scale, void *work, float *grad, double *loss);
+/* One Adam step (bias-corrected at `step` >= 1) on the message-passing model's weights; clears grad. */
+PgmStatus pgm_mpnn_adam(void *stream, float *weights, float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                        float eps, int step);
+const char *pgm_mpnn_last_error(void);
+
 /* ------------------------------------------------------------------ tcgen05 dense layers
  * No counterpart in the reference (its learned models run through XLA).  C = act(A W^T + bias) on
  * the 5th-generation tensor cores: A (M, lda) BF16 with the first K of every row used (lda a

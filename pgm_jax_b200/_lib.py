@@ -26,7 +26,8 @@ EXPORTS = (
     "pgm_graph_end", "pgm_graph_launch", "pgm_graph_destroy", "pgm_field_static", "pgm_static_last_error",
     "pgm_set_nn_model", "pgm_nn_features", "pgm_nn_param_count", "pgm_nn_predict", "pgm_nn_loss_grad", "pgm_nn_adam",
     "pgm_nn_last_error", "pgm_set_nn_fallback", "pgm_nn_fallback_stats", "pgm_tuning", "pgm_set_tuning", "pgm_autotune",
-    "pgm_iel_len", "pgm_tc_gemm", "pgm_tc_last_error",
+    "pgm_iel_len", "pgm_tc_gemm", "pgm_tc_last_error", "pgm_mpnn_param_count", "pgm_set_mpnn_model", "pgm_nn_graph",
+    "pgm_mpnn_work_bytes", "pgm_mpnn_predict", "pgm_mpnn_loss_grad", "pgm_mpnn_adam", "pgm_mpnn_last_error",
 )
 
 STATUS_ROW_OVERFLOW = 0x1
@@ -149,6 +150,16 @@ def load(path: str | None = None):
     lib.pgm_nn_loss_grad.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_float, vp, vp]
     lib.pgm_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
     lib.pgm_nn_last_error.restype = C.c_char_p
+    lib.pgm_set_mpnn_model.argtypes = [H, vp, C.c_float, C.c_float]
+    lib.pgm_nn_graph.argtypes = [H, vp, vp, vp, C.c_int]
+    lib.pgm_mpnn_work_bytes.argtypes = [C.c_int, C.c_int]
+    lib.pgm_mpnn_work_bytes.restype = C.c_longlong
+    lib.pgm_mpnn_predict.argtypes = [vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, vp, vp]
+    lib.pgm_mpnn_loss_grad.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, vp, vp, vp]
+    lib.pgm_mpnn_last_error.restype = C.c_char_p
+    lib.pgm_mpnn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
+    for n in ("pgm_set_mpnn_model", "pgm_nn_graph", "pgm_mpnn_predict", "pgm_mpnn_loss_grad", "pgm_mpnn_adam"):
+        getattr(lib, n).restype = C.c_int
     lib.pgm_tc_gemm.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp]
     lib.pgm_tc_gemm.restype = C.c_int
     lib.pgm_tc_last_error.restype = C.c_char_p
@@ -177,6 +188,11 @@ def load(path: str | None = None):
         getattr(lib, n).restype = C.c_int
     _lib = lib
     return lib
+
+
+def check_mpnn(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(f"pgm_b200 error {rc}: {load().pgm_mpnn_last_error().decode()}")
 
 
 def check(rc: int) -> None:

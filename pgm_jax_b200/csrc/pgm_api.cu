@@ -16,6 +16,13 @@
 #include "../../include/pgm_b200.h"
 #include "pgm_kernels.cuh"
 
+namespace pgmmp_engine {  // the message-passing model of the learned guess (pgm_mpnn.cu)
+size_t work_bytes(int n);
+cudaError_t set_weights(const float *flat, void *work, int n, cudaStream_t st);
+cudaError_t predict(const float *flat, void *work, const float *inv, const float *vec, const float4 *edges, const int *ecount,
+                    int emax, int n, float sigma, float rg, float *mu, cudaStream_t st, int prio);
+}  // namespace pgmmp_engine
+
 namespace {
 
 thread_local std::string g_err;
@@ -110,6 +117,8 @@ struct EngineBase {
   virtual int elec_capacity() const = 0;
   virtual int max_vdw_count() = 0;
   virtual void set_nn(const float *w, float sigma, float rg) = 0;
+  virtual void set_mpnn(const float *w, int nparam, float sigma, float rg) = 0;
+  virtual void nn_graph(cudaStream_t st, float4 *edges, int *counts, int emax) = 0;
   virtual void set_nn_fallback(double factor) = 0;
   virtual void set_tuning(int rowfield_lanes, int forces_blocks, int sweep_early) = 0;
   virtual void autotune(cudaStream_t st) = 0;
@@ -210,6 +219,9 @@ struct Engine : EngineBase {
   DBuf<double> mu_tmp, forces_tmp, energy_tmp;
   DBuf<float> nn_w, nn_inv, nn_vec, nn_mu, nn_chan;  // learned guess: model and per-atom features
   DBuf<__nv_bfloat16> nn_wb;  // the model's weight matrices in BF16 (converted when the model is set)
+  bool mp_on = false;         // the message-passing model instead of the per-atom MLP
+  DBuf<float> mp_w;           // its FP32 parameters
+  DBuf<unsigned char> mp_work;  // its activations and BF16 weights
   bool nn_on = false;
   // extended-Lagrangian dipoles: the recurrence's coefficients, delta, the reciprocal potential of
   // delta alone and its energy accumulators (shadow potential)
@@ -819,8 +831,34 @@ struct Engine : EngineBase {
     }
   }
 
+  // The message-passing model (pgm_mpnn.cu) on the same features and on the graph the row build
+  // writes; it replaces the MLP as the learned guess until set_nn or set_mpnn(null).
+  void set_mpnn(const float *w, int nparam, float sigma, float rg) override {
+    ++generation;
+    mp_on = w != nullptr;
+    nn_on = mp_on;
+    if (w) {
+      mp_w.alloc(nparam);
+      CK(cudaMemcpy(mp_w.p, w, sizeof(float) * nparam, cudaMemcpyDeviceToDevice));
+      mp_work.alloc(pgmmp_engine::work_bytes(nt));
+      CK(pgmmp_engine::set_weights(mp_w.p, mp_work.p, nt, 0));
+      CK(cudaDeviceSynchronize());
+    }
+    CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
+    nn_sigma = sigma;
+    nn_rg = rg;
+  }
+  // The graph of the last step (edges (x, y, z, partner) per atom, up to emax, and their counts).
+  void nn_graph(cudaStream_t st, float4 *edges, int *counts, int emax) override {
+    if (!nn_e4.p) throw CudaError{"the graph is kept only with predictor 5 (learned guess)"};
+    CK(cudaMemcpy2DAsync(edges, sizeof(float4) * emax, nn_e4.p, sizeof(float4) * NN_EMAX, sizeof(float4) * std::min(emax, NN_EMAX),
+                         nt, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(counts, nn_ne.p, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
+  }
+
   void set_nn(const float *w, float sigma, float rg) override {
     ++generation;  // a captured step depends on whether a model is set, and on sigma and rg
+    mp_on = false;
     nn_on = w != nullptr;
     if (w) {
       CK(cudaMemcpy(nn_w.p, w, sizeof(float) * pgmnn::NN_NPARAM, cudaMemcpyDeviceToDevice));
@@ -915,7 +953,9 @@ struct Engine : EngineBase {
       } else if (which == 11) {
         pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, nn_chan.p, nn_sigma, nn_rg, nn_inv.p, nn_vec.p, nullptr);
       } else {  // 12: the model
-        CK(pgmnn::nn_predict_launch(nn_w.p, nn_wb.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st));
+        CK(mp_on ? pgmmp_engine::predict(mp_w.p, mp_work.p, nn_inv.p, nn_vec.p, nn_e4.p, nn_ne.p, NN_EMAX, nt, nn_sigma, nn_rg,
+                                         nn_mu.p, st, 0)
+                 : pgmnn::nn_predict_launch(nn_w.p, nn_wb.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, st));
       }
     };
     long long l0 = launches;
@@ -1002,7 +1042,9 @@ struct Engine : EngineBase {
     CK(cudaEventRecord(ev_nn_fork, st));
     CK(cudaStreamWaitEvent(nn_st, ev_nn_fork, 0));
     nn_inputs(nn_st, a, hist, nn_bl.p, nn_valid.p, nn_bl.p, nn_inv.p, nn_vec.p, nn_valid.p);
-    cudaError_t e = pgmnn::nn_predict_launch(nn_w.p, nn_wb.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, nn_st, prio_hi);
+    cudaError_t e = mp_on ? pgmmp_engine::predict(mp_w.p, mp_work.p, nn_inv.p, nn_vec.p, nn_e4.p, nn_ne.p, NN_EMAX, nt, nn_sigma,
+                                                  nn_rg, nn_mu.p, nn_st, prio_hi)
+                          : pgmnn::nn_predict_launch(nn_w.p, nn_wb.p, nn_inv.p, nn_vec.p, nt, nn_mu.p, nn_st, prio_hi);
     if (e != cudaSuccess) throw CudaError{std::string("nn_predict: ") + cudaGetErrorString(e)};
     ++launches;
     CK(cudaEventRecord(ev_nn_join, nn_st));
@@ -1706,6 +1748,28 @@ PgmStatus pgm_nn_fallback_stats(PgmHandle *h, long long *fallbacks, double *ref_
   try {
     CK(cudaSetDevice(h->device));
     h->eng->nn_fallback_stats(fallbacks, ref_err);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_set_mpnn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff) {
+  if (!h || !(sigma > 0) || !(graph_cutoff > 0)) return fail(PGM_ERR_INVALID, "bad argument");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->set_mpnn(weights, pgm_mpnn_param_count(), sigma, graph_cutoff);
+    return PGM_OK;
+  } catch (CudaError &e) {
+    return fail(PGM_ERR_CUDA, e.msg);
+  }
+}
+
+PgmStatus pgm_nn_graph(PgmHandle *h, void *stream, void *edges, int *counts, int emax) {
+  if (!h || !edges || !counts || emax <= 0) return fail(PGM_ERR_INVALID, "bad argument");
+  try {
+    CK(cudaSetDevice(h->device));
+    h->eng->nn_graph((cudaStream_t)stream, (float4 *)edges, counts, emax);
     return PGM_OK;
   } catch (CudaError &e) {
     return fail(PGM_ERR_CUDA, e.msg);

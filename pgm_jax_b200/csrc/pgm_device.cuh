@@ -135,6 +135,15 @@ __device__ __forceinline__ void erf_kernels(T a, T r, T B[4]) {
     B[1] = c0 * a2x2 * acc1;
     B[2] = c0 * a2x2 * a2x2 * acc2;
     B[3] = c0 * a2x2 * a2x2 * a2x2 * acc3;
+  } else if (s > (sizeof(T) == 4 ? T(30) : T(56))) {
+    // far beyond the screening length: erf(a r) rounds to 1 and the terms of exp(-a^2 r^2), which
+    // enter B_n with at most (2 a^2 r^2)^3 (2 a r / sqrt(pi)) / 15, stay below 1e-8 (FP32) or
+    // 1e-18 (FP64) of it, so B_n are the bare Coulomb ones, (2n - 1)!! / r^(2n+1)
+    const T ir = T(1) / r, ir2 = ir * ir;
+    B[0] = ir;
+    B[1] = B[0] * ir2;
+    B[2] = T(3) * B[1] * ir2;
+    B[3] = T(5) * B[2] * ir2;
   } else {
     const T ir = T(1) / r, ir2 = ir * ir;
     const T c = c0 * t_exp(-s);

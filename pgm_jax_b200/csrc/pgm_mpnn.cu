@@ -1,12 +1,460 @@
-// pgm_mpnn.cu -- the learned guess's message-passing network: its dense layers on tcgen05 tensor
-// cores (pgm_tc.cuh) and the exported entry points.
+// pgm_mpnn.cu -- the learned guess's message-passing network on the short-range graph.
+//
+// Per atom i, from the features of the channel and feature passes (pgm_kernels.cuh: 16 rotation
+// invariants inv_i and 15 vector channels v_i,c), on the graph of the row entries closer than the
+// graph cutoff rg (the list the row build writes: per atom up to emax edges (x, y, z, partner)):
+//   h0 = SiLU(W0 inv + b0)                                       16 -> 64
+//   two message-passing layers:
+//     g = W_g h                                                  64 -> 64 = 8 radial x 8 features
+//     a_i[f] = sum_(i,j) sum_r phi_r(d_ij) g_j[8 r + f]          messages over the graph
+//     u = SiLU(W_a [h; a; 0] + b_a)                              80 -> 64
+//     h <- h + W_b u + b_b                                       64 -> 64 (residual)
+//   c = W_o h + b_o                                              64 -> 16 (15 used)
+//   prediction sigma sum_c c_c v_i,c                             (e nm; rotates with the system)
+// phi_r(d) = exp(-((d - r rg / 7) 7 / rg)^2) (cos(pi d / rg) + 1) / 2, r = 0..7.
+// The dense layers run on the tcgen05 tensor cores (pgm_tc.cuh: BF16 operands, FP32 accumulation,
+// bias / SiLU / residual in the epilogue); the message sums and the readout on the CUDA cores.
+// Training: the same forward with the pre-activations kept, then the backward pass: activation
+// gradients through the transposed weights on the tensor cores (BF16 operands), the transposed
+// message sum (the graph is symmetric: d_ij = d_ji), and the weight gradients as FP32 sums over
+// the atoms of the batch on the CUDA cores.  The NumPy restatement (oracle/nn_oracle.py mpnn_*)
+// rounds to BF16 at the same points.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <string>
 
 #include "../../include/pgm_b200.h"
 #include "pgm_tc.cuh"
+
+namespace pgmmp {
+
+constexpr int IN = 16, HID = 64, R = 8, F = 8, ZW = 80, COEF = 16, CH = 15;
+static_assert(R * F == HID && HID + F + 8 == ZW, "g holds R x F message features; Z = [h; a; 8 zeros]");
+// flat FP32 parameters: W0 (64 x 16), b0, [Wg (64 x 64), Wa (64 x 80), ba, Wb (64 x 64), bb] x 2, Wo (16 x 64), bo
+constexpr int L_SIZE = HID * HID + HID * ZW + HID + HID * HID + HID;
+constexpr int NPARAM = HID * IN + HID + 2 * L_SIZE + COEF * HID + COEF;
+// BF16 copies: forward (out x in) and transposed (in x out) of W0? (forward only), Wg, Wa, Wb, Wo
+constexpr int WB_FWD = HID * IN + 2 * (HID * HID + HID * ZW + HID * HID) + COEF * HID;
+
+struct View {
+  const float *W0, *b0, *Wg[2], *Wa[2], *ba[2], *Wb[2], *bb[2], *Wo, *bo;
+};
+__host__ __device__ inline View view(const float *p) {
+  View v;
+  v.W0 = p; v.b0 = p + HID * IN;
+  const float *q = v.b0 + HID;
+  for (int l = 0; l < 2; ++l) {
+    v.Wg[l] = q; v.Wa[l] = q + HID * HID; v.ba[l] = v.Wa[l] + HID * ZW; v.Wb[l] = v.ba[l] + HID; v.bb[l] = v.Wb[l] + HID * HID;
+    q = v.bb[l] + HID;
+  }
+  v.Wo = q; v.bo = q + COEF * HID;
+  return v;
+}
+// the gradient has the same layout
+struct GView {
+  float *W0, *b0, *Wg[2], *Wa[2], *ba[2], *Wb[2], *bb[2], *Wo, *bo;
+};
+inline GView gview(float *p) {
+  View v = view(p);
+  GView g;
+  g.W0 = const_cast<float *>(v.W0); g.b0 = const_cast<float *>(v.b0);
+  for (int l = 0; l < 2; ++l) {
+    g.Wg[l] = const_cast<float *>(v.Wg[l]); g.Wa[l] = const_cast<float *>(v.Wa[l]); g.ba[l] = const_cast<float *>(v.ba[l]);
+    g.Wb[l] = const_cast<float *>(v.Wb[l]); g.bb[l] = const_cast<float *>(v.bb[l]);
+  }
+  g.Wo = const_cast<float *>(v.Wo); g.bo = const_cast<float *>(v.bo);
+  return g;
+}
+
+// BF16 weights: forward copies (out x in) and, for the backward pass, transposed copies (in x out).
+struct WB {
+  __nv_bfloat16 *W0, *Wg[2], *Wa[2], *Wb[2], *Wo;        // forward
+  __nv_bfloat16 *WgT[2], *WaT[2], *WbT[2], *WoT;          // transposed
+};
+constexpr int WB_ELEMS = WB_FWD + 2 * (HID * HID + ZW * HID + HID * HID) + HID * COEF;
+inline WB wb_view(__nv_bfloat16 *p) {
+  WB w;
+  w.W0 = p; p += HID * IN;
+  for (int l = 0; l < 2; ++l) { w.Wg[l] = p; p += HID * HID; w.Wa[l] = p; p += HID * ZW; w.Wb[l] = p; p += HID * HID; }
+  w.Wo = p; p += COEF * HID;
+  for (int l = 0; l < 2; ++l) { w.WgT[l] = p; p += HID * HID; w.WaT[l] = p; p += ZW * HID; w.WbT[l] = p; p += HID * HID; }
+  w.WoT = p;
+  return w;
+}
+
+// (out x in) FP32 -> BF16 as is and transposed
+__global__ void k_convert(const float *W, int out, int in, __nv_bfloat16 *Wf, __nv_bfloat16 *Wt) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= out * in) return;
+  int o = t / in, i = t - o * in;
+  __nv_bfloat16 b = __float2bfloat16(W[t]);
+  if (Wf) Wf[t] = b;
+  if (Wt) Wt[(size_t)i * out + o] = b;
+}
+
+// Radial functions of an edge of length d (float, as the NumPy restatement).
+__device__ __forceinline__ float radial(int r, float d, float rg) {
+  const float mu = r * (rg / (R - 1)), gam = ((R - 1) / rg) * ((R - 1) / rg);
+  const float fc = 0.5f * (cosf(3.14159265358979f * d / rg) + 1.0f);
+  const float x = d - mu;
+  return expf(-gam * x * x) * fc;
+}
+
+// Messages, one warp per atom: lane = 4 r + q holds features 2 q, 2 q + 1 of radial r; a_i[f] =
+// sum over the atom's edges of phi_r(d) g_j[8 r + f], summed over r by a butterfly, written as
+// BF16 into columns 64..71 of the atom's row of Z (ldz).  Edges past emax are not read.
+__global__ void k_aggregate(const __nv_bfloat16 *__restrict__ G, int ldg, const float4 *__restrict__ edges,
+                            const int *__restrict__ ecount, int emax, int n, float rg, __nv_bfloat16 *__restrict__ Z, int ldz) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp, r = lane >> 2, q = lane & 3;
+  const int ne = min(ecount[i], emax);
+  const float4 *e = edges + (size_t)i * emax;
+  float a0 = 0.f, a1 = 0.f;
+  for (int t = 0; t < ne; ++t) {
+    const float4 ed = e[t];
+    const int j = __float_as_int(ed.w);
+    const float d = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
+    const float ph = radial(r, d, rg);
+    const __nv_bfloat162 g2 = *reinterpret_cast<const __nv_bfloat162 *>(G + (size_t)j * ldg + 8 * r + 2 * q);
+    a0 += ph * __bfloat162float(g2.x);
+    a1 += ph * __bfloat162float(g2.y);
+  }
+#pragma unroll
+  for (int o = 4; o < 32; o <<= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+  }
+  if (lane < 4) {
+    __nv_bfloat162 v;
+    v.x = __float2bfloat16(a0);
+    v.y = __float2bfloat16(a1);
+    *reinterpret_cast<__nv_bfloat162 *>(Z + (size_t)i * ldz + HID + 2 * q) = v;
+  }
+}
+
+// The transposed message sum, one warp per atom j: dg_j[8 r + f] = sum over j's edges (j, i) of
+// phi_r(d) da_i[f] (the graph is symmetric), as FP32 (for the weight gradient) and BF16.
+__global__ void k_aggregate_t(const float *__restrict__ dZ, int ldd, const float4 *__restrict__ edges,
+                              const int *__restrict__ ecount, int emax, int n, float rg, float *__restrict__ dG,
+                              __nv_bfloat16 *__restrict__ dGb) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int j = warp, r = lane >> 2, q = lane & 3;
+  const int ne = min(ecount[j], emax);
+  const float4 *e = edges + (size_t)j * emax;
+  float g0 = 0.f, g1 = 0.f;
+  for (int t = 0; t < ne; ++t) {
+    const float4 ed = e[t];
+    const int i = __float_as_int(ed.w);
+    const float d = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
+    const float ph = radial(r, d, rg);
+    const float2 da = *reinterpret_cast<const float2 *>(dZ + (size_t)i * ldd + HID + 2 * q);
+    g0 += ph * da.x;
+    g1 += ph * da.y;
+  }
+  const size_t o = (size_t)j * HID + 8 * r + 2 * q;
+  dG[o] = g0; dG[o + 1] = g1;
+  dGb[o] = __float2bfloat16(g0); dGb[o + 1] = __float2bfloat16(g1);
+}
+
+// Prediction mu_i = sigma sum_c C[i, c] v[i, c] (FP32).
+__global__ void k_readout(const float *__restrict__ C, const float *__restrict__ vec, int n, float sigma, float *__restrict__ mu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float m[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int c = 0; c < CH; ++c) {
+    const float w = C[(size_t)i * COEF + c];
+    for (int k = 0; k < 3; ++k) m[k] += w * vec[((size_t)i * CH + c) * 3 + k];
+  }
+  for (int k = 0; k < 3; ++k) mu[3 * (size_t)i + k] = sigma * m[k];
+}
+
+// Loss scale sum |mu - t|^2 (FP64 sum) and dC[i, c] = sigma (dL/dmu_i . v_ic) (0 for c = 15), as FP32
+// and BF16.
+__global__ void k_loss(const float *__restrict__ C, const float *__restrict__ vec, const float *__restrict__ target, int n,
+                       float sigma, float scale, double *loss, float *__restrict__ dC, __nv_bfloat16 *__restrict__ dCb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double l = 0.0;
+  if (i < n) {
+    float m[3] = {0.f, 0.f, 0.f};
+    for (int c = 0; c < CH; ++c) {
+      const float w = C[(size_t)i * COEF + c];
+      for (int k = 0; k < 3; ++k) m[k] += w * vec[((size_t)i * CH + c) * 3 + k];
+    }
+    float dm[3];
+    for (int k = 0; k < 3; ++k) {
+      const float e = sigma * m[k] - target[3 * (size_t)i + k];
+      l += (double)scale * e * e;
+      dm[k] = 2.0f * scale * e;
+    }
+    for (int c = 0; c < COEF; ++c) {
+      float v = 0.f;
+      if (c < CH)
+        for (int k = 0; k < 3; ++k) v += dm[k] * vec[((size_t)i * CH + c) * 3 + k];
+      v *= sigma;
+      dC[(size_t)i * COEF + c] = v;
+      dCb[(size_t)i * COEF + c] = __float2bfloat16(v);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+  if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss, l);
+}
+
+// u = BF16(SiLU(z)) into rows of ldu (training keeps z).
+__global__ void k_silu_round(const float *__restrict__ z, int n, int w, __nv_bfloat16 *__restrict__ u, int ldu) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * w) return;
+  const int i = t / w, c = t - i * w;
+  const float x = z[t];
+  u[(size_t)i * ldu + c] = __float2bfloat16(x / (1.0f + expf(-x)));
+}
+
+// dz = d * SiLU'(z) as FP32 and BF16.
+__global__ void k_dsilu(const float *__restrict__ d, const float *__restrict__ z, int total, float *__restrict__ dz,
+                        __nv_bfloat16 *__restrict__ dzb) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const float x = z[t], s = 1.0f / (1.0f + expf(-x));
+  const float v = d[t] * s * (1.0f + x * (1.0f - s));
+  dz[t] = v;
+  if (dzb) dzb[t] = __float2bfloat16(v);
+}
+
+// dh (n x 64) += dZ[:, :64] (ld 80) + dGh (n x 64); also the BF16 copy of the new dh.
+__global__ void k_add_dh(float *__restrict__ dh, const float *__restrict__ dZ, const float *__restrict__ dGh, int n,
+                         __nv_bfloat16 *__restrict__ dhb) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * HID) return;
+  const int i = t / HID, c = t - i * HID;
+  const float v = dh[t] + dZ[(size_t)i * ZW + c] + dGh[t];
+  dh[t] = v;
+  dhb[t] = __float2bfloat16(v);
+}
+
+__global__ void k_to_bf16(const float *__restrict__ x, int total, __nv_bfloat16 *__restrict__ y) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < total) y[t] = __float2bfloat16(x[t]);
+}
+
+// Weight gradients on the CUDA cores: dW[o, k] += sum_m dY[m, o] X[m, k] (X BF16, the first K of
+// rows of ldx), db[o] += sum_m dY[m, o]; rows in chunks of 32 staged in shared memory, FP32 sums
+// per thread, one atomic add per output and block.
+template <int NO, int KI>
+__global__ void __launch_bounds__(256) k_wgrad(const float *__restrict__ dY, int ldy, const __nv_bfloat16 *__restrict__ X, int ldx,
+                                               int M, float *__restrict__ dW, float *__restrict__ db) {
+  constexpr int CH_ROWS = 32;
+  constexpr int PER = (NO * KI + 255) / 256;
+  __shared__ float sY[CH_ROWS][NO];
+  __shared__ float sX[CH_ROWS][KI];
+  float acc[PER], accb = 0.f;
+#pragma unroll
+  for (int p = 0; p < PER; ++p) acc[p] = 0.f;
+  for (int m0 = blockIdx.x * CH_ROWS; m0 < M; m0 += gridDim.x * CH_ROWS) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < CH_ROWS * NO; t += 256) {
+      const int r = t / NO, o = t - r * NO;
+      sY[r][o] = m0 + r < M ? dY[(size_t)(m0 + r) * ldy + o] : 0.f;
+    }
+    for (int t = threadIdx.x; t < CH_ROWS * KI; t += 256) {
+      const int r = t / KI, k = t - r * KI;
+      sX[r][k] = m0 + r < M ? __bfloat162float(X[(size_t)(m0 + r) * ldx + k]) : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int e = threadIdx.x + 256 * p;
+      if (e < NO * KI) {
+        const int o = e / KI, k = e - o * KI;
+        float s = 0.f;
+#pragma unroll 8
+        for (int r = 0; r < CH_ROWS; ++r) s += sY[r][o] * sX[r][k];
+        acc[p] += s;
+      }
+    }
+    if (db && threadIdx.x < NO)
+      for (int r = 0; r < CH_ROWS; ++r) accb += sY[r][threadIdx.x];
+  }
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int e = threadIdx.x + 256 * p;
+    if (e < NO * KI && acc[p] != 0.f) atomicAdd(&dW[e], acc[p]);
+  }
+  if (db && threadIdx.x < NO && accb != 0.f) atomicAdd(&db[threadIdx.x], accb);
+}
+
+// Workspace of the forward pass (inference) and of training, in bytes, for n atoms.
+struct Work {
+  __nv_bfloat16 *X0, *HZ[3], *Gb, *U;  // inputs; h with its message columns (n x 80) per layer; g; u
+  float *Cc;                           // coefficients (n x 16)
+  // training only
+  float *z0, *zu[2];                   // pre-activations
+  __nv_bfloat16 *Gk[2], *Uk[2];        // g and u of both layers
+  float *dC, *dh, *dU, *dzu, *dZ, *dG, *dGh;
+  __nv_bfloat16 *dCb, *dhb, *dzub, *dGb;
+  __nv_bfloat16 *wb;                   // BF16 weights
+  int *err;
+};
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+inline size_t work_bytes(int n, bool train) {
+  size_t b = 0;
+  auto add = [&](size_t bytes) { b += align256(bytes); };
+  add((size_t)n * IN * 2);
+  for (int k = 0; k < 3; ++k) add((size_t)n * ZW * 2);
+  add((size_t)n * HID * 2); add((size_t)n * HID * 2);
+  add((size_t)n * COEF * 4);
+  if (train) {
+    add((size_t)n * HID * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4);
+    for (int k = 0; k < 4; ++k) add((size_t)n * HID * 2);
+    add((size_t)n * COEF * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4);
+    add((size_t)n * ZW * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4);
+    add((size_t)n * COEF * 2); add((size_t)n * HID * 2); add((size_t)n * HID * 2); add((size_t)n * HID * 2);
+  }
+  add((size_t)WB_ELEMS * 2);
+  add(256);
+  return b;
+}
+inline Work work_view(void *base, int n, bool train) {
+  Work w = {};
+  uint8_t *p = static_cast<uint8_t *>(base);
+  auto take = [&](size_t bytes) { void *q = p; p += align256(bytes); return q; };
+  w.X0 = (__nv_bfloat16 *)take((size_t)n * IN * 2);
+  for (int k = 0; k < 3; ++k) w.HZ[k] = (__nv_bfloat16 *)take((size_t)n * ZW * 2);
+  w.Gb = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.U = (__nv_bfloat16 *)take((size_t)n * HID * 2);
+  w.Cc = (float *)take((size_t)n * COEF * 4);
+  if (train) {
+    w.z0 = (float *)take((size_t)n * HID * 4); w.zu[0] = (float *)take((size_t)n * HID * 4); w.zu[1] = (float *)take((size_t)n * HID * 4);
+    w.Gk[0] = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.Gk[1] = (__nv_bfloat16 *)take((size_t)n * HID * 2);
+    w.Uk[0] = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.Uk[1] = (__nv_bfloat16 *)take((size_t)n * HID * 2);
+    w.dC = (float *)take((size_t)n * COEF * 4); w.dh = (float *)take((size_t)n * HID * 4); w.dU = (float *)take((size_t)n * HID * 4);
+    w.dzu = (float *)take((size_t)n * HID * 4); w.dZ = (float *)take((size_t)n * ZW * 4); w.dG = (float *)take((size_t)n * HID * 4);
+    w.dGh = (float *)take((size_t)n * HID * 4);
+    w.dCb = (__nv_bfloat16 *)take((size_t)n * COEF * 2); w.dhb = (__nv_bfloat16 *)take((size_t)n * HID * 2);
+    w.dzub = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.dGb = (__nv_bfloat16 *)take((size_t)n * HID * 2);
+  }
+  w.wb = (__nv_bfloat16 *)take((size_t)WB_ELEMS * 2);
+  w.err = (int *)take(256);
+  return w;
+}
+
+#define MPCK(x)                      \
+  do {                               \
+    cudaError_t e_ = (x);            \
+    if (e_ != cudaSuccess) return e_; \
+  } while (0)
+
+inline int blocks(long long n, int b = 256) { return (int)((n + b - 1) / b); }
+
+cudaError_t convert_weights(const float *flat, Work &w, cudaStream_t st) {
+  View v = view(flat);
+  WB b = wb_view(w.wb);
+  k_convert<<<blocks(HID * IN), 256, 0, st>>>(v.W0, HID, IN, b.W0, nullptr);
+  for (int l = 0; l < 2; ++l) {
+    k_convert<<<blocks(HID * HID), 256, 0, st>>>(v.Wg[l], HID, HID, b.Wg[l], b.WgT[l]);
+    k_convert<<<blocks(HID * ZW), 256, 0, st>>>(v.Wa[l], HID, ZW, b.Wa[l], b.WaT[l]);
+    k_convert<<<blocks(HID * HID), 256, 0, st>>>(v.Wb[l], HID, HID, b.Wb[l], b.WbT[l]);
+  }
+  k_convert<<<blocks(COEF * HID), 256, 0, st>>>(v.Wo, COEF, HID, b.Wo, b.WoT);
+  return cudaGetLastError();
+}
+
+// The forward pass; with train, the pre-activations and every layer's g and u are kept.
+cudaError_t forward(const float *flat, Work &w, const float *inv, const float4 *edges, const int *ecount, int emax, int n,
+                    float rg, bool train, cudaStream_t st, int prio) {
+  using namespace pgmtc;
+  View v = view(flat);
+  WB b = wb_view(w.wb);
+  k_to_bf16<<<blocks((long long)n * IN), 256, 0, st>>>(inv, n * IN, w.X0);
+  if (train) {
+    MPCK((gemm<IN, HID, ACT_NONE, float>(w.X0, IN, n, b.W0, v.b0, w.z0, HID, w.err, st)));
+    k_silu_round<<<blocks((long long)n * HID), 256, 0, st>>>(w.z0, n, HID, w.HZ[0], ZW);
+  } else {
+    MPCK((gemm<IN, HID, ACT_SILU, __nv_bfloat16>(w.X0, IN, n, b.W0, v.b0, w.HZ[0], ZW, w.err, st, nullptr, 0, prio)));
+  }
+  for (int l = 0; l < 2; ++l) {
+    __nv_bfloat16 *H = w.HZ[l], *Hn = w.HZ[l + 1];
+    __nv_bfloat16 *G = train ? w.Gk[l] : w.Gb, *U = train ? w.Uk[l] : w.U;
+    MPCK((gemm<HID, HID, ACT_NONE, __nv_bfloat16>(H, ZW, n, b.Wg[l], nullptr, G, HID, w.err, st, nullptr, 0, prio)));
+    k_aggregate<<<blocks((long long)n * 32), 256, 0, st>>>(G, HID, edges, ecount, emax, n, rg, H, ZW);
+    if (train) {
+      MPCK((gemm<ZW, HID, ACT_NONE, float>(H, ZW, n, b.Wa[l], v.ba[l], w.zu[l], HID, w.err, st)));
+      k_silu_round<<<blocks((long long)n * HID), 256, 0, st>>>(w.zu[l], n, HID, U, HID);
+    } else {
+      MPCK((gemm<ZW, HID, ACT_SILU, __nv_bfloat16>(H, ZW, n, b.Wa[l], v.ba[l], U, HID, w.err, st, nullptr, 0, prio)));
+    }
+    MPCK((gemm<HID, HID, ACT_NONE, __nv_bfloat16>(U, HID, n, b.Wb[l], v.bb[l], Hn, ZW, w.err, st, H, ZW, prio)));
+  }
+  MPCK((gemm<HID, COEF, ACT_NONE, float>(w.HZ[2], ZW, n, b.Wo, v.bo, w.Cc, COEF, w.err, st, nullptr, 0, prio)));
+  return cudaGetLastError();
+}
+
+// Loss and gradient (added into grad) of a batch whose forward pass ran with train.
+cudaError_t backward(const float *flat, Work &w, const float *inv, const float *vec, const float *target, const float4 *edges,
+                     const int *ecount, int emax, int n, float sigma, float rg, float scale, float *grad, double *loss,
+                     cudaStream_t st) {
+  using namespace pgmtc;
+  (void)inv;
+  GView g = gview(grad);
+  WB b = wb_view(w.wb);
+  const int wgb = std::min(blocks(n, 32), 1184);
+  k_loss<<<blocks(n), 256, 0, st>>>(w.Cc, vec, target, n, sigma, scale, loss, w.dC, w.dCb);
+  k_wgrad<COEF, HID><<<wgb, 256, 0, st>>>(w.dC, COEF, w.HZ[2], ZW, n, g.Wo, g.bo);
+  MPCK((gemm<COEF, HID, ACT_NONE, float>(w.dCb, COEF, n, b.WoT, nullptr, w.dh, HID, w.err, st)));
+  k_to_bf16<<<blocks((long long)n * HID), 256, 0, st>>>(w.dh, n * HID, w.dhb);
+  for (int l = 1; l >= 0; --l) {
+    // h_{l+1} = h_l + W_b u + b_b
+    k_wgrad<HID, HID><<<wgb, 256, 0, st>>>(w.dh, HID, w.Uk[l], HID, n, g.Wb[l], g.bb[l]);
+    MPCK((gemm<HID, HID, ACT_NONE, float>(w.dhb, HID, n, b.WbT[l], nullptr, w.dU, HID, w.err, st)));
+    k_dsilu<<<blocks((long long)n * HID), 256, 0, st>>>(w.dU, w.zu[l], n * HID, w.dzu, w.dzub);
+    k_wgrad<HID, ZW><<<wgb, 256, 0, st>>>(w.dzu, HID, w.HZ[l], ZW, n, g.Wa[l], g.ba[l]);
+    MPCK((gemm<HID, ZW, ACT_NONE, float>(w.dzub, HID, n, b.WaT[l], nullptr, w.dZ, ZW, w.err, st)));
+    k_aggregate_t<<<blocks((long long)n * 32), 256, 0, st>>>(w.dZ, ZW, edges, ecount, emax, n, rg, w.dG, w.dGb);
+    k_wgrad<HID, HID><<<wgb, 256, 0, st>>>(w.dG, HID, w.HZ[l], ZW, n, g.Wg[l], nullptr);
+    MPCK((gemm<HID, HID, ACT_NONE, float>(w.dGb, HID, n, b.WgT[l], nullptr, w.dGh, HID, w.err, st)));
+    k_add_dh<<<blocks((long long)n * HID), 256, 0, st>>>(w.dh, w.dZ, w.dGh, n, w.dhb);
+  }
+  k_dsilu<<<blocks((long long)n * HID), 256, 0, st>>>(w.dh, w.z0, n * HID, w.dzu, nullptr);
+  k_wgrad<HID, IN><<<wgb, 256, 0, st>>>(w.dzu, HID, w.X0, IN, n, g.W0, g.b0);
+  return cudaGetLastError();
+}
+
+__global__ void k_adam(float *w, float *g, float *m, float *v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float gt = g[t];
+  const float mt = b1 * m[t] + (1.f - b1) * gt, vt = b2 * v[t] + (1.f - b2) * gt * gt;
+  m[t] = mt;
+  v[t] = vt;
+  w[t] -= lr * (mt / c1) / (sqrtf(vt / c2) + eps);
+  g[t] = 0.f;
+}
+
+thread_local std::string g_mp_err;
+
+}  // namespace pgmmp
+
+namespace pgmmp_engine {
+// For the engine (pgm_api.cu): predict mu on its stream from its features and graph.
+size_t work_bytes(int n) { return pgmmp::work_bytes(n, false); }
+cudaError_t set_weights(const float *flat, void *work, int n, cudaStream_t st) {
+  pgmmp::Work w = pgmmp::work_view(work, n, false);
+  cudaError_t e = cudaMemsetAsync(work, 0, pgmmp::work_bytes(n, false), st);  // the zero columns 72..79 of Z
+  if (e != cudaSuccess) return e;
+  return pgmmp::convert_weights(flat, w, st);
+}
+cudaError_t predict(const float *flat, void *work, const float *inv, const float *vec, const float4 *edges, const int *ecount,
+                    int emax, int n, float sigma, float rg, float *mu, cudaStream_t st, int prio) {
+  pgmmp::Work w = pgmmp::work_view(work, n, false);
+  cudaError_t e = pgmmp::forward(flat, w, inv, edges, ecount, emax, n, rg, false, st, prio);
+  if (e != cudaSuccess) return e;
+  pgmmp::k_readout<<<pgmmp::blocks(n), 256, 0, st>>>(w.Cc, vec, n, sigma, mu);
+  return cudaGetLastError();
+}
+}  // namespace pgmmp_engine
 
 namespace {
 thread_local std::string g_tc_err;
@@ -51,6 +499,63 @@ PgmStatus pgm_tc_gemm(void *stream, int K, int N, int act, int out_f32, const vo
     g_tc_err = std::string("pgm_tc_gemm: ") + cudaGetErrorString(e);
     return PGM_ERR_CUDA;
   }
+  return PGM_OK;
+}
+
+int pgm_mpnn_param_count(void) { return pgmmp::NPARAM; }
+long long pgm_mpnn_work_bytes(int n, int train) { return (long long)pgmmp::work_bytes(n, train != 0); }
+const char *pgm_mpnn_last_error(void) { return pgmmp::g_mp_err.c_str(); }
+
+static PgmStatus mp_fail(PgmStatus s, const std::string &m) {
+  pgmmp::g_mp_err = m;
+  return s;
+}
+
+PgmStatus pgm_mpnn_predict(void *stream, const float *weights, const float *inv, const float *vec, const void *edges,
+                           const int *ecount, int emax, int n, float sigma, float graph_cutoff, void *work, float *mu) {
+  if (!weights || !inv || !vec || !edges || !ecount || !work || !mu || n <= 0 || emax <= 0 || !(graph_cutoff > 0))
+    return mp_fail(PGM_ERR_INVALID, "pgm_mpnn_predict: bad argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  pgmmp::Work w = pgmmp::work_view(work, n, false);
+  cudaError_t e = cudaMemsetAsync(work, 0, pgmmp::work_bytes(n, false), st);
+  if (e == cudaSuccess) e = pgmmp::convert_weights(weights, w, st);
+  if (e == cudaSuccess)
+    e = pgmmp::forward(weights, w, inv, (const float4 *)edges, ecount, emax, n, graph_cutoff, false, st, 0);
+  if (e == cudaSuccess) {
+    pgmmp::k_readout<<<pgmmp::blocks(n), 256, 0, st>>>(w.Cc, vec, n, sigma, mu);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) return mp_fail(PGM_ERR_CUDA, std::string("pgm_mpnn_predict: ") + cudaGetErrorString(e));
+  return PGM_OK;
+}
+
+PgmStatus pgm_mpnn_loss_grad(void *stream, const float *weights, const float *inv, const float *vec, const float *target,
+                             const void *edges, const int *ecount, int emax, int n, float sigma, float graph_cutoff,
+                             float scale, void *work, float *grad, double *loss) {
+  if (!weights || !inv || !vec || !target || !edges || !ecount || !work || !grad || !loss || n <= 0 || emax <= 0 ||
+      !(graph_cutoff > 0))
+    return mp_fail(PGM_ERR_INVALID, "pgm_mpnn_loss_grad: bad argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  pgmmp::Work w = pgmmp::work_view(work, n, true);
+  cudaError_t e = cudaMemsetAsync(work, 0, pgmmp::work_bytes(n, true), st);
+  if (e == cudaSuccess) e = pgmmp::convert_weights(weights, w, st);
+  if (e == cudaSuccess)
+    e = pgmmp::forward(weights, w, inv, (const float4 *)edges, ecount, emax, n, graph_cutoff, true, st, 0);
+  if (e == cudaSuccess)
+    e = pgmmp::backward(weights, w, inv, vec, target, (const float4 *)edges, ecount, emax, n, sigma, graph_cutoff, scale, grad,
+                        loss, st);
+  if (e != cudaSuccess) return mp_fail(PGM_ERR_CUDA, std::string("pgm_mpnn_loss_grad: ") + cudaGetErrorString(e));
+  return PGM_OK;
+}
+
+PgmStatus pgm_mpnn_adam(void *stream, float *weights, float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                        float eps, int step) {
+  if (!weights || !grad || !m || !v || step < 1) return mp_fail(PGM_ERR_INVALID, "pgm_mpnn_adam: bad argument");
+  const int n = pgmmp::NPARAM;
+  const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+  pgmmp::k_adam<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(weights, grad, m, v, n, lr, beta1, beta2, eps, c1, c2);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return mp_fail(PGM_ERR_CUDA, std::string("pgm_mpnn_adam: ") + cudaGetErrorString(e));
   return PGM_OK;
 }
 

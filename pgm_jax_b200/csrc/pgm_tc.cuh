@@ -76,13 +76,15 @@ __device__ __forceinline__ void store_val<float>(float *p, float v) { *p = v; }
 template <>
 __device__ __forceinline__ void store_val<__nv_bfloat16>(__nv_bfloat16 *p, float v) { *p = __float2bfloat16(v); }
 
-// C = act(A W^T + bias) for one 128-row tile per CTA.  A: M rows of lda BF16 (the first K used),
-// 16-byte aligned rows; W: N x K BF16 (K contiguous); bias: N floats or null; C: M rows of ldc.
+// C = act(A W^T + bias) (+ Res) for one 128-row tile per CTA.  A: M rows of lda BF16 (the first K
+// used), 16-byte aligned rows; W: N x K BF16 (K contiguous); bias: N floats or null; Res: null or
+// M rows of ldr BF16 added after the activation (a residual connection); C: M rows of ldc.
 // K: a multiple of 16 up to 256; N: a multiple of 16 up to 256.
 template <int K, int N, int ACT, typename OutT>
 __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__restrict__ A, int lda, int M,
                                                      const __nv_bfloat16 *__restrict__ W, const float *__restrict__ bias,
-                                                     OutT *__restrict__ C, int ldc, int *err) {
+                                                     OutT *__restrict__ C, int ldc, int *err,
+                                                     const __nv_bfloat16 *__restrict__ Res = nullptr, int ldr = 0) {
   static_assert(K % 16 == 0 && K >= 16 && K <= 256, "K: a multiple of 16 up to 256");
   static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N: a multiple of 16 up to 256");
   constexpr int NCOL = tmem_cols(N);
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__rest
         for (int j = 0; j < 16; ++j) {
           float x = __uint_as_float(v[j]) + (bias ? bias[c0 + j] : 0.0f);
           if (ACT == ACT_SILU) x = x / (1.0f + __expf(-x));
+          if (Res) x += __bfloat162float(Res[(size_t)row * ldr + c0 + j]);
           store_val<OutT>(C + (size_t)row * ldc + c0 + j, x);
         }
       }
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__rest
 // Launch: ceil(M / 128) CTAs of 128 threads with the tile's shared memory.
 template <int K, int N, int ACT, typename OutT>
 cudaError_t gemm(const __nv_bfloat16 *A, int lda, int M, const __nv_bfloat16 *W, const float *bias, OutT *C, int ldc, int *err,
-                 cudaStream_t st) {
+                 cudaStream_t st, const __nv_bfloat16 *Res = nullptr, int ldr = 0, int priority = 0) {
   if (M <= 0) return cudaSuccess;
   const size_t sm = smem_bytes(K, N);
   static bool attr = false;
@@ -184,8 +187,17 @@ cudaError_t gemm(const __nv_bfloat16 *A, int lda, int M, const __nv_bfloat16 *W,
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_tc_gemm<K, N, ACT, OutT><<<(M + TM - 1) / TM, THREADS, sm, st>>>(A, lda, M, W, bias, C, ldc, err);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((M + TM - 1) / TM);
+  cfg.blockDim = dim3(THREADS);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributePriority;
+  at[0].val.priority = priority;
+  cfg.attrs = at;
+  cfg.numAttrs = priority ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k_tc_gemm<K, N, ACT, OutT>, A, lda, M, W, bias, C, ldc, err, Res, ldr);
 }
 
 }  // namespace pgmtc

@@ -152,3 +152,137 @@ def guess_errors(model: GuessModel, data: dict) -> dict:
     t = data["target"]
     rms = lambda x: float(torch.sqrt(torch.mean(x * x)))  # noqa: E731
     return {"model": rms(pred - t), "mu4": rms(t), "mu1": rms(data["prev"] - t)}
+
+
+# ----------------------------------------------------------------------------- message passing
+EMAX = 128  # graph edges kept per atom (the row build's list)
+MPNN_SHAPES = [(64, 16), (64,)] + [(64, 64), (64, 80), (64,), (64, 64), (64,)] * 2 + [(16, 64), (16,)]
+
+
+def mpnn_init_weights(seed: int = 0) -> np.ndarray:
+    """Flat FP32 weights of the message-passing model (csrc/pgm_mpnn.cu): random input, message
+    and update layers (the residual branches scaled down), a zero output layer, so the untrained
+    model predicts no correction (the guess is mu4)."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for k, shape in enumerate(MPNN_SHAPES):
+        if len(shape) == 1:
+            parts.append(np.zeros(shape))
+        elif k == len(MPNN_SHAPES) - 2:  # W_o
+            parts.append(np.zeros(shape))
+        else:
+            scale = 1.0 / np.sqrt(shape[1]) * (0.3 if shape == (64, 64) and k % 5 == 0 else 1.0)
+            parts.append(rng.normal(scale=scale, size=shape))
+    flat = np.concatenate([p.ravel() for p in parts]).astype(np.float32)
+    assert flat.size == _lib.load().pgm_mpnn_param_count()
+    return flat
+
+
+class MPNNModel:
+    """The 2-layer message-passing model of the learned guess on the short-range graph (device
+    weights and Adam state): per atom an embedding of the 16 invariants, two rounds of messages
+    along the graph's edges expanded in 8 radial functions, and the coefficients of the 15 vector
+    channels (csrc/pgm_mpnn.cu; its dense layers on the tcgen05 tensor cores)."""
+
+    def __init__(self, weights: np.ndarray | None = None, device: int = 0, seed: int = 0) -> None:
+        self.dev = torch.device("cuda", device)
+        w = mpnn_init_weights(seed) if weights is None else np.asarray(weights, np.float32)
+        self.w = torch.tensor(w, device=self.dev)
+        self.g = torch.zeros_like(self.w)
+        self.m = torch.zeros_like(self.w)
+        self.v = torch.zeros_like(self.w)
+        self.step = 0
+        self.lib = _lib.load()
+        self._work = {}
+
+    def _stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _ws(self, n: int, train: bool) -> torch.Tensor:
+        key = (n, train)
+        if key not in self._work:
+            self._work[key] = torch.empty(int(self.lib.pgm_mpnn_work_bytes(n, int(train))), dtype=torch.uint8, device=self.dev)
+        return self._work[key]
+
+    def predict(self, frame: dict) -> torch.Tensor:
+        n = frame["inv"].shape[0]
+        mu = torch.empty((n, 3), dtype=torch.float32, device=self.dev)
+        _lib.check_mpnn(self.lib.pgm_mpnn_predict(self._stream(), _p(self.w), _p(frame["inv"]), _p(frame["vec"]),
+                                                  _p(frame["edges"]), _p(frame["counts"]), EMAX, n, SIGMA, GRAPH_CUTOFF,
+                                                  _p(self._ws(n, False)), _p(mu)))
+        return mu
+
+    def loss_grad(self, frame: dict, scale: float) -> float:
+        """Adds d loss / d w to self.g; returns loss = scale * sum |mu - target|^2."""
+        n = frame["inv"].shape[0]
+        loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        _lib.check_mpnn(self.lib.pgm_mpnn_loss_grad(self._stream(), _p(self.w), _p(frame["inv"]), _p(frame["vec"]),
+                                                    _p(frame["target"]), _p(frame["edges"]), _p(frame["counts"]), EMAX, n,
+                                                    SIGMA, GRAPH_CUTOFF, float(scale), _p(self._ws(n, True)), _p(self.g),
+                                                    _p(loss)))
+        return float(loss.item())
+
+    def adam(self, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
+        self.step += 1
+        _lib.check_mpnn(self.lib.pgm_mpnn_adam(self._stream(), _p(self.w), _p(self.g), _p(self.m), _p(self.v), lr, beta1,
+                                               beta2, eps, self.step))
+
+    def train(self, frames: list, iters: int = 1000, lr: float = 2e-3, seed: int = 0, log=None) -> list:
+        """Adam with one whole frame (its graph) per step, frames in a seeded random order; returns
+        the losses (mean |mu - target|^2 / SIGMA^2 per atom)."""
+        rng = np.random.default_rng(seed)
+        losses = []
+        for it in range(iters):
+            f = frames[int(rng.integers(len(frames)))]
+            scale = 1.0 / (f["inv"].shape[0] * SIGMA**2)
+            loss = self.loss_grad(f, scale)
+            self.adam(lr=lr * 0.5 * (1.0 + np.cos(np.pi * it / iters)))
+            losses.append(loss)
+            if log and (it % 100 == 0 or it == iters - 1):
+                log(f"  train {it:5d}  loss {loss:.4e}")
+        return losses
+
+    def install(self, ff) -> None:
+        """Use the model as the solver's initial guess (predictor "nn")."""
+        _lib.check(ff._lib.pgm_set_mpnn_model(ff._h, _p(self.w), SIGMA, GRAPH_CUTOFF))
+
+
+def collect_frames(md, steps: int) -> list:
+    """As collect(), frame by frame with each frame's graph (edges (N, EMAX, 4) float32 as the row
+    build writes them, counts (N,) int32): the training data of the message-passing model."""
+    ff = md.ff
+    frames = []
+    bl_prev = None
+    for _ in range(steps):
+        md.stream.synchronize()
+        count = int(md.ind.count.min())
+        with torch.cuda.stream(md.stream):
+            hist = md.ind.hist.clone()
+        md.step()
+        with torch.cuda.stream(md.stream):
+            inv, vec, bl = features(ff, md.pos, md.box, hist, bl_prev)
+            x4 = 4.0 * hist[0] - 6.0 * hist[1] + 4.0 * hist[2] - hist[3]
+            target = (md.ind.mu - x4).to(torch.float32)
+            prev = (hist[0] - x4).to(torch.float32)
+            edges = torch.empty((ff.n, EMAX, 4), dtype=torch.float32, device=ff.device)
+            counts = torch.empty(ff.n, dtype=torch.int32, device=ff.device)
+            _lib.check(ff._lib.pgm_nn_graph(ff._h, ff._stream(), _p(edges), _p(counts), EMAX))
+        md.stream.synchronize()
+        if count >= 4 and bl_prev is not None:
+            frames.append({"inv": inv, "vec": vec, "target": target, "prev": prev, "edges": edges, "counts": counts})
+        bl_prev = bl
+    return frames
+
+
+def frame_errors(model: MPNNModel, frames: list) -> dict:
+    """RMS error (e nm) over frames of mu4 + the model's correction, mu4 and the previous step's dipoles."""
+    se = {"model": 0.0, "mu4": 0.0, "mu1": 0.0}
+    cnt = 0
+    for f in frames:
+        pred = model.predict(f)
+        t = f["target"]
+        se["model"] += float(torch.sum((pred - t) ** 2))
+        se["mu4"] += float(torch.sum(t * t))
+        se["mu1"] += float(torch.sum((f["prev"] - t) ** 2))
+        cnt += t.numel()
+    return {k: float(np.sqrt(v / cnt)) for k, v in se.items()}

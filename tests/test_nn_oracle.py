@@ -27,3 +27,27 @@ def test_exact_gradient_equals_finite_differences():
         lm = N.loss_grad(flat - d, inv, vec, tgt, 1.0 / (n * 0.02**2), rounded=False)[0]
         fd = (lp - lm) / (2 * h)
         assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(fd)), (k, fd, g[k])
+
+
+def test_mpnn_oracle_gradient_equals_central_differences():
+    """The message-passing model's analytic gradient (unrounded) against central differences."""
+    rng = np.random.default_rng(4)
+    n, ne = 40, 300
+    src = rng.integers(0, n, ne)
+    dst = (src + 1 + rng.integers(0, n - 1, ne)) % n
+    src, dst = np.concatenate([src, dst]), np.concatenate([dst, src])  # symmetric graph
+    d = np.concatenate([rng.uniform(0.1, 0.5, ne)] * 2)
+    phi = N.radial(d, 0.5)
+    inv = rng.normal(size=(n, N.N_IN))
+    vec = rng.normal(scale=0.01, size=(n, N.N_CH, 3))
+    tgt = rng.normal(scale=1e-4, size=(n, 3))
+    w = rng.normal(scale=0.2, size=N.mpnn_nparam())
+    loss, g = N.mpnn_loss_grad(w, inv, vec, src, dst, phi, tgt, 2e-4, 1e6, rounded=False)
+    h = 1e-6
+    for k in rng.choice(w.size, 25, replace=False):
+        e = np.zeros_like(w)
+        e[k] = h
+        lp = N.mpnn_loss_grad(w + e, inv, vec, src, dst, phi, tgt, 2e-4, 1e6, rounded=False)[0]
+        lm = N.mpnn_loss_grad(w - e, inv, vec, src, dst, phi, tgt, 2e-4, 1e6, rounded=False)[0]
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-5 * max(1e-3, abs(fd)), (k, fd, g[k])
