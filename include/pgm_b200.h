@@ -330,7 +330,8 @@ const char *pgm_mpnn_last_error(void);
 /* ------------------------------------------------------------------ tcgen05 dense layers
  * No counterpart in the reference (its learned models run through XLA).  C = act(A W^T + bias) on
  * the 5th-generation tensor cores: A (M, lda) BF16 with the first K of every row used (lda a
- * multiple of 8), W (N, K) BF16, bias N floats or NULL, C (M, ldc) FP32 (out_f32) or BF16; act 0
+ * multiple of 8), W (N, K) BF16, bias N floats or NULL, C (M, ldc) FP32 (out_f32, ldc a multiple of
+ * 4) or BF16 (ldc a multiple of 8); A, W and C 16-byte aligned, else PGM_ERR_INVALID; act 0
  * none, 1 SiLU; BF16 products accumulated in FP32 (tensor memory).  Compiled (K, N): (16, 64),
  * (64, 64), (64, 128), (80, 64), (64, 32), (128, 16); others return PGM_ERR_UNSUPPORTED.  *err
  * (device int) is set when a tile's wait for its MMAs gave up (it is never expected to). */

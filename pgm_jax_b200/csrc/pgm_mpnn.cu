@@ -98,67 +98,96 @@ __global__ void k_convert(const float *W, int out, int in, __nv_bfloat16 *Wf, __
 // Radial functions of an edge of length d (float, as the NumPy restatement).
 __device__ __forceinline__ float radial(int r, float d, float rg) {
   const float mu = r * (rg / (R - 1)), gam = ((R - 1) / rg) * ((R - 1) / rg);
-  const float fc = 0.5f * (cosf(3.14159265358979f * d / rg) + 1.0f);
+  const float fc = 0.5f * (cospif(d / rg) + 1.0f);  // cos(pi d / rg), d / rg in [0, 1]
   const float x = d - mu;
   return expf(-gam * x * x) * fc;
 }
 
-// Messages, one warp per atom: lane = 4 r + q holds features 2 q, 2 q + 1 of radial r; a_i[f] =
-// sum over the atom's edges of phi_r(d) g_j[8 r + f], summed over r by a butterfly, written as
-// BF16 into columns 64..71 of the atom's row of Z (ldz).  Edges past emax are not read.
-__global__ void k_aggregate(const __nv_bfloat16 *__restrict__ G, int ldg, const float4 *__restrict__ edges,
-                            const int *__restrict__ ecount, int emax, int n, float rg, __nv_bfloat16 *__restrict__ Z, int ldz) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int i = warp, r = lane >> 2, q = lane & 3;
-  const int ne = min(ecount[i], emax);
-  const float4 *e = edges + (size_t)i * emax;
-  float a0 = 0.f, a1 = 0.f;
-  for (int t = 0; t < ne; ++t) {
-    const float4 ed = e[t];
-    const int j = __float_as_int(ed.w);
-    const float d = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
-    const float ph = radial(r, d, rg);
-    const __nv_bfloat162 g2 = *reinterpret_cast<const __nv_bfloat162 *>(G + (size_t)j * ldg + 8 * r + 2 * q);
-    a0 += ph * __bfloat162float(g2.x);
-    a1 += ph * __bfloat162float(g2.y);
-  }
+// Eight floats rounded to BF16, packed for one 16-byte store.
+__device__ __forceinline__ int4 pack_bf16x8(const float *x) {
+  int4 o;
+  int *w = &o.x;
 #pragma unroll
-  for (int o = 4; o < 32; o <<= 1) {
-    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+  for (int k = 0; k < 4; ++k) {
+    const __nv_bfloat162 b = __floats2bfloat162_rn(x[2 * k], x[2 * k + 1]);
+    w[k] = *reinterpret_cast<const int *>(&b);
   }
-  if (lane < 4) {
-    __nv_bfloat162 v;
-    v.x = __float2bfloat16(a0);
-    v.y = __float2bfloat16(a1);
-    *reinterpret_cast<__nv_bfloat162 *>(Z + (size_t)i * ldz + HID + 2 * q) = v;
-  }
+  return o;
 }
 
-// The transposed message sum, one warp per atom j: dg_j[8 r + f] = sum over j's edges (j, i) of
-// phi_r(d) da_i[f] (the graph is symmetric), as FP32 (for the weight gradient) and BF16.
-__global__ void k_aggregate_t(const float *__restrict__ dZ, int ldd, const float4 *__restrict__ edges,
-                              const int *__restrict__ ecount, int emax, int n, float rg, float *__restrict__ dG,
-                              __nv_bfloat16 *__restrict__ dGb) {
+// Messages, one warp per atom, four edges per round: lane 8 s + r takes edge t0 + s and radial r,
+// loads the 8 features g_j[8 r .. 8 r + 7] as one 16-byte access (a warp reads four whole 128-byte
+// rows of g at once) and accumulates phi_r(d) g_j[8 r + f] for f = 0..7; a butterfly over the 32
+// lanes sums edges and radials, and a_i[f] goes as BF16 into columns 64..71 of the atom's row of Z
+// (ldz).  The next round's edges are loaded one round ahead.  Edges past emax are not read; ldg and
+// ldz are multiples of 8 and G, Z 16-byte aligned.
+__global__ void __launch_bounds__(256) k_aggregate(const __nv_bfloat16 *__restrict__ G, int ldg,
+                                                   const float4 *__restrict__ edges, const int *__restrict__ ecount,
+                                                   int emax, int n, float rg, __nv_bfloat16 *__restrict__ Z, int ldz) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= n) return;
-  const int j = warp, r = lane >> 2, q = lane & 3;
+  const int i = warp, s = lane >> 3, r = lane & 7;
+  const int ne = min(ecount[i], emax);
+  const float4 *e = edges + (size_t)i * emax;
+  float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float4 nx = s < ne ? __ldg(e + s) : make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int t0 = 0; t0 < ne; t0 += 4) {
+    const float4 ed = nx;
+    const bool ok = t0 + s < ne && (unsigned)__float_as_int(ed.w) < (unsigned)n;  // a bad partner is skipped
+    if (t0 + 4 + s < ne) nx = __ldg(e + t0 + 4 + s);
+    const float ph = ok ? radial(r, sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z), rg) : 0.f;
+    const int j = ok ? __float_as_int(ed.w) : i;
+    const int4 raw = __ldg(reinterpret_cast<const int4 *>(G + (size_t)j * ldg + 8 * r));
+    const __nv_bfloat162 *g2 = reinterpret_cast<const __nv_bfloat162 *>(&raw);
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const float2 v = __bfloat1622float2(g2[f]);
+      a[2 * f] += ph * v.x;
+      a[2 * f + 1] += ph * v.y;
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+    for (int f = 0; f < 8; ++f) a[f] += __shfl_xor_sync(0xffffffffu, a[f], o);
+  if (lane == 0) *reinterpret_cast<int4 *>(Z + (size_t)i * ldz + HID) = pack_bf16x8(a);
+}
+
+// The transposed message sum, one warp per atom j (the graph is symmetric): dg_j[8 r + f] = sum
+// over j's edges (j, i) of phi_r(d) da_i[f], with the lanes as in k_aggregate (lane 8 s + r: edge
+// t0 + s, radial r, all 8 f), summed over s by a butterfly; written as FP32 (for the weight
+// gradient) and BF16.  ldd a multiple of 4, dZ 16-byte aligned.
+__global__ void __launch_bounds__(256) k_aggregate_t(const float *__restrict__ dZ, int ldd, const float4 *__restrict__ edges,
+                                                     const int *__restrict__ ecount, int emax, int n, float rg,
+                                                     float *__restrict__ dG, __nv_bfloat16 *__restrict__ dGb) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int j = warp, s = lane >> 3, r = lane & 7;
   const int ne = min(ecount[j], emax);
   const float4 *e = edges + (size_t)j * emax;
-  float g0 = 0.f, g1 = 0.f;
-  for (int t = 0; t < ne; ++t) {
-    const float4 ed = e[t];
-    const int i = __float_as_int(ed.w);
-    const float d = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
-    const float ph = radial(r, d, rg);
-    const float2 da = *reinterpret_cast<const float2 *>(dZ + (size_t)i * ldd + HID + 2 * q);
-    g0 += ph * da.x;
-    g1 += ph * da.y;
+  float g[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float4 nx = s < ne ? __ldg(e + s) : make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int t0 = 0; t0 < ne; t0 += 4) {
+    const float4 ed = nx;
+    const bool ok = t0 + s < ne && (unsigned)__float_as_int(ed.w) < (unsigned)n;
+    if (t0 + 4 + s < ne) nx = __ldg(e + t0 + 4 + s);
+    const float ph = ok ? radial(r, sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z), rg) : 0.f;
+    const int i = ok ? __float_as_int(ed.w) : j;
+    const float4 *da = reinterpret_cast<const float4 *>(dZ + (size_t)i * ldd + HID);
+    const float4 d0 = __ldg(da), d1 = __ldg(da + 1);
+    g[0] += ph * d0.x; g[1] += ph * d0.y; g[2] += ph * d0.z; g[3] += ph * d0.w;
+    g[4] += ph * d1.x; g[5] += ph * d1.y; g[6] += ph * d1.z; g[7] += ph * d1.w;
   }
-  const size_t o = (size_t)j * HID + 8 * r + 2 * q;
-  dG[o] = g0; dG[o + 1] = g1;
-  dGb[o] = __float2bfloat16(g0); dGb[o + 1] = __float2bfloat16(g1);
+#pragma unroll
+  for (int o = 8; o < 32; o <<= 1)
+#pragma unroll
+    for (int f = 0; f < 8; ++f) g[f] += __shfl_xor_sync(0xffffffffu, g[f], o);
+  if (s == 0) {
+    float4 *o = reinterpret_cast<float4 *>(dG + (size_t)j * HID + 8 * r);
+    o[0] = make_float4(g[0], g[1], g[2], g[3]);
+    o[1] = make_float4(g[4], g[5], g[6], g[7]);
+    *reinterpret_cast<int4 *>(dGb + (size_t)j * HID + 8 * r) = pack_bf16x8(g);
+  }
 }
 
 // Prediction mu_i = sigma sum_c C[i, c] v[i, c] (FP32).
@@ -478,8 +507,9 @@ const char *pgm_tc_last_error(void) { return g_tc_err.c_str(); }
 
 PgmStatus pgm_tc_gemm(void *stream, int K, int N, int act, int out_f32, const void *A, int lda, int M, const void *W,
                       const float *bias, void *C, int ldc, int *err) {
-  if (!A || !W || !C || !err || M < 0 || lda < K || ldc < N || lda % 8 || (act != 0 && act != 1)) {
-    g_tc_err = "pgm_tc_gemm: bad argument";
+  const bool misaligned = ((uintptr_t)A | (uintptr_t)W | (uintptr_t)C) % 16 != 0 || ldc % (out_f32 ? 4 : 8) != 0;
+  if (!A || !W || !C || !err || M < 0 || lda < K || ldc < N || lda % 8 || misaligned || (act != 0 && act != 1)) {
+    g_tc_err = "pgm_tc_gemm: bad argument (null pointer, negative size, or a stride or pointer off 16 bytes)";
     return PGM_ERR_INVALID;
   }
   const __nv_bfloat16 *a = (const __nv_bfloat16 *)A, *w = (const __nv_bfloat16 *)W;

@@ -79,7 +79,8 @@ __device__ __forceinline__ void store_val<__nv_bfloat16>(__nv_bfloat16 *p, float
 // C = act(A W^T + bias) (+ Res) for one 128-row tile per CTA.  A: M rows of lda BF16 (the first K
 // used), 16-byte aligned rows; W: N x K BF16 (K contiguous); bias: N floats or null; Res: null or
 // M rows of ldr BF16 added after the activation (a residual connection); C: M rows of ldc.
-// K: a multiple of 16 up to 256; N: a multiple of 16 up to 256.
+// K: a multiple of 16 up to 256; N: a multiple of 16 up to 256; lda, ldr and ldc multiples of 8
+// (each thread moves 16 values of its row with 16-byte accesses).
 template <int K, int N, int ACT, typename OutT>
 __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__restrict__ A, int lda, int M,
                                                      const __nv_bfloat16 *__restrict__ W, const float *__restrict__ bias,
@@ -160,12 +161,29 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__rest
           : "r"(taddr + (uint32_t)c0));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row < M) {
+        float x[16];
+        __nv_bfloat16 rb[16];
+        if (Res) {  // 2 x 16-byte loads of the residual row segment
+          *reinterpret_cast<int4 *>(rb) = *reinterpret_cast<const int4 *>(Res + (size_t)row * ldr + c0);
+          *reinterpret_cast<int4 *>(rb + 8) = *reinterpret_cast<const int4 *>(Res + (size_t)row * ldr + c0 + 8);
+        }
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          float x = __uint_as_float(v[j]) + (bias ? bias[c0 + j] : 0.0f);
-          if (ACT == ACT_SILU) x = x / (1.0f + __expf(-x));
-          if (Res) x += __bfloat162float(Res[(size_t)row * ldr + c0 + j]);
-          store_val<OutT>(C + (size_t)row * ldc + c0 + j, x);
+          x[j] = __uint_as_float(v[j]) + (bias ? bias[c0 + j] : 0.0f);
+          if (ACT == ACT_SILU) x[j] = x[j] / (1.0f + __expf(-x[j]));
+          if (Res) x[j] += __bfloat162float(rb[j]);
+        }
+        OutT *dst = C + (size_t)row * ldc + c0;  // 16-byte aligned: ldc a multiple of 8, c0 of 16
+        if constexpr (sizeof(OutT) == 2) {
+          __nv_bfloat16 o[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16(x[j]);
+          reinterpret_cast<int4 *>(dst)[0] = *reinterpret_cast<const int4 *>(o);
+          reinterpret_cast<int4 *>(dst)[1] = *reinterpret_cast<const int4 *>(o + 8);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            reinterpret_cast<float4 *>(dst)[j] = make_float4(x[4 * j], x[4 * j + 1], x[4 * j + 2], x[4 * j + 3]);
         }
       }
     }

@@ -30,7 +30,7 @@ def geometric_ladder(t_min: float, t_max: float, n: int) -> np.ndarray:
     """n temperatures t_min (t_max / t_min)^(k / (n - 1)) [K] (remd.py:127-158); ValueError unless
     n >= 2 and 0 < t_min < t_max."""
     if int(n) < 2 or not (0.0 < t_min < t_max):
-        raise ValueError("need n >= 2 and 0 < t_min < t_max")
+        raise ValueError(f"a temperature ladder takes at least 2 rungs and 0 < t_min < t_max (got n={n}, {t_min}, {t_max})")
     k = np.arange(int(n), dtype=float)
     return float(t_min) * np.exp(np.log(float(t_max) / float(t_min)) * k / (int(n) - 1))
 
@@ -60,7 +60,7 @@ def metropolis(u, pairs: Sequence[tuple[int, int]], uniforms) -> tuple[np.ndarra
     used: set[int] = set()
     for k, (i, j) in enumerate(pairs):
         if i == j or i in used or j in used:
-            raise ValueError("exchange pairs must be disjoint")
+            raise ValueError(f"replica {i} or {j} appears in two exchange pairs of one attempt")
         used.add(i)
         used.add(j)
         delta = (u[i, j] - u[i, i]) + (u[j, i] - u[j, j])
