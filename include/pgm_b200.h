@@ -298,12 +298,12 @@ const char *pgm_nn_last_error(void);
 /* ------------------------------------------------------------------ message-passing guess
  * No counterpart in the reference.  The 2-layer message-passing model of the learned guess on the
  * graph of the row entries closer than graph_cutoff (pgm_mpnn.cu): h0 = SiLU(W0 inv + b0) (16 ->
- * 64); per layer g = W_g h (64 = 8 radial x 8 features), messages a_i[f] = sum over the graph of
- * sum_r phi_r(d_ij) g_j[8 r + f] (phi_r: 8 Gaussians times a cosine cutoff), h += W_b SiLU(W_a
- * [h; a; 0] + b_a) + b_b (80 -> 64 -> 64); c = W_o h + b_o (16); mu = sigma sum_c c_c v_c over the
- * 15 vector channels.  BF16 weights and activations, FP32 accumulation on the tcgen05 tensor
- * cores.  Weights: pgm_mpnn_param_count() FP32 (W0, b0, then per layer Wg, Wa, ba, Wb, bb, then
- * Wo, bo; matrices out x in, row-major). */
+ * 64); per layer a continuous-filter convolution: g = W_g h (16 features), a_i[f] = sum_r
+ * W_f[f, r] sum over the graph of phi_r(d_ij) g_j[f] (phi_r: 8 Gaussians times a cosine cutoff),
+ * h += W_b SiLU(W_a [h; a] + b_a) + b_b (80 -> 64 -> 64); c = W_o h + b_o (16); mu = sigma sum_c
+ * c_c v_c over the 15 vector channels.  BF16 weights and activations, FP32 accumulation on the
+ * tcgen05 tensor cores.  Weights: pgm_mpnn_param_count() FP32 (W0, b0, then per layer Wg, Wf, Wa,
+ * ba, Wb, bb, then Wo, bo; matrices out x in, row-major). */
 int pgm_mpnn_param_count(void);
 /* Use it as the learned guess of predictor 5 (weights device FP32; NULL: no model). */
 PgmStatus pgm_set_mpnn_model(PgmHandle *h, const float *weights, float sigma, float graph_cutoff);

@@ -77,13 +77,16 @@ def loss_grad(flat, inv, vec, target, scale: float, rounded: bool = True):
 
 # ----------------------------------------------------------------------------- message passing
 # The 2-layer message-passing model of csrc/pgm_mpnn.cu: per atom h0 = SiLU(W0 inv + b0) (64);
-# per layer g = W_g h (64 = 8 radial x 8 features), the message a_i[f] = sum over the graph's
-# edges (i, j) of sum_r phi_r(d_ij) g_j[8 r + f], u = SiLU(W_a [h; a; 0] + b_a) (80 -> 64),
-# h <- h + W_b u + b_b; coefficients c = W_o h + b_o (16, the first 15 used) and the prediction
-# SIGMA sum_c c_c v_c.  Weight matrices are (out, in); BF16 rounding where the tensor-core path
-# rounds (GEMM operands, h, g, a, u), FP32-like sums elsewhere (here float64).
-M_HID, M_R, M_F, M_COEF = 64, 8, 8, 16
-MPNN_SHAPES = [(64, 16), (64,)] + [(64, 64), (64, 80), (64,), (64, 64), (64,)] * 2 + [(16, 64), (16,)]
+# per layer g = W_g h (16 message features) and a continuous-filter convolution over the graph's
+# edges (Schuett et al., SchNet, 2017): s_i[r, f] = sum over edges (i, j) of phi_r(d_ij) g_j[f],
+# a_i[f] = sum_r W_f[f, r] s_i[r, f] (the filter psi_f(d) = sum_r W_f[f, r] phi_r(d) is linear in
+# the 8 radial functions); u = SiLU(W_a [h; a] + b_a) (80 -> 64), h <- h + W_b u + b_b;
+# coefficients c = W_o h + b_o (16, the first 15 used) and the prediction SIGMA sum_c c_c v_c.
+# Weight matrices are (out, in); BF16 rounding where the tensor-core path rounds (GEMM operands,
+# h, g, a, u, and the radial values of the forward sums), FP32-like sums elsewhere (here float64).
+M_HID, M_R, M_F, M_COEF = 64, 8, 16, 16
+MPNN_SHAPES = [(64, 16), (64,)] + [(M_F, 64), (M_F, M_R), (64, 64 + M_F), (64,), (64, 64), (64,)] * 2 + [(16, 64), (16,)]
+_PER_LAYER = 6
 
 
 def mpnn_nparam() -> int:
@@ -91,14 +94,15 @@ def mpnn_nparam() -> int:
 
 
 def mpnn_unpack(flat):
+    """(W0, b0, [(Wg, Wf, Wa, ba, Wb, bb)] * 2, Wo, bo) in float64."""
     o, out = 0, []
     for shape in MPNN_SHAPES:
         size = int(np.prod(shape))
         out.append(np.asarray(flat[o:o + size], np.float64).reshape(shape))
         o += size
     W0, b0 = out[0], out[1]
-    layers = [out[2 + 5 * l: 7 + 5 * l] for l in range(2)]
-    return W0, b0, layers, out[12], out[13]
+    layers = [out[2 + _PER_LAYER * l: 2 + _PER_LAYER * (l + 1)] for l in range(2)]
+    return W0, b0, layers, out[-2], out[-1]
 
 
 def radial(d, rg):
@@ -110,20 +114,20 @@ def radial(d, rg):
     return (np.exp(-gam * (d - mu) ** 2) * fc).astype(np.float64)
 
 
-def _aggregate(g, src, dst, phi):
-    """a[i, f] = sum over edges e with src[e] = i of sum_r phi[e, r] g[dst[e], 8 r + f]."""
+def _sums(g, src, dst, phi):
+    """s[i, r, f] = sum over edges e with src[e] = i of phi[e, r] g[dst[e], f]."""
     n = g.shape[0]
-    gr = g[dst].reshape(-1, M_R, M_F)
-    msg = np.einsum("er,erf->ef", phi, gr)
-    a = np.zeros((n, M_F))
-    np.add.at(a, src, msg)
-    return a
+    msg = np.einsum("er,ef->erf", phi, g[dst])
+    s = np.zeros((n, M_R, M_F))
+    np.add.at(s, src, msg)
+    return s
 
 
-def _aggregate_t(da, src, dst, phi, n):
-    """The transposed aggregation: dg[j, 8 r + f] = sum over edges e with dst[e] = j of phi[e, r] da[src[e], f]."""
-    contrib = np.einsum("er,ef->erf", phi, da[src]).reshape(-1, M_R * M_F)
-    dg = np.zeros((n, M_R * M_F))
+def _sums_t(da, Wf, src, dst, phi, n):
+    """The transposed convolution: dg[j, f] = sum over edges e with dst[e] = j of
+    sum_r phi[e, r] W_f[f, r] da[src[e], f]."""
+    contrib = (phi @ Wf.T) * da[src]
+    dg = np.zeros((n, M_F))
     np.add.at(dg, dst, contrib)
     return dg
 
@@ -132,19 +136,19 @@ def mpnn_forward(flat, inv, vec, src, dst, phi, sigma, rounded=True):
     """Prediction (n, 3) and the cache of the backward pass."""
     r = bf16 if rounded else (lambda x: np.asarray(x, np.float64))
     W0, b0, layers, Wo, bo = mpnn_unpack(flat)
-    n = inv.shape[0]
     x0 = r(inv)
     z0 = x0 @ r(W0).T + b0
     h = r(silu(z0))
     cache = {"x0": x0, "z0": z0, "layers": []}
-    for Wg, Wa, ba, Wb, bb in layers:
+    for Wg, Wf, Wa, ba, Wb, bb in layers:
         g = r(h @ r(Wg).T)
-        a = r(_aggregate(g, src, dst, phi))
-        Z = np.concatenate([h, a, np.zeros((n, 8))], 1)
+        s = _sums(g, src, dst, r(phi))  # the forward sums take the radial values in BF16 (tensor-core operands)
+        a = r(np.einsum("nrf,fr->nf", s, Wf))
+        Z = np.concatenate([h, a], 1)
         zu = Z @ r(Wa).T + ba
         u = r(silu(zu))
         hn = r(h + (u @ r(Wb).T + bb))
-        cache["layers"].append({"h": h, "g": g, "Z": Z, "zu": zu, "u": u})
+        cache["layers"].append({"h": h, "g": g, "s": s, "Z": Z, "zu": zu, "u": u})
         h = hn
     c = h @ r(Wo).T + bo
     cache["h2"] = h
@@ -164,12 +168,11 @@ def mpnn_loss_grad(flat, inv, vec, src, dst, phi, target, sigma, scale, rounded=
     dmu = 2.0 * scale * e
     dc = np.zeros((n, M_COEF))
     dc[:, :N_CH] = sigma * np.einsum("nk,nck->nc", dmu, vec)
-    grads = {}
-    grads["Wo"] = dc.T @ C["h2"]
-    grads["bo"] = dc.sum(0)
+    gWo = dc.T @ C["h2"]
+    gbo = dc.sum(0)
     dh = r(dc) @ r(Wo)
     lg = []
-    for (Wg, Wa, ba, Wb, bb), L in zip(layers[::-1], C["layers"][::-1]):
+    for (Wg, Wf, Wa, ba, Wb, bb), L in zip(layers[::-1], C["layers"][::-1]):
         gWb = dh.T @ L["u"]
         gbb = dh.sum(0)
         du = r(dh) @ r(Wb)
@@ -177,16 +180,17 @@ def mpnn_loss_grad(flat, inv, vec, src, dst, phi, target, sigma, scale, rounded=
         gWa = dzu.T @ L["Z"]
         gba = dzu.sum(0)
         dZ = r(dzu) @ r(Wa)
-        da = dZ[:, 64:72]
-        dg = _aggregate_t(da, src, dst, phi, n)
+        da = dZ[:, 64:]
+        gWf = np.einsum("nf,nrf->fr", da, L["s"])
+        dg = _sums_t(da, Wf, src, dst, phi, n)
         gWg = dg.T @ L["h"]
         dh = dh + dZ[:, :64] + r(dg) @ r(Wg)
-        lg.append((gWg, gWa, gba, gWb, gbb))
+        lg.append((gWg, gWf, gWa, gba, gWb, gbb))
     dz0 = dh * dsilu(C["z0"])
     gW0 = dz0.T @ C["x0"]
     gb0 = dz0.sum(0)
     flat_g = [gW0.ravel(), gb0]
     for t in lg[::-1]:
         flat_g += [x.ravel() for x in t]
-    flat_g += [grads["Wo"].ravel(), grads["bo"]]
+    flat_g += [gWo.ravel(), gbo]
     return loss, np.concatenate(flat_g)

@@ -4,21 +4,23 @@
 // invariants inv_i and 15 vector channels v_i,c), on the graph of the row entries closer than the
 // graph cutoff rg (the list the row build writes: per atom up to emax edges (x, y, z, partner)):
 //   h0 = SiLU(W0 inv + b0)                                       16 -> 64
-//   two message-passing layers:
-//     g = W_g h                                                  64 -> 64 = 8 radial x 8 features
-//     a_i[f] = sum_(i,j) sum_r phi_r(d_ij) g_j[8 r + f]          messages over the graph
-//     u = SiLU(W_a [h; a; 0] + b_a)                              80 -> 64
+//   two message-passing layers, each a continuous-filter convolution (SchNet, Schuett et al. 2017):
+//     g = W_g h                                                  64 -> 16 message features
+//     s_i[r, f] = sum_(i,j) phi_r(d_ij) g_j[f]                   sums over the graph's edges
+//     a_i[f] = sum_r W_f[f, r] s_i[r, f]                         filter psi_f(d) = sum_r W_f[f, r] phi_r(d)
+//     u = SiLU(W_a [h; a] + b_a)                                 80 -> 64
 //     h <- h + W_b u + b_b                                       64 -> 64 (residual)
 //   c = W_o h + b_o                                              64 -> 16 (15 used)
 //   prediction sigma sum_c c_c v_i,c                             (e nm; rotates with the system)
-// phi_r(d) = exp(-((d - r rg / 7) 7 / rg)^2) (cos(pi d / rg) + 1) / 2, r = 0..7.
+// phi_r(d) = exp(-((d - r rg / 7) 7 / rg)^2) (cos(pi d / rg) + 1) / 2, r = 0..7.  An edge costs one
+// 32-byte read of g_j (16 BF16 features) however many radial functions there are.
 // The dense layers run on the tcgen05 tensor cores (pgm_tc.cuh: BF16 operands, FP32 accumulation,
-// bias / SiLU / residual in the epilogue); the message sums and the readout on the CUDA cores.
-// Training: the same forward with the pre-activations kept, then the backward pass: activation
-// gradients through the transposed weights on the tensor cores (BF16 operands), the transposed
-// message sum (the graph is symmetric: d_ij = d_ji), and the weight gradients as FP32 sums over
-// the atoms of the batch on the CUDA cores.  The NumPy restatement (oracle/nn_oracle.py mpnn_*)
-// rounds to BF16 at the same points.
+// bias / SiLU / residual in the epilogue); the edge sums and the readout on the CUDA cores.
+// Training: the same forward with the pre-activations and the sums s kept, then the backward pass:
+// activation gradients through the transposed weights on the tensor cores (BF16 operands), the
+// transposed convolution (the graph is symmetric: d_ij = d_ji), and the weight gradients as FP32
+// sums over the atoms of the batch on the CUDA cores.  The NumPy restatement
+// (oracle/nn_oracle.py mpnn_*) rounds to BF16 at the same points.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -31,23 +33,24 @@
 
 namespace pgmmp {
 
-constexpr int IN = 16, HID = 64, R = 8, F = 8, ZW = 80, COEF = 16, CH = 15;
-static_assert(R * F == HID && HID + F + 8 == ZW, "g holds R x F message features; Z = [h; a; 8 zeros]");
-// flat FP32 parameters: W0 (64 x 16), b0, [Wg (64 x 64), Wa (64 x 80), ba, Wb (64 x 64), bb] x 2, Wo (16 x 64), bo
-constexpr int L_SIZE = HID * HID + HID * ZW + HID + HID * HID + HID;
+constexpr int IN = 16, HID = 64, R = 8, F = 16, ZW = HID + F, COEF = 16, CH = 15;
+// flat FP32 parameters: W0 (64 x 16), b0, [Wg (16 x 64), Wf (16 x 8), Wa (64 x 80), ba, Wb (64 x 64), bb] x 2,
+// Wo (16 x 64), bo
+constexpr int L_SIZE = F * HID + F * R + HID * ZW + HID + HID * HID + HID;
 constexpr int NPARAM = HID * IN + HID + 2 * L_SIZE + COEF * HID + COEF;
-// BF16 copies: forward (out x in) and transposed (in x out) of W0? (forward only), Wg, Wa, Wb, Wo
-constexpr int WB_FWD = HID * IN + 2 * (HID * HID + HID * ZW + HID * HID) + COEF * HID;
+// BF16 copies: forward (out x in) of W0, Wg, Wa, Wb, Wo
+constexpr int WB_FWD = HID * IN + 2 * (F * HID + HID * ZW + HID * HID) + COEF * HID;
 
 struct View {
-  const float *W0, *b0, *Wg[2], *Wa[2], *ba[2], *Wb[2], *bb[2], *Wo, *bo;
+  const float *W0, *b0, *Wg[2], *Wf[2], *Wa[2], *ba[2], *Wb[2], *bb[2], *Wo, *bo;
 };
 __host__ __device__ inline View view(const float *p) {
   View v;
   v.W0 = p; v.b0 = p + HID * IN;
   const float *q = v.b0 + HID;
   for (int l = 0; l < 2; ++l) {
-    v.Wg[l] = q; v.Wa[l] = q + HID * HID; v.ba[l] = v.Wa[l] + HID * ZW; v.Wb[l] = v.ba[l] + HID; v.bb[l] = v.Wb[l] + HID * HID;
+    v.Wg[l] = q; v.Wf[l] = q + F * HID; v.Wa[l] = v.Wf[l] + F * R; v.ba[l] = v.Wa[l] + HID * ZW;
+    v.Wb[l] = v.ba[l] + HID; v.bb[l] = v.Wb[l] + HID * HID;
     q = v.bb[l] + HID;
   }
   v.Wo = q; v.bo = q + COEF * HID;
@@ -55,32 +58,34 @@ __host__ __device__ inline View view(const float *p) {
 }
 // the gradient has the same layout
 struct GView {
-  float *W0, *b0, *Wg[2], *Wa[2], *ba[2], *Wb[2], *bb[2], *Wo, *bo;
+  float *W0, *b0, *Wg[2], *Wf[2], *Wa[2], *ba[2], *Wb[2], *bb[2], *Wo, *bo;
 };
 inline GView gview(float *p) {
   View v = view(p);
   GView g;
   g.W0 = const_cast<float *>(v.W0); g.b0 = const_cast<float *>(v.b0);
   for (int l = 0; l < 2; ++l) {
-    g.Wg[l] = const_cast<float *>(v.Wg[l]); g.Wa[l] = const_cast<float *>(v.Wa[l]); g.ba[l] = const_cast<float *>(v.ba[l]);
+    g.Wg[l] = const_cast<float *>(v.Wg[l]); g.Wf[l] = const_cast<float *>(v.Wf[l]);
+    g.Wa[l] = const_cast<float *>(v.Wa[l]); g.ba[l] = const_cast<float *>(v.ba[l]);
     g.Wb[l] = const_cast<float *>(v.Wb[l]); g.bb[l] = const_cast<float *>(v.bb[l]);
   }
   g.Wo = const_cast<float *>(v.Wo); g.bo = const_cast<float *>(v.bo);
   return g;
 }
 
-// BF16 weights: forward copies (out x in) and, for the backward pass, transposed copies (in x out).
+// BF16 weights: forward copies (out x in) and, for the backward pass, transposed copies (in x out);
+// every matrix starts on a 16-byte boundary (its element count is a multiple of 8).
 struct WB {
   __nv_bfloat16 *W0, *Wg[2], *Wa[2], *Wb[2], *Wo;        // forward
   __nv_bfloat16 *WgT[2], *WaT[2], *WbT[2], *WoT;          // transposed
 };
-constexpr int WB_ELEMS = WB_FWD + 2 * (HID * HID + ZW * HID + HID * HID) + HID * COEF;
+constexpr int WB_ELEMS = WB_FWD + 2 * (HID * F + ZW * HID + HID * HID) + HID * COEF;
 inline WB wb_view(__nv_bfloat16 *p) {
   WB w;
   w.W0 = p; p += HID * IN;
-  for (int l = 0; l < 2; ++l) { w.Wg[l] = p; p += HID * HID; w.Wa[l] = p; p += HID * ZW; w.Wb[l] = p; p += HID * HID; }
+  for (int l = 0; l < 2; ++l) { w.Wg[l] = p; p += F * HID; w.Wa[l] = p; p += HID * ZW; w.Wb[l] = p; p += HID * HID; }
   w.Wo = p; p += COEF * HID;
-  for (int l = 0; l < 2; ++l) { w.WgT[l] = p; p += HID * HID; w.WaT[l] = p; p += ZW * HID; w.WbT[l] = p; p += HID * HID; }
+  for (int l = 0; l < 2; ++l) { w.WgT[l] = p; p += HID * F; w.WaT[l] = p; p += ZW * HID; w.WbT[l] = p; p += HID * HID; }
   w.WoT = p;
   return w;
 }
@@ -115,79 +120,215 @@ __device__ __forceinline__ int4 pack_bf16x8(const float *x) {
   return o;
 }
 
-// Messages, one warp per atom, four edges per round: lane 8 s + r takes edge t0 + s and radial r,
-// loads the 8 features g_j[8 r .. 8 r + 7] as one 16-byte access (a warp reads four whole 128-byte
-// rows of g at once) and accumulates phi_r(d) g_j[8 r + f] for f = 0..7; a butterfly over the 32
-// lanes sums edges and radials, and a_i[f] goes as BF16 into columns 64..71 of the atom's row of Z
-// (ldz).  The next round's edges are loaded one round ahead.  Edges past emax are not read; ldg and
-// ldz are multiples of 8 and G, Z 16-byte aligned.
-__global__ void __launch_bounds__(256) k_aggregate(const __nv_bfloat16 *__restrict__ G, int ldg,
-                                                   const float4 *__restrict__ edges, const int *__restrict__ ecount,
-                                                   int emax, int n, float rg, __nv_bfloat16 *__restrict__ Z, int ldz) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int i = warp, s = lane >> 3, r = lane & 7;
-  const int ne = min(ecount[i], emax);
-  const float4 *e = edges + (size_t)i * emax;
-  float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  float4 nx = s < ne ? __ldg(e + s) : make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int t0 = 0; t0 < ne; t0 += 4) {
-    const float4 ed = nx;
-    const bool ok = t0 + s < ne && (unsigned)__float_as_int(ed.w) < (unsigned)n;  // a bad partner is skipped
-    if (t0 + 4 + s < ne) nx = __ldg(e + t0 + 4 + s);
-    const float ph = ok ? radial(r, sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z), rg) : 0.f;
-    const int j = ok ? __float_as_int(ed.w) : i;
-    const int4 raw = __ldg(reinterpret_cast<const int4 *>(G + (size_t)j * ldg + 8 * r));
-    const __nv_bfloat162 *g2 = reinterpret_cast<const __nv_bfloat162 *>(&raw);
+// acc[f] += ph * (16 BF16 values of q0, q1)
+__device__ __forceinline__ void fma_bf16x16(float *acc, float ph, int4 q0, int4 q1) {
+  const __nv_bfloat162 *b0 = reinterpret_cast<const __nv_bfloat162 *>(&q0);
+  const __nv_bfloat162 *b1 = reinterpret_cast<const __nv_bfloat162 *>(&q1);
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      const float2 v = __bfloat1622float2(g2[f]);
-      a[2 * f] += ph * v.x;
-      a[2 * f + 1] += ph * v.y;
-    }
+  for (int k = 0; k < 4; ++k) {
+    const float2 u = __bfloat1622float2(b0[k]), v = __bfloat1622float2(b1[k]);
+    acc[2 * k] += ph * u.x;
+    acc[2 * k + 1] += ph * u.y;
+    acc[8 + 2 * k] += ph * v.x;
+    acc[8 + 2 * k + 1] += ph * v.y;
   }
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1)
-#pragma unroll
-    for (int f = 0; f < 8; ++f) a[f] += __shfl_xor_sync(0xffffffffu, a[f], o);
-  if (lane == 0) *reinterpret_cast<int4 *>(Z + (size_t)i * ldz + HID) = pack_bf16x8(a);
 }
 
-// The transposed message sum, one warp per atom j (the graph is symmetric): dg_j[8 r + f] = sum
-// over j's edges (j, i) of phi_r(d) da_i[f], with the lanes as in k_aggregate (lane 8 s + r: edge
-// t0 + s, radial r, all 8 f), summed over s by a butterfly; written as FP32 (for the weight
-// gradient) and BF16.  ldd a multiple of 4, dZ 16-byte aligned.
-__global__ void __launch_bounds__(256) k_aggregate_t(const float *__restrict__ dZ, int ldd, const float4 *__restrict__ edges,
-                                                     const int *__restrict__ ecount, int emax, int n, float rg,
-                                                     float *__restrict__ dG, __nv_bfloat16 *__restrict__ dGb) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int j = warp, s = lane >> 3, r = lane & 7;
-  const int ne = min(ecount[j], emax);
-  const float4 *e = edges + (size_t)j * emax;
-  float g[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  float4 nx = s < ne ? __ldg(e + s) : make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int t0 = 0; t0 < ne; t0 += 4) {
-    const float4 ed = nx;
-    const bool ok = t0 + s < ne && (unsigned)__float_as_int(ed.w) < (unsigned)n;
-    if (t0 + 4 + s < ne) nx = __ldg(e + t0 + 4 + s);
-    const float ph = ok ? radial(r, sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z), rg) : 0.f;
-    const int i = ok ? __float_as_int(ed.w) : j;
-    const float4 *da = reinterpret_cast<const float4 *>(dZ + (size_t)i * ldd + HID);
-    const float4 d0 = __ldg(da), d1 = __ldg(da + 1);
-    g[0] += ph * d0.x; g[1] += ph * d0.y; g[2] += ph * d0.z; g[3] += ph * d0.w;
-    g[4] += ph * d1.x; g[5] += ph * d1.y; g[6] += ph * d1.z; g[7] += ph * d1.w;
+// The edge sums of one warp per atom.  Edges in blocks of 32: lane l loads edge b0 + l and evaluates
+// its length and cosine cutoff once; then rounds of four edges: lane 8 s + r takes edge t + s
+// (its length, cutoff and partner by shuffles) and radial r, and accumulates phi_r(d) x[partner][f]
+// for the F = 16 values x of the partner (LOAD fetches them; the 8 lanes of an edge read the same
+// 32 or 64 bytes).  After the loop each lane holds its slot's share of the sums over r.  A partner
+// index outside [0, n) is skipped.
+template <typename Load>
+__device__ __forceinline__ void edge_sums(const float4 *__restrict__ e, int ne, int n, int self, float rg, int lane, float *acc,
+                                          Load &&load) {
+  const int s = lane >> 3, r = lane & 7;
+  const float mu = r * (rg / (R - 1)), gam = ((R - 1) / rg) * ((R - 1) / rg);
+  for (int b0 = 0; b0 < ne; b0 += 32) {
+    float dl = 0.f, fcl = 0.f;
+    int jl = self;
+    if (b0 + lane < ne) {
+      const float4 ed = __ldg(e + b0 + lane);
+      const int j = __float_as_int(ed.w);
+      if ((unsigned)j < (unsigned)n) {
+        dl = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
+        fcl = 0.5f * (cospif(dl / rg) + 1.0f);
+        jl = j;
+      }
+    }
+    const int nb = min(32, ne - b0);
+    for (int t = 0; t < nb; t += 4) {
+      const float d = __shfl_sync(0xffffffffu, dl, t + s), fc = __shfl_sync(0xffffffffu, fcl, t + s);
+      const int j = __shfl_sync(0xffffffffu, jl, t + s);
+      const float x = d - mu;
+      load(j, __expf(-gam * x * x) * fc, acc);  // lanes past the block's edges: fc = 0, j = self
+    }
   }
 #pragma unroll
   for (int o = 8; o < 32; o <<= 1)
 #pragma unroll
-    for (int f = 0; f < 8; ++f) g[f] += __shfl_xor_sync(0xffffffffu, g[f], o);
-  if (s == 0) {
-    float4 *o = reinterpret_cast<float4 *>(dG + (size_t)j * HID + 8 * r);
-    o[0] = make_float4(g[0], g[1], g[2], g[3]);
-    o[1] = make_float4(g[4], g[5], g[6], g[7]);
-    *reinterpret_cast<int4 *>(dGb + (size_t)j * HID + 8 * r) = pack_bf16x8(g);
+    for (int f = 0; f < F; ++f) acc[f] += __shfl_xor_sync(0xffffffffu, acc[f], o);
+}
+
+// out[f] = sum_r W_f[f, r] acc_r[f] over the 8 lanes r of a slot (every lane ends with the sum).
+__device__ __forceinline__ void filter_sum(float *acc, const float *__restrict__ Wf, int r) {
+#pragma unroll
+  for (int f = 0; f < F; ++f) acc[f] *= __ldg(Wf + f * R + r);
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+    for (int f = 0; f < F; ++f) acc[f] += __shfl_xor_sync(0xffffffffu, acc[f], o);
+}
+
+// The convolution of one layer, one warp per atom i: s_i[r, f] = sum over the atom's edges of
+// phi_r(d) g_j[f] (G: n x 16 BF16, 16-byte aligned rows), a_i[f] = sum_r W_f[f, r] s_i[r, f] as
+// BF16 into columns 64..79 of the atom's row of Z (ldz a multiple of 2); with S the sums s_i (n x 8
+// x 16 FP32, for training).  Edges past emax are not read; a partner outside [0, n) is skipped.
+//
+// s_i = Phi^T G_i is a product over the edges (K), done with BF16 warp MMAs (m16n8k16, FP32
+// accumulation): A = the radial values phi_r(d_e) rounded to BF16 (rows r = 0..7; rows 8..15
+// zero), B = the partners' rows of G (16 edges x 16 features, two n8 tiles), staged through 1 KB
+// of shared memory per warp and read transposed by ldmatrix.  Edges come in blocks of 32: lane l
+// loads edge b0 + l (length, cosine cutoff, partner), and the partners' rows of both 16-edge halves
+// (one 16-byte load per lane each) are in flight while the radial values are formed.
+constexpr int AGG_WARPS = 8;
+__global__ void __launch_bounds__(32 * AGG_WARPS) k_aggregate(const __nv_bfloat16 *__restrict__ G,
+                                                              const float4 *__restrict__ edges,
+                                                              const int *__restrict__ ecount, int emax, int n, float rg,
+                                                              const float *__restrict__ Wf, __nv_bfloat16 *__restrict__ Z,
+                                                              int ldz, float *__restrict__ S) {
+  __shared__ __align__(16) __nv_bfloat16 tile[AGG_WARPS][32][F];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * AGG_WARPS + wib;
+  if (i >= n) return;  // whole warps leave: nothing below synchronises the block
+  const int g = lane >> 2, tq = lane & 3;  // MMA fragment coordinates: row / column group
+  const int ne = min(ecount[i], emax);
+  const float4 *e = edges + (size_t)i * emax;
+  const float mu = g * (rg / (R - 1)), gam = ((R - 1) / rg) * ((R - 1) / rg);
+  float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};  // n-tiles 0 (f 0..7) and 1 (f 8..15)
+  const uint32_t tbase = (uint32_t)__cvta_generic_to_shared(&tile[wib][0][0]);
+  for (int b0 = 0; b0 < ne; b0 += 32) {
+    float dl = 0.f, fcl = 0.f;
+    int jl = i;
+    if (b0 + lane < ne) {
+      const float4 ed = __ldg(e + b0 + lane);
+      const int j = __float_as_int(ed.w);
+      if ((unsigned)j < (unsigned)n) {
+        dl = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
+        fcl = 0.5f * (cospif(dl / rg) + 1.0f);
+        jl = j;
+      }
+    }
+    // rows of G: lane l brings half l & 1 of edge (l >> 1) of each 16-edge half h
+    int4 q[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = __shfl_sync(0xffffffffu, jl, 16 * h + (lane >> 1));
+      q[h] = __ldg(reinterpret_cast<const int4 *>(G + (size_t)j * F) + (lane & 1));
+    }
+    // A fragments: row g (radial), columns 2 tq, 2 tq + 1 (+ 8) = edges of the half
+    uint32_t afr[2][2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) {
+        float ph[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int src = 16 * h + 8 * kk + 2 * tq + u;
+          const float d = __shfl_sync(0xffffffffu, dl, src), fc = __shfl_sync(0xffffffffu, fcl, src);
+          const float x = d - mu;
+          ph[u] = __expf(-gam * x * x) * fc;  // fc = 0 past the edges
+        }
+        const __nv_bfloat162 p2 = __floats2bfloat162_rn(ph[0], ph[1]);
+        afr[h][kk] = *reinterpret_cast<const uint32_t *>(&p2);
+      }
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      *reinterpret_cast<int4 *>(&tile[wib][16 * h + (lane >> 1)][8 * (lane & 1)]) = q[h];
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      // matrices: (edges 0-7, f 0-7), (edges 8-15, f 0-7), (edges 0-7, f 8-15), (edges 8-15, f 8-15)
+      const int m = lane >> 3, rr = lane & 7;
+      const uint32_t addr = tbase + (uint32_t)(((16 * h + rr + 8 * (m & 1)) * F + 8 * (m >> 1)) * 2);
+      uint32_t b[4];
+      asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
+                   : "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3])
+                   : "r"(addr));
+      asm volatile(
+          "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+          "{%0, %1, %2, %3};"
+          : "+f"(c0[0]), "+f"(c0[1]), "+f"(c0[2]), "+f"(c0[3])
+          : "r"(afr[h][0]), "r"(0u), "r"(afr[h][1]), "r"(0u), "r"(b[0]), "r"(b[1]));
+      asm volatile(
+          "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+          "{%0, %1, %2, %3};"
+          : "+f"(c1[0]), "+f"(c1[1]), "+f"(c1[2]), "+f"(c1[3])
+          : "r"(afr[h][0]), "r"(0u), "r"(afr[h][1]), "r"(0u), "r"(b[2]), "r"(b[3]));
+    }
   }
+  // lane (g, tq) holds s_i[g][2 tq + {0, 1}] (c0[0..1]) and s_i[g][8 + 2 tq + {0, 1}] (c1[0..1])
+  if (S) {
+    float *o = S + ((size_t)i * R + g) * F;
+    *reinterpret_cast<float2 *>(o + 2 * tq) = make_float2(c0[0], c0[1]);
+    *reinterpret_cast<float2 *>(o + 8 + 2 * tq) = make_float2(c1[0], c1[1]);
+  }
+  float v[4] = {c0[0] * __ldg(Wf + (2 * tq) * R + g), c0[1] * __ldg(Wf + (2 * tq + 1) * R + g),
+                c1[0] * __ldg(Wf + (8 + 2 * tq) * R + g), c1[1] * __ldg(Wf + (9 + 2 * tq) * R + g)};
+#pragma unroll
+  for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if (lane < 4) {
+    __nv_bfloat162 *z = reinterpret_cast<__nv_bfloat162 *>(Z + (size_t)i * ldz + HID);
+    z[tq] = __floats2bfloat162_rn(v[0], v[1]);
+    z[4 + tq] = __floats2bfloat162_rn(v[2], v[3]);
+  }
+}
+
+// The transposed convolution, one warp per atom j (the graph is symmetric): dg_j[f] = sum over j's
+// edges (j, i) of psi_f(d) da_i[f], da = columns 64..79 of the rows of dZ (ldd a multiple of 4,
+// 16-byte aligned), as FP32 (for the weight gradient) and BF16 (n x 16 each).
+__global__ void __launch_bounds__(256) k_aggregate_t(const float *__restrict__ dZ, int ldd, const float4 *__restrict__ edges,
+                                                     const int *__restrict__ ecount, int emax, int n, float rg,
+                                                     const float *__restrict__ Wf, float *__restrict__ dG,
+                                                     __nv_bfloat16 *__restrict__ dGb) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int j = warp;
+  float acc[F];
+#pragma unroll
+  for (int f = 0; f < F; ++f) acc[f] = 0.f;
+  edge_sums(edges + (size_t)j * emax, min(ecount[j], emax), n, j, rg, lane, acc, [&](int i, float ph, float *a) {
+    const float4 *dp = reinterpret_cast<const float4 *>(dZ + (size_t)i * ldd + HID);
+#pragma unroll
+    for (int k = 0; k < F / 4; ++k) {
+      const float4 v = __ldg(dp + k);
+      a[4 * k] += ph * v.x; a[4 * k + 1] += ph * v.y; a[4 * k + 2] += ph * v.z; a[4 * k + 3] += ph * v.w;
+    }
+  });
+  filter_sum(acc, Wf, lane & 7);
+  if (lane == 0) {
+    float4 *o = reinterpret_cast<float4 *>(dG + (size_t)j * F);
+#pragma unroll
+    for (int k = 0; k < F / 4; ++k) o[k] = make_float4(acc[4 * k], acc[4 * k + 1], acc[4 * k + 2], acc[4 * k + 3]);
+    int4 *b = reinterpret_cast<int4 *>(dGb + (size_t)j * F);
+    b[0] = pack_bf16x8(acc);
+    b[1] = pack_bf16x8(acc + 8);
+  }
+}
+
+// The filter weights' gradient: dWf[f, r] += sum_i da_i[f] s_i[r, f] (da: columns 64..79 of dZ);
+// thread r F + f of a 128-thread block, atoms in a grid-stride loop, one atomic add per block.
+__global__ void __launch_bounds__(R * F) k_wf_grad(const float *__restrict__ dZ, int ldd, const float *__restrict__ S, int n,
+                                                   float *__restrict__ dWf) {
+  const int t = threadIdx.x, r = t / F, f = t - r * F;
+  float acc = 0.f;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) acc += dZ[(size_t)i * ldd + HID + f] * S[(size_t)i * R * F + t];
+  atomicAdd(&dWf[f * R + r], acc);
 }
 
 // Prediction mu_i = sigma sum_c C[i, c] v[i, c] (FP32).
@@ -318,55 +459,67 @@ __global__ void __launch_bounds__(256) k_wgrad(const float *__restrict__ dY, int
 
 // Workspace of the forward pass (inference) and of training, in bytes, for n atoms.
 struct Work {
-  __nv_bfloat16 *X0, *HZ[3], *Gb, *U;  // inputs; h with its message columns (n x 80) per layer; g; u
+  __nv_bfloat16 *X0, *HZ[3], *Gb, *U;  // inputs; h with its message columns (n x 80) per layer; g (n x 16); u
   float *Cc;                           // coefficients (n x 16)
   // training only
   float *z0, *zu[2];                   // pre-activations
   __nv_bfloat16 *Gk[2], *Uk[2];        // g and u of both layers
+  float *Sk[2];                        // the edge sums s (n x 8 x 16) of both layers
   float *dC, *dh, *dU, *dzu, *dZ, *dG, *dGh;
   __nv_bfloat16 *dCb, *dhb, *dzub, *dGb;
   __nv_bfloat16 *wb;                   // BF16 weights
   int *err;
 };
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+// The buffers in order (bytes); work_bytes and work_view walk the same list.
+template <typename Take>
+inline void work_layout(int n, bool train, Take &&take) {
+  const size_t N = (size_t)n;
+  take(N * IN * 2);
+  for (int k = 0; k < 3; ++k) take(N * ZW * 2);
+  take(N * F * 2); take(N * HID * 2);
+  take(N * COEF * 4);
+  if (train) {
+    for (int k = 0; k < 3; ++k) take(N * HID * 4);       // z0, zu[0], zu[1]
+    for (int k = 0; k < 2; ++k) take(N * F * 2);         // Gk
+    for (int k = 0; k < 2; ++k) take(N * HID * 2);       // Uk
+    for (int k = 0; k < 2; ++k) take(N * R * F * 4);     // Sk
+    take(N * COEF * 4); take(N * HID * 4); take(N * HID * 4); take(N * HID * 4);  // dC, dh, dU, dzu
+    take(N * ZW * 4); take(N * F * 4); take(N * HID * 4);                          // dZ, dG, dGh
+    take(N * COEF * 2); take(N * HID * 2); take(N * HID * 2); take(N * F * 2);      // dCb, dhb, dzub, dGb
+  }
+  take((size_t)WB_ELEMS * 2);
+  take(256);
+}
 inline size_t work_bytes(int n, bool train) {
   size_t b = 0;
-  auto add = [&](size_t bytes) { b += align256(bytes); };
-  add((size_t)n * IN * 2);
-  for (int k = 0; k < 3; ++k) add((size_t)n * ZW * 2);
-  add((size_t)n * HID * 2); add((size_t)n * HID * 2);
-  add((size_t)n * COEF * 4);
-  if (train) {
-    add((size_t)n * HID * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4);
-    for (int k = 0; k < 4; ++k) add((size_t)n * HID * 2);
-    add((size_t)n * COEF * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4);
-    add((size_t)n * ZW * 4); add((size_t)n * HID * 4); add((size_t)n * HID * 4);
-    add((size_t)n * COEF * 2); add((size_t)n * HID * 2); add((size_t)n * HID * 2); add((size_t)n * HID * 2);
-  }
-  add((size_t)WB_ELEMS * 2);
-  add(256);
+  work_layout(n, train, [&](size_t bytes) { b += align256(bytes); });
   return b;
 }
 inline Work work_view(void *base, int n, bool train) {
-  Work w = {};
+  void *q[40];
+  int k = 0;
   uint8_t *p = static_cast<uint8_t *>(base);
-  auto take = [&](size_t bytes) { void *q = p; p += align256(bytes); return q; };
-  w.X0 = (__nv_bfloat16 *)take((size_t)n * IN * 2);
-  for (int k = 0; k < 3; ++k) w.HZ[k] = (__nv_bfloat16 *)take((size_t)n * ZW * 2);
-  w.Gb = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.U = (__nv_bfloat16 *)take((size_t)n * HID * 2);
-  w.Cc = (float *)take((size_t)n * COEF * 4);
+  work_layout(n, train, [&](size_t bytes) { q[k++] = p; p += align256(bytes); });
+  Work w = {};
+  int t = 0;
+  auto bf = [&]() { return static_cast<__nv_bfloat16 *>(q[t++]); };
+  auto fl = [&]() { return static_cast<float *>(q[t++]); };
+  w.X0 = bf();
+  for (int l = 0; l < 3; ++l) w.HZ[l] = bf();
+  w.Gb = bf(); w.U = bf();
+  w.Cc = fl();
   if (train) {
-    w.z0 = (float *)take((size_t)n * HID * 4); w.zu[0] = (float *)take((size_t)n * HID * 4); w.zu[1] = (float *)take((size_t)n * HID * 4);
-    w.Gk[0] = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.Gk[1] = (__nv_bfloat16 *)take((size_t)n * HID * 2);
-    w.Uk[0] = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.Uk[1] = (__nv_bfloat16 *)take((size_t)n * HID * 2);
-    w.dC = (float *)take((size_t)n * COEF * 4); w.dh = (float *)take((size_t)n * HID * 4); w.dU = (float *)take((size_t)n * HID * 4);
-    w.dzu = (float *)take((size_t)n * HID * 4); w.dZ = (float *)take((size_t)n * ZW * 4); w.dG = (float *)take((size_t)n * HID * 4);
-    w.dGh = (float *)take((size_t)n * HID * 4);
-    w.dCb = (__nv_bfloat16 *)take((size_t)n * COEF * 2); w.dhb = (__nv_bfloat16 *)take((size_t)n * HID * 2);
-    w.dzub = (__nv_bfloat16 *)take((size_t)n * HID * 2); w.dGb = (__nv_bfloat16 *)take((size_t)n * HID * 2);
+    w.z0 = fl(); w.zu[0] = fl(); w.zu[1] = fl();
+    w.Gk[0] = bf(); w.Gk[1] = bf();
+    w.Uk[0] = bf(); w.Uk[1] = bf();
+    w.Sk[0] = fl(); w.Sk[1] = fl();
+    w.dC = fl(); w.dh = fl(); w.dU = fl(); w.dzu = fl();
+    w.dZ = fl(); w.dG = fl(); w.dGh = fl();
+    w.dCb = bf(); w.dhb = bf(); w.dzub = bf(); w.dGb = bf();
   }
-  w.wb = (__nv_bfloat16 *)take((size_t)WB_ELEMS * 2);
-  w.err = (int *)take(256);
+  w.wb = bf();
+  w.err = static_cast<int *>(q[t++]);
   return w;
 }
 
@@ -383,7 +536,7 @@ cudaError_t convert_weights(const float *flat, Work &w, cudaStream_t st) {
   WB b = wb_view(w.wb);
   k_convert<<<blocks(HID * IN), 256, 0, st>>>(v.W0, HID, IN, b.W0, nullptr);
   for (int l = 0; l < 2; ++l) {
-    k_convert<<<blocks(HID * HID), 256, 0, st>>>(v.Wg[l], HID, HID, b.Wg[l], b.WgT[l]);
+    k_convert<<<blocks(F * HID), 256, 0, st>>>(v.Wg[l], F, HID, b.Wg[l], b.WgT[l]);
     k_convert<<<blocks(HID * ZW), 256, 0, st>>>(v.Wa[l], HID, ZW, b.Wa[l], b.WaT[l]);
     k_convert<<<blocks(HID * HID), 256, 0, st>>>(v.Wb[l], HID, HID, b.Wb[l], b.WbT[l]);
   }
@@ -391,7 +544,7 @@ cudaError_t convert_weights(const float *flat, Work &w, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// The forward pass; with train, the pre-activations and every layer's g and u are kept.
+// The forward pass; with train, the pre-activations, every layer's g and u and the edge sums are kept.
 cudaError_t forward(const float *flat, Work &w, const float *inv, const float4 *edges, const int *ecount, int emax, int n,
                     float rg, bool train, cudaStream_t st, int prio) {
   using namespace pgmtc;
@@ -407,8 +560,9 @@ cudaError_t forward(const float *flat, Work &w, const float *inv, const float4 *
   for (int l = 0; l < 2; ++l) {
     __nv_bfloat16 *H = w.HZ[l], *Hn = w.HZ[l + 1];
     __nv_bfloat16 *G = train ? w.Gk[l] : w.Gb, *U = train ? w.Uk[l] : w.U;
-    MPCK((gemm<HID, HID, ACT_NONE, __nv_bfloat16>(H, ZW, n, b.Wg[l], nullptr, G, HID, w.err, st, nullptr, 0, prio)));
-    k_aggregate<<<blocks((long long)n * 32), 256, 0, st>>>(G, HID, edges, ecount, emax, n, rg, H, ZW);
+    MPCK((gemm<HID, F, ACT_NONE, __nv_bfloat16>(H, ZW, n, b.Wg[l], nullptr, G, F, w.err, st, nullptr, 0, prio)));
+    k_aggregate<<<blocks(n, AGG_WARPS), 32 * AGG_WARPS, 0, st>>>(G, edges, ecount, emax, n, rg, v.Wf[l], H, ZW,
+                                                                 train ? w.Sk[l] : nullptr);
     if (train) {
       MPCK((gemm<ZW, HID, ACT_NONE, float>(H, ZW, n, b.Wa[l], v.ba[l], w.zu[l], HID, w.err, st)));
       k_silu_round<<<blocks((long long)n * HID), 256, 0, st>>>(w.zu[l], n, HID, U, HID);
@@ -427,6 +581,7 @@ cudaError_t backward(const float *flat, Work &w, const float *inv, const float *
                      cudaStream_t st) {
   using namespace pgmtc;
   (void)inv;
+  View v = view(flat);
   GView g = gview(grad);
   WB b = wb_view(w.wb);
   const int wgb = std::min(blocks(n, 32), 1184);
@@ -441,9 +596,10 @@ cudaError_t backward(const float *flat, Work &w, const float *inv, const float *
     k_dsilu<<<blocks((long long)n * HID), 256, 0, st>>>(w.dU, w.zu[l], n * HID, w.dzu, w.dzub);
     k_wgrad<HID, ZW><<<wgb, 256, 0, st>>>(w.dzu, HID, w.HZ[l], ZW, n, g.Wa[l], g.ba[l]);
     MPCK((gemm<HID, ZW, ACT_NONE, float>(w.dzub, HID, n, b.WaT[l], nullptr, w.dZ, ZW, w.err, st)));
-    k_aggregate_t<<<blocks((long long)n * 32), 256, 0, st>>>(w.dZ, ZW, edges, ecount, emax, n, rg, w.dG, w.dGb);
-    k_wgrad<HID, HID><<<wgb, 256, 0, st>>>(w.dG, HID, w.HZ[l], ZW, n, g.Wg[l], nullptr);
-    MPCK((gemm<HID, HID, ACT_NONE, float>(w.dGb, HID, n, b.WgT[l], nullptr, w.dGh, HID, w.err, st)));
+    k_wf_grad<<<std::min(n, 1184), R * F, 0, st>>>(w.dZ, ZW, w.Sk[l], n, g.Wf[l]);
+    k_aggregate_t<<<blocks((long long)n * 32), 256, 0, st>>>(w.dZ, ZW, edges, ecount, emax, n, rg, v.Wf[l], w.dG, w.dGb);
+    k_wgrad<F, HID><<<wgb, 256, 0, st>>>(w.dG, F, w.HZ[l], ZW, n, g.Wg[l], nullptr);
+    MPCK((gemm<F, HID, ACT_NONE, float>(w.dGb, F, n, b.WgT[l], nullptr, w.dGh, HID, w.err, st)));
     k_add_dh<<<blocks((long long)n * HID), 256, 0, st>>>(w.dh, w.dZ, w.dGh, n, w.dhb);
   }
   k_dsilu<<<blocks((long long)n * HID), 256, 0, st>>>(w.dh, w.z0, n * HID, w.dzu, nullptr);
@@ -471,7 +627,7 @@ namespace pgmmp_engine {
 size_t work_bytes(int n) { return pgmmp::work_bytes(n, false); }
 cudaError_t set_weights(const float *flat, void *work, int n, cudaStream_t st) {
   pgmmp::Work w = pgmmp::work_view(work, n, false);
-  cudaError_t e = cudaMemsetAsync(work, 0, pgmmp::work_bytes(n, false), st);  // the zero columns 72..79 of Z
+  cudaError_t e = cudaMemsetAsync(w.err, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   return pgmmp::convert_weights(flat, w, st);
 }
@@ -547,7 +703,7 @@ PgmStatus pgm_mpnn_predict(void *stream, const float *weights, const float *inv,
     return mp_fail(PGM_ERR_INVALID, "pgm_mpnn_predict: bad argument");
   cudaStream_t st = (cudaStream_t)stream;
   pgmmp::Work w = pgmmp::work_view(work, n, false);
-  cudaError_t e = cudaMemsetAsync(work, 0, pgmmp::work_bytes(n, false), st);
+  cudaError_t e = cudaMemsetAsync(w.err, 0, sizeof(int), st);
   if (e == cudaSuccess) e = pgmmp::convert_weights(weights, w, st);
   if (e == cudaSuccess)
     e = pgmmp::forward(weights, w, inv, (const float4 *)edges, ecount, emax, n, graph_cutoff, false, st, 0);
@@ -567,7 +723,7 @@ PgmStatus pgm_mpnn_loss_grad(void *stream, const float *weights, const float *in
     return mp_fail(PGM_ERR_INVALID, "pgm_mpnn_loss_grad: bad argument");
   cudaStream_t st = (cudaStream_t)stream;
   pgmmp::Work w = pgmmp::work_view(work, n, true);
-  cudaError_t e = cudaMemsetAsync(work, 0, pgmmp::work_bytes(n, true), st);
+  cudaError_t e = cudaMemsetAsync(w.err, 0, sizeof(int), st);
   if (e == cudaSuccess) e = pgmmp::convert_weights(weights, w, st);
   if (e == cudaSuccess)
     e = pgmmp::forward(weights, w, inv, (const float4 *)edges, ecount, emax, n, graph_cutoff, true, st, 0);

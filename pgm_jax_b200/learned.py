@@ -156,22 +156,22 @@ def guess_errors(model: GuessModel, data: dict) -> dict:
 
 # ----------------------------------------------------------------------------- message passing
 EMAX = 128  # graph edges kept per atom (the row build's list)
-MPNN_SHAPES = [(64, 16), (64,)] + [(64, 64), (64, 80), (64,), (64, 64), (64,)] * 2 + [(16, 64), (16,)]
+# W0, b0, per layer (W_g, W_f, W_a, b_a, W_b, b_b), W_o, b_o: (out, in) matrices
+MPNN_SHAPES = [(64, 16), (64,)] + [(16, 64), (16, 8), (64, 80), (64,), (64, 64), (64,)] * 2 + [(16, 64), (16,)]
 
 
 def mpnn_init_weights(seed: int = 0) -> np.ndarray:
-    """Flat FP32 weights of the message-passing model (csrc/pgm_mpnn.cu): random input, message
-    and update layers (the residual branches scaled down), a zero output layer, so the untrained
-    model predicts no correction (the guess is mu4)."""
+    """Flat FP32 weights of the message-passing model (csrc/pgm_mpnn.cu): random input, message,
+    filter and update layers (the filters and the residual branches scaled down), a zero output
+    layer, so the untrained model predicts no correction (the guess is mu4)."""
     rng = np.random.default_rng(seed)
     parts = []
     for k, shape in enumerate(MPNN_SHAPES):
-        if len(shape) == 1:
-            parts.append(np.zeros(shape))
-        elif k == len(MPNN_SHAPES) - 2:  # W_o
+        role = (k - 2) % 6 if 2 <= k < 14 else None  # 0 W_g, 1 W_f, 2 W_a, 4 W_b
+        if len(shape) == 1 or k == len(MPNN_SHAPES) - 2:  # biases, W_o
             parts.append(np.zeros(shape))
         else:
-            scale = 1.0 / np.sqrt(shape[1]) * (0.3 if shape == (64, 64) and k % 5 == 0 else 1.0)
+            scale = 1.0 / np.sqrt(shape[1]) * (0.3 if role in (1, 4) else 1.0)
             parts.append(rng.normal(scale=scale, size=shape))
     flat = np.concatenate([p.ravel() for p in parts]).astype(np.float32)
     assert flat.size == _lib.load().pgm_mpnn_param_count()

@@ -44,7 +44,9 @@ def test_mpnn_oracle_gradient_equals_central_differences():
     w = rng.normal(scale=0.2, size=N.mpnn_nparam())
     loss, g = N.mpnn_loss_grad(w, inv, vec, src, dst, phi, tgt, 2e-4, 1e6, rounded=False)
     h = 1e-6
-    for k in rng.choice(w.size, 25, replace=False):
+    bounds = np.cumsum([0] + [int(np.prod(sh)) for sh in N.MPNN_SHAPES])
+    every_block = [int(rng.integers(lo, hi)) for lo, hi in zip(bounds[:-1], bounds[1:])]
+    for k in every_block + list(rng.choice(w.size, 10, replace=False)):
         e = np.zeros_like(w)
         e[k] = h
         lp = N.mpnn_loss_grad(w + e, inv, vec, src, dst, phi, tgt, 2e-4, 1e6, rounded=False)[0]
