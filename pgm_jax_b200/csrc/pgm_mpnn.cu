@@ -575,6 +575,223 @@ cudaError_t forward(const float *flat, Work &w, const float *inv, const float4 *
   return cudaGetLastError();
 }
 
+// ---- inference with the dense layers fused: three tile kernels (one CTA of 128 threads per 128
+// atoms) around the two edge-sum launches.  IN: h0 = SiLU(W0 inv + b0) and g = W_g h0; MID (layer
+// 0): u = SiLU(W_a [h0; a] + b_a), h1 = h0 + W_b u + b_b, g = W_g' h1; OUT (layer 1): u, h2 and
+// c = W_o h2 + b_o with the readout mu = sigma sum_c c_c v_c.  The products of a tile run back to
+// back on the tensor cores (u and h stay in shared memory, the accumulators in 64 TMEM columns),
+// so only h (for the residual and the next layer), g and mu reach global memory.  The values are
+// rounded to BF16 at the same points as the separate dense layers (forward()).
+constexpr int FM_IN = 0, FM_MID = 1, FM_OUT = 2;
+template <int MODE>
+struct Fused {
+  static constexpr int KA = MODE == FM_IN ? IN : ZW;    // K of the first product
+  static constexpr int N3 = MODE == FM_OUT ? COEF : F;  // N of the last product
+  static constexpr size_t A = (size_t)pgmtc::TM * KA * 2, W1 = (size_t)HID * KA * 2,
+                          W2 = MODE == FM_IN ? 0 : (size_t)HID * HID * 2, UH = (size_t)pgmtc::TM * HID * 2,
+                          W3 = (size_t)N3 * HID * 2;
+  static constexpr size_t bytes = A + W1 + W2 + UH + W3 + 64;
+};
+template <int K_, int N_>
+struct KN {  // the shape of one product: K, N
+  static constexpr int K = K_, N = N_;
+};
+struct FusedArgs {
+  const float *inv;                  // IN: FP32 invariants (n x 16)
+  const __nv_bfloat16 *Z;            // MID / OUT: h and a (n x 80)
+  const __nv_bfloat16 *W1, *W2, *W3;  // W0 or W_a; W_b; W_g of the next layer or W_o (BF16, out x in)
+  const float *b1, *b2, *b3;         // their biases (b3: null for W_g)
+  __nv_bfloat16 *Hout;               // IN / MID: the new h into columns 0..63 of rows of ZW
+  __nv_bfloat16 *Gout;               // IN / MID: g (n x 16)
+  const float *vec;                  // OUT: channels (n x 15 x 3)
+  float sigma;
+  float *mu;                         // OUT: prediction (n x 3)
+  int n;
+  int *err;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(pgmtc::THREADS) k_mp_fused(FusedArgs p) {
+  using namespace pgmtc;
+  using S = Fused<MODE>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sA = smem, *sW1 = sA + S::A, *sW2 = sW1 + S::W1, *sUH = sW2 + S::W2, *sW3 = sUH + S::UH;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sW3 + S::W3);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  int *gave_up = reinterpret_cast<int *>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int m0 = blockIdx.x * TM, row = m0 + tid, valid = min(TM, p.n - m0);
+  const bool live = row < p.n;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(64));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    *gave_up = 0;
+  }
+  if constexpr (MODE == FM_IN) {  // FP32 invariants -> BF16, 8 per thread and step
+    for (int c = tid; c < TM * 2; c += THREADS) {
+      const int r = c >> 1, kc = c & 1;
+      float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (r < valid) {
+        const float4 *q = reinterpret_cast<const float4 *>(p.inv + (size_t)(m0 + r) * IN + 8 * kc);
+        const float4 u = q[0], v = q[1];
+        x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w; x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
+      }
+      st_bf16x8(sA + tile_off(r, 8 * kc, IN), x);
+    }
+  } else {
+    stage_bf16<TM, ZW>(sA, p.Z + (size_t)m0 * ZW, ZW, valid);
+  }
+  stage_bf16<HID, S::KA>(sW1, p.W1, S::KA, HID);
+  if constexpr (MODE != FM_IN) stage_bf16<HID, HID>(sW2, p.W2, HID, HID);
+  stage_bf16<S::N3, HID>(sW3, p.W3, HID, S::N3);
+  tc_barrier();
+  const uint32_t tmem = *tslot, tl = tmem + ((uint32_t)(32 * warp) << 16), b = smem_u32(bar);
+  uint32_t phase = 0;
+  // a product into TMEM columns 0..N-1, then its wait (an abandoned wait stops the rest of the tile)
+  auto product = [&](auto kn, uint32_t a0, uint32_t w0) -> bool {
+    constexpr int K = decltype(kn)::K, N = decltype(kn)::N;
+    if (*gave_up) return false;
+    if (tid == 0) mma_issue<K, N>(tmem, a0, w0, b);
+    __syncwarp();
+    // one answer for the whole block: the epilogue's TMEM loads are warp-collective
+    const bool ok = __syncthreads_and(mma_wait(b, phase, p.err));
+    phase ^= 1u;
+    if (!ok && tid == 0) *gave_up = 1;
+    return ok;
+  };
+  using P1 = KN<S::KA, HID>;
+  using P2 = KN<HID, HID>;
+  using P3 = KN<HID, S::N3>;
+
+  if (product(P1{}, smem_u32(sA), smem_u32(sW1))) {
+#pragma unroll
+    for (int c0 = 0; c0 < HID; c0 += 16) {
+      float x[16];
+      tmem_ld16(tl + c0, x);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const float z = x[j] + p.b1[c0 + j];
+        x[j] = z / (1.0f + __expf(-z));
+      }
+      // IN: h0 (global and the A operand of the last product); MID / OUT: u (A of the second)
+      st_bf16x8(sUH + tile_off(tid, c0, HID), x);
+      st_bf16x8(sUH + tile_off(tid, c0 + 8, HID), x + 8);
+      if (MODE == FM_IN && live) {
+        st_bf16x8(p.Hout + (size_t)row * ZW + c0, x);
+        st_bf16x8(p.Hout + (size_t)row * ZW + c0 + 8, x + 8);
+      }
+    }
+  }
+  tc_barrier();
+  if constexpr (MODE != FM_IN) {
+    if (product(P2{}, smem_u32(sUH), smem_u32(sW2))) {
+#pragma unroll
+      for (int c0 = 0; c0 < HID; c0 += 16) {
+        float x[16];
+        tmem_ld16(tl + c0, x);
+        const __nv_bfloat162 *hr0 = reinterpret_cast<const __nv_bfloat162 *>(sA + tile_off(tid, c0, ZW));
+        const __nv_bfloat162 *hr1 = reinterpret_cast<const __nv_bfloat162 *>(sA + tile_off(tid, c0 + 8, ZW));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const float2 u = __bfloat1622float2(hr0[k]), v = __bfloat1622float2(hr1[k]);
+          x[2 * k] += p.b2[c0 + 2 * k] + u.x;
+          x[2 * k + 1] += p.b2[c0 + 2 * k + 1] + u.y;
+          x[8 + 2 * k] += p.b2[c0 + 8 + 2 * k] + v.x;
+          x[8 + 2 * k + 1] += p.b2[c0 + 8 + 2 * k + 1] + v.y;
+        }
+        st_bf16x8(sUH + tile_off(tid, c0, HID), x);  // the second product is complete: u is free
+        st_bf16x8(sUH + tile_off(tid, c0 + 8, HID), x + 8);
+        if (MODE == FM_MID && live) {
+          st_bf16x8(p.Hout + (size_t)row * ZW + c0, x);
+          st_bf16x8(p.Hout + (size_t)row * ZW + c0 + 8, x + 8);
+        }
+      }
+    }
+    tc_barrier();
+  }
+  if (product(P3{}, smem_u32(sUH), smem_u32(sW3))) {
+    float x[16];
+    tmem_ld16(tl, x);  // by every thread of the warp (a .sync.aligned load), live rows or not
+    if (!live) {
+    } else if constexpr (MODE == FM_OUT) {
+      float m[3] = {0.f, 0.f, 0.f};
+      const float *v = p.vec + (size_t)row * CH * 3;
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        const float w = x[c] + p.b3[c];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) m[k] += w * v[3 * c + k];
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) p.mu[3 * (size_t)row + k] = p.sigma * m[k];
+    } else {
+      st_bf16x8(p.Gout + (size_t)row * F, x);
+      st_bf16x8(p.Gout + (size_t)row * F + 8, x + 8);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
+}
+
+template <int MODE>
+cudaError_t launch_fused(const FusedArgs &a, cudaStream_t st, int prio) {
+  if (a.n <= 0) return cudaSuccess;
+  const size_t sm = Fused<MODE>::bytes;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_mp_fused<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((a.n + pgmtc::TM - 1) / pgmtc::TM);
+  cfg.blockDim = dim3(pgmtc::THREADS);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributePriority;
+  at[0].val.priority = prio;
+  cfg.attrs = at;
+  cfg.numAttrs = prio ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k_mp_fused<MODE>, a);
+}
+
+// Inference: mu (n x 3) from the invariants, channels and graph; five launches.
+cudaError_t predict_fused(const float *flat, Work &w, const float *inv, const float *vec, const float4 *edges, const int *ecount,
+                          int emax, int n, float sigma, float rg, float *mu, cudaStream_t st, int prio) {
+  View v = view(flat);
+  WB b = wb_view(w.wb);
+  FusedArgs a = {};
+  a.n = n;
+  a.err = w.err;
+  a.inv = inv;
+  a.W1 = b.W0; a.b1 = v.b0; a.W3 = b.Wg[0];
+  a.Hout = w.HZ[0]; a.Gout = w.Gb;
+  MPCK(launch_fused<FM_IN>(a, st, prio));
+  for (int l = 0; l < 2; ++l) {
+    k_aggregate<<<blocks(n, AGG_WARPS), 32 * AGG_WARPS, 0, st>>>(w.Gb, edges, ecount, emax, n, rg, v.Wf[l], w.HZ[l], ZW,
+                                                                 nullptr);
+    FusedArgs m = {};
+    m.n = n;
+    m.err = w.err;
+    m.Z = w.HZ[l];
+    m.W1 = b.Wa[l]; m.b1 = v.ba[l]; m.W2 = b.Wb[l]; m.b2 = v.bb[l];
+    if (l == 0) {
+      m.W3 = b.Wg[1]; m.Hout = w.HZ[1]; m.Gout = w.Gb;
+      MPCK(launch_fused<FM_MID>(m, st, prio));
+    } else {
+      m.W3 = b.Wo; m.b3 = v.bo; m.vec = vec; m.sigma = sigma; m.mu = mu;
+      MPCK(launch_fused<FM_OUT>(m, st, prio));
+    }
+  }
+  return cudaGetLastError();
+}
+
 // Loss and gradient (added into grad) of a batch whose forward pass ran with train.
 cudaError_t backward(const float *flat, Work &w, const float *inv, const float *vec, const float *target, const float4 *edges,
                      const int *ecount, int emax, int n, float sigma, float rg, float scale, float *grad, double *loss,
@@ -634,10 +851,7 @@ cudaError_t set_weights(const float *flat, void *work, int n, cudaStream_t st) {
 cudaError_t predict(const float *flat, void *work, const float *inv, const float *vec, const float4 *edges, const int *ecount,
                     int emax, int n, float sigma, float rg, float *mu, cudaStream_t st, int prio) {
   pgmmp::Work w = pgmmp::work_view(work, n, false);
-  cudaError_t e = pgmmp::forward(flat, w, inv, edges, ecount, emax, n, rg, false, st, prio);
-  if (e != cudaSuccess) return e;
-  pgmmp::k_readout<<<pgmmp::blocks(n), 256, 0, st>>>(w.Cc, vec, n, sigma, mu);
-  return cudaGetLastError();
+  return pgmmp::predict_fused(flat, w, inv, vec, edges, ecount, emax, n, sigma, rg, mu, st, prio);
 }
 }  // namespace pgmmp_engine
 
@@ -706,11 +920,7 @@ PgmStatus pgm_mpnn_predict(void *stream, const float *weights, const float *inv,
   cudaError_t e = cudaMemsetAsync(w.err, 0, sizeof(int), st);
   if (e == cudaSuccess) e = pgmmp::convert_weights(weights, w, st);
   if (e == cudaSuccess)
-    e = pgmmp::forward(weights, w, inv, (const float4 *)edges, ecount, emax, n, graph_cutoff, false, st, 0);
-  if (e == cudaSuccess) {
-    pgmmp::k_readout<<<pgmmp::blocks(n), 256, 0, st>>>(w.Cc, vec, n, sigma, mu);
-    e = cudaGetLastError();
-  }
+    e = pgmmp::predict_fused(weights, w, inv, vec, (const float4 *)edges, ecount, emax, n, sigma, graph_cutoff, mu, st, 0);
   if (e != cudaSuccess) return mp_fail(PGM_ERR_CUDA, std::string("pgm_mpnn_predict: ") + cudaGetErrorString(e));
   return PGM_OK;
 }
