@@ -188,105 +188,167 @@ __device__ __forceinline__ void filter_sum(float *acc, const float *__restrict__
 //
 // s_i = Phi^T G_i is a product over the edges (K), done with BF16 warp MMAs (m16n8k16, FP32
 // accumulation): A = the radial values phi_r(d_e) rounded to BF16 (rows r = 0..7; rows 8..15
-// zero), B = the partners' rows of G (16 edges x 16 features, two n8 tiles), staged through 1 KB
-// of shared memory per warp and read transposed by ldmatrix.  Edges come in blocks of 32: lane l
-// loads edge b0 + l (length, cosine cutoff, partner), and the partners' rows of both 16-edge halves
-// (one 16-byte load per lane each) are in flight while the radial values are formed.
-constexpr int AGG_WARPS = 8;
-__global__ void __launch_bounds__(32 * AGG_WARPS) k_aggregate(const __nv_bfloat16 *__restrict__ G,
+// zero), B = the partners' rows of G (16 edges x 16 features, two n8 tiles), read transposed from
+// shared memory by ldmatrix.  The kernel is bound by the latency of its two dependent loads (edge
+// list -> partner rows), so both go through asynchronous copies into shared memory (cp.async: many
+// in flight per thread without registers): a warp walks atoms i, i + W, ... (W warps in the grid),
+// copying the next atom's first 64 list slots while it works on the current one, and the partner
+// rows of a 64-edge window (4 copies of 16 bytes per lane) are in flight while the radial values are
+// formed.
+constexpr int AGG_WARPS = 8, AGG_WIN = 64;
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+// slots s0 .. s0 + 63 of a list of emax slots (slots past emax: zeros; nothing past them is read)
+__device__ __forceinline__ void agg_list(uint32_t dst, const float4 *__restrict__ e, int s0, int emax, int lane) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int sl = s0 + 32 * h + lane;
+    cp_async16(dst + (uint32_t)(32 * h + lane) * 16u, sl < emax ? e + sl : e, sl < emax);
+  }
+}
+
+__global__ void __launch_bounds__(32 * AGG_WARPS, 4) k_aggregate(const __nv_bfloat16 *__restrict__ G,
                                                               const float4 *__restrict__ edges,
                                                               const int *__restrict__ ecount, int emax, int n, float rg,
                                                               const float *__restrict__ Wf, __nv_bfloat16 *__restrict__ Z,
                                                               int ldz, float *__restrict__ S) {
-  __shared__ __align__(16) __nv_bfloat16 tile[AGG_WARPS][32][F];
+  __shared__ __align__(16) __nv_bfloat16 tile[AGG_WARPS][AGG_WIN][F];  // partner rows of a window
+  __shared__ __align__(16) float4 lists[AGG_WARPS][2][AGG_WIN];        // list slots, double-buffered
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * AGG_WARPS + wib;
+  const int nw = gridDim.x * AGG_WARPS;
+  int i = blockIdx.x * AGG_WARPS + wib;
   if (i >= n) return;  // whole warps leave: nothing below synchronises the block
   const int g = lane >> 2, tq = lane & 3;  // MMA fragment coordinates: row / column group
-  const int ne = min(ecount[i], emax);
-  const float4 *e = edges + (size_t)i * emax;
   const float mu = g * (rg / (R - 1)), gam = ((R - 1) / rg) * ((R - 1) / rg);
-  float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};  // n-tiles 0 (f 0..7) and 1 (f 8..15)
   const uint32_t tbase = (uint32_t)__cvta_generic_to_shared(&tile[wib][0][0]);
-  for (int b0 = 0; b0 < ne; b0 += 32) {
-    float dl = 0.f, fcl = 0.f;
-    int jl = i;
-    if (b0 + lane < ne) {
-      const float4 ed = __ldg(e + b0 + lane);
-      const int j = __float_as_int(ed.w);
-      if ((unsigned)j < (unsigned)n) {
-        dl = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
-        fcl = 0.5f * (cospif(dl / rg) + 1.0f);
-        jl = j;
+  const uint32_t lbase = (uint32_t)__cvta_generic_to_shared(&lists[wib][0][0]);
+  int cur = 0;
+  agg_list(lbase, edges + (size_t)i * emax, 0, emax, lane);
+  cp_async_commit();
+  int ne = min(ecount[i], emax);
+  for (; i < n; i += nw) {
+    const int inext = i + nw;
+    if (inext < n) agg_list(lbase + (uint32_t)(1 - cur) * AGG_WIN * 16u, edges + (size_t)inext * emax, 0, emax, lane);
+    cp_async_commit();  // (an empty group past the last atom keeps the count)
+    const int nne = inext < n ? min(ecount[inext], emax) : 0;
+    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};  // n-tiles 0 (f 0..7) and 1 (f 8..15)
+    for (int b0 = 0; b0 < ne; b0 += AGG_WIN) {
+      if (b0 == 0) {
+        cp_async_wait<1>();  // this atom's first slots (the next atom's may still be in flight)
+      } else {               // windows past the first (long lists): copied and awaited here
+        agg_list(lbase + (uint32_t)cur * AGG_WIN * 16u, edges + (size_t)i * emax, b0, emax, lane);
+        cp_async_commit();
+        cp_async_wait<0>();
       }
-    }
-    // rows of G: lane l brings half l & 1 of edge (l >> 1) of each 16-edge half h
-    int4 q[2];
+      __syncwarp();
+      // per slot: length, cosine cutoff, partner (slots past the list: cutoff 0, partner i)
+      float dl[2], fcl[2];
+      int jl[2];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int j = __shfl_sync(0xffffffffu, jl, 16 * h + (lane >> 1));
-      q[h] = __ldg(reinterpret_cast<const int4 *>(G + (size_t)j * F) + (lane & 1));
-    }
-    // A fragments: row g (radial), columns 2 tq, 2 tq + 1 (+ 8) = edges of the half
-    uint32_t afr[2][2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-      for (int kk = 0; kk < 2; ++kk) {
-        float ph[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int src = 16 * h + 8 * kk + 2 * tq + u;
-          const float d = __shfl_sync(0xffffffffu, dl, src), fc = __shfl_sync(0xffffffffu, fcl, src);
-          const float x = d - mu;
-          ph[u] = __expf(-gam * x * x) * fc;  // fc = 0 past the edges
+      for (int w = 0; w < 2; ++w) {
+        const float4 ed = lists[wib][cur][32 * w + lane];
+        const int j = __float_as_int(ed.w);
+        dl[w] = 0.f; fcl[w] = 0.f; jl[w] = i;
+        if (b0 + 32 * w + lane < ne && (unsigned)j < (unsigned)n) {
+          dl[w] = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
+          fcl[w] = 0.5f * (cospif(dl[w] / rg) + 1.0f);
+          jl[w] = j;
         }
-        const __nv_bfloat162 p2 = __floats2bfloat162_rn(ph[0], ph[1]);
-        afr[h][kk] = *reinterpret_cast<const uint32_t *>(&p2);
       }
-    __syncwarp();
+      const int nq = min(4, (ne - b0 + 15) >> 4);  // 16-edge quarters of the window in use
+      // partner rows: lane l copies half l & 1 of edge 16 q + (l >> 1) of quarter q
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
-      *reinterpret_cast<int4 *>(&tile[wib][16 * h + (lane >> 1)][8 * (lane & 1)]) = q[h];
-    __syncwarp();
+      for (int q = 0; q < 4; ++q)
+        if (q < nq) {
+          const int j = __shfl_sync(0xffffffffu, jl[q >> 1], 16 * (q & 1) + (lane >> 1));
+          cp_async16(tbase + (uint32_t)(((16 * q + (lane >> 1)) * F + 8 * (lane & 1)) * 2),
+                     reinterpret_cast<const int4 *>(G + (size_t)j * F) + (lane & 1), true);
+        }
+      cp_async_commit();
+      // A fragments: row g (radial), columns 2 tq, 2 tq + 1 (+ 8) = edges of the quarter
+      uint32_t afr[4][2];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      // matrices: (edges 0-7, f 0-7), (edges 8-15, f 0-7), (edges 0-7, f 8-15), (edges 8-15, f 8-15)
-      const int m = lane >> 3, rr = lane & 7;
-      const uint32_t addr = tbase + (uint32_t)(((16 * h + rr + 8 * (m & 1)) * F + 8 * (m >> 1)) * 2);
-      uint32_t b[4];
-      asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
-                   : "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3])
-                   : "r"(addr));
-      asm volatile(
-          "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-          "{%0, %1, %2, %3};"
-          : "+f"(c0[0]), "+f"(c0[1]), "+f"(c0[2]), "+f"(c0[3])
-          : "r"(afr[h][0]), "r"(0u), "r"(afr[h][1]), "r"(0u), "r"(b[0]), "r"(b[1]));
-      asm volatile(
-          "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-          "{%0, %1, %2, %3};"
-          : "+f"(c1[0]), "+f"(c1[1]), "+f"(c1[2]), "+f"(c1[3])
-          : "r"(afr[h][0]), "r"(0u), "r"(afr[h][1]), "r"(0u), "r"(b[2]), "r"(b[3]));
+      for (int q = 0; q < 4; ++q)
+        if (q < nq) {
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {
+            float ph[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const int src = 16 * (q & 1) + 8 * kk + 2 * tq + u;
+              const float d = __shfl_sync(0xffffffffu, dl[q >> 1], src), fc = __shfl_sync(0xffffffffu, fcl[q >> 1], src);
+              const float x = d - mu;
+              ph[u] = __expf(-gam * x * x) * fc;  // fc = 0 past the edges
+            }
+            const __nv_bfloat162 p2 = __floats2bfloat162_rn(ph[0], ph[1]);
+            afr[q][kk] = *reinterpret_cast<const uint32_t *>(&p2);
+          }
+        }
+      cp_async_wait<0>();  // the partner rows (and the next atom's slots, issued earlier)
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (q < nq) {
+          // matrices: (edges 0-7, f 0-7), (edges 8-15, f 0-7), (edges 0-7, f 8-15), (edges 8-15, f 8-15)
+          const int m = lane >> 3, rr = lane & 7;
+          const uint32_t addr = tbase + (uint32_t)(((16 * q + rr + 8 * (m & 1)) * F + 8 * (m >> 1)) * 2);
+          uint32_t bq[4];
+          asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
+                       : "=r"(bq[0]), "=r"(bq[1]), "=r"(bq[2]), "=r"(bq[3])
+                       : "r"(addr));
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+              "{%0, %1, %2, %3};"
+              : "+f"(c0[0]), "+f"(c0[1]), "+f"(c0[2]), "+f"(c0[3])
+              : "r"(afr[q][0]), "r"(0u), "r"(afr[q][1]), "r"(0u), "r"(bq[0]), "r"(bq[1]));
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+              "{%0, %1, %2, %3};"
+              : "+f"(c1[0]), "+f"(c1[1]), "+f"(c1[2]), "+f"(c1[3])
+              : "r"(afr[q][0]), "r"(0u), "r"(afr[q][1]), "r"(0u), "r"(bq[2]), "r"(bq[3]));
+        }
+      __syncwarp();  // the tile and the slots are rewritten by the next window or atom
     }
-  }
-  // lane (g, tq) holds s_i[g][2 tq + {0, 1}] (c0[0..1]) and s_i[g][8 + 2 tq + {0, 1}] (c1[0..1])
-  if (S) {
-    float *o = S + ((size_t)i * R + g) * F;
-    *reinterpret_cast<float2 *>(o + 2 * tq) = make_float2(c0[0], c0[1]);
-    *reinterpret_cast<float2 *>(o + 8 + 2 * tq) = make_float2(c1[0], c1[1]);
-  }
-  float v[4] = {c0[0] * __ldg(Wf + (2 * tq) * R + g), c0[1] * __ldg(Wf + (2 * tq + 1) * R + g),
-                c1[0] * __ldg(Wf + (8 + 2 * tq) * R + g), c1[1] * __ldg(Wf + (9 + 2 * tq) * R + g)};
+    if (ne == 0) cp_async_wait<1>();  // keep the group count in step for an atom without edges
+    // lane (g, tq) holds s_i[g][2 tq + {0, 1}] (c0[0..1]) and s_i[g][8 + 2 tq + {0, 1}] (c1[0..1])
+    if (S) {
+      float *o = S + ((size_t)i * R + g) * F;
+      *reinterpret_cast<float2 *>(o + 2 * tq) = make_float2(c0[0], c0[1]);
+      *reinterpret_cast<float2 *>(o + 8 + 2 * tq) = make_float2(c1[0], c1[1]);
+    }
+    float v[4] = {c0[0] * __ldg(Wf + (2 * tq) * R + g), c0[1] * __ldg(Wf + (2 * tq + 1) * R + g),
+                  c1[0] * __ldg(Wf + (8 + 2 * tq) * R + g), c1[1] * __ldg(Wf + (9 + 2 * tq) * R + g)};
 #pragma unroll
-  for (int o = 4; o < 32; o <<= 1)
+    for (int o = 4; o < 32; o <<= 1)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-  if (lane < 4) {
-    __nv_bfloat162 *z = reinterpret_cast<__nv_bfloat162 *>(Z + (size_t)i * ldz + HID);
-    z[tq] = __floats2bfloat162_rn(v[0], v[1]);
-    z[4 + tq] = __floats2bfloat162_rn(v[2], v[3]);
+      for (int k = 0; k < 4; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if (lane < 4) {
+      __nv_bfloat162 *z = reinterpret_cast<__nv_bfloat162 *>(Z + (size_t)i * ldz + HID);
+      z[tq] = __floats2bfloat162_rn(v[0], v[1]);
+      z[4 + tq] = __floats2bfloat162_rn(v[2], v[3]);
+    }
+    cur = 1 - cur;
+    ne = nne;
   }
+  cp_async_wait<0>();
+}
+
+// Grid of the edge-sum kernels: enough warps for every SM to hold its share at full occupancy,
+// each warp walking atoms at the grid's stride.
+inline int agg_blocks(int n) {
+  static int resident = 0;  // blocks of k_aggregate that fit on the device at once
+  if (!resident) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_aggregate, 32 * AGG_WARPS, 0);
+    resident = std::max(1, sms) * std::max(1, per);
+  }
+  return std::max(1, std::min((n + AGG_WARPS - 1) / AGG_WARPS, resident));
 }
 
 // The transposed convolution, one warp per atom j (the graph is symmetric): dg_j[f] = sum over j's
@@ -561,7 +623,7 @@ cudaError_t forward(const float *flat, Work &w, const float *inv, const float4 *
     __nv_bfloat16 *H = w.HZ[l], *Hn = w.HZ[l + 1];
     __nv_bfloat16 *G = train ? w.Gk[l] : w.Gb, *U = train ? w.Uk[l] : w.U;
     MPCK((gemm<HID, F, ACT_NONE, __nv_bfloat16>(H, ZW, n, b.Wg[l], nullptr, G, F, w.err, st, nullptr, 0, prio)));
-    k_aggregate<<<blocks(n, AGG_WARPS), 32 * AGG_WARPS, 0, st>>>(G, edges, ecount, emax, n, rg, v.Wf[l], H, ZW,
+    k_aggregate<<<agg_blocks(n), 32 * AGG_WARPS, 0, st>>>(G, edges, ecount, emax, n, rg, v.Wf[l], H, ZW,
                                                                  train ? w.Sk[l] : nullptr);
     if (train) {
       MPCK((gemm<ZW, HID, ACT_NONE, float>(H, ZW, n, b.Wa[l], v.ba[l], w.zu[l], HID, w.err, st)));
@@ -631,23 +693,28 @@ __global__ void __launch_bounds__(pgmtc::THREADS) k_mp_fused(FusedArgs p) {
     asm volatile("fence.mbarrier_init.release.cluster;");
     *gave_up = 0;
   }
-  if constexpr (MODE == FM_IN) {  // FP32 invariants -> BF16, 8 per thread and step
-    for (int c = tid; c < TM * 2; c += THREADS) {
-      const int r = c >> 1, kc = c & 1;
-      float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      if (r < valid) {
-        const float4 *q = reinterpret_cast<const float4 *>(p.inv + (size_t)(m0 + r) * IN + 8 * kc);
-        const float4 u = q[0], v = q[1];
-        x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w; x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
+  // weights (and the tile of Z) by asynchronous copies, all in flight together
+  if constexpr (MODE != FM_IN) stage_async<TM, ZW>(sA, p.Z + (size_t)m0 * ZW, ZW, valid);
+  stage_async<HID, S::KA>(sW1, p.W1, S::KA, HID);
+  if constexpr (MODE != FM_IN) stage_async<HID, HID>(sW2, p.W2, HID, HID);
+  stage_async<S::N3, HID>(sW3, p.W3, HID, S::N3);
+  if constexpr (MODE == FM_IN) {  // FP32 invariants -> BF16: row tid, both halves loaded before either is stored
+    float x[16];
+    if (tid < valid) {
+      const float4 *q = reinterpret_cast<const float4 *>(p.inv + (size_t)row * IN);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 u = q[k];
+        x[4 * k] = u.x; x[4 * k + 1] = u.y; x[4 * k + 2] = u.z; x[4 * k + 3] = u.w;
       }
-      st_bf16x8(sA + tile_off(r, 8 * kc, IN), x);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) x[k] = 0.f;
     }
-  } else {
-    stage_bf16<TM, ZW>(sA, p.Z + (size_t)m0 * ZW, ZW, valid);
+    st_bf16x8(sA + tile_off(tid, 0, IN), x);
+    st_bf16x8(sA + tile_off(tid, 8, IN), x + 8);
   }
-  stage_bf16<HID, S::KA>(sW1, p.W1, S::KA, HID);
-  if constexpr (MODE != FM_IN) stage_bf16<HID, HID>(sW2, p.W2, HID, HID);
-  stage_bf16<S::N3, HID>(sW3, p.W3, HID, S::N3);
+  cp_async_wait_all();
   tc_barrier();
   const uint32_t tmem = *tslot, tl = tmem + ((uint32_t)(32 * warp) << 16), b = smem_u32(bar);
   uint32_t phase = 0;
@@ -774,7 +841,7 @@ cudaError_t predict_fused(const float *flat, Work &w, const float *inv, const fl
   a.Hout = w.HZ[0]; a.Gout = w.Gb;
   MPCK(launch_fused<FM_IN>(a, st, prio));
   for (int l = 0; l < 2; ++l) {
-    k_aggregate<<<blocks(n, AGG_WARPS), 32 * AGG_WARPS, 0, st>>>(w.Gb, edges, ecount, emax, n, rg, v.Wf[l], w.HZ[l], ZW,
+    k_aggregate<<<agg_blocks(n), 32 * AGG_WARPS, 0, st>>>(w.Gb, edges, ecount, emax, n, rg, v.Wf[l], w.HZ[l], ZW,
                                                                  nullptr);
     FusedArgs m = {};
     m.n = n;
@@ -844,6 +911,7 @@ namespace pgmmp_engine {
 size_t work_bytes(int n) { return pgmmp::work_bytes(n, false); }
 cudaError_t set_weights(const float *flat, void *work, int n, cudaStream_t st) {
   pgmmp::Work w = pgmmp::work_view(work, n, false);
+  (void)pgmmp::agg_blocks(n);  // the occupancy query once, before any stream capture
   cudaError_t e = cudaMemsetAsync(w.err, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   return pgmmp::convert_weights(flat, w, st);

@@ -85,6 +85,108 @@ __device__ __forceinline__ void store_val<float>(float *p, float v) { *p = v; }
 template <>
 __device__ __forceinline__ void store_val<__nv_bfloat16>(__nv_bfloat16 *p, float v) { *p = __float2bfloat16(v); }
 
+// ---- building blocks of fused tile kernels (one CTA of THREADS threads per 128-row tile; thread t
+// owns row t of the tile in every epilogue: warp w reads TMEM lanes 32 w .. 32 w + 31)
+
+// Stages ROWS x K BF16 (rows of ld elements, 16-byte aligned; rows at or past `valid` as zeros)
+// into the K-major core-matrix layout at dst.
+template <int ROWS, int K>
+__device__ __forceinline__ void stage_bf16(uint8_t *dst, const __nv_bfloat16 *__restrict__ src, int ld, int valid) {
+  constexpr int KC = K / 8;
+  for (int c = threadIdx.x; c < ROWS * KC; c += blockDim.x) {
+    const int r = c / KC, kc = c - r * KC;
+    int4 v = make_int4(0, 0, 0, 0);
+    if (r < valid) v = *reinterpret_cast<const int4 *>(src + (size_t)r * ld + 8 * kc);
+    *reinterpret_cast<int4 *>(dst + tile_off(r, 8 * kc, K)) = v;
+  }
+}
+
+// The same with asynchronous copies (cp.async, 16 bytes each, zero-filled past `valid`): every
+// copy of the thread in flight at once; cp_async_wait_all() before the tile is used.
+template <int ROWS, int K>
+__device__ __forceinline__ void stage_async(uint8_t *dst, const __nv_bfloat16 *__restrict__ src, int ld, int valid) {
+  constexpr int KC = K / 8;
+  for (int c = threadIdx.x; c < ROWS * KC; c += blockDim.x) {
+    const int r = c / KC, kc = c - r * KC;
+    const bool ok = r < valid;
+    const __nv_bfloat16 *from = ok ? src + (size_t)r * ld + 8 * kc : src;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst + tile_off(r, 8 * kc, K))), "l"(from),
+                 "r"(ok ? 16 : 0)
+                 : "memory");
+  }
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// K / 16 MMAs (M = 128, N, BF16, FP32 accumulation into TMEM columns tmem..tmem + N - 1) from
+// K-major operands at shared addresses a0 (128 x K) and w0 (N x K); one thread issues them and
+// commits to the mbarrier bar.
+template <int K, int N>
+__device__ __forceinline__ void mma_issue(uint32_t tmem, uint32_t a0, uint32_t w0, uint32_t bar) {
+  const uint32_t id = idesc_bf16(TM, N);
+#pragma unroll
+  for (int ks = 0; ks < K / 16; ++ks) {
+    const uint64_t da = smem_desc(a0 + 256 * ks, 128, (K / 8) * 128);
+    const uint64_t dw = smem_desc(w0 + 256 * ks, 128, (K / 8) * 128);
+    const uint32_t acc = ks > 0 ? 1u : 0u;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "l"(da), "l"(dw), "r"(id), "r"(acc));
+  }
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// 16 FP32 columns c0 .. c0 + 15 of this warp's 32 TMEM lanes (lane = row of the thread).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *x) {
+  uint32_t v[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = __uint_as_float(v[j]);
+}
+
+// Generic-proxy writes of shared memory made visible to the tensor core, and the block's threads
+// (their tensor-memory reads included) ordered before what follows.
+__device__ __forceinline__ void tc_barrier() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Waits for phase `parity` of the MMAs' mbarrier; on giving up sets *err, waits once more (also
+// bounded) for the MMAs in flight, and returns false.
+__device__ __forceinline__ bool mma_wait(uint32_t bar, uint32_t parity, int *err) {
+  bool ok = mbar_wait(bar, parity, 1 << 22);
+  if (!ok) {
+    if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
+    mbar_wait(bar, parity, 1 << 22);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  return ok;
+}
+
+// Eight floats rounded to BF16 and stored as one 16-byte access.
+__device__ __forceinline__ void st_bf16x8(void *dst, const float *x) {
+  int4 o;
+  int *w = &o.x;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const __nv_bfloat162 b = __floats2bfloat162_rn(x[2 * k], x[2 * k + 1]);
+    w[k] = *reinterpret_cast<const int *>(&b);
+  }
+  *reinterpret_cast<int4 *>(dst) = o;
+}
+
 // C = act(A W^T + bias) (+ Res) for one 128-row tile per CTA.  A: M rows of lda BF16 (the first K
 // used), 16-byte aligned rows; W: N x K BF16 (K contiguous); bias: N floats or null; Res: null or
 // M rows of ldr BF16 added after the activation (a residual connection); C: M rows of ldc.
@@ -113,18 +215,11 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__rest
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
-  // stage the tile of A (rows past M as zeros) and W, 16 bytes (8 values of one core-matrix row) at a time
-  constexpr int KC = K / 8;
-  for (int c = tid; c < TM * KC; c += THREADS) {
-    const int r = c / KC, kc = c - r * KC;
-    int4 v = make_int4(0, 0, 0, 0);
-    if (m0 + r < M) v = *reinterpret_cast<const int4 *>(A + (size_t)(m0 + r) * lda + 8 * kc);
-    *reinterpret_cast<int4 *>(sA + tile_off(r, 8 * kc, K)) = v;
-  }
-  for (int c = tid; c < N * KC; c += THREADS) {
-    const int r = c / KC, kc = c - r * KC;
-    *reinterpret_cast<int4 *>(sW + tile_off(r, 8 * kc, K)) = *reinterpret_cast<const int4 *>(W + (size_t)r * K + 8 * kc);
-  }
+  // stage the tile of A (rows past M as zeros) and W, 16 bytes (8 values of one core-matrix row) per
+  // asynchronous copy
+  stage_async<TM, K>(sA, A + (size_t)m0 * lda, lda, M - m0);
+  stage_async<N, K>(sW, W, K, N);
+  cp_async_wait_all();
   // the tensor core reads shared memory through the async proxy
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -201,89 +296,6 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__rest
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL));
-}
-
-// ---- building blocks of fused tile kernels (one CTA of THREADS threads per 128-row tile; thread t
-// owns row t of the tile in every epilogue: warp w reads TMEM lanes 32 w .. 32 w + 31)
-
-// Stages ROWS x K BF16 (rows of ld elements, 16-byte aligned; rows at or past `valid` as zeros)
-// into the K-major core-matrix layout at dst.
-template <int ROWS, int K>
-__device__ __forceinline__ void stage_bf16(uint8_t *dst, const __nv_bfloat16 *__restrict__ src, int ld, int valid) {
-  constexpr int KC = K / 8;
-  for (int c = threadIdx.x; c < ROWS * KC; c += blockDim.x) {
-    const int r = c / KC, kc = c - r * KC;
-    int4 v = make_int4(0, 0, 0, 0);
-    if (r < valid) v = *reinterpret_cast<const int4 *>(src + (size_t)r * ld + 8 * kc);
-    *reinterpret_cast<int4 *>(dst + tile_off(r, 8 * kc, K)) = v;
-  }
-}
-
-// K / 16 MMAs (M = 128, N, BF16, FP32 accumulation into TMEM columns tmem..tmem + N - 1) from
-// K-major operands at shared addresses a0 (128 x K) and w0 (N x K); one thread issues them and
-// commits to the mbarrier bar.
-template <int K, int N>
-__device__ __forceinline__ void mma_issue(uint32_t tmem, uint32_t a0, uint32_t w0, uint32_t bar) {
-  const uint32_t id = idesc_bf16(TM, N);
-#pragma unroll
-  for (int ks = 0; ks < K / 16; ++ks) {
-    const uint64_t da = smem_desc(a0 + 256 * ks, 128, (K / 8) * 128);
-    const uint64_t dw = smem_desc(w0 + 256 * ks, 128, (K / 8) * 128);
-    const uint32_t acc = ks > 0 ? 1u : 0u;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-        "l"(da), "l"(dw), "r"(id), "r"(acc));
-  }
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-// 16 FP32 columns c0 .. c0 + 15 of this warp's 32 TMEM lanes (lane = row of the thread).
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *x) {
-  uint32_t v[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
-      "[%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int j = 0; j < 16; ++j) x[j] = __uint_as_float(v[j]);
-}
-
-// Generic-proxy writes of shared memory made visible to the tensor core, and the block's threads
-// (their tensor-memory reads included) ordered before what follows.
-__device__ __forceinline__ void tc_barrier() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-// Waits for phase `parity` of the MMAs' mbarrier; on giving up sets *err, waits once more (also
-// bounded) for the MMAs in flight, and returns false.
-__device__ __forceinline__ bool mma_wait(uint32_t bar, uint32_t parity, int *err) {
-  bool ok = mbar_wait(bar, parity, 1 << 22);
-  if (!ok) {
-    if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
-    mbar_wait(bar, parity, 1 << 22);
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  return ok;
-}
-
-// Eight floats rounded to BF16 and stored as one 16-byte access.
-__device__ __forceinline__ void st_bf16x8(void *dst, const float *x) {
-  int4 o;
-  int *w = &o.x;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const __nv_bfloat162 b = __floats2bfloat162_rn(x[2 * k], x[2 * k + 1]);
-    w[k] = *reinterpret_cast<const int *>(&b);
-  }
-  *reinterpret_cast<int4 *>(dst) = o;
 }
 
 // Launch: ceil(M / 128) CTAs of 128 threads with the tile's shared memory.
