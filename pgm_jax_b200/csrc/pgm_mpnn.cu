@@ -218,14 +218,15 @@ __global__ void __launch_bounds__(32 * AGG_WARPS, 4) k_aggregate(const __nv_bflo
                                                               int ldz, float *__restrict__ S) {
   __shared__ __align__(16) __nv_bfloat16 tile[AGG_WARPS][AGG_WIN][F];  // partner rows of a window
   __shared__ __align__(16) float4 lists[AGG_WARPS][2][AGG_WIN];        // list slots, double-buffered
+  __shared__ __align__(16) __nv_bfloat16 phis[AGG_WARPS][AGG_WIN][R];  // radial values of a window
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nw = gridDim.x * AGG_WARPS;
   int i = blockIdx.x * AGG_WARPS + wib;
   if (i >= n) return;  // whole warps leave: nothing below synchronises the block
   const int g = lane >> 2, tq = lane & 3;  // MMA fragment coordinates: row / column group
-  const float mu = g * (rg / (R - 1)), gam = ((R - 1) / rg) * ((R - 1) / rg);
   const uint32_t tbase = (uint32_t)__cvta_generic_to_shared(&tile[wib][0][0]);
   const uint32_t lbase = (uint32_t)__cvta_generic_to_shared(&lists[wib][0][0]);
+  const uint32_t pbase = (uint32_t)__cvta_generic_to_shared(&phis[wib][0][0]);
   int cur = 0;
   agg_list(lbase, edges + (size_t)i * emax, 0, emax, lane);
   cp_async_commit();
@@ -245,19 +246,41 @@ __global__ void __launch_bounds__(32 * AGG_WARPS, 4) k_aggregate(const __nv_bflo
         cp_async_wait<0>();
       }
       __syncwarp();
-      // per slot: length, cosine cutoff, partner (slots past the list: cutoff 0, partner i)
-      float dl[2], fcl[2];
+      // per slot (lane, 32 + lane): partner and the 8 radial values as BF16 into the warp's phi tile
+      // (phi_r = exp(-(t - r)^2) fc with t = 7 d / rg by the recurrence phi_r = phi_(r-1) q_r,
+      // q_r = exp(2 t - 2 r + 1): two exponentials per edge; slots past the list: zeros, partner i)
       int jl[2];
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
         const float4 ed = lists[wib][cur][32 * w + lane];
         const int j = __float_as_int(ed.w);
-        dl[w] = 0.f; fcl[w] = 0.f; jl[w] = i;
-        if (b0 + 32 * w + lane < ne && (unsigned)j < (unsigned)n) {
-          dl[w] = sqrtf(ed.x * ed.x + ed.y * ed.y + ed.z * ed.z);
-          fcl[w] = 0.5f * (cospif(dl[w] / rg) + 1.0f);
-          jl[w] = j;
+        const bool ok = b0 + 32 * w + lane < ne && (unsigned)j < (unsigned)n;
+        jl[w] = ok ? j : i;
+        float ph[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) ph[r] = 0.f;
+        if (ok) {
+          const float r2 = ed.x * ed.x + ed.y * ed.y + ed.z * ed.z;
+          const float d = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+          const float fc = 0.5f * (__cosf(3.14159265f * d / rg) + 1.0f);
+          const float t = d * ((R - 1) / rg);
+          float v = __expf(-t * t) * fc, q = __expf(2.0f * t - 1.0f);
+          ph[0] = v;
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            v *= q;
+            q *= 0.135335283f;  // exp(-2)
+            ph[r] = v;
+          }
         }
+        int4 pk;
+        int *pw = &pk.x;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const __nv_bfloat162 b2 = __floats2bfloat162_rn(ph[2 * k], ph[2 * k + 1]);
+          pw[k] = *reinterpret_cast<const int *>(&b2);
+        }
+        *reinterpret_cast<int4 *>(&phis[wib][32 * w + lane][0]) = pk;
       }
       const int nq = min(4, (ne - b0 + 15) >> 4);  // 16-edge quarters of the window in use
       // partner rows: lane l copies half l & 1 of edge 16 q + (l >> 1) of quarter q
@@ -269,32 +292,20 @@ __global__ void __launch_bounds__(32 * AGG_WARPS, 4) k_aggregate(const __nv_bflo
                      reinterpret_cast<const int4 *>(G + (size_t)j * F) + (lane & 1), true);
         }
       cp_async_commit();
-      // A fragments: row g (radial), columns 2 tq, 2 tq + 1 (+ 8) = edges of the quarter
-      uint32_t afr[4][2];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (q < nq) {
-#pragma unroll
-          for (int kk = 0; kk < 2; ++kk) {
-            float ph[2];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              const int src = 16 * (q & 1) + 8 * kk + 2 * tq + u;
-              const float d = __shfl_sync(0xffffffffu, dl[q >> 1], src), fc = __shfl_sync(0xffffffffu, fcl[q >> 1], src);
-              const float x = d - mu;
-              ph[u] = __expf(-gam * x * x) * fc;  // fc = 0 past the edges
-            }
-            const __nv_bfloat162 p2 = __floats2bfloat162_rn(ph[0], ph[1]);
-            afr[q][kk] = *reinterpret_cast<const uint32_t *>(&p2);
-          }
-        }
       cp_async_wait<0>();  // the partner rows (and the next atom's slots, issued earlier)
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         if (q < nq) {
-          // matrices: (edges 0-7, f 0-7), (edges 8-15, f 0-7), (edges 0-7, f 8-15), (edges 8-15, f 8-15)
           const int m = lane >> 3, rr = lane & 7;
+          // A: (edges 0-7, r 0-7) and (edges 8-15, r 0-7) of the phi tile, transposed: row g =
+          // radial, columns 2 tq, 2 tq + 1 (+ 8) = edges
+          uint32_t af[2];
+          const uint32_t pa = pbase + (uint32_t)((16 * q + rr + 8 * (m & 1)) * R * 2);
+          asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0, %1}, [%2];"
+                       : "=r"(af[0]), "=r"(af[1])
+                       : "r"(pa));
+          // B: (edges 0-7, f 0-7), (edges 8-15, f 0-7), (edges 0-7, f 8-15), (edges 8-15, f 8-15)
           const uint32_t addr = tbase + (uint32_t)(((16 * q + rr + 8 * (m & 1)) * F + 8 * (m >> 1)) * 2);
           uint32_t bq[4];
           asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
@@ -304,12 +315,12 @@ __global__ void __launch_bounds__(32 * AGG_WARPS, 4) k_aggregate(const __nv_bflo
               "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
               "{%0, %1, %2, %3};"
               : "+f"(c0[0]), "+f"(c0[1]), "+f"(c0[2]), "+f"(c0[3])
-              : "r"(afr[q][0]), "r"(0u), "r"(afr[q][1]), "r"(0u), "r"(bq[0]), "r"(bq[1]));
+              : "r"(af[0]), "r"(0u), "r"(af[1]), "r"(0u), "r"(bq[0]), "r"(bq[1]));
           asm volatile(
               "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
               "{%0, %1, %2, %3};"
               : "+f"(c1[0]), "+f"(c1[1]), "+f"(c1[2]), "+f"(c1[3])
-              : "r"(afr[q][0]), "r"(0u), "r"(afr[q][1]), "r"(0u), "r"(bq[2]), "r"(bq[3]));
+              : "r"(af[0]), "r"(0u), "r"(af[1]), "r"(0u), "r"(bq[2]), "r"(bq[3]));
         }
       __syncwarp();  // the tile and the slots are rewritten by the next window or atom
     }
@@ -443,7 +454,7 @@ __global__ void k_silu_round(const float *__restrict__ z, int n, int w, __nv_bfl
   if (t >= n * w) return;
   const int i = t / w, c = t - i * w;
   const float x = z[t];
-  u[(size_t)i * ldu + c] = __float2bfloat16(x / (1.0f + expf(-x)));
+  u[(size_t)i * ldu + c] = __float2bfloat16(__fdividef(x, 1.0f + __expf(-x)));
 }
 
 // dz = d * SiLU'(z) as FP32 and BF16.
@@ -652,7 +663,8 @@ struct Fused {
   static constexpr size_t A = (size_t)pgmtc::TM * KA * 2, W1 = (size_t)HID * KA * 2,
                           W2 = MODE == FM_IN ? 0 : (size_t)HID * HID * 2, UH = (size_t)pgmtc::TM * HID * 2,
                           W3 = (size_t)N3 * HID * 2;
-  static constexpr size_t bytes = A + W1 + W2 + UH + W3 + 64;
+  static constexpr size_t BIAS = (size_t)(HID + HID + COEF) * 4;  // b1, b2, b3 as FP32
+  static constexpr size_t bytes = A + W1 + W2 + UH + W3 + BIAS + 64;
 };
 template <int K_, int N_>
 struct KN {  // the shape of one product: K, N
@@ -678,7 +690,8 @@ __global__ void __launch_bounds__(pgmtc::THREADS) k_mp_fused(FusedArgs p) {
   using S = Fused<MODE>;
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t *sA = smem, *sW1 = sA + S::A, *sW2 = sW1 + S::W1, *sUH = sW2 + S::W2, *sW3 = sUH + S::UH;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sW3 + S::W3);
+  float *sb = reinterpret_cast<float *>(sW3 + S::W3);  // b1 (64), b2 (64), b3 (16)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sW3 + S::W3 + S::BIAS);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
   int *gave_up = reinterpret_cast<int *>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -714,8 +727,16 @@ __global__ void __launch_bounds__(pgmtc::THREADS) k_mp_fused(FusedArgs p) {
     st_bf16x8(sA + tile_off(tid, 0, IN), x);
     st_bf16x8(sA + tile_off(tid, 8, IN), x + 8);
   }
+  for (int t = tid; t < HID + HID + COEF; t += THREADS) {
+    float v = 0.f;  // absent biases (b2 of IN, b3 of W_g) as zeros
+    if (t < HID) v = p.b1[t];
+    else if (t < 2 * HID) { if (p.b2) v = p.b2[t - HID]; }
+    else if (p.b3) v = p.b3[t - 2 * HID];
+    sb[t] = v;
+  }
   cp_async_wait_all();
   tc_barrier();
+  const float *b1 = sb, *b2 = sb + HID, *b3 = sb + 2 * HID;
   const uint32_t tmem = *tslot, tl = tmem + ((uint32_t)(32 * warp) << 16), b = smem_u32(bar);
   uint32_t phase = 0;
   // a product into TMEM columns 0..N-1, then its wait (an abandoned wait stops the rest of the tile)
@@ -741,8 +762,8 @@ __global__ void __launch_bounds__(pgmtc::THREADS) k_mp_fused(FusedArgs p) {
       tmem_ld16(tl + c0, x);
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        const float z = x[j] + p.b1[c0 + j];
-        x[j] = z / (1.0f + __expf(-z));
+        const float z = x[j] + b1[c0 + j];
+        x[j] = __fdividef(z, 1.0f + __expf(-z));
       }
       // IN: h0 (global and the A operand of the last product); MID / OUT: u (A of the second)
       st_bf16x8(sUH + tile_off(tid, c0, HID), x);
@@ -765,10 +786,10 @@ __global__ void __launch_bounds__(pgmtc::THREADS) k_mp_fused(FusedArgs p) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           const float2 u = __bfloat1622float2(hr0[k]), v = __bfloat1622float2(hr1[k]);
-          x[2 * k] += p.b2[c0 + 2 * k] + u.x;
-          x[2 * k + 1] += p.b2[c0 + 2 * k + 1] + u.y;
-          x[8 + 2 * k] += p.b2[c0 + 8 + 2 * k] + v.x;
-          x[8 + 2 * k + 1] += p.b2[c0 + 8 + 2 * k + 1] + v.y;
+          x[2 * k] += b2[c0 + 2 * k] + u.x;
+          x[2 * k + 1] += b2[c0 + 2 * k + 1] + u.y;
+          x[8 + 2 * k] += b2[c0 + 8 + 2 * k] + v.x;
+          x[8 + 2 * k + 1] += b2[c0 + 8 + 2 * k + 1] + v.y;
         }
         st_bf16x8(sUH + tile_off(tid, c0, HID), x);  // the second product is complete: u is free
         st_bf16x8(sUH + tile_off(tid, c0 + 8, HID), x + 8);
@@ -778,18 +799,38 @@ __global__ void __launch_bounds__(pgmtc::THREADS) k_mp_fused(FusedArgs p) {
         }
       }
     }
+    if constexpr (MODE == FM_OUT) {
+      // the tile's channels (contiguous: 128 rows x 15 x 3 floats) into the free A and W1 regions,
+      // in flight during the last product; read back per row without bank conflicts (stride 45)
+      static_assert(S::A + S::W1 >= (size_t)TM * CH * 3 * 4, "room for the channels");
+      __syncthreads();  // every thread is past its residual reads of the A region
+      const int nbytes = valid * CH * 3 * 4;
+      const char *src = reinterpret_cast<const char *>(p.vec + (size_t)m0 * CH * 3);
+      for (int c = tid; c * 16 < nbytes; c += THREADS) {
+        const int sz = min(16, nbytes - 16 * c);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(sA + 16 * c)), "l"(src + 16 * c),
+                     "r"(sz)
+                     : "memory");
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     tc_barrier();
   }
-  if (product(P3{}, smem_u32(sUH), smem_u32(sW3))) {
+  const bool ok3 = product(P3{}, smem_u32(sUH), smem_u32(sW3));
+  if constexpr (MODE == FM_OUT) {  // the channels: own copies complete, then everyone's
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+  }
+  if (ok3) {
     float x[16];
     tmem_ld16(tl, x);  // by every thread of the warp (a .sync.aligned load), live rows or not
     if (!live) {
     } else if constexpr (MODE == FM_OUT) {
       float m[3] = {0.f, 0.f, 0.f};
-      const float *v = p.vec + (size_t)row * CH * 3;
+      const float *v = reinterpret_cast<const float *>(sA) + tid * CH * 3;
 #pragma unroll
       for (int c = 0; c < CH; ++c) {
-        const float w = x[c] + p.b3[c];
+        const float w = x[c] + b3[c];
 #pragma unroll
         for (int k = 0; k < 3; ++k) m[k] += w * v[3 * c + k];
       }

@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(const __nv_bfloat16 *__rest
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           x[j] = __uint_as_float(v[j]) + (bias ? bias[c0 + j] : 0.0f);
-          if (ACT == ACT_SILU) x[j] = x[j] / (1.0f + __expf(-x[j]));
+          if (ACT == ACT_SILU) x[j] = __fdividef(x[j], 1.0f + __expf(-x[j]));
           if (Res) x[j] += __bfloat162float(rb[j]);
         }
         OutT *dst = C + (size_t)row * ldc + c0;  // 16-byte aligned: ldc a multiple of 8, c0 of 16
