@@ -8,10 +8,11 @@ max|alpha r| / mean|alpha b| <= 1e-6.  A step is one captured CUDA graph: rigid-
 Langevin, the force call (rows, PME, CG as a device-side while loop, energy / forces / virial),
 closing kick.  `--workload water4096` runs the same line on 4,096 waters (4.966 nm, PME 96^3).
 
-The headline run starts every solve from the learned guess: plain-solver MD on the 4,096-water box
-writes the training pairs, the model trains on the GPU (outside the timed region), then the timed
-MD uses it.  Beside it, the same MD with plain CG from the previous step's dipoles (mu1) and from
-the reference's default mu4 predictor.
+The headline run starts every solve from the learned guess, the 2-layer message-passing model on the
+0.5 nm graph: plain-solver MD on the 4,096-water box writes the training frames, the model trains on
+the GPU (outside the timed region), then the timed MD uses it.  Beside it, the same MD with plain CG
+from the previous step's dipoles (mu1) and from the reference's default mu4 predictor, and with the
+per-atom MLP guess (`--model mlp` makes the MLP the headline and measures the network beside it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
 
@@ -49,6 +50,7 @@ BOXES = {
 }
 W = dict(BOXES["water32768"], name="water32768")  # the workload of this run (set from --workload)
 TRAIN_BOX = "water4096"  # the learned guess trains on pairs written by the plain solver on this box
+MODEL = ["mpnn"]  # the headline's learned guess (set from --model)
 
 
 def config() -> dict:
@@ -56,7 +58,8 @@ def config() -> dict:
     K = W["grid"]
     return {
         "workload": f"{n_w} rigid pGM3P-25 waters, {W['edge']} nm box, PME {K}^3 o6, rc 0.9 nm, beta 4.0/nm, Langevin "
-        "298 K gamma 2/ps, dt 1 fs, mixed precision, CG tol 1e-6 from the learned guess (trained on 4096-water frames)",
+        "298 K gamma 2/ps, dt 1 fs, mixed precision, CG tol 1e-6 from the learned guess "
+        f"({'2-layer message-passing model' if MODEL[0] == 'mpnn' else 'per-atom MLP'}, trained on 4096-water frames)",
         "atoms": W["atoms"],
         "pme_grid": [K, K, K],
         "cutoff_nm": 0.9,
@@ -276,8 +279,9 @@ def train_guess(rank: int, torch, kind: str) -> tuple:
         model = MPNNModel(seed=0, device=torch.cuda.current_device())
         model.train(train, iters=iters, lr=2e-3)
         pairs = sum(int(f["inv"].shape[0]) for f in train)
-        what = ("2-layer message-passing model on the 0.5 nm graph (64 hidden, 8 radial x 8 message features; "
-                "tcgen05 BF16 dense layers, FP32 accumulation), one frame per Adam step")
+        what = ("2-layer message-passing model on the 0.5 nm graph (64 hidden; continuous-filter convolutions: 16 "
+                "message features, filters over 8 radial functions; edge sums as BF16 warp MMAs, dense layers as fused "
+                "tcgen05 tiles, FP32 accumulation), one frame per Adam step")
     else:
         iters = 2000
         train = collect(md, frames)
@@ -387,6 +391,8 @@ def run_engine(args) -> None:
     del md
     # plain CG on the same workload: from the previous step's dipoles and from mu4
     plain = {p: run_plain(s, pos, H, rank, p, args, torch) for p in (("mu1", "mu4") if args.nn else ())}
+    other = "mlp" if args.model == "mpnn" else "mpnn"
+    alt = run_learned(s, pos, H, rank, other, args, torch) if (args.nn and args.other_model) else None
     acc = accuracy_vs_oracle(s, final, torch) if (rank == 0 and args.cpu_baseline) else None
     value = ws * ns_per_day(ms_max)
     if rank == 0:
@@ -415,6 +421,9 @@ def run_engine(args) -> None:
             line["learned_guess"] = train_info
             line["plain_cg"] = plain
             line["nn_over_plain_cg"] = {p: ns_per_day(ms_max) / v["value"] for p, v in plain.items()}
+            if alt:
+                alt["over_plain_cg"] = {p: alt["value"] / v["value"] for p, v in plain.items()}
+                line["learned_guess_" + other] = alt
         if args.cpu_baseline:
             r = cpu_reference(2, 1, budget_s=30.0)
             line["cpu_baseline"] = {"value": r["value"], "unit": "ns/day", "cores": r["cores"], "kind": "port",
@@ -503,6 +512,29 @@ def run_plain(s, pos, H, rank, predictor, args, torch) -> dict:
     return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "cg_iters_per_step": n_it, "steps": steps,
             "predictor": {"mu1": "previous step's dipoles", "mu4": "4 mu1 - 6 mu2 + 4 mu3 - mu4 (the reference's default)"}[
                 predictor]}
+
+
+def run_learned(s, pos, H, rank, kind, args, torch) -> dict:
+    """The same MD with the other learned guess (trained the same way), timed like the headline."""
+    from pgm_jax_b200.forcefield import PGMForceField
+    from pgm_jax_b200.md import RigidMD
+
+    model, info = train_guess(rank, torch, kind)
+    ff = PGMForceField(s, H, settings(predictor="nn"), device=torch.cuda.current_device())
+    md = RigidMD(ff, pos, H, temperature=TEMP, dt_fs=DT_FS, gamma_ps=GAMMA, seed=1 + rank)
+    equilibrate(md)
+    model.install(ff)
+    for _ in range(max(1, args.warmup) + 4):
+        md.step()
+    md.capture()
+    md.run(3)
+    md.stream.synchronize()
+    steps = max(10, min(args.steps, 300))
+    ms, n_it = timed_replays(md, steps, torch)
+    fb = int(ff.nn_fallback_stats()["fallbacks"][0])
+    del md, ff, model
+    return {"value": ns_per_day(ms), "unit": "ns/day", "ms_per_step": ms, "cg_iters_per_step": n_it, "steps": steps,
+            "model": info["model"], "train_seconds": info["seconds"], "fallbacks_in_run": fb}
 
 
 def run_e2e(md, ff, steps, torch, lib, _lib, state_on_device: bool = True) -> dict:
@@ -765,10 +797,11 @@ def main() -> None:
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-nn", dest="nn", action="store_false", help="plain mu4 CG only, without the learned guess")
-    ap.add_argument("--model", default="mlp", choices=["mlp", "mpnn"],
-                    help="the learned guess: the per-atom MLP on the graph's features (the default: the same "
-                    "held-out error as the message-passing model at a fraction of its cost) or the 2-layer "
-                    "message-passing model")
+    ap.add_argument("--model", default="mpnn", choices=["mpnn", "mlp"],
+                    help="the learned guess of the headline: the 2-layer message-passing model (default) or the "
+                    "per-atom MLP on the graph's features; the other one is measured beside it")
+    ap.add_argument("--no-other-model", dest="other_model", action="store_false",
+                    help="skip the MD with the other learned guess")
     ap.add_argument("--workload", default="water32768", choices=["water32768", "water4096", "batch", "pimd", "npt"],
                     help="water32768: the headline; water4096 the same line on the smaller box; the others print "
                     "their own line (one GPU)")
@@ -779,6 +812,7 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    MODEL[0] = args.model
     if args.elec_cutoff:
         from pgm_jax_b200.forcefield import elec_cutoff_settings
 
