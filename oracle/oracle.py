@@ -36,7 +36,7 @@ class _Set(C.Structure):
         ("order", _i), ("tol", _d), ("max_iter", _i), ("predictor", _i), ("fused", _i), ("norm_refresh", _i),
         ("peek", _d), ("nthreads", _i), ("elec_cutoff", _d),
         ("iel", _i), ("iel_order", _i), ("iel_kappa", _d), ("iel_alpha", _d), ("iel_omega", _d), ("iel_precond", _i),
-        ("iel_iter", _i), ("iel_shadow", _i),
+        ("iel_iter", _i), ("iel_shadow", _i), ("local_cut", _d), ("local_niter", _i),
     ]
 
 
@@ -111,7 +111,7 @@ class Oracle:
             float("nan") if st.get("iel_kappa") is None else float(st["iel_kappa"]),
             float("nan") if st.get("iel_alpha") is None else float(st["iel_alpha"]), float(st.get("iel_omega", 1.0)),
             {"jacobi": 0, "block": 1}[st.get("iel_precond", "block")], int(st.get("iel_iter", 1)),
-            int(st.get("iel_shadow", True)),
+            int(st.get("iel_shadow", True)), float(st.get("local_cut", 0.3)), int(st.get("local_niter", 0)),
         )
         self.iel = st.get("iel", "none") != "none"
 

@@ -693,15 +693,66 @@ static double dot(const double *a, const double *b, int m) {
     return s;
 }
 
-/* Jacobi PCG with the Polak-Ribiere beta, pmemd-pgm's max-norm test and the peek step
- * (forcefield.py:1714-1821). */
+/* The short-range operator of the local preconditioner: A_loc v = v / alpha + the row field of v over
+ * the electrostatic row entries closer than local_cut (forcefield.py:1771-1772). */
+static void apply_A_loc(ctx_t *C, const double *v, double *out) {
+    const rows_t *R = &C->R;
+    int n = C->sys->n;
+    const double lc2 = C->s->local_cut * C->s->local_cut;
+#pragma omp parallel for schedule(dynamic, 32)
+    for (int i = 0; i < n; ++i) {
+        double f[3] = {0, 0, 0};
+        for (long long o = R->start[i]; o < R->start[i + 1]; ++o) {
+            const double *x = R->x + 3 * o;
+            if (!R->we[o] || x[0] * x[0] + x[1] * x[1] + x[2] * x[2] >= lc2) continue;
+            const double *G = R->G + 4 * o, *dk = v + 3 * R->k[o];
+            double dkx = dk[0] * x[0] + dk[1] * x[1] + dk[2] * x[2];
+            for (int j = 0; j < 3; ++j) f[j] += -G[2] * dkx * x[j] + G[1] * dk[j];
+        }
+        for (int j = 0; j < 3; ++j) out[3 * i + j] = v[3 * i + j] / C->sys->alpha[i] + f[j];
+    }
+}
+
+/* z = M^-1 r: Jacobi z = alpha r, refined with local_niter > 0 by that many inner CG iterations on
+ * A_loc from z (forcefield.py:1766-1792). */
+static void precond(ctx_t *C, const double *r, double *z) {
+    int n = C->sys->n, m = 3 * n;
+    const double *al = C->sys->alpha;
+    for (int i = 0; i < m; ++i) z[i] = al[i / 3] * r[i];
+    if (C->s->local_niter <= 0) return;
+    double *rr = malloc(sizeof(double) * m), *p = malloc(sizeof(double) * m), *Ap = malloc(sizeof(double) * m);
+    apply_A_loc(C, z, Ap);
+    for (int i = 0; i < m; ++i) {
+        rr[i] = r[i] - Ap[i];
+        p[i] = al[i / 3] * rr[i];
+    }
+    double rz = dot(rr, p, m);
+    for (int it = 0; it < C->s->local_niter; ++it) {
+        apply_A_loc(C, p, Ap);
+        double a = rz / fmax(dot(p, Ap, m), 1e-300), rzn = 0.0;
+        for (int i = 0; i < m; ++i) {
+            z[i] += a * p[i];
+            rr[i] -= a * Ap[i];
+            rzn += rr[i] * al[i / 3] * rr[i];
+        }
+        double b = rzn / fmax(rz, 1e-300);
+        for (int i = 0; i < m; ++i) p[i] = al[i / 3] * rr[i] + b * p[i];
+        rz = rzn;
+    }
+    free(rr);
+    free(p);
+    free(Ap);
+}
+
+/* PCG (Jacobi, or the local preconditioner: flexible) with the Polak-Ribiere beta, pmemd-pgm's
+ * max-norm test and the peek step (forcefield.py:1714-1821). */
 static void cg_to(ctx_t *C, double *x, double *r, double norm, double tol, int max_iter, int *iters, double *resid) {
     const pgmo_settings *s = C->s;
     int n = C->sys->n, m = 3 * n;
     const double *al = C->sys->alpha;
     double *z = malloc(sizeof(double) * m), *p = malloc(sizeof(double) * m), *Ap = malloc(sizeof(double) * m),
            *rn = malloc(sizeof(double) * m);
-    for (int i = 0; i < m; ++i) z[i] = al[i / 3] * r[i];
+    precond(C, r, z);
     memcpy(p, z, sizeof(double) * m);
     double rz = dot(r, z, m);
     double err = 0.0;
@@ -718,12 +769,11 @@ static void cg_to(ctx_t *C, double *x, double *r, double norm, double tol, int m
         }
         double num = 0.0, rzn = 0.0;
         err = 0.0;
+        precond(C, rn, z);
         for (int i = 0; i < m; ++i) {
-            double zn = al[i / 3] * rn[i];
-            num += zn * (rn[i] - r[i]);
-            rzn += rn[i] * zn;
-            z[i] = zn;
-            err = fmax(err, fabs(zn));
+            num += z[i] * (rn[i] - r[i]);
+            rzn += rn[i] * z[i];
+            err = fmax(err, fabs(al[i / 3] * rn[i]));
         }
         err /= norm;
         double beta = num / fmax(rz, 1e-300);

@@ -58,6 +58,8 @@ typedef struct {
     int iel_precond;       /* 0 jacobi, 1 block (molecules of 2..8 atoms) */
     int iel_iter;          /* scf: CG iterations per step (0: to tol) */
     int iel_shadow;        /* 0scf: energy and forces of the shadow potential */
+    double local_cut;      /* local preconditioner: cutoff of its short-range rows [nm] (forcefield.py:302-305) */
+    int local_niter;       /* its inner CG iterations; 0: Jacobi */
 } pgmo_settings;
 
 typedef struct {

@@ -286,3 +286,45 @@ def frame_errors(model: MPNNModel, frames: list) -> dict:
         se["mu1"] += float(torch.sum((f["prev"] - t) ** 2))
         cnt += t.numel()
     return {k: float(np.sqrt(v / cnt)) for k, v in se.items()}
+
+
+def random_frame(n: int, degree: int = 52, seed: int = 0, device: int = 0) -> dict:
+    """A seeded synthetic frame of the message-passing model's inputs on the device: n atoms with
+    `degree` edges each (random partners, lengths uniform in [0.1, 0.5) nm, random directions), the
+    16 invariants N(0, 1) and the 15 vector channels N(0, 0.02^2) -- the sizes of a water box's
+    0.5 nm graph (about 52 edges per atom), for timing and profiling the inference kernels."""
+    dev = torch.device("cuda", device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    edges = torch.zeros((n, EMAX, 4), device=dev)
+    d = torch.randn((n, degree, 3), device=dev, generator=g)
+    d = d / d.norm(dim=-1, keepdim=True) * (0.1 + 0.4 * torch.rand((n, degree, 1), device=dev, generator=g))
+    edges[:, :degree, :3] = d
+    edges[:, :degree, 3] = torch.randint(0, n, (n, degree), device=dev, generator=g, dtype=torch.int32).view(torch.float32)
+    return {"inv": torch.randn((n, N_IN), device=dev, generator=g),
+            "vec": 0.02 * torch.randn((n, N_CH, 3), device=dev, generator=g),
+            "edges": edges, "counts": torch.full((n,), degree, dtype=torch.int32, device=dev),
+            "target": 1e-4 * torch.randn((n, 3), device=dev, generator=g)}
+
+
+def _time_inference(n: int, reps: int = 20) -> None:
+    """Mean time of the message-passing model's inference (pgm_mpnn_predict: weight conversion and
+    the five kernels) on a synthetic frame of n atoms, CUDA events on the current stream."""
+    frame = random_frame(n)
+    m = MPNNModel()
+    for _ in range(3):
+        m.predict(frame)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        m.predict(frame)
+    b.record()
+    torch.cuda.synchronize()
+    print(f"message-passing inference, {n} atoms: {a.elapsed_time(b) / reps * 1e3:.1f} us per call")
+
+
+if __name__ == "__main__":
+    import sys
+
+    _time_inference(int(sys.argv[1]) if len(sys.argv) > 1 else 98304)

@@ -157,3 +157,21 @@ def test_oracle_matches_reference_golden_pgm3p25_512(pgm3p25_512_system, golden_
     assert np.sqrt(np.sum((r["mu"] - mu) ** 2) / np.sum(mu**2)) <= 1e-8
     W = g["double.strain"]
     assert np.abs(r["virial"] - W).max() <= 1e-6 * np.abs(W).max()
+
+
+def test_oracle_local_preconditioner_same_solution_fewer_iterations(pgm3p25_512_system, golden_pgm3p25_512):
+    """The local preconditioner (inner CG on the row entries closer than local_cut, flexible PCG;
+    forcefield.py:1766-1811) converges to the same dipoles as Jacobi PCG in fewer outer
+    iterations, and local_niter = 0 is Jacobi itself (the golden's 9 iterations)."""
+    from conftest import PGM3P25_512_SETTINGS
+
+    g = golden_pgm3p25_512
+    out = {}
+    for ni in (0, 2):
+        st = dict(PGM3P25_512_SETTINGS, dipole_tol=1e-9, max_iter=100, local_cut=0.3, local_niter=ni)
+        out[ni] = O.Oracle(pgm3p25_512_system, st).compute(g["pos"], g["box"])
+    assert out[2]["iterations"] < out[0]["iterations"]
+    assert np.abs(out[2]["mu"] - out[0]["mu"]).max() <= 1e-7 * np.abs(out[0]["mu"]).max()
+    assert abs(out[2]["energy"]["total"] - out[0]["energy"]["total"]) <= 1e-10 * abs(out[0]["energy"]["total"])
+    st = dict(PGM3P25_512_SETTINGS, local_niter=0)
+    assert O.Oracle(pgm3p25_512_system, st).compute(g["pos"], g["box"])["iterations"] == int(g["double.iterations"])
