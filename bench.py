@@ -72,6 +72,8 @@ def config() -> dict:
         "equilibration": f"{W['equil_steps']} steps of 1 fs at gamma 20/ps from the lattice start, before timing",
         **({"split_rows": f"electrostatics {SPLIT['elec_cutoff']} nm, beta {SPLIT['ewald_beta']:.4f}/nm, LJ 0.9 nm"}
            if SPLIT else {}),
+        "preconditioner": (f"local: {LOCAL['local_niter']} inner CG iterations on the row entries inside 0.3 nm "
+                           "(forcefield.py:1766-1792), every arm" if LOCAL["local_niter"] else "Jacobi (the reference's default)"),
     }
 
 
@@ -97,12 +99,16 @@ ROWFIELD_NCU_DRAM_BYTES, ROWFIELD_NCU_PAIRS = 93.654784e6 + 3.39328e6, 3.745e6
 SPLIT: dict = {}  # --elec-cutoff: split rows (elec_cutoff, ewald_beta for it; the meshes fit its spacing)
 
 
+LOCAL = {"local_niter": 0}  # --local-niter: the local preconditioner in every arm (0: Jacobi, the reference's default)
+
+
 def settings(precision="mixed", predictor="mu4", grid=None):
     from pgm_jax_b200.forcefield import MDSettings
 
     K = W["grid"] if grid is None else grid
     return MDSettings(precision=precision, cutoff=0.9, ewald_beta=SPLIT.get("ewald_beta", 4.0), pme_grid=(K, K, K),
-                      pme_order=6, dipole_tol=TOL, max_iter=100, predictor=predictor, elec_cutoff=SPLIT.get("elec_cutoff"))
+                      pme_order=6, dipole_tol=TOL, max_iter=100, predictor=predictor, elec_cutoff=SPLIT.get("elec_cutoff"),
+                      local_cut=0.3, local_niter=LOCAL["local_niter"])
 
 
 def headline_box(seed: int = 0):
@@ -807,12 +813,15 @@ def main() -> None:
                     "their own line (one GPU)")
     ap.add_argument("--equil-steps", type=int, default=None,
                     help="relaxation steps of the lattice start before timing (default: the workload's)")
+    ap.add_argument("--local-niter", type=int, default=0,
+                    help="the local preconditioner (inner CG iterations on the entries inside 0.3 nm) in every arm")
     ap.add_argument("--elec-cutoff", type=float, default=None,
                     help="split rows: electrostatics cutoff [nm] below the 0.9 nm LJ cutoff (Ewald coefficient for it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     MODEL[0] = args.model
+    LOCAL["local_niter"] = args.local_niter
     if args.elec_cutoff:
         from pgm_jax_b200.forcefield import elec_cutoff_settings
 

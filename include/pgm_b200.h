@@ -43,6 +43,8 @@ typedef enum {
 #define PGM_STATUS_NONFINITE    0x4u   /* non-finite energy */
 #define PGM_STATUS_BAD_BOX      0x8u   /* box not lower triangular / too small for the cutoff */
 #define PGM_STATUS_LIST_OVERFLOW 0x10u /* an atom had more candidates within cutoff + skin than the list capacity */
+#define PGM_STATUS_SHORT_OVERFLOW 0x20u /* local preconditioner: an atom had more than 48 entries inside local_cut;
+                                          the first 48 were used (results valid, iterations may differ) */
 
 /* Settings of one handle: the MDSettings fields of the path (forcefield.py:386-516). */
 typedef struct {
@@ -89,6 +91,13 @@ typedef struct {
     int iel_no_shadow;  /* 0scf: 0 the energy and forces of the shadow potential U(R, x + delta) -
                            U_es(0, delta) (the reference's default, exact and conserved); 1 the
                            fixed-dipole energy and forces at mu */
+    /* The local preconditioner of the CG (Induction.local_cut / local_niter, forcefield.py:302-305,
+       1766-1792): z = M^-1 r by local_niter inner CG iterations on alpha^-1 v + the row field of v
+       over the entries closer than local_cut (at most 48 per atom: PGM_STATUS_SHORT_OVERFLOW),
+       started from alpha r; the outer CG is then flexible.  local_niter 0: Jacobi (the default).
+       Not with iel. */
+    double local_cut;   /* [nm], below the (electrostatics) cutoff */
+    int local_niter;    /* 0..8 */
 } PgmSettings;
 
 /* One system of the batch: topology and parameters (host arrays, copied at creation). */
@@ -243,7 +252,9 @@ PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, floa
  * rowfield_lanes, the lanes that share one neighbour row in the CG matvec's row stream (32: a warp
  * per atom; 16, 8: two or four atoms per warp); forces_blocks_per_sm, the minimum resident blocks of
  * 256 threads the force pass is compiled for (2, 3, 4: registers against warps); sweep_early, the
- * order of the CG sweep's concurrent parts.  Unless fixed by
+ * order of the CG sweep's concurrent parts; rowfield_grid, the row field beside the FFT chain on
+ * every SM (0) or on 1 or 2 blocks per SM at the highest priority, the FFT passes filling the rest
+ * of each SM.  Unless fixed by
  * pgm_set_tuning, the first pgm_compute that is not being captured times every variant on its own
  * rows (CUDA events on its stream, the mean of 10 launches after one) and keeps the fastest;
  * handles of the same precision, order, atoms, row capacity and grid size in one process share the
@@ -259,11 +270,13 @@ typedef struct {
                                   (on p), 1 at the start of the sweep (on z; the rows of p = z +
                                   beta p_prev combined in the gather) */
     double sweep_ms[2];        /* timed sweeps of the two schedules [ms] */
+    int rowfield_grid;         /* 0 (one block per 8 rows), 1 or 2 blocks per SM beside the FFT chain */
+    double grid_ms[3];         /* timed sweeps with rowfield_grid 0, 1, 2 [ms] */
 } PgmTuning;
 PgmStatus pgm_tuning(PgmHandle *h, PgmTuning *out);
-/* Fix the variants (0, or -1 for sweep_early, leaves one as it is; all so: autotune again at the
- * next direct step). */
-PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm, int sweep_early);
+/* Fix the variants (0, or -1 for sweep_early and rowfield_grid, leaves one as it is; all so:
+ * autotune again at the next direct step). */
+PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm, int sweep_early, int rowfield_grid);
 /* Time the variants now on the last step's rows (synchronises the stream). */
 PgmStatus pgm_autotune(PgmHandle *h, void *stream);
 

@@ -35,13 +35,14 @@ STATUS_CG_MAXITER = 0x2
 STATUS_NONFINITE = 0x4
 STATUS_BAD_BOX = 0x8
 STATUS_LIST_OVERFLOW = 0x10
+STATUS_SHORT_OVERFLOW = 0x20
 
 
 class PgmTuning(C.Structure):
     _fields_ = [
         ("rowfield_lanes", C.c_int), ("forces_blocks_per_sm", C.c_int), ("rowfield_ms", C.c_double * 3),
         ("forces_ms", C.c_double * 3), ("tuned", C.c_int), ("from_cache", C.c_int), ("sweep_early", C.c_int),
-        ("sweep_ms", C.c_double * 2),
+        ("sweep_ms", C.c_double * 2), ("rowfield_grid", C.c_int), ("grid_ms", C.c_double * 3),
     ]
 
 
@@ -53,7 +54,7 @@ class PgmSettings(C.Structure):
         ("row_capacity", C.c_int), ("skin", C.c_double), ("list_capacity", C.c_int), ("elec_cutoff", C.c_double),
         ("elec_capacity", C.c_int), ("iel", C.c_int), ("iel_order", C.c_int), ("iel_custom", C.c_int),
         ("iel_kappa", C.c_double), ("iel_alpha", C.c_double), ("iel_omega", C.c_double), ("iel_precond", C.c_int),
-        ("iel_iter", C.c_int), ("iel_no_shadow", C.c_int),
+        ("iel_iter", C.c_int), ("iel_no_shadow", C.c_int), ("local_cut", C.c_double), ("local_niter", C.c_int),
     ]
 
 
@@ -166,7 +167,7 @@ def load(path: str | None = None):
     lib.pgm_iel_len.argtypes = [C.c_int]
     lib.pgm_iel_len.restype = C.c_int
     lib.pgm_tuning.argtypes = [H, C.POINTER(PgmTuning)]
-    lib.pgm_set_tuning.argtypes = [H, C.c_int, C.c_int, C.c_int]
+    lib.pgm_set_tuning.argtypes = [H, C.c_int, C.c_int, C.c_int, C.c_int]
     lib.pgm_autotune.argtypes = [H, vp]
     for n in ("pgm_tuning", "pgm_set_tuning", "pgm_autotune"):
         getattr(lib, n).restype = C.c_int

@@ -120,7 +120,7 @@ struct EngineBase {
   virtual void set_mpnn(const float *w, int nparam, float sigma, float rg) = 0;
   virtual void nn_graph(cudaStream_t st, float4 *edges, int *counts, int emax) = 0;
   virtual void set_nn_fallback(double factor) = 0;
-  virtual void set_tuning(int rowfield_lanes, int forces_blocks, int sweep_early) = 0;
+  virtual void set_tuning(int rowfield_lanes, int forces_blocks, int sweep_early, int rowfield_grid) = 0;
   virtual void autotune(cudaStream_t st) = 0;
   virtual PgmTuning tuning() const = 0;
   virtual void nn_fallback_stats(long long *fallbacks, double *ref_err) = 0;
@@ -241,6 +241,12 @@ struct Engine : EngineBase {
   DBuf<int> nn_valid;  // nn_bl holds a previous step
   DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by the row build)
   DBuf<int> nn_ne;
+  // local preconditioner (set.local_niter > 0): short entries' row slots and counts, their compact
+  // copy (entry-major), the inner CG's vectors
+  static constexpr int SH_MAX = 48;
+  DBuf<int> sh_slot, sh_n, c_k;
+  DBuf<T> c_x, c_y, c_z, c_g1, c_g2;
+  DBuf<pgm::v4<T>> LRR, LZZ, LP0, LP1, DRv;
   static constexpr int NN_EMAX = 128;
   float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
   int *h_any = nullptr;
@@ -252,6 +258,7 @@ struct Engine : EngineBase {
   bool in_body = false;  // enqueueing the body of a conditional node (its own capture sequence)
   bool overlap = true;  // row field on a second stream beside the FFT chain
   int prio_hi = 0;      // the device's highest stream priority (the learned guess's kernels)
+  int nsm = 148;        // multiprocessors of the device
   long long per_iter = 0;
 
   ~Engine() {
@@ -301,6 +308,11 @@ struct Engine : EngineBase {
     a.max_count = dmax.p;
     a.mce = mce; a.rnv = split ? rnv.p : nullptr; a.rce2 = rc_e * rc_e;
     a.nn_e4 = nn_e4.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
+    if (set.local_niter > 0) {
+      a.sh_slot = sh_slot.p; a.sh_n = sh_n.p; a.sh_max = SH_MAX; a.lc2 = set.local_cut * set.local_cut;
+      a.c_k = c_k.p; a.c_x = c_x.p; a.c_y = c_y.p; a.c_z = c_z.p; a.c_g1 = c_g1.p; a.c_g2 = c_g2.p;
+      a.LRR = LRR.p; a.LZZ = LZZ.p; a.LP0 = LP0.p; a.LP1 = LP1.p; a.DR = DRv.p;
+    }
     a.X = X.p; a.R = R.p; a.Z = Z.p; a.P = Pv.p; a.AP = AP.p; a.B = Bv.p; a.D = D.p; a.F = Fv.p; a.Fp = Fpv.p;
     a.Q = Q.p; a.Phi = Phi.p; a.Ginf = Ginf.p; a.C = C.p; a.tw = tw.p; a.bmod = bmod.p;
     a.forces = forces; a.dEdd = dEdd.p;
@@ -597,6 +609,13 @@ struct Engine : EngineBase {
     nn_w.alloc(pgmnn::NN_NPARAM); nn_wb.alloc(pgmnn::NN_WB_ELEMS); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
     nn_mu.alloc((size_t)nt * 3); nn_chan.alloc((size_t)nt * pgm::NN_CHAN); nn_bl.alloc(nt); nn_valid.alloc(1);
     if (set.predictor == 5) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
+    if (set.local_niter > 0) {
+      const size_t ns = (size_t)nt * SH_MAX;
+      sh_slot.alloc(ns); sh_n.alloc(nt); c_k.alloc(ns);
+      c_x.alloc(ns); c_y.alloc(ns); c_z.alloc(ns); c_g1.alloc(ns); c_g2.alloc(ns);
+      LRR.alloc(nt); LZZ.alloc(nt); LP0.alloc(nt); LP1.alloc(nt); DRv.alloc(nt);
+      CK(cudaMemset(sh_n.p, 0, sizeof(int) * nt));
+    }
     CK(cudaMemset(nn_valid.p, 0, sizeof(int)));
     CK(cudaMallocHost(&h_any, sizeof(int)));
     CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
@@ -607,6 +626,11 @@ struct Engine : EngineBase {
     CK(cudaEventCreateWithFlags(&ev_join_b, cudaEventDisableTiming));
     int prio_lo = 0;
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    {
+      int d = 0;
+      CK(cudaGetDevice(&d));
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d));
+    }
     CK(cudaStreamCreateWithPriority(&nn_st, cudaStreamNonBlocking, prio_hi));
     CK(cudaEventCreateWithFlags(&ev_nn_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_nn_join, cudaEventDisableTiming));
@@ -714,14 +738,21 @@ struct Engine : EngineBase {
   // The tuned kernels: the CG matvec's row stream k_rowfield (lanes per row 32 / 16 / 8: how a
   // neighbour row is split over a warp) and the force pass k_forces (at least 2 / 3 / 4 blocks of
   // 256 threads per SM: registers against resident warps).
+  // beside: forked beside the FFT chain, where the tuned grid limit (tune.rowfield_grid blocks per
+  // SM, at the highest priority) applies; 0 or not beside: one block per 8 rows.
   template <bool WITH_Q, int ACT>
-  void rowfield(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin, pgm::v4<T> *out, bool pdl, int lpr = 0) {
+  void rowfield(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin, pgm::v4<T> *out, bool pdl, int lpr = 0,
+                bool beside = false, int grid_per_sm = -1) {
+    const int g = grid_per_sm >= 0 ? grid_per_sm : tune.rowfield_grid;
     auto go = [&](auto L) {
       constexpr int LPR = decltype(L)::value;
       if (pdl) {
-        launch_pdl(pgm::k_rowfield<T, WITH_Q, ACT, LPR>, nwblk, 8 * LPR, 0, st, a, vin, out);
+        launch_pdl(pgm::k_rowfield<T, WITH_Q, ACT, LPR>, nwblk, 8 * LPR, 0, st, a, vin, out, nwblk);
+      } else if (beside && g > 0) {
+        launch_prio(pgm::k_rowfield<T, WITH_Q, ACT, LPR>, (unsigned)std::min(nwblk, g * nsm), 8 * LPR, 0, st, prio_hi, a,
+                    vin, out, nwblk);
       } else {
-        pgm::k_rowfield<T, WITH_Q, ACT, LPR><<<nwblk, 8 * LPR, 0, st>>>(a, vin, out);
+        pgm::k_rowfield<T, WITH_Q, ACT, LPR><<<nwblk, 8 * LPR, 0, st>>>(a, vin, out, nwblk);
         check_launch();
       }
     };
@@ -747,12 +778,13 @@ struct Engine : EngineBase {
     else if (b == 4) go(std::integral_constant<int, 4>{});
     else go(std::integral_constant<int, 3>{});
   }
-  void set_tuning(int lanes, int blocks, int early) override {
+  void set_tuning(int lanes, int blocks, int early, int grid) override {
     ++generation;  // captured steps hold the old variants
-    tune_fixed = lanes > 0 || blocks > 0 || early >= 0;
+    tune_fixed = lanes > 0 || blocks > 0 || early >= 0 || grid >= 0;
     if (lanes > 0) tune.rowfield_lanes = lanes;
     if (blocks > 0) tune.forces_blocks_per_sm = blocks;
     if (early >= 0) tune.sweep_early = early;
+    if (grid >= 0) tune.rowfield_grid = grid;
     if (!tune_fixed) tune.tuned = 0;  // autotune again at the next direct step
   }
   PgmTuning tuning() const override { return tune; }
@@ -804,6 +836,15 @@ struct Engine : EngineBase {
         tune.sweep_ms[v] = time([&] { sweep<false, true, 0, 1>(st, a, Pv.p, AP.p); });
       }
       tune.sweep_early = tune.sweep_ms[1] < tune.sweep_ms[0] ? 1 : 0;
+      // the row field beside the FFT chain on all SMs, or on 1 or 2 blocks per SM at the highest
+      // priority (the FFT passes fill the rest of each SM)
+      int bg = 0;
+      for (int v = 0; v < 3; ++v) {
+        tune.rowfield_grid = v;
+        tune.grid_ms[v] = time([&] { sweep<false, true, 0, 1>(st, a, Pv.p, AP.p); });
+        if (tune.grid_ms[v] < tune.grid_ms[bg]) bg = v;
+      }
+      tune.rowfield_grid = bg;
     }
     CK(cudaMemsetAsync(Q.p, 0, sizeof(T) * rgrid, st));  // leave the spread grid cleared
     launches = l0;
@@ -936,6 +977,7 @@ struct Engine : EngineBase {
       else if (which == 4) {
         pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
         pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a);
+        if (set.local_niter > 0) pgm::k_short_compact<T><<<grid1(nt), 256, 0, st>>>(a);
       }
       else if (which == 5 || which == 6) {  // the first FFT pass (plane or k3), after the spread with 6
         if (which == 6) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
@@ -1067,6 +1109,7 @@ struct Engine : EngineBase {
     launch_pdl(pgm::k_rows<T>, nwblk, 256, 0, st, a);
     if (nn_hist) nn_fork(st, a, nn_hist);
     launch_pdl(pgm::k_row_kernels<T>, (int)(((size_t)nt * mc + 255) / 256), 256, 0, st, a);
+    if (set.local_niter > 0) launch_pdl(pgm::k_short_compact<T>, grid1(nt), 256, 0, st, a);
     launch_pdl(pgm::k_influence<T>, (int)std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st, a, (long long)cgrid);
   }
 
@@ -1119,7 +1162,7 @@ struct Engine : EngineBase {
       // direction it takes z (the rows of p = z + beta p_prev are combined in the gather)
       CK(cudaEventRecord(ef, st));
       CK(cudaStreamWaitEvent(ax, ef, 0));
-      rowfield<WITH_Q, ACT>(ax, a, UPDATE_P ? Z.p : vin, Fv.p, false);
+      rowfield<WITH_Q, ACT>(ax, a, UPDATE_P ? Z.p : vin, Fv.p, false, 0, true);
       CK(cudaEventRecord(ej, ax));
       launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
       fft_chain(st, a, ACT, false);
@@ -1130,7 +1173,7 @@ struct Engine : EngineBase {
     launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
     CK(cudaEventRecord(ef, st));
     CK(cudaStreamWaitEvent(ax, ef, 0));
-    rowfield<WITH_Q, ACT>(ax, a, vin, Fv.p, false);
+    rowfield<WITH_Q, ACT>(ax, a, vin, Fv.p, false, 0, true);
     CK(cudaEventRecord(ej, ax));
     fft_chain(st, a, ACT, false);
     CK(cudaStreamWaitEvent(st, ej, 0));
@@ -1138,9 +1181,35 @@ struct Engine : EngineBase {
     launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false>, nwblk, 256, 0, st, a, vin, out);
   }
 
-  // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check.
+  // The local preconditioner's chain z = M^-1 r (k_lp_start, then per inner iteration k_lp_ap and
+  // k_lp_step), for the systems ACT selects (0 all, 1 iterating, 3 falling back); MODE 0 ends with
+  // p = z and r.z (a start), MODE 1 with the outer CG's check (an iteration).
+  template <int ACT, int MODE>
+  void local_precond(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
+    const int L = set.local_niter;
+    launch_pdl(pgm::k_lp_start<T, ACT>, ntblk, 256, 0, st, a);
+    for (int j = 1; j <= L; ++j) {
+      pgm::v4<T> *cur = (j & 1) ? LP0.p : LP1.p, *prev = (j & 1) ? LP1.p : LP0.p;
+      if (j == 1) launch_pdl(pgm::k_lp_ap<T, ACT, true>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)prev, cur);
+      else launch_pdl(pgm::k_lp_ap<T, ACT, false>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)prev, cur);
+      if (j < L)
+        launch_pdl(pgm::k_lp_step<T, ACT, false, MODE>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)cur, nsys, set.dipole_tol,
+                   set.max_iter, dany.p, cond, use_cond, cg_done.p);
+      else
+        launch_pdl(pgm::k_lp_step<T, ACT, true, MODE>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)cur, nsys, set.dipole_tol,
+                   set.max_iter, dany.p, cond, use_cond, cg_done.p);
+    }
+  }
+
+  // One CG iteration: p = z + beta p spread, FFTs, A p with p.Ap, update, per-system check (with
+  // the local preconditioner: the update, then its chain, whose last kernel checks).
   void iteration(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
     sweep<false, true, 1, 1>(st, a, Pv.p, AP.p);
+    if (set.local_niter > 0) {
+      launch_pdl(pgm::k_cg_update_r<T>, ntblk, 256, 0, st, a);
+      local_precond<1, 1>(st, a, cond, use_cond);
+      return;
+    }
     launch_pdl(pgm::k_cg_update_check<T>, ntblk, 256, 0, st, a, nsys, set.dipole_tol, set.max_iter, dany.p, cond, use_cond,
                cg_done.p);
   }
@@ -1241,14 +1310,24 @@ struct Engine : EngineBase {
     };
     if (captured) conditional_node(st, cond2, cudaGraphCondTypeIf, plain_start);
     else plain_start(st);
-    pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+    if (set.local_niter > 0) {
+      pgm::k_cg_init<T, false, true><<<ntblk, 256, 0, st>>>(a); check_launch();
+      local_precond<0, 0>(st, a, 0, 0);
+    } else {
+      pgm::k_cg_init<T><<<ntblk, 256, 0, st>>>(a); check_launch();
+    }
     launch_pdl(pgm::k_cg_begin, 1, 256, 0, st, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p,
                mode == 0 && set.predictor == 5 ? nn_fb_factor : 0.0, 0, condfb, captured && check_nn ? 1 : 0, dfb.p);
     if (check_nn) {
       auto fallback = [&](cudaStream_t s2) {
         launch_pdl(pgm::k_fb_prep<T>, grid1(nt), 256, 0, s2, a, (const float *)nn_mu.p);
         sweep<false, false, 3, 1>(s2, a, D.p, AP.p);  // A delta
-        launch_pdl(pgm::k_cg_init<T, true>, ntblk, 256, 0, s2, a, (const float *)nn_mu.p);
+        if (set.local_niter > 0) {
+          launch_pdl(pgm::k_cg_init<T, true, true>, ntblk, 256, 0, s2, a, (const float *)nn_mu.p);
+          local_precond<3, 0>(s2, a, 0, 0);
+        } else {
+          launch_pdl(pgm::k_cg_init<T, true>, ntblk, 256, 0, s2, a, (const float *)nn_mu.p);
+        }
         launch_pdl(pgm::k_cg_begin, 1, 256, 0, s2, d_cg.p, nsys, set.dipole_tol, set.max_iter, dany.p, nn_fb_factor, 1,
                    condfb, 0, (int *)nullptr);
       };
@@ -1486,6 +1565,12 @@ PgmStatus pgm_create(const PgmSettings *s, const PgmSystemDesc *systems, int n, 
     return fail(PGM_ERR_INVALID, "iel_order must be 0 or 3..9");
   if (s->iel && (s->iel_omega < 0 || s->iel_iter < 0 || s->iel_precond < 0 || s->iel_precond > 1))
     return fail(PGM_ERR_INVALID, "iel_omega >= 0, iel_iter >= 0, iel_precond 0 (block) or 1 (jacobi)");
+  if (s->local_niter < 0 || s->local_niter > 8) return fail(PGM_ERR_INVALID, "local_niter must be 0..8");
+  if (s->local_niter > 0 && s->iel)
+    return fail(PGM_ERR_INVALID, "the local preconditioner (local_niter > 0) is not combined with iel");
+  if (s->local_niter > 0 &&
+      !(s->local_cut > 0 && s->local_cut < s->cutoff && (s->elec_cutoff <= 0 || s->local_cut < s->elec_cutoff)))
+    return fail(PGM_ERR_INVALID, "local_cut must be positive and below the (electrostatics) cutoff");
   if (s->elec < 0 || s->elec > 3) return fail(PGM_ERR_INVALID, "elec must be 0..3 (q, qp, qi, qpi)");
   if (s->vdw < 0 || s->vdw > 1) return fail(PGM_ERR_INVALID, "vdw must be 0 (none) or 1 (lj)");
   if (s->precision < 0 || s->precision > 1) return fail(PGM_ERR_INVALID, "precision must be 0 (mixed) or 1 (double)");
@@ -1717,12 +1802,14 @@ PgmStatus pgm_tuning(PgmHandle *h, PgmTuning *out) {
   return PGM_OK;
 }
 
-PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm, int sweep_early) {
+PgmStatus pgm_set_tuning(PgmHandle *h, int rowfield_lanes, int forces_blocks_per_sm, int sweep_early, int rowfield_grid) {
   if (!h || !(rowfield_lanes == 0 || rowfield_lanes == 8 || rowfield_lanes == 16 || rowfield_lanes == 32) ||
       !(forces_blocks_per_sm == 0 || (forces_blocks_per_sm >= 2 && forces_blocks_per_sm <= 4)) || sweep_early < -1 ||
-      sweep_early > 1)
-    return fail(PGM_ERR_INVALID, "rowfield_lanes 0, 8, 16 or 32; forces_blocks_per_sm 0, 2, 3 or 4; sweep_early -1, 0 or 1");
-  h->eng->set_tuning(rowfield_lanes, forces_blocks_per_sm, sweep_early);
+      sweep_early > 1 || rowfield_grid < -1 || rowfield_grid > 2)
+    return fail(PGM_ERR_INVALID,
+                "rowfield_lanes 0, 8, 16 or 32; forces_blocks_per_sm 0, 2, 3 or 4; sweep_early -1, 0 or 1; "
+                "rowfield_grid -1, 0, 1 or 2");
+  h->eng->set_tuning(rowfield_lanes, forces_blocks_per_sm, sweep_early, rowfield_grid);
   return PGM_OK;
 }
 

@@ -81,6 +81,8 @@ struct CGSys {
   // iteration limit for this system (tol_s < 0, maxit_s < 0: the settings').
   int iel_ext, iel_first, maxit_s, pad2_;
   double tol_s;
+  // local preconditioner: inner r.z (accumulated, and the next one), p.Ap, and beta of the inner CG
+  double acc_lrz, acc_lrz2, acc_lpap, lb;
 };
 
 // Per-system accumulators of the energy pass.

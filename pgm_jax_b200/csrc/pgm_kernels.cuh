@@ -71,6 +71,17 @@ struct Dev {
   int *nn_ne;
   int nn_emax;
   float nn_rg2;
+  // local preconditioner (local_niter > 0, forcefield.py:1766-1792): the row entries with
+  // r^2 < lc2 as row slots per atom (sh_slot [atom][sh_max], sh_n; written by the row build),
+  // compacted once per step entry-major by k_short_compact (entry e of atom i at e nt + i) into
+  // c_k, c_x, c_y, c_z, c_g1, c_g2; the inner CG's vectors rr (LRR), alpha rr (LZZ), its directions
+  // (LP0 / LP1, alternating), and r_new - r_old of the outer update (DR)
+  int *sh_slot, *sh_n;
+  int sh_max;
+  double lc2;
+  int *c_k;
+  T *c_x, *c_y, *c_z, *c_g1, *c_g2;
+  v4<T> *LRR, *LZZ, *LP0, *LP1, *DR;
   // iEL/0-SCF shadow energy: delta (Dl) and the reciprocal potential of delta alone (Phi2);
   // iel_keep = 1 - 1/omega for pairs inside a preconditioner block when iel_keep_on
   const v4<T> *Dl;
@@ -368,7 +379,7 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 // G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] (forcefield.py:1314-1338, kernels.py:76-118).
 template <typename T>
 __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, double x, double y, double z, size_t base, int &count,
-                                         int lane, int i, int &ecount, int &vcount, bool special) {
+                                         int lane, int i, int &ecount, int &vcount, int &scount, bool special) {
   const unsigned lt = (1u << lane) - 1u;
   const double r2 = x * x + y * y + z * z;
   bool kv = false;
@@ -393,6 +404,13 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
       a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
     }
     vcount += __popc(bv);
+  }
+  if (a.sh_slot) {  // the local preconditioner's entries: their row slots
+    const bool sh = keep && slot < a.mce && r2 < a.lc2;
+    const unsigned sb = __ballot_sync(0xffffffffu, sh);
+    const int at = scount + __popc(sb & lt);
+    if (sh && at < a.sh_max) a.sh_slot[(size_t)i * a.sh_max + at] = slot;
+    scount += __popc(sb);
   }
   if (a.nn_e4) {  // the learned guess's graph edges: the short entries, with their displacement
     const bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
@@ -420,7 +438,7 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   double4 pi = a.pos4[i];
   double rc2 = a.cutoff * a.cutoff;
   size_t base = (size_t)i * a.mc;
-  int count = 0, ecount = 0, vcount = 0;
+  int count = 0, ecount = 0, vcount = 0, scount = 0;
   int mf = a.molfirst[i], me = a.molend[i];
   for (int j0 = mf; j0 < me; j0 += 32) {
     int j = j0 + lane;
@@ -432,7 +450,7 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, true);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, true);
   }
   int nsp = count;
   int mi = (int)pi.w;
@@ -468,12 +486,16 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, false);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, false);
   }
   if (lane == 0) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
     if (a.nn_e4) a.nn_ne[i] = ecount;
+    if (a.sh_slot) {
+      a.sh_n[i] = min(scount, a.sh_max);
+      if (scount > a.sh_max) atomicOr(&a.status[s], 0x20u);  // the preconditioner kept the first sh_max
+    }
     if (count > a.mce) atomicOr(&a.status[s], 0x1u);
     atomicMax(a.max_count, count);
     if (a.rnv) {
@@ -1210,18 +1232,21 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
 // (Engine::autotune).  The lane partial sums are combined by a butterfly within each LPR group,
 // so the variants differ only in the order of the row's additions.
 template <typename T, bool WITH_Q, int ACT, int LPR = 32>
-__global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ F) {
+__global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ F, int nvb) {
   static_assert(LPR == 32 || LPR == 16 || LPR == 8, "lanes per row");
   pdl_enter();
   const int sub = threadIdx.x / LPR, lane = threadIdx.x % LPR;
-  int s = a.wb_sys[blockIdx.x];
-  int i = a.wb_atom0[blockIdx.x] + sub;
+  // blocks of 8 rows (nvb of them); a grid smaller than nvb walks them at its stride (the row field
+  // beside the FFT chain on a limited number of SMs)
+  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+  int s = a.wb_sys[vb];
+  int i = a.wb_atom0[vb] + sub;
   const SysInfo &S = a.sys[s];
-  if (ACT == 1 && !a.cg[s].active) return;  // uniform over the block
-  if (ACT == 2 && !a.cg[s].sweep2) return;
-  if (ACT == 3 && !a.cg[s].fallback) return;
+  if (ACT == 1 && !a.cg[s].active) continue;  // uniform over the block
+  if (ACT == 2 && !a.cg[s].sweep2) continue;
+  if (ACT == 3 && !a.cg[s].fallback) continue;
   const bool valid = i < S.atom0 + S.natom;
-  if (LPR == 32 && !valid) return;  // uniform over the warp
+  if (LPR == 32 && !valid) continue;  // uniform over the warp
   int n = valid ? min(a.rn[i], a.mce) : 0;
   size_t base = (size_t)(valid ? i : 0) * a.mc;
   T f0 = 0, f1 = 0, f2 = 0;
@@ -1280,6 +1305,7 @@ __global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__r
     v4<T> o;
     o.x = f0; o.y = f1; o.z = f2; o.w = T(0);
     F[i] = o;
+  }
   }
 }
 
@@ -1730,7 +1756,8 @@ __global__ void k_start3(Dev<T> a) {
 // CG initialisation: z = alpha r, p = z, r.z and max|alpha r| (forcefield.py:1796-1819).
 // FB (the learned guess's fallback, systems with the flag only): first back to the extrapolation,
 // x = x4 = x - delta and r0 = b - A x4 = r0 + A delta (A delta in AP).
-template <typename T, bool FB = false>
+// LOCAL (the local preconditioner): only max|alpha r|; z, p and r.z come from its kernels.
+template <typename T, bool FB = false, bool LOCAL = false>
 __global__ void k_cg_init(Dev<T> a, const float *delta = nullptr) {
   __shared__ double red[THREADS_PER_BLOCK / 32];
   __shared__ unsigned long long mx[THREADS_PER_BLOCK / 32];
@@ -1752,9 +1779,11 @@ __global__ void k_cg_init(Dev<T> a, const float *delta = nullptr) {
     T al = a.alpha[i];
     v4<T> z;
     z.x = al * r.x; z.y = al * r.y; z.z = al * r.z; z.w = T(0);
-    a.Z[i] = z;
-    a.P[i] = z;
-    rz = double(r.x * z.x) + double(r.y * z.y) + double(r.z * z.z);
+    if (!LOCAL) {
+      a.Z[i] = z;
+      a.P[i] = z;
+      rz = double(r.x * z.x) + double(r.y * z.y) + double(r.z * z.z);
+    }
     m = fmax(fabs(double(z.x)), fmax(fabs(double(z.y)), fabs(double(z.z))));
   }
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1918,6 +1947,248 @@ __global__ void k_cg_update_check(Dev<T> a, int nsys, double tol, int max_iter, 
   __threadfence();
   cg_check_body(a.cg, nsys, tol, max_iter, any, cond, use_cond);
   if (threadIdx.x == 0) *done = 0u;
+}
+
+// ------------------------------------------------------------------ local preconditioner
+// z = M^-1 r with local_niter > 0 inner CG iterations on A_loc v = v / alpha + sum over the row
+// entries closer than local_cut of T v_k, T v = -G2 (v . x) x + G1 v (the row field's pair term),
+// started from z = alpha r (forcefield.py:1766-1792; the outer CG is then flexible, with the
+// Polak-Ribiere beta it already uses).  Thread per atom; the short entries compacted entry-major.
+
+// Once per step after the row kernels: the short entries' partner, displacement and G1, G2.
+template <typename T>
+__global__ void k_short_compact(Dev<T> a) {
+  pdl_enter();  // launched as a programmatic dependent of the previous kernel
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nt) return;
+  const int n = a.sh_n[i];
+  const size_t base = (size_t)i * a.mc;
+  for (int e = 0; e < n; ++e) {
+    const size_t o = base + a.sh_slot[(size_t)i * a.sh_max + e], c = (size_t)e * a.nt + i;
+    a.c_k[c] = a.rk[o];
+    a.c_x[c] = a.rx[o]; a.c_y[c] = a.ry[o]; a.c_z[c] = a.rz[o];
+    a.c_g1[c] = a.rg1[o]; a.c_g2[c] = a.rg2[o];
+  }
+}
+
+// sum over atom i's short entries of T v_k (get(k) = v_k)
+template <typename T, typename Get>
+__device__ __forceinline__ void short_sum(const Dev<T> &a, int i, Get &&get, T &f0, T &f1, T &f2) {
+  const int n = a.sh_n[i];
+#pragma unroll 4
+  for (int e = 0; e < n; ++e) {
+    const size_t c = (size_t)e * a.nt + i;
+    const T x = a.c_x[c], y = a.c_y[c], z = a.c_z[c], g1 = a.c_g1[c], g2 = a.c_g2[c];
+    const v4<T> v = get(a.c_k[c]);
+    const T cc = -g2 * (v.x * x + v.y * y + v.z * z);
+    f0 += cc * x + g1 * v.x;
+    f1 += cc * y + g1 * v.y;
+    f2 += cc * z + g1 * v.z;
+  }
+}
+
+// the block's sum of v added to *dst (one atomic per block)
+__device__ __forceinline__ void block_add(double v, double *dst) {
+  __shared__ double red[THREADS_PER_BLOCK / 32];
+  v = warp_sum<double>(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < THREADS_PER_BLOCK / 32; ++w) t += red[w];
+    atomicAdd(dst, t);
+  }
+}
+
+// Which systems a chain kernel serves: 0 all, 1 the iterating ones, 3 those falling back.
+__device__ __forceinline__ bool lp_skip(int act, const CGSys &G) {
+  return (act == 1 && !G.active) || (act == 3 && !G.fallback);
+}
+
+// Inner start: z = alpha r, rr = r - A_loc(alpha r) = -sum T (alpha r)_k, zz = alpha rr (the first
+// inner direction), partial rr . zz.
+template <typename T, int ACT>
+__global__ void k_lp_start(Dev<T> a) {
+  pdl_enter();
+  const int s = a.tb_sys[blockIdx.x];
+  CGSys &G = a.cg[s];
+  if (lp_skip(ACT, G)) return;  // uniform over the block
+  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const SysInfo &S = a.sys[s];
+  double rz = 0.0;
+  if (i < S.atom0 + S.natom) {
+    T f0 = 0, f1 = 0, f2 = 0;
+    short_sum(a, i, [&](int k) {
+      const v4<T> r = a.R[k];
+      const T al = a.alpha[k];
+      v4<T> w;
+      w.x = al * r.x; w.y = al * r.y; w.z = al * r.z; w.w = T(0);
+      return w;
+    }, f0, f1, f2);
+    const v4<T> r = a.R[i];
+    const T al = a.alpha[i];
+    v4<T> z, rr, zz;
+    z.x = al * r.x; z.y = al * r.y; z.z = al * r.z; z.w = T(0);
+    rr.x = -f0; rr.y = -f1; rr.z = -f2; rr.w = T(0);
+    zz.x = al * rr.x; zz.y = al * rr.y; zz.z = al * rr.z; zz.w = T(0);
+    a.Z[i] = z;
+    a.LRR[i] = rr;
+    a.LZZ[i] = zz;
+    a.LP0[i] = zz;  // the first inner direction (kept: the next direction adds to it)
+    rz = double(rr.x * zz.x) + double(rr.y * zz.y) + double(rr.z * zz.z);
+  }
+  block_add(rz, &G.acc_lrz);
+}
+
+// Inner direction and its product: p = zz (FIRST) or zz + lb p_prev (written to Pout), Ap =
+// A_loc(p) into AP (the neighbours' p formed the same way), partial p . Ap.
+template <typename T, int ACT, bool FIRST>
+__global__ void k_lp_ap(Dev<T> a, const v4<T> *__restrict__ Pin, v4<T> *__restrict__ Pout) {
+  pdl_enter();
+  const int s = a.tb_sys[blockIdx.x];
+  CGSys &G = a.cg[s];
+  if (lp_skip(ACT, G)) return;
+  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const SysInfo &S = a.sys[s];
+  const T b = T(G.lb);
+  auto pget = [&](int k) {
+    v4<T> p = a.LZZ[k];
+    if (!FIRST) {
+      const v4<T> q = Pin[k];
+      p.x += b * q.x; p.y += b * q.y; p.z += b * q.z;
+    }
+    return p;
+  };
+  double pap = 0.0;
+  if (i < S.atom0 + S.natom) {
+    T f0 = 0, f1 = 0, f2 = 0;
+    short_sum(a, i, pget, f0, f1, f2);
+    const v4<T> p = pget(i);
+    const T ia = a.ialpha[i];
+    v4<T> ap;
+    ap.x = p.x * ia + f0; ap.y = p.y * ia + f1; ap.z = p.z * ia + f2; ap.w = T(0);
+    if (!FIRST) Pout[i] = p;
+    a.AP[i] = ap;
+    pap = double(p.x * ap.x) + double(p.y * ap.y) + double(p.z * ap.z);
+  }
+  block_add(pap, &G.acc_lpap);
+}
+
+// Inner update: z += al p (al = rr.zz / p.Ap); not LAST: rr -= al Ap, zz = alpha rr, partial rr.zz
+// for the next inner iteration.  LAST: the outer quantities -- MODE 0 (start, fallback): p = z
+// and r.z; MODE 1 (iteration): z.(r_new - r_old) and r_new.z.  The block that finishes last
+// evaluates the inner scalars (lb, the next rr.zz) and, in MODE 1, the outer CG's per-system check
+// and loop condition (cg_check_body).
+template <typename T, int ACT, bool LAST, int MODE>
+__global__ void k_lp_step(Dev<T> a, const v4<T> *__restrict__ Pcur, int nsys, double tol, int max_iter, int *any,
+                          cudaGraphConditionalHandle cond, int use_cond, unsigned *done) {
+  pdl_enter();
+  {
+    const int s = a.tb_sys[blockIdx.x];
+    CGSys &G = a.cg[s];
+    if (!lp_skip(ACT, G)) {
+      const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+      const SysInfo &S = a.sys[s];
+      const T al = T(G.acc_lrz / fmax(G.acc_lpap, 1e-300));
+      double v0 = 0.0, v1 = 0.0;
+      if (i < S.atom0 + S.natom) {
+        const v4<T> p = Pcur[i];
+        v4<T> z = a.Z[i];
+        z.x += al * p.x; z.y += al * p.y; z.z += al * p.z;
+        a.Z[i] = z;
+        if (!LAST) {
+          const v4<T> ap = a.AP[i];
+          v4<T> rr = a.LRR[i], zz;
+          const T alpha = a.alpha[i];
+          rr.x -= al * ap.x; rr.y -= al * ap.y; rr.z -= al * ap.z;
+          zz.x = alpha * rr.x; zz.y = alpha * rr.y; zz.z = alpha * rr.z; zz.w = T(0);
+          a.LRR[i] = rr;
+          a.LZZ[i] = zz;
+          v0 = double(rr.x * zz.x) + double(rr.y * zz.y) + double(rr.z * zz.z);
+        } else if (MODE == 0) {
+          const v4<T> r = a.R[i];
+          a.P[i] = z;
+          v0 = double(r.x * z.x) + double(r.y * z.y) + double(r.z * z.z);
+        } else {
+          const v4<T> r = a.R[i], dr = a.DR[i];
+          v0 = double(z.x * dr.x) + double(z.y * dr.y) + double(z.z * dr.z);
+          v1 = double(r.x * z.x) + double(r.y * z.y) + double(r.z * z.z);
+        }
+      }
+      if (!LAST) {
+        block_add(v0, &G.acc_lrz2);
+      } else if (MODE == 0) {
+        block_add(v0, &G.acc_rz);
+      } else {
+        block_add(v0, &G.acc_num);
+        __syncthreads();
+        block_add(v1, &G.acc_rz);
+      }
+    }
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's partial sums are visible before it is counted
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+    CGSys &G = a.cg[s];
+    if (!LAST) {
+      G.lb = G.acc_lrz2 / fmax(G.acc_lrz, 1e-300);
+      G.acc_lrz = G.acc_lrz2;
+    } else {
+      G.acc_lrz = 0.0;
+    }
+    G.acc_lrz2 = 0.0;
+    G.acc_lpap = 0.0;
+  }
+  if (LAST && MODE == 1) {
+    __syncthreads();
+    cg_check_body(a.cg, nsys, tol, max_iter, any, cond, use_cond);
+  }
+  if (threadIdx.x == 0) *done = 0u;
+}
+
+// The outer CG update with the local preconditioner (thread per atom): x += st p, r_new = r - st
+// Ap, DR = r_new - r, and max|alpha r_new| (the convergence test stays pmemd-pgm's); z, r.z and
+// the check follow in the preconditioner's kernels.
+template <typename T>
+__global__ void k_cg_update_r(Dev<T> a) {
+  pdl_enter();
+  __shared__ unsigned long long mx[THREADS_PER_BLOCK / 32];
+  const int s = a.tb_sys[blockIdx.x];
+  CGSys &G = a.cg[s];
+  if (!G.active) return;  // uniform over the block
+  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const SysInfo &S = a.sys[s];
+  double m = 0.0;
+  if (i < S.atom0 + S.natom) {
+    const T st = T(G.rz / fmax(G.acc_pap, 1e-300));
+    v4<T> x = a.X[i], r = a.R[i];
+    const v4<T> p = a.P[i], ap = a.AP[i];
+    const T al = a.alpha[i];
+    x.x += st * p.x; x.y += st * p.y; x.z += st * p.z;
+    v4<T> rn, dr;
+    rn.x = r.x - st * ap.x; rn.y = r.y - st * ap.y; rn.z = r.z - st * ap.z; rn.w = T(0);
+    dr.x = rn.x - r.x; dr.y = rn.y - r.y; dr.z = rn.z - r.z; dr.w = T(0);
+    a.X[i] = x;
+    a.R[i] = rn;
+    a.DR[i] = dr;
+    m = fmax(fabs(double(al * rn.x)), fmax(fabs(double(al * rn.y)), fabs(double(al * rn.z))));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = (unsigned long long)__double_as_longlong(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long mm = 0;
+    for (int w = 0; w < THREADS_PER_BLOCK / 32; ++w) mm = max(mm, mx[w]);
+    atomicMax(&G.acc_max, mm);
+  }
 }
 
 // After the loop: the peek step mu = x + peek alpha r (forcefield.py:1819-1820), the dipoles

@@ -32,11 +32,11 @@ ELEC_LEVELS = {"q": 0, "qp": 1, "qi": 2, "qpi": 3}
 PREDICTORS = {"none": 0, "mu1": 1, "mu3": 3, "mu4": 4, "nn": 5}
 
 # The settings of MDSettings that this engine implements, with the reference's defaults
-# (forcefield.py:142-516).  Other reference settings (IPS, DE / GVDW, the local preconditioner, the
-# "ls" predictor, differentiable solves) are outside this path.
+# (forcefield.py:142-516).  Other reference settings (IPS, DE / GVDW, the "ls" predictor,
+# differentiable solves) are outside this path.
 _OUT_OF_SCOPE = {
     "long_range",
-    "ips_order", "ips_boundary", "de_alpha", "de_beta", "gvdw_rep", "local_cut", "local_niter",
+    "ips_order", "ips_boundary", "de_alpha", "de_beta", "gvdw_rep",
     "extrap_order", "extrap_steps", "differentiable", "adjoint_tol", "neighbor_list",
 }
 
@@ -61,6 +61,9 @@ class MDSettings:
     fused: bool = True
     norm_refresh: int = 1000
     peek: float = 0.65
+    # the local preconditioner (Induction.local_cut / local_niter, forcefield.py:302-305): 0 = Jacobi
+    local_cut: float = 0.3
+    local_niter: int = 0
     precision: str = "mixed"
     # extended-Lagrangian dipoles (ExtendedLagrangian, forcefield.py:246-282)
     iel: str = "none"
@@ -102,6 +105,14 @@ class MDSettings:
             raise ValueError(f"iel_precond {self.iel_precond!r} (block | jacobi)")
         if not (self.iel_omega > 0) or self.iel_iter < 0:
             raise ValueError("iel_omega must be positive and iel_iter >= 0")
+        if not (0 <= self.local_niter <= 8):
+            raise ValueError("local_niter must be 0..8")
+        if self.local_niter > 0:
+            rc = self.elec_cutoff if self.split_rows else self.cutoff
+            if not (0 < self.local_cut < rc):
+                raise ValueError("local_cut must be positive and below the (electrostatics) cutoff")
+            if self.iel != "none":
+                raise ValueError("the local preconditioner (local_niter > 0) is not combined with iel")
 
     @property
     def split_rows(self) -> bool:
@@ -233,7 +244,7 @@ class PGMForceField:
             float(settings.iel_kappa if settings.iel_kappa is not None else _XL_TABLE[settings.iel_order][0]),
             float(settings.iel_alpha if settings.iel_alpha is not None else _XL_TABLE[settings.iel_order][1]),
             float(settings.iel_omega), 0 if settings.iel_precond == "block" else 1, int(settings.iel_iter),
-            int(not settings.iel_shadow),
+            int(not settings.iel_shadow), float(settings.local_cut), int(settings.local_niter),
         )
         descs = (_lib.PgmSystemDesc * self.nsys)()
         self._keep = []
@@ -490,12 +501,15 @@ class PGMForceField:
         t = _lib.PgmTuning()
         _lib.check(self._lib.pgm_tuning(self._h, C.byref(t)))
         return {"rowfield_lanes": t.rowfield_lanes, "forces_blocks_per_sm": t.forces_blocks_per_sm,
-                "sweep_early": t.sweep_early, "rowfield_ms": list(t.rowfield_ms), "forces_ms": list(t.forces_ms),
-                "sweep_ms": list(t.sweep_ms), "tuned": bool(t.tuned), "from_cache": bool(t.from_cache)}
+                "sweep_early": t.sweep_early, "rowfield_grid": t.rowfield_grid, "rowfield_ms": list(t.rowfield_ms),
+                "forces_ms": list(t.forces_ms), "sweep_ms": list(t.sweep_ms), "grid_ms": list(t.grid_ms),
+                "tuned": bool(t.tuned), "from_cache": bool(t.from_cache)}
 
-    def set_tuning(self, rowfield_lanes: int = 0, forces_blocks_per_sm: int = 0, sweep_early: int = -1) -> None:
+    def set_tuning(self, rowfield_lanes: int = 0, forces_blocks_per_sm: int = 0, sweep_early: int = -1,
+                   rowfield_grid: int = -1) -> None:
         """Fix the kernel variants (0 / -1 keeps one; all so: autotune again at the next direct step)."""
-        _lib.check(self._lib.pgm_set_tuning(self._h, int(rowfield_lanes), int(forces_blocks_per_sm), int(sweep_early)))
+        _lib.check(self._lib.pgm_set_tuning(self._h, int(rowfield_lanes), int(forces_blocks_per_sm), int(sweep_early),
+                                            int(rowfield_grid)))
 
     def autotune(self) -> dict:
         """Time the kernel variants now on the last step's rows; returns tuning()."""

@@ -88,3 +88,15 @@ def test_step_bytes_formula():
     # 3.76 M pairs, 6 iterations, 96^3: about 1.1 GB per step (the 4096-water example)
     b = bench.bytes_per_step(12288, 3.76e6, 6, 96)
     assert 1.0e9 < b < 1.2e9
+
+
+def test_local_preconditioner_settings_are_checked():
+    """local_niter 0..8, local_cut below the cutoff, not with iel."""
+    from pgm_jax_b200.forcefield import MDSettings
+
+    with pytest.raises(ValueError):
+        MDSettings(local_niter=1, local_cut=0.95)
+    with pytest.raises(ValueError):
+        MDSettings(local_niter=1, iel="0scf")
+    with pytest.raises(ValueError):
+        MDSettings(local_niter=9)

@@ -17,12 +17,13 @@ def make_md(system, pos, H, prec="double", gamma=0.0, dt=0.5, **kw):
     return RigidMD(ff, pos, H, temperature=300.0, dt_fs=dt, gamma_ps=gamma, seed=3)
 
 
-@pytest.mark.parametrize("gamma", [0.0, 5.0])
-def test_graph_replay_equals_direct_steps(small_box_system, gamma):
-    """The captured step (CG as a device-side while loop, row field beside the FFTs) is the direct step."""
+@pytest.mark.parametrize("gamma,niter", [(0.0, 0), (5.0, 0), (5.0, 2)])
+def test_graph_replay_equals_direct_steps(small_box_system, gamma, niter):
+    """The captured step (CG as a device-side while loop, row field beside the FFTs; with niter > 0
+    the local preconditioner's chain inside the loop) is the direct step."""
     s, pos, H = small_box_system
-    a = make_md(s, pos, H, gamma=gamma)
-    b = make_md(s, pos, H, gamma=gamma)
+    a = make_md(s, pos, H, gamma=gamma, local_niter=niter)
+    b = make_md(s, pos, H, gamma=gamma, local_niter=niter)
     for _ in range(4):
         a.step()
     b.capture()

@@ -447,3 +447,46 @@ def test_water4096_frame_matches_oracle():
     assert abs(float(m.energy["total"][0]) - r["energy"]["total"]) <= 1e-6 * abs(r["energy"]["total"])
     assert rms_rel(m.forces.cpu().numpy(), r["forces"]) <= 1e-5
     assert rms_rel(m.induction.mu.cpu().numpy(), r["mu"]) <= 1e-5
+
+
+@pytest.mark.parametrize("prec,niter", [("double", 1), ("double", 2), ("mixed", 1), ("double", 3)])
+def test_local_preconditioner_steps_match_oracle(pgm3p25_512_system, golden_pgm3p25_512, prec, niter):
+    """The local preconditioner (local_niter inner CG iterations on the row entries closer than
+    local_cut = 0.3 nm, forcefield.py:1766-1811) over five mu4 steps of the pGM3P-25 512-water frame
+    with small displacements: FP64 energy, forces and dipoles as the oracle's, and the same outer
+    iterations; fewer outer iterations than Jacobi; mixed precision within its tolerance."""
+    from conftest import PGM3P25_512_SETTINGS
+
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+
+    s, g = pgm3p25_512_system, golden_pgm3p25_512
+    tol = 1e-8 if prec == "double" else 1e-6
+    st = dict(PGM3P25_512_SETTINGS, dipole_tol=tol, max_iter=100, local_cut=0.3, local_niter=niter)
+    o = O.Oracle(s, st)
+    oj = O.Oracle(s, dict(st, local_niter=0))
+    ff = PGMForceField(s, g["box"], MDSettings(precision=prec, **st))
+    ind_o, ind_j, ind_g = o.init_induction(), oj.init_induction(), ff.init_induction()
+    rng = np.random.default_rng(5)
+    x = g["pos"].copy()
+    its, its_j = [], []
+    for step in range(5):
+        x = x + rng.normal(scale=2e-4, size=x.shape)
+        ro = o.compute(x, g["box"], ind_o)
+        ind_o = ro["induction"]
+        rj = oj.compute(x, g["box"], ind_j)
+        ind_j = rj["induction"]
+        rg = ff.compute(x, g["box"], None, ind_g)
+        ind_g = rg.induction
+        assert int(rg.status[0]) == 0
+        e_ref = ro["energy"]["total"]
+        assert abs(float(rg.energy["total"][0]) - e_ref) <= (1e-10 if prec == "double" else 1e-6) * abs(e_ref)
+        assert rms_rel(rg.forces.cpu().numpy(), ro["forces"]) <= (1e-8 if prec == "double" else 1e-5)
+        assert rms_rel(rg.induction.mu.cpu().numpy(), ro["mu"]) <= (1e-8 if prec == "double" else 1e-5)
+        if prec == "double":
+            assert int(rg.iterations[0]) == ro["iterations"], (step, int(rg.iterations[0]), ro["iterations"])
+        else:
+            assert abs(int(rg.iterations[0]) - ro["iterations"]) <= 1
+        its.append(ro["iterations"])
+        its_j.append(rj["iterations"])
+    assert sum(its) < sum(its_j), (its, its_j)
+

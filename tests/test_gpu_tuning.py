@@ -1,6 +1,7 @@
 """The autotuner's kernel variants (GPU): every choice of lanes per row in the CG matvec's row
-stream, of blocks per SM in the force pass and of the order of the CG sweep's concurrent parts (the
-row field of p, or of z combined with the previous direction's) computes the same step (FP64: only
+stream, of blocks per SM in the force pass, of the order of the CG sweep's concurrent parts (the
+row field of p, or of z combined with the previous direction's) and of the row field's grid beside
+the FFT chain (all SMs, or 1 or 2 blocks per SM at the highest priority) computes the same step (FP64: only
 the order of additions changes), and the first direct step of a handle times them and keeps the
 fastest."""
 
@@ -9,7 +10,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [(32, 3, 0), (16, 2, 1), (8, 4, 0), (16, 3, 1), (8, 2, 1), (32, 4, 1)]
+VARIANTS = [(32, 3, 0, 0), (16, 2, 1, 1), (8, 4, 0, 2), (16, 3, 1, 2), (8, 2, 1, 0), (32, 4, 1, 1), (32, 3, 0, 1)]
 
 
 def _box():
@@ -26,12 +27,13 @@ def test_every_variant_computes_the_same_step(prec):
 
     s, pos, H, st = _box()
     out = []
-    for lanes, blocks, early in VARIANTS:
+    for lanes, blocks, early, grid in VARIANTS:
         ff = PGMForceField(s, H, MDSettings(precision=prec, **st))
-        ff.set_tuning(lanes, blocks, early)
+        ff.set_tuning(lanes, blocks, early, grid)
         r = ff.compute(pos, H)
         t = ff.tuning()
-        assert (t["rowfield_lanes"], t["forces_blocks_per_sm"], t["sweep_early"]) == (lanes, blocks, early) and not t["tuned"]
+        assert (t["rowfield_lanes"], t["forces_blocks_per_sm"], t["sweep_early"], t["rowfield_grid"]) == (
+            lanes, blocks, early, grid) and not t["tuned"]
         out.append((float(r.energy["total"][0]), r.forces.cpu().numpy(), r.induction.mu.cpu().numpy(), int(r.iterations[0])))
     e0, f0, m0, i0 = out[0]
     tol = 1e-12 if prec == "double" else 1e-6
@@ -53,6 +55,7 @@ def test_first_direct_step_autotunes():
     assert t["tuned"] and t["rowfield_lanes"] in (32, 16, 8) and t["forces_blocks_per_sm"] in (2, 3, 4)
     assert all(ms > 0 for ms in t["rowfield_ms"] + t["forces_ms"] + t["sweep_ms"])
     assert t["sweep_early"] == (1 if t["sweep_ms"][1] < t["sweep_ms"][0] else 0)
+    assert all(ms > 0 for ms in t["grid_ms"]) and t["grid_ms"][t["rowfield_grid"]] == min(t["grid_ms"])
     assert t["rowfield_ms"][[32, 16, 8].index(t["rowfield_lanes"])] == min(t["rowfield_ms"])
     # a second handle of the same shape takes the choice from the cache
     ff2 = PGMForceField(s, H, MDSettings(precision="mixed", **st))
