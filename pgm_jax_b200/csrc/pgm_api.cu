@@ -241,10 +241,10 @@ struct Engine : EngineBase {
   DBuf<int> nn_valid;  // nn_bl holds a previous step
   DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by the row build)
   DBuf<int> nn_ne;
-  // local preconditioner (set.local_niter > 0): short entries' row slots and counts, their compact
-  // copy (entry-major), the inner CG's vectors
+  // local preconditioner (set.local_niter > 0): the short entries (entry-major) and their counts,
+  // the inner CG's vectors
   static constexpr int SH_MAX = 48;
-  DBuf<int> sh_slot, sh_n, c_k;
+  DBuf<int> sh_n, c_k;
   DBuf<T> c_x, c_y, c_z, c_g1, c_g2;
   DBuf<pgm::v4<T>> LRR, LZZ, LP0, LP1, DRv;
   static constexpr int NN_EMAX = 128;
@@ -309,7 +309,7 @@ struct Engine : EngineBase {
     a.mce = mce; a.rnv = split ? rnv.p : nullptr; a.rce2 = rc_e * rc_e;
     a.nn_e4 = nn_e4.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
     if (set.local_niter > 0) {
-      a.sh_slot = sh_slot.p; a.sh_n = sh_n.p; a.sh_max = SH_MAX; a.lc2 = set.local_cut * set.local_cut;
+      a.sh_n = sh_n.p; a.sh_max = SH_MAX; a.lc2 = set.local_cut * set.local_cut;
       a.c_k = c_k.p; a.c_x = c_x.p; a.c_y = c_y.p; a.c_z = c_z.p; a.c_g1 = c_g1.p; a.c_g2 = c_g2.p;
       a.LRR = LRR.p; a.LZZ = LZZ.p; a.LP0 = LP0.p; a.LP1 = LP1.p; a.DR = DRv.p;
     }
@@ -611,7 +611,7 @@ struct Engine : EngineBase {
     if (set.predictor == 5) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
     if (set.local_niter > 0) {
       const size_t ns = (size_t)nt * SH_MAX;
-      sh_slot.alloc(ns); sh_n.alloc(nt); c_k.alloc(ns);
+      sh_n.alloc(nt); c_k.alloc(ns);
       c_x.alloc(ns); c_y.alloc(ns); c_z.alloc(ns); c_g1.alloc(ns); c_g2.alloc(ns);
       LRR.alloc(nt); LZZ.alloc(nt); LP0.alloc(nt); LP1.alloc(nt); DRv.alloc(nt);
       CK(cudaMemset(sh_n.p, 0, sizeof(int) * nt));
@@ -977,7 +977,7 @@ struct Engine : EngineBase {
       else if (which == 4) {
         pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
         pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a);
-        if (set.local_niter > 0) pgm::k_short_compact<T><<<grid1(nt), 256, 0, st>>>(a);
+        if (set.local_niter > 0) pgm::k_short_kernels<T><<<grid1(nt), 256, 0, st>>>(a);
       }
       else if (which == 5 || which == 6) {  // the first FFT pass (plane or k3), after the spread with 6
         if (which == 6) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
@@ -1109,7 +1109,7 @@ struct Engine : EngineBase {
     launch_pdl(pgm::k_rows<T>, nwblk, 256, 0, st, a);
     if (nn_hist) nn_fork(st, a, nn_hist);
     launch_pdl(pgm::k_row_kernels<T>, (int)(((size_t)nt * mc + 255) / 256), 256, 0, st, a);
-    if (set.local_niter > 0) launch_pdl(pgm::k_short_compact<T>, grid1(nt), 256, 0, st, a);
+    if (set.local_niter > 0) launch_pdl(pgm::k_short_kernels<T>, grid1(nt), 256, 0, st, a);
     launch_pdl(pgm::k_influence<T>, (int)std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st, a, (long long)cgrid);
   }
 

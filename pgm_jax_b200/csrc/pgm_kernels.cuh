@@ -72,11 +72,11 @@ struct Dev {
   int nn_emax;
   float nn_rg2;
   // local preconditioner (local_niter > 0, forcefield.py:1766-1792): the row entries with
-  // r^2 < lc2 as row slots per atom (sh_slot [atom][sh_max], sh_n; written by the row build),
-  // compacted once per step entry-major by k_short_compact (entry e of atom i at e nt + i) into
-  // c_k, c_x, c_y, c_z, c_g1, c_g2; the inner CG's vectors rr (LRR), alpha rr (LZZ), its directions
-  // (LP0 / LP1, alternating), and r_new - r_old of the outer update (DR)
-  int *sh_slot, *sh_n;
+  // r^2 < lc2, entry-major (entry e of atom i at e nt + i, at most sh_max, sh_n per atom): partner
+  // and displacement written by the row build, G1 and G2 by k_short_kernels; the inner CG's vectors
+  // rr (LRR), alpha rr (LZZ), its directions (LP0 / LP1, alternating), and r_new - r_old of the
+  // outer update (DR)
+  int *sh_n;
   int sh_max;
   double lc2;
   int *c_k;
@@ -405,11 +405,15 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
     }
     vcount += __popc(bv);
   }
-  if (a.sh_slot) {  // the local preconditioner's entries: their row slots
+  if (a.sh_n) {  // the local preconditioner's entries: partner and displacement, entry-major
     const bool sh = keep && slot < a.mce && r2 < a.lc2;
     const unsigned sb = __ballot_sync(0xffffffffu, sh);
     const int at = scount + __popc(sb & lt);
-    if (sh && at < a.sh_max) a.sh_slot[(size_t)i * a.sh_max + at] = slot;
+    if (sh && at < a.sh_max) {
+      const size_t c = (size_t)at * a.nt + i;
+      a.c_k[c] = j;
+      a.c_x[c] = T(x); a.c_y[c] = T(y); a.c_z[c] = T(z);
+    }
     scount += __popc(sb);
   }
   if (a.nn_e4) {  // the learned guess's graph edges: the short entries, with their displacement
@@ -492,7 +496,7 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
     if (a.nn_e4) a.nn_ne[i] = ecount;
-    if (a.sh_slot) {
+    if (a.sh_n) {
       a.sh_n[i] = min(scount, a.sh_max);
       if (scount > a.sh_max) atomicOr(&a.status[s], 0x20u);  // the preconditioner kept the first sh_max
     }
@@ -1955,19 +1959,25 @@ __global__ void k_cg_update_check(Dev<T> a, int nsys, double tol, int max_iter, 
 // started from z = alpha r (forcefield.py:1766-1792; the outer CG is then flexible, with the
 // Polak-Ribiere beta it already uses).  Thread per atom; the short entries compacted entry-major.
 
-// Once per step after the row kernels: the short entries' partner, displacement and G1, G2.
+// Once per step after the row build: G1, G2 of the short entries (the row build wrote partner and
+// displacement), by the same arithmetic as k_row_kernels on the same rounded displacements.
 template <typename T>
-__global__ void k_short_compact(Dev<T> a) {
+__global__ void k_short_kernels(Dev<T> a) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nt) return;
   const int n = a.sh_n[i];
-  const size_t base = (size_t)i * a.mc;
+  const T Ri = a.radius[i];
   for (int e = 0; e < n; ++e) {
-    const size_t o = base + a.sh_slot[(size_t)i * a.sh_max + e], c = (size_t)e * a.nt + i;
-    a.c_k[c] = a.rk[o];
-    a.c_x[c] = a.rx[o]; a.c_y[c] = a.ry[o]; a.c_z[c] = a.rz[o];
-    a.c_g1[c] = a.rg1[o]; a.c_g2[c] = a.rg2[o];
+    const size_t c = (size_t)e * a.nt + i;
+    const T x = a.c_x[c], y = a.c_y[c], z = a.c_z[c], Rk = a.radius[a.c_k[c]];
+    const T r = t_sqrt(x * x + y * y + z * z);
+    const T aik = t_rsqrt(T(2) * (Ri * Ri + Rk * Rk));
+    T A[4], Bb[4];
+    erf_kernels<T>(aik, r, A);
+    erf_kernels<T>(T(a.beta), r, Bb);
+    a.c_g1[c] = A[1] - Bb[1];
+    a.c_g2[c] = A[2] - Bb[2];
   }
 }
 
