@@ -5,9 +5,9 @@ Headline workload (one GPU): 32,768 pGM3P-25 waters (98,304 atoms) on a seeded j
 lattice in a 9.93 nm cubic box, cutoff 0.9 nm, Ewald 4.0 / nm, PME 192^3 order 6, mixed precision
 (FP32 pair / PME / CG vectors, FP64 reductions), Langevin NVT 298 K with gamma 2 / ps, dt 1 fs, CG to
 max|alpha r| / mean|alpha b| <= 1e-6 with the reference's local preconditioner (one inner CG
-iteration on the row entries inside 0.3 nm; `--local-niter 0` for Jacobi, the reference's default).  A step is one captured CUDA graph: rigid-body kick/drift/
-Langevin, the force call (rows, PME, CG as a device-side while loop, energy / forces / virial),
-closing kick.  `--workload water4096` runs the same line on 4,096 waters (4.966 nm, PME 96^3).
+iteration on the row entries inside 0.3 nm; `--local-niter 0` for Jacobi, the reference's default).
+A step is one captured CUDA graph: rigid-body kick/drift/Langevin, the force call (rows, PME, CG
+as a device-side while loop, energy / forces / virial), closing kick.  `--workload water4096` runs the same line on 4,096 waters (4.966 nm, PME 96^3).
 
 The headline run starts every solve from the learned guess, the 2-layer message-passing model on the
 0.5 nm graph: plain-solver MD on the 4,096-water box writes the training frames, the model trains on
