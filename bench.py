@@ -216,7 +216,8 @@ def cpu_reference(steps: int, warmup: int, budget_s: float = 120.0):
 
     s, pos, H = headline_box()
     K = W["grid"]
-    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(K, K, K), pme_order=6, dipole_tol=TOL, max_iter=100)
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(K, K, K), pme_order=6, dipole_tol=TOL, max_iter=100,
+              local_cut=0.3, local_niter=LOCAL["local_niter"])
     cores = os.cpu_count() or 1
     o = O.Oracle(s, st, nthreads=cores)
     ind = o.init_induction()
@@ -241,7 +242,8 @@ def cpu_reference(steps: int, warmup: int, budget_s: float = 120.0):
         "value": ns_per_day(ms), "ms_per_step": ms, "cores": cores, "steps_timed": len(times),
         "cg_iters_per_step": float(np.mean(iters)),
         "sample": f"{len(times)} force steps of the {W['atoms'] // 3}-water workload (FP64 oracle, {cores} threads, "
-        f"mu4 predictor, CG 1e-6) on a smooth drift trajectory, after {n_fill} untimed steps that fill the history; "
+        f"mu4 predictor, CG 1e-6, local preconditioner {LOCAL['local_niter']} inner iterations) on a smooth drift "
+        f"trajectory, after {n_fill} untimed steps that fill the history; "
         "the rigid-body integrator's cost (<1%) is not included",
     }
 
