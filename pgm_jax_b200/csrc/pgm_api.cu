@@ -209,6 +209,7 @@ struct Engine : EngineBase {
   DBuf<double4> pperm, off, dEdd;
   DBuf<int> cell_of, slot_of, cell_count, cell_start, cell_atoms;
   DBuf<double4> spos, pos_ref, pos4;
+  DBuf<float4> pos4f;  // mixed precision: wrapped FP32 positions for the row build
   DBuf<int> cand, ncand, nb_flag;
   DBuf<long long> nb_builds;
   DBuf<int> rn, rnsp, rk, dmax, dany;
@@ -301,7 +302,7 @@ struct Engine : EngineBase {
     a.cell_atoms = cell_atoms.p;
     a.spos = spos.p;
     a.skin = skin; a.cc = cc; a.nb_flag = nb_flag.p; a.nb_builds = nb_builds.p; a.cand = cand.p; a.ncand = ncand.p;
-    a.pos_ref = pos_ref.p; a.pos4 = pos4.p;
+    a.pos_ref = pos_ref.p; a.pos4 = pos4.p; a.pos4f = pos4f.p;
     a.idx = idx; a.idx_width = idx_width;
     a.rn = rn.p; a.rnsp = rnsp.p; a.rk = rk.p;
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
@@ -565,7 +566,8 @@ struct Engine : EngineBase {
     base.alloc(nt); frac.alloc(nt); X.alloc(nt); R.alloc(nt); Z.alloc(nt); Pv.alloc(nt); AP.alloc(nt); Bv.alloc(nt); D.alloc(nt); Fv.alloc(nt); Fpv.alloc(nt);
     pperm.alloc(nt); off.alloc(nt); dEdd.alloc(nt);
     cell_of.alloc(nt); slot_of.alloc(nt); cell_count.alloc(ncell); cell_start.alloc(ncell + 1); cell_atoms.alloc(nt); spos.alloc(nt);
-    pos_ref.alloc(nt); pos4.alloc(nt); ncand.alloc(nt); cand.alloc((size_t)nt * cc); nb_flag.alloc(1); nb_builds.alloc(1);
+    pos_ref.alloc(nt); pos4.alloc(nt); ncand.alloc(nt);
+    if (sizeof(T) == 4) pos4f.alloc(nt); cand.alloc((size_t)nt * cc); nb_flag.alloc(1); nb_builds.alloc(1);
     CK(cudaMemset(cell_count.p, 0, sizeof(int) * ncell));
     CK(cudaMemset(nb_builds.p, 0, sizeof(long long)));
     { int one = 1; CK(cudaMemcpy(nb_flag.p, &one, sizeof(int), cudaMemcpyHostToDevice)); }

@@ -31,6 +31,7 @@ struct Dev {
   int *cand, *ncand;      // candidates (N, cc) and counts
   double4 *pos_ref;       // positions at the last rebuild
   double4 *pos4;          // positions this step, .w = molecule
+  float4 *pos4f;          // FP32 rows (mixed precision): the positions wrapped into the box, .w = molecule
   int max_iter;
   const SysInfo *sys;
   BoxInfo *box;
@@ -188,6 +189,11 @@ __global__ void k_prep(Dev<T> a) {
   }
   a.pperm[i] = p;
   a.pos4[i] = make_double4(px, py, pz, (double)a.molid[i]);
+  if (a.pos4f) {  // wrapped: |coordinates| below the box's, so FP32 keeps displacements to ~1e-6 nm
+    double w[3];
+    for (int c = 0; c < 3; ++c) w[c] = uc[0] * B.H[0 * 3 + c] + uc[1] * B.H[1 * 3 + c] + uc[2] * B.H[2 * 3 + c];
+    a.pos4f[i] = make_float4(float(w[0]), float(w[1]), float(w[2]), float(a.molid[i]));
+  }
   // Verlet list: rebuild when an atom moved more than skin / 2 since the last build
   double4 r0 = a.pos_ref[i];
   double dx = px - r0.x, dy = py - r0.y, dz = pz - r0.z;
@@ -425,6 +431,16 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
   }
 }
 
+// FP32 sequential minimum image (the mixed-precision row build's candidate loop).
+__device__ __forceinline__ void min_image_fast_f(float &x, float &y, float &z, const float *H, const float *id) {
+  float n = rintf(z * id[2]);
+  x -= n * H[6]; y -= n * H[7]; z -= n * H[8];
+  n = rintf(y * id[1]);
+  x -= n * H[3]; y -= n * H[4];
+  n = rintf(x * id[0]);
+  x -= n * H[0];
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
@@ -476,21 +492,57 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
       if (j >= 0) pj = a.pos4[j];
     }
   };
-  int jn = -1;
-  double4 pn = make_double4(0, 0, 0, -1);
-  load(lane, jn, pn);
-  for (int c0 = 0; c0 < nc; c0 += 32) {
-    int j = jn;
-    double4 pj = pn;
-    load(c0 + 32 + lane, jn, pn);  // prefetch the next chunk
-    bool keep = false;
-    double x = 0, y = 0, z = 0;
-    if (j >= 0 && (int)pj.w != mi) {
-      x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
-      min_image_fast(x, y, z, H, id);
-      keep = x * x + y * y + z * z < rc2;
+  if (sizeof(T) == 4 && a.pos4f) {
+    // mixed precision: FP32 displacements from the wrapped FP32 positions (16-byte gathers; the
+    // rows store FP32 displacements anyway)
+    float Hf[9], idf[3];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Hf[k] = float(H[k]);
+    idf[0] = float(id[0]); idf[1] = float(id[1]); idf[2] = float(id[2]);
+    const float4 pf = a.pos4f[i];
+    const float rc2f = float(rc2);
+    auto loadf = [&](int c, int &j, float4 &pj) {
+      j = -1;
+      if (c < nc) {
+        int jl = row[c];
+        if (a.idx) j = (jl >= 0 && jl < S.natom) ? S.atom0 + jl : -1;
+        else j = jl;
+        if (j >= 0) pj = a.pos4f[j];
+      }
+    };
+    int jn = -1;
+    float4 pn = make_float4(0.f, 0.f, 0.f, -1.f);
+    loadf(lane, jn, pn);
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      int j = jn;
+      float4 pj = pn;
+      loadf(c0 + 32 + lane, jn, pn);  // prefetch the next chunk
+      bool keep = false;
+      float x = 0.f, y = 0.f, z = 0.f;
+      if (j >= 0 && (int)pj.w != mi) {
+        x = pf.x - pj.x; y = pf.y - pj.y; z = pf.z - pj.z;
+        min_image_fast_f(x, y, z, Hf, idf);
+        keep = x * x + y * y + z * z < rc2f;
+      }
+      row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, false);
     }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, false);
+  } else {
+    int jn = -1;
+    double4 pn = make_double4(0, 0, 0, -1);
+    load(lane, jn, pn);
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      int j = jn;
+      double4 pj = pn;
+      load(c0 + 32 + lane, jn, pn);  // prefetch the next chunk
+      bool keep = false;
+      double x = 0, y = 0, z = 0;
+      if (j >= 0 && (int)pj.w != mi) {
+        x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
+        min_image_fast(x, y, z, H, id);
+        keep = x * x + y * y + z * z < rc2;
+      }
+      row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, false);
+    }
   }
   if (lane == 0) {
     a.rn[i] = count;
