@@ -41,6 +41,31 @@ def golden_pgm3p25_512():
 
 
 @pytest.fixture(scope="session")
+def golden_pmemd_pbc_512():
+    return dict(np.load(os.path.join(GOLDEN, "pmemd_pbc_512.npz")))
+
+
+# The pmemd-pgm single point of the same 512-water frame (data/validation/amber_ref/pmemd_pbc/mdin
+# of pGM-JAX): cut 10 A, ew_coeff 0.38 / A, PME 72^3 order 8, vdwmeth 0 (no LJ tail), SCF tol 1e-9.
+PMEMD_PBC_SETTINGS = dict(cutoff=1.0, ewald_beta=3.8, pme_grid=(72, 72, 72), pme_order=8, lj_lrc=False,
+                          dipole_tol=1e-10, max_iter=500)
+# Amber's pGM uses Tinker's Coulomb constant: electrostatic energy and forces scale by this ratio
+# (scripts/validation/validate_amber.py of pGM-JAX, units.py:31-36).
+AMBER_KE_SCALE = (332.05382 * 4.184 / 10.0) / 138.935458
+
+
+def pmemd_compare(energy_elec_kj, energy_vdw_kj, forces_elec, forces_total, mu_nm, golden):
+    """(EELEC relative deviation, VDWAALS deviation [kcal/mol], force RMSD [kcal/mol/A], dipole RMSD
+    [e A]) against the stored pmemd-pgm run, from our electrostatic-only and total forces [kJ/mol/nm]."""
+    e = energy_elec_kj / 4.184 * AMBER_KE_SCALE
+    f = (forces_elec * AMBER_KE_SCALE + (forces_total - forces_elec)) / 41.84
+    rms = lambda x: float(np.sqrt(np.mean(x * x)))  # noqa: E731
+    return (abs(e - float(golden["eelec_kcal"])) / abs(float(golden["eelec_kcal"])),
+            abs(energy_vdw_kj / 4.184 - float(golden["vdw_kcal"])), rms(f - golden["forces_kcal_A"]),
+            rms(10.0 * mu_nm - golden["mu_e_A"]))
+
+
+@pytest.fixture(scope="session")
 def pgm3p25_512_system():
     from pgm_jax_b200.systems import System, pgm3p25_water
 

@@ -27,9 +27,18 @@ variable's scale_factor as pgm_jax/md/io.py:54-70 reads them -- and a truncated-
 27.201 A, 109.47 deg), turned into the lower-triangular box of pgm_jax/md/box.py:291-314
 (box_from_cell) and nm as the regression case does.  The velocities are stored for the 10-step NVE
 install check of tests/test_water512.py (step-10 Epot -2114884.256504 kJ/mol, T 291.356783 K).
+
+pmemd_pbc_512.npz -- the independent pmemd-pgm (Amber) single point on the same frame, as the
+reference keeps it in data/validation/amber_ref/pmemd_pbc (mdin: cut 10 A, ew_coeff 0.38 / A, PME
+72^3 order 8, vdwmeth 0, dipole_scf_tol 1e-9): step-0 EELEC and VDWAALS of mdout [kcal/mol], the
+forces of mdfrc [kcal/mol/A, stored as FP32 by pmemd], and the induced dipoles of the last CG
+iterate cpu_cg_iter_041.dat [e A].  Amber's pGM uses Tinker's Coulomb constant; the comparison
+scales the electrostatic energy and forces by 332.05382 kcal/mol A / (138.935458 kJ/mol nm / 4.184
+* 10) as scripts/validation/validate_amber.py does.
 """
 
 import os
+import re
 import sys
 
 import numpy as np
@@ -90,6 +99,25 @@ def main(ref: str) -> None:
             out[f"{tag}.{k}"] = g[f"{tag}.{k}"]
     np.savez_compressed(os.path.join(HERE, "ff_pgm3p25_512.npz"), **out)
     print("wrote", os.path.join(HERE, "ff_pgm3p25_512.npz"), sorted(out))
+
+    out = pmemd_pbc(ref)
+    np.savez_compressed(os.path.join(HERE, "pmemd_pbc_512.npz"), **out)
+    print("wrote", os.path.join(HERE, "pmemd_pbc_512.npz"), sorted(out))
+
+
+def pmemd_pbc(ref: str) -> dict:
+    """Step-0 energies, forces and induced dipoles of the reference's stored pmemd-pgm run."""
+    from scipy.io import netcdf_file
+
+    d = os.path.join(ref, "data", "validation", "amber_ref", "pmemd_pbc")
+    txt = open(os.path.join(d, "mdout")).read()
+    blk = txt[txt.index("NSTEP =        0"):]
+    get = lambda k: float(re.search(rf"{k}\s*=\s*(-?\d+\.\d+)", blk).group(1))  # noqa: E731
+    f = netcdf_file(os.path.join(d, "mdfrc"), "r", mmap=False)
+    forces = np.array(f.variables["forces"][:], float)[0]
+    f.close()
+    mu = np.loadtxt(os.path.join(d, "cpu_cg_iter_041.dat"), comments="#")[:, 1:4]
+    return {"eelec_kcal": get("EELEC"), "vdw_kcal": get("VDWAALS"), "forces_kcal_A": forces, "mu_e_A": mu}
 
 
 if __name__ == "__main__":

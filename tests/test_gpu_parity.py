@@ -490,3 +490,25 @@ def test_local_preconditioner_steps_match_oracle(pgm3p25_512_system, golden_pgm3
         its_j.append(rj["iterations"])
     assert sum(its) < sum(its_j), (its, its_j)
 
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_pmemd_pgm_single_point(pgm3p25_512_system, golden_pgm3p25_512, golden_pmemd_pbc_512, prec):
+    """The engine against the independent pmemd-pgm single point (PME 72^3 order 8, 10 A cutoff, no
+    LJ tail) on the water512 frame: FP64 as tight as the oracle (EELEC 1e-9, forces at pmemd's FP32
+    storage, dipoles 1e-9 e A RMS); mixed precision at its tolerance."""
+    from conftest import PMEMD_PBC_SETTINGS, pmemd_compare
+
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+
+    s, g = pgm3p25_512_system, golden_pgm3p25_512
+    st = dict(PMEMD_PBC_SETTINGS, dipole_tol=1e-10 if prec == "double" else 1e-6)
+    r = PGMForceField(s, g["box"], MDSettings(precision=prec, **st)).compute(g["pos"], g["box"])
+    re_ = PGMForceField(s, g["box"], MDSettings(precision=prec, **dict(st, vdw="none"))).compute(g["pos"], g["box"])
+    assert int(r.status[0]) == 0
+    de, dv, df, dmu = pmemd_compare(float(r.energy["elec"][0]), float(r.energy["vdw"][0]), re_.forces.cpu().numpy(),
+                                    r.forces.cpu().numpy(), r.induction.mu.cpu().numpy(), golden_pmemd_pbc_512)
+    if prec == "double":
+        assert de <= 1e-9 and dv <= 1e-4 and df <= 2e-6 and dmu <= 1e-9, (de, dv, df, dmu)
+    else:
+        assert de <= 1e-6 and dv <= 1e-3 and df <= 36.0 * 1e-5 and dmu <= 0.12 * 1e-5, (de, dv, df, dmu)
+

@@ -175,3 +175,23 @@ def test_oracle_local_preconditioner_same_solution_fewer_iterations(pgm3p25_512_
     assert abs(out[2]["energy"]["total"] - out[0]["energy"]["total"]) <= 1e-10 * abs(out[0]["energy"]["total"])
     st = dict(PGM3P25_512_SETTINGS, local_niter=0)
     assert O.Oracle(pgm3p25_512_system, st).compute(g["pos"], g["box"])["iterations"] == int(g["double.iterations"])
+
+
+def test_oracle_matches_pmemd_pgm(pgm3p25_512_system, golden_pgm3p25_512, golden_pmemd_pbc_512):
+    """The independent pmemd-pgm (Amber) single point that pGM-JAX keeps for validation
+    (data/validation/amber_ref/pmemd_pbc): PME 72^3 order 8, 10 A cutoff, ewald 0.38 / A, no LJ tail,
+    on the water512 frame.  EELEC (Tinker's Coulomb constant) to 1e-9 relative (mdout prints 4
+    decimals of 5e5), VDWAALS to its printed digits, forces to the FP32 precision pmemd stores them
+    in, induced dipoles to 1e-10 e A RMS."""
+    from conftest import PMEMD_PBC_SETTINGS, pmemd_compare
+
+    g = golden_pgm3p25_512
+    r = O.Oracle(pgm3p25_512_system, PMEMD_PBC_SETTINGS).compute(g["pos"], g["box"])
+    re_ = O.Oracle(pgm3p25_512_system, dict(PMEMD_PBC_SETTINGS, vdw="none")).compute(g["pos"], g["box"])
+    de, dv, df, dmu = pmemd_compare(r["energy"]["elec"], r["energy"]["vdw"], re_["forces"], r["forces"], r["mu"],
+                                    golden_pmemd_pbc_512)
+    assert de <= 1e-9, de
+    assert dv <= 1e-4, dv
+    assert df <= 2e-6, df
+    assert dmu <= 1e-10, dmu
+
