@@ -91,3 +91,44 @@ def test_water512_install_check(pgm3p25_512_system, golden_pgm3p25_512, prec):
     assert abs(T - 291.356783) <= rtol_t * 291.356783, T
     assert abs(etot[9] - etot[4]) < 0.5
     assert int(md.result.status[0]) == 0
+
+
+def test_c1_nve_trajectory_matches_oracle():
+    """The FP64 configuration of the benchmarks (512 rigid pGM3P-25 waters on the seeded jittered
+    8x8x8 lattice, 2.483 nm box, cutoff 0.9 nm, Ewald 4.0 / nm, PME 48^3 order 6, CG 1e-8, Maxwell
+    velocities at 298 K, NVE, dt 1 fs, 10 steps) against the NumPy NO_SQUISH restatement driven by
+    the FP64 oracle's forces: potential energy every step within 1e-9 relative, final positions
+    within 1e-9 nm."""
+    import sys
+
+    sys.path.insert(0, __import__("os").path.join(__import__("os").path.dirname(__file__), "..", "oracle"))
+    import oracle as O
+    from rigid_oracle import RigidNVE
+
+    from pgm_jax_b200.forcefield import MDSettings, PGMForceField
+    from pgm_jax_b200.md import RigidMD
+    from pgm_jax_b200.systems import water_box
+
+    s, pos, H = water_box(8, 2.483, seed=0)
+    rng = np.random.default_rng(11)
+    kT = 0.0083144626181532 * 298.0
+    vel = rng.normal(size=(s.n, 3)) * np.sqrt(kT / np.asarray(s.masses, float))[:, None]
+    st = dict(cutoff=0.9, ewald_beta=4.0, pme_grid=(48, 48, 48), pme_order=6, lj_lrc=True, dipole_tol=1e-8, max_iter=100)
+    ff = PGMForceField(s, H, MDSettings(precision="double", **st))
+    md = RigidMD(ff, pos, H, temperature=298.0, dt_fs=1.0, gamma_ps=0.0, velocities=vel)
+    o = O.Oracle(s, st)
+    state = {"ind": o.init_induction()}
+
+    def forces(x):
+        r = o.compute(x, H, state["ind"])
+        state["ind"] = r["induction"]
+        return r["forces"], r["energy"]["total"]
+
+    ref = RigidNVE(s, pos, H, vel, forces)
+    for step in range(10):
+        md.step()
+        ref.step(0.001)
+        e = float(md.energy()["total"][0])
+        assert abs(e - ref.epot) <= 1e-9 * abs(ref.epot), (step, e, ref.epot)
+    assert np.abs(md.pos.cpu().numpy() - ref.positions()).max() <= 1e-9
+    assert int(md.result.status[0]) == 0
