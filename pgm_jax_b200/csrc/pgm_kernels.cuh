@@ -791,13 +791,18 @@ __device__ __forceinline__ void butterfly(c2<T> *v, T sg) {
 }
 
 // One Stockham stage (radix R, NS points already combined) of nl lines of length L in shared
-// memory: v_r = x[j + r L/R] w^(r k), k = j mod NS, DFT_R, y[(j / NS) NS R + k + r NS].
-template <typename T, int R>
+// memory: v_r = x[j + r L/R] w^(r k), k = j mod NS, DFT_R, y[(j / NS) NS R + k + r NS].  LF (lines
+// fastest): consecutive threads take the same j of consecutive lines, for line strides ld that are
+// odd in 8-byte words, where the stride-R writes of the first stage would otherwise hit the same
+// shared-memory banks; otherwise consecutive threads take consecutive j of one line.
+template <typename T, int R, bool LF = false>
 __device__ __forceinline__ void fft_stage(const c2<T> *x, c2<T> *y, int L, int NS, int nl, int ld, const c2<T> *tw, int sign) {
   const int LR = L / R, stride = L / (NS * R);
   const T sg = T(sign);
   for (int w = threadIdx.x; w < LR * nl; w += blockDim.x) {
-    int line = w / LR, j = w - line * LR;
+    int line, j;
+    if (LF) { j = w / nl; line = w - j * nl; }
+    else { line = w / LR; j = w - line * LR; }
     int k = j % NS;
     const c2<T> *in = x + line * ld;
     c2<T> *out = y + line * ld;
@@ -821,14 +826,14 @@ __device__ __forceinline__ void fft_stage(const c2<T> *x, c2<T> *y, int L, int N
 }
 
 // Compile-time length: every index constant folds (L, R, NS template-known).
-template <typename T, int L, int ST, int NS>
+template <typename T, int L, int ST, int NS, bool LF = false>
 __device__ __forceinline__ c2<T> *fft_run_ct(c2<T> *x, c2<T> *y, int nl, int ld, const c2<T> *tw, int sign) {
   if constexpr (ST == fft_nst(L)) {
     return x;
   } else {
     constexpr int R = fft_radix(L, ST);
-    fft_stage<T, R>(x, y, L, NS, nl, ld, tw, sign);
-    return fft_run_ct<T, L, ST + 1, NS * R>(y, x, nl, ld, tw, sign);
+    fft_stage<T, R, LF>(x, y, L, NS, nl, ld, tw, sign);
+    return fft_run_ct<T, L, ST + 1, NS * R, LF>(y, x, nl, ld, tw, sign);
   }
 }
 
@@ -848,11 +853,11 @@ __device__ c2<T> *fft_run_rt(c2<T> *x, c2<T> *y, int L, int nl, int ld, const in
   return x;
 }
 
-template <typename T, int L>
+template <typename T, int L, bool LF = false>
 __device__ __forceinline__ c2<T> *fft_lines(c2<T> *x, c2<T> *y, int Lrt, int nl, int ld, const int *rad, int nst, const c2<T> *tw,
                                             int sign) {
   if constexpr (L == 0) return fft_run_rt<T>(x, y, Lrt, nl, ld, rad, nst, tw, sign);
-  else return fft_run_ct<T, L, 0, 1>(x, y, nl, ld, tw, sign);
+  else return fft_run_ct<T, L, 0, 1, LF>(x, y, nl, ld, tw, sign);
 }
 
 // Global -> shared staging of `total` elements by the FFT_THREADS threads of a pass: with a
@@ -1025,7 +1030,7 @@ __global__ void __launch_bounds__(256) k_fft_y(Dev<T> a, const int *gsys, const 
     T *Qs = a.Q + S.rgrid0;
     for (size_t t = q0 + threadIdx.x; t < q1; t += blockDim.x) Qs[t] = T(0);
   }
-  c2<T> *res = fft_lines<T, L>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], tws, sign);
+  c2<T> *res = fft_lines<T, L, true>(x, y, K2, FFT_TILE, ld, S.rad[1], S.nst[1], tws, sign);
   for (int t = threadIdx.x; t < K2 * FFT_TILE; t += blockDim.x) {
     int k2 = t / FFT_TILE, c = t - k2 * FFT_TILE;
     int col = c0 + c;
@@ -1103,7 +1108,7 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane_fwd(Dev<T> a, const
     col[m * LD + 2 * cl + 1] = X1;
   }
   __syncthreads();
-  c2<T> *res2 = fft_lines<T, L>(col, res, K, Kh, LD, S.rad[1], S.nst[1], tws, -1);
+  c2<T> *res2 = fft_lines<T, L, true>(col, res, K, Kh, LD, S.rad[1], S.nst[1], tws, -1);
   c2<T> *C = a.C + S.cgrid0 + (size_t)k1 * K * Kh;
   for (int t = threadIdx.x; t < K * Kh; t += PLANE_THREADS) {
     const int k2 = t / Kh, m3 = t - k2 * Kh;
@@ -1141,7 +1146,7 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane_inv(Dev<T> a, const
     }
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(A, B, K, Kh, LD, S.rad[1], S.nst[1], tws, +1);
+  c2<T> *res = fft_lines<T, L, true>(A, B, K, Kh, LD, S.rad[1], S.nst[1], tws, +1);
   c2<T> *lin = res == A ? B : A;
   // rows 2cl, 2cl + 1 back into complex line cl (z = a + i b) over the full k3 range (Hermitian)
   for (int t = threadIdx.x; t < NP * K; t += PLANE_THREADS) {
@@ -1219,7 +1224,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
     }
     __syncthreads();  // y is the transform's scratch from here
   }
-  c2<T> *res = fft_lines<T, L>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], tws, -1);
+  c2<T> *res = fft_lines<T, L, true>(x, y, K1, FFT_TILE, ld, S.rad[0], S.nst[0], tws, -1);
   c2<T> *oth = res == x ? y : x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const BoxInfo &B = a.box[s];
@@ -1269,7 +1274,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
     atomicAdd(&a.eacc[s].vinf[threadIdx.x], v);
   }
-  c2<T> *res2 = fft_lines<T, L>(res, oth, K1, FFT_TILE, ld, S.rad[0], S.nst[0], tws, +1);
+  c2<T> *res2 = fft_lines<T, L, true>(res, oth, K1, FFT_TILE, ld, S.rad[0], S.nst[0], tws, +1);
   for (int t = threadIdx.x; t < K1 * FFT_TILE; t += blockDim.x) {
     int k1 = t / FFT_TILE, c = t - k1 * FFT_TILE;
     int col = c0 + c;
