@@ -918,21 +918,22 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, co
   int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;  // first real line
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
+  const int lx = K3 + 1;  // line stride in shared memory: odd in 8-byte words (no bank conflicts)
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * lx, *tws = y + FFT_PAIRS * lx;
   T *Q = a.Q + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];  // twiddles in shared memory
   staged_copy<2 * FFT_PAIRS * L>(
       2 * np * K3, [&](int t) { return Q[t]; },
       [&](int t, T v) {
         int rl = t / K3, k = t - rl * K3;
-        reinterpret_cast<T *>(&x[(rl >> 1) * K3 + k])[rl & 1] = v;
+        reinterpret_cast<T *>(&x[(rl >> 1) * lx + k])[rl & 1] = v;
       });
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, -1);
+  c2<T> *res = fft_lines<T, L, true>(x, y, K3, np, lx, S.rad[2], S.nst[2], tws, -1);
   c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
   for (int t = threadIdx.x; t < np * K3h; t += blockDim.x) {
     int cl = t / K3h, m = t - cl * K3h;
-    c2<T> Z = res[cl * K3 + m], W = res[cl * K3 + (m == 0 ? 0 : K3 - m)];
+    c2<T> Z = res[cl * lx + m], W = res[cl * lx + (m == 0 ? 0 : K3 - m)];
     c2<T> A, Bv;
     A.x = T(0.5) * (Z.x + W.x); A.y = T(0.5) * (Z.y - W.y);
     T dx = Z.x - W.x, dy = Z.y + W.y;  // (Z - conj W) / (2 i)
@@ -955,7 +956,8 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
   int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
+  const int lx = K3 + 1;  // line stride in shared memory: odd in 8-byte words (no bank conflicts)
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * lx, *tws = y + FFT_PAIRS * lx;
   const c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
   for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];
   staged_copy<FFT_PAIRS * L>(
@@ -974,14 +976,14 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
         if (up) { A.y = -A.y; Bv.y = -Bv.y; }
         c2<T> Z;
         Z.x = A.x - Bv.y; Z.y = A.y + Bv.x;
-        x[cl * K3 + m] = Z;
+        x[cl * lx + m] = Z;
       });
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, +1);
+  c2<T> *res = fft_lines<T, L, true>(x, y, K3, np, lx, S.rad[2], S.nst[2], tws, +1);
   T *Phi = a.Phi + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
     int rl = t / K3, k = t - rl * K3;
-    c2<T> z = res[(rl >> 1) * K3 + k];
+    c2<T> z = res[(rl >> 1) * lx + k];
     Phi[t] = (rl & 1) ? z.y : z.x;
   }
 }
@@ -1082,7 +1084,7 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane_fwd(Dev<T> a, const
     const int t = threadIdx.x + j * PLANE_THREADS;
     if (t < NV) {
       const int cl = t / Q4, q = t - cl * Q4;
-      c2<T> *d = A + cl * K + 4 * q;
+      c2<T> *d = A + cl * LD + 4 * q;  // line stride LD: odd in 8-byte words
       d[0].x = lo[j].x; d[0].y = hi[j].x;
       d[1].x = lo[j].y; d[1].y = hi[j].y;
       d[2].x = lo[j].z; d[2].y = hi[j].z;
@@ -1094,12 +1096,12 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane_fwd(Dev<T> a, const
     }
   }
   __syncthreads();
-  c2<T> *res = fft_lines<T, L>(A, B, K, NP, K, S.rad[2], S.nst[2], tws, -1);
+  c2<T> *res = fft_lines<T, L, true>(A, B, K, NP, LD, S.rad[2], S.nst[2], tws, -1);
   c2<T> *col = res == A ? B : A;
   // untangle line cl into rows 2cl, 2cl + 1 (m3 = 0..K/2), stored as k2-columns
   for (int t = threadIdx.x; t < NP * Kh; t += PLANE_THREADS) {
     const int cl = t / Kh, m = t - cl * Kh;
-    const c2<T> Z = res[cl * K + m], W = res[cl * K + (m == 0 ? 0 : K - m)];
+    const c2<T> Z = res[cl * LD + m], W = res[cl * LD + (m == 0 ? 0 : K - m)];
     c2<T> X0, X1;
     X0.x = T(0.5) * (Z.x + W.x); X0.y = T(0.5) * (Z.y - W.y);
     const T dx = Z.x - W.x, dy = Z.y + W.y;  // (Z - conj W) / (2 i)
@@ -1158,15 +1160,15 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane_inv(Dev<T> a, const
     if (up) { X0.y = -X0.y; X1.y = -X1.y; }
     c2<T> Z;
     Z.x = X0.x - X1.y; Z.y = X0.y + X1.x;
-    lin[cl * K + m] = Z;
+    lin[cl * LD + m] = Z;  // line stride LD: odd in 8-byte words
   }
   __syncthreads();
-  c2<T> *res2 = fft_lines<T, L>(lin, res, K, NP, K, S.rad[2], S.nst[2], tws, +1);
+  c2<T> *res2 = fft_lines<T, L, true>(lin, res, K, NP, LD, S.rad[2], S.nst[2], tws, +1);
   using V = v4<T>;
   V *Pp = reinterpret_cast<V *>(a.Phi + S.rgrid0 + (size_t)k1 * K * K);
   for (int t = threadIdx.x; t < NP * Q4; t += PLANE_THREADS) {
     const int cl = t / Q4, q = t - cl * Q4;
-    const c2<T> *z = res2 + cl * K + 4 * q;
+    const c2<T> *z = res2 + cl * LD + 4 * q;
     V r0, r1;
     r0.x = z[0].x; r0.y = z[1].x; r0.z = z[2].x; r0.w = z[3].x;
     r1.x = z[0].y; r1.y = z[1].y; r1.z = z[2].y; r1.w = z[3].y;
