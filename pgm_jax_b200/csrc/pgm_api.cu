@@ -510,7 +510,7 @@ struct Engine : EngineBase {
         }
         g->ng = (int)gs.size();
         g->ntiles = gt.back();
-        g->smem = (axis == 2 ? (size_t)2 * pgm::FFT_PAIRS * (K + 1) : (size_t)2 * pgm::FFT_TILE * (K + 1)) * sizeof(pgm::c2<T>) +
+        g->smem = (axis == 2 ? (size_t)2 * pgm::FFT_PAIRS * K : (size_t)2 * pgm::FFT_TILE * (K + 1)) * sizeof(pgm::c2<T>) +
                   (size_t)K * sizeof(pgm::c2<T>);  // + the twiddle table
         g->sys.upload(gs);
         g->tile0.upload(gt);

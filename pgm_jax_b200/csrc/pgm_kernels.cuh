@@ -918,22 +918,21 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Dev<T> a, const int *gsys, co
   int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;  // first real line
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
-  const int lx = K3 + 1;  // line stride in shared memory: odd in 8-byte words (no bank conflicts)
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * lx, *tws = y + FFT_PAIRS * lx;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
   T *Q = a.Q + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];  // twiddles in shared memory
   staged_copy<2 * FFT_PAIRS * L>(
       2 * np * K3, [&](int t) { return Q[t]; },
       [&](int t, T v) {
         int rl = t / K3, k = t - rl * K3;
-        reinterpret_cast<T *>(&x[(rl >> 1) * lx + k])[rl & 1] = v;
+        reinterpret_cast<T *>(&x[(rl >> 1) * K3 + k])[rl & 1] = v;
       });
   __syncthreads();
-  c2<T> *res = fft_lines<T, L, true>(x, y, K3, np, lx, S.rad[2], S.nst[2], tws, -1);
+  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, -1);
   c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
   for (int t = threadIdx.x; t < np * K3h; t += blockDim.x) {
     int cl = t / K3h, m = t - cl * K3h;
-    c2<T> Z = res[cl * lx + m], W = res[cl * lx + (m == 0 ? 0 : K3 - m)];
+    c2<T> Z = res[cl * K3 + m], W = res[cl * K3 + (m == 0 ? 0 : K3 - m)];
     c2<T> A, Bv;
     A.x = T(0.5) * (Z.x + W.x); A.y = T(0.5) * (Z.y - W.y);
     T dx = Z.x - W.x, dy = Z.y + W.y;  // (Z - conj W) / (2 i)
@@ -956,8 +955,7 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
   int tile = blockIdx.x - gtile0[g];
   int l0 = tile * 2 * FFT_PAIRS;
   int np = min(FFT_PAIRS, (nlines - l0) / 2);
-  const int lx = K3 + 1;  // line stride in shared memory: odd in 8-byte words (no bank conflicts)
-  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * lx, *tws = y + FFT_PAIRS * lx;
+  c2<T> *x = reinterpret_cast<c2<T> *>(smem_raw), *y = x + FFT_PAIRS * K3, *tws = y + FFT_PAIRS * K3;
   const c2<T> *C = a.C + S.cgrid0 + (size_t)l0 * K3h;
   for (int t = threadIdx.x; t < K3; t += blockDim.x) tws[t] = a.tw[S.tw[2] + t];
   staged_copy<FFT_PAIRS * L>(
@@ -976,14 +974,14 @@ __global__ void __launch_bounds__(256) k_fft_x_inv(Dev<T> a, const int *gsys, co
         if (up) { A.y = -A.y; Bv.y = -Bv.y; }
         c2<T> Z;
         Z.x = A.x - Bv.y; Z.y = A.y + Bv.x;
-        x[cl * lx + m] = Z;
+        x[cl * K3 + m] = Z;
       });
   __syncthreads();
-  c2<T> *res = fft_lines<T, L, true>(x, y, K3, np, lx, S.rad[2], S.nst[2], tws, +1);
+  c2<T> *res = fft_lines<T, L>(x, y, K3, np, K3, S.rad[2], S.nst[2], tws, +1);
   T *Phi = a.Phi + S.rgrid0 + (size_t)l0 * K3;
   for (int t = threadIdx.x; t < 2 * np * K3; t += blockDim.x) {
     int rl = t / K3, k = t - rl * K3;
-    c2<T> z = res[(rl >> 1) * lx + k];
+    c2<T> z = res[(rl >> 1) * K3 + k];
     Phi[t] = (rl & 1) ? z.y : z.x;
   }
 }
