@@ -662,7 +662,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restric
       // A(j1, j2) t3 + B(j1, j2) u3 with A = (q t1 + e1 u1) t2 + e2 t1 u2, B = e3 t1 t2.
       const int g0 = b.z >> 2, ng = ((b.z + P - 1) >> 2) - g0 + 1, K34 = K3 >> 2;
       for (int sl = lane; sl < P * P * ng; sl += 32) {
-        int r = sl / ng, gi = sl - r * ng;
+        int r = ng == 2 ? (sl >> 1) : (ng == 3 ? sl / 3 : sl / ng), gi = sl - r * ng;  // no runtime division for 2, 3
         int j1 = r / P, j2 = r - j1 * P;
         T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2];
         T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2];
@@ -1441,7 +1441,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
       // one work item per (stencil row, group)
       const int g0i = b.z >> 2, ng = ((b.z + P - 1) >> 2) - g0i + 1, K34 = K3 >> 2;
       for (int sl = lane; sl < P * P * ng; sl += 32) {
-        const int r = sl / ng, gi = sl - r * ng;
+        const int r = ng == 2 ? (sl >> 1) : (ng == 3 ? sl / 3 : sl / ng), gi = sl - r * ng;  // no runtime division for 2, 3
         const int j1 = r / P, j2 = r - j1 * P;
         int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
         int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
