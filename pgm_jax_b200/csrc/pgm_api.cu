@@ -240,7 +240,7 @@ struct Engine : EngineBase {
   const double *last_hist = nullptr;  // the history of the last predictor solve (profiling)
   DBuf<float4> nn_bl;  // the graph's permanent field of the last solve (for the change channel)
   DBuf<int> nn_valid;  // nn_bl holds a previous step
-  DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by the row build)
+  DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by k_nn_edges)
   DBuf<int> nn_ne;
   // local preconditioner (set.local_niter > 0): the short entries (entry-major) and their counts,
   // the inner CG's vectors
@@ -610,7 +610,7 @@ struct Engine : EngineBase {
     mu_tmp.alloc((size_t)3 * nt); forces_tmp.alloc((size_t)3 * nt); energy_tmp.alloc((size_t)3 * n);
     nn_w.alloc(pgmnn::NN_NPARAM); nn_wb.alloc(pgmnn::NN_WB_ELEMS); nn_inv.alloc((size_t)nt * pgmnn::NN_IN); nn_vec.alloc((size_t)nt * pgmnn::NN_CH * 3);
     nn_mu.alloc((size_t)nt * 3); nn_chan.alloc((size_t)nt * pgm::NN_CHAN); nn_bl.alloc(nt); nn_valid.alloc(1);
-    if (set.predictor == 5) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
+    if (set.predictor == 5) ensure_graph();
     if (set.local_niter > 0) {
       const size_t ns = (size_t)nt * SH_MAX;
       sh_n.alloc(nt); c_k.alloc(ns);
@@ -876,8 +876,15 @@ struct Engine : EngineBase {
 
   // The message-passing model (pgm_mpnn.cu) on the same features and on the graph the row build
   // writes; it replaces the MLP as the learned guess until set_nn or set_mpnn(null).
+  // The graph's edge list (allocated with predictor 5, else when a model is installed or the
+  // features are asked for).
+  void ensure_graph() {
+    if (!nn_e4.p) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
+  }
+
   void set_mpnn(const float *w, int nparam, float sigma, float rg) override {
     ++generation;
+    ensure_graph();
     mp_on = w != nullptr;
     nn_on = mp_on;
     if (w) {
@@ -900,6 +907,7 @@ struct Engine : EngineBase {
   }
 
   void set_nn(const float *w, float sigma, float rg) override {
+    ensure_graph();
     ++generation;  // a captured step depends on whether a model is set, and on sigma and rg
     mp_on = false;
     nn_on = w != nullptr;
@@ -913,10 +921,12 @@ struct Engine : EngineBase {
     nn_rg = rg;
   }
 
-  // The model's inputs at a geometry: rows, then the graph's permanent field (written to bl_out;
-  // its change from bl_prev, when given, is a channel) and the history channels.
+  // The model's inputs at a geometry: the graph's edges, then its permanent field (written to
+  // bl_out; its change from bl_prev, when given, is a channel) and the history channels.
   void nn_inputs(cudaStream_t st, pgm::Dev<T> &a, const double *hist, const float4 *bl_prev, const int *valid, float4 *bl_out,
                  float *inv, float *vec, int *set_valid) {
+    if (!a.nn_e4) throw CudaError{"the learned guess's graph list is not allocated"};
+    launch_prio(pgm::k_nn_edges<T>, nwblk, 256, 0, st, prio_hi, a);
     launch_prio(pgm::k_nn_chan<T>, nwblk, 256, 0, st, prio_hi, a, hist, bl_prev, valid, nn_rg, bl_out, nn_chan.p);
     launch_prio(pgm::k_nn_features<T>, nwblk, 256, 0, st, prio_hi, a, (const float *)nn_chan.p, nn_sigma, nn_rg, inv, vec,
                 set_valid);
@@ -925,6 +935,7 @@ struct Engine : EngineBase {
   void nn_features(cudaStream_t st, const double *pos, const double *box, const double *hist, const float *bl_prev,
                    float *bl_out, float *inv, float *vec) override {
     launches = 0;
+    ensure_graph();
     CK(cudaMemsetAsync(d_status.p, 0, sizeof(unsigned) * nsys, st));
     pgm::Dev<T> a = dev(pos, nullptr, 0, forces_tmp.p, d_status.p);
     prepare(st, a, box);
@@ -978,8 +989,6 @@ struct Engine : EngineBase {
       } else if (which == 3) forces_pass(st, a, nullptr, false);
       else if (which == 4) {
         pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
-        pgm::k_row_kernels<T><<<(int)(((size_t)nt * mc + 255) / 256), 256, 0, st>>>(a);
-        if (set.local_niter > 0) pgm::k_short_kernels<T><<<grid1(nt), 256, 0, st>>>(a);
       }
       else if (which == 5 || which == 6) {  // the first FFT pass (plane or k3), after the spread with 6
         if (which == 6) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
@@ -1080,8 +1089,8 @@ struct Engine : EngineBase {
 
   // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
   // cell list, rows, influence function.
-  // The learned guess's inputs and prediction for this step's rows: forked onto nn_st after the
-  // row build, beside the row kernels and the influence function; solve() joins it.
+  // The learned guess's graph, inputs and prediction for this step: forked onto nn_st after the
+  // candidate list, beside the row build and the influence function; solve() joins it.
   void nn_fork(cudaStream_t st, pgm::Dev<T> &a, const double *hist) {
     CK(cudaEventRecord(ev_nn_fork, st));
     CK(cudaStreamWaitEvent(nn_st, ev_nn_fork, 0));
@@ -1108,10 +1117,8 @@ struct Engine : EngineBase {
                  nb_builds.p);
       launch_pdl(pgm::k_nb_lower, 1, 1, 0, st, nb_flag.p, nb_builds.p);
     }
-    launch_pdl(pgm::k_rows<T>, nwblk, 256, 0, st, a);
     if (nn_hist) nn_fork(st, a, nn_hist);
-    launch_pdl(pgm::k_row_kernels<T>, (int)(((size_t)nt * mc + 255) / 256), 256, 0, st, a);
-    if (set.local_niter > 0) launch_pdl(pgm::k_short_kernels<T>, grid1(nt), 256, 0, st, a);
+    launch_pdl(pgm::k_rows<T>, nwblk, 256, 0, st, a);
     launch_pdl(pgm::k_influence<T>, (int)std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st, a, (long long)cgrid);
   }
 
@@ -1298,7 +1305,7 @@ struct Engine : EngineBase {
       last_hist = ind->hist;
       if (use_nn && !nn_forked) nn_fork(st, a, ind->hist);
       if (use_nn) {
-        CK(cudaStreamWaitEvent(st, ev_nn_join, 0));  // the prediction, computed beside the row kernels
+        CK(cudaStreamWaitEvent(st, ev_nn_join, 0));  // the prediction, computed beside the row build
         nn_forked = false;
       }
       launch_pdl(pgm::k_start1<T>, grid1(nt), 256, 0, st, a, (const double *)ind->hist, K, cc[0], cc[1], cc[2], cc[3],

@@ -66,15 +66,15 @@ struct Dev {
   int *rnv;
   double rce2;
   // the learned guess's graph (the row entries with float(r^2) < nn_rg2): per atom up to nn_emax
-  // edges (x, y, z, partner bits) in row order and the count, written by the row build when
-  // nn_e4 is set (a count above nn_emax: the consumers scan the row)
+  // edges (x, y, z, partner bits) in row order and the full count, written by k_nn_edges (the
+  // consumers read the first nn_emax)
   float4 *nn_e4;
   int *nn_ne;
   int nn_emax;
   float nn_rg2;
   // local preconditioner (local_niter > 0, forcefield.py:1766-1792): the row entries with
   // r^2 < lc2, entry-major (entry e of atom i at e nt + i, at most sh_max, sh_n per atom): partner
-  // and displacement written by the row build, G1 and G2 by k_short_kernels; the inner CG's vectors
+  // displacement, G1 and G2 written by the row build; the inner CG's vectors
   // rr (LRR), alpha rr (LZZ), its directions (LP0 / LP1, alternating), and r_new - r_old of the
   // outer update (DR)
   int *sh_n;
@@ -377,15 +377,124 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 }
 
 // ------------------------------------------------------------------ pair rows
-// Two kernels.  k_rows: one warp per atom finds the row -- the molecule partners (always kept
-// inside the cutoff; the rigid special table of md/topology.py:161-178), then the candidates of the
-// Verlet list (or the caller's rows), masked to r < rc (forcefield.py:1140-1195) -- and writes k, x,
-// y, z compacted by ballot; the next chunk of candidates is loaded before the current one is
-// tested.  k_row_kernels: one thread per row entry evaluates the radial kernels
-// G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r] (forcefield.py:1314-1338, kernels.py:76-118).
+// k_rows: one warp per atom finds the row -- the molecule partners (always kept inside the cutoff;
+// the rigid special table of md/topology.py:161-178), then the candidates of the Verlet list (or
+// the caller's rows), masked to r < rc (forcefield.py:1140-1195) -- and writes k, x, y, z compacted
+// by ballot, with the radial kernels G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r]
+// (forcefield.py:1314-1338, kernels.py:76-118) of every entry, evaluated by the lane that keeps it
+// from the rounded displacement it stores.  k_nn_edges runs the same scan for the learned guess's
+// graph on its own stream.
+
+// FP32 sequential minimum image (the mixed-precision row build's candidate loop).
+__device__ __forceinline__ void min_image_fast_f(float &x, float &y, float &z, const float *H, const float *id) {
+  float n = rintf(z * id[2]);
+  x -= n * H[6]; y -= n * H[7]; z -= n * H[8];
+  n = rintf(y * id[1]);
+  x -= n * H[3]; y -= n * H[4];
+  n = rintf(x * id[0]);
+  x -= n * H[0];
+}
+
+// The row scan of atom i by one warp: the molecule partners (special = true), then the candidates,
+// one entry per lane and round, the next round's candidate loaded before the current one is tested.
+// visit(keep, j, x, y, z, special) runs on all 32 lanes every round (it may use warp collectives);
+// keep is r < rc for an entry of another atom, false on lanes without one.  Mixed precision: the
+// candidates' FP32 displacements from the wrapped FP32 positions (16-byte gathers; the rows store
+// FP32 displacements anyway).
+template <typename T, typename Visit>
+__device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, const BoxInfo &B, int i, int lane, Visit &&visit) {
+  double H[9], id[3];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) H[k] = B.H[k];
+  id[0] = B.idiag[0]; id[1] = B.idiag[1]; id[2] = B.idiag[2];
+  const double4 pi = a.pos4[i];
+  const double rc2 = a.cutoff * a.cutoff;
+  const int mf = a.molfirst[i], me = a.molend[i];
+  for (int j0 = mf; j0 < me; j0 += 32) {
+    int j = j0 + lane;
+    bool keep = false;
+    double x = 0, y = 0, z = 0;
+    if (j < me && j != i) {
+      double4 pj = a.pos4[j];
+      x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
+      min_image_fast(x, y, z, H, id);
+      keep = x * x + y * y + z * z < rc2;
+    }
+    visit(keep, j, x, y, z, true);
+  }
+  const int mi = (int)pi.w;
+  const int *row;
+  int nc;
+  if (a.idx) {  // the caller's candidate rows (local indices, padding natom)
+    row = a.idx + (size_t)i * a.idx_width;
+    nc = a.idx_width;
+  } else {      // the engine's Verlet candidates (within cutoff + skin at the last rebuild)
+    row = a.cand + (size_t)i * a.cc;
+    nc = min(a.ncand[i], a.cc);
+  }
+  auto partner = [&](int c) {
+    int j = -1;
+    if (c < nc) {
+      int jl = row[c];
+      if (a.idx) j = (jl >= 0 && jl < S.natom) ? S.atom0 + jl : -1;
+      else j = jl;
+    }
+    return j;
+  };
+  if (sizeof(T) == 4 && a.pos4f) {
+    float Hf[9], idf[3];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Hf[k] = float(H[k]);
+    idf[0] = float(id[0]); idf[1] = float(id[1]); idf[2] = float(id[2]);
+    const float4 pf = a.pos4f[i];
+    const float rc2f = float(rc2);
+    int jn = partner(lane);
+    float4 pn = jn >= 0 ? a.pos4f[jn] : make_float4(0.f, 0.f, 0.f, -1.f);
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      const int j = jn;
+      const float4 pj = pn;
+      jn = partner(c0 + 32 + lane);  // prefetch the next round
+      if (jn >= 0) pn = a.pos4f[jn];
+      bool keep = false;
+      float x = 0.f, y = 0.f, z = 0.f;
+      if (j >= 0 && (int)pj.w != mi) {
+        x = pf.x - pj.x; y = pf.y - pj.y; z = pf.z - pj.z;
+        min_image_fast_f(x, y, z, Hf, idf);
+        keep = x * x + y * y + z * z < rc2f;
+      }
+      visit(keep, j, x, y, z, false);
+    }
+  } else {
+    int jn = partner(lane);
+    double4 pn = jn >= 0 ? a.pos4[jn] : make_double4(0, 0, 0, -1);
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      const int j = jn;
+      const double4 pj = pn;
+      jn = partner(c0 + 32 + lane);  // prefetch the next round
+      if (jn >= 0) pn = a.pos4[jn];
+      bool keep = false;
+      double x = 0, y = 0, z = 0;
+      if (j >= 0 && (int)pj.w != mi) {
+        x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
+        min_image_fast(x, y, z, H, id);
+        keep = x * x + y * y + z * z < rc2;
+      }
+      visit(keep, j, x, y, z, false);
+    }
+  }
+}
+
+// Whether a row entry (keep: r < rc) is an edge of the learned guess's graph: r < rg, and inside the
+// electrostatics cutoff with split rows.
+template <typename T>
+__device__ __forceinline__ bool nn_is_edge(const Dev<T> &a, bool keep, double x, double y, double z) {
+  const double r2 = x * x + y * y + z * z;
+  return keep && !(a.rnv && !(r2 < a.rce2)) && float(r2) < a.nn_rg2;
+}
+
 template <typename T>
 __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, double x, double y, double z, size_t base, int &count,
-                                         int lane, int i, int &ecount, int &vcount, int &scount, bool special) {
+                                         int lane, int i, T Ri, int &vcount, int &scount, bool special) {
   const unsigned lt = (1u << lane) - 1u;
   const double r2 = x * x + y * y + z * z;
   bool kv = false;
@@ -395,10 +504,20 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
   }
   unsigned bal = __ballot_sync(0xffffffffu, keep);
   const int slot = count + __popc(bal & lt);
+  T g1 = T(0), g2 = T(0);
   if (keep && slot < a.mce) {
-    size_t o = base + slot;
+    const size_t o = base + slot;
+    const T xt = T(x), yt = T(y), zt = T(z);
     a.rk[o] = j;
-    a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
+    a.rx[o] = xt; a.ry[o] = yt; a.rz[o] = zt;
+    const T r = t_sqrt(xt * xt + yt * yt + zt * zt), Rk = a.radius[j];
+    const T aik = t_rsqrt(T(2) * (Ri * Ri + Rk * Rk));
+    T A[4], Bb[4];
+    erf_kernels<T>(aik, r, A);
+    erf_kernels<T>(T(a.beta), r, Bb);
+    g1 = A[1] - Bb[1];
+    g2 = A[2] - Bb[2];
+    a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = g1; a.rg2[o] = g2; a.rg3[o] = A[3] - Bb[3];
   }
   count += __popc(bal);
   if (a.rnv) {
@@ -411,7 +530,7 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
     }
     vcount += __popc(bv);
   }
-  if (a.sh_n) {  // the local preconditioner's entries: partner and displacement, entry-major
+  if (a.sh_n) {  // the local preconditioner's entries: partner, displacement, G1, G2, entry-major
     const bool sh = keep && slot < a.mce && r2 < a.lc2;
     const unsigned sb = __ballot_sync(0xffffffffu, sh);
     const int at = scount + __popc(sb & lt);
@@ -419,135 +538,30 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
       const size_t c = (size_t)at * a.nt + i;
       a.c_k[c] = j;
       a.c_x[c] = T(x); a.c_y[c] = T(y); a.c_z[c] = T(z);
+      a.c_g1[c] = g1; a.c_g2[c] = g2;
     }
     scount += __popc(sb);
   }
-  if (a.nn_e4) {  // the learned guess's graph edges: the short entries, with their displacement
-    const bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
-    const unsigned eb = __ballot_sync(0xffffffffu, sh);
-    const int at = ecount + __popc(eb & lt);
-    if (sh && at < a.nn_emax) a.nn_e4[(size_t)i * a.nn_emax + at] = make_float4(float(x), float(y), float(z), __int_as_float(j));
-    ecount += __popc(eb);
-  }
-}
-
-// FP32 sequential minimum image (the mixed-precision row build's candidate loop).
-__device__ __forceinline__ void min_image_fast_f(float &x, float &y, float &z, const float *H, const float *id) {
-  float n = rintf(z * id[2]);
-  x -= n * H[6]; y -= n * H[7]; z -= n * H[8];
-  n = rintf(y * id[1]);
-  x -= n * H[3]; y -= n * H[4];
-  n = rintf(x * id[0]);
-  x -= n * H[0];
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int blk = blockIdx.x;
-  int s = a.wb_sys[blk];
-  int i = a.wb_atom0[blk] + warp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = a.wb_sys[blockIdx.x];
+  const int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
   if (i >= S.atom0 + S.natom) return;
-  const BoxInfo &B = a.box[s];
-  double H[9], id[3];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) H[k] = B.H[k];
-  id[0] = B.idiag[0]; id[1] = B.idiag[1]; id[2] = B.idiag[2];
-  double4 pi = a.pos4[i];
-  double rc2 = a.cutoff * a.cutoff;
-  size_t base = (size_t)i * a.mc;
-  int count = 0, ecount = 0, vcount = 0, scount = 0;
-  int mf = a.molfirst[i], me = a.molend[i];
-  for (int j0 = mf; j0 < me; j0 += 32) {
-    int j = j0 + lane;
-    bool keep = false;
-    double x = 0, y = 0, z = 0;
-    if (j < me && j != i) {
-      double4 pj = a.pos4[j];
-      x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
-      min_image_fast(x, y, z, H, id);
-      keep = x * x + y * y + z * z < rc2;
-    }
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, true);
-  }
-  int nsp = count;
-  int mi = (int)pi.w;
-  const int *row;
-  int nc;
-  if (a.idx) {  // the caller's candidate rows (local indices, padding natom)
-    row = a.idx + (size_t)i * a.idx_width;
-    nc = a.idx_width;
-  } else {      // the engine's Verlet candidates (within cutoff + skin at the last rebuild)
-    row = a.cand + (size_t)i * a.cc;
-    nc = min(a.ncand[i], a.cc);
-  }
-  auto load = [&](int c, int &j, double4 &pj) {
-    j = -1;
-    if (c < nc) {
-      int jl = row[c];
-      if (a.idx) j = (jl >= 0 && jl < S.natom) ? S.atom0 + jl : -1;
-      else j = jl;
-      if (j >= 0) pj = a.pos4[j];
-    }
-  };
-  if (sizeof(T) == 4 && a.pos4f) {
-    // mixed precision: FP32 displacements from the wrapped FP32 positions (16-byte gathers; the
-    // rows store FP32 displacements anyway)
-    float Hf[9], idf[3];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) Hf[k] = float(H[k]);
-    idf[0] = float(id[0]); idf[1] = float(id[1]); idf[2] = float(id[2]);
-    const float4 pf = a.pos4f[i];
-    const float rc2f = float(rc2);
-    auto loadf = [&](int c, int &j, float4 &pj) {
-      j = -1;
-      if (c < nc) {
-        int jl = row[c];
-        if (a.idx) j = (jl >= 0 && jl < S.natom) ? S.atom0 + jl : -1;
-        else j = jl;
-        if (j >= 0) pj = a.pos4f[j];
-      }
-    };
-    int jn = -1;
-    float4 pn = make_float4(0.f, 0.f, 0.f, -1.f);
-    loadf(lane, jn, pn);
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-      int j = jn;
-      float4 pj = pn;
-      loadf(c0 + 32 + lane, jn, pn);  // prefetch the next chunk
-      bool keep = false;
-      float x = 0.f, y = 0.f, z = 0.f;
-      if (j >= 0 && (int)pj.w != mi) {
-        x = pf.x - pj.x; y = pf.y - pj.y; z = pf.z - pj.z;
-        min_image_fast_f(x, y, z, Hf, idf);
-        keep = x * x + y * y + z * z < rc2f;
-      }
-      row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, false);
-    }
-  } else {
-    int jn = -1;
-    double4 pn = make_double4(0, 0, 0, -1);
-    load(lane, jn, pn);
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-      int j = jn;
-      double4 pj = pn;
-      load(c0 + 32 + lane, jn, pn);  // prefetch the next chunk
-      bool keep = false;
-      double x = 0, y = 0, z = 0;
-      if (j >= 0 && (int)pj.w != mi) {
-        x = pi.x - pj.x; y = pi.y - pj.y; z = pi.z - pj.z;
-        min_image_fast(x, y, z, H, id);
-        keep = x * x + y * y + z * z < rc2;
-      }
-      row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, ecount, vcount, scount, false);
-    }
-  }
+  const T Ri = a.radius[i];
+  const size_t base = (size_t)i * a.mc;
+  int count = 0, vcount = 0, scount = 0, nsp = 0;
+  row_scan(a, S, a.box[s], i, lane, [&](bool keep, int j, double x, double y, double z, bool special) {
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, Ri, vcount, scount, special);
+    if (special) nsp = count;
+  });
   if (lane == 0) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
-    if (a.nn_e4) a.nn_ne[i] = ecount;
     if (a.sh_n) {
       a.sh_n[i] = min(scount, a.sh_max);
       if (scount > a.sh_max) atomicOr(&a.status[s], 0x20u);  // the preconditioner kept the first sh_max
@@ -562,22 +576,26 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   }
 }
 
+// The learned guess's graph: the row entries closer than rg (partner and FP32 displacement, in row
+// order, at most nn_emax kept; nn_ne the full count), by the row scan's own arithmetic, one warp per
+// atom.  It reads only positions and candidates, so it runs beside the row build.
 template <typename T>
-__global__ void __launch_bounds__(256) k_row_kernels(Dev<T> a) {
-  pdl_enter();  // launched as a programmatic dependent of the previous kernel
-  size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  int i = (int)(t / a.mc), slot = (int)(t - (size_t)i * a.mc);
-  if (i >= a.nt || slot >= min(a.rn[i], a.mce)) return;
-  size_t o = (size_t)i * a.mc + slot;
-  T x = a.rx[o], y = a.ry[o], z = a.rz[o];
-  int k = a.rk[o];
-  T Ri = a.radius[i], Rk = a.radius[k];
-  T r = t_sqrt(x * x + y * y + z * z);
-  T aik = t_rsqrt(T(2) * (Ri * Ri + Rk * Rk));
-  T A[4], Bb[4];
-  erf_kernels<T>(aik, r, A);
-  erf_kernels<T>(T(a.beta), r, Bb);
-  a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = A[1] - Bb[1]; a.rg2[o] = A[2] - Bb[2]; a.rg3[o] = A[3] - Bb[3];
+__global__ void __launch_bounds__(256, 6) k_nn_edges(Dev<T> a) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = a.wb_sys[blockIdx.x];
+  const int i = a.wb_atom0[blockIdx.x] + warp;
+  const SysInfo &S = a.sys[s];
+  if (i >= S.atom0 + S.natom) return;
+  float4 *out = a.nn_e4 + (size_t)i * a.nn_emax;
+  int ecount = 0;
+  row_scan(a, S, a.box[s], i, lane, [&](bool keep, int j, double x, double y, double z, bool) {
+    const bool e = nn_is_edge(a, keep, x, y, z);
+    const unsigned eb = __ballot_sync(0xffffffffu, e);
+    const int at = ecount + __popc(eb & ((1u << lane) - 1u));
+    if (e && at < a.nn_emax) out[at] = make_float4(float(x), float(y), float(z), __int_as_float(j));
+    ecount += __popc(eb);
+  });
+  if (lane == 0) a.nn_ne[i] = ecount;
 }
 
 // ------------------------------------------------------------------ PME influence function
@@ -1537,23 +1555,12 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
 // c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
 // NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
 constexpr int NN_CHAN = 12;
-// The graph edges of atom i: from the list the row build wrote, one edge per lane and round, or,
-// when the list overflowed (or there is none), by a scan of the row (each edge on the lane that
-// reads it).
+// The graph edges of atom i from the list k_nn_edges wrote, one edge per lane and round (edges past
+// nn_emax are not read, as in the message-passing model).
 template <typename T, typename F>
 __device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, F &&edge) {
   const int lane = threadIdx.x & 31;
-  const int ne = a.nn_e4 ? a.nn_ne[i] : a.nn_emax + 1;
-  if (ne > a.nn_emax) {
-    const int n = min(a.rn[i], a.mce);
-    const size_t base = (size_t)i * a.mc;
-    for (int t = lane; t < n; t += 32) {
-      const size_t o = base + t;
-      const double x = a.rx[o], y = a.ry[o], z = a.rz[o];
-      if (float(x * x + y * y + z * z) < a.nn_rg2) edge(a.rk[o], float(x), float(y), float(z), t);
-    }
-    return;
-  }
+  const int ne = min(a.nn_ne[i], a.nn_emax);
   const float4 *list = a.nn_e4 + (size_t)i * a.nn_emax;
   for (int e = lane; e < ne; e += 32) {
     const float4 v = list[e];
@@ -2015,28 +2022,6 @@ __global__ void k_cg_update_check(Dev<T> a, int nsys, double tol, int max_iter, 
 // entries closer than local_cut of T v_k, T v = -G2 (v . x) x + G1 v (the row field's pair term),
 // started from z = alpha r (forcefield.py:1766-1792; the outer CG is then flexible, with the
 // Polak-Ribiere beta it already uses).  Thread per atom; the short entries compacted entry-major.
-
-// Once per step after the row build: G1, G2 of the short entries (the row build wrote partner and
-// displacement), by the same arithmetic as k_row_kernels on the same rounded displacements.
-template <typename T>
-__global__ void k_short_kernels(Dev<T> a) {
-  pdl_enter();  // launched as a programmatic dependent of the previous kernel
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nt) return;
-  const int n = a.sh_n[i];
-  const T Ri = a.radius[i];
-  for (int e = 0; e < n; ++e) {
-    const size_t c = (size_t)e * a.nt + i;
-    const T x = a.c_x[c], y = a.c_y[c], z = a.c_z[c], Rk = a.radius[a.c_k[c]];
-    const T r = t_sqrt(x * x + y * y + z * z);
-    const T aik = t_rsqrt(T(2) * (Ri * Ri + Rk * Rk));
-    T A[4], Bb[4];
-    erf_kernels<T>(aik, r, A);
-    erf_kernels<T>(T(a.beta), r, Bb);
-    a.c_g1[c] = A[1] - Bb[1];
-    a.c_g2[c] = A[2] - Bb[2];
-  }
-}
 
 // sum over atom i's short entries of T v_k (get(k) = v_k)
 template <typename T, typename Get>
