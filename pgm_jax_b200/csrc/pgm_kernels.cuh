@@ -66,8 +66,8 @@ struct Dev {
   int *rnv;
   double rce2;
   // the learned guess's graph (the row entries with float(r^2) < nn_rg2): per atom up to nn_emax
-  // edges (x, y, z, partner bits) in row order and the full count, written by k_nn_edges (the
-  // consumers read the first nn_emax)
+  // edges (x, y, z, partner bits) in row order and the full count, written by the row build when
+  // nn_e4 is set (the consumers read the first nn_emax)
   float4 *nn_e4;
   int *nn_ne;
   int nn_emax;
@@ -382,8 +382,8 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 // the caller's rows), masked to r < rc (forcefield.py:1140-1195) -- and writes k, x, y, z compacted
 // by ballot, with the radial kernels G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r]
 // (forcefield.py:1314-1338, kernels.py:76-118) of every entry, evaluated by the lane that keeps it
-// from the rounded displacement it stores.  k_nn_edges runs the same scan for the learned guess's
-// graph on its own stream.
+// from the rounded displacement it stores; with them the local preconditioner's short entries and
+// the learned guess's graph edges.
 
 // FP32 sequential minimum image (the mixed-precision row build's candidate loop).
 __device__ __forceinline__ void min_image_fast_f(float &x, float &y, float &z, const float *H, const float *id) {
@@ -484,17 +484,9 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
   }
 }
 
-// Whether a row entry (keep: r < rc) is an edge of the learned guess's graph: r < rg, and inside the
-// electrostatics cutoff with split rows.
-template <typename T>
-__device__ __forceinline__ bool nn_is_edge(const Dev<T> &a, bool keep, double x, double y, double z) {
-  const double r2 = x * x + y * y + z * z;
-  return keep && !(a.rnv && !(r2 < a.rce2)) && float(r2) < a.nn_rg2;
-}
-
 template <typename T>
 __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, double x, double y, double z, size_t base, int &count,
-                                         int lane, int i, T Ri, int &vcount, int &scount, bool special) {
+                                         int lane, int i, T Ri, int &ecount, int &vcount, int &scount, bool special) {
   const unsigned lt = (1u << lane) - 1u;
   const double r2 = x * x + y * y + z * z;
   bool kv = false;
@@ -542,6 +534,13 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
     }
     scount += __popc(sb);
   }
+  if (a.nn_e4) {  // the learned guess's graph edges: the entries closer than rg, with their displacement
+    const bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
+    const unsigned eb = __ballot_sync(0xffffffffu, sh);
+    const int at = ecount + __popc(eb & lt);
+    if (sh && at < a.nn_emax) a.nn_e4[(size_t)i * a.nn_emax + at] = make_float4(float(x), float(y), float(z), __int_as_float(j));
+    ecount += __popc(eb);
+  }
 }
 
 template <typename T>
@@ -554,14 +553,15 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   if (i >= S.atom0 + S.natom) return;
   const T Ri = a.radius[i];
   const size_t base = (size_t)i * a.mc;
-  int count = 0, vcount = 0, scount = 0, nsp = 0;
+  int count = 0, ecount = 0, vcount = 0, scount = 0, nsp = 0;
   row_scan(a, S, a.box[s], i, lane, [&](bool keep, int j, double x, double y, double z, bool special) {
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, Ri, vcount, scount, special);
+    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, Ri, ecount, vcount, scount, special);
     if (special) nsp = count;
   });
   if (lane == 0) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
+    if (a.nn_e4) a.nn_ne[i] = ecount;
     if (a.sh_n) {
       a.sh_n[i] = min(scount, a.sh_max);
       if (scount > a.sh_max) atomicOr(&a.status[s], 0x20u);  // the preconditioner kept the first sh_max
@@ -574,28 +574,6 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
       atomicMax(a.max_count + 1, vcount);
     }
   }
-}
-
-// The learned guess's graph: the row entries closer than rg (partner and FP32 displacement, in row
-// order, at most nn_emax kept; nn_ne the full count), by the row scan's own arithmetic, one warp per
-// atom.  It reads only positions and candidates, so it runs beside the row build.
-template <typename T>
-__global__ void __launch_bounds__(256, 6) k_nn_edges(Dev<T> a) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int s = a.wb_sys[blockIdx.x];
-  const int i = a.wb_atom0[blockIdx.x] + warp;
-  const SysInfo &S = a.sys[s];
-  if (i >= S.atom0 + S.natom) return;
-  float4 *out = a.nn_e4 + (size_t)i * a.nn_emax;
-  int ecount = 0;
-  row_scan(a, S, a.box[s], i, lane, [&](bool keep, int j, double x, double y, double z, bool) {
-    const bool e = nn_is_edge(a, keep, x, y, z);
-    const unsigned eb = __ballot_sync(0xffffffffu, e);
-    const int at = ecount + __popc(eb & ((1u << lane) - 1u));
-    if (e && at < a.nn_emax) out[at] = make_float4(float(x), float(y), float(z), __int_as_float(j));
-    ecount += __popc(eb);
-  });
-  if (lane == 0) a.nn_ne[i] = ecount;
 }
 
 // ------------------------------------------------------------------ PME influence function
@@ -1555,7 +1533,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
 // c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
 // NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
 constexpr int NN_CHAN = 12;
-// The graph edges of atom i from the list k_nn_edges wrote, one edge per lane and round (edges past
+// The graph edges of atom i from the list the row build wrote, one edge per lane and round (edges past
 // nn_emax are not read, as in the message-passing model).
 template <typename T, typename F>
 __device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, F &&edge) {

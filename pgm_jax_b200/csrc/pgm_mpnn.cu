@@ -2,7 +2,7 @@
 //
 // Per atom i, from the features of the channel and feature passes (pgm_kernels.cuh: 16 rotation
 // invariants inv_i and 15 vector channels v_i,c), on the graph of the row entries closer than the
-// graph cutoff rg (the list k_nn_edges writes: per atom up to emax edges (x, y, z, partner)):
+// graph cutoff rg (the list the row build writes: per atom up to emax edges (x, y, z, partner)):
 //   h0 = SiLU(W0 inv + b0)                                       16 -> 64
 //   two message-passing layers, each a continuous-filter convolution (SchNet, Schuett et al. 2017):
 //     g = W_g h                                                  64 -> 16 message features

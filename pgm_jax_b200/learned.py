@@ -155,7 +155,7 @@ def guess_errors(model: GuessModel, data: dict) -> dict:
 
 
 # ----------------------------------------------------------------------------- message passing
-EMAX = 128  # graph edges kept per atom (the list k_nn_edges writes)
+EMAX = 128  # graph edges kept per atom (the row build's list)
 # W0, b0, per layer (W_g, W_f, W_a, b_a, W_b, b_b), W_o, b_o: (out, in) matrices
 MPNN_SHAPES = [(64, 16), (64,)] + [(16, 64), (16, 8), (64, 80), (64,), (64, 64), (64,)] * 2 + [(16, 64), (16,)]
 
