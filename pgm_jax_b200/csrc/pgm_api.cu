@@ -240,7 +240,7 @@ struct Engine : EngineBase {
   const double *last_hist = nullptr;  // the history of the last predictor solve (profiling)
   DBuf<float4> nn_bl;  // the graph's permanent field of the last solve (for the change channel)
   DBuf<int> nn_valid;  // nn_bl holds a previous step
-  DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by k_nn_edges)
+  DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by the row build)
   DBuf<int> nn_ne;
   // local preconditioner (set.local_niter > 0): the short entries (entry-major) and their counts,
   // the inner CG's vectors
@@ -921,12 +921,12 @@ struct Engine : EngineBase {
     nn_rg = rg;
   }
 
-  // The model's inputs at a geometry: the graph's edges, then its permanent field (written to
-  // bl_out; its change from bl_prev, when given, is a channel) and the history channels.
+  // The model's inputs at a geometry (the row build wrote the graph's edges): the graph's permanent
+  // field (written to bl_out; its change from bl_prev, when given, is a channel) and the history
+  // channels.
   void nn_inputs(cudaStream_t st, pgm::Dev<T> &a, const double *hist, const float4 *bl_prev, const int *valid, float4 *bl_out,
                  float *inv, float *vec, int *set_valid) {
     if (!a.nn_e4) throw CudaError{"the learned guess's graph list is not allocated"};
-    launch_prio(pgm::k_nn_edges<T>, nwblk, 256, 0, st, prio_hi, a);
     launch_prio(pgm::k_nn_chan<T>, nwblk, 256, 0, st, prio_hi, a, hist, bl_prev, valid, nn_rg, bl_out, nn_chan.p);
     launch_prio(pgm::k_nn_features<T>, nwblk, 256, 0, st, prio_hi, a, (const float *)nn_chan.p, nn_sigma, nn_rg, inv, vec,
                 set_valid);
@@ -1089,8 +1089,8 @@ struct Engine : EngineBase {
 
   // Geometry of a step: box, fractional coordinates and permanent dipoles, molecular offsets,
   // cell list, rows, influence function.
-  // The learned guess's graph, inputs and prediction for this step: forked onto nn_st after the
-  // candidate list, beside the row build and the influence function; solve() joins it.
+  // The learned guess's inputs and prediction for this step's graph: forked onto nn_st after the
+  // row build, beside the influence function and the solve's set-up; solve() joins it.
   void nn_fork(cudaStream_t st, pgm::Dev<T> &a, const double *hist) {
     CK(cudaEventRecord(ev_nn_fork, st));
     CK(cudaStreamWaitEvent(nn_st, ev_nn_fork, 0));
@@ -1117,8 +1117,8 @@ struct Engine : EngineBase {
                  nb_builds.p);
       launch_pdl(pgm::k_nb_lower, 1, 1, 0, st, nb_flag.p, nb_builds.p);
     }
-    if (nn_hist) nn_fork(st, a, nn_hist);
     launch_pdl(pgm::k_rows<T>, nwblk, 256, 0, st, a);
+    if (nn_hist) nn_fork(st, a, nn_hist);
     launch_pdl(pgm::k_influence<T>, (int)std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st, a, (long long)cgrid);
   }
 
@@ -1196,11 +1196,11 @@ struct Engine : EngineBase {
   template <int ACT, int MODE>
   void local_precond(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
     const int L = set.local_niter;
-    launch_pdl(pgm::k_lp_start<T, ACT>, ntblk, 256, 0, st, a);
+    launch_pdl(pgm::k_lp_start<T, ACT>, ntblk, pgm::LP_THREADS, 0, st, a);
     for (int j = 1; j <= L; ++j) {
       pgm::v4<T> *cur = (j & 1) ? LP0.p : LP1.p, *prev = (j & 1) ? LP1.p : LP0.p;
-      if (j == 1) launch_pdl(pgm::k_lp_ap<T, ACT, true>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)prev, cur);
-      else launch_pdl(pgm::k_lp_ap<T, ACT, false>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)prev, cur);
+      if (j == 1) launch_pdl(pgm::k_lp_ap<T, ACT, true>, ntblk, pgm::LP_THREADS, 0, st, a, (const pgm::v4<T> *)prev, cur);
+      else launch_pdl(pgm::k_lp_ap<T, ACT, false>, ntblk, pgm::LP_THREADS, 0, st, a, (const pgm::v4<T> *)prev, cur);
       if (j < L)
         launch_pdl(pgm::k_lp_step<T, ACT, false, MODE>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)cur, nsys, set.dipole_tol,
                    set.max_iter, dany.p, cond, use_cond, cg_done.p);
