@@ -398,9 +398,9 @@ __device__ __forceinline__ void min_image_fast_f(float &x, float &y, float &z, c
 // The row scan of atom i by one warp: the molecule partners (special = true), then the candidates,
 // one entry per lane and round, the next round's candidate loaded before the current one is tested.
 // visit(keep, j, x, y, z, special) runs on all 32 lanes every round (it may use warp collectives);
-// keep is r < rc for an entry of another atom, false on lanes without one.  Mixed precision: the
-// candidates' FP32 displacements from the wrapped FP32 positions (16-byte gathers; the rows store
-// FP32 displacements anyway).
+// keep is r < rc for an entry of another atom, false on lanes without one; the displacement comes
+// as T, as the rows store it.  Mixed precision: the candidates' FP32 displacements from the wrapped
+// FP32 positions (16-byte gathers), the molecule partners' rounded from FP64.
 template <typename T, typename Visit>
 __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, const BoxInfo &B, int i, int lane, Visit &&visit) {
   double H[9], id[3];
@@ -420,7 +420,7 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
       min_image_fast(x, y, z, H, id);
       keep = x * x + y * y + z * z < rc2;
     }
-    visit(keep, j, x, y, z, true);
+    visit(keep, j, T(x), T(y), T(z), true);
   }
   const int mi = (int)pi.w;
   const int *row;
@@ -479,18 +479,18 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
         min_image_fast(x, y, z, H, id);
         keep = x * x + y * y + z * z < rc2;
       }
-      visit(keep, j, x, y, z, false);
+      visit(keep, j, T(x), T(y), T(z), false);
     }
   }
 }
 
 template <typename T>
-__device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, double x, double y, double z, size_t base, int &count,
-                                         int lane, int i, T Ri, int &ecount, int &vcount, int &scount, bool special) {
+__device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x, T y, T z, size_t base, int &count, int lane,
+                                         int i, T Ri, int &ecount, int &vcount, int &scount, bool special) {
   const unsigned lt = (1u << lane) - 1u;
-  const double r2 = x * x + y * y + z * z;
+  const T r2 = x * x + y * y + z * z;  // the tests below in the rows' precision
   bool kv = false;
-  if (a.rnv && keep && !(r2 < a.rce2)) {  // split rows: beyond elec_cutoff only pairs with an LJ term stay
+  if (a.rnv && keep && !(r2 < T(a.rce2))) {  // split rows: beyond elec_cutoff only pairs with an LJ term stay
     kv = !special && j >= 0 && a.seps[i] * a.seps[j] != T(0);  // molecule partners have LJ weight 0
     keep = false;
   }
@@ -499,10 +499,9 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
   T g1 = T(0), g2 = T(0);
   if (keep && slot < a.mce) {
     const size_t o = base + slot;
-    const T xt = T(x), yt = T(y), zt = T(z);
     a.rk[o] = j;
-    a.rx[o] = xt; a.ry[o] = yt; a.rz[o] = zt;
-    const T r = t_sqrt(xt * xt + yt * yt + zt * zt), Rk = a.radius[j];
+    a.rx[o] = x; a.ry[o] = y; a.rz[o] = z;
+    const T r = t_sqrt(r2), Rk = a.radius[j];
     const T aik = t_rsqrt(T(2) * (Ri * Ri + Rk * Rk));
     T A[4], Bb[4];
     erf_kernels<T>(aik, r, A);
@@ -518,18 +517,18 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, doub
     if (kv && sv < a.mc - a.mce) {
       size_t o = base + a.mce + sv;
       a.rk[o] = j;
-      a.rx[o] = T(x); a.ry[o] = T(y); a.rz[o] = T(z);
+      a.rx[o] = x; a.ry[o] = y; a.rz[o] = z;
     }
     vcount += __popc(bv);
   }
   if (a.sh_n) {  // the local preconditioner's entries: partner, displacement, G1, G2, entry-major
-    const bool sh = keep && slot < a.mce && r2 < a.lc2;
+    const bool sh = keep && slot < a.mce && r2 < T(a.lc2);
     const unsigned sb = __ballot_sync(0xffffffffu, sh);
     const int at = scount + __popc(sb & lt);
     if (sh && at < a.sh_max) {
       const size_t c = (size_t)at * a.nt + i;
       a.c_k[c] = j;
-      a.c_x[c] = T(x); a.c_y[c] = T(y); a.c_z[c] = T(z);
+      a.c_x[c] = x; a.c_y[c] = y; a.c_z[c] = z;
       a.c_g1[c] = g1; a.c_g2[c] = g2;
     }
     scount += __popc(sb);
@@ -554,7 +553,7 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   const T Ri = a.radius[i];
   const size_t base = (size_t)i * a.mc;
   int count = 0, ecount = 0, vcount = 0, scount = 0, nsp = 0;
-  row_scan(a, S, a.box[s], i, lane, [&](bool keep, int j, double x, double y, double z, bool special) {
+  row_scan(a, S, a.box[s], i, lane, [&](bool keep, int j, T x, T y, T z, bool special) {
     row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, Ri, ecount, vcount, scount, special);
     if (special) nsp = count;
   });
@@ -2001,12 +2000,18 @@ __global__ void k_cg_update_check(Dev<T> a, int nsys, double tol, int max_iter, 
 // started from z = alpha r (forcefield.py:1766-1792; the outer CG is then flexible, with the
 // Polak-Ribiere beta it already uses).  Thread per atom; the short entries compacted entry-major.
 
-// sum over atom i's short entries of T v_k (get(k) = v_k)
+// The inner kernels run LP_LANES threads per atom (consecutive lanes; blocks of 256 atoms), each
+// summing every LP_LANES-th short entry, so that more entry gathers are in flight.
+constexpr int LP_LANES = 4;
+constexpr int LP_THREADS = THREADS_PER_BLOCK * LP_LANES;
+
+// sum over atom i's short entries of T v_k (get(k) = v_k), entries q, q + LP_LANES, ... on lane q
+// of the atom's group, then combined over the group (every lane of the warp takes part; an atom
+// past the system's end has n = 0)
 template <typename T, typename Get>
-__device__ __forceinline__ void short_sum(const Dev<T> &a, int i, Get &&get, T &f0, T &f1, T &f2) {
-  const int n = a.sh_n[i];
-#pragma unroll 4
-  for (int e = 0; e < n; ++e) {
+__device__ __forceinline__ void short_sum(const Dev<T> &a, int i, int n, int q, Get &&get, T &f0, T &f1, T &f2) {
+#pragma unroll 2
+  for (int e = q; e < n; e += LP_LANES) {
     const size_t c = (size_t)e * a.nt + i;
     const T x = a.c_x[c], y = a.c_y[c], z = a.c_z[c], g1 = a.c_g1[c], g2 = a.c_g2[c];
     const v4<T> v = get(a.c_k[c]);
@@ -2014,6 +2019,26 @@ __device__ __forceinline__ void short_sum(const Dev<T> &a, int i, Get &&get, T &
     f0 += cc * x + g1 * v.x;
     f1 += cc * y + g1 * v.y;
     f2 += cc * z + g1 * v.z;
+  }
+#pragma unroll
+  for (int o = 1; o < LP_LANES; o <<= 1) {
+    f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+  }
+}
+
+// the sum over a block of NT threads of v added to *dst (one atomic per block)
+template <int NT>
+__device__ __forceinline__ void block_add_n(double v, double *dst) {
+  __shared__ double red[NT / 32];
+  v = warp_sum<double>(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < NT / 32; ++w) t += red[w];
+    atomicAdd(dst, t);
   }
 }
 
@@ -2036,63 +2061,73 @@ __device__ __forceinline__ bool lp_skip(int act, const CGSys &G) {
 }
 
 // Inner start: z = alpha r, rr = r - A_loc(alpha r) = -sum T (alpha r)_k, zz = alpha rr (the first
-// inner direction), partial rr . zz.
+// inner direction), partial rr . zz.  LP_LANES threads per atom; lane q writes the q-th vector.
 template <typename T, int ACT>
-__global__ void k_lp_start(Dev<T> a) {
+__global__ void __launch_bounds__(LP_THREADS) k_lp_start(Dev<T> a) {
   pdl_enter();
   const int s = a.tb_sys[blockIdx.x];
   CGSys &G = a.cg[s];
   if (lp_skip(ACT, G)) return;  // uniform over the block
-  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const int q = threadIdx.x % LP_LANES;
+  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x / LP_LANES;
   const SysInfo &S = a.sys[s];
+  const bool valid = i < S.atom0 + S.natom;
+  T f0 = 0, f1 = 0, f2 = 0;
+  short_sum(a, i, valid ? a.sh_n[i] : 0, q, [&](int k) {
+    const v4<T> r = a.R[k];
+    const T al = a.alpha[k];
+    v4<T> w;
+    w.x = al * r.x; w.y = al * r.y; w.z = al * r.z; w.w = T(0);
+    return w;
+  }, f0, f1, f2);
   double rz = 0.0;
-  if (i < S.atom0 + S.natom) {
-    T f0 = 0, f1 = 0, f2 = 0;
-    short_sum(a, i, [&](int k) {
-      const v4<T> r = a.R[k];
-      const T al = a.alpha[k];
-      v4<T> w;
-      w.x = al * r.x; w.y = al * r.y; w.z = al * r.z; w.w = T(0);
-      return w;
-    }, f0, f1, f2);
-    const v4<T> r = a.R[i];
+  if (valid) {
     const T al = a.alpha[i];
-    v4<T> z, rr, zz;
-    z.x = al * r.x; z.y = al * r.y; z.z = al * r.z; z.w = T(0);
+    v4<T> rr, zz;
     rr.x = -f0; rr.y = -f1; rr.z = -f2; rr.w = T(0);
     zz.x = al * rr.x; zz.y = al * rr.y; zz.z = al * rr.z; zz.w = T(0);
-    a.Z[i] = z;
-    a.LRR[i] = rr;
-    a.LZZ[i] = zz;
-    a.LP0[i] = zz;  // the first inner direction (kept: the next direction adds to it)
-    rz = double(rr.x * zz.x) + double(rr.y * zz.y) + double(rr.z * zz.z);
+    if (q == 0) {
+      const v4<T> r = a.R[i];
+      v4<T> z;
+      z.x = al * r.x; z.y = al * r.y; z.z = al * r.z; z.w = T(0);
+      a.Z[i] = z;
+      rz = double(rr.x * zz.x) + double(rr.y * zz.y) + double(rr.z * zz.z);
+    } else if (q == 1) {
+      a.LRR[i] = rr;
+    } else if (q == 2) {
+      a.LZZ[i] = zz;
+    } else {
+      a.LP0[i] = zz;  // the first inner direction (kept: the next direction adds to it)
+    }
   }
-  block_add(rz, &G.acc_lrz);
+  block_add_n<LP_THREADS>(rz, &G.acc_lrz);
 }
 
 // Inner direction and its product: p = zz (FIRST) or zz + lb p_prev (written to Pout), Ap =
-// A_loc(p) into AP (the neighbours' p formed the same way), partial p . Ap.
+// A_loc(p) into AP (the neighbours' p formed the same way), partial p . Ap.  LP_LANES threads per atom.
 template <typename T, int ACT, bool FIRST>
-__global__ void k_lp_ap(Dev<T> a, const v4<T> *__restrict__ Pin, v4<T> *__restrict__ Pout) {
+__global__ void __launch_bounds__(LP_THREADS) k_lp_ap(Dev<T> a, const v4<T> *__restrict__ Pin, v4<T> *__restrict__ Pout) {
   pdl_enter();
   const int s = a.tb_sys[blockIdx.x];
   CGSys &G = a.cg[s];
   if (lp_skip(ACT, G)) return;
-  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
+  const int q = threadIdx.x % LP_LANES;
+  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x / LP_LANES;
   const SysInfo &S = a.sys[s];
+  const bool valid = i < S.atom0 + S.natom;
   const T b = T(G.lb);
   auto pget = [&](int k) {
     v4<T> p = a.LZZ[k];
     if (!FIRST) {
-      const v4<T> q = Pin[k];
-      p.x += b * q.x; p.y += b * q.y; p.z += b * q.z;
+      const v4<T> u = Pin[k];
+      p.x += b * u.x; p.y += b * u.y; p.z += b * u.z;
     }
     return p;
   };
+  T f0 = 0, f1 = 0, f2 = 0;
+  short_sum(a, i, valid ? a.sh_n[i] : 0, q, pget, f0, f1, f2);
   double pap = 0.0;
-  if (i < S.atom0 + S.natom) {
-    T f0 = 0, f1 = 0, f2 = 0;
-    short_sum(a, i, pget, f0, f1, f2);
+  if (valid && q == 0) {
     const v4<T> p = pget(i);
     const T ia = a.ialpha[i];
     v4<T> ap;
@@ -2101,7 +2136,7 @@ __global__ void k_lp_ap(Dev<T> a, const v4<T> *__restrict__ Pin, v4<T> *__restri
     a.AP[i] = ap;
     pap = double(p.x * ap.x) + double(p.y * ap.y) + double(p.z * ap.z);
   }
-  block_add(pap, &G.acc_lpap);
+  block_add_n<LP_THREADS>(pap, &G.acc_lpap);
 }
 
 // Inner update: z += al p (al = rr.zz / p.Ap); not LAST: rr -= al Ap, zz = alpha rr, partial rr.zz
@@ -2146,13 +2181,13 @@ __global__ void k_lp_step(Dev<T> a, const v4<T> *__restrict__ Pcur, int nsys, do
         }
       }
       if (!LAST) {
-        block_add(v0, &G.acc_lrz2);
+        block_add_n<THREADS_PER_BLOCK>(v0, &G.acc_lrz2);
       } else if (MODE == 0) {
-        block_add(v0, &G.acc_rz);
+        block_add_n<THREADS_PER_BLOCK>(v0, &G.acc_rz);
       } else {
-        block_add(v0, &G.acc_num);
+        block_add_n<THREADS_PER_BLOCK>(v0, &G.acc_num);
         __syncthreads();
-        block_add(v1, &G.acc_rz);
+        block_add_n<THREADS_PER_BLOCK>(v1, &G.acc_rz);
       }
     }
   }
