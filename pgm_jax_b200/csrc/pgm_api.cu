@@ -241,6 +241,7 @@ struct Engine : EngineBase {
   DBuf<float4> nn_bl;  // the graph's permanent field of the last solve (for the change channel)
   DBuf<int> nn_valid;  // nn_bl holds a previous step
   DBuf<float4> nn_e4;  // the learned guess's graph edges per atom (written by the row build)
+  DBuf<float2> nn_g;  // G1, G2 of each edge
   DBuf<int> nn_ne;
   // local preconditioner (set.local_niter > 0): the short entries (entry-major) and their counts,
   // the inner CG's vectors
@@ -308,7 +309,7 @@ struct Engine : EngineBase {
     a.rx = rx.p; a.ry = ry.p; a.rz = rz.p; a.rg0 = rg0.p; a.rg1 = rg1.p; a.rg2 = rg2.p; a.rg3 = rg3.p;
     a.max_count = dmax.p;
     a.mce = mce; a.rnv = split ? rnv.p : nullptr; a.rce2 = rc_e * rc_e;
-    a.nn_e4 = nn_e4.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
+    a.nn_e4 = nn_e4.p; a.nn_g = nn_g.p; a.nn_ne = nn_ne.p; a.nn_emax = NN_EMAX; a.nn_rg2 = nn_rg * nn_rg;
     if (set.local_niter > 0) {
       a.sh_n = sh_n.p; a.sh_max = SH_MAX; a.lc2 = set.local_cut * set.local_cut;
       a.c_k = c_k.p; a.c_x = c_x.p; a.c_y = c_y.p; a.c_z = c_z.p; a.c_g1 = c_g1.p; a.c_g2 = c_g2.p;
@@ -879,7 +880,7 @@ struct Engine : EngineBase {
   // The graph's edge list (allocated with predictor 5, else when a model is installed or the
   // features are asked for).
   void ensure_graph() {
-    if (!nn_e4.p) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
+    if (!nn_e4.p) { nn_e4.alloc((size_t)nt * NN_EMAX); nn_g.alloc((size_t)nt * NN_EMAX); nn_ne.alloc(nt); }
   }
 
   void set_mpnn(const float *w, int nparam, float sigma, float rg) override {
@@ -1196,11 +1197,11 @@ struct Engine : EngineBase {
   template <int ACT, int MODE>
   void local_precond(cudaStream_t st, pgm::Dev<T> &a, cudaGraphConditionalHandle cond, int use_cond) {
     const int L = set.local_niter;
-    launch_pdl(pgm::k_lp_start<T, ACT>, ntblk, pgm::LP_THREADS, 0, st, a);
+    launch_pdl(pgm::k_lp_start<T, ACT>, ntblk, 256, 0, st, a);
     for (int j = 1; j <= L; ++j) {
       pgm::v4<T> *cur = (j & 1) ? LP0.p : LP1.p, *prev = (j & 1) ? LP1.p : LP0.p;
-      if (j == 1) launch_pdl(pgm::k_lp_ap<T, ACT, true>, ntblk, pgm::LP_THREADS, 0, st, a, (const pgm::v4<T> *)prev, cur);
-      else launch_pdl(pgm::k_lp_ap<T, ACT, false>, ntblk, pgm::LP_THREADS, 0, st, a, (const pgm::v4<T> *)prev, cur);
+      if (j == 1) launch_pdl(pgm::k_lp_ap<T, ACT, true>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)prev, cur);
+      else launch_pdl(pgm::k_lp_ap<T, ACT, false>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)prev, cur);
       if (j < L)
         launch_pdl(pgm::k_lp_step<T, ACT, false, MODE>, ntblk, 256, 0, st, a, (const pgm::v4<T> *)cur, nsys, set.dipole_tol,
                    set.max_iter, dany.p, cond, use_cond, cg_done.p);

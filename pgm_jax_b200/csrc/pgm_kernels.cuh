@@ -67,8 +67,10 @@ struct Dev {
   double rce2;
   // the learned guess's graph (the row entries with float(r^2) < nn_rg2): per atom up to nn_emax
   // edges (x, y, z, partner bits) in row order and the full count, written by the row build when
-  // nn_e4 is set (the consumers read the first nn_emax)
+  // nn_e4 is set (the consumers read the first nn_emax), with the pair kernels G1, G2 of each edge
+  // in nn_g (same slots)
   float4 *nn_e4;
+  float2 *nn_g;
   int *nn_ne;
   int nn_emax;
   float nn_rg2;
@@ -537,7 +539,11 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
     const bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
     const unsigned eb = __ballot_sync(0xffffffffu, sh);
     const int at = ecount + __popc(eb & lt);
-    if (sh && at < a.nn_emax) a.nn_e4[(size_t)i * a.nn_emax + at] = make_float4(float(x), float(y), float(z), __int_as_float(j));
+    if (sh && at < a.nn_emax) {
+      const size_t o = (size_t)i * a.nn_emax + at;
+      a.nn_e4[o] = make_float4(float(x), float(y), float(z), __int_as_float(j));
+      a.nn_g[o] = make_float2(float(g1), float(g2));
+    }
     ecount += __popc(eb);
   }
 }
@@ -1561,15 +1567,10 @@ __global__ void __launch_bounds__(256, 8) k_nn_chan(Dev<T> a, const double *hist
   if (i >= S.atom0 + S.natom) return;
   (void)rg;  // the graph radius is a.nn_rg2 here
   float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-  const float Ri = float(a.radius[i]), beta = float(a.beta);
-  for_graph_edges(a, i, [&](int k, float x, float y, float z, int) {
-    // the pair kernels G1, G2 of the edge, evaluated here (not read from the rows) so that this
-    // pass can run beside the row-kernel evaluation
-    const float Rk = float(a.radius[k]), r = sqrtf(x * x + y * y + z * z);
-    float A[4], Bb[4];
-    erf_kernels<float>(rsqrtf(2.f * (Ri * Ri + Rk * Rk)), r, A);
-    erf_kernels<float>(beta, r, Bb);
-    const float g1 = A[1] - Bb[1], g2 = A[2] - Bb[2];
+  const float2 *G = a.nn_g + (size_t)i * a.nn_emax;
+  for_graph_edges(a, i, [&](int k, float x, float y, float z, int e) {
+    const float2 g = G[e];  // the edge's pair kernels G1, G2, as the row build evaluated them
+    const float g1 = g.x, g2 = g.y;
     double4 pk = a.pperm[k];
     float px = float(pk.x), py = float(pk.y), pz = float(pk.z);
     float c = -float(a.q[k]) * g1 - g2 * (px * x + py * y + pz * z);
@@ -1685,23 +1686,33 @@ __global__ void __launch_bounds__(256, 4) k_nn_features(Dev<T> a, const float *c
   if (lane < 4) V[9 + 32 + lane] = tail[lane];
   float sq = mine * mine;
   float n2 = sq + __shfl_down_sync(0xffffffffu, sq, 1) + __shfl_down_sync(0xffffffffu, sq, 2);
-  if (lane < 24 && lane % 3 == 0) F[8 + lane / 3] = asinhf(sqrtf(n2) * is);
-  if (lane != 0) return;
+  // the 16 invariants on 16 lanes at once: F[8 + l / 3] on lanes l = 0, 3, .., 21 (the group norms),
+  // F[l - 24] on lanes 24..31 (the atom's own channels, |mu1|, alpha, radius); V[0..8] the own channels
   const float *ci = chan + (size_t)i * NN_CHAN;
-  float self[3][3] = {{ci[0], ci[1], ci[2]}, {ci[3], ci[4], ci[5]}, {ci[6], ci[7], ci[8]}};
-  const float m1[3] = {ci[9], ci[10], ci[11]};
-  for (int c = 0; c < 3; ++c)
-    for (int x = 0; x < 3; ++x) V[3 * c + x] = self[c][x];
-  auto dot = [](const float *p, const float *q) { return p[0] * q[0] + p[1] * q[1] + p[2] * q[2]; };
-  auto norm3 = [](const float *p) { return sqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]); };
-  F[0] = float(a.alpha[i]) * 1e3f;
-  F[1] = float(a.radius[i]) / 0.06f;
-  F[2] = asinhf(norm3(self[0]) * is);
-  F[3] = norm3(m1) * 50.f;
-  F[4] = asinhf(norm3(self[1]) * is);
-  F[5] = asinhf(norm3(self[2]) * is);
-  F[6] = asinhf(dot(self[0], self[1]) * is2);
-  F[7] = asinhf(dot(self[0], self[2]) * is2);
+  if (lane < 9) V[lane] = ci[lane];
+  float arg = 0.f;
+  bool ash = true;
+  int slot = -1;
+  if (lane < 24) {
+    if (lane % 3 == 0) { arg = sqrtf(n2) * is; slot = 8 + lane / 3; }
+  } else {
+    const float s0[3] = {ci[0], ci[1], ci[2]}, s1[3] = {ci[3], ci[4], ci[5]}, s2[3] = {ci[6], ci[7], ci[8]};
+    const float m1[3] = {ci[9], ci[10], ci[11]};
+    auto dot = [](const float *p, const float *q) { return p[0] * q[0] + p[1] * q[1] + p[2] * q[2]; };
+    auto norm3 = [](const float *p) { return sqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]); };
+    slot = lane - 24;
+    switch (slot) {
+      case 0: arg = float(a.alpha[i]) * 1e3f; ash = false; break;
+      case 1: arg = float(a.radius[i]) / 0.06f; ash = false; break;
+      case 2: arg = norm3(s0) * is; break;
+      case 3: arg = norm3(m1) * 50.f; ash = false; break;
+      case 4: arg = norm3(s1) * is; break;
+      case 5: arg = norm3(s2) * is; break;
+      case 6: arg = dot(s0, s1) * is2; break;
+      default: arg = dot(s0, s2) * is2; break;
+    }
+  }
+  if (slot >= 0) F[slot] = ash ? asinhf(arg) : arg;
 }
 
 template <typename T>
@@ -2000,18 +2011,12 @@ __global__ void k_cg_update_check(Dev<T> a, int nsys, double tol, int max_iter, 
 // started from z = alpha r (forcefield.py:1766-1792; the outer CG is then flexible, with the
 // Polak-Ribiere beta it already uses).  Thread per atom; the short entries compacted entry-major.
 
-// The inner kernels run LP_LANES threads per atom (consecutive lanes; blocks of 256 atoms), each
-// summing every LP_LANES-th short entry, so that more entry gathers are in flight.
-constexpr int LP_LANES = 4;
-constexpr int LP_THREADS = THREADS_PER_BLOCK * LP_LANES;
-
-// sum over atom i's short entries of T v_k (get(k) = v_k), entries q, q + LP_LANES, ... on lane q
-// of the atom's group, then combined over the group (every lane of the warp takes part; an atom
-// past the system's end has n = 0)
+// sum over atom i's short entries of T v_k (get(k) = v_k)
 template <typename T, typename Get>
-__device__ __forceinline__ void short_sum(const Dev<T> &a, int i, int n, int q, Get &&get, T &f0, T &f1, T &f2) {
-#pragma unroll 2
-  for (int e = q; e < n; e += LP_LANES) {
+__device__ __forceinline__ void short_sum(const Dev<T> &a, int i, Get &&get, T &f0, T &f1, T &f2) {
+  const int n = a.sh_n[i];
+#pragma unroll 4
+  for (int e = 0; e < n; ++e) {
     const size_t c = (size_t)e * a.nt + i;
     const T x = a.c_x[c], y = a.c_y[c], z = a.c_z[c], g1 = a.c_g1[c], g2 = a.c_g2[c];
     const v4<T> v = get(a.c_k[c]);
@@ -2019,26 +2024,6 @@ __device__ __forceinline__ void short_sum(const Dev<T> &a, int i, int n, int q, 
     f0 += cc * x + g1 * v.x;
     f1 += cc * y + g1 * v.y;
     f2 += cc * z + g1 * v.z;
-  }
-#pragma unroll
-  for (int o = 1; o < LP_LANES; o <<= 1) {
-    f0 += __shfl_xor_sync(0xffffffffu, f0, o);
-    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
-    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
-  }
-}
-
-// the sum over a block of NT threads of v added to *dst (one atomic per block)
-template <int NT>
-__device__ __forceinline__ void block_add_n(double v, double *dst) {
-  __shared__ double red[NT / 32];
-  v = warp_sum<double>(v);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0;
-    for (int w = 0; w < NT / 32; ++w) t += red[w];
-    atomicAdd(dst, t);
   }
 }
 
@@ -2061,73 +2046,63 @@ __device__ __forceinline__ bool lp_skip(int act, const CGSys &G) {
 }
 
 // Inner start: z = alpha r, rr = r - A_loc(alpha r) = -sum T (alpha r)_k, zz = alpha rr (the first
-// inner direction), partial rr . zz.  LP_LANES threads per atom; lane q writes the q-th vector.
+// inner direction), partial rr . zz.
 template <typename T, int ACT>
-__global__ void __launch_bounds__(LP_THREADS) k_lp_start(Dev<T> a) {
+__global__ void k_lp_start(Dev<T> a) {
   pdl_enter();
   const int s = a.tb_sys[blockIdx.x];
   CGSys &G = a.cg[s];
   if (lp_skip(ACT, G)) return;  // uniform over the block
-  const int q = threadIdx.x % LP_LANES;
-  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x / LP_LANES;
+  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
   const SysInfo &S = a.sys[s];
-  const bool valid = i < S.atom0 + S.natom;
-  T f0 = 0, f1 = 0, f2 = 0;
-  short_sum(a, i, valid ? a.sh_n[i] : 0, q, [&](int k) {
-    const v4<T> r = a.R[k];
-    const T al = a.alpha[k];
-    v4<T> w;
-    w.x = al * r.x; w.y = al * r.y; w.z = al * r.z; w.w = T(0);
-    return w;
-  }, f0, f1, f2);
   double rz = 0.0;
-  if (valid) {
+  if (i < S.atom0 + S.natom) {
+    T f0 = 0, f1 = 0, f2 = 0;
+    short_sum(a, i, [&](int k) {
+      const v4<T> r = a.R[k];
+      const T al = a.alpha[k];
+      v4<T> w;
+      w.x = al * r.x; w.y = al * r.y; w.z = al * r.z; w.w = T(0);
+      return w;
+    }, f0, f1, f2);
+    const v4<T> r = a.R[i];
     const T al = a.alpha[i];
-    v4<T> rr, zz;
+    v4<T> z, rr, zz;
+    z.x = al * r.x; z.y = al * r.y; z.z = al * r.z; z.w = T(0);
     rr.x = -f0; rr.y = -f1; rr.z = -f2; rr.w = T(0);
     zz.x = al * rr.x; zz.y = al * rr.y; zz.z = al * rr.z; zz.w = T(0);
-    if (q == 0) {
-      const v4<T> r = a.R[i];
-      v4<T> z;
-      z.x = al * r.x; z.y = al * r.y; z.z = al * r.z; z.w = T(0);
-      a.Z[i] = z;
-      rz = double(rr.x * zz.x) + double(rr.y * zz.y) + double(rr.z * zz.z);
-    } else if (q == 1) {
-      a.LRR[i] = rr;
-    } else if (q == 2) {
-      a.LZZ[i] = zz;
-    } else {
-      a.LP0[i] = zz;  // the first inner direction (kept: the next direction adds to it)
-    }
+    a.Z[i] = z;
+    a.LRR[i] = rr;
+    a.LZZ[i] = zz;
+    a.LP0[i] = zz;  // the first inner direction (kept: the next direction adds to it)
+    rz = double(rr.x * zz.x) + double(rr.y * zz.y) + double(rr.z * zz.z);
   }
-  block_add_n<LP_THREADS>(rz, &G.acc_lrz);
+  block_add(rz, &G.acc_lrz);
 }
 
 // Inner direction and its product: p = zz (FIRST) or zz + lb p_prev (written to Pout), Ap =
-// A_loc(p) into AP (the neighbours' p formed the same way), partial p . Ap.  LP_LANES threads per atom.
+// A_loc(p) into AP (the neighbours' p formed the same way), partial p . Ap.
 template <typename T, int ACT, bool FIRST>
-__global__ void __launch_bounds__(LP_THREADS) k_lp_ap(Dev<T> a, const v4<T> *__restrict__ Pin, v4<T> *__restrict__ Pout) {
+__global__ void k_lp_ap(Dev<T> a, const v4<T> *__restrict__ Pin, v4<T> *__restrict__ Pout) {
   pdl_enter();
   const int s = a.tb_sys[blockIdx.x];
   CGSys &G = a.cg[s];
   if (lp_skip(ACT, G)) return;
-  const int q = threadIdx.x % LP_LANES;
-  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x / LP_LANES;
+  const int i = a.tb_atom0[blockIdx.x] + threadIdx.x;
   const SysInfo &S = a.sys[s];
-  const bool valid = i < S.atom0 + S.natom;
   const T b = T(G.lb);
   auto pget = [&](int k) {
     v4<T> p = a.LZZ[k];
     if (!FIRST) {
-      const v4<T> u = Pin[k];
-      p.x += b * u.x; p.y += b * u.y; p.z += b * u.z;
+      const v4<T> q = Pin[k];
+      p.x += b * q.x; p.y += b * q.y; p.z += b * q.z;
     }
     return p;
   };
-  T f0 = 0, f1 = 0, f2 = 0;
-  short_sum(a, i, valid ? a.sh_n[i] : 0, q, pget, f0, f1, f2);
   double pap = 0.0;
-  if (valid && q == 0) {
+  if (i < S.atom0 + S.natom) {
+    T f0 = 0, f1 = 0, f2 = 0;
+    short_sum(a, i, pget, f0, f1, f2);
     const v4<T> p = pget(i);
     const T ia = a.ialpha[i];
     v4<T> ap;
@@ -2136,7 +2111,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_lp_ap(Dev<T> a, const v4<T> *__r
     a.AP[i] = ap;
     pap = double(p.x * ap.x) + double(p.y * ap.y) + double(p.z * ap.z);
   }
-  block_add_n<LP_THREADS>(pap, &G.acc_lpap);
+  block_add(pap, &G.acc_lpap);
 }
 
 // Inner update: z += al p (al = rr.zz / p.Ap); not LAST: rr -= al Ap, zz = alpha rr, partial rr.zz
@@ -2181,13 +2156,13 @@ __global__ void k_lp_step(Dev<T> a, const v4<T> *__restrict__ Pcur, int nsys, do
         }
       }
       if (!LAST) {
-        block_add_n<THREADS_PER_BLOCK>(v0, &G.acc_lrz2);
+        block_add(v0, &G.acc_lrz2);
       } else if (MODE == 0) {
-        block_add_n<THREADS_PER_BLOCK>(v0, &G.acc_rz);
+        block_add(v0, &G.acc_rz);
       } else {
-        block_add_n<THREADS_PER_BLOCK>(v0, &G.acc_num);
+        block_add(v0, &G.acc_num);
         __syncthreads();
-        block_add_n<THREADS_PER_BLOCK>(v1, &G.acc_rz);
+        block_add(v1, &G.acc_rz);
       }
     }
   }
