@@ -1636,10 +1636,11 @@ __device__ __forceinline__ float nn_aggregate(const Dev<T> &a, int i, const floa
   float acc[36];
 #pragma unroll
   for (int o = 0; o < 36; ++o) acc[o] = 0.f;
+  const float irg = 1.f / rg;
   for_graph_edges(a, i, [&](int j, float x, float y, float z, int) {
     float r = sqrtf(x * x + y * y + z * z);
     float ir = 1.f / r, u[3] = {x * ir, y * ir, z * ir};
-    float fc = 0.5f * (cospif(r / rg) + 1.f);
+    float fc = 0.5f * (cospif(r * irg) + 1.f);
     float phi[2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
@@ -2590,9 +2591,10 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
       if (a.lj && t >= nsp && ep != T(0)) {  // LJ: not for molecule partners, nor pairs without an LJ term
         T rm = rhi + pk.y;
         T r2 = x * x + y * y + z * z;
-        T s2 = rm * rm / r2, s6 = s2 * s2 * s2;
+        const T ir2 = T(1) / r2;
+        T s2 = rm * rm * ir2, s6 = s2 * s2 * s2;
         el += ep * (s6 * s6 - T(2) * s6);
-        T dl = ep * T(12) * (s6 - s6 * s6) / r2;
+        T dl = ep * T(12) * (s6 - s6 * s6) * ir2;
         gl0 += dl * x; gl1 += dl * y; gl2 += dl * z;
         kx += dl * x; ky += dl * y; kz += dl * z;
       }
@@ -2632,9 +2634,10 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
         T x = a.rx[o], y = a.ry[o], z = a.rz[o];
         T rm = rhi + a.rminh[k], ep = sei * a.seps[k];
         T r2 = x * x + y * y + z * z;
-        T s2 = rm * rm / r2, s6 = s2 * s2 * s2;
+        const T ir2 = T(1) / r2;
+        T s2 = rm * rm * ir2, s6 = s2 * s2 * s2;
         el += ep * (s6 * s6 - T(2) * s6);
-        T dl = ep * T(12) * (s6 - s6 * s6) / r2;
+        T dl = ep * T(12) * (s6 - s6 * s6) * ir2;
         gl0 += dl * x; gl1 += dl * y; gl2 += dl * z;
         T kx = dl * x, ky = dl * y, kz = dl * z;
         w[0] += kx * x; w[1] += kx * y; w[2] += kx * z;
