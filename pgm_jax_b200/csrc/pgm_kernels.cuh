@@ -496,10 +496,28 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
     kv = !special && j >= 0 && a.seps[i] * a.seps[j] != T(0);  // molecule partners have LJ weight 0
     keep = false;
   }
-  unsigned bal = __ballot_sync(0xffffffffu, keep);
+  // the slots first (all lanes take part in the ballots), then one branch for an entry's stores
+  const unsigned bal = __ballot_sync(0xffffffffu, keep);
   const int slot = count + __popc(bal & lt);
-  T g1 = T(0), g2 = T(0);
-  if (keep && slot < a.mce) {
+  count += __popc(bal);
+  const bool kept = keep && slot < a.mce;
+  bool sh = false, ed = false;
+  int at_s = 0, at_e = 0;
+  if (a.sh_n) {  // the local preconditioner's entries: partner, displacement, G1, G2, entry-major
+    sh = kept && r2 < T(a.lc2);
+    const unsigned sb = __ballot_sync(0xffffffffu, sh);
+    at_s = scount + __popc(sb & lt);
+    scount += __popc(sb);
+    sh = sh && at_s < a.sh_max;
+  }
+  if (a.nn_e4) {  // the learned guess's graph edges: the entries closer than rg, with G1, G2
+    ed = kept && float(r2) < a.nn_rg2;
+    const unsigned eb = __ballot_sync(0xffffffffu, ed);
+    at_e = ecount + __popc(eb & lt);
+    ecount += __popc(eb);
+    ed = ed && at_e < a.nn_emax;
+  }
+  if (kept) {
     const size_t o = base + slot;
     a.rk[o] = j;
     a.rx[o] = x; a.ry[o] = y; a.rz[o] = z;
@@ -508,43 +526,29 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
     T A[4], Bb[4];
     erf_kernels<T>(aik, r, A);
     erf_kernels<T>(T(a.beta), r, Bb);
-    g1 = A[1] - Bb[1];
-    g2 = A[2] - Bb[2];
+    const T g1 = A[1] - Bb[1], g2 = A[2] - Bb[2];
     a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = g1; a.rg2[o] = g2; a.rg3[o] = A[3] - Bb[3];
-  }
-  count += __popc(bal);
-  if (a.rnv) {
-    unsigned bv = __ballot_sync(0xffffffffu, kv);
-    const int sv = vcount + __popc(bv & lt);
-    if (kv && sv < a.mc - a.mce) {
-      size_t o = base + a.mce + sv;
-      a.rk[o] = j;
-      a.rx[o] = x; a.ry[o] = y; a.rz[o] = z;
-    }
-    vcount += __popc(bv);
-  }
-  if (a.sh_n) {  // the local preconditioner's entries: partner, displacement, G1, G2, entry-major
-    const bool sh = keep && slot < a.mce && r2 < T(a.lc2);
-    const unsigned sb = __ballot_sync(0xffffffffu, sh);
-    const int at = scount + __popc(sb & lt);
-    if (sh && at < a.sh_max) {
-      const size_t c = (size_t)at * a.nt + i;
+    if (sh) {
+      const size_t c = (size_t)at_s * a.nt + i;
       a.c_k[c] = j;
       a.c_x[c] = x; a.c_y[c] = y; a.c_z[c] = z;
       a.c_g1[c] = g1; a.c_g2[c] = g2;
     }
-    scount += __popc(sb);
-  }
-  if (a.nn_e4) {  // the learned guess's graph edges: the entries closer than rg, with their displacement
-    const bool sh = keep && slot < a.mce && float(r2) < a.nn_rg2;
-    const unsigned eb = __ballot_sync(0xffffffffu, sh);
-    const int at = ecount + __popc(eb & lt);
-    if (sh && at < a.nn_emax) {
-      const size_t o = (size_t)i * a.nn_emax + at;
-      a.nn_e4[o] = make_float4(float(x), float(y), float(z), __int_as_float(j));
-      a.nn_g[o] = make_float2(float(g1), float(g2));
+    if (ed) {
+      const size_t e = (size_t)i * a.nn_emax + at_e;
+      a.nn_e4[e] = make_float4(float(x), float(y), float(z), __int_as_float(j));
+      a.nn_g[e] = make_float2(float(g1), float(g2));
     }
-    ecount += __popc(eb);
+  }
+  if (a.rnv) {
+    const unsigned bv = __ballot_sync(0xffffffffu, kv);
+    const int sv = vcount + __popc(bv & lt);
+    if (kv && sv < a.mc - a.mce) {
+      const size_t o = base + a.mce + sv;
+      a.rk[o] = j;
+      a.rx[o] = x; a.ry[o] = y; a.rz[o] = z;
+    }
+    vcount += __popc(bv);
   }
 }
 
