@@ -2582,14 +2582,16 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
       T dix = di.x * x + di.y * y + di.z * z;
       T dkx = dk.x * x + dk.y * y + dk.z * z;
       T didk = di.x * dk.x + di.y * dk.y + di.z * dk.z;
-      T tt = qi * dkx - qk * dix;
-      ee += qi * qk * G0 + tt * G1 - G2 * dix * dkx + G1 * didk;
-      T radial = -qi * qk * G1 - tt * G2 + G3 * dix * dkx - G2 * didk;
-      T gxv = radial * x + qi * G1 * dk.x - qk * G1 * di.x - G2 * (di.x * dkx + dk.x * dix);
-      T gyv = radial * y + qi * G1 * dk.y - qk * G1 * di.y - G2 * (di.y * dkx + dk.y * dix);
-      T gzv = radial * z + qi * G1 * dk.z - qk * G1 * di.z - G2 * (di.z * dkx + dk.z * dix);
-      T c = -qk * G1 - G2 * dkx;
-      fd0 += c * x + G1 * dk.x; fd1 += c * y + G1 * dk.y; fd2 += c * z + G1 * dk.z;
+      const T qq = qi * qk, pp = dix * dkx;
+      const T tt = qi * dkx - qk * dix;
+      ee += qq * G0 + tt * G1 - G2 * pp + G1 * didk;
+      const T radial = -qq * G1 - tt * G2 + G3 * pp - G2 * didk;
+      // the gradient is radial x + u1 dk - u2 di, the field of (q_k, d_k) G1 dk - u2 x
+      const T u1 = qi * G1 - G2 * dix, u2 = qk * G1 + G2 * dkx;
+      T gxv = radial * x + u1 * dk.x - u2 * di.x;
+      T gyv = radial * y + u1 * dk.y - u2 * di.y;
+      T gzv = radial * z + u1 * dk.z - u2 * di.z;
+      fd0 += G1 * dk.x - u2 * x; fd1 += G1 * dk.y - u2 * y; fd2 += G1 * dk.z - u2 * z;
       T kx = T(KE) * gxv, ky = T(KE) * gyv, kz = T(KE) * gzv;
       T ep = sei * pk.z;
       if (a.lj && t >= nsp && ep != T(0)) {  // LJ: not for molecule partners, nor pairs without an LJ term
