@@ -250,6 +250,8 @@ struct Engine : EngineBase {
   DBuf<T> c_x, c_y, c_z, c_g1, c_g2;
   DBuf<pgm::v4<T>> LRR, LZZ, LP0, LP1, DRv;
   static constexpr int NN_EMAX = 128;
+  // lanes per atom of the spread and the PME gather (32: a warp per atom; 16: two atoms per warp)
+  static constexpr int SPREAD_LPA = 16, GATHER_LPA = 16;
   float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
   int *h_any = nullptr;
   const double *last_pos = nullptr;
@@ -984,7 +986,7 @@ struct Engine : EngineBase {
     CK(cudaEventCreate(&e1));
     auto one = [&]() {
       if (which == 0) pgm::k_rowmat<T, P, false, 1, 0><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
-      else if (which == 1) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
+      else if (which == 1) pgm::k_spread<T, P, false, false, 0, SPREAD_LPA><<<nwblk, 8 * SPREAD_LPA, 0, st>>>(a, Pv.p);
       else if (which == 2) {
         fft_chain(st, a, 0, false);
       } else if (which == 3) forces_pass(st, a, nullptr, false);
@@ -992,14 +994,14 @@ struct Engine : EngineBase {
         pgm::k_rows<T><<<nwblk, 256, 0, st>>>(a);
       }
       else if (which == 5 || which == 6) {  // the first FFT pass (plane or k3), after the spread with 6
-        if (which == 6) pgm::k_spread<T, P, false, false, 0><<<nwblk, 256, 0, st>>>(a, Pv.p);
+        if (which == 6) pgm::k_spread<T, P, false, false, 0, SPREAD_LPA><<<nwblk, 8 * SPREAD_LPA, 0, st>>>(a, Pv.p);
         plane_fwd(st, a, 0);
         for (auto &g : gx)
           with_fft_len(g->K, [&](auto Lc) {
             pgm::k_fft_x_fwd<T, decltype(Lc)::value><<<g->ntiles, pgm::FFT_THREADS, g->smem, st>>>(a, g->sys.p, g->tile0.p, g->ng, 0);
           });
       } else if (which == 7) rowfield<false, 0>(st, a, Pv.p, Fv.p, false);
-      else if (which == 8) pgm::k_rowmat<T, P, false, 1, 0, false><<<nwblk, 256, 0, st>>>(a, Pv.p, AP.p);
+      else if (which == 8) pgm::k_rowmat<T, P, false, 1, 0, false, false, GATHER_LPA><<<nwblk, 8 * GATHER_LPA, 0, st>>>(a, Pv.p, AP.p);
       else if (which == 9) {  // a whole operator sweep with the row/PME overlap
         sweep<false, false, 0, 1>(st, a, Pv.p, AP.p);
       } else if (which == 10) {  // the learned guess's channel pass (rewrites the same graph field)
@@ -1144,7 +1146,7 @@ struct Engine : EngineBase {
   template <bool WITH_Q, bool UPDATE_P, int ACT, bool ENERGY>
   void pme(cudaStream_t st, pgm::Dev<T> &a, const pgm::v4<T> *vin) {
     // Q is zero here: cleared at creation and, after every spread, by the forward k2 FFT pass
-    launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
+    launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT, SPREAD_LPA>, nwblk, 8 * SPREAD_LPA, 0, st, a, vin);
     fft_chain(st, a, ACT, ENERGY);
   }
 
@@ -1157,11 +1159,11 @@ struct Engine : EngineBase {
       // one stream: the row field runs between the spread and the first FFT pass, while the L2
       // still processes the spread's atomic adds, then the FFTs and the PME gather
       // Q is zero here: cleared at creation and, after every spread, by the forward k2 FFT pass
-      pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT><<<nwblk, 256, 0, st>>>(a, vin); check_launch();
+      pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT, SPREAD_LPA><<<nwblk, 8 * SPREAD_LPA, 0, st>>>(a, vin); check_launch();
       const pgm::v4<T> *dv = UPDATE_P ? Pv.p : vin;
       rowfield<WITH_Q, ACT>(st, a, dv, Fv.p, true);
       fft_chain(st, a, ACT, false);
-      launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false>, nwblk, 256, 0, st, a, dv, out);
+      launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false, false, GATHER_LPA>, nwblk, 8 * GATHER_LPA, 0, st, a, dv, out);
       return;
     }
     // the loop body is captured as a sequence of its own: it forks to its own stream
@@ -1174,13 +1176,13 @@ struct Engine : EngineBase {
       CK(cudaStreamWaitEvent(ax, ef, 0));
       rowfield<WITH_Q, ACT>(ax, a, UPDATE_P ? Z.p : vin, Fv.p, false, 0, true);
       CK(cudaEventRecord(ej, ax));
-      launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
+      launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT, SPREAD_LPA>, nwblk, 8 * SPREAD_LPA, 0, st, a, vin);
       fft_chain(st, a, ACT, false);
       CK(cudaStreamWaitEvent(st, ej, 0));
-      launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false, UPDATE_P>, nwblk, 256, 0, st, a, vin, out);
+      launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false, UPDATE_P, GATHER_LPA>, nwblk, 8 * GATHER_LPA, 0, st, a, vin, out);
       return;
     }
-    launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT>, nwblk, 256, 0, st, a, vin);
+    launch_pdl(pgm::k_spread<T, P, WITH_Q, UPDATE_P, ACT, SPREAD_LPA>, nwblk, 8 * SPREAD_LPA, 0, st, a, vin);
     CK(cudaEventRecord(ef, st));
     CK(cudaStreamWaitEvent(ax, ef, 0));
     rowfield<WITH_Q, ACT>(ax, a, vin, Fv.p, false, 0, true);
@@ -1188,7 +1190,7 @@ struct Engine : EngineBase {
     fft_chain(st, a, ACT, false);
     CK(cudaStreamWaitEvent(st, ej, 0));
     // a programmatic dependent of the last FFT pass; griddepcontrol.wait also covers the joined row field
-    launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false>, nwblk, 256, 0, st, a, vin, out);
+    launch_pdl(pgm::k_rowmat<T, P, WITH_Q, MODE, ACT, false, false, GATHER_LPA>, nwblk, 8 * GATHER_LPA, 0, st, a, vin, out);
   }
 
   // The local preconditioner's chain z = M^-1 r (k_lp_start, then per inner iteration k_lp_ap and

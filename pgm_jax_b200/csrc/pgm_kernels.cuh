@@ -621,11 +621,31 @@ __global__ void k_influence(Dev<T> a, long long total) {
 // ------------------------------------------------------------------ spread (pme.py:306-337)
 // One warp per atom, the P^3 stencil over the lanes, atomic adds into the system's grid.  With
 // UPDATE_P the CG direction is first advanced, p = z + beta p (forcefield.py:1812), and spread.
-template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT>
-__global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
+// An atom's group of LPA lanes (32: the warp; 16: a half warp): its shuffle mask, and the sum over
+// it (the warp's own reduction for a whole warp).
+template <int LPA>
+__device__ __forceinline__ unsigned group_mask() {
+  if constexpr (LPA == 32) return 0xffffffffu;
+  else return ((1u << LPA) - 1u) << ((threadIdx.x & 31) & ~(LPA - 1));
+}
+template <typename T, int LPA>
+__device__ __forceinline__ T group_sum(T v, unsigned m) {
+  if constexpr (LPA == 32) {
+    return warp_sum<T>(v);
+  } else {
+#pragma unroll
+    for (int o = LPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o);
+    return v;
+  }
+}
+
+template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT, int LPA = 32>
+__global__ void __launch_bounds__(8 * LPA) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
+  static_assert(LPA == 32 || LPA == 16, "lanes per atom");
   pdl_enter();
-  __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ T sh[WARPS_PER_BLOCK][2][3][P];  // per atom of the block
+  const int warp = threadIdx.x / LPA, lane = threadIdx.x % LPA;  // the atom's group of LPA lanes
+  const unsigned gm = group_mask<LPA>();
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
@@ -638,7 +658,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restric
     v4<T> z = a.Z[i], p = a.P[i];
     T bt = T(a.cg[s].beta);
     d.x = z.x + bt * p.x; d.y = z.y + bt * p.y; d.z = z.z + bt * p.z; d.w = T(0);
-    __syncwarp();
+    __syncwarp(gm);
     if (lane == 0) a.P[i] = d;
   } else {
     d = vin[i];
@@ -652,7 +672,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restric
 #pragma unroll
     for (int k = 0; k < P; ++k) { sh[warp][0][lane][k] = th[k]; sh[warp][1][lane][k] = dth[k]; }
   }
-  __syncwarp();
+  __syncwarp(gm);
   T e[3];
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax)
@@ -666,7 +686,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restric
       // groups of 4 (2.4x fewer L2 atomic operations than one per point); the weight of a point is
       // A(j1, j2) t3 + B(j1, j2) u3 with A = (q t1 + e1 u1) t2 + e2 t1 u2, B = e3 t1 t2.
       const int g0 = b.z >> 2, ng = ((b.z + P - 1) >> 2) - g0 + 1, K34 = K3 >> 2;
-      for (int sl = lane; sl < P * P * ng; sl += 32) {
+      for (int sl = lane; sl < P * P * ng; sl += LPA) {
         int r = ng == 2 ? (sl >> 1) : (ng == 3 ? sl / 3 : sl / ng), gi = sl - r * ng;  // no runtime division for 2, 3
         int j1 = r / P, j2 = r - j1 * P;
         T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2];
@@ -687,7 +707,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev<T> a, const v4<T> *__restric
       return;
     }
   }
-  for (int p = lane; p < P * P * P; p += 32) {
+  for (int p = lane; p < P * P * P; p += LPA) {
     int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
     T t1 = sh[warp][0][0][j1], t2 = sh[warp][0][1][j2], t3 = sh[warp][0][2][j3];
     T u1 = sh[warp][1][0][j1], u2 = sh[warp][1][1][j2], u3 = sh[warp][1][2][j3];
@@ -1378,12 +1398,14 @@ __global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__r
 // ROWS: the row sum is computed here; otherwise it is read from a.F (k_rowfield).  COMBINE (the
 // CG direction's sweep with the row field started before the spread): a.F holds the rows of
 // z, and the rows of p = z + beta p_prev are a.F + beta a.Fp (a.Fp: those of p_prev, rewritten).
-template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true, bool COMBINE = false>
-__global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
+template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true, bool COMBINE = false, int LPA = 32>
+__global__ void __launch_bounds__(8 * LPA) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
+  static_assert(LPA == 32 || LPA == 16, "lanes per atom");
   pdl_enter();
-  __shared__ T sh[WARPS_PER_BLOCK][2][3][P];
+  __shared__ T sh[WARPS_PER_BLOCK][2][3][P];  // per atom of the block
   __shared__ double red[WARPS_PER_BLOCK];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x / LPA, lane = threadIdx.x % LPA;  // the atom's group of LPA lanes
+  const unsigned gm = group_mask<LPA>();
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
@@ -1411,7 +1433,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
       const float4 *x4 = reinterpret_cast<const float4 *>(a.rx + base), *y4 = reinterpret_cast<const float4 *>(a.ry + base),
                    *z4 = reinterpret_cast<const float4 *>(a.rz + base), *p4 = reinterpret_cast<const float4 *>(a.rg1 + base),
                    *q4 = reinterpret_cast<const float4 *>(a.rg2 + base);
-      for (int t4 = lane; 4 * t4 < n; t4 += 32) {
+      for (int t4 = lane; 4 * t4 < n; t4 += LPA) {
         int4 kk = k4[t4];
         float4 xx = x4[t4], yy = y4[t4], zz = z4[t4], g1 = p4[t4], g2 = q4[t4];
         int t = 4 * t4;
@@ -1421,7 +1443,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
         if (t + 3 < n) pair(kk.w, xx.w, yy.w, zz.w, g1.w, g2.w);
       }
     } else {
-      for (int t = lane; t < n; t += 32) {
+      for (int t = lane; t < n; t += LPA) {
         size_t o = base + t;
         pair(a.rk[o], a.rx[o], a.ry[o], a.rz[o], a.rg1[o], a.rg2[o]);
       }
@@ -1435,7 +1457,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
 #pragma unroll
       for (int k = 0; k < P; ++k) { sh[warp][0][lane][k] = th[k]; sh[warp][1][lane][k] = dth[k]; }
     }
-    __syncwarp();
+    __syncwarp(gm);
     const T *phi = a.Phi + S.rgrid0;
     const int K1 = S.K[0], K2 = S.K[1], K3 = S.K[2];
     T g0 = 0, g1 = 0, g2 = 0;
@@ -1445,7 +1467,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
       // 16-byte loads: along k3 the P points of a stencil row fall into ng aligned groups of 4;
       // one work item per (stencil row, group)
       const int g0i = b.z >> 2, ng = ((b.z + P - 1) >> 2) - g0i + 1, K34 = K3 >> 2;
-      for (int sl = lane; sl < P * P * ng; sl += 32) {
+      for (int sl = lane; sl < P * P * ng; sl += LPA) {
         const int r = ng == 2 ? (sl >> 1) : (ng == 3 ? sl / 3 : sl / ng), gi = sl - r * ng;  // no runtime division for 2, 3
         const int j1 = r / P, j2 = r - j1 * P;
         int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
@@ -1468,7 +1490,7 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
         }
       }
     } else {
-      for (int p = lane; p < P * P * P; p += 32) {
+      for (int p = lane; p < P * P * P; p += LPA) {
         int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
         int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
         int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
@@ -1481,8 +1503,8 @@ __global__ void __launch_bounds__(256) k_rowmat(Dev<T> a, const v4<T> *__restric
         g2 += ph * t1 * t2 * u3;
       }
     }
-    if (ROWS) { f0 = warp_sum<T>(f0); f1 = warp_sum<T>(f1); f2 = warp_sum<T>(f2); }
-    g0 = warp_sum<T>(g0); g1 = warp_sum<T>(g1); g2 = warp_sum<T>(g2);
+    if (ROWS) { f0 = group_sum<T, LPA>(f0, gm); f1 = group_sum<T, LPA>(f1, gm); f2 = group_sum<T, LPA>(f2, gm); }
+    g0 = group_sum<T, LPA>(g0, gm); g1 = group_sum<T, LPA>(g1, gm); g2 = group_sum<T, LPA>(g2, gm);
     if (lane == 0) {
       if (!ROWS) { v4<T> fr = a.F[i]; f0 = fr.x; f1 = fr.y; f2 = fr.z; }
       if (COMBINE) {
