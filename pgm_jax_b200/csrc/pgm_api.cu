@@ -250,8 +250,9 @@ struct Engine : EngineBase {
   DBuf<T> c_x, c_y, c_z, c_g1, c_g2;
   DBuf<pgm::v4<T>> LRR, LZZ, LP0, LP1, DRv;
   static constexpr int NN_EMAX = 128;
-  // lanes per atom of the spread and the PME gather (32: a warp per atom; 16: two atoms per warp)
-  static constexpr int SPREAD_LPA = 16, GATHER_LPA = 16;
+  // lanes per atom of the spread, the PME gather and the force pass (32: a warp per atom; 16, 8: two,
+  // four atoms per warp)
+  static constexpr int SPREAD_LPA = 8, GATHER_LPA = 8, FORCES_LPA = 16;
   float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
   int *h_any = nullptr;
   const double *last_pos = nullptr;
@@ -770,11 +771,11 @@ struct Engine : EngineBase {
     auto go = [&](auto B) {
       constexpr int MINB = decltype(B)::value;
       if (shadow) {  // iEL/0-SCF: the shadow potential's energy and forces
-        launch_pdl(pgm::k_forces<T, P, MINB, true>, nwblk, 256, 0, st, a, mu);
+        launch_pdl(pgm::k_forces<T, P, MINB, true, FORCES_LPA>, nwblk, 8 * FORCES_LPA, 0, st, a, mu);
       } else if (pdl) {
-        launch_pdl(pgm::k_forces<T, P, MINB>, nwblk, 256, 0, st, a, mu);
+        launch_pdl(pgm::k_forces<T, P, MINB, false, FORCES_LPA>, nwblk, 8 * FORCES_LPA, 0, st, a, mu);
       } else {
-        pgm::k_forces<T, P, MINB><<<nwblk, 256, 0, st>>>(a, mu);
+        pgm::k_forces<T, P, MINB, false, FORCES_LPA><<<nwblk, 8 * FORCES_LPA, 0, st>>>(a, mu);
         check_launch();
       }
     };

@@ -641,7 +641,7 @@ __device__ __forceinline__ T group_sum(T v, unsigned m) {
 
 template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT, int LPA = 32>
 __global__ void __launch_bounds__(8 * LPA) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
-  static_assert(LPA == 32 || LPA == 16, "lanes per atom");
+  static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
   pdl_enter();
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];  // per atom of the block
   const int warp = threadIdx.x / LPA, lane = threadIdx.x % LPA;  // the atom's group of LPA lanes
@@ -1400,7 +1400,7 @@ __global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__r
 // z, and the rows of p = z + beta p_prev are a.F + beta a.Fp (a.Fp: those of p_prev, rewritten).
 template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true, bool COMBINE = false, int LPA = 32>
 __global__ void __launch_bounds__(8 * LPA) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
-  static_assert(LPA == 32 || LPA == 16, "lanes per atom");
+  static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
   pdl_enter();
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];  // per atom of the block
   __shared__ double red[WARPS_PER_BLOCK];
@@ -2557,12 +2557,14 @@ __global__ void k_iel_finish(Dev<T> a, double *mu, double *hist, double *xl, Iel
 // atoms with the block preconditioner, the i-side delta scaled by a.iel_keep = 1 - 1/omega); their
 // position gradients at fixed delta go to the forces, not to the virial (the fixed-mu strain
 // derivative); the sums of |delta|^2 and |delta|^2 / (2 alpha) go to the energy accumulators.
-template <typename T, int P, int MINB = 3, bool SHADOW = false>
-__global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu) {
+template <typename T, int P, int MINB = 3, bool SHADOW = false, int LPA = 32>
+__global__ void __launch_bounds__(8 * LPA, MINB * 32 / LPA) k_forces(Dev<T> a, const double *mu) {
+  static_assert(LPA == 32 || LPA == 16, "lanes per atom");
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
-  __shared__ T sh[WARPS_PER_BLOCK][3][3][P];
+  __shared__ T sh[WARPS_PER_BLOCK][3][3][P];  // per atom of the block
   __shared__ double red[WARPS_PER_BLOCK][16];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x / LPA, lane = threadIdx.x % LPA;  // the atom's group of LPA lanes
+  const unsigned gm = group_mask<LPA>();
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
@@ -2638,7 +2640,7 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
                    *z4 = reinterpret_cast<const float4 *>(a.rz + base), *h0 = reinterpret_cast<const float4 *>(a.rg0 + base),
                    *h1 = reinterpret_cast<const float4 *>(a.rg1 + base), *h2 = reinterpret_cast<const float4 *>(a.rg2 + base),
                    *h3 = reinterpret_cast<const float4 *>(a.rg3 + base);
-      for (int t4 = lane; 4 * t4 < n; t4 += 32) {
+      for (int t4 = lane; 4 * t4 < n; t4 += LPA) {
         int4 kk = __ldcs(k4 + t4);
         float4 xx = __ldcs(x4 + t4), yy = __ldcs(y4 + t4), zz = __ldcs(z4 + t4);
         float4 a0 = __ldcs(h0 + t4), a1 = __ldcs(h1 + t4), a2 = __ldcs(h2 + t4), a3 = __ldcs(h3 + t4);
@@ -2649,14 +2651,14 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
         if (t + 3 < n) pair(kk.w, xx.w, yy.w, zz.w, a0.w, a1.w, a2.w, a3.w, t + 3);
       }
     } else {
-      for (int t = lane; t < n; t += 32) {
+      for (int t = lane; t < n; t += LPA) {
         size_t o = base + t;
         pair(a.rk[o], a.rx[o], a.ry[o], a.rz[o], a.rg0[o], a.rg1[o], a.rg2[o], a.rg3[o], t);
       }
     }
     if (a.rnv) {  // split rows: the LJ pairs between elec_cutoff and cutoff
       const int nv = min(a.rnv[i], a.mc - a.mce);
-      for (int t = lane; t < nv; t += 32) {
+      for (int t = lane; t < nv; t += LPA) {
         size_t o = base + a.mce + t;
         int k = a.rk[o];
         T x = a.rx[o], y = a.ry[o], z = a.rz[o];
@@ -2682,7 +2684,7 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
 #pragma unroll
       for (int k = 0; k < P; ++k) { sh[warp][0][lane][k] = th[k]; sh[warp][1][lane][k] = dth[k]; sh[warp][2][lane][k] = d2[k]; }
     }
-    __syncwarp();
+    __syncwarp(gm);
     T es[9];
 #pragma unroll
     for (int bb = 0; bb < 3; ++bb)
@@ -2700,7 +2702,7 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
       const T f2 = Dli.x * es[2] + Dli.y * es[5] + Dli.z * es[8];
       const T *phi2 = a.Phi2 + S.rgrid0;
       T h0 = 0, h1 = 0, h2 = 0;
-      for (int p = lane; p < P * P * P; p += 32) {
+      for (int p = lane; p < P * P * P; p += LPA) {
         int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
         int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
         int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
@@ -2718,7 +2720,7 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
       gs1 = gs1 - h0 * es[3] - h1 * es[4] - h2 * es[5];
       gs2 = gs2 - h0 * es[6] - h1 * es[7] - h2 * es[8];
     }
-    for (int p = lane; p < P * P * P; p += 32) {
+    for (int p = lane; p < P * P * P; p += LPA) {
       int j1 = p / (P * P), j2 = (p / P) % P, j3 = p % P;
       int i1 = b.x + j1; if (i1 >= K1) i1 -= K1;
       int i2 = b.y + j2; if (i2 >= K2) i2 -= K2;
@@ -2737,9 +2739,9 @@ __global__ void __launch_bounds__(256, MINB) k_forces(Dev<T> a, const double *mu
     T red_in[24] = {gx0, gx1, gx2, gl0, gl1, gl2, fd0, fd1, fd2, ee, el, ge0, ge1, ge2, gw0, gw1, gw2,
                     w[0], w[1], w[2], w[3], w[4], w[5], w[6]};
 #pragma unroll
-    for (int k = 0; k < 24; ++k) red_in[k] = warp_sum<T>(red_in[k]);
-    T w7 = warp_sum<T>(w[7]), w8 = warp_sum<T>(w[8]);
-    if constexpr (SHADOW) { gs0 = warp_sum<T>(gs0); gs1 = warp_sum<T>(gs1); gs2 = warp_sum<T>(gs2); }
+    for (int k = 0; k < 24; ++k) red_in[k] = group_sum<T, LPA>(red_in[k], gm);
+    T w7 = group_sum<T, LPA>(w[7], gm), w8 = group_sum<T, LPA>(w[8], gm);
+    if constexpr (SHADOW) { gs0 = group_sum<T, LPA>(gs0, gm); gs1 = group_sum<T, LPA>(gs1, gm); gs2 = group_sum<T, LPA>(gs2, gm); }
     if (lane == 0) {
       double gd[3], gr[3];
       for (int bb = 0; bb < 3; ++bb) {
