@@ -387,6 +387,24 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 // from the rounded displacement it stores; with them the local preconditioner's short entries and
 // the learned guess's graph edges.
 
+// An atom's group of LPA lanes (32: the warp; 16, 8: a half, a quarter warp): its shuffle mask, and the sum over
+// it (the warp's own reduction for a whole warp).
+template <int LPA>
+__device__ __forceinline__ unsigned group_mask() {
+  if constexpr (LPA == 32) return 0xffffffffu;
+  else return ((1u << LPA) - 1u) << ((threadIdx.x & 31) & ~(LPA - 1));
+}
+template <typename T, int LPA>
+__device__ __forceinline__ T group_sum(T v, unsigned m) {
+  if constexpr (LPA == 32) {
+    return warp_sum<T>(v);
+  } else {
+#pragma unroll
+    for (int o = LPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o);
+    return v;
+  }
+}
+
 // FP32 sequential minimum image (the mixed-precision row build's candidate loop).
 __device__ __forceinline__ void min_image_fast_f(float &x, float &y, float &z, const float *H, const float *id) {
   float n = rintf(z * id[2]);
@@ -397,13 +415,14 @@ __device__ __forceinline__ void min_image_fast_f(float &x, float &y, float &z, c
   x -= n * H[0];
 }
 
-// The row scan of atom i by one warp: the molecule partners (special = true), then the candidates,
-// one entry per lane and round, the next round's candidate loaded before the current one is tested.
-// visit(keep, j, x, y, z, special) runs on all 32 lanes every round (it may use warp collectives);
+// The row scan of atom i by its group of LPA lanes: the molecule partners (special = true), then the
+// candidates, one entry per lane and round, the next round's candidate loaded before the current one
+// is tested.  visit(keep, j, x, y, z, special) runs on all LPA lanes every round (it may use the
+// group's collectives);
 // keep is r < rc for an entry of another atom, false on lanes without one; the displacement comes
 // as T, as the rows store it.  Mixed precision: the candidates' FP32 displacements from the wrapped
 // FP32 positions (16-byte gathers), the molecule partners' rounded from FP64.
-template <typename T, typename Visit>
+template <typename T, int LPA, typename Visit>
 __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, const BoxInfo &B, int i, int lane, Visit &&visit) {
   double H[9], id[3];
 #pragma unroll
@@ -412,7 +431,7 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
   const double4 pi = a.pos4[i];
   const double rc2 = a.cutoff * a.cutoff;
   const int mf = a.molfirst[i], me = a.molend[i];
-  for (int j0 = mf; j0 < me; j0 += 32) {
+  for (int j0 = mf; j0 < me; j0 += LPA) {
     int j = j0 + lane;
     bool keep = false;
     double x = 0, y = 0, z = 0;
@@ -452,10 +471,10 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
     const float rc2f = float(rc2);
     int jn = partner(lane);
     float4 pn = jn >= 0 ? a.pos4f[jn] : make_float4(0.f, 0.f, 0.f, -1.f);
-    for (int c0 = 0; c0 < nc; c0 += 32) {
+    for (int c0 = 0; c0 < nc; c0 += LPA) {
       const int j = jn;
       const float4 pj = pn;
-      jn = partner(c0 + 32 + lane);  // prefetch the next round
+      jn = partner(c0 + LPA + lane);  // prefetch the next round
       if (jn >= 0) pn = a.pos4f[jn];
       bool keep = false;
       float x = 0.f, y = 0.f, z = 0.f;
@@ -469,10 +488,10 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
   } else {
     int jn = partner(lane);
     double4 pn = jn >= 0 ? a.pos4[jn] : make_double4(0, 0, 0, -1);
-    for (int c0 = 0; c0 < nc; c0 += 32) {
+    for (int c0 = 0; c0 < nc; c0 += LPA) {
       const int j = jn;
       const double4 pj = pn;
-      jn = partner(c0 + 32 + lane);  // prefetch the next round
+      jn = partner(c0 + LPA + lane);  // prefetch the next round
       if (jn >= 0) pn = a.pos4[jn];
       bool keep = false;
       double x = 0, y = 0, z = 0;
@@ -487,9 +506,10 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
 }
 
 template <typename T>
-__device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x, T y, T z, size_t base, int &count, int lane,
+__device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x, T y, T z, size_t base, int &count, unsigned gm,
                                          int i, T Ri, int &ecount, int &vcount, int &scount, bool special) {
-  const unsigned lt = (1u << lane) - 1u;
+  const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;  // the lanes below this one (the group's bits only
+                                                          // are set in its ballots)
   const T r2 = x * x + y * y + z * z;  // the tests below in the rows' precision
   bool kv = false;
   if (a.rnv && keep && !(r2 < T(a.rce2))) {  // split rows: beyond elec_cutoff only pairs with an LJ term stay
@@ -497,7 +517,7 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
     keep = false;
   }
   // the slots first (all lanes take part in the ballots), then one branch for an entry's stores
-  const unsigned bal = __ballot_sync(0xffffffffu, keep);
+  const unsigned bal = __ballot_sync(gm, keep);
   const int slot = count + __popc(bal & lt);
   count += __popc(bal);
   const bool kept = keep && slot < a.mce;
@@ -505,14 +525,14 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
   int at_s = 0, at_e = 0;
   if (a.sh_n) {  // the local preconditioner's entries: partner, displacement, G1, G2, entry-major
     sh = kept && r2 < T(a.lc2);
-    const unsigned sb = __ballot_sync(0xffffffffu, sh);
+    const unsigned sb = __ballot_sync(gm, sh);
     at_s = scount + __popc(sb & lt);
     scount += __popc(sb);
     sh = sh && at_s < a.sh_max;
   }
   if (a.nn_e4) {  // the learned guess's graph edges: the entries closer than rg, with G1, G2
     ed = kept && float(r2) < a.nn_rg2;
-    const unsigned eb = __ballot_sync(0xffffffffu, ed);
+    const unsigned eb = __ballot_sync(gm, ed);
     at_e = ecount + __popc(eb & lt);
     ecount += __popc(eb);
     ed = ed && at_e < a.nn_emax;
@@ -541,7 +561,7 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
     }
   }
   if (a.rnv) {
-    const unsigned bv = __ballot_sync(0xffffffffu, kv);
+    const unsigned bv = __ballot_sync(gm, kv);
     const int sv = vcount + __popc(bv & lt);
     if (kv && sv < a.mc - a.mce) {
       const size_t o = base + a.mce + sv;
@@ -552,10 +572,12 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
+template <typename T, int LPA = 32>
+__global__ void __launch_bounds__(8 * LPA, 6 * 32 / LPA) k_rows(Dev<T> a) {
+  static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x / LPA, lane = threadIdx.x % LPA;  // the atom's group of LPA lanes
+  const unsigned gm = group_mask<LPA>();
   const int s = a.wb_sys[blockIdx.x];
   const int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
@@ -563,8 +585,8 @@ __global__ void __launch_bounds__(256, 6) k_rows(Dev<T> a) {
   const T Ri = a.radius[i];
   const size_t base = (size_t)i * a.mc;
   int count = 0, ecount = 0, vcount = 0, scount = 0, nsp = 0;
-  row_scan(a, S, a.box[s], i, lane, [&](bool keep, int j, T x, T y, T z, bool special) {
-    row_keep<T>(a, keep, j, x, y, z, base, count, lane, i, Ri, ecount, vcount, scount, special);
+  row_scan<T, LPA>(a, S, a.box[s], i, lane, [&](bool keep, int j, T x, T y, T z, bool special) {
+    row_keep<T>(a, keep, j, x, y, z, base, count, gm, i, Ri, ecount, vcount, scount, special);
     if (special) nsp = count;
   });
   if (lane == 0) {
@@ -621,24 +643,6 @@ __global__ void k_influence(Dev<T> a, long long total) {
 // ------------------------------------------------------------------ spread (pme.py:306-337)
 // One warp per atom, the P^3 stencil over the lanes, atomic adds into the system's grid.  With
 // UPDATE_P the CG direction is first advanced, p = z + beta p (forcefield.py:1812), and spread.
-// An atom's group of LPA lanes (32: the warp; 16: a half warp): its shuffle mask, and the sum over
-// it (the warp's own reduction for a whole warp).
-template <int LPA>
-__device__ __forceinline__ unsigned group_mask() {
-  if constexpr (LPA == 32) return 0xffffffffu;
-  else return ((1u << LPA) - 1u) << ((threadIdx.x & 31) & ~(LPA - 1));
-}
-template <typename T, int LPA>
-__device__ __forceinline__ T group_sum(T v, unsigned m) {
-  if constexpr (LPA == 32) {
-    return warp_sum<T>(v);
-  } else {
-#pragma unroll
-    for (int o = LPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o);
-    return v;
-  }
-}
-
 template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT, int LPA = 32>
 __global__ void __launch_bounds__(8 * LPA) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
   static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
