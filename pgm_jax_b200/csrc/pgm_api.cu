@@ -250,9 +250,9 @@ struct Engine : EngineBase {
   DBuf<T> c_x, c_y, c_z, c_g1, c_g2;
   DBuf<pgm::v4<T>> LRR, LZZ, LP0, LP1, DRv;
   static constexpr int NN_EMAX = 128;
-  // lanes per atom of the spread, the PME gather, the force pass and the row build (32: a warp per
-  // atom; 16, 8: two, four atoms per warp)
-  static constexpr int SPREAD_LPA = 8, GATHER_LPA = 8, FORCES_LPA = 16, ROWS_LPA = 32;
+  // lanes per atom of the spread, the PME gather, the force pass, the row build and the learned
+  // guess's channel pass (32: a warp per atom; 16, 8: two, four atoms per warp)
+  static constexpr int SPREAD_LPA = 8, GATHER_LPA = 8, FORCES_LPA = 8, ROWS_LPA = 32, CHAN_LPA = 32;
   float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
   int *h_any = nullptr;
   const double *last_pos = nullptr;
@@ -931,7 +931,7 @@ struct Engine : EngineBase {
   void nn_inputs(cudaStream_t st, pgm::Dev<T> &a, const double *hist, const float4 *bl_prev, const int *valid, float4 *bl_out,
                  float *inv, float *vec, int *set_valid) {
     if (!a.nn_e4) throw CudaError{"the learned guess's graph list is not allocated"};
-    launch_prio(pgm::k_nn_chan<T>, nwblk, 256, 0, st, prio_hi, a, hist, bl_prev, valid, nn_rg, bl_out, nn_chan.p);
+    launch_prio(pgm::k_nn_chan<T, CHAN_LPA>, nwblk, 8 * CHAN_LPA, 0, st, prio_hi, a, hist, bl_prev, valid, nn_rg, bl_out, nn_chan.p);
     launch_prio(pgm::k_nn_features<T>, nwblk, 256, 0, st, prio_hi, a, (const float *)nn_chan.p, nn_sigma, nn_rg, inv, vec,
                 set_valid);
   }
@@ -1006,7 +1006,7 @@ struct Engine : EngineBase {
       else if (which == 9) {  // a whole operator sweep with the row/PME overlap
         sweep<false, false, 0, 1>(st, a, Pv.p, AP.p);
       } else if (which == 10) {  // the learned guess's channel pass (rewrites the same graph field)
-        pgm::k_nn_chan<T><<<nwblk, 256, 0, st>>>(a, last_hist, nn_bl.p, nullptr, nn_rg, nn_bl.p, nn_chan.p);
+        pgm::k_nn_chan<T, CHAN_LPA><<<nwblk, 8 * CHAN_LPA, 0, st>>>(a, last_hist, nn_bl.p, nullptr, nn_rg, nn_bl.p, nn_chan.p);
       } else if (which == 11) {
         pgm::k_nn_features<T><<<nwblk, 256, 0, st>>>(a, nn_chan.p, nn_sigma, nn_rg, nn_inv.p, nn_vec.p, nullptr);
       } else {  // 12: the model

@@ -645,7 +645,7 @@ __global__ void k_influence(Dev<T> a, long long total) {
 // UPDATE_P the CG direction is first advanced, p = z + beta p (forcefield.py:1812), and spread.
 template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT, int LPA = 32>
 __global__ void __launch_bounds__(8 * LPA) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
-  static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
+  static_assert(LPA == 32 || LPA == 16 || LPA == 8 || LPA == 4, "lanes per atom");
   pdl_enter();
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];  // per atom of the block
   const int warp = threadIdx.x / LPA, lane = threadIdx.x % LPA;  // the atom's group of LPA lanes
@@ -1404,7 +1404,7 @@ __global__ void __launch_bounds__(8 * LPR) k_rowfield(Dev<T> a, const v4<T> *__r
 // z, and the rows of p = z + beta p_prev are a.F + beta a.Fp (a.Fp: those of p_prev, rewritten).
 template <typename T, int P, bool WITH_Q, int MODE, int ACT, bool ROWS = true, bool COMBINE = false, int LPA = 32>
 __global__ void __launch_bounds__(8 * LPA) k_rowmat(Dev<T> a, const v4<T> *__restrict__ D, v4<T> *__restrict__ out) {
-  static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
+  static_assert(LPA == 32 || LPA == 16 || LPA == 8 || LPA == 4, "lanes per atom");
   pdl_enter();
   __shared__ T sh[WARPS_PER_BLOCK][2][3][P];  // per atom of the block
   __shared__ double red[WARPS_PER_BLOCK];
@@ -1570,12 +1570,12 @@ __global__ void __launch_bounds__(8 * LPA) k_rowmat(Dev<T> a, const v4<T> *__res
 constexpr int NN_CHAN = 12;
 // The graph edges of atom i from the list the row build wrote, one edge per lane and round (edges past
 // nn_emax are not read, as in the message-passing model).
-template <typename T, typename F>
+template <int LPA = 32, typename T, typename F>
 __device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, F &&edge) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x % LPA;
   const int ne = min(a.nn_ne[i], a.nn_emax);
   const float4 *list = a.nn_e4 + (size_t)i * a.nn_emax;
-  for (int e = lane; e < ne; e += 32) {
+  for (int e = lane; e < ne; e += LPA) {
     const float4 v = list[e];
     edge(__float_as_int(v.w), v.x, v.y, v.z, e);
   }
@@ -1587,10 +1587,12 @@ __device__ __forceinline__ void for_graph_edges(const Dev<T> &a, int i, F &&edge
 // (e nm): c0 = alpha_i (b_i - b_prev,i) (zero when there is no previous b), c1 = mu1 - mu2,
 // c2 = x4 - mu1.  b overwrites b_prev (the same thread reads it first), for the next step.
 // NN_CHAN floats per atom: c0, c1, c2 (3 each) and mu1 (3).
-template <typename T>
-__global__ void __launch_bounds__(256, 8) k_nn_chan(Dev<T> a, const double *hist, const float4 *bl_prev, const int *valid,
-                                                 float rg, float4 *bl_out, float *chan) {
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+template <typename T, int LPA = 32>
+__global__ void __launch_bounds__(8 * LPA, 8 * 32 / LPA) k_nn_chan(Dev<T> a, const double *hist, const float4 *bl_prev,
+                                                                  const int *valid, float rg, float4 *bl_out, float *chan) {
+  static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
+  const int warp = threadIdx.x / LPA, lane = threadIdx.x % LPA;  // the atom's group of LPA lanes
+  const unsigned gm = group_mask<LPA>();
   int s = a.wb_sys[blockIdx.x];
   int i = a.wb_atom0[blockIdx.x] + warp;
   const SysInfo &S = a.sys[s];
@@ -1598,7 +1600,7 @@ __global__ void __launch_bounds__(256, 8) k_nn_chan(Dev<T> a, const double *hist
   (void)rg;  // the graph radius is a.nn_rg2 here
   float f0 = 0.f, f1 = 0.f, f2 = 0.f;
   const float2 *G = a.nn_g + (size_t)i * a.nn_emax;
-  for_graph_edges(a, i, [&](int k, float x, float y, float z, int e) {
+  for_graph_edges<LPA>(a, i, [&](int k, float x, float y, float z, int e) {
     const float2 g = G[e];  // the edge's pair kernels G1, G2, as the row build evaluated them
     const float g1 = g.x, g2 = g.y;
     double4 pk = a.pperm[k];
@@ -1608,7 +1610,7 @@ __global__ void __launch_bounds__(256, 8) k_nn_chan(Dev<T> a, const double *hist
     f1 += c * y + g1 * py;
     f2 += c * z + g1 * pz;
   });
-  f0 = -warp_sum<float>(f0); f1 = -warp_sum<float>(f1); f2 = -warp_sum<float>(f2);
+  f0 = -group_sum<float, LPA>(f0, gm); f1 = -group_sum<float, LPA>(f1, gm); f2 = -group_sum<float, LPA>(f2, gm);
   if (lane >= 3) return;
   // lanes 0..2 write one component each
   const float fb = lane == 0 ? f0 : (lane == 1 ? f1 : f2);
@@ -2563,7 +2565,7 @@ __global__ void k_iel_finish(Dev<T> a, double *mu, double *hist, double *xl, Iel
 // derivative); the sums of |delta|^2 and |delta|^2 / (2 alpha) go to the energy accumulators.
 template <typename T, int P, int MINB = 3, bool SHADOW = false, int LPA = 32>
 __global__ void __launch_bounds__(8 * LPA, MINB * 32 / LPA) k_forces(Dev<T> a, const double *mu) {
-  static_assert(LPA == 32 || LPA == 16, "lanes per atom");
+  static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
   __shared__ T sh[WARPS_PER_BLOCK][3][3][P];  // per atom of the block
   __shared__ double red[WARPS_PER_BLOCK][16];
