@@ -250,10 +250,10 @@ PgmStatus pgm_set_nn_model(PgmHandle *h, const float *weights, float sigma, floa
 /* ------------------------------------------------------------------ autotuner
  * No counterpart in the reference (XLA chooses its own fusions).  The kernel variants of a handle:
  * rowfield_lanes, the lanes that share one neighbour row in the CG matvec's row stream (32: a warp
- * per atom; 16, 8: two or four atoms per warp); forces_blocks_per_sm, the minimum resident blocks of
- * 256 threads the force pass is compiled for (2, 3, 4: registers against warps); sweep_early, the
+ * per atom; 16, 8: two or four atoms per warp); forces_blocks_per_sm, the force pass's register
+ * budget, as resident blocks of 256 threads per SM (2, 3, 4: registers against warps); sweep_early, the
  * order of the CG sweep's concurrent parts; rowfield_grid, the row field beside the FFT chain on
- * every SM (0) or on 1 or 2 blocks per SM at the highest priority, the FFT passes filling the rest
+ * every SM (0) or on 4 or 8 blocks per SM (1, 2) at the highest priority, the FFT passes filling the rest
  * of each SM.  Unless fixed by
  * pgm_set_tuning, the first pgm_compute that is not being captured times every variant on its own
  * rows (CUDA events on its stream, the mean of 10 launches after one) and keeps the fastest;
@@ -270,7 +270,7 @@ typedef struct {
                                   (on p), 1 at the start of the sweep (on z; the rows of p = z +
                                   beta p_prev combined in the gather) */
     double sweep_ms[2];        /* timed sweeps of the two schedules [ms] */
-    int rowfield_grid;         /* 0 (one block per 8 rows), 1 or 2 blocks per SM beside the FFT chain */
+    int rowfield_grid;         /* 0 (one block per 8 rows), 1 or 2: 4 or 8 blocks per SM beside the FFT chain */
     double grid_ms[3];         /* timed sweeps with rowfield_grid 0, 1, 2 [ms] */
 } PgmTuning;
 PgmStatus pgm_tuning(PgmHandle *h, PgmTuning *out);

@@ -754,9 +754,9 @@ struct Engine : EngineBase {
       constexpr int LPR = decltype(L)::value;
       if (pdl) {
         launch_pdl(pgm::k_rowfield<T, WITH_Q, ACT, LPR>, nwblk, 8 * LPR, 0, st, a, vin, out, nwblk);
-      } else if (beside && g > 0) {
-        launch_prio(pgm::k_rowfield<T, WITH_Q, ACT, LPR>, (unsigned)std::min(nwblk, g * nsm), 8 * LPR, 0, st, prio_hi, a,
-                    vin, out, nwblk);
+      } else if (beside && g > 0) {  // variant g: 4 g blocks per SM, walking the rows at the grid's stride
+        launch_prio(pgm::k_rowfield<T, WITH_Q, ACT, LPR>, (unsigned)std::min(nwblk, 4 * g * nsm), 8 * LPR, 0, st, prio_hi,
+                    a, vin, out, nwblk);
       } else {
         pgm::k_rowfield<T, WITH_Q, ACT, LPR><<<nwblk, 8 * LPR, 0, st>>>(a, vin, out, nwblk);
         check_launch();
@@ -842,7 +842,7 @@ struct Engine : EngineBase {
         tune.sweep_ms[v] = time([&] { sweep<false, true, 0, 1>(st, a, Pv.p, AP.p); });
       }
       tune.sweep_early = tune.sweep_ms[1] < tune.sweep_ms[0] ? 1 : 0;
-      // the row field beside the FFT chain on all SMs, or on 1 or 2 blocks per SM at the highest
+      // the row field beside the FFT chain on all SMs, or on 4 or 8 blocks per SM at the highest
       // priority (the FFT passes fill the rest of each SM)
       int bg = 0;
       for (int v = 0; v < 3; ++v) {
