@@ -641,8 +641,10 @@ __global__ void k_influence(Dev<T> a, long long total) {
 }
 
 // ------------------------------------------------------------------ spread (pme.py:306-337)
-// One warp per atom, the P^3 stencil over the lanes, atomic adds into the system's grid.  With
-// UPDATE_P the CG direction is first advanced, p = z + beta p (forcefield.py:1812), and spread.
+// A group of LPA lanes per atom (a warp, or 16 / 8 lanes: two or four atoms per warp, whose B-spline
+// weights, stencil rounds and tails proceed together), the P^3 stencil over the group's lanes, atomic
+// adds into the system's grid.  With UPDATE_P the CG direction is first advanced, p = z + beta p
+// (forcefield.py:1812), and spread.
 template <typename T, int P, bool WITH_Q, bool UPDATE_P, int ACT, int LPA = 32>
 __global__ void __launch_bounds__(8 * LPA) k_spread(Dev<T> a, const v4<T> *__restrict__ vin) {
   static_assert(LPA == 32 || LPA == 16 || LPA == 8 || LPA == 4, "lanes per atom");
@@ -1312,7 +1314,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(Dev<T> a, const int *gsys, c
 }
 
 // ------------------------------------------------------------------ row field + PME gather
-// One warp per atom.  s_i = sum_k de_ik/dd_i (forcefield.py:1395-1402) + dU_rec/dd_i
+// One warp (or group of LPA lanes) per atom.  s_i = sum_k de_ik/dd_i (forcefield.py:1395-1402) + dU_rec/dd_i
 // (pme.py:378-388), then by MODE:
 //   0 FIELD  out = -(s - c_self d)                       (forcefield.py:1428-1433)
 //   1 OPER   out = d / alpha + s - c_self d, and p.Ap    (forcefield.py:1694-1712, 1806-1807)
@@ -2554,7 +2556,7 @@ __global__ void k_iel_finish(Dev<T> a, double *mu, double *hist, double *xl, Iel
 }
 
 // ------------------------------------------------------------------ energy, forces, virial
-// One warp per atom over its row: pair energies and their row gradients with the analytic
+// One group of LPA lanes per atom over its row: pair energies and their row gradients with the analytic
 // kernels G0..G3 (forcefield.py:2294-2360), LJ rows, the row field at (q, d) (dE/dd), the pair
 // virial sum g (x) x - gx (x) off; then the PME gradients of the atom: dU/dd and dU/dr through the
 // spline derivatives (the autodiff of pme.py:390-411 written out).
