@@ -253,6 +253,8 @@ struct Engine : EngineBase {
   // lanes per atom of the spread, the PME gather, the force pass, the row build and the learned
   // guess's channel pass (32: a warp per atom; 16, 8: two, four atoms per warp)
   static constexpr int SPREAD_LPA = 8, GATHER_LPA = 8, FORCES_LPA = 8, ROWS_LPA = 32, CHAN_LPA = 32;
+  // the row build evaluates the kernels after its scan (true) or in it, on the keeping lanes (false)
+  static constexpr bool ROWS_TWO_PHASE = true;
   float nn_sigma = 2e-4f, nn_rg = 0.5f;  // until pgm_set_nn_model
   int *h_any = nullptr;
   const double *last_pos = nullptr;
@@ -992,7 +994,7 @@ struct Engine : EngineBase {
         fft_chain(st, a, 0, false);
       } else if (which == 3) forces_pass(st, a, nullptr, false);
       else if (which == 4) {
-        pgm::k_rows<T, ROWS_LPA><<<nwblk, 8 * ROWS_LPA, 0, st>>>(a);
+        pgm::k_rows<T, ROWS_LPA, ROWS_TWO_PHASE><<<nwblk, 8 * ROWS_LPA, 0, st>>>(a);
       }
       else if (which == 5 || which == 6) {  // the first FFT pass (plane or k3), after the spread with 6
         if (which == 6) pgm::k_spread<T, P, false, false, 0, SPREAD_LPA><<<nwblk, 8 * SPREAD_LPA, 0, st>>>(a, Pv.p);
@@ -1121,7 +1123,7 @@ struct Engine : EngineBase {
                  nb_builds.p);
       launch_pdl(pgm::k_nb_lower, 1, 1, 0, st, nb_flag.p, nb_builds.p);
     }
-    launch_pdl(pgm::k_rows<T, ROWS_LPA>, nwblk, 8 * ROWS_LPA, 0, st, a);
+    launch_pdl(pgm::k_rows<T, ROWS_LPA, ROWS_TWO_PHASE>, nwblk, 8 * ROWS_LPA, 0, st, a);
     if (nn_hist) nn_fork(st, a, nn_hist);
     launch_pdl(pgm::k_influence<T>, (int)std::min<long long>(4096, (cgrid + 255) / 256), 256, 0, st, a, (long long)cgrid);
   }

@@ -382,10 +382,10 @@ __global__ void k_nb_lower(int *flag, long long *builds) {
 // k_rows: one warp per atom finds the row -- the molecule partners (always kept inside the cutoff;
 // the rigid special table of md/topology.py:161-178), then the candidates of the Verlet list (or
 // the caller's rows), masked to r < rc (forcefield.py:1140-1195) -- and writes k, x, y, z compacted
-// by ballot, with the radial kernels G_n = B_n[erf(a r)/r] - B_n[erf(beta r)/r]
-// (forcefield.py:1314-1338, kernels.py:76-118) of every entry, evaluated by the lane that keeps it
-// from the rounded displacement it stores; with them the local preconditioner's short entries and
-// the learned guess's graph edges.
+// by ballot; then the same warp evaluates the radial kernels G_n = B_n[erf(a r)/r] -
+// B_n[erf(beta r)/r] (forcefield.py:1314-1338, kernels.py:76-118) of its row's entries from the
+// rounded displacements it stored, every lane busy, and writes with them the local
+// preconditioner's short entries and the learned guess's graph edges.
 
 // An atom's group of LPA lanes (32: the warp; 16, 8: a half, a quarter warp): its shuffle mask, and the sum over
 // it (the warp's own reduction for a whole warp).
@@ -505,7 +505,7 @@ __device__ __forceinline__ void row_scan(const Dev<T> &a, const SysInfo &S, cons
   }
 }
 
-template <typename T>
+template <typename T, bool EVAL>
 __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x, T y, T z, size_t base, int &count, unsigned gm,
                                          int i, T Ri, int &ecount, int &vcount, int &scount, bool special) {
   const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;  // the lanes below this one (the group's bits only
@@ -521,6 +521,13 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
   const int slot = count + __popc(bal & lt);
   count += __popc(bal);
   const bool kept = keep && slot < a.mce;
+  if constexpr (!EVAL) {  // the entry alone; its kernels, short entry and edge follow the scan
+    if (kept) {
+      const size_t o = base + slot;
+      a.rk[o] = j;
+      a.rx[o] = x; a.ry[o] = y; a.rz[o] = z;
+    }
+  } else {
   bool sh = false, ed = false;
   int at_s = 0, at_e = 0;
   if (a.sh_n) {  // the local preconditioner's entries: partner, displacement, G1, G2, entry-major
@@ -560,6 +567,7 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
       a.nn_g[e] = make_float2(float(g1), float(g2));
     }
   }
+  }
   if (a.rnv) {
     const unsigned bv = __ballot_sync(gm, kv);
     const int sv = vcount + __popc(bv & lt);
@@ -572,7 +580,9 @@ __device__ __forceinline__ void row_keep(const Dev<T> &a, bool keep, int j, T x,
   }
 }
 
-template <typename T, int LPA = 32>
+// TWO_PHASE: the scan stores the entries only; then the group evaluates the kernels of its row
+// (read back from L2) with every lane busy, and assigns the short entries and graph edges in row order.
+template <typename T, int LPA = 32, bool TWO_PHASE = false>
 __global__ void __launch_bounds__(8 * LPA, 6 * 32 / LPA) k_rows(Dev<T> a) {
   static_assert(LPA == 32 || LPA == 16 || LPA == 8, "lanes per atom");
   pdl_enter();  // launched as a programmatic dependent of the previous kernel
@@ -586,9 +596,59 @@ __global__ void __launch_bounds__(8 * LPA, 6 * 32 / LPA) k_rows(Dev<T> a) {
   const size_t base = (size_t)i * a.mc;
   int count = 0, ecount = 0, vcount = 0, scount = 0, nsp = 0;
   row_scan<T, LPA>(a, S, a.box[s], i, lane, [&](bool keep, int j, T x, T y, T z, bool special) {
-    row_keep<T>(a, keep, j, x, y, z, base, count, gm, i, Ri, ecount, vcount, scount, special);
+    row_keep<T, !TWO_PHASE>(a, keep, j, x, y, z, base, count, gm, i, Ri, ecount, vcount, scount, special);
     if (special) nsp = count;
   });
+  if constexpr (TWO_PHASE) {
+    __syncwarp(gm);  // the row, stored by the group's lanes, visible to all of them
+    const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+    const int n = min(count, a.mce);
+    const T beta = T(a.beta), lc2 = T(a.lc2);
+    for (int t0 = 0; t0 < n; t0 += LPA) {
+      const int t = t0 + lane;
+      const bool in = t < n;
+      const size_t o = base + (in ? t : 0);
+      const int j = in ? a.rk[o] : 0;
+      const T x = in ? a.rx[o] : T(0), y = in ? a.ry[o] : T(0), z = in ? a.rz[o] : T(0);
+      const T r2 = x * x + y * y + z * z;
+      bool sh = false, ed = false;
+      int at_s = 0, at_e = 0;
+      if (a.sh_n) {  // the local preconditioner's entries: partner, displacement, G1, G2, entry-major
+        sh = in && r2 < lc2;
+        const unsigned sb = __ballot_sync(gm, sh);
+        at_s = scount + __popc(sb & lt);
+        scount += __popc(sb);
+        sh = sh && at_s < a.sh_max;
+      }
+      if (a.nn_e4) {  // the learned guess's graph edges: the entries closer than rg, with G1, G2
+        ed = in && float(r2) < a.nn_rg2;
+        const unsigned eb = __ballot_sync(gm, ed);
+        at_e = ecount + __popc(eb & lt);
+        ecount += __popc(eb);
+        ed = ed && at_e < a.nn_emax;
+      }
+      if (in) {
+        const T r = t_sqrt(r2), Rk = a.radius[j];
+        const T aik = t_rsqrt(T(2) * (Ri * Ri + Rk * Rk));
+        T A[4], Bb[4];
+        erf_kernels<T>(aik, r, A);
+        erf_kernels<T>(beta, r, Bb);
+        const T g1 = A[1] - Bb[1], g2 = A[2] - Bb[2];
+        a.rg0[o] = A[0] - Bb[0]; a.rg1[o] = g1; a.rg2[o] = g2; a.rg3[o] = A[3] - Bb[3];
+        if (sh) {
+          const size_t c = (size_t)at_s * a.nt + i;
+          a.c_k[c] = j;
+          a.c_x[c] = x; a.c_y[c] = y; a.c_z[c] = z;
+          a.c_g1[c] = g1; a.c_g2[c] = g2;
+        }
+        if (ed) {
+          const size_t e = (size_t)i * a.nn_emax + at_e;
+          a.nn_e4[e] = make_float4(float(x), float(y), float(z), __int_as_float(j));
+          a.nn_g[e] = make_float2(float(g1), float(g2));
+        }
+      }
+    }
+  }
   if (lane == 0) {
     a.rn[i] = count;
     a.rnsp[i] = nsp;
