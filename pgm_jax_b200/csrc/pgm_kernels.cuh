@@ -604,12 +604,23 @@ __global__ void __launch_bounds__(8 * LPA, 6 * 32 / LPA) k_rows(Dev<T> a) {
     const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
     const int n = min(count, a.mce);
     const T beta = T(a.beta), lc2 = T(a.lc2);
+    // the next round's entry is loaded before the current one is evaluated
+    auto load = [&](int t, int &j, T &x, T &y, T &z) {
+      const bool in = t < n;
+      const size_t o = base + (in ? t : 0);
+      j = in ? a.rk[o] : 0;
+      x = in ? a.rx[o] : T(0); y = in ? a.ry[o] : T(0); z = in ? a.rz[o] : T(0);
+    };
+    int jn;
+    T xn, yn, zn;
+    load(lane, jn, xn, yn, zn);
     for (int t0 = 0; t0 < n; t0 += LPA) {
       const int t = t0 + lane;
       const bool in = t < n;
       const size_t o = base + (in ? t : 0);
-      const int j = in ? a.rk[o] : 0;
-      const T x = in ? a.rx[o] : T(0), y = in ? a.ry[o] : T(0), z = in ? a.rz[o] : T(0);
+      const int j = jn;
+      const T x = xn, y = yn, z = zn;
+      load(t + LPA, jn, xn, yn, zn);
       const T r2 = x * x + y * y + z * z;
       bool sh = false, ed = false;
       int at_s = 0, at_e = 0;
